@@ -1,0 +1,11 @@
+"""petch_b200 -- B200-native drop-in for petch's per-step 3D etch loop.
+
+The public surface mirrors petch (Domain / SF6O2 / Process / Result, run_etch_3d,
+mc_flux_3d_coupled, Flags, PAR); every stage runs as hand-written sm_100a CUDA kernels in
+libpetchb200.so, reached through a C ABI (include/petch_b200.h) with ctypes.
+"""
+from . import _lib
+from .levelset import (make_trench_3d, reinit_fsm, advect_3d_gpu, reinit_fsm_dev, advect_dev,
+                       seed_field, grid_shape)
+
+__version__ = "0.1.0"

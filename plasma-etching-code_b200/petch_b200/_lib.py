@@ -1,0 +1,81 @@
+"""ctypes binding of libpetchb200.so (the C ABI declared in include/petch_b200.h).
+
+Every call takes raw device pointers; the helpers here turn torch CUDA tensors into pointers and
+raise PetchError on a non-zero status.  There is no CPU fallback: if the library is missing the
+first call raises.
+"""
+import ctypes
+import os
+
+import torch
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libpetchb200.so")
+
+P = ctypes.c_void_p
+I = ctypes.c_int  # noqa: E741
+L = ctypes.c_longlong
+F = ctypes.c_float
+D = ctypes.c_double
+
+# name -> argtypes (restype is int status for all of them)
+SIGNATURES = {
+    "petch_abi_version": [],
+    "petch_last_error": [ctypes.c_char_p, I],
+    "petch_seed_level_set": [P, P, I, I, I, D, D, D, D, D, D, I, P],
+    "petch_advect": [P, P, P, P, P, I, I, I, F, F, I, P],
+    "petch_reinit_eik": [P, P, P, P, I, I, I, D, F, F, I, P],
+}
+
+_lib = None
+
+
+class PetchError(RuntimeError):
+    def __init__(self, status, what, msg):
+        super().__init__(f"{what} failed with status {status}: {msg}")
+        self.status = status
+
+
+def lib():
+    """The loaded library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with petch_b200.build.build()")
+        so = ctypes.CDLL(LIB_PATH)
+        for name, args in SIGNATURES.items():
+            fn = getattr(so, name)
+            fn.argtypes = args
+            fn.restype = ctypes.c_int
+        _lib = so
+    return _lib
+
+
+def last_error():
+    buf = ctypes.create_string_buffer(512)
+    lib().petch_last_error(buf, 512)
+    return buf.value.decode(errors="replace")
+
+
+def call(name, *args):
+    """Invoke `name`; raise PetchError unless it returns PETCH_OK."""
+    rc = getattr(lib(), name)(*args)
+    if rc != 0:
+        raise PetchError(rc, name, last_error())
+    return rc
+
+
+def ptr(t):
+    """Device pointer of a CUDA tensor (None -> NULL)."""
+    if t is None:
+        return None
+    if not t.is_cuda:
+        raise ValueError("expected a CUDA tensor")
+    if not t.is_contiguous():
+        raise ValueError("expected a contiguous tensor")
+    return t.data_ptr()
+
+
+def stream_ptr(stream=None):
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream

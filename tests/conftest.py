@@ -1,0 +1,19 @@
+"""Test configuration: puts the package and the oracle on sys.path and registers the `gpu` mark.
+
+`-m "not gpu"` runs here (no GPU): the oracle against the golden fixtures, host-side logic, and the
+C-ABI library's load/export/argument checks.  `-m gpu` runs on a B200 and compares the CUDA path,
+called through the C ABI, with the oracle.
+"""
+import os
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+for p in (os.path.join(ROOT, "plasma-etching-code_b200"), ROOT):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (runs on the B200 box)")
