@@ -67,9 +67,163 @@ int petch_advect(float* phi, float* tmp, const float* F, const uint8_t* mask,
  * phi_out = sign(phi_in) * min(U, cap) with sign(0) = +1.  big = band + 4 dx and
  * cap = band + dx as the reference computes them (float64, rounded to float32); dx is taken in
  * double so that 1/dx is rounded once, as the reference's host does; n_iter >= 1.
- * phi_in may alias phi_out.  u_a, u_b: scratch of nx*ny*nz floats each. */
+ * phi_in may alias phi_out.  u_a, u_b: scratch of nx*ny*nz floats each.
+ * mode 0 is reinit_fsm exactly.  mode 1 is the stand-in for skfmm.distance on the initial field
+ * (make_trench_3d, petch/threed.py:56): nodes where phi_in == 0 are frozen at distance 0 and stay
+ * 0, as fast marching keeps them on the front. */
 int petch_reinit_eik(const float* phi_in, float* phi_out, float* u_a, float* u_b, int nx,
-                     int ny, int nz, double dx, float big, float cap, int n_iter, void* stream);
+                     int ny, int nz, double dx, float big, float cap, int n_iter, int mode,
+                     void* stream);
+
+
+/* ------------------------------------------------------------------------------------------ */
+/* Surface mesh + BVH (one caller-allocated device buffer, rebuilt each step)                  */
+/* ------------------------------------------------------------------------------------------ */
+
+/* Segments of a mesh buffer, in order (offsets from petch_mesh_layout):
+ *   0 hdr int32[16]: [0] faces F, [1] vertices V, [2] BVH leaves, [3] error bits
+ *     (1 face overflow, 2 vertex overflow, 4 hash full, 8 non-manifold edge), [8..13] root box
+ *   1 vnode f32[3*MV] vertex position / dx     2 verts f32[3*MV] vertex position (um)
+ *   3 faces i32[3*MT] (winding normal points into the gas)    4 tri f32[12*MT] tracer copy
+ *   5 area f32[MT] max(area, 1e-9)   6 normal f32[3*MT]   7 centroid f32[3*MT]
+ *   8 fmask u8[MT] faces_in_mask     9 nbr i32[3*MT] edge neighbours (-1 none)
+ *  10 nbrw f32[3*MT] max(0, n_i.n_j) 11..15 BVH (leaf codes, leaf starts, nodes, links, flags) */
+#define PETCH_MESH_SEGMENTS 16
+
+/* Byte offsets of the segments and the total size of a mesh buffer for the given capacities. */
+int petch_mesh_layout(int max_tris, int max_verts, long long* offsets, int n_offsets,
+                      long long* total_bytes);
+
+/* Scratch bytes petch_mesh_build needs for an (nx, ny, nz) grid. */
+int petch_mesh_scratch_bytes(int nx, int ny, int nz, int max_tris, long long* bytes);
+
+/* Replaces extract_mesh_3d_gpu + faces_in_mask + _edge_adjacency + _smooth_prep_dev + wp.Mesh
+ * (petch/threed.py:62-125, 228-257, 1608-1616, 1674-1675): marching cubes at phi = 0 (phi > 0
+ * solid) emitting faces in Morton order of their cubes, float64 areas / centroids, winding normals,
+ * faces_in_mask(Lx, Ly, sub_top, mask_th, width, hole), edge neighbours with smoothing weights,
+ * and a linear BVH over the surface cubes.  Counts stay on the device (hdr). */
+int petch_mesh_build(const float* phi, int nx, int ny, int nz, double dx, double Lx, double Ly,
+                     double sub_top, double mask_th, double width, int hole, void* mesh,
+                     int max_tris, int max_verts, void* scratch, long long scratch_bytes,
+                     void* stream);
+
+/* ------------------------------------------------------------------------------------------ */
+/* Monte-Carlo flux (Philox4x32-10 streams keyed by (seed, species), counted by ray id)        */
+/* ------------------------------------------------------------------------------------------ */
+
+typedef struct petch_domain {
+    float lx, ly, lz;   /* source plane extent and open top (Lx, Ly, Lz) */
+    float z_src;        /* source plane height, Lz - dx */
+    int periodic;       /* 1: periodic x/y wrap for rays that miss (par['periodic_y']) */
+} petch_domain;
+
+typedef struct petch_ion_params {  /* the float32 arguments of _trace3d_ion_yield */
+    float meanE, sigmaE;
+    float A_sp, Eth_sp, B_sp, A_ie, Eth_ie, A_p, Eth_p;
+    float inflect, minang, n_l, A_en, minE, thrmin, thrmax;
+    float sigma;        /* ion angular spread of the source (par['ion_ang_sigma']) */
+} petch_ion_params;
+
+/* Replaces _gen_source + _trace3d_ion_yield (petch/threed.py:441-458, 599-712): n_ion ions
+ * generated and traced on the device.  tally4 (16-byte aligned float4[max_tris]) receives per
+ * face (sputter, ion-enhanced, passivation, arrival) and ang the cos-weighted arrival; both are
+ * zeroed first.  work: int[2] device words: [0] ray counter (reset by every trace call), [1] error
+ * bits OR-ed by every kernel (1 = traversal bound hit, 2 = active list full) until the caller
+ * clears them. */
+int petch_trace_ions(const void* mesh, int max_tris, int max_verts, const petch_domain* dom,
+                     const petch_ion_params* p, uint32_t seed, int n_ion, float* tally4,
+                     float* ang, int* work, void* stream);
+
+/* Replaces _gen_source + _trace3d_cov_rr (petch/threed.py:441-458, 549-596): n_neu
+ * Russian-roulette neutrals with sticking bare[f] * beta (bare NULL = 1); flux (float[max_tris],
+ * zeroed first) receives the arriving weight.  stream_id separates species / fixed-point
+ * iterations that share a seed. */
+int petch_trace_neutrals(const void* mesh, int max_tris, int max_verts, const petch_domain* dom,
+                         const float* bare, float beta, uint32_t seed, uint32_t stream_id,
+                         int n_neu, float* flux, int* work, void* stream);
+
+/* Replaces _trace3d (petch/threed.py:352-406), the legacy species of mc_flux_3d and the
+ * non-faithful ion of mc_flux_3d_coupled: first-hit / specular ions (ion = 1, source tilt sigma)
+ * or neutrals with fixed sticking and n_reemit diffuse re-emissions; no lateral wrap. */
+int petch_trace_legacy(const void* mesh, int max_tris, int max_verts, const petch_domain* dom,
+                       int ion, float sigma, float sticking, int n_reemit, int specular,
+                       float cos_thr, float eta, uint32_t seed, int n, float* flux, float* angacc,
+                       int* work, void* stream);
+
+/* Replaces extend_velocity_gpu + _extend_kernel (petch/threed.py:1324-1346): Fs = V[nearest face]
+ * on cells with |phi| < band, else 0.  fold_mask = 1: mask cells get -1 (petch_advect's pinned
+ * marker, mask may not be NULL) and band cells with Fs > 0 are appended to active (if not NULL;
+ * count in *n_active, overflow past max_active sets work[1] bit 2). */
+int petch_extend_velocity(const void* mesh, int max_tris, int max_verts, const float* phi,
+                          const uint8_t* mask, int nx, int ny, int nz, double dx, double band,
+                          const float* V, float* Fs, int fold_mask, int* active, int* n_active,
+                          int max_active, int* work, void* stream);
+
+/* Replaces gpu_warmstart_bare + _nearest_face_cov (petch/threed.py:1619-1639): bare[f] =
+ * clip(prev_bare[nearest face of the previous mesh to centroid f], 0, 1), 1 if none. */
+int petch_warmstart(const void* prev_mesh, int prev_max_tris, int prev_max_verts,
+                    const float* prev_bare, const void* mesh, int max_tris, int max_verts,
+                    float* bare, int* work, void* stream);
+
+/* ------------------------------------------------------------------------------------------ */
+/* Per-face post-processing and surface chemistry (float64 arithmetic, float32 arrays)         */
+/* ------------------------------------------------------------------------------------------ */
+
+typedef struct petch_chem_params {
+    double ionFlux, Fflux, Oflux;      /* PAR['ionFlux'], ['Fflux'], ['Oflux'] */
+    double k_sigma, beta_sigma;        /* Belen couplings */
+    double rho, rate_scale;            /* density factor, rate calibration */
+    double fnorm_E, fnorm_O;           /* surface_rate_belen's flux normalisation (default 1) */
+    double s_F, s_O;                   /* Langmuir sticking (surface_rate_langmuir) */
+    double Yie, Ysp, Yp;               /* IED-integrated yields (chemistry._yields) */
+    double B_sp;                       /* sputter angular coefficient */
+    int yield_angular;                 /* 0 = "cosine", 1 = "viennaps" */
+    int chemistry;                     /* 0 = "langmuir", 1 = "belen" */
+} petch_chem_params;
+
+/* Replaces _norm_clip + smooth_flux_dev (petch/threed.py:165-214, _finish :783-790):
+ * out = clamp((fl / area) * scale, lo, hi) (no clamp if clip == 0), then n_smooth passes of
+ * the 1-neighbour smoothing, each blended with its own input by alpha.  tmp_a, tmp_b: float[MT]. */
+int petch_norm_smooth(const void* mesh, int max_tris, int max_verts, const float* fl, float scale,
+                      float lo, float hi, int clip, int n_smooth, float alpha, float* out,
+                      float* tmp_a, float* tmp_b, void* stream);
+
+/* Replaces the faithful-ion post-processing of mc_flux_3d_coupled (petch/threed.py:814-823):
+ * from petch_trace_ions' tallies, y_sp/y_ie/y_ip = smoothed (tally / area) * norm (the ion
+ * yields, no clip), m_i = smoothed (arrival / area) * norm, cos_i = ang / max(arrival, 1e-9)
+ * where arrival > 0 (unsmoothed).  smooth_flux_gpu semantics: n_smooth passes, one final blend
+ * by alpha.  tmp: float[5 * max_tris]. */
+int petch_ion_post(const void* mesh, int max_tris, int max_verts, const float* tally4,
+                   const float* ang, float norm, int n_smooth, float alpha, float* y_sp, float* y_ie,
+                   float* y_ip, float* m_i, float* cos_i, float* tmp, void* stream);
+
+/* Replaces _cos_k (petch/threed.py:179-185): out = ang / fl where fl > 0, else 0. */
+int petch_cos_ratio(const void* mesh, int max_tris, int max_verts, const float* fl,
+                    const float* ang, float* out, void* stream);
+
+/* Replaces _belen_coverages + the bare update of the fixed point (petch/threed.py:715-737,
+ * 903-904): bare = clip(1 - thetaF - thetaO, 0, 1).  y_ie / y_ip: the faithful-ion yields, or
+ * both NULL for the analytic yields (Yie, Yp with the angular factor of cos_i). */
+int petch_belen_bare(const void* mesh, int max_tris, int max_verts, const petch_chem_params* p,
+                     const float* m_i, const float* m_F, const float* m_O, const float* cos_i,
+                     const float* y_ie, const float* y_ip, float* bare, void* stream);
+
+/* Replaces surface_rate (chemistry.py:83-92 -> belen.py:26-63 / chemistry.py:96-114) and
+ * run_etch_3d's guard (petch/threed.py:1721-1728): V per face, 0 on faces_in_mask faces,
+ * non-finite values zeroed.  stats: int[2] device, [0] = non-finite count, [1] = float bits of
+ * max(V) (for the CFL substep count).  Yields: all three or NULL (analytic). */
+int petch_surface_rate(const void* mesh, int max_tris, int max_verts, const petch_chem_params* p,
+                       const float* m_i, const float* m_F, const float* m_O, const float* cos_i,
+                       const float* y_sp, const float* y_ie, const float* y_ip, float* V,
+                       int* stats, void* stream);
+
+/* petch_advect restricted to a narrow band, with identical results: cells listed in `active`
+ * (F > 0, not mask, from petch_extend_velocity) are updated each substep; mask cells (mask_idx)
+ * are re-pinned to mask_phi after the first substep; every other cell keeps its value.
+ * tmp: nx*ny*nz floats of scratch. */
+int petch_advect_sparse(float* phi, float* tmp, const float* F, const float* mask_phi,
+                        const int* mask_idx, int n_mask, const int* active, int n_active, int nx,
+                        int ny, int nz, float inv_dx, float dt_sub, int nsub, void* stream);
 
 #ifdef __cplusplus
 }

@@ -134,6 +134,9 @@ __device__ __forceinline__ bool frozen(float u) { return signbit(u); }
 
 // _eik_init (threed.py:1455-1479): interface cells (a face neighbour, index-clamped, of opposite
 // sign) get the sub-cell distance min(|phi0| / max(|grad phi0|, 0.5), 1.8 dx) and are frozen.
+// SEED (the skfmm.distance stand-in used for the initial field): nodes where phi0 is exactly 0
+// lie on the front and are frozen at distance 0, as fast marching treats them.
+template <bool SEED>
 __global__ void __launch_bounds__(kBlock) k_eik_init(const float* __restrict__ phi0,
                                                      float* __restrict__ U, Grid g, float inv_dx,
                                                      float big) {
@@ -150,7 +153,9 @@ __global__ void __launch_bounds__(kBlock) k_eik_init(const float* __restrict__ p
         float ozp = phi0[k <= g.nz - 2 ? c + 1 : c];
         bool iface = (v * oxm < 0.0f) || (v * oxp < 0.0f) || (v * oym < 0.0f) ||
                      (v * oyp < 0.0f) || (v * ozm < 0.0f) || (v * ozp < 0.0f);
-        if (iface) {
+        if (SEED && v == 0.0f) {
+            U[c] = -0.0f;
+        } else if (iface) {
             float gx = (oxp - oxm) * 0.5f * inv_dx;
             float gy = (oyp - oym) * 0.5f * inv_dx;
             float gz = (ozp - ozm) * 0.5f * inv_dx;
@@ -166,7 +171,7 @@ __global__ void __launch_bounds__(kBlock) k_eik_init(const float* __restrict__ p
 
 // _eik_jacobi (threed.py:1482-1512); FINAL additionally writes sign(phi_in) * min(U, cap)
 // (reinit_fsm's finalisation, threed.py:1535-1537) instead of U.
-template <bool FINAL>
+template <bool FINAL, bool SEED>
 __global__ void __launch_bounds__(kBlock) k_eik_sweep(const float* __restrict__ Uin,
                                                       float* __restrict__ Uout,
                                                       const float* __restrict__ phi_in,
@@ -194,7 +199,8 @@ __global__ void __launch_bounds__(kBlock) k_eik_sweep(const float* __restrict__ 
         }
         if (FINAL) {
             float s = phi_in[c];
-            phi_out[c] = (s < 0.0f ? -1.0f : 1.0f) * fminf(un, cap);
+            float sg = s < 0.0f ? -1.0f : (SEED && s == 0.0f ? 0.0f : 1.0f);
+            phi_out[c] = sg * fminf(un, cap) + 0.0f;
         } else {
             Uout[c] = un;
         }
@@ -245,7 +251,7 @@ extern "C" int petch_advect(float* phi, float* tmp, const float* F, const uint8_
 
 extern "C" int petch_reinit_eik(const float* phi_in, float* phi_out, float* u_a, float* u_b,
                                 int nx, int ny, int nz, double dx, float big, float cap, int n_iter,
-                                void* stream) {
+                                int mode, void* stream) {
     PETCH_REQUIRE(phi_in && phi_out && u_a && u_b, "petch_reinit_eik: null pointer");
     PETCH_REQUIRE(nx > 0 && ny > 0 && nz > 0 && dx > 0, "petch_reinit_eik: bad grid");
     PETCH_REQUIRE(n_iter >= 1, "petch_reinit_eik: n_iter must be >= 1");
@@ -256,18 +262,23 @@ extern "C" int petch_reinit_eik(const float* phi_in, float* phi_out, float* u_a,
     cudaStream_t st = petch::as_stream(stream);
     int blocks = petch::grid_for(g.n, kBlock);
     const float dxf = (float)dx, inv_dx = (float)(1.0 / dx);
-    k_eik_init<<<blocks, kBlock, 0, st>>>(phi_in, u_a, g, inv_dx, big);
+    PETCH_REQUIRE(mode == 0 || mode == 1, "petch_reinit_eik: mode must be 0 or 1");
+    if (mode == 1) k_eik_init<true><<<blocks, kBlock, 0, st>>>(phi_in, u_a, g, inv_dx, big);
+    else k_eik_init<false><<<blocks, kBlock, 0, st>>>(phi_in, u_a, g, inv_dx, big);
     PETCH_LAUNCH_CHECK("k_eik_init");
     float* a = u_a;
     float* b = u_b;
     for (int it = 0; it < n_iter - 1; ++it) {
-        k_eik_sweep<false><<<blocks, kBlock, 0, st>>>(a, b, nullptr, nullptr, g, dxf, big, cap);
+        k_eik_sweep<false, false><<<blocks, kBlock, 0, st>>>(a, b, nullptr, nullptr, g, dxf, big, cap);
         PETCH_LAUNCH_CHECK("k_eik_sweep");
         float* t = a;
         a = b;
         b = t;
     }
-    k_eik_sweep<true><<<blocks, kBlock, 0, st>>>(a, nullptr, phi_in, phi_out, g, dxf, big, cap);
+    if (mode == 1)
+        k_eik_sweep<true, true><<<blocks, kBlock, 0, st>>>(a, nullptr, phi_in, phi_out, g, dxf, big, cap);
+    else
+        k_eik_sweep<true, false><<<blocks, kBlock, 0, st>>>(a, nullptr, phi_in, phi_out, g, dxf, big, cap);
     PETCH_LAUNCH_CHECK("k_eik_sweep<final>");
     return PETCH_OK;
 }

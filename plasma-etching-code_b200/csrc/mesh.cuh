@@ -1,0 +1,77 @@
+// Device mesh object: one caller-allocated buffer holding the marching-cubes surface, per-face
+// geometry, edge adjacency and the BVH, in a fixed structure-of-arrays layout.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace petch {
+
+enum MeshSeg {
+    SEG_HDR = 0,     // int32[16]: see HDR_* below
+    SEG_VNODE,       // float[3*MV]  vertex position in node-index units (x/dx)
+    SEG_VERTS,       // float[3*MV]  vertex position (um), float32(vnode * dx)
+    SEG_FACES,       // int32[3*MT]  vertex ids, wound so cross(b-a, c-a) points into the gas
+    SEG_TRI,         // float4[3*MT] per-face vertices for the tracer (w unused)
+    SEG_AREA,        // float[MT]    max(area, 1e-9)
+    SEG_NORMAL,      // float[3*MT]  unit winding normal (0 for degenerate faces)
+    SEG_CENTROID,    // float[3*MT]
+    SEG_FMASK,       // uint8[MT]    centroid inside the un-etched mask (faces_in_mask)
+    SEG_NBR,         // int32[3*MT]  face across edge (v0v1, v1v2, v2v0), -1 if none
+    SEG_NBRW,        // float[3*MT]  smoothing weight max(0, n_i . n_j)
+    SEG_LEAF_CODE,   // uint32[MT]   Morton index of the leaf's cube
+    SEG_LEAF_START,  // int32[MT+1]  first face of each leaf (faces of a cube are contiguous)
+    SEG_NODES,       // float4[4*MT] binary BVH internal nodes (two child boxes + links)
+    SEG_PARENT,      // int32[2*MT]  parent link: internal i at [i], leaf l at [MT + l]
+    SEG_FLAGS,       // int32[MT]    refit arrival counters
+    SEG_COUNT
+};
+
+enum MeshHdr {
+    HDR_F = 0,        // faces
+    HDR_V = 1,        // vertices
+    HDR_L = 2,        // BVH leaves (surface cubes)
+    HDR_ERR = 3,      // error bits (MESH_ERR_*)
+    HDR_MT = 4,       // face capacity
+    HDR_MV = 5,       // vertex capacity
+    HDR_NONMANIFOLD = 6,
+    HDR_ROOTBOX = 8   // float[6] at hdr[8..13]: root bounds lo.xyz, hi.xyz
+};
+
+enum MeshErr {
+    MESH_ERR_TRI_OVERFLOW = 1,
+    MESH_ERR_VERT_OVERFLOW = 2,
+    MESH_ERR_HASH_FULL = 4,
+    MESH_ERR_NONMANIFOLD = 8
+};
+
+struct MeshLayout {
+    long long off[SEG_COUNT];
+    long long total;
+};
+
+MeshLayout mesh_layout(int max_tris, int max_verts);
+
+// Typed view of a mesh buffer.
+struct MeshView {
+    int* hdr;
+    float* vnode;
+    float* verts;
+    int* faces;
+    float4* tri;
+    float* area;
+    float* normal;
+    float* centroid;
+    uint8_t* fmask;
+    int* nbr;
+    float* nbrw;
+    uint32_t* leaf_code;
+    int* leaf_start;
+    float4* nodes;
+    int* parent;
+    int* flags;
+    int MT, MV;
+};
+
+MeshView mesh_view(void* base, int max_tris, int max_verts);
+
+}  // namespace petch

@@ -1,0 +1,515 @@
+// Flux kernels: Monte-Carlo ions and Russian-roulette neutrals on the device BVH, plus the
+// nearest-face queries (velocity extension and coverage warm start).
+//
+// Work distribution: persistent lanes with per-lane refill.  A lane whose ray has ended takes the
+// next ray id from a global counter (one atomic per warp per refill), so warps stay full through
+// the long bounce tails of the Russian-roulette and reflected-ion paths instead of idling behind
+// their longest ray.  Sources are generated in-kernel from the ray's Philox stream; there are no
+// origin/direction arrays.
+#include "common.cuh"
+#include "mesh.cuh"
+#include "trace.cuh"
+
+namespace petch {
+namespace {
+
+constexpr int kTB = 128;
+constexpr unsigned kFull = 0xffffffffu;
+
+struct Domain {
+    float lx, ly, lz, z_src;
+    int periodic;
+};
+
+// _apply_bc (threed.py:289-349) fused with the bounce query: with periodic lateral boundaries, a
+// ray that misses the surface and leaves through x or y before the open top re-enters at the
+// opposite face with the same direction (<= 256 wraps, then one last query, as the reference's
+// loop followed by the kernel's own query).  `o` is updated to the origin the hit is measured from.
+__device__ __forceinline__ HitRec query_bc(const MeshView& m, int L, float3& o, float3 d,
+                                           const Domain& D, int* err) {
+    if (!D.periodic) return closest_hit(m, L, make_ray(o, d), 1.0e6f, err);
+    for (int w = 0; w < 256; ++w) {
+        HitRec h = closest_hit(m, L, make_ray(o, d), 1.0e6f, err);
+        if (h.f >= 0) return h;
+        float tx = 1.0e30f, ty = 1.0e30f, tz = 1.0e30f;
+        if (d.x > 1.0e-9f) tx = (D.lx - o.x) / d.x;
+        if (d.x < -1.0e-9f) tx = (0.0f - o.x) / d.x;
+        if (d.y > 1.0e-9f) ty = (D.ly - o.y) / d.y;
+        if (d.y < -1.0e-9f) ty = (0.0f - o.y) / d.y;
+        if (d.z > 1.0e-9f) tz = (D.lz - o.z) / d.z;
+        if (tx < tz && tx < ty && tx > 1.0e-7f) {
+            float hy = o.y + tx * d.y, hz = o.z + tx * d.z;
+            o = make_float3(d.x < 0.0f ? D.lx - 1.0e-4f : 1.0e-4f, hy, hz);
+        } else if (ty < tz && ty < 1.0e29f && ty > 1.0e-7f) {
+            float hx = o.x + ty * d.x, hz = o.z + ty * d.z;
+            o = make_float3(hx, d.y < 0.0f ? D.ly - 1.0e-4f : 1.0e-4f, hz);
+        } else {
+            return h;   // escapes through the open top
+        }
+    }
+    return closest_hit(m, L, make_ray(o, d), 1.0e6f, err);
+}
+
+// _gen_source (threed.py:441-458): origin uniform on [0,Lx]x[0,Ly] at z_src; ion direction from
+// a Gaussian tilt (sigma) in x and y, neutral direction cosine-distributed about -z.
+__device__ __forceinline__ void source(Rng& g, bool ion, float sigma, const Domain& D, float3& o,
+                                       float3& d) {
+    float ox = g.uniform() * D.lx;
+    float oy = g.uniform() * D.ly;
+    o = make_float3(ox, oy, D.z_src);
+    if (ion) {
+        float ax = g.normal() * sigma, ay = g.normal() * sigma;
+        d = make_float3(sinf(ax), sinf(ay), -cosf(ax) * cosf(ay));
+    } else {
+        float r1 = g.uniform(), r2 = g.uniform();
+        float ct = sqrtf(r1), s = sqrtf(1.0f - r1), ph = 6.2831853f * r2;
+        d = make_float3(s * cosf(ph), s * sinf(ph), -ct);
+    }
+    d = normalize3(d);
+}
+
+// Cosine-weighted re-emission about n with the reference's tangent frame (threed.py:584-595).
+__device__ __forceinline__ float3 cosine_emit(Rng& g, float3 n) {
+    float3 a = fabsf(n.x) > 0.9f ? make_float3(0.0f, 1.0f, 0.0f) : make_float3(1.0f, 0.0f, 0.0f);
+    float3 t = normalize3(cross3(a, n));
+    float3 b = cross3(n, t);
+    float r1 = g.uniform(), r2 = g.uniform();
+    float ct = sqrtf(r1), st = sqrtf(1.0f - r1), ph = 6.2831853f * r2;
+    return (st * cosf(ph)) * t + (st * sinf(ph)) * b + ct * n;
+}
+
+// Warp-cooperative refill: lanes with ray == -1 take consecutive ids from *counter.
+__device__ __forceinline__ bool refill(int& ray, int n, int* counter) {
+    const int lane = threadIdx.x & 31;
+    bool need = (ray == -1);
+    unsigned mask = __ballot_sync(kFull, need);
+    if (mask) {
+        int leader = __ffs(mask) - 1;
+        int base = 0;
+        if (lane == leader) base = atomicAdd(counter, __popc(mask));
+        base = __shfl_sync(kFull, base, leader);
+        if (need) {
+            int idx = base + __popc(mask & ((1u << lane) - 1u));
+            ray = idx < n ? idx : -2;
+            return ray >= 0;
+        }
+    }
+    return false;
+}
+
+}  // namespace
+}  // namespace petch
+
+
+namespace petch {
+namespace {
+
+struct IonP {
+    float meanE, sigmaE, A_sp, Eth_sp, B_sp, A_ie, Eth_ie, A_p, Eth_p;
+    float inflect, minang, n_l, A_en, minE, thrmin, thrmax, sigma;
+};
+
+__global__ void k_zero_faces(const int* hdr, int MT, float* a, int na, float* b, int nb) {
+    const int F = min(hdr[HDR_F], MT);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < F * na; i += gridDim.x * blockDim.x) a[i] = 0.0f;
+    if (b)
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < F * nb; i += gridDim.x * blockDim.x) b[i] = 0.0f;
+}
+
+// _trace3d_ion_yield (threed.py:599-712): per ion E ~ N(meanE, sigmaE) clipped at 0; on every hit
+// deposit the yield-weighted sputter / ion-enhanced / passivation rates, the weight and
+// cos * weight; then angle-dependent sticking, energy loss (<= 4 truncated-normal tries),
+// weight reduction and coned-cosine reflection about the specular axis (<= 64 accept-reject
+// draws); at most 1024 bounces.  tal4[f] = (sp, ie, ip, arr), ang[f] = sum cos * w.
+__global__ void __launch_bounds__(kTB) k_ions(MeshView m, Domain D, IonP P, uint32_t seed, int n,
+                                              int* work, float4* __restrict__ tal4,
+                                              float* __restrict__ ang) {
+    const int L = min(m.hdr[HDR_L], m.MT);
+    const float PI_2 = 1.5707963f;
+    const float sEsp = sqrtf(P.Eth_sp), sEie = sqrtf(P.Eth_ie), sEp = sqrtf(P.Eth_p);
+    int err = 0;
+    int ray = -1, bounce = 0;
+    Rng g;
+    float3 o, d;
+    float E = 0.0f, w = 0.0f;
+    while (true) {
+        if (refill(ray, n, work)) {
+            g.init(seed, 0x696f6e73u, (uint32_t)ray);
+            source(g, true, P.sigma, D, o, d);
+            E = P.meanE + P.sigmaE * g.normal();
+            if (E < 0.0f) E = 0.0f;
+            w = 1.0f;
+            bounce = 0;
+        }
+        if (__all_sync(kFull, ray == -2)) break;
+        if (ray < 0) continue;
+        // ---- one bounce ----
+        HitRec h = query_bc(m, L, o, d, D, &err);
+        bool done = true;
+        if (h.f >= 0) {
+            float3 nrm = face_normal(m, h.f);
+            if (dot3(nrm, d) > 0.0f) nrm = -nrm;
+            float cosT = -dot3(d, nrm);
+            cosT = fminf(fmaxf(cosT, 0.0f), 1.0f);
+            float incAng = acosf(cosT);
+            float sqrtE = sqrtf(E);
+            float f_sp = fmaxf((1.0f + P.B_sp * (1.0f - cosT * cosT)) * cosT, 0.0f);
+            float f_ie = 1.0f;
+            if (cosT < 0.5f) f_ie = fmaxf(3.0f - 6.0f * incAng / 3.14159265f, 0.0f);
+            float4 dep = make_float4(P.A_sp * fmaxf(sqrtE - sEsp, 0.0f) * f_sp * w,
+                                     P.A_ie * fmaxf(sqrtE - sEie, 0.0f) * f_ie * w,
+                                     P.A_p * fmaxf(sqrtE - sEp, 0.0f) * f_ie * w, w);
+            atomicAdd(tal4 + h.f, dep);
+            atomicAdd(ang + h.f, cosT * w);
+            float stick = 1.0f;
+            if (incAng > P.thrmin) {
+                float rr = (incAng - P.thrmin) / (P.thrmax - P.thrmin);
+                rr = fminf(fmaxf(rr, 0.0f), 1.0f);
+                stick = 1.0f - rr;
+            }
+            if (stick < 1.0f) {
+                float Eref;
+                if (incAng >= P.inflect)
+                    Eref = 1.0f - (1.0f - P.A_en) * (PI_2 - incAng) / (PI_2 - P.inflect);
+                else
+                    Eref = P.A_en * powf(incAng / P.inflect, P.n_l);
+                float newE = Eref * E;
+                for (int e = 0; e < 4; ++e) {
+                    float cand = Eref * E + 0.1f * E * g.normal();
+                    if (cand >= 0.0f && cand <= E) {
+                        newE = cand;
+                        break;
+                    }
+                }
+                newE = fminf(fmaxf(newE, 0.0f), E);
+                if (newE > P.minE) {
+                    E = newE;
+                    w = w - w * stick;
+                    if (w > 1.0e-4f) {
+                        float3 hit = o + h.t * d;
+                        float3 axis = normalize3(d - (2.0f * dot3(d, nrm)) * nrm);
+                        float3 tt, bb;
+                        if (axis.z < -0.9999999f) {
+                            tt = make_float3(0.0f, -1.0f, 0.0f);
+                            bb = make_float3(-1.0f, 0.0f, 0.0f);
+                        } else {
+                            float aa = 1.0f / (1.0f + axis.z);
+                            float cc = -axis.x * axis.y * aa;
+                            tt = make_float3(1.0f - axis.x * axis.x * aa, cc, -axis.x);
+                            bb = make_float3(cc, 1.0f - axis.y * axis.y * aa, -axis.y);
+                        }
+                        float maxcone = PI_2 - fminf(incAng, P.minang);
+                        float theta = 0.0f;
+                        for (int q = 0; q < 64; ++q) {
+                            float uu = sqrtf(g.uniform());
+                            float ss = sqrtf(fmaxf(1.0f - uu, 0.0f));
+                            theta = maxcone * ss;
+                            if (g.uniform() * theta * uu <= cosf(PI_2 * ss) * sinf(theta)) break;
+                        }
+                        float ph = 6.2831853f * g.uniform();
+                        float st = sinf(theta);
+                        float3 nd = (st * cosf(ph)) * tt + (st * sinf(ph)) * bb + cosf(theta) * axis;
+                        nd = normalize3(nd);
+                        float dn = dot3(nd, nrm);
+                        if (dn <= 0.0f) nd = nd - (2.0f * dn) * nrm;
+                        d = nd;
+                        o = hit + 1.0e-4f * nrm;
+                        done = false;
+                    }
+                }
+            }
+        }
+        if (!done && ++bounce >= 1024) done = true;
+        if (done) ray = -1;
+    }
+    if (err) atomicOr(work + 1, err);
+}
+
+// _trace3d_cov_rr (threed.py:549-596): weighted neutral, deposit the weight on every hit,
+// W *= 1 - bare[f] * beta, stop at W <= 1e-6, Russian roulette below 0.1 (survive with
+// probability W / 0.3 at weight 0.3), cosine re-emission; at most 1024 bounces.
+__global__ void __launch_bounds__(kTB) k_neutrals(MeshView m, Domain D, const float* __restrict__ bare,
+                                                  float beta, uint32_t seed, uint32_t domain, int n,
+                                                  int* work, float* __restrict__ flux) {
+    const int L = min(m.hdr[HDR_L], m.MT);
+    int err = 0;
+    int ray = -1, bounce = 0;
+    Rng g;
+    float3 o, d;
+    float w = 0.0f;
+    while (true) {
+        if (refill(ray, n, work)) {
+            g.init(seed, domain, (uint32_t)ray);
+            source(g, false, 0.0f, D, o, d);
+            w = 1.0f;
+            bounce = 0;
+        }
+        if (__all_sync(kFull, ray == -2)) break;
+        if (ray < 0) continue;
+        HitRec h = query_bc(m, L, o, d, D, &err);
+        bool done = true;
+        if (h.f >= 0) {
+            float3 nrm = face_normal(m, h.f);
+            if (dot3(nrm, d) > 0.0f) nrm = -nrm;
+            atomicAdd(flux + h.f, w);
+            float S = (bare ? __ldg(bare + h.f) : 1.0f) * beta;
+            w = w - w * S;
+            if (w > 1.0e-6f) {
+                bool alive = true;
+                if (w < 0.1f) {
+                    if (g.uniform() < (1.0f - w / 0.3f)) alive = false;
+                    else w = 0.3f;
+                }
+                if (alive) {
+                    float3 hit = o + h.t * d;
+                    d = cosine_emit(g, nrm);
+                    o = hit + 1.0e-4f * nrm;
+                    done = false;
+                }
+            }
+        }
+        if (!done && ++bounce >= 1024) done = true;
+        if (done) ray = -1;
+    }
+    if (err) atomicOr(work + 1, err);
+}
+
+// _trace3d (threed.py:352-406), the legacy first-hit / fixed-re-emission species used when
+// ion_reflection is off: specular == 1 deposits (1 - R) and reflects specularly below cos_thr
+// with energy retention eta; otherwise the particle sticks with probability `sticking` or after
+// n_reemit re-emissions, depositing its weight and weight * cos.
+__global__ void __launch_bounds__(kTB) k_legacy(MeshView m, Domain D, int ion, float sigma,
+                                                float sticking, int n_reemit, int specular,
+                                                float cos_thr, float eta, uint32_t seed,
+                                                uint32_t domain, int n, int* work,
+                                                float* __restrict__ flux, float* __restrict__ angacc) {
+    const int L = min(m.hdr[HDR_L], m.MT);
+    int err = 0;
+    int ray = -1, bounce = 0;
+    Rng g;
+    float3 o, d;
+    float w = 0.0f;
+    Domain Dn = D;
+    Dn.periodic = 0;
+    while (true) {
+        if (refill(ray, n, work)) {
+            g.init(seed, domain, (uint32_t)ray);
+            source(g, ion != 0, sigma, D, o, d);
+            w = 1.0f;
+            bounce = 0;
+        }
+        if (__all_sync(kFull, ray == -2)) break;
+        if (ray < 0) continue;
+        HitRec h = query_bc(m, L, o, d, Dn, &err);
+        bool done = true;
+        if (h.f >= 0) {
+            float3 nrm = face_normal(m, h.f);
+            if (dot3(nrm, d) > 0.0f) nrm = -nrm;
+            float cosang = fmaxf(-dot3(d, nrm), 0.0f);
+            if (specular == 1) {
+                if (cosang >= cos_thr || bounce == n_reemit) {
+                    atomicAdd(flux + h.f, w);
+                    atomicAdd(angacc + h.f, w * cosang);
+                } else {
+                    float R = (cos_thr - cosang) / cos_thr;
+                    float dep = w * (1.0f - R);
+                    atomicAdd(flux + h.f, dep);
+                    atomicAdd(angacc + h.f, dep * cosang);
+                    w = w * R * eta;
+                    float3 hit = o + h.t * d;
+                    d = d - (2.0f * dot3(d, nrm)) * nrm;
+                    o = hit + 1.0e-4f * nrm;
+                    done = false;
+                }
+            } else {
+                float u = g.uniform();
+                if (u < sticking || bounce == n_reemit) {
+                    atomicAdd(flux + h.f, w);
+                    atomicAdd(angacc + h.f, w * cosang);
+                } else {
+                    float3 hit = o + h.t * d;
+                    d = cosine_emit(g, nrm);
+                    o = hit + 1.0e-4f * nrm;
+                    done = false;
+                }
+            }
+        }
+        if (!done && ++bounce > n_reemit) done = true;
+        if (done) ray = -1;
+    }
+    if (err) atomicOr(work + 1, err);
+}
+
+struct GridArgs {
+    int nx, ny, nz;
+    long long plane, n;
+    double dx, band;
+};
+
+// extend_velocity_gpu / _extend_kernel (threed.py:1324-1346): cells with |phi| < band take the
+// velocity of the nearest face (search radius first limited to band + 2 dx, widened to the
+// reference's 1e6 if nothing is found there); all other cells get 0.  With fold != 0, mask cells
+// are written as -1 (the advection's pinned-cell marker) and band cells with F > 0 are listed in
+// `active` for the sparse advection.
+__global__ void __launch_bounds__(kTB) k_extend(MeshView m, GridArgs G, const float* __restrict__ phi,
+                                                const uint8_t* __restrict__ mask,
+                                                const float* __restrict__ V, float* __restrict__ Fs,
+                                                int fold, int* active, int* n_active, int max_active,
+                                                int* work) {
+    const int L = min(m.hdr[HDR_L], m.MT);
+    int err = 0;
+    const float r_near = (float)(G.band + 2.0 * G.dx);
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < G.n;
+         c += (long long)gridDim.x * blockDim.x) {
+        float v = phi[c];
+        bool pinned = fold && mask && mask[c];
+        float out = 0.0f;
+        if ((double)fabsf(v) < G.band) {
+            long long r = c / G.nz;
+            int k = (int)(c - r * G.nz);
+            int i = (int)(r / G.ny);
+            int j = (int)(r - (long long)i * G.ny);
+            float3 p = make_float3((float)(i * G.dx), (float)(j * G.dx), (float)(k * G.dx));
+            int f = nearest_face(m, L, p, r_near * r_near, &err);
+            if (f < 0) f = nearest_face(m, L, p, 1.0e12f, &err);
+            if (f >= 0) out = V[f];
+        }
+        if (pinned) out = -1.0f;
+        Fs[c] = out;
+        if (fold && active && out > 0.0f) {
+            int s = atomicAdd(n_active, 1);
+            if (s < max_active) active[s] = (int)c;
+            else err |= 2;
+        }
+    }
+    if (err) atomicOr(work + 1, err);
+}
+
+// _nearest_face_cov + gpu_warmstart_bare (threed.py:1619-1639): each new face centroid takes
+// the coverage of the nearest face of the previous mesh (1.0 if none), clipped to [0, 1] as
+// mc_flux_3d_coupled does with bare_init.
+__global__ void __launch_bounds__(kTB) k_warmstart(MeshView prev, const float* __restrict__ prev_bare,
+                                                   MeshView cur, float* __restrict__ bare, int* work) {
+    const int Lp = min(prev.hdr[HDR_L], prev.MT);
+    const int F = min(cur.hdr[HDR_F], cur.MT);
+    int err = 0;
+    for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < F; f += gridDim.x * blockDim.x) {
+        float3 p = make_float3(cur.centroid[3 * f], cur.centroid[3 * f + 1], cur.centroid[3 * f + 2]);
+        int q = nearest_face(prev, Lp, p, 1.0e12f, &err);
+        float b = q >= 0 ? prev_bare[q] : 1.0f;
+        bare[f] = fminf(fmaxf(b, 0.0f), 1.0f);
+    }
+    if (err) atomicOr(work + 1, err);
+}
+
+int persistent_blocks(const void* kernel, int block) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0) != cudaSuccess ||
+        per_sm < 1)
+        per_sm = 1;
+    return per_sm * sm_count();
+}
+
+}  // namespace
+}  // namespace petch
+
+using namespace petch;
+
+static Domain to_domain(const petch_domain* d) {
+    Domain D;
+    D.lx = d->lx;
+    D.ly = d->ly;
+    D.lz = d->lz;
+    D.z_src = d->z_src;
+    D.periodic = d->periodic;
+    return D;
+}
+
+extern "C" int petch_trace_ions(const void* mesh, int max_tris, int max_verts,
+                                const petch_domain* dom, const petch_ion_params* p, uint32_t seed,
+                                int n_ion, float* tally4, float* ang, int* work, void* stream) {
+    PETCH_REQUIRE(mesh && dom && p && tally4 && ang && work, "petch_trace_ions: null pointer");
+    PETCH_REQUIRE(n_ion >= 0 && max_tris > 0 && max_verts > 0, "petch_trace_ions: bad size");
+    PETCH_REQUIRE(((uintptr_t)tally4 & 15) == 0, "petch_trace_ions: tally4 must be 16-byte aligned");
+    cudaStream_t st = as_stream(stream);
+    MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
+    IonP P{p->meanE, p->sigmaE, p->A_sp, p->Eth_sp, p->B_sp, p->A_ie, p->Eth_ie, p->A_p, p->Eth_p,
+           p->inflect, p->minang, p->n_l, p->A_en, p->minE, p->thrmin, p->thrmax, p->sigma};
+    k_zero_faces<<<grid_for(4LL * max_tris, 256), 256, 0, st>>>(m.hdr, max_tris, tally4, 4, ang, 1);
+    PETCH_LAUNCH_CHECK("k_zero_faces");
+    PETCH_CUDA(cudaMemsetAsync(work, 0, sizeof(int), st), "reset ray counter");
+    if (n_ion == 0) return PETCH_OK;
+    k_ions<<<persistent_blocks((const void*)k_ions, kTB), kTB, 0, st>>>(
+        m, to_domain(dom), P, seed, n_ion, work, (float4*)tally4, ang);
+    PETCH_LAUNCH_CHECK("k_ions");
+    return PETCH_OK;
+}
+
+extern "C" int petch_trace_neutrals(const void* mesh, int max_tris, int max_verts,
+                                    const petch_domain* dom, const float* bare, float beta,
+                                    uint32_t seed, uint32_t stream_id, int n_neu, float* flux,
+                                    int* work, void* stream) {
+    PETCH_REQUIRE(mesh && dom && flux && work, "petch_trace_neutrals: null pointer");
+    PETCH_REQUIRE(n_neu >= 0 && max_tris > 0 && max_verts > 0, "petch_trace_neutrals: bad size");
+    cudaStream_t st = as_stream(stream);
+    MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
+    k_zero_faces<<<grid_for(max_tris, 256), 256, 0, st>>>(m.hdr, max_tris, flux, 1, nullptr, 0);
+    PETCH_LAUNCH_CHECK("k_zero_faces");
+    PETCH_CUDA(cudaMemsetAsync(work, 0, sizeof(int), st), "reset ray counter");
+    if (n_neu == 0) return PETCH_OK;
+    k_neutrals<<<persistent_blocks((const void*)k_neutrals, kTB), kTB, 0, st>>>(
+        m, to_domain(dom), bare, beta, seed, 0x6e657500u ^ stream_id, n_neu, work, flux);
+    PETCH_LAUNCH_CHECK("k_neutrals");
+    return PETCH_OK;
+}
+
+extern "C" int petch_trace_legacy(const void* mesh, int max_tris, int max_verts,
+                                  const petch_domain* dom, int ion, float sigma, float sticking,
+                                  int n_reemit, int specular, float cos_thr, float eta,
+                                  uint32_t seed, int n, float* flux, float* angacc, int* work,
+                                  void* stream) {
+    PETCH_REQUIRE(mesh && dom && flux && angacc && work, "petch_trace_legacy: null pointer");
+    PETCH_REQUIRE(n >= 0 && n_reemit >= 0 && max_tris > 0 && max_verts > 0,
+                  "petch_trace_legacy: bad size");
+    cudaStream_t st = as_stream(stream);
+    MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
+    k_zero_faces<<<grid_for(max_tris, 256), 256, 0, st>>>(m.hdr, max_tris, flux, 1, angacc, 1);
+    PETCH_LAUNCH_CHECK("k_zero_faces");
+    PETCH_CUDA(cudaMemsetAsync(work, 0, sizeof(int), st), "reset ray counter");
+    if (n == 0) return PETCH_OK;
+    k_legacy<<<persistent_blocks((const void*)k_legacy, kTB), kTB, 0, st>>>(
+        m, to_domain(dom), ion, sigma, sticking, n_reemit, specular, cos_thr, eta, seed,
+        ion ? 0x6c696f6eu : 0x6c6e6575u, n, work, flux, angacc);
+    PETCH_LAUNCH_CHECK("k_legacy");
+    return PETCH_OK;
+}
+
+extern "C" int petch_extend_velocity(const void* mesh, int max_tris, int max_verts,
+                                     const float* phi, const uint8_t* mask, int nx, int ny, int nz,
+                                     double dx, double band, const float* V, float* Fs, int fold_mask,
+                                     int* active, int* n_active, int max_active, int* work,
+                                     void* stream) {
+    PETCH_REQUIRE(mesh && phi && V && Fs && work, "petch_extend_velocity: null pointer");
+    PETCH_REQUIRE(nx > 0 && ny > 0 && nz > 0 && dx > 0, "petch_extend_velocity: bad grid");
+    PETCH_REQUIRE(!fold_mask || !active || n_active, "petch_extend_velocity: n_active is null");
+    cudaStream_t st = as_stream(stream);
+    MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
+    GridArgs G{nx, ny, nz, (long long)ny * nz, (long long)nx * ny * nz, dx, band};
+    if (fold_mask && active) PETCH_CUDA(cudaMemsetAsync(n_active, 0, sizeof(int), st), "memset n_active");
+    k_extend<<<grid_for(G.n, kTB, 16), kTB, 0, st>>>(m, G, phi, mask, V, Fs, fold_mask, active,
+                                                     n_active, max_active, work);
+    PETCH_LAUNCH_CHECK("k_extend");
+    return PETCH_OK;
+}
+
+extern "C" int petch_warmstart(const void* prev_mesh, int prev_max_tris, int prev_max_verts,
+                               const float* prev_bare, const void* mesh, int max_tris,
+                               int max_verts, float* bare, int* work, void* stream) {
+    PETCH_REQUIRE(prev_mesh && prev_bare && mesh && bare && work, "petch_warmstart: null pointer");
+    cudaStream_t st = as_stream(stream);
+    MeshView pm = mesh_view(const_cast<void*>(prev_mesh), prev_max_tris, prev_max_verts);
+    MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
+    k_warmstart<<<grid_for(max_tris, kTB), kTB, 0, st>>>(pm, prev_bare, m, bare, work);
+    PETCH_LAUNCH_CHECK("k_warmstart");
+    return PETCH_OK;
+}

@@ -5,7 +5,9 @@ mc_flux_3d_coupled, Flags, PAR); every stage runs as hand-written sm_100a CUDA k
 libpetchb200.so, reached through a C ABI (include/petch_b200.h) with ctypes.
 """
 from . import _lib
-from .levelset import (make_trench_3d, reinit_fsm, advect_3d_gpu, reinit_fsm_dev, advect_dev,
-                       seed_field, grid_shape)
+from .params import PAR, Flags, DEFAULT_FLAGS
+from .levelset import reinit_fsm, advect_3d_gpu, reinit_fsm_dev, advect_dev, seed_field, grid_shape
+from .threed import (make_trench_3d, run_etch_3d, extract_mesh_3d, center_depth_3d, max_depth_3d,
+                     DeviceMesh, EtchEngine)
 
 __version__ = "0.1.0"

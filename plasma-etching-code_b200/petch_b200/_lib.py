@@ -18,13 +18,54 @@ L = ctypes.c_longlong
 F = ctypes.c_float
 D = ctypes.c_double
 
+U = ctypes.c_uint32
+LLP = ctypes.POINTER(ctypes.c_longlong)
+
+
+class Domain(ctypes.Structure):
+    """petch_domain"""
+    _fields_ = [("lx", F), ("ly", F), ("lz", F), ("z_src", F), ("periodic", I)]
+
+
+class IonParams(ctypes.Structure):
+    """petch_ion_params"""
+    _fields_ = [(n, F) for n in ("meanE", "sigmaE", "A_sp", "Eth_sp", "B_sp", "A_ie", "Eth_ie",
+                                 "A_p", "Eth_p", "inflect", "minang", "n_l", "A_en", "minE",
+                                 "thrmin", "thrmax", "sigma")]
+
+
+class ChemParams(ctypes.Structure):
+    """petch_chem_params"""
+    _fields_ = [(n, D) for n in ("ionFlux", "Fflux", "Oflux", "k_sigma", "beta_sigma", "rho",
+                                 "rate_scale", "fnorm_E", "fnorm_O", "s_F", "s_O", "Yie", "Ysp",
+                                 "Yp", "B_sp")] + [("yield_angular", I), ("chemistry", I)]
+
+
+DP = ctypes.POINTER(Domain)
+IP = ctypes.POINTER(IonParams)
+CP = ctypes.POINTER(ChemParams)
+
 # name -> argtypes (restype is int status for all of them)
 SIGNATURES = {
     "petch_abi_version": [],
     "petch_last_error": [ctypes.c_char_p, I],
     "petch_seed_level_set": [P, P, I, I, I, D, D, D, D, D, D, I, P],
     "petch_advect": [P, P, P, P, P, I, I, I, F, F, I, P],
-    "petch_reinit_eik": [P, P, P, P, I, I, I, D, F, F, I, P],
+    "petch_reinit_eik": [P, P, P, P, I, I, I, D, F, F, I, I, P],
+    "petch_mesh_layout": [I, I, LLP, I, LLP],
+    "petch_mesh_scratch_bytes": [I, I, I, I, LLP],
+    "petch_mesh_build": [P, I, I, I, D, D, D, D, D, D, I, P, I, I, P, L, P],
+    "petch_trace_ions": [P, I, I, DP, IP, U, I, P, P, P, P],
+    "petch_trace_neutrals": [P, I, I, DP, P, F, U, U, I, P, P, P],
+    "petch_trace_legacy": [P, I, I, DP, I, F, F, I, I, F, F, U, I, P, P, P, P],
+    "petch_extend_velocity": [P, I, I, P, P, I, I, I, D, D, P, P, I, P, P, I, P, P],
+    "petch_warmstart": [P, I, I, P, P, I, I, P, P, P],
+    "petch_norm_smooth": [P, I, I, P, F, F, F, I, I, F, P, P, P, P],
+    "petch_ion_post": [P, I, I, P, P, F, I, F, P, P, P, P, P, P, P],
+    "petch_cos_ratio": [P, I, I, P, P, P, P],
+    "petch_belen_bare": [P, I, I, CP, P, P, P, P, P, P, P, P],
+    "petch_surface_rate": [P, I, I, CP, P, P, P, P, P, P, P, P, P, P],
+    "petch_advect_sparse": [P, P, P, P, P, I, P, I, I, I, I, F, F, I, P],
 }
 
 _lib = None

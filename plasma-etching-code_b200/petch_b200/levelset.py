@@ -6,8 +6,6 @@ Each function mirrors the reference signature (petch/threed.py) and accepts eith
 returns float32 tensors).  All arithmetic runs in the CUDA library; nothing is computed on the host
 except the scalar parameters, which follow the reference's float64 host formulas.
 """
-import math
-
 import numpy as np
 import torch
 
@@ -35,8 +33,9 @@ def seed_field(nx, ny, nz, dx, Lx, Ly, sub_top, mask_th, width, hole, stream=Non
     return phi, mask
 
 
-def reinit_fsm_dev(phi, dx, band, n_iter=None, out=None, scratch=None, stream=None):
-    """reinit_fsm on a CUDA float32 grid (threed.py:1515-1537); returns the redistanced grid."""
+def reinit_fsm_dev(phi, dx, band, n_iter=None, out=None, scratch=None, stream=None, mode=0):
+    """reinit_fsm on a CUDA float32 grid (threed.py:1515-1537); returns the redistanced grid.
+    mode=1: the seed-field variant (zero nodes frozen on the front, see petch_reinit_eik)."""
     if n_iter is None:
         n_iter = int(np.ceil(band / dx)) + 4
     big = float(band + 4.0 * dx)
@@ -47,7 +46,7 @@ def reinit_fsm_dev(phi, dx, band, n_iter=None, out=None, scratch=None, stream=No
     if scratch is None:
         scratch = (torch.empty_like(phi), torch.empty_like(phi))
     _lib.call("petch_reinit_eik", _lib.ptr(phi), _lib.ptr(out), _lib.ptr(scratch[0]),
-              _lib.ptr(scratch[1]), nx, ny, nz, float(dx), big, cap, int(n_iter),
+              _lib.ptr(scratch[1]), nx, ny, nz, float(dx), big, cap, int(n_iter), int(mode),
               _lib.stream_ptr(stream))
     return out
 
@@ -79,23 +78,3 @@ def advect_3d_gpu(phi, Fspeed, mask, mask_phi, dx, dt, nsub):
     m = _dev(mask, torch.uint8)
     out = advect_dev(p, _dev(Fspeed), m, _dev(mask_phi), dx, dt, nsub)
     return out.double().cpu().numpy() if host else out
-
-
-def seed_band_iters(dx, cells=24):
-    """Sweep count for redistancing the seed field: `cells` cells of exact distance."""
-    return cells + 4
-
-
-def make_trench_3d(Lx, Ly, Lz, dx, trench_width, mask_th, sub_top, hole=False, seed_cells=24):
-    """Drop-in for threed.make_trench_3d: the same CSG field and mask, redistanced on the device
-    by the Eikonal solver out to `seed_cells` cells (the reference uses skfmm.distance over the
-    whole grid; beyond the band the etch loop never reads more than the sign).
-    Returns the reference's geo dict with numpy arrays."""
-    nx, ny, nz = grid_shape(Lx, Ly, Lz, dx)
-    phi_a, mask = seed_field(nx, ny, nz, dx, Lx, Ly, sub_top, mask_th, trench_width, hole)
-    band = seed_cells * dx
-    phi = reinit_fsm_dev(phi_a, dx, band, n_iter=int(math.ceil(seed_cells)) + 4)
-    xs, ys, zs = np.arange(nx) * dx, np.arange(ny) * dx, np.arange(nz) * dx
-    return dict(xs=xs, ys=ys, zs=zs, dx=dx, phi=phi.double().cpu().numpy(),
-                mask=mask.bool().cpu().numpy(), Lx=Lx, Ly=Ly, Lz=Lz, sub_top=sub_top,
-                trench_width=trench_width, hole=hole)

@@ -1,0 +1,569 @@
+"""The per-step 3D etch loop on the device (drop-in for petch/threed.py's run_etch_3d,
+mc_flux_3d_coupled, mc_flux_3d and helpers).
+
+One step, all in libpetchb200.so kernels on one CUDA stream:
+
+    mesh build (marching cubes -> faces, geometry, adjacency, BVH)
+    -> warm-start coverage (nearest face of the previous mesh)
+    -> ions (faithful ViennaPS reflection) -> yields / m_i / cos_i (normalised + smoothed)
+    -> coverage fixed point: F and O Russian-roulette neutrals -> Belen coverages -> bare
+    -> surface rate V -> velocity extension into the band (+ active-cell list)
+    -- one small device->host read: max V, band size, counts and error bits --
+    -> nsub CFL substeps of upwind advection on the band -> Jacobi Godunov-Eikonal reinit
+
+Host code only derives scalars (seeds, CFL substep count, float64 constants) the way the
+reference's host code does; no per-face or per-cell arithmetic happens on the CPU.
+"""
+import ctypes
+import math
+import time
+import warnings
+
+import numpy as np
+import torch
+
+from . import _lib
+from .chemistry import _yields
+from .levelset import grid_shape, reinit_fsm_dev, seed_field
+from .params import DEFAULT_FLAGS, PAR
+
+SEGMENTS = ("hdr", "vnode", "verts", "faces", "tri", "area", "normal", "centroid", "fmask", "nbr",
+            "nbrw", "leaf_code", "leaf_start", "nodes", "parent", "flags")
+
+MESH_ERR_TRI_OVERFLOW, MESH_ERR_VERT_OVERFLOW, MESH_ERR_HASH_FULL, MESH_ERR_NONMANIFOLD = 1, 2, 4, 8
+
+
+def _sp():
+    return torch.cuda.current_stream().cuda_stream
+
+
+class DeviceMesh:
+    """Surface mesh + BVH in one device buffer (the role of wp.Mesh plus extract_mesh_3d's
+    arrays).  Counts live on the device in `hdr`; `n_faces()` reads them (a sync)."""
+
+    def __init__(self, max_tris, max_verts=None):
+        self.MT = int(max_tris)
+        self.MV = int(max_verts if max_verts is not None else max_tris)
+        offs = (ctypes.c_longlong * len(SEGMENTS))()
+        total = ctypes.c_longlong()
+        _lib.call("petch_mesh_layout", self.MT, self.MV, offs, len(SEGMENTS), ctypes.byref(total))
+        self.off = list(offs)
+        self.buf = torch.empty(int(total.value), dtype=torch.uint8, device="cuda")
+        MT, MV = self.MT, self.MV
+        self.hdr = self._view(0, torch.int32, 16)
+        self.vnode = self._view(1, torch.float32, 3 * MV).view(MV, 3)
+        self.verts = self._view(2, torch.float32, 3 * MV).view(MV, 3)
+        self.faces = self._view(3, torch.int32, 3 * MT).view(MT, 3)
+        self.area = self._view(5, torch.float32, MT)
+        self.normal = self._view(6, torch.float32, 3 * MT).view(MT, 3)
+        self.centroid = self._view(7, torch.float32, 3 * MT).view(MT, 3)
+        self.fmask = self._view(8, torch.uint8, MT)
+        self.nbr = self._view(9, torch.int32, 3 * MT).view(MT, 3)
+        self.nbrw = self._view(10, torch.float32, 3 * MT).view(MT, 3)
+        self.hdr.zero_()
+
+    def _view(self, seg, dtype, n):
+        item = torch.empty((), dtype=dtype).element_size()
+        a = self.off[seg]
+        return self.buf[a:a + n * item].view(dtype)
+
+    @property
+    def id(self):
+        return self.buf.data_ptr()
+
+    def counts(self):
+        h = self.hdr[:8].cpu().numpy()
+        return dict(F=int(h[0]), V=int(h[1]), L=int(h[2]), err=int(h[3]))
+
+    def n_faces(self):
+        return min(int(self.hdr[0].item()), self.MT)
+
+    def build(self, phi, dx, geo, scratch):
+        nx, ny, nz = phi.shape
+        _lib.call("petch_mesh_build", phi.data_ptr(), nx, ny, nz, float(dx), float(geo['Lx']),
+                  float(geo['Ly']), float(geo['sub_top']), float(geo['mask_th']),
+                  float(geo['trench_width']), int(bool(geo['hole'])), self.id, self.MT, self.MV,
+                  scratch.data_ptr(), scratch.numel(), _sp())
+
+    # host copies trimmed to the live counts (for the drop-in API / tests)
+    def host_arrays(self):
+        c = self.counts()
+        F, V = min(c['F'], self.MT), min(c['V'], self.MV)
+        return (self.verts[:V].cpu().numpy(), self.faces[:F].cpu().numpy(),
+                self.centroid[:F].double().cpu().numpy(), self.area[:F].double().cpu().numpy())
+
+
+def mesh_scratch_bytes(shape, max_tris):
+    b = ctypes.c_longlong()
+    _lib.call("petch_mesh_scratch_bytes", *shape, int(max_tris), ctypes.byref(b))
+    return int(b.value)
+
+
+def default_capacity(shape):
+    """Starting face capacity: ~4 faces per boundary cell of the domain box (grown on demand)."""
+    nx, ny, nz = shape
+    return int(max(65536, 8 * (nx * ny + ny * nz + nx * nz)))
+
+
+# --------------------------------------------------------------------------------------------
+# parameters
+# --------------------------------------------------------------------------------------------
+def domain_params(geo, par):
+    d = _lib.Domain()
+    d.lx, d.ly, d.lz = float(geo['Lx']), float(geo['Ly']), float(geo['Lz'])
+    d.z_src = float(geo['Lz'] - geo['dx'])
+    d.periodic = int(par.get('periodic_y', 0))
+    return d
+
+
+def ion_params(par):
+    """The float arguments of _trace3d_ion_yield as mc_flux_3d_coupled computes them
+    (threed.py:800-812)."""
+    p = _lib.IonParams()
+    inflect = float(par.get('inflectAngle', 1.55334303))
+    minang = float(par.get('minAngle', 1.3962634))
+    n_l = float(par.get('n_l', 10.0))
+    A_en = 1.0 / (1.0 + n_l * (1.5707963 / inflect - 1.0))
+    p.meanE, p.sigmaE = float(par['Emean']), float(par['Esig'])
+    p.A_sp, p.Eth_sp, p.B_sp = float(par['A_sp']), float(par['Eth_sp']), float(par['B_sp'])
+    p.A_ie, p.Eth_ie = float(par['A_ie']), float(par['Eth_ie'])
+    p.A_p, p.Eth_p = float(par['A_p']), float(par['Eth_p'])
+    p.inflect, p.minang, p.n_l, p.A_en = inflect, minang, n_l, float(A_en)
+    p.minE = float(min(par['Eth_ie'], par['Eth_sp']))
+    p.thrmin = float(par.get('thetaRMin', 1.2217305))
+    p.thrmax = float(par.get('thetaRMax', 1.5707963))
+    p.sigma = float(par['ion_ang_sigma'])
+    return p
+
+
+def chem_params(par, flags):
+    c = _lib.ChemParams()
+    for k in ("ionFlux", "Fflux", "Oflux", "k_sigma", "beta_sigma", "rho", "rate_scale", "s_F",
+              "s_O", "B_sp"):
+        setattr(c, k, float(par.get(k, PAR.get(k, 0.0))))
+    c.fnorm_E = float(par.get('fnorm_E', 1.0))
+    c.fnorm_O = float(par.get('fnorm_O', 1.0))
+    c.Yie, c.Ysp, c.Yp = _yields(par)
+    mode = "cosine" if flags is None else getattr(flags, "yield_angular", "cosine")
+    c.yield_angular = 1 if mode == "viennaps" else 0
+    chem = "langmuir" if flags is None else getattr(flags, "chemistry", "langmuir")
+    if chem not in ("langmuir", "belen"):
+        raise ValueError(f"unknown chemistry model: {chem}")
+    c.chemistry = 1 if chem == "belen" else 0
+    return c
+
+
+def _unsupported(flags, par):
+    nt = getattr(flags, "neutral_transport", "mc")
+    if nt in ("knudsen", "dda"):
+        raise NotImplementedError(f"neutral_transport={nt!r} is outside this engine's scope")
+    if getattr(flags, "surface_charging", False) or getattr(flags, "floor_charge_throttle", False):
+        raise NotImplementedError("surface charging models are outside this engine's scope")
+    if getattr(flags, "redeposition", False):
+        raise NotImplementedError("redeposition is not implemented yet")
+    if par.get('cov_transport', 'rr') != 'rr':
+        raise NotImplementedError("only the Russian-roulette coverage transport (cov_transport='rr')")
+    if par.get('charge_alpha', 0.0) > 0.0 and getattr(flags, "surface_charging", False):
+        raise NotImplementedError("surface charging models are outside this engine's scope")
+
+
+# --------------------------------------------------------------------------------------------
+# the engine: all buffers of one run
+# --------------------------------------------------------------------------------------------
+class EtchEngine:
+    """Device state of one etch run on an (nx, ny, nz) grid."""
+
+    def __init__(self, geo, par, flags, max_tris=None):
+        self.geo, self.par, self.flags = geo, par, flags
+        self.shape = tuple(int(s) for s in geo['phi_dev'].shape)
+        self.ncell = int(np.prod(self.shape))
+        self.dx = float(geo['dx'])
+        dev = dict(device="cuda")
+        self.phi = geo['phi_dev']
+        self.tmp = torch.empty_like(self.phi)
+        self.ua = torch.empty_like(self.phi)
+        self.ub = torch.empty_like(self.phi)
+        self.F = torch.zeros_like(self.phi)
+        self.mask = geo['mask_dev']
+        self.mask_phi = geo['mask_phi_dev']
+        self.mask_idx = torch.nonzero(self.mask.view(-1)).view(-1).to(torch.int32)
+        self.active = torch.empty(self.ncell, dtype=torch.int32, **dev)
+        self.small = torch.zeros(16, dtype=torch.int32, **dev)   # work(2) stats(2) n_active(1)
+        self.host = torch.zeros(16, dtype=torch.int32).pin_memory()
+        self.dom = domain_params(geo, par)
+        self.ionp = ion_params(par)
+        self.chem = chem_params(par, flags)
+        self._alloc_faces(max_tris or default_capacity(self.shape))
+        self.prev = None          # (mesh, bare) of the previous step for the warm start
+        self.spare = None
+
+    def _alloc_faces(self, MT):
+        self.MT = int(MT)
+        dev = dict(device="cuda", dtype=torch.float32)
+        self.mesh = DeviceMesh(self.MT)
+        self.scratch = torch.empty(mesh_scratch_bytes(self.shape, self.MT), dtype=torch.uint8,
+                                   device="cuda")
+        MT = self.MT
+        self.tal4 = torch.empty((MT, 4), **dev)
+        self.ang = torch.empty(MT, **dev)
+        self.flux = torch.empty(MT, **dev)
+        self.m_i = torch.empty(MT, **dev)
+        self.m_F = torch.empty(MT, **dev)
+        self.m_O = torch.empty(MT, **dev)
+        self.cos_i = torch.empty(MT, **dev)
+        self.y = torch.empty((3, MT), **dev)
+        self.bare = torch.empty(MT, **dev)
+        self.V = torch.empty(MT, **dev)
+        self.tmp5 = torch.empty(5 * MT, **dev)
+
+    def grow(self, need):
+        MT = max(int(need * 1.5), 2 * self.MT)
+        self._alloc_faces(MT)
+
+    # ---- stages ----
+    def build_mesh(self):
+        self.mesh.build(self.phi, self.dx, self.geo, self.scratch)
+
+    def flux_coupled(self, n_ion, n_neu, seed, warm):
+        """mc_flux_3d_coupled (threed.py:740-905) on the device."""
+        par, flags, m = self.par, self.flags, self.mesh
+        s = _sp()
+        A_src = float(self.geo['Lx'] * self.geo['Ly'])
+        n_smooth = int(par.get('flux_smooth', 1))
+        alpha = float(par.get('flux_smooth_alpha', 1.0))
+        work = self.small[0:2]
+        faithful = (flags is not None and getattr(flags, "ion_reflection", False)
+                    and getattr(flags, "chemistry", "langmuir") == "belen")
+        bare_init = False
+        if warm and self.prev is not None:
+            pm, pb = self.prev
+            _lib.call("petch_warmstart", pm.id, pm.MT, pm.MV, pb.data_ptr(), m.id, m.MT, m.MV,
+                      self.bare.data_ptr(), work.data_ptr(), s)
+            bare_init = True
+        if faithful:
+            _lib.call("petch_trace_ions", m.id, m.MT, m.MV, ctypes.byref(self.dom),
+                      ctypes.byref(self.ionp), int(seed * 9 + 1) & 0xffffffff, int(n_ion),
+                      self.tal4.data_ptr(), self.ang.data_ptr(), work.data_ptr(), s)
+            _lib.call("petch_ion_post", m.id, m.MT, m.MV, self.tal4.data_ptr(), self.ang.data_ptr(),
+                      float(A_src / n_ion), n_smooth, alpha, self.y[0].data_ptr(),
+                      self.y[1].data_ptr(), self.y[2].data_ptr(), self.m_i.data_ptr(),
+                      self.cos_i.data_ptr(), self.tmp5.data_ptr(), s)
+            yields = (self.y[0].data_ptr(), self.y[1].data_ptr(), self.y[2].data_ptr())
+        else:
+            # legacy first-hit ion (threed.py:825-840): m_i normalised, clipped at 1.5, smoothed
+            _lib.call("petch_trace_legacy", m.id, m.MT, m.MV, ctypes.byref(self.dom), 1,
+                      float(par['ion_ang_sigma']), 1.0, 0, 0, 0.34, 0.8,
+                      int(seed * 9 + 1) & 0xffffffff, int(n_ion), self.flux.data_ptr(),
+                      self.ang.data_ptr(), work.data_ptr(), s)
+            _lib.call("petch_cos_ratio", m.id, m.MT, m.MV, self.flux.data_ptr(),
+                      self.ang.data_ptr(), self.cos_i.data_ptr(), s)
+            _lib.call("petch_norm_smooth", m.id, m.MT, m.MV, self.flux.data_ptr(),
+                      float(A_src / n_ion), 0.0, 1.5, 1, n_smooth, alpha, self.m_i.data_ptr(),
+                      self.tmp5.data_ptr(), self.tmp5[m.MT:].data_ptr(), s)
+            yields = (None, None, None)
+        n_fp = int(par.get('n_fp', 1 if bare_init else 4))
+        if not bare_init:
+            self.bare.fill_(1.0)
+        betaE, betaO = float(par.get('betaE', 0.7)), float(par.get('betaO', 1.0))
+        for it in range(n_fp):
+            for beta, out, sd in ((betaE, self.m_F, seed * 9 + 2 + 2 * it),
+                                  (betaO, self.m_O, seed * 9 + 3 + 2 * it)):
+                _lib.call("petch_trace_neutrals", m.id, m.MT, m.MV, ctypes.byref(self.dom),
+                          self.bare.data_ptr(), beta, int(sd) & 0xffffffff, 0, int(n_neu),
+                          self.flux.data_ptr(), work.data_ptr(), s)
+                _lib.call("petch_norm_smooth", m.id, m.MT, m.MV, self.flux.data_ptr(),
+                          float(A_src / n_neu), 0.0, 8.0, 1, n_smooth, alpha, out.data_ptr(),
+                          self.tmp5.data_ptr(), self.tmp5[m.MT:].data_ptr(), s)
+            _lib.call("petch_belen_bare", m.id, m.MT, m.MV, ctypes.byref(self.chem),
+                      self.m_i.data_ptr(), self.m_F.data_ptr(), self.m_O.data_ptr(),
+                      self.cos_i.data_ptr(), yields[1], yields[2], self.bare.data_ptr(), s)
+        self.yields = yields
+        return n_fp
+
+    def flux_legacy(self, n_ion, n_neu, seed, ion_reflection):
+        """mc_flux_3d (threed.py:472-507): legacy species, no smoothing, clipped fluxes."""
+        par, m = self.par, self.mesh
+        s = _sp()
+        A_src = float(self.geo['Lx'] * self.geo['Ly'])
+        work = self.small[0:2]
+        sF = float(par['s_F'])
+        sO = float(par['s_O'])
+        if getattr(self.flags, "chemistry", "langmuir") == "belen":
+            sF, sO = float(par['betaE']), float(par['betaO'])
+        spec, nre = (1, 3) if ion_reflection else (0, 0)
+        _lib.call("petch_trace_legacy", m.id, m.MT, m.MV, ctypes.byref(self.dom), 1,
+                  float(par['ion_ang_sigma']), 1.0, nre, spec, 0.34, 0.8,
+                  int(seed * 9 + 1) & 0xffffffff, int(n_ion), self.flux.data_ptr(),
+                  self.ang.data_ptr(), work.data_ptr(), s)
+        _lib.call("petch_cos_ratio", m.id, m.MT, m.MV, self.flux.data_ptr(), self.ang.data_ptr(),
+                  self.cos_i.data_ptr(), s)
+        _lib.call("petch_norm_smooth", m.id, m.MT, m.MV, self.flux.data_ptr(), float(A_src / n_ion),
+                  0.0, 1.5, 1, 0, 1.0, self.m_i.data_ptr(), self.tmp5.data_ptr(),
+                  self.tmp5[m.MT:].data_ptr(), s)
+        for stick, out, sd in ((sF, self.m_F, seed * 9 + 2), (sO, self.m_O, seed * 9 + 3)):
+            _lib.call("petch_trace_legacy", m.id, m.MT, m.MV, ctypes.byref(self.dom), 0, 0.0,
+                      stick, 12, 0, 0.34, 0.8, int(sd) & 0xffffffff, int(n_neu),
+                      self.flux.data_ptr(), self.ang.data_ptr(), work.data_ptr(), s)
+            _lib.call("petch_norm_smooth", m.id, m.MT, m.MV, self.flux.data_ptr(),
+                      float(A_src / n_neu), 0.0, 4.0, 1, 0, 1.0, out.data_ptr(),
+                      self.tmp5.data_ptr(), self.tmp5[m.MT:].data_ptr(), s)
+        self.yields = (None, None, None)
+
+    def rate_and_extend(self, band):
+        m = self.mesh
+        s = _sp()
+        y = self.yields
+        stats = self.small[2:4]
+        _lib.call("petch_surface_rate", m.id, m.MT, m.MV, ctypes.byref(self.chem),
+                  self.m_i.data_ptr(), self.m_F.data_ptr(), self.m_O.data_ptr(),
+                  self.cos_i.data_ptr(), y[0], y[1], y[2], self.V.data_ptr(), stats.data_ptr(), s)
+        nx, ny, nz = self.shape
+        _lib.call("petch_extend_velocity", m.id, m.MT, m.MV, self.phi.data_ptr(),
+                  self.mask.data_ptr(), nx, ny, nz, self.dx, float(band), self.V.data_ptr(),
+                  self.F.data_ptr(), 1, self.active.data_ptr(), self.small[4:5].data_ptr(),
+                  self.ncell, self.small[0:2].data_ptr(), s)
+
+    def sync_status(self):
+        """The step's single device->host read: mesh counts/errors + rate stats + band size."""
+        self.host[0:8].copy_(self.mesh.hdr[0:8], non_blocking=True)
+        self.host[8:13].copy_(self.small[0:5], non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        h = self.host.numpy()
+        return dict(F=int(h[0]), V=int(h[1]), L=int(h[2]), mesh_err=int(h[3]),
+                    trace_err=int(h[9]), nonfinite=int(h[10]),
+                    vmax=float(np.array([h[11]], np.int32).view(np.float32)[0]),
+                    n_active=int(h[12]))
+
+    def advect(self, dt_sub, nsub, n_active):
+        nx, ny, nz = self.shape
+        _lib.call("petch_advect_sparse", self.phi.data_ptr(), self.tmp.data_ptr(),
+                  self.F.data_ptr(), self.mask_phi.data_ptr(), self.mask_idx.data_ptr(),
+                  int(self.mask_idx.numel()), self.active.data_ptr(), int(n_active), nx, ny, nz,
+                  float(1.0 / self.dx), float(dt_sub), int(nsub), _sp())
+
+    def reinit(self, band_r):
+        reinit_fsm_dev(self.phi, self.dx, band_r, out=self.phi, scratch=(self.ua, self.ub))
+
+    def end_step(self, warm):
+        """Keep this step's mesh + coverage for the next step's warm start."""
+        if warm:
+            old = self.prev
+            self.prev = (self.mesh, self.bare)
+            if old is not None and old[0].MT == self.MT:
+                self.mesh, self.bare = old
+            else:
+                self.mesh = DeviceMesh(self.MT)
+                self.bare = torch.empty(self.MT, device="cuda", dtype=torch.float32)
+
+
+# --------------------------------------------------------------------------------------------
+# drop-in functions
+# --------------------------------------------------------------------------------------------
+def make_trench_3d(Lx, Ly, Lz, dx, trench_width, mask_th, sub_top, hole=False, seed_cells=24,
+                   host=True):
+    """make_trench_3d (threed.py:32-59): the CSG field and mask, redistanced on the device.
+    skfmm.distance is replaced by the Jacobi Godunov-Eikonal solve out to `seed_cells` cells
+    (the etch loop reads nothing but the sign beyond the narrow band)."""
+    nx, ny, nz = grid_shape(Lx, Ly, Lz, dx)
+    phi_a, mask = seed_field(nx, ny, nz, dx, Lx, Ly, sub_top, mask_th, trench_width, hole)
+    phi = reinit_fsm_dev(phi_a, dx, seed_cells * dx, n_iter=seed_cells + 4, mode=1)
+    xs, ys, zs = np.arange(nx) * dx, np.arange(ny) * dx, np.arange(nz) * dx
+    geo = dict(xs=xs, ys=ys, zs=zs, dx=dx, Lx=Lx, Ly=Ly, Lz=Lz, sub_top=sub_top,
+               trench_width=trench_width, hole=hole, phi_dev=phi, mask_dev=mask)
+    if host:
+        geo['phi'] = phi.double().cpu().numpy()
+        geo['mask'] = mask.bool().cpu().numpy()
+    return geo
+
+
+def run_etch_3d(Lx=10.0, Ly=4.0, Lz=14.0, dx=0.4, trench_width=4.0, mask_th=2.0,
+                sub_top=10.0, t_end=2.0, n_steps=20, hole=False, par=None, flags=None,
+                n_ion=20000, n_neu=20000, reinit_every=1, extend="gpu",
+                reinit_method="skfmm", verbose=True, record_depth_every=0, seed_offset=0,
+                rays_per_point=None, record_frames=False, surf_smooth=0.0,
+                etch_stop_z=None, max_tris=None, step_callback=None):
+    """run_etch_3d (threed.py:1643-1795) on the device.  Same arguments and the same returned
+    `geo` dict (numpy phi / mask, timings, optional depth_history / frames).
+
+    reinit_method: every method runs the Jacobi Godunov-Eikonal reinit ('fsm'); the reference's
+    skfmm / PDE variants are CPU or legacy paths.  extend must be 'gpu' (nearest face)."""
+    if par is None:
+        par = PAR
+    if flags is None:
+        flags = DEFAULT_FLAGS
+    _unsupported(flags, par)
+    if extend != "gpu":
+        raise NotImplementedError("only the nearest-face ('gpu') velocity extension is provided")
+    if surf_smooth and surf_smooth > 0.0:
+        raise NotImplementedError("surf_smooth is not implemented")
+    nt = getattr(flags, "neutral_transport", "mc")
+    if nt == "radiosity":
+        raise NotImplementedError("neutral_transport='radiosity' is not implemented yet")
+    mc_par = par
+    if getattr(flags, "chemistry", "langmuir") == "belen":
+        mc_par = dict(par)
+        mc_par['s_F'] = par['betaE']
+        mc_par['s_O'] = par['betaO']
+    torch.cuda.init()
+    geo = make_trench_3d(Lx, Ly, Lz, dx, trench_width, mask_th, sub_top, hole=hole, host=False)
+    geo['mask_th'] = mask_th
+    geo['mask_phi_dev'] = geo['phi_dev'].clone()
+    dt = t_end / n_steps
+    band = 4 * dx
+    timings = dict(flux=0.0, extend=0.0, reinit=0.0, mesh=0.0, advect=0.0, total=0.0, nsub_max=0)
+    warm = getattr(flags, "warm_start_coverage", False)
+    coupled = getattr(flags, "coverage_sticking", False)
+    eng = EtchEngine(geo, par, flags, max_tris=max_tris)
+    t0 = time.time()
+    step = 0
+    while step < n_steps:
+        seed = step + seed_offset
+        eng.small.zero_()
+        eng.build_mesh()
+        if rays_per_point is not None:
+            F_now = eng.mesh.n_faces()
+            n_eff = max(int(rays_per_point) * F_now, 1000)
+            n_ion_s, n_neu_s = n_eff, n_eff
+        else:
+            n_ion_s, n_neu_s = n_ion, n_neu
+        if coupled:
+            eng.flux_coupled(n_ion_s, n_neu_s, seed, warm)
+        else:
+            eng.par = mc_par
+            eng.flux_legacy(n_ion_s, n_neu_s, seed, getattr(flags, "ion_reflection", False))
+            eng.par = par
+        eng.rate_and_extend(band)
+        st = eng.sync_status()
+        if st['mesh_err'] & (MESH_ERR_TRI_OVERFLOW | MESH_ERR_VERT_OVERFLOW | MESH_ERR_HASH_FULL):
+            eng.grow(max(st['F'], st['V']))       # redo this step with larger buffers
+            eng.prev = None if eng.prev is None else eng.prev
+            continue
+        if st['trace_err']:
+            raise RuntimeError(f"step {step}: device traversal limit hit (error bits {st['trace_err']})")
+        if st['nonfinite']:
+            warnings.warn(f"step {step}: {st['nonfinite']} non-finite surface velocities (NaN/inf) "
+                          "zeroed; check flux normalization / coverage if this persists.",
+                          RuntimeWarning)
+        vmx = st['vmax'] if st['F'] > 0 else 0.0
+        Vmax = max(vmx if np.isfinite(vmx) else 0.0, 1e-6)
+        nsub = max(1, min(int(np.ceil(Vmax * dt / (0.4 * dx))), 160))
+        timings['nsub_max'] = max(timings['nsub_max'], nsub)
+        if etch_stop_z is not None:
+            below = torch.from_numpy(geo['zs'] < float(etch_stop_z)).to("cuda")
+            Fv = eng.F.view(eng.shape)
+            Fv[:, :, below] = torch.where(Fv[:, :, below] < 0, Fv[:, :, below], 0.0)
+        eng.advect(dt / nsub, nsub, min(st['n_active'], eng.ncell))
+        if (step + 1) % reinit_every == 0 or step == n_steps - 1:
+            eng.reinit(band + 2.0 * dx)
+        eng.end_step(warm and coupled)
+        if record_depth_every and (step % record_depth_every == 0 or step == n_steps - 1):
+            g2 = _host_geo(geo, eng.phi)
+            geo.setdefault('depth_history', []).append((step + 1, _depth3d(g2)))
+            if record_frames:
+                jc = eng.shape[1] // 2
+                geo.setdefault('frames', []).append(
+                    dict(step=step + 1, t=(step + 1) / n_steps * t_end, depth=_depth3d(g2),
+                         phi_xz=g2['phi'][:, jc, :].copy()))
+        if verbose and step % 5 == 0:
+            g2 = _host_geo(geo, eng.phi)
+            print(f"  step {step:3d}/{n_steps}  faces {st['F']:5d}  depth ~ {_depth3d(g2):5.2f}  "
+                  f"Vmax {Vmax:.3f}")
+        if step_callback is not None:
+            step_callback(step, eng, st)
+        step += 1
+    torch.cuda.current_stream().synchronize()
+    timings['total'] = time.time() - t0
+    geo['phi'] = eng.phi.double().cpu().numpy()
+    geo['mask'] = eng.mask.bool().cpu().numpy()
+    geo['timings'] = timings
+    geo['engine'] = eng
+    for k in ('phi_dev', 'mask_dev', 'mask_phi_dev'):
+        geo.pop(k, None)
+    return geo
+
+
+def _host_geo(geo, phi_dev):
+    g = dict(geo)
+    g['phi'] = phi_dev.double().cpu().numpy()
+    return g
+
+
+# ---- depth metrics (threed.py:1798-1869): host post-processing of the final level set ----
+def _column_floor(phi, i, j):
+    col = phi[i, j, :] < 0
+    k = len(col) - 1
+    if not col[k]:
+        return None
+    while k > 0 and col[k - 1]:
+        k -= 1
+    return k
+
+
+def _depth3d(geo, half=1.0):
+    """center_depth_3d: sub_top - median floor over the central columns inside the opening."""
+    phi, xs, ys, zs = geo['phi'], geo['xs'], geo['ys'], geo['zs']
+    cx, cy = geo['Lx'] / 2, geo['Ly'] / 2
+    r_feat = geo.get('trench_width', 2.0) / 2.0 - geo['dx']
+    hx = max(min(half, r_feat), geo['dx'])
+    ic = np.where(np.abs(xs - cx) <= hx)[0]
+    if geo.get('hole', False):
+        jc = np.where(np.abs(ys - cy) <= hx)[0]
+        inside = lambda i, j: (xs[i] - cx) ** 2 + (ys[j] - cy) ** 2 <= r_feat ** 2  # noqa: E731
+    else:
+        jc = np.where(np.abs(ys - cy) <= half)[0]
+        inside = lambda i, j: True  # noqa: E731
+    floors = []
+    for i in ic:
+        for j in jc:
+            if not inside(i, j):
+                continue
+            k = _column_floor(phi, i, j)
+            if k is not None:
+                floors.append(zs[k])
+    if not floors:
+        return 0.0
+    return float(geo['sub_top'] - np.median(floors))
+
+
+def center_depth_3d(geo, half=1.0):
+    return _depth3d(geo, half)
+
+
+def max_depth_3d(geo):
+    """max_depth_3d: sub_top - 5th-percentile floor over the feature footprint."""
+    phi, xs, ys, zs = geo['phi'], geo['xs'], geo['ys'], geo['zs']
+    cx, cy = geo['Lx'] / 2.0, geo['Ly'] / 2.0
+    r = geo.get('trench_width', 4.0) / 2.0
+    if geo.get('hole', False):
+        ii, jj = np.where((xs[:, None] - cx) ** 2 + (ys[None, :] - cy) ** 2 <= (r + geo['dx']) ** 2)
+        cols = list(zip(ii, jj))
+    else:
+        ix = np.where(np.abs(xs - cx) <= r + geo['dx'])[0]
+        cols = [(i, j) for i in ix for j in range(len(ys))]
+    floors = []
+    for i, j in cols:
+        k = _column_floor(phi, i, j)
+        if k is not None:
+            floors.append(zs[k])
+    if not floors:
+        return 0.0
+    return float(geo['sub_top'] - np.percentile(floors, 5))
+
+
+def extract_mesh_3d(phi, dx, geo=None):
+    """extract_mesh_3d (threed.py:62-69): (verts f32, faces i32, centroids f64, areas f64) from
+    the device marching cubes (areas floored at 1e-9 as every consumer applies)."""
+    phi_t = phi if isinstance(phi, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(phi))
+    phi_t = phi_t.to("cuda", torch.float32).contiguous()
+    shape = tuple(phi_t.shape)
+    g = geo or dict(Lx=0.0, Ly=0.0, sub_top=-1e30, mask_th=0.0, trench_width=0.0, hole=False)
+    MT = default_capacity(shape)
+    while True:
+        mesh = DeviceMesh(MT)
+        scratch = torch.empty(mesh_scratch_bytes(shape, MT), dtype=torch.uint8, device="cuda")
+        mesh.build(phi_t, dx, dict(g, mask_th=g.get('mask_th', 0.0)), scratch)
+        c = mesh.counts()
+        if c['err'] & (MESH_ERR_TRI_OVERFLOW | MESH_ERR_VERT_OVERFLOW | MESH_ERR_HASH_FULL):
+            MT = 2 * max(MT, c['F'], c['V'])
+            continue
+        return mesh.host_arrays()

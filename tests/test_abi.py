@@ -33,7 +33,7 @@ def test_abi_version():
 
 @pytest.mark.parametrize("name,args", [
     ("petch_advect", [None, None, None, None, None, 4, 4, 4, 1.0, 0.1, 1, None]),
-    ("petch_reinit_eik", [None, None, None, None, 4, 4, 4, 0.25, 1.0, 1.0, 3, None]),
+    ("petch_reinit_eik", [None, None, None, None, 4, 4, 4, 0.25, 1.0, 1.0, 3, 0, None]),
     ("petch_seed_level_set", [None, None, 4, 4, 4, 0.25, 1.0, 1.0, 0.5, 0.2, 0.4, 1, None]),
 ])
 def test_null_pointers_rejected(name, args):
