@@ -35,6 +35,9 @@ enum {
 /* ABI version (bumped on any signature change). */
 int petch_abi_version(void);
 
+/* Number of kernel launches this library has enqueued since it was loaded (all threads). */
+int petch_launch_count(long long* n);
+
 /* Copies the last error message of the calling host thread into buf (NUL-terminated, <= n bytes).
  * Returns the message length. */
 int petch_last_error(char* buf, int n);
@@ -164,6 +167,16 @@ int petch_extend_velocity(const void* mesh, int max_tris, int max_verts, const f
 int petch_warmstart(const void* prev_mesh, int prev_max_tris, int prev_max_verts,
                     const float* prev_bare, const void* mesh, int max_tris, int max_verts,
                     float* bare, int* work, void* stream);
+
+/* Replaces wp.mesh_query_ray (used by every petch trace kernel): closest hit of each ray
+ * (o, d: float[3n]) with 0 <= t < tmax; face = -1 on a miss. */
+int petch_raycast(const void* mesh, int max_tris, int max_verts, const float* o, const float* d,
+                  int n, float tmax, int* face, float* t, int* work, void* stream);
+
+/* Replaces wp.mesh_query_point_no_sign (petch/threed.py:1328, 1626): nearest face of each point
+ * (float[3n]) within max_dist, ties to the lower face index; -1 if none. */
+int petch_nearest_face(const void* mesh, int max_tris, int max_verts, const float* p, int n,
+                       float max_dist, int* face, int* work, void* stream);
 
 /* ------------------------------------------------------------------------------------------ */
 /* Per-face post-processing and surface chemistry (float64 arithmetic, float32 arrays)         */

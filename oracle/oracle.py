@@ -1,16 +1,27 @@
-"""ORACLE -- test infrastructure only.  ctypes wrapper around liboracle.so, the FP64 CPU
-restatement of petch's per-step 3D etch loop (oracle_*.cpp; each function cites the reference
-lines it follows).  Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
-this module; the product (plasma-etching-code_b200/petch_b200) never does.
+"""ORACLE -- test infrastructure only.  ctypes wrapper around liboracle.so (the FP64 C++
+restatement in oracle_*.cpp) plus the numpy restatement of the per-face host arithmetic, and the
+oracle etch loop.  Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference
+leg use this module; the product (plasma-etching-code_b200/petch_b200) never imports it.
 
-    import oracle.oracle as orc
-    orc.build()                     # g++ -O2 -fopenmp (no GPU needed)
-    phi = orc.reinit(phi, dx, band)
+Reference lines followed (paths within the reference project):
+  mc_flux_3d_coupled   petch/threed.py:740-905     normalisation, smoothing, fixed point
+  smooth_flux          petch/threed.py:129-148     pair scatter, np.add.at
+  _belen_coverages     petch/threed.py:715-737
+  surface_rate_belen   petch/belen.py:26-63 ; surface_rate_langmuir petch/chemistry.py:96-114
+  angular_factors / _yields / _ied_yield   petch/chemistry.py:10-59
+  run_etch_3d          petch/threed.py:1643-1795   CFL, band, seeds, warm start
+  extend_velocity_gpu  petch/threed.py:1333-1346 ; faces_in_mask :1608-1616
+  _depth3d / max_depth_3d petch/threed.py:1798-1869
+Parity pinning: level-set stages and the per-face arithmetic against tests/golden/*.npz made by
+running the reference's own code (tests/golden/make_golden.py); Monte-Carlo stages statistically
+against the reference kernels' per-face means (tests/golden/flux.npz).  Marching cubes and the seed
+distance (skfmm) are third-party in the reference: parity unpinned there.
 """
 import ctypes
 import glob
 import os
 import subprocess
+import time
 
 import numpy as np
 
@@ -21,25 +32,37 @@ _lib = None
 _P = ctypes.c_void_p
 _I = ctypes.c_int
 _D = ctypes.c_double
-_L = ctypes.c_longlong
+_U64 = ctypes.c_uint64
 
 _SIGS = {
-    "orc_seed": [_P, _P, _I, _I, _I, _D, _D, _D, _D, _D, _D, _I],
-    "orc_advect": [_P, _P, _P, _P, _I, _I, _I, _D, _D, _I],
-    "orc_reinit": [_P, _P, _I, _I, _I, _D, _D, _I],
+    "orc_seed": ([_P, _P, _I, _I, _I, _D, _D, _D, _D, _D, _D, _I], None),
+    "orc_advect": ([_P, _P, _P, _P, _I, _I, _I, _D, _D, _I], None),
+    "orc_reinit": ([_P, _P, _I, _I, _I, _D, _D, _I], None),
+    "orc_reinit_mode": ([_P, _P, _I, _I, _I, _D, _D, _I, _I], None),
+    "orc_mesh_build": ([_P, _I, _I, _I, _D, _D, _D, _D, _D, _D, _I], _P),
+    "orc_mesh_from_arrays": ([_P, _I, _P, _I], _P),
+    "orc_mesh_free": ([_P], None),
+    "orc_mesh_counts": ([_P, _P], None),
+    "orc_mesh_get": ([_P, _I, _P], None),
+    "orc_mesh_raycast": ([_P, _P, _P, _I, _P, _P], None),
+    "orc_mesh_nearest": ([_P, _P, _I, _P], None),
+    "orc_trace_ions": ([_P, _P, _P, _U64, _I, _P], None),
+    "orc_trace_neutrals": ([_P, _P, _P, _D, _U64, _U64, _I, _P], None),
+    "orc_trace_legacy": ([_P, _P, _I, _D, _D, _I, _I, _D, _D, _U64, _I, _P, _P], None),
 }
 
 
 def build(force=False):
     """Compile every oracle_*.cpp into liboracle.so (skipped when up to date)."""
     srcs = sorted(glob.glob(os.path.join(HERE, "oracle_*.cpp")))
-    hdrs = glob.glob(os.path.join(HERE, "*.h"))
-    newest = max(os.path.getmtime(s) for s in srcs + hdrs)
+    newest = max(os.path.getmtime(s) for s in srcs)
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
-        cmd = ["g++", "-O2", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-o", LIB, *srcs]
+        tmp = LIB + f".{os.getpid()}.tmp"
+        cmd = ["g++", "-O2", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-o", tmp, *srcs]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("oracle build failed:\n" + r.stderr)
+        os.replace(tmp, LIB)
     return LIB
 
 
@@ -48,10 +71,10 @@ def lib():
     if _lib is None:
         build()
         _lib = ctypes.CDLL(LIB)
-        for name, args in _SIGS.items():
+        for name, (args, res) in _SIGS.items():
             f = getattr(_lib, name)
             f.argtypes = args
-            f.restype = None
+            f.restype = res
     return _lib
 
 
@@ -93,3 +116,444 @@ def reinit(phi, dx, band, n_iter=None):
     nx, ny, nz = phi.shape
     lib().orc_reinit(_p(phi), _p(out), nx, ny, nz, float(dx), float(band), int(n_iter))
     return out
+
+
+def seed_distance(phi_a, dx, cells=24):
+    """Stand-in for skfmm.distance on the seed field: nodes with phi == 0 stay on the front at
+    distance 0, the rest are redistanced from the front out to `cells` cells."""
+    phi = _f64(phi_a)
+    out = np.empty_like(phi)
+    nx, ny, nz = phi.shape
+    lib().orc_reinit_mode(_p(phi), _p(out), nx, ny, nz, float(dx), float(cells * dx),
+                          int(cells + 4), 1)
+    return out
+
+
+def seed_distance_numpy(phi_a, dx, cells=24):
+    """The same seed distance in plain numpy (cross-check of the C++ path)."""
+    return _zero_front_distance(_f64(phi_a), dx, cells * dx, cells + 4)
+
+
+def _zero_front_distance(phi_a, dx, band, n_iter):
+    """Jacobi sweeps with zero nodes frozen at 0 plus the sign-change interface of reinit_fsm,
+    in numpy."""
+    big = band + 4 * dx
+    nx, ny, nz = phi_a.shape
+    U = np.full(phi_a.shape, big)
+    fz = np.zeros(phi_a.shape, bool)
+    # interface cells (reinit_fsm's _eik_init) + zero nodes
+    pad = np.pad(phi_a, 1, mode="edge")
+    c = phi_a
+    nb = [pad[2:, 1:-1, 1:-1], pad[:-2, 1:-1, 1:-1], pad[1:-1, 2:, 1:-1], pad[1:-1, :-2, 1:-1],
+          pad[1:-1, 1:-1, 2:], pad[1:-1, 1:-1, :-2]]
+    iface = np.zeros_like(fz)
+    for o in nb:
+        iface |= (c * o) < 0
+    gx = (nb[0] - nb[1]) * 0.5 / dx
+    gy = (nb[2] - nb[3]) * 0.5 / dx
+    gz = (nb[4] - nb[5]) * 0.5 / dx
+    grad0 = np.maximum(np.sqrt(gx * gx + gy * gy + gz * gz), 0.5)
+    D = np.minimum(np.abs(c) / grad0, 1.8 * dx)
+    U[iface] = D[iface]
+    fz |= iface
+    U[c == 0] = 0.0
+    fz |= c == 0
+    for _ in range(n_iter):
+        P = np.pad(U, 1, mode="constant", constant_values=big)
+        ax = np.minimum(P[2:, 1:-1, 1:-1], P[:-2, 1:-1, 1:-1])
+        ay = np.minimum(P[1:-1, 2:, 1:-1], P[1:-1, :-2, 1:-1])
+        az = np.minimum(P[1:-1, 1:-1, 2:], P[1:-1, 1:-1, :-2])
+        a = np.sort(np.stack([ax, ay, az]), axis=0)
+        x = a[0] + dx
+        d2 = np.maximum(2 * dx * dx - (a[0] - a[1]) ** 2, 0)
+        x2 = 0.5 * (a[0] + a[1] + np.sqrt(d2))
+        s1 = a[0] + a[1] + a[2]
+        s2 = a[0] ** 2 + a[1] ** 2 + a[2] ** 2
+        x3 = (s1 + np.sqrt(np.maximum(s1 * s1 - 3 * (s2 - dx * dx), 0))) / 3
+        cand = np.where(x <= a[1], x, np.where(x2 <= a[2], x2, x3))
+        U = np.where(fz, U, np.minimum(U, cand))
+    sg = np.sign(phi_a)
+    return sg * np.minimum(U, band + dx)
+
+
+# ------------------------------- mesh -------------------------------
+class Mesh:
+    """Oracle mesh (marching cubes + geometry + adjacency + CPU BVH)."""
+
+    def __init__(self, handle):
+        self.h = handle
+        c = np.zeros(2, np.int32)
+        lib().orc_mesh_counts(self.h, _p(c))
+        self.F, self.V = int(c[0]), int(c[1])
+        F, V = self.F, self.V
+
+        def get(which, shape, dt):
+            a = np.empty(shape, dt)
+            if a.size:
+                lib().orc_mesh_get(self.h, which, _p(a))
+            return a
+
+        self.vnode = get(0, (V, 3), np.float64)
+        self.verts = get(1, (V, 3), np.float64)
+        self.faces = get(2, (F, 3), np.int32)
+        self.area = get(3, (F,), np.float64)
+        self.normal = get(4, (F, 3), np.float64)
+        self.centroid = get(5, (F, 3), np.float64)
+        self.fmask = get(6, (F,), np.uint8).astype(bool)
+        self.nbr = get(7, (F, 3), np.int32)
+        self.nbrw = get(8, (F, 3), np.float64)
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.orc_mesh_free(self.h)
+            self.h = None
+
+    def raycast(self, o, d):
+        o, d = _f64(o), _f64(d)
+        n = len(o)
+        f = np.empty(n, np.int32)
+        t = np.empty(n, np.float64)
+        lib().orc_mesh_raycast(self.h, _p(o), _p(d), n, _p(f), _p(t))
+        return f, t
+
+    def nearest(self, p):
+        p = _f64(p)
+        f = np.empty(len(p), np.int32)
+        if len(p):
+            lib().orc_mesh_nearest(self.h, _p(p), len(p), _p(f))
+        return f
+
+    def pairs(self):
+        """Edge-neighbour face pairs (i < j), the set _edge_adjacency produces."""
+        i = np.repeat(np.arange(self.F), 3)
+        j = self.nbr.reshape(-1)
+        k = (j >= 0) & (i < j)
+        return np.stack([i[k], j[k]], axis=1)
+
+
+def mesh_build(phi, dx, geo):
+    phi = np.ascontiguousarray(phi, dtype=np.float32)
+    nx, ny, nz = phi.shape
+    h = lib().orc_mesh_build(_p(phi), nx, ny, nz, float(dx), float(geo['Lx']), float(geo['Ly']),
+                             float(geo['sub_top']), float(geo['mask_th']),
+                             float(geo['trench_width']), int(bool(geo['hole'])))
+    return Mesh(h)
+
+
+def mesh_from_arrays(verts, faces):
+    v = _f64(verts)
+    f = np.ascontiguousarray(faces, dtype=np.int32)
+    return Mesh(lib().orc_mesh_from_arrays(_p(v), len(v), _p(f), len(f)))
+
+
+# ------------------------------- flux -------------------------------
+def _dom(geo, par):
+    return np.array([geo['Lx'], geo['Ly'], geo['Lz'], geo['Lz'] - geo['dx'],
+                     float(par.get('periodic_y', 0))], np.float64)
+
+
+def ion_prm(par):
+    inflect = float(par.get('inflectAngle', 1.55334303))
+    minang = float(par.get('minAngle', 1.3962634))
+    n_l = float(par.get('n_l', 10.0))
+    A_en = 1.0 / (1.0 + n_l * (1.5707963 / inflect - 1.0))
+    return np.array([par['Emean'], par['Esig'], par['A_sp'], par['Eth_sp'], par['B_sp'],
+                     par['A_ie'], par['Eth_ie'], par['A_p'], par['Eth_p'], inflect, minang, n_l,
+                     A_en, min(par['Eth_ie'], par['Eth_sp']), par.get('thetaRMin', 1.2217305),
+                     par.get('thetaRMax', 1.5707963), par['ion_ang_sigma']], np.float64)
+
+
+def trace_ions(mesh, geo, par, seed, n):
+    tal = np.zeros(5 * mesh.F, np.float64)
+    lib().orc_trace_ions(mesh.h, _p(ion_prm(par)), _p(_dom(geo, par)), int(seed) & (2**64 - 1),
+                         int(n), _p(tal))
+    return tal.reshape(mesh.F, 5)
+
+
+def trace_neutrals(mesh, geo, par, bare, beta, seed, n, domain=0):
+    fl = np.zeros(mesh.F, np.float64)
+    b = None if bare is None else _f64(bare)
+    lib().orc_trace_neutrals(mesh.h, _p(_dom(geo, par)), None if b is None else _p(b),
+                             float(beta), int(seed) & (2**64 - 1), int(domain), int(n), _p(fl))
+    return fl
+
+
+def trace_legacy(mesh, geo, par, ion, sigma, sticking, n_reemit, specular, cos_thr, eta, seed, n):
+    fl = np.zeros(mesh.F, np.float64)
+    ang = np.zeros(mesh.F, np.float64)
+    lib().orc_trace_legacy(mesh.h, _p(_dom(geo, par)), int(ion), float(sigma), float(sticking),
+                           int(n_reemit), int(specular), float(cos_thr), float(eta),
+                           int(seed) & (2**64 - 1), int(n), _p(fl), _p(ang))
+    return fl, ang
+
+
+# ------------------------------- per-face arithmetic (numpy) -------------------------------
+def smooth(flux, normals, pairs, n_iter=1, alpha=1.0):
+    """smooth_flux (threed.py:129-148), np.add.at pair scatter."""
+    if len(pairs) == 0 or n_iter <= 0 or alpha <= 0.0:
+        return flux
+    raw = np.asarray(flux, np.float64)
+    out = raw.copy()
+    i, j = pairs[:, 0], pairs[:, 1]
+    w = np.maximum(0.0, np.sum(normals[i] * normals[j], axis=1))
+    for _ in range(n_iter):
+        num = out.copy()
+        den = np.ones(len(out))
+        np.add.at(num, i, out[j] * w)
+        np.add.at(den, i, w)
+        np.add.at(num, j, out[i] * w)
+        np.add.at(den, j, w)
+        out = num / den
+    return out if alpha >= 1.0 else (1.0 - alpha) * raw + alpha * out
+
+
+def _ied_yield(A, Eth, par):
+    mode = par.get('ied_mode', 'mean')
+    Em = float(par['Emean'])
+    sEth = np.sqrt(max(Eth, 0.0))
+    if mode == 'mean':
+        return float(A * max(np.sqrt(max(Em, 0.0)) - sEth, 0.0))
+    if mode == 'gauss':
+        Es = float(par.get('Esig', 10.0))
+        z = np.linspace(-3.5, 3.5, 25)
+        w = np.exp(-0.5 * z * z)
+        w /= w.sum()
+        E = np.clip(Em + Es * z, 0.0, None)
+        return float((w * A * np.maximum(np.sqrt(E) - sEth, 0.0)).sum())
+    dE = float(par.get('ied_dE', 40.0))
+    ph = np.linspace(0.0, np.pi, 49)
+    E = np.clip(Em + 0.5 * dE * np.cos(ph), 0.0, None)
+    return float(np.mean(A * np.maximum(np.sqrt(E) - sEth, 0.0)))
+
+
+def yields(par):
+    return (_ied_yield(par['A_ie'], par['Eth_ie'], par), _ied_yield(par['A_sp'], par['Eth_sp'], par),
+            _ied_yield(par['A_p'], par['Eth_p'], par))
+
+
+def angular_factors(cos_i, par, mode):
+    c = np.clip(cos_i, 0.0, 1.0)
+    if mode == "viennaps":
+        B = par.get('B_sp', 9.3)
+        f_sp = np.maximum((1.0 + B * (1.0 - c * c)) * c, 0.0)
+        th = np.arccos(c)
+        f_ie = np.where(c >= 0.5, 1.0, np.maximum(3.0 - 6.0 * th / np.pi, 0.0))
+        return f_ie, f_sp
+    return c, c
+
+
+def belen_coverages(m_i, m_F, m_O, cos_i, par, yield_angular, ion_yield=None):
+    Yie, Ysp, Yp = yields(par)
+    f_ie, _ = angular_factors(cos_i, par, yield_angular)
+    Fi = par['ionFlux'] * m_i
+    eps = 1e-9
+    if ion_yield is not None:
+        GY_ie = par['ionFlux'] * ion_yield[1]
+        GY_p = par['ionFlux'] * ion_yield[2]
+    else:
+        GY_ie = Yie * f_ie * Fi
+        GY_p = Yp * f_ie * Fi
+    Gb_E = par['Fflux'] * m_F + eps
+    Gb_P = par['Oflux'] * m_O + eps
+    a = (par['k_sigma'] + 2.0 * GY_ie) / Gb_E
+    b = (par['beta_sigma'] + GY_p) / Gb_P
+    thF = 1.0 / (1.0 + a * (1.0 + 1.0 / (b + eps)))
+    thO = 1.0 / (1.0 + b * (1.0 + 1.0 / (a + eps)))
+    return thF, thO
+
+
+def surface_rate(m_i, m_F, m_O, cos_i, is_mask, par, chemistry, yield_angular, ion_yield=None):
+    Yie, Ysp, Yp = yields(par)
+    f_ie, f_sp = angular_factors(cos_i, par, yield_angular)
+    Fi = par['ionFlux'] * m_i
+    Yie_a, Ysp_a, Yp_a = Yie * f_ie, Ysp * f_sp, Yp * f_ie
+    eps = 1e-9
+    if chemistry == "belen":
+        if ion_yield is not None:
+            sp, ie, ip = ion_yield
+            GY_ie, GY_p = par['ionFlux'] * ie, par['ionFlux'] * ip
+            sputter, ion_enh = par['ionFlux'] * sp, par['ionFlux'] * ie
+        else:
+            GY_ie, GY_p = Yie_a * Fi, Yp_a * Fi
+            sputter, ion_enh = Ysp_a * Fi, Yie_a * Fi
+        Gb_E = par['Fflux'] * m_F / par.get('fnorm_E', 1.0) + eps
+        Gb_P = par['Oflux'] * m_O / par.get('fnorm_O', 1.0) + eps
+        a = (par['k_sigma'] + 2.0 * GY_ie) / Gb_E
+        b = (par['beta_sigma'] + GY_p) / Gb_P
+        thF = 1.0 / (1.0 + a * (1.0 + 1.0 / (b + eps)))
+        rate = par['k_sigma'] * thF / 4.0 + sputter + thF * ion_enh
+        V = (1.0 / par['rho']) * rate * par['rate_scale']
+    else:
+        Fev, Fp = par['Fflux'] * m_F, par['Oflux'] * m_O
+        rF = par['s_F'] * Fev / (Yie_a * Fi + eps)
+        rO = par['s_O'] * Fp / (Yp_a * Fi + eps)
+        bare = 1.0 / (1.0 + rF + rO)
+        thF = rF * bare
+        V = (1.0 / par['rho']) * (Yie_a * Fi * thF + Ysp_a * Fi * bare) * par['rate_scale']
+    V = np.array(V, dtype=np.float64)
+    V[is_mask] = 0.0
+    return V
+
+
+def flux_coupled(mesh, geo, par, flags, n_ion, n_neu, seed, bare_init=None, tt=None):
+    """mc_flux_3d_coupled (faithful-ion / legacy-ion branches, RR neutrals) on the oracle mesh.
+    Returns (m_i, m_F, m_O, cos_i, bare, ion_yield-or-None).  tt: optional dict that accumulates
+    the seconds spent in the ray tracers under key 'trace'."""
+    tt = {} if tt is None else tt
+    tt.setdefault('trace', 0.0)
+
+    def timed(fn, *a):
+        t0 = time.time()
+        r = fn(*a)
+        tt['trace'] += time.time() - t0
+        return r
+
+    A_src = geo['Lx'] * geo['Ly']
+    A = np.maximum(mesh.area, 1e-9)
+    n_smooth = int(par.get('flux_smooth', 1))
+    alpha = float(par.get('flux_smooth_alpha', 1.0))
+    pairs = mesh.pairs()
+    sm = (lambda x: smooth(x, mesh.normal, pairs, n_smooth, alpha)) if n_smooth > 0 else (lambda x: x)
+    faithful = getattr(flags, "ion_reflection", False) and getattr(flags, "chemistry", "langmuir") == "belen"
+    iy = None
+    if faithful:
+        tal = timed(trace_ions, mesh, geo, par, seed * 9 + 1, n_ion)
+        norm = A_src / n_ion
+        iy = tuple(sm((tal[:, q] / A) * norm) for q in range(3))
+        fi, ai = tal[:, 3], tal[:, 4]
+        m_i = sm((fi / A) * norm)
+        cos_i = np.where(fi > 0, ai / np.maximum(fi, 1e-9), 0.0)
+    else:
+        fi, ai = timed(trace_legacy, mesh, geo, par, 1, par['ion_ang_sigma'], 1.0, 0, 0, 0.34,
+                       0.8, seed * 9 + 1, n_ion)
+        cos_i = np.where(fi > 0, ai / np.where(fi > 0, fi, 1.0), 0.0)
+        m_i = sm(np.clip((fi / A) * (A_src / n_ion), 0.0, 1.5))
+    n_fp = int(par.get('n_fp', 1 if bare_init is not None else 4))
+    bare = np.ones(mesh.F) if bare_init is None else np.clip(np.asarray(bare_init, float), 0.0, 1.0)
+    betaE, betaO = par.get('betaE', 0.7), par.get('betaO', 1.0)
+    m_F = m_O = np.zeros(mesh.F)
+    ya = getattr(flags, "yield_angular", "cosine")
+    for it in range(n_fp):
+        fF = timed(trace_neutrals, mesh, geo, par, bare, betaE, seed * 9 + 2 + 2 * it, n_neu)
+        m_F = sm(np.clip((fF / A) * (A_src / n_neu), 0.0, 8.0))
+        fO = timed(trace_neutrals, mesh, geo, par, bare, betaO, seed * 9 + 3 + 2 * it, n_neu)
+        m_O = sm(np.clip((fO / A) * (A_src / n_neu), 0.0, 8.0))
+        thF, thO = belen_coverages(m_i, m_F, m_O, cos_i, par, ya, iy)
+        bare = np.clip(1.0 - thF - thO, 0.0, 1.0)
+    return m_i, m_F, m_O, cos_i, bare, iy
+
+
+# ------------------------------- the loop -------------------------------
+def depth3d(geo, phi, half=1.0):
+    """_depth3d (threed.py:1798-1834)."""
+    xs, ys, zs = geo['xs'], geo['ys'], geo['zs']
+    cx, cy = geo['Lx'] / 2, geo['Ly'] / 2
+    r_feat = geo.get('trench_width', 2.0) / 2.0 - geo['dx']
+    hx = max(min(half, r_feat), geo['dx'])
+    ic = np.where(np.abs(xs - cx) <= hx)[0]
+    if geo.get('hole', False):
+        jc = np.where(np.abs(ys - cy) <= hx)[0]
+    else:
+        jc = np.where(np.abs(ys - cy) <= half)[0]
+    floors = []
+    for i in ic:
+        for j in jc:
+            if geo.get('hole', False) and (xs[i] - cx) ** 2 + (ys[j] - cy) ** 2 > r_feat ** 2:
+                continue
+            col = phi[i, j, :] < 0
+            k = len(col) - 1
+            if not col[k]:
+                continue
+            while k > 0 and col[k - 1]:
+                k -= 1
+            floors.append(zs[k])
+    return 0.0 if not floors else float(geo['sub_top'] - np.median(floors))
+
+
+def run_etch_3d(Lx, Ly, Lz, dx, trench_width, mask_th, sub_top, t_end, n_steps, hole, par, flags,
+                n_ion, n_neu, seed_offset=0, record_depth_every=0, max_seconds=None, steps=None,
+                stage_times=None):
+    """run_etch_3d (threed.py:1643-1795) with the oracle's stages (coverage-coupled MC path, FSM
+    reinit, nearest-face extension).  Runs `steps` (default n_steps) steps of the n_steps
+    schedule.  Returns (phi, depth_history, stats); stage_times (list) receives one dict of stage
+    seconds per step."""
+    nx, ny, nz = int(round(Lx / dx)), int(round(Ly / dx)), int(round(Lz / dx))
+    phi_a, mask = seed(nx, ny, nz, dx, Lx, Ly, sub_top, mask_th, trench_width, hole)
+    phi = seed_distance(phi_a.astype(np.float32), dx).astype(np.float32)
+    mask_phi = phi.copy()
+    geo = dict(Lx=Lx, Ly=Ly, Lz=Lz, dx=dx, sub_top=sub_top, mask_th=mask_th,
+               trench_width=trench_width, hole=hole, xs=np.arange(nx) * dx,
+               ys=np.arange(ny) * dx, zs=np.arange(nz) * dx)
+    dt = t_end / n_steps
+    band = 4 * dx
+    warm = getattr(flags, "warm_start_coverage", False)
+    prev = None
+    hist = []
+    t0 = time.time()
+    steps_done = 0
+    for step in range(n_steps if steps is None else min(steps, n_steps)):
+        st = dict(trace=0.0)
+        ta = time.time()
+        mesh = mesh_build(phi, dx, geo)
+        st['mesh'] = time.time() - ta
+        ta = time.time()
+        bi = None
+        if warm and prev is not None:
+            pm, pb = prev
+            q = pm.nearest(mesh.centroid.astype(np.float32).astype(np.float64))
+            bi = np.where(q >= 0, pb[np.maximum(q, 0)], 1.0)
+        m_i, m_F, m_O, cos_i, bare, iy = flux_coupled(mesh, geo, par, flags, n_ion, n_neu,
+                                                      step + seed_offset, bi, tt=st)
+        prev = (mesh, bare)
+        V = surface_rate(m_i, m_F, m_O, cos_i, mesh.fmask, par,
+                         getattr(flags, "chemistry", "langmuir"),
+                         getattr(flags, "yield_angular", "cosine"), iy)
+        V = np.nan_to_num(V, nan=0.0, posinf=0.0, neginf=0.0).astype(np.float32).astype(np.float64)
+        st['flux_rate'] = time.time() - ta
+        ta = time.time()
+        bandm = np.abs(phi.astype(np.float64)) < band
+        ii, jj, kk = np.nonzero(bandm)
+        pts = np.stack([geo['xs'][ii], geo['ys'][jj], geo['zs'][kk]], axis=1)
+        pts = pts.astype(np.float32).astype(np.float64)
+        Fs = np.zeros(phi.shape)
+        if len(pts) and mesh.F:
+            q = mesh.nearest(pts)
+            Fs[ii, jj, kk] = np.where(q >= 0, V[np.maximum(q, 0)], 0.0)
+        st['extend'] = time.time() - ta
+        vmx = float(np.max(V)) if V.size else 0.0
+        Vmax = max(vmx if np.isfinite(vmx) else 0.0, 1e-6)
+        nsub = max(1, min(int(np.ceil(Vmax * dt / (0.4 * dx))), 160))
+        ta = time.time()
+        phi = advect(phi, Fs.astype(np.float32), mask, mask_phi, 1.0 / dx, dt / nsub, nsub)
+        st['advect'] = time.time() - ta
+        ta = time.time()
+        phi = reinit(phi.astype(np.float32), dx, band + 2.0 * dx).astype(np.float32)
+        st['reinit'] = time.time() - ta
+        st['nsub'] = nsub
+        if stage_times is not None:
+            stage_times.append(st)
+        steps_done += 1
+        if record_depth_every and (step % record_depth_every == 0 or step == n_steps - 1):
+            hist.append((step + 1, depth3d(geo, phi)))
+        if max_seconds is not None and time.time() - t0 > max_seconds:
+            break
+    return phi, hist, dict(seconds=time.time() - t0, steps=steps_done)
+
+
+def timed_steps(workload, t_end, n_steps, par, flags, n_rays, n_rays_full, steps, budget_s):
+    """The oracle loop on `workload` at n_rays rays per species for up to `steps` steps (stopping
+    once budget_s seconds have passed); per step, the measured stage seconds and the full step
+    time with the tracing time scaled linearly to n_rays_full."""
+    st = []
+    _, _, info = run_etch_3d(workload['Lx'], workload['Ly'], workload['Lz'], workload['dx'],
+                             workload['trench_width'], workload['mask_th'], workload['sub_top'],
+                             t_end, n_steps, workload['hole'], par, flags, n_rays, n_rays,
+                             steps=steps, max_seconds=budget_s, stage_times=st)
+    scale = n_rays_full / n_rays
+    full = []
+    for s in st:
+        tot = s['mesh'] + s['flux_rate'] + s['extend'] + s['advect'] + s['reinit']
+        full.append(tot + s['trace'] * (scale - 1.0))
+    keys = ('mesh', 'trace', 'flux_rate', 'extend', 'advect', 'reinit')
+    mean = {k: round(float(np.mean([s[k] for s in st])), 3) for k in keys}
+    return dict(steps=info['steps'], full_step_seconds=full, stage_seconds=mean)

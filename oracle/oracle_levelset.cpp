@@ -106,8 +106,18 @@ void orc_advect(double* phi, const double* F, const uint8_t* mask, const double*
 }
 
 // reinit_fsm(phi, dx, band, n_iter): big = band + 4dx, cap = band + dx.
+// seed != 0: the skfmm.distance stand-in for the seed field (phi == 0 nodes frozen at 0 and kept
+// at 0).
+void orc_reinit_mode(const double* phi0, double* phi_out, int nx, int ny, int nz, double dx,
+                     double band, int n_iter, int seed);
+
 void orc_reinit(const double* phi0, double* phi_out, int nx, int ny, int nz, double dx,
                 double band, int n_iter) {
+    orc_reinit_mode(phi0, phi_out, nx, ny, nz, dx, band, n_iter, 0);
+}
+
+void orc_reinit_mode(const double* phi0, double* phi_out, int nx, int ny, int nz, double dx,
+                     double band, int n_iter, int seed) {
     G g(nx, ny, nz);
     const double big = band + 4.0 * dx, cap = band + dx, inv_dx = 1.0 / dx;
     std::vector<double> U((size_t)g.n), B((size_t)g.n);
@@ -122,7 +132,10 @@ void orc_reinit(const double* phi0, double* phi_out, int nx, int ny, int nz, dou
                 double oym = phi0[g.at(i, std::max(j - 1, 0), k)], oyp = phi0[g.at(i, std::min(j + 1, ny - 1), k)];
                 double ozm = phi0[g.at(i, j, std::max(k - 1, 0))], ozp = phi0[g.at(i, j, std::min(k + 1, nz - 1))];
                 bool iface = v * oxm < 0 || v * oxp < 0 || v * oym < 0 || v * oyp < 0 || v * ozm < 0 || v * ozp < 0;
-                if (iface) {
+                if (seed && v == 0.0) {
+                    U[c] = 0.0;
+                    fz[c] = 1;
+                } else if (iface) {
                     double gx = (oxp - oxm) * 0.5 * inv_dx, gy = (oyp - oym) * 0.5 * inv_dx,
                            gz = (ozp - ozm) * 0.5 * inv_dx;
                     double grad0 = std::max(std::sqrt(gx * gx + gy * gy + gz * gz), 0.5);
@@ -156,9 +169,10 @@ void orc_reinit(const double* phi0, double* phi_out, int nx, int ny, int nz, dou
                 }
         std::swap(U, B);
     }
+#pragma omp parallel for
     for (long long c = 0; c < g.n; ++c) {
-        double s = phi0[c] < 0.0 ? -1.0 : 1.0;
-        phi_out[c] = s * std::min(U[c], cap);
+        double s = phi0[c] < 0.0 ? -1.0 : (seed && phi0[c] == 0.0 ? 0.0 : 1.0);
+        phi_out[c] = s * std::min(U[c], cap) + 0.0;
     }
 }
 

@@ -1,7 +1,7 @@
 // Error reporting and device queries shared by every entry point.
+#include <atomic>
 #include <cstdarg>
 #include <cstring>
-#include <mutex>
 #include "common.cuh"
 
 namespace petch {
@@ -20,6 +20,10 @@ int cuda_fail(cudaError_t e, const char* what) {
     return PETCH_E_CUDA;
 }
 
+static std::atomic<long long> g_launches{0};
+
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
 int sm_count() {
     static int cache[64] = {0};
     int dev = 0;
@@ -36,6 +40,15 @@ int sm_count() {
 }  // namespace petch
 
 extern "C" int petch_abi_version(void) { return 1; }
+
+extern "C" int petch_launch_count(long long* n) {
+    if (!n) {
+        petch::set_error("petch_launch_count: null pointer");
+        return PETCH_E_INVALID;
+    }
+    *n = petch::g_launches.load(std::memory_order_relaxed);
+    return PETCH_OK;
+}
 
 extern "C" int petch_last_error(char* buf, int n) {
     int len = (int)strlen(petch::g_last_error);

@@ -18,6 +18,9 @@ inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s
 // Number of SMs on the current device (cached per device).
 int sm_count();
 
+// Kernel launches enqueued by this library since load (read with petch_launch_count).
+void count_launch();
+
 // Blocks for a grid-stride kernel: a multiple of the SM count, capped by the work.
 inline int grid_for(long long n, int block, int per_sm = 8) {
     long long want = (n + block - 1) / block;
@@ -31,6 +34,7 @@ inline int grid_for(long long n, int block, int per_sm = 8) {
 
 #define PETCH_LAUNCH_CHECK(what)                                   \
     do {                                                           \
+        petch::count_launch();                                     \
         cudaError_t _e = cudaGetLastError();                       \
         if (_e != cudaSuccess) return petch::cuda_fail(_e, what);  \
     } while (0)

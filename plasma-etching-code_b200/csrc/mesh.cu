@@ -9,7 +9,8 @@
 //      threed.py:96-99, faces_in_mask threed.py:1608-1616);
 //   3. edge adjacency (replaces _edge_adjacency's argsort, threed.py:103-125) through a device
 //      hash table of (min vertex, max vertex) keys, stored per face as its three edge neighbours
-//      with the smoothing weights max(0, n_i . n_j) (_edge_weights_k, threed.py:237-242);
+//      with the smoothing weights max(0, n_i . n_j) (_edge_weights_k, threed.py:237-242).  An
+//      edge pairs its faces only when it has exactly two (see k_adj_insert);
 //   4. a binary linear BVH (Karras 2012) over the surface cubes (one leaf = the 1..5 faces of one
 //      cube) with a bottom-up box refit, replacing wp.Mesh (threed.py:1674-1675).
 #include <cub/cub.cuh>
@@ -355,8 +356,12 @@ __device__ __forceinline__ unsigned long long edge_key(int a, int b) {
     return ((unsigned long long)lo << 32) | hi;
 }
 
-__global__ void __launch_bounds__(kB) k_adj_insert(MeshView m, unsigned long long* keys, int* hf0,
-                                                   int* hf1, int hbits) {
+// Each edge key's slot counts its faces and sums their ids; an edge with exactly two faces
+// pairs them (the other face is sum - self).  Edges with one face (domain boundary) or more than
+// two (fan diagonals that coincide across an ambiguous cube face) get no neighbour, which keeps
+// the relation symmetric and independent of thread order.
+__global__ void __launch_bounds__(kB) k_adj_insert(MeshView m, unsigned long long* keys, int* hcnt,
+                                                   int* hsum, int hbits) {
     const int F = min(m.hdr[HDR_F], m.MT);
     const uint32_t hmask = (1u << hbits) - 1u;
     for (int x = blockIdx.x * kB + threadIdx.x; x < 3 * F; x += gridDim.x * kB) {
@@ -376,7 +381,8 @@ __global__ void __launch_bounds__(kB) k_adj_insert(MeshView m, unsigned long lon
             atomicOr(&m.hdr[HDR_ERR], MESH_ERR_HASH_FULL);
             continue;
         }
-        if (atomicCAS(&hf0[s], -1, f) != -1 && atomicCAS(&hf1[s], -1, f) != -1) {
+        atomicAdd(&hsum[s], f);
+        if (atomicAdd(&hcnt[s], 1) == 2) {
             atomicOr(&m.hdr[HDR_ERR], MESH_ERR_NONMANIFOLD);
             atomicAdd(&m.hdr[HDR_NONMANIFOLD], 1);
         }
@@ -384,7 +390,7 @@ __global__ void __launch_bounds__(kB) k_adj_insert(MeshView m, unsigned long lon
 }
 
 __global__ void __launch_bounds__(kB) k_adj_lookup(MeshView m, const unsigned long long* keys,
-                                                   const int* hf0, const int* hf1, int hbits) {
+                                                   const int* hcnt, const int* hsum, int hbits) {
     const int F = min(m.hdr[HDR_F], m.MT);
     const uint32_t hmask = (1u << hbits) - 1u;
     for (int x = blockIdx.x * kB + threadIdx.x; x < 3 * F; x += gridDim.x * kB) {
@@ -395,8 +401,7 @@ __global__ void __launch_bounds__(kB) k_adj_lookup(MeshView m, const unsigned lo
         for (uint32_t probe = 0; probe <= hmask; ++probe) {
             unsigned long long k = keys[s];
             if (k == key) {
-                int a = hf0[s], b = hf1[s];
-                other = (a == f) ? b : a;
+                if (hcnt[s] == 2) other = hsum[s] - f;
                 break;
             }
             if (k == kEmpty) break;
@@ -636,8 +641,8 @@ extern "C" int petch_mesh_build(const float* phi, int nx, int ny, int nz, double
 
     long long H = 1LL << s.hbits;
     PETCH_CUDA(cudaMemsetAsync(s.hkeys, 0xff, 8 * H, st), "memset hash keys");
-    PETCH_CUDA(cudaMemsetAsync(s.hf0, 0xff, 4 * H, st), "memset hash f0");
-    PETCH_CUDA(cudaMemsetAsync(s.hf1, 0xff, 4 * H, st), "memset hash f1");
+    PETCH_CUDA(cudaMemsetAsync(s.hf0, 0, 4 * H, st), "memset hash counts");
+    PETCH_CUDA(cudaMemsetAsync(s.hf1, 0, 4 * H, st), "memset hash sums");
     int eb = grid_for(3LL * max_tris, kB);
     k_adj_insert<<<eb, kB, 0, st>>>(m, s.hkeys, s.hf0, s.hf1, s.hbits);
     PETCH_LAUNCH_CHECK("k_adj_insert");

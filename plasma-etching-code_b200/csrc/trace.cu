@@ -402,6 +402,31 @@ __global__ void __launch_bounds__(kTB) k_warmstart(MeshView prev, const float* _
     if (err) atomicOr(work + 1, err);
 }
 
+__global__ void __launch_bounds__(kTB) k_raycast(MeshView m, const float* __restrict__ o,
+                                                 const float* __restrict__ d, int n, float tmax,
+                                                 int* __restrict__ face, float* __restrict__ t,
+                                                 int* work) {
+    const int L = min(m.hdr[HDR_L], m.MT);
+    int err = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float3 oo = make_float3(o[3 * i], o[3 * i + 1], o[3 * i + 2]);
+        float3 dd = make_float3(d[3 * i], d[3 * i + 1], d[3 * i + 2]);
+        HitRec h = closest_hit(m, L, make_ray(oo, dd), tmax, &err);
+        face[i] = h.f;
+        t[i] = h.f >= 0 ? h.t : 0.0f;
+    }
+    if (err) atomicOr(work + 1, err);
+}
+
+__global__ void __launch_bounds__(kTB) k_nearest(MeshView m, const float* __restrict__ p, int n,
+                                                 float r2max, int* __restrict__ face, int* work) {
+    const int L = min(m.hdr[HDR_L], m.MT);
+    int err = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        face[i] = nearest_face(m, L, make_float3(p[3 * i], p[3 * i + 1], p[3 * i + 2]), r2max, &err);
+    if (err) atomicOr(work + 1, err);
+}
+
 int persistent_blocks(const void* kernel, int block) {
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0) != cudaSuccess ||
@@ -511,5 +536,29 @@ extern "C" int petch_warmstart(const void* prev_mesh, int prev_max_tris, int pre
     MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
     k_warmstart<<<grid_for(max_tris, kTB), kTB, 0, st>>>(pm, prev_bare, m, bare, work);
     PETCH_LAUNCH_CHECK("k_warmstart");
+    return PETCH_OK;
+}
+
+extern "C" int petch_raycast(const void* mesh, int max_tris, int max_verts, const float* o,
+                             const float* d, int n, float tmax, int* face, float* t, int* work,
+                             void* stream) {
+    PETCH_REQUIRE(mesh && (n == 0 || (o && d && face && t)) && work, "petch_raycast: null pointer");
+    PETCH_REQUIRE(n >= 0, "petch_raycast: n must be >= 0");
+    if (n == 0) return PETCH_OK;
+    MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
+    k_raycast<<<grid_for(n, kTB, 16), kTB, 0, as_stream(stream)>>>(m, o, d, n, tmax, face, t, work);
+    PETCH_LAUNCH_CHECK("k_raycast");
+    return PETCH_OK;
+}
+
+extern "C" int petch_nearest_face(const void* mesh, int max_tris, int max_verts, const float* p,
+                                  int n, float max_dist, int* face, int* work, void* stream) {
+    PETCH_REQUIRE(mesh && (n == 0 || (p && face)) && work, "petch_nearest_face: null pointer");
+    PETCH_REQUIRE(n >= 0, "petch_nearest_face: n must be >= 0");
+    if (n == 0) return PETCH_OK;
+    MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
+    k_nearest<<<grid_for(n, kTB, 16), kTB, 0, as_stream(stream)>>>(m, p, n, max_dist * max_dist,
+                                                                    face, work);
+    PETCH_LAUNCH_CHECK("k_nearest");
     return PETCH_OK;
 }

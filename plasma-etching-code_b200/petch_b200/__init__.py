@@ -10,4 +10,10 @@ from .levelset import reinit_fsm, advect_3d_gpu, reinit_fsm_dev, advect_dev, see
 from .threed import (make_trench_3d, run_etch_3d, extract_mesh_3d, center_depth_3d, max_depth_3d,
                      DeviceMesh, EtchEngine)
 
+from .api import Domain, SF6O2, Process, Result
+
+__all__ = ["Domain", "SF6O2", "Process", "Result", "PAR", "Flags", "DEFAULT_FLAGS", "run_etch_3d",
+           "make_trench_3d", "extract_mesh_3d", "center_depth_3d", "max_depth_3d", "reinit_fsm",
+           "advect_3d_gpu", "DeviceMesh", "EtchEngine"]
+
 __version__ = "0.1.0"

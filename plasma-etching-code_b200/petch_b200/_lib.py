@@ -48,6 +48,7 @@ CP = ctypes.POINTER(ChemParams)
 # name -> argtypes (restype is int status for all of them)
 SIGNATURES = {
     "petch_abi_version": [],
+    "petch_launch_count": [LLP],
     "petch_last_error": [ctypes.c_char_p, I],
     "petch_seed_level_set": [P, P, I, I, I, D, D, D, D, D, D, I, P],
     "petch_advect": [P, P, P, P, P, I, I, I, F, F, I, P],
@@ -66,6 +67,8 @@ SIGNATURES = {
     "petch_belen_bare": [P, I, I, CP, P, P, P, P, P, P, P, P],
     "petch_surface_rate": [P, I, I, CP, P, P, P, P, P, P, P, P, P, P],
     "petch_advect_sparse": [P, P, P, P, P, I, P, I, I, I, I, F, F, I, P],
+    "petch_raycast": [P, I, I, P, P, I, F, P, P, P, P],
+    "petch_nearest_face": [P, I, I, P, I, F, P, P, P],
 }
 
 _lib = None
@@ -115,6 +118,13 @@ def ptr(t):
     if not t.is_contiguous():
         raise ValueError("expected a contiguous tensor")
     return t.data_ptr()
+
+
+def launch_count():
+    """Kernel launches enqueued by libpetchb200.so so far."""
+    n = ctypes.c_longlong()
+    call("petch_launch_count", ctypes.byref(n))
+    return int(n.value)
 
 
 def stream_ptr(stream=None):

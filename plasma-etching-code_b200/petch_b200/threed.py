@@ -37,6 +37,46 @@ def _sp():
     return torch.cuda.current_stream().cuda_stream
 
 
+class EventTimer:
+    """CUDA-event intervals on the current stream, grouped by name; read once at the end of a run
+    (no per-interval synchronisation)."""
+
+    def __init__(self):
+        self.open = {}
+        self.pairs = {}
+        self.pool = []
+
+    def _ev(self):
+        return self.pool.pop() if self.pool else torch.cuda.Event(enable_timing=True)
+
+    def start(self, name):
+        e = self._ev()
+        e.record()
+        self.open[name] = e
+
+    def stop(self, name):
+        e = self._ev()
+        e.record()
+        self.pairs.setdefault(name, []).append((self.open.pop(name), e))
+
+    def totals_ms(self):
+        torch.cuda.current_stream().synchronize()
+        out = {k: [a.elapsed_time(b) for a, b in v] for k, v in self.pairs.items()}
+        for v in self.pairs.values():
+            for a, b in v:
+                self.pool += [a, b]
+        self.pairs = {}
+        return out
+
+
+class _NoTimer:
+    def start(self, name):
+        pass
+
+    def stop(self, name):
+        pass
+
+
 class DeviceMesh:
     """Surface mesh + BVH in one device buffer (the role of wp.Mesh plus extract_mesh_3d's
     arrays).  Counts live on the device in `hdr`; `n_faces()` reads them (a sync)."""
@@ -195,7 +235,7 @@ class EtchEngine:
         self.chem = chem_params(par, flags)
         self._alloc_faces(max_tris or default_capacity(self.shape))
         self.prev = None          # (mesh, bare) of the previous step for the warm start
-        self.spare = None
+        self.ktimer = _NoTimer()  # set to an EventTimer to time individual trace launches
 
     def _alloc_faces(self, MT):
         self.MT = int(MT)
@@ -241,9 +281,11 @@ class EtchEngine:
                       self.bare.data_ptr(), work.data_ptr(), s)
             bare_init = True
         if faithful:
+            self.ktimer.start("k_ions")
             _lib.call("petch_trace_ions", m.id, m.MT, m.MV, ctypes.byref(self.dom),
                       ctypes.byref(self.ionp), int(seed * 9 + 1) & 0xffffffff, int(n_ion),
                       self.tal4.data_ptr(), self.ang.data_ptr(), work.data_ptr(), s)
+            self.ktimer.stop("k_ions")
             _lib.call("petch_ion_post", m.id, m.MT, m.MV, self.tal4.data_ptr(), self.ang.data_ptr(),
                       float(A_src / n_ion), n_smooth, alpha, self.y[0].data_ptr(),
                       self.y[1].data_ptr(), self.y[2].data_ptr(), self.m_i.data_ptr(),
@@ -268,9 +310,11 @@ class EtchEngine:
         for it in range(n_fp):
             for beta, out, sd in ((betaE, self.m_F, seed * 9 + 2 + 2 * it),
                                   (betaO, self.m_O, seed * 9 + 3 + 2 * it)):
+                self.ktimer.start("k_neutrals")
                 _lib.call("petch_trace_neutrals", m.id, m.MT, m.MV, ctypes.byref(self.dom),
                           self.bare.data_ptr(), beta, int(sd) & 0xffffffff, 0, int(n_neu),
                           self.flux.data_ptr(), work.data_ptr(), s)
+                self.ktimer.stop("k_neutrals")
                 _lib.call("petch_norm_smooth", m.id, m.MT, m.MV, self.flux.data_ptr(),
                           float(A_src / n_neu), 0.0, 8.0, 1, n_smooth, alpha, out.data_ptr(),
                           self.tmp5.data_ptr(), self.tmp5[m.MT:].data_ptr(), s)
@@ -381,12 +425,16 @@ def run_etch_3d(Lx=10.0, Ly=4.0, Lz=14.0, dx=0.4, trench_width=4.0, mask_th=2.0,
                 n_ion=20000, n_neu=20000, reinit_every=1, extend="gpu",
                 reinit_method="skfmm", verbose=True, record_depth_every=0, seed_offset=0,
                 rays_per_point=None, record_frames=False, surf_smooth=0.0,
-                etch_stop_z=None, max_tris=None, step_callback=None):
+                etch_stop_z=None, max_tris=None, phi_init=None, hooks=None):
     """run_etch_3d (threed.py:1643-1795) on the device.  Same arguments and the same returned
-    `geo` dict (numpy phi / mask, timings, optional depth_history / frames).
+    `geo` dict (numpy phi / mask, `timings` per stage from CUDA events, optional depth_history /
+    frames).
 
     reinit_method: every method runs the Jacobi Godunov-Eikonal reinit ('fsm'); the reference's
-    skfmm / PDE variants are CPU or legacy paths.  extend must be 'gpu' (nearest face)."""
+    skfmm / PDE variants are CPU or legacy paths.  extend must be 'gpu' (nearest face).
+    Extensions: phi_init (host or device initial level set, replacing the seed field; the mask
+    and mask_phi still come from the geometry), max_tris (initial face capacity, grown on
+    demand), hooks (dict of callables: before_step(step, eng), after_step(step, eng, status))."""
     if par is None:
         par = PAR
     if flags is None:
@@ -399,44 +447,58 @@ def run_etch_3d(Lx=10.0, Ly=4.0, Lz=14.0, dx=0.4, trench_width=4.0, mask_th=2.0,
     nt = getattr(flags, "neutral_transport", "mc")
     if nt == "radiosity":
         raise NotImplementedError("neutral_transport='radiosity' is not implemented yet")
+    hooks = hooks or {}
     mc_par = par
     if getattr(flags, "chemistry", "langmuir") == "belen":
         mc_par = dict(par)
         mc_par['s_F'] = par['betaE']
         mc_par['s_O'] = par['betaO']
     torch.cuda.init()
+    t_wall = time.time()
     geo = make_trench_3d(Lx, Ly, Lz, dx, trench_width, mask_th, sub_top, hole=hole, host=False)
+    if phi_init is not None:
+        src = phi_init if isinstance(phi_init, torch.Tensor) else torch.from_numpy(
+            np.ascontiguousarray(phi_init))
+        geo['phi_dev'] = src.to("cuda", torch.float32).contiguous().view(geo['phi_dev'].shape)
     geo['mask_th'] = mask_th
     geo['mask_phi_dev'] = geo['phi_dev'].clone()
     dt = t_end / n_steps
     band = 4 * dx
-    timings = dict(flux=0.0, extend=0.0, reinit=0.0, mesh=0.0, advect=0.0, total=0.0, nsub_max=0)
+    timings = dict(flux=0.0, extend=0.0, reinit=0.0, mesh=0.0, advect=0.0, rate=0.0, total=0.0,
+                   nsub_max=0)
     warm = getattr(flags, "warm_start_coverage", False)
     coupled = getattr(flags, "coverage_sticking", False)
     eng = EtchEngine(geo, par, flags, max_tris=max_tris)
-    t0 = time.time()
+    st_timer = EventTimer()
     step = 0
     while step < n_steps:
         seed = step + seed_offset
+        if 'before_step' in hooks:
+            hooks['before_step'](step, eng)
         eng.small.zero_()
+        st_timer.start("mesh")
         eng.build_mesh()
+        st_timer.stop("mesh")
         if rays_per_point is not None:
             F_now = eng.mesh.n_faces()
             n_eff = max(int(rays_per_point) * F_now, 1000)
             n_ion_s, n_neu_s = n_eff, n_eff
         else:
             n_ion_s, n_neu_s = n_ion, n_neu
+        st_timer.start("flux")
         if coupled:
             eng.flux_coupled(n_ion_s, n_neu_s, seed, warm)
         else:
             eng.par = mc_par
             eng.flux_legacy(n_ion_s, n_neu_s, seed, getattr(flags, "ion_reflection", False))
             eng.par = par
+        st_timer.stop("flux")
+        st_timer.start("extend")
         eng.rate_and_extend(band)
+        st_timer.stop("extend")
         st = eng.sync_status()
         if st['mesh_err'] & (MESH_ERR_TRI_OVERFLOW | MESH_ERR_VERT_OVERFLOW | MESH_ERR_HASH_FULL):
             eng.grow(max(st['F'], st['V']))       # redo this step with larger buffers
-            eng.prev = None if eng.prev is None else eng.prev
             continue
         if st['trace_err']:
             raise RuntimeError(f"step {step}: device traversal limit hit (error bits {st['trace_err']})")
@@ -452,10 +514,15 @@ def run_etch_3d(Lx=10.0, Ly=4.0, Lz=14.0, dx=0.4, trench_width=4.0, mask_th=2.0,
             below = torch.from_numpy(geo['zs'] < float(etch_stop_z)).to("cuda")
             Fv = eng.F.view(eng.shape)
             Fv[:, :, below] = torch.where(Fv[:, :, below] < 0, Fv[:, :, below], 0.0)
+        st_timer.start("advect")
         eng.advect(dt / nsub, nsub, min(st['n_active'], eng.ncell))
+        st_timer.stop("advect")
         if (step + 1) % reinit_every == 0 or step == n_steps - 1:
+            st_timer.start("reinit")
             eng.reinit(band + 2.0 * dx)
+            st_timer.stop("reinit")
         eng.end_step(warm and coupled)
+        st['nsub'] = nsub
         if record_depth_every and (step % record_depth_every == 0 or step == n_steps - 1):
             g2 = _host_geo(geo, eng.phi)
             geo.setdefault('depth_history', []).append((step + 1, _depth3d(g2)))
@@ -468,13 +535,15 @@ def run_etch_3d(Lx=10.0, Ly=4.0, Lz=14.0, dx=0.4, trench_width=4.0, mask_th=2.0,
             g2 = _host_geo(geo, eng.phi)
             print(f"  step {step:3d}/{n_steps}  faces {st['F']:5d}  depth ~ {_depth3d(g2):5.2f}  "
                   f"Vmax {Vmax:.3f}")
-        if step_callback is not None:
-            step_callback(step, eng, st)
+        if 'after_step' in hooks:
+            hooks['after_step'](step, eng, st)
         step += 1
-    torch.cuda.current_stream().synchronize()
-    timings['total'] = time.time() - t0
+    ms = st_timer.totals_ms()
+    for k, v in ms.items():
+        timings[k] = float(np.sum(v)) / 1e3
     geo['phi'] = eng.phi.double().cpu().numpy()
     geo['mask'] = eng.mask.bool().cpu().numpy()
+    timings['total'] = time.time() - t_wall
     geo['timings'] = timings
     geo['engine'] = eng
     for k in ('phi_dev', 'mask_dev', 'mask_phi_dev'):

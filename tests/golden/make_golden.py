@@ -89,7 +89,160 @@ def levelset():
     np.savez_compressed(os.path.join(HERE, "levelset.npz"), **out)
 
 
-GROUPS = {"levelset": levelset}
+def _oracle():
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    import oracle.oracle as orc
+    return orc
+
+
+def _small_mesh(hole, nx=14, ny=14, nz=18, dx=0.25):
+    """A small etched-feature mesh from the oracle's marching cubes (the reference's own MC is
+    skimage/Warp, not restated): a masked hole or trench with a partly etched floor."""
+    orc = _oracle()
+    Lx, Ly, Lz = nx * dx, ny * dx, nz * dx
+    sub_top, mask_th, width = 3.0, 0.75, 1.5
+    phi_a, mask = orc.seed(nx, ny, nz, dx, Lx, Ly, sub_top, mask_th, width, hole)
+    X, Y, Z = np.meshgrid(np.arange(nx) * dx, np.arange(ny) * dx, np.arange(nz) * dx, indexing="ij")
+    r = np.sqrt((X - Lx / 2) ** 2 + (Y - Ly / 2) ** 2) if hole else np.abs(X - Lx / 2)
+    # CSG difference: material minus a pit {r < width/2, z > 1.6} below the opening
+    phi_a = np.minimum(phi_a, np.maximum(r - width / 2, 1.6 - Z))
+    phi = orc.reinit(phi_a.astype(np.float32), dx, 6 * dx).astype(np.float32)
+    geo = dict(Lx=Lx, Ly=Ly, Lz=Lz, dx=dx, sub_top=sub_top, mask_th=mask_th, trench_width=width,
+               hole=hole, xs=np.arange(nx) * dx, ys=np.arange(ny) * dx, zs=np.arange(nz) * dx,
+               phi=phi.astype(np.float64))
+    m = orc.mesh_build(phi, dx, geo)
+    return m, geo, phi
+
+
+def surface():
+    """Per-face arithmetic: adjacency, smoothing (host and device forms), Belen coverages,
+    surface rates, faces_in_mask, yields, depth metrics."""
+    import petch.belen as belen
+    import petch.chemistry as chem
+    out = {}
+    rng = np.random.default_rng(7)
+    m, geo, phi = _small_mesh(True)
+    verts, faces = m.verts.astype(np.float32), m.faces
+    out["mesh_verts"], out["mesh_faces"], out["mesh_normal"] = verts, faces, m.normal
+    pairs = t3._edge_adjacency(faces)
+    out["pairs"] = pairs
+    fl = rng.uniform(0.0, 3.0, len(faces))
+    out["smooth_in"] = fl
+    for n_iter, alpha in ((1, 1.0), (2, 1.0), (1, 0.5)):
+        out[f"smooth_host_{n_iter}_{alpha}"] = t3.smooth_flux(fl, m.normal, pairs, n_iter, alpha)
+    prep = t3._smooth_prep_dev(verts, faces, pairs)
+    out["prep_ww"] = np.asarray(prep["ww"])
+    for alpha in (1.0, 0.5):
+        out[f"smooth_dev_{alpha}"] = t3.smooth_flux_dev(t3.wp.array(fl, dtype=float), prep,
+                                                        alpha=alpha).numpy()
+    # chemistry on random per-face inputs
+    F = 400
+    m_i = rng.uniform(0.0, 1.5, F); m_F = rng.uniform(0.0, 2.0, F); m_O = rng.uniform(0.0, 2.0, F)
+    cos_i = rng.uniform(-0.1, 1.1, F); cos_i[:5] = [0.0, 0.5, 1.0, 0.49999, -0.2]
+    iy = tuple(rng.uniform(0.0, 5.0, F) for _ in range(3))
+    is_mask = rng.random(F) < 0.2
+    out.update(c_m_i=m_i, c_m_F=m_F, c_m_O=m_O, c_cos_i=cos_i, c_iy=np.stack(iy), c_is_mask=is_mask)
+    par = dict(t3.PAR)
+    for ya in ("cosine", "viennaps"):
+        for ied in ("mean", "gauss", "bimodal"):
+            p = dict(par, ied_mode=ied, rate_scale=0.7)
+            fl_b = t3.DEFAULT_FLAGS.__class__(chemistry="belen", yield_angular=ya)
+            fl_l = t3.DEFAULT_FLAGS.__class__(chemistry="langmuir", yield_angular=ya)
+            out[f"yields_{ied}"] = np.array(chem._yields(p))
+            thF, thO = t3._belen_coverages(m_i, m_F, m_O, cos_i, p, fl_b)
+            out[f"cov_{ya}_{ied}"] = np.stack([thF, thO])
+            out[f"rate_belen_{ya}_{ied}"] = belen.surface_rate_belen(m_i, m_F, m_O, cos_i, is_mask,
+                                                                     p, fl_b)
+            out[f"rate_langmuir_{ya}_{ied}"] = chem.surface_rate_langmuir(m_i, m_F, m_O, cos_i,
+                                                                          is_mask, p, fl_l)
+            p2 = dict(p, _ion_yield=iy)
+            thF, thO = t3._belen_coverages(m_i, m_F, m_O, cos_i, p2, fl_b)
+            out[f"covy_{ya}_{ied}"] = np.stack([thF, thO])
+            out[f"ratey_belen_{ya}_{ied}"] = belen.surface_rate_belen(m_i, m_F, m_O, cos_i,
+                                                                      is_mask, p2, fl_b)
+    # faces_in_mask: random centroids plus exact band edges
+    for hole in (True, False):
+        g = dict(Lx=4.0, Ly=3.0, sub_top=2.0)
+        c = np.stack([rng.uniform(0, 4, 300), rng.uniform(0, 3, 300), rng.uniform(1.5, 3.0, 300)], 1)
+        c[:4, 2] = [2.0, 2.5, 2.5 - 1e-12, 1.9999999]
+        c[4:8, 0] = [2.0 - 0.6, 2.0 + 0.6, 2.0, 2.6]
+        key = "hole" if hole else "trench"
+        out[f"fim_{key}_c"] = c
+        out[f"fim_{key}"] = t3.faces_in_mask(c, g, 0.5, 1.2, hole=hole)
+    # depth metrics on etched level sets
+    for hole in (True, False):
+        mm, g, ph = _small_mesh(hole)
+        key = "hole" if hole else "trench"
+        g = dict(g, phi=ph.astype(np.float64))
+        out[f"depth_{key}_phi"] = ph
+        out[f"depth_{key}"] = np.array([t3.center_depth_3d(g), t3.max_depth_3d(g),
+                                        t3.center_depth_3d(g, half=0.4)])
+    np.savez_compressed(os.path.join(HERE, "surface.npz"), **out)
+
+
+def _mean_se(fn, seeds):
+    runs = np.stack([fn(s) for s in seeds])
+    return runs.mean(0), runs.std(0, ddof=1) / np.sqrt(len(seeds))
+
+
+def flux():
+    """Monte-Carlo kernels of the reference (shim-executed) on small meshes: per-face means and
+    standard errors over independent seeds."""
+    out = {}
+    wp = t3.wp
+    rng = np.random.default_rng(11)
+    for hole in (True, False):
+        key = "hole" if hole else "trench"
+        m, geo, phi = _small_mesh(hole, nx=10, ny=10, nz=14, dx=0.3)
+        verts, faces = m.verts, m.faces
+        F = len(faces)
+        mesh = wp.Mesh(points=wp.array(verts, dtype=wp.vec3),
+                       indices=wp.array(faces.flatten(), dtype=wp.int32))
+        Lx, Ly, Lz = geo['Lx'], geo['Ly'], geo['Lz']
+        periodic = 0 if hole else 1
+        z_src = Lz - geo['dx']
+        out[f"{key}_verts"], out[f"{key}_faces"] = verts, faces
+        out[f"{key}_geo"] = np.array([Lx, Ly, Lz, geo['dx'], periodic])
+        bare = rng.uniform(0.2, 1.0, F)
+        out[f"{key}_bare"] = bare
+        n = 6000
+        par = dict(t3.PAR)
+
+        def neutral(sd):
+            o, d = t3.gen_source_gpu('neutral', n, Lx, Ly, z_src, 0.0, sd)
+            f = wp.zeros(F, dtype=float)
+            wp.launch(t3._trace3d_cov_rr, dim=n, inputs=[mesh.id, o, d, wp.array(bare), 0.7, sd, f,
+                                                         Lx, Ly, Lz, periodic])
+            return f.numpy() / n
+
+        def ion(sd):
+            o, d = t3.gen_source_gpu('ion', n, Lx, Ly, z_src, par['ion_ang_sigma'], sd)
+            arrs = [wp.zeros(F, dtype=float) for _ in range(5)]
+            inflect, minang, n_l = par['inflectAngle'], par['minAngle'], par['n_l']
+            A_en = 1.0 / (1.0 + n_l * (1.5707963 / inflect - 1.0))
+            wp.launch(t3._trace3d_ion_yield, dim=n, inputs=[
+                mesh.id, o, d, sd, par['Emean'], par['Esig'], par['A_sp'], par['Eth_sp'], par['B_sp'],
+                par['A_ie'], par['Eth_ie'], par['A_p'], par['Eth_p'], inflect, minang, n_l, A_en,
+                min(par['Eth_ie'], par['Eth_sp']), par['thetaRMin'], par['thetaRMax'],
+                Lx, Ly, Lz, periodic, *arrs])
+            return np.stack([a.numpy() for a in arrs]) / n
+
+        def legacy(sd):
+            o, d = t3.gen_source_gpu('neutral', n, Lx, Ly, z_src, 0.0, sd)
+            f, a = wp.zeros(F, dtype=float), wp.zeros(F, dtype=float)
+            wp.launch(t3._trace3d, dim=n, inputs=[mesh.id, o, d, 0.2, 12, sd, 0, 0.34, 0.8, f, a])
+            return np.stack([f.numpy(), a.numpy()]) / n
+
+        for name, fn in (("neutral", neutral), ("ion", ion), ("legacy", legacy)):
+            t0 = time.time()
+            mean, se = _mean_se(fn, range(100, 108))
+            print(f"  {key} {name}: {time.time() - t0:.1f}s", flush=True)
+            out[f"{key}_{name}_mean"], out[f"{key}_{name}_se"] = mean, se
+            out[f"{key}_{name}_n"] = np.array([n * 8])
+    np.savez_compressed(os.path.join(HERE, "flux.npz"), **out)
+
+
+GROUPS = {"levelset": levelset, "surface": surface, "flux": flux}
 
 if __name__ == "__main__":
     for g in (sys.argv[1:] or list(GROUPS)):

@@ -1,0 +1,126 @@
+"""Monte-Carlo flux kernels on the device against (a) the reference's own kernels' per-face means
+(tests/golden/flux.npz, shim-executed) with a chi-square test on the per-face differences, and
+(b) the FP64 oracle at high ray counts with the criterion per-face relative L2 <= 2% (plus the
+measured noise floor).  Different random streams on all three sides: estimator parity."""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+import oracle.oracle as orc
+from conftest import GOLDEN
+from gpu_helpers import cuda_ions, cuda_legacy, cuda_mesh, cuda_neutrals, small_feature
+from petch_b200 import params
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def gold():
+    return np.load(os.path.join(GOLDEN, "flux.npz"))
+
+
+def _mesh(key, gold):
+    phi, geo = small_feature(key == "hole", nx=10, ny=10, nz=14, dx=0.3)
+    m = cuda_mesh(phi, geo['dx'], geo)
+    np.testing.assert_array_equal(m.faces[:m.F].cpu().numpy(), gold[f"{key}_faces"])
+    return m, geo, phi
+
+
+def _chi2(x, se_x, g, se_g):
+    v = se_x ** 2 + se_g ** 2
+    k = v > 0
+    z2 = (x[k] - g[k]) ** 2 / v[k]
+    return float(z2.mean()), float(np.sqrt(z2.max()))
+
+
+def _cuda_mean_se(fn, seeds):
+    runs = np.stack([fn(s) for s in seeds])
+    return runs.mean(0), runs.std(0, ddof=1) / np.sqrt(len(seeds))
+
+
+@pytest.mark.parametrize("key", ["hole", "trench"])
+def test_neutral_vs_reference_kernel(gold, key):
+    m, geo, _ = _mesh(key, gold)
+    n = 500_000
+    x, sx = _cuda_mean_se(lambda s: cuda_neutrals(m, geo, gold[f"{key}_bare"], 0.7, s, n) / n,
+                          range(1, 9))
+    chi, zmax = _chi2(x, sx, gold[f"{key}_neutral_mean"], gold[f"{key}_neutral_se"])
+    assert chi < 1.6, (chi, zmax)
+    assert x.sum() == pytest.approx(gold[f"{key}_neutral_mean"].sum(), rel=0.03)
+
+
+@pytest.mark.parametrize("key", ["hole", "trench"])
+def test_ion_vs_reference_kernel(gold, key):
+    m, geo, _ = _mesh(key, gold)
+    n = 500_000
+    par = dict(params.PAR)
+    x, sx = _cuda_mean_se(lambda s: cuda_ions(m, geo, par, s, n).T / n, range(1, 9))
+    g, sg = gold[f"{key}_ion_mean"], gold[f"{key}_ion_se"]
+    for q in range(5):
+        chi, zmax = _chi2(x[q], sx[q], g[q], sg[q])
+        assert chi < 1.6, (q, chi, zmax)
+        assert x[q].sum() == pytest.approx(g[q].sum(), rel=0.03)
+
+
+@pytest.mark.parametrize("key", ["hole", "trench"])
+def test_legacy_vs_reference_kernel(gold, key):
+    m, geo, _ = _mesh(key, gold)
+    n = 500_000
+    x, sx = _cuda_mean_se(lambda s: np.stack(cuda_legacy(m, dict(geo, periodic_y=0), 0, 0.0, 0.2,
+                                                         12, 0, s, n)) / n, range(1, 9))
+    g, sg = gold[f"{key}_legacy_mean"], gold[f"{key}_legacy_se"]
+    for q in range(2):
+        chi, zmax = _chi2(x[q], sx[q], g[q], sg[q])
+        assert chi < 1.6, (q, chi, zmax)
+
+
+def _rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+@pytest.mark.parametrize("hole", [True, False])
+def test_neutral_vs_oracle_rel_l2(hole):
+    """Per-face relative L2 <= 2% against the FP64 oracle at high ray counts (noise measured
+    from two independent device runs and subtracted in quadrature)."""
+    phi, geo = small_feature(hole)
+    m = cuda_mesh(phi, geo['dx'], geo)
+    o = orc.mesh_build(phi, geo['dx'], geo)
+    rng = np.random.default_rng(0)
+    bare = rng.uniform(0.1, 1.0, m.F)
+    n = 4_000_000
+    a = cuda_neutrals(m, geo, bare, 0.7, 11, n)
+    b = cuda_neutrals(m, geo, bare, 0.7, 12, n)
+    r = orc.trace_neutrals(o, geo, geo, bare, 0.7, 5, n)
+    noise = _rel_l2(a, b) / np.sqrt(2)
+    err = _rel_l2(0.5 * (a + b), r)
+    assert np.sqrt(max(err ** 2 - 1.5 * noise ** 2, 0.0)) <= 0.02, (err, noise)
+
+
+@pytest.mark.parametrize("hole", [True, False])
+def test_ion_vs_oracle_rel_l2(hole):
+    phi, geo = small_feature(hole)
+    m = cuda_mesh(phi, geo['dx'], geo)
+    o = orc.mesh_build(phi, geo['dx'], geo)
+    par = dict(params.PAR, periodic_y=geo['periodic_y'])
+    n = 4_000_000
+    a = cuda_ions(m, geo, par, 21, n)
+    b = cuda_ions(m, geo, par, 22, n)
+    r = orc.trace_ions(o, geo, par, 7, n)
+    for q in range(5):
+        noise = _rel_l2(a[:, q], b[:, q]) / np.sqrt(2)
+        err = _rel_l2(0.5 * (a[:, q] + b[:, q]), r[:, q])
+        assert np.sqrt(max(err ** 2 - 1.5 * noise ** 2, 0.0)) <= 0.02, (q, err, noise)
+
+
+def test_replay_same_seed_same_paths():
+    """Philox streams are keyed by (seed, ray): the same seed reproduces every path; the
+    per-face tallies then differ only by float-atomic summation order."""
+    phi, geo = small_feature(True)
+    m = cuda_mesh(phi, geo['dx'], geo)
+    a = cuda_neutrals(m, geo, None, 0.7, 3, 200_000)
+    b = cuda_neutrals(m, geo, None, 0.7, 3, 200_000)
+    c = cuda_neutrals(m, geo, None, 0.7, 4, 200_000)
+    np.testing.assert_allclose(a, b, rtol=1e-5, atol=1e-3)
+    assert np.abs(a - c).max() > 1.0

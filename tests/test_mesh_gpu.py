@@ -1,0 +1,138 @@
+"""Device marching cubes / geometry / adjacency / BVH queries against the oracle (same
+triangulation spec, independent implementation): topology and vertex positions bit-identical,
+float64-derived geometry to 1e-6, queries identical except exact ties."""
+import numpy as np
+import pytest
+import torch
+
+import oracle.oracle as orc
+from gpu_helpers import cuda_mesh, hole_seed, small_feature, stream
+from petch_b200 import _lib
+
+pytestmark = pytest.mark.gpu
+
+
+def _fields():
+    out = {}
+    n, dx = 40, 0.1
+    X, Y, Z = np.meshgrid(*(np.arange(n) * dx,) * 3, indexing="ij")
+    sph = 1.3 - np.sqrt((X - 2.0) ** 2 + (Y - 1.95) ** 2 + (Z - 2.05) ** 2)
+    out["sphere"] = (sph.astype(np.float32), dx, dict(Lx=4.0, Ly=4.0, Lz=4.0, dx=dx, sub_top=-1e9,
+                                                      mask_th=0.0, trench_width=0.0, hole=False))
+    rng = np.random.default_rng(3)
+    noisy = (sph + rng.normal(0, 0.04, sph.shape)).astype(np.float32)
+    noisy[rng.random(noisy.shape) < 0.02] = 0.0           # exact zeros on nodes
+    out["noisy_zeros"] = (noisy, dx, out["sphere"][2])
+    for hole in (True, False):
+        phi, geo = small_feature(hole)
+        out["pit_" + ("hole" if hole else "trench")] = (phi, geo['dx'], geo)
+    phi, _, geo = hole_seed()
+    out["config0_seed"] = (phi, geo['dx'], geo)
+    return out
+
+
+FIELDS = _fields() if torch.cuda.is_available() else {}
+
+
+@pytest.mark.parametrize("name", sorted(FIELDS) or ["none"])
+def test_mesh_matches_oracle(name):
+    phi, dx, geo = FIELDS[name]
+    m = cuda_mesh(phi, dx, geo)
+    o = orc.mesh_build(phi, dx, geo)
+    assert (m.F, m.V) == (o.F, o.V)
+    if name != "noisy_zeros":
+        assert int(m.hdr[6].item()) == 0                  # smooth fields: every edge has <= 2 faces
+    np.testing.assert_array_equal(m.faces[:m.F].cpu().numpy(), o.faces)
+    np.testing.assert_array_equal(m.vnode[:m.V].double().cpu().numpy(), o.vnode)
+    np.testing.assert_array_equal(m.verts[:m.V].double().cpu().numpy(), o.verts)
+    np.testing.assert_allclose(m.area[:m.F].double().cpu().numpy(), o.area, rtol=1e-6, atol=1e-12)
+    np.testing.assert_allclose(m.centroid[:m.F].double().cpu().numpy(), o.centroid, rtol=0,
+                               atol=1e-5)
+    np.testing.assert_allclose(m.normal[:m.F].double().cpu().numpy(), o.normal, atol=2e-5)
+    np.testing.assert_array_equal(m.fmask[:m.F].bool().cpu().numpy(), o.fmask)
+    np.testing.assert_array_equal(m.nbr[:m.F].cpu().numpy(), o.nbr)
+    np.testing.assert_allclose(m.nbrw[:m.F].double().cpu().numpy(), o.nbrw, atol=2e-5)
+
+
+def test_sphere_is_closed_and_outward():
+    phi, dx, geo = FIELDS["sphere"]
+    m = cuda_mesh(phi, dx, geo)
+    assert (m.nbr[:m.F] >= 0).all()
+    c = m.centroid[:m.F].cpu().numpy() - np.array([2.0, 1.95, 2.05])
+    assert (np.sum(c * m.normal[:m.F].cpu().numpy(), 1) > 0).all()   # winding normal -> gas
+    assert abs(m.area[:m.F].double().sum().item() / (4 * np.pi * 1.3 ** 2) - 1) < 5e-3
+
+
+@pytest.mark.parametrize("name", ["sphere", "pit_hole", "config0_seed"])
+def test_raycast_matches_oracle(name):
+    phi, dx, geo = FIELDS[name]
+    m = cuda_mesh(phi, dx, geo)
+    o = orc.mesh_build(phi, dx, geo)
+    rng = np.random.default_rng(5)
+    n = 20000
+    lo = np.array([0.0, 0.0, 0.0])
+    hi = np.array(phi.shape) * dx
+    org = rng.uniform(lo, hi, (n, 3)).astype(np.float32)
+    d = rng.normal(size=(n, 3))
+    d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+    of, ot = o.raycast(org.astype(np.float64), d.astype(np.float64))
+    face = torch.empty(n, dtype=torch.int32, device="cuda")
+    t = torch.empty(n, device="cuda")
+    work = torch.zeros(2, dtype=torch.int32, device="cuda")
+    org_d, d_d = torch.from_numpy(org).cuda(), torch.from_numpy(d).cuda()   # keep both alive
+    _lib.call("petch_raycast", m.id, m.MT, m.MV, org_d.data_ptr(), d_d.data_ptr(), n, 1e6,
+              face.data_ptr(), t.data_ptr(), work.data_ptr(), stream())
+    cf, ct = face.cpu().numpy(), t.cpu().numpy()
+    assert work[1].item() == 0
+    same = cf == of
+    assert same.mean() > 0.999, same.mean()
+    # disagreements are exact ties at shared edges/vertices: same distance
+    diff = ~same
+    assert np.all((cf[diff] >= 0) == (of[diff] >= 0))
+    np.testing.assert_allclose(ct[diff & (cf >= 0)], ot[diff & (cf >= 0)], rtol=1e-4, atol=1e-5)
+    np.testing.assert_allclose(ct[same & (cf >= 0)], ot[same & (cf >= 0)], rtol=1e-4, atol=1e-5)
+
+
+@pytest.mark.parametrize("name", ["sphere", "pit_trench"])
+def test_nearest_face_matches_oracle(name):
+    phi, dx, geo = FIELDS[name]
+    m = cuda_mesh(phi, dx, geo)
+    o = orc.mesh_build(phi, dx, geo)
+    rng = np.random.default_rng(9)
+    n = 20000
+    p = rng.uniform(0, np.array(phi.shape) * dx, (n, 3)).astype(np.float32)
+    of = o.nearest(p.astype(np.float64))
+    face = torch.empty(n, dtype=torch.int32, device="cuda")
+    work = torch.zeros(2, dtype=torch.int32, device="cuda")
+    p_d = torch.from_numpy(p).cuda()
+    _lib.call("petch_nearest_face", m.id, m.MT, m.MV, p_d.data_ptr(), n, 1e6, face.data_ptr(),
+              work.data_ptr(), stream())
+    cf = face.cpu().numpy()
+    same = cf == of
+    assert same.mean() > 0.9, same.mean()      # the rest must be exact ties, checked below
+    # where they differ the two faces are equidistant (exact ties at shared edges / vertices)
+    for i in np.nonzero(~same)[0][:200]:
+        q = p[i].astype(np.float64)
+        da = _point_tri_d2(q, o.verts[o.faces[cf[i]]])
+        db = _point_tri_d2(q, o.verts[o.faces[of[i]]])
+        assert abs(np.sqrt(da) - np.sqrt(db)) <= 1e-5 * max(1.0, np.sqrt(db))
+
+
+def _point_tri_d2(p, tri):
+    """Squared distance from p to a triangle, by projection onto the plane or the edges."""
+    a, b, c = tri
+    n = np.cross(b - a, c - a)
+    nn = np.dot(n, n)
+    if nn > 0:
+        x = p - np.dot(p - a, n) / nn * n
+        w0 = np.dot(np.cross(b - a, x - a), n)
+        w1 = np.dot(np.cross(c - b, x - b), n)
+        w2 = np.dot(np.cross(a - c, x - c), n)
+        if (w0 >= 0 and w1 >= 0 and w2 >= 0) or (w0 <= 0 and w1 <= 0 and w2 <= 0):
+            return float(np.sum((p - x) ** 2))
+    best = np.inf
+    for u, v in ((a, b), (b, c), (c, a)):
+        e = v - u
+        t = np.clip(np.dot(p - u, e) / max(np.dot(e, e), 1e-300), 0.0, 1.0)
+        best = min(best, float(np.sum((p - (u + t * e)) ** 2)))
+    return best
