@@ -27,13 +27,14 @@ static long long align256(long long x) { return (x + 255) & ~255LL; }
 
 MeshLayout mesh_layout(int MT, int MV) {
     const long long sz[SEG_COUNT] = {
-        64,                          // hdr
+        4LL * HDR_INTS,              // hdr
         12LL * MV, 12LL * MV,        // vnode, verts
         12LL * MT, 48LL * MT,        // faces, tri
         4LL * MT, 12LL * MT, 12LL * MT, 1LL * MT,  // area, normal, centroid, fmask
         12LL * MT, 12LL * MT,        // nbr, nbrw
         4LL * MT, 4LL * (MT + 1),    // leaf_code, leaf_start
-        64LL * MT, 8LL * MT, 4LL * MT  // nodes, parent, flags
+        64LL * MT, 8LL * MT, 4LL * MT, // nodes, parent, flags
+        96LL * MT, 24LL * MT          // wnodes, wfront
     };
     MeshLayout L;
     long long o = 0;
@@ -65,6 +66,8 @@ MeshView mesh_view(void* base, int MT, int MV) {
     v.nodes = (float4*)(b + L.off[SEG_NODES]);
     v.parent = (int*)(b + L.off[SEG_PARENT]);
     v.flags = (int*)(b + L.off[SEG_FLAGS]);
+    v.wnodes = (WNode*)(b + L.off[SEG_WNODES]);
+    v.wfront = (int2*)(b + L.off[SEG_WFRONT]);
     v.MT = MT;
     v.MV = MV;
     return v;
@@ -73,6 +76,7 @@ MeshView mesh_view(void* base, int MT, int MV) {
 namespace {
 
 constexpr int kB = 256;
+constexpr int kWideLevels = 32;   // >= the binary tree depth (<= 31 Morton bits + 1)
 
 // Morton enumeration of an (nx, ny, nz) node grid: axis a gets ceil(log2(n_a)) bits and the bits
 // are interleaved from the least significant level up (x, y, z within a level); an axis that has
@@ -517,6 +521,189 @@ __global__ void __launch_bounds__(kB) k_bvh_refit(MeshView m) {
     }
 }
 
+// ---- 8-wide BVH: greedy top-down collapse of the binary tree, one launch per level ----------
+// Each wide node starts from one binary node's two children and repeatedly opens the internal
+// child with the largest box surface area until it holds 8 children or only leaves remain; its
+// internal children become the next level's wide nodes.  Levels are BFS-ordered, so the top of
+// the tree is a prefix of the node array (staged in shared memory by the tracers).
+
+struct Box {
+    float lo[3], hi[3];
+};
+
+__device__ __forceinline__ Box slot_box(const float4* nodes, int p, int slot) {
+    const float* n = reinterpret_cast<const float*>(nodes + 4 * p);
+    Box b;
+    if (slot == 0) {
+        b.lo[0] = n[0]; b.hi[0] = n[1]; b.lo[1] = n[2]; b.hi[1] = n[3]; b.lo[2] = n[8]; b.hi[2] = n[9];
+    } else {
+        b.lo[0] = n[4]; b.hi[0] = n[5]; b.lo[1] = n[6]; b.hi[1] = n[7]; b.lo[2] = n[10]; b.hi[2] = n[11];
+    }
+    return b;
+}
+
+__device__ __forceinline__ float box_area(const Box& b) {
+    float x = b.hi[0] - b.lo[0], y = b.hi[1] - b.lo[1], z = b.hi[2] - b.lo[2];
+    return x * y + y * z + z * x;
+}
+
+__device__ __forceinline__ int leaf_ref(const MeshView& m, int l) {
+    int s = m.leaf_start[l], e = m.leaf_start[l + 1];
+    int Fc = min(m.hdr[HDR_F], m.MT);
+    s = min(s, Fc);
+    e = min(e, Fc);
+    return -((s << 3) | (e - s)) - 1;
+}
+
+// Quantise `nc` child boxes into node w.
+__device__ void write_wnode(WNode* out, const Box* cb, const int* ref, int nc) {
+    float lo[3] = {3e38f, 3e38f, 3e38f}, hi[3] = {-3e38f, -3e38f, -3e38f};
+    for (int k = 0; k < nc; ++k)
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = fminf(lo[a], cb[k].lo[a]);
+            hi[a] = fmaxf(hi[a], cb[k].hi[a]);
+        }
+    int eb[3];
+    double p[3], sc[3];
+    for (int a = 0; a < 3; ++a) {
+        // scale s = 2^e with the node's extent in <= 255 quanta from a float origin p <= lo
+        double ext = (double)hi[a] - (double)lo[a];
+        int e = -60;
+        if (ext > 0.0) frexp(ext / 255.0, &e);
+        e = max(e, -60);
+        double s = 0.0, pf = 0.0;
+        for (int tries = 0; tries < 4; ++tries, ++e) {
+            s = ldexp(1.0, e);
+            float pa = (float)(floor((double)lo[a] / s) * s);
+            if ((double)pa > (double)lo[a]) pa = nextafterf(pa, -3e38f);
+            pf = (double)pa;
+            if (ceil(((double)hi[a] - pf) / s) <= 255.0) break;
+        }
+        p[a] = pf;
+        sc[a] = s;
+        eb[a] = min(max(e + 127, 1), 254);
+    }
+    uint8_t q[48];
+    for (int k = 0; k < 8; ++k)
+        for (int a = 0; a < 3; ++a) {
+            uint8_t ql = 0, qh = 0;
+            if (k < nc) {
+                double l = floor(((double)cb[k].lo[a] - p[a]) / sc[a]);
+                double h = ceil(((double)cb[k].hi[a] - p[a]) / sc[a]);
+                ql = (uint8_t)fmin(fmax(l, 0.0), 255.0);
+                qh = (uint8_t)fmin(fmax(h, 0.0), 255.0);
+            }
+            q[16 * a + k] = ql;
+            q[16 * a + 8 + k] = qh;
+        }
+    WNode n;
+    n.px = (float)p[0];
+    n.py = (float)p[1];
+    n.pz = (float)p[2];
+    n.meta = (uint32_t)eb[0] | ((uint32_t)eb[1] << 8) | ((uint32_t)eb[2] << 16) | ((uint32_t)nc << 24);
+    for (int w = 0; w < 12; ++w)
+        n.q[w] = (uint32_t)q[4 * w] | ((uint32_t)q[4 * w + 1] << 8) | ((uint32_t)q[4 * w + 2] << 16) |
+                 ((uint32_t)q[4 * w + 3] << 24);
+    for (int k = 0; k < 8; ++k) n.child[k] = k < nc ? ref[k] : 0;
+    *out = n;
+}
+
+__global__ void k_wide_init(MeshView m) {
+    const int L = min(m.hdr[HDR_L], m.MT);
+    m.hdr[HDR_WC + 0] = 0;
+    m.hdr[HDR_WC + 1] = 0;
+    m.hdr[HDR_WC + 2] = 0;
+    m.hdr[HDR_WLEVELS] = 0;
+    if (L <= 0) {
+        m.hdr[HDR_WN] = 0;
+        return;
+    }
+    if (L == 1) {
+        Box b;
+        for (int a = 0; a < 3; ++a) {
+            b.lo[a] = __int_as_float(m.hdr[HDR_ROOTBOX + a]);
+            b.hi[a] = __int_as_float(m.hdr[HDR_ROOTBOX + 3 + a]);
+        }
+        int r = leaf_ref(m, 0);
+        write_wnode(m.wnodes, &b, &r, 1);
+        m.hdr[HDR_WN] = 1;
+        m.hdr[HDR_WLEVELS] = 1;
+        return;
+    }
+    m.wfront[0] = make_int2(0, 0);
+    m.hdr[HDR_WC + 0] = 1;
+    m.hdr[HDR_WN] = 1;
+}
+
+__global__ void __launch_bounds__(128) k_wide_level(MeshView m, int level) {
+    int* cin = &m.hdr[HDR_WC + level % 3];
+    int* cout = &m.hdr[HDR_WC + (level + 1) % 3];
+    const int n = *cin;
+    if (n == 0) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        m.hdr[HDR_WC + (level + 2) % 3] = 0;
+        atomicMax(&m.hdr[HDR_WLEVELS], level + 1);
+    }
+    const int2* fin = m.wfront + (long long)(level % 3) * m.MT;
+    int2* fout = m.wfront + (long long)((level + 1) % 3) * m.MT;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int2 it = fin[i];
+        int b = it.x, w = it.y;
+        Box cb[8];
+        int ref[8];
+        float area[8];
+        float4 l = m.nodes[4 * b + 3];
+        ref[0] = __float_as_int(l.x);
+        ref[1] = __float_as_int(l.y);
+        cb[0] = slot_box(m.nodes, b, 0);
+        cb[1] = slot_box(m.nodes, b, 1);
+        area[0] = box_area(cb[0]);
+        area[1] = box_area(cb[1]);
+        int nc = 2;
+        while (nc < 8) {
+            int best = -1;
+            float ba = -1.0f;
+            for (int k = 0; k < nc; ++k)
+                if (ref[k] >= 0 && area[k] > ba) {
+                    ba = area[k];
+                    best = k;
+                }
+            if (best < 0) break;
+            int bn = ref[best];
+            float4 ll = m.nodes[4 * bn + 3];
+            ref[best] = __float_as_int(ll.x);
+            cb[best] = slot_box(m.nodes, bn, 0);
+            area[best] = box_area(cb[best]);
+            ref[nc] = __float_as_int(ll.y);
+            cb[nc] = slot_box(m.nodes, bn, 1);
+            area[nc] = box_area(cb[nc]);
+            ++nc;
+        }
+        int nint = 0;
+        for (int k = 0; k < nc; ++k) nint += ref[k] >= 0;
+        int base = nint ? atomicAdd(&m.hdr[HDR_WN], nint) : 0;
+        int fpos = nint ? atomicAdd(cout, nint) : 0;
+        int out[8];
+        int r = 0;
+        for (int k = 0; k < nc; ++k) {
+            if (ref[k] >= 0) {
+                int wi = base + r;
+                if (wi < m.MT && fpos + r < m.MT) {
+                    fout[fpos + r] = make_int2(ref[k], wi);
+                    out[k] = wi;
+                } else {
+                    out[k] = -1;   // capacity cannot be exceeded (wide nodes <= binary nodes)
+                    atomicOr(&m.hdr[HDR_ERR], MESH_ERR_TRI_OVERFLOW);
+                }
+                ++r;
+            } else {
+                out[k] = leaf_ref(m, ~ref[k]);
+            }
+        }
+        write_wnode(m.wnodes + w, cb, out, nc);
+    }
+}
+
 struct Scratch {
     uint16_t* info;
     uint32_t* voff;
@@ -654,5 +841,12 @@ extern "C" int petch_mesh_build(const float* phi, int nx, int ny, int nz, double
     PETCH_LAUNCH_CHECK("k_bvh_internal");
     k_bvh_refit<<<fb, kB, 0, st>>>(m);
     PETCH_LAUNCH_CHECK("k_bvh_refit");
+    k_wide_init<<<1, 1, 0, st>>>(m);
+    PETCH_LAUNCH_CHECK("k_wide_init");
+    int wb = grid_for(max_tris / 4 + 1, 128);
+    for (int level = 0; level < kWideLevels; ++level) {
+        k_wide_level<<<wb, 128, 0, st>>>(m, level);
+        PETCH_LAUNCH_CHECK("k_wide_level");
+    }
     return PETCH_OK;
 }

@@ -23,6 +23,8 @@ enum MeshSeg {
     SEG_NODES,       // float4[4*MT] binary BVH internal nodes (two child boxes + links)
     SEG_PARENT,      // int32[2*MT]  parent link: internal i at [i], leaf l at [MT + l]
     SEG_FLAGS,       // int32[MT]    refit arrival counters
+    SEG_WNODES,      // WNode[MT]    8-wide quantised BVH (the tracer's acceleration structure)
+    SEG_WFRONT,      // int2[3*MT]   collapse frontiers (binary node, wide node)
     SEG_COUNT
 };
 
@@ -34,8 +36,24 @@ enum MeshHdr {
     HDR_MT = 4,       // face capacity
     HDR_MV = 5,       // vertex capacity
     HDR_NONMANIFOLD = 6,
-    HDR_ROOTBOX = 8   // float[6] at hdr[8..13]: root bounds lo.xyz, hi.xyz
+    HDR_WN = 7,       // wide BVH nodes
+    HDR_ROOTBOX = 8,  // float[6] at hdr[8..13]: root bounds lo.xyz, hi.xyz
+    HDR_WLEVELS = 14, // wide BVH depth (levels built)
+    HDR_WC = 16,      // int[3] at hdr[16..18]: rotating collapse frontier counters
+    HDR_INTS = 32
 };
+
+// 8-wide BVH node, 96 bytes.  Child a-axis bounds are lo = p_a + qlo * s_a and
+// hi = p_a + qhi * s_a with s_a = 2^(e_a - 127) (the biased exponent byte), rounded outward
+// when quantised.  child[k] >= 0: internal node index; child[k] < 0: leaf, -(start * 8 + count)
+// - 1 with the leaf's faces [start, start + count) (count <= 5).
+struct __align__(16) WNode {
+    float px, py, pz;
+    uint32_t meta;        // ex | ey << 8 | ez << 16 | nchild << 24
+    uint32_t q[12];       // bytes: qlo_x[8] qhi_x[8] qlo_y[8] qhi_y[8] qlo_z[8] qhi_z[8]
+    int32_t child[8];
+};
+static_assert(sizeof(WNode) == 96, "WNode must be 96 bytes");
 
 enum MeshErr {
     MESH_ERR_TRI_OVERFLOW = 1,
@@ -69,6 +87,8 @@ struct MeshView {
     float4* nodes;
     int* parent;
     int* flags;
+    WNode* wnodes;
+    int2* wfront;
     int MT, MV;
 };
 

@@ -25,11 +25,11 @@ struct Domain {
 // ray that misses the surface and leaves through x or y before the open top re-enters at the
 // opposite face with the same direction (<= 256 wraps, then one last query, as the reference's
 // loop followed by the kernel's own query).  `o` is updated to the origin the hit is measured from.
-__device__ __forceinline__ HitRec query_bc(const MeshView& m, int L, float3& o, float3 d,
-                                           const Domain& D, int* err) {
-    if (!D.periodic) return closest_hit(m, L, make_ray(o, d), 1.0e6f, err);
+__device__ __forceinline__ HitRec query_bc(const Tracer& T, float3& o, float3 d, const Domain& D,
+                                           int* err) {
+    if (!D.periodic) return closest_hit_wide(T, make_ray(o, d), 1.0e6f, err);
     for (int w = 0; w < 256; ++w) {
-        HitRec h = closest_hit(m, L, make_ray(o, d), 1.0e6f, err);
+        HitRec h = closest_hit_wide(T, make_ray(o, d), 1.0e6f, err);
         if (h.f >= 0) return h;
         float tx = 1.0e30f, ty = 1.0e30f, tz = 1.0e30f;
         if (d.x > 1.0e-9f) tx = (D.lx - o.x) / d.x;
@@ -47,7 +47,7 @@ __device__ __forceinline__ HitRec query_bc(const MeshView& m, int L, float3& o, 
             return h;   // escapes through the open top
         }
     }
-    return closest_hit(m, L, make_ray(o, d), 1.0e6f, err);
+    return closest_hit_wide(T, make_ray(o, d), 1.0e6f, err);
 }
 
 // _gen_source (threed.py:441-458): origin uniform on [0,Lx]x[0,Ly] at z_src; ion direction from
@@ -124,7 +124,8 @@ __global__ void k_zero_faces(const int* hdr, int MT, float* a, int na, float* b,
 __global__ void __launch_bounds__(kTB) k_ions(MeshView m, Domain D, IonP P, uint32_t seed, int n,
                                               int* work, float4* __restrict__ tal4,
                                               float* __restrict__ ang) {
-    const int L = min(m.hdr[HDR_L], m.MT);
+    extern __shared__ float4 s_wn[];
+    const Tracer T = make_tracer(m, s_wn);
     const float PI_2 = 1.5707963f;
     const float sEsp = sqrtf(P.Eth_sp), sEie = sqrtf(P.Eth_ie), sEp = sqrtf(P.Eth_p);
     int err = 0;
@@ -144,7 +145,7 @@ __global__ void __launch_bounds__(kTB) k_ions(MeshView m, Domain D, IonP P, uint
         if (__all_sync(kFull, ray == -2)) break;
         if (ray < 0) continue;
         // ---- one bounce ----
-        HitRec h = query_bc(m, L, o, d, D, &err);
+        HitRec h = query_bc(T, o, d, D, &err);
         bool done = true;
         if (h.f >= 0) {
             float3 nrm = face_normal(m, h.f);
@@ -231,7 +232,8 @@ __global__ void __launch_bounds__(kTB) k_ions(MeshView m, Domain D, IonP P, uint
 __global__ void __launch_bounds__(kTB) k_neutrals(MeshView m, Domain D, const float* __restrict__ bare,
                                                   float beta, uint32_t seed, uint32_t domain, int n,
                                                   int* work, float* __restrict__ flux) {
-    const int L = min(m.hdr[HDR_L], m.MT);
+    extern __shared__ float4 s_wn[];
+    const Tracer T = make_tracer(m, s_wn);
     int err = 0;
     int ray = -1, bounce = 0;
     Rng g;
@@ -246,7 +248,7 @@ __global__ void __launch_bounds__(kTB) k_neutrals(MeshView m, Domain D, const fl
         }
         if (__all_sync(kFull, ray == -2)) break;
         if (ray < 0) continue;
-        HitRec h = query_bc(m, L, o, d, D, &err);
+        HitRec h = query_bc(T, o, d, D, &err);
         bool done = true;
         if (h.f >= 0) {
             float3 nrm = face_normal(m, h.f);
@@ -283,7 +285,8 @@ __global__ void __launch_bounds__(kTB) k_legacy(MeshView m, Domain D, int ion, f
                                                 float cos_thr, float eta, uint32_t seed,
                                                 uint32_t domain, int n, int* work,
                                                 float* __restrict__ flux, float* __restrict__ angacc) {
-    const int L = min(m.hdr[HDR_L], m.MT);
+    extern __shared__ float4 s_wn[];
+    const Tracer T = make_tracer(m, s_wn);
     int err = 0;
     int ray = -1, bounce = 0;
     Rng g;
@@ -300,7 +303,7 @@ __global__ void __launch_bounds__(kTB) k_legacy(MeshView m, Domain D, int ion, f
         }
         if (__all_sync(kFull, ray == -2)) break;
         if (ray < 0) continue;
-        HitRec h = query_bc(m, L, o, d, Dn, &err);
+        HitRec h = query_bc(T, o, d, Dn, &err);
         bool done = true;
         if (h.f >= 0) {
             float3 nrm = face_normal(m, h.f);
@@ -406,12 +409,13 @@ __global__ void __launch_bounds__(kTB) k_raycast(MeshView m, const float* __rest
                                                  const float* __restrict__ d, int n, float tmax,
                                                  int* __restrict__ face, float* __restrict__ t,
                                                  int* work) {
-    const int L = min(m.hdr[HDR_L], m.MT);
+    extern __shared__ float4 s_wn[];
+    const Tracer T = make_tracer(m, s_wn);
     int err = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         float3 oo = make_float3(o[3 * i], o[3 * i + 1], o[3 * i + 2]);
         float3 dd = make_float3(d[3 * i], d[3 * i + 1], d[3 * i + 2]);
-        HitRec h = closest_hit(m, L, make_ray(oo, dd), tmax, &err);
+        HitRec h = closest_hit_wide(T, make_ray(oo, dd), tmax, &err);
         face[i] = h.f;
         t[i] = h.f >= 0 ? h.t : 0.0f;
     }
@@ -427,9 +431,11 @@ __global__ void __launch_bounds__(kTB) k_nearest(MeshView m, const float* __rest
     if (err) atomicOr(work + 1, err);
 }
 
+constexpr int kSmemBytes = kSmemNodes * 96;
+
 int persistent_blocks(const void* kernel, int block) {
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, kSmemBytes) != cudaSuccess ||
         per_sm < 1)
         per_sm = 1;
     return per_sm * sm_count();
@@ -464,7 +470,7 @@ extern "C" int petch_trace_ions(const void* mesh, int max_tris, int max_verts,
     PETCH_LAUNCH_CHECK("k_zero_faces");
     PETCH_CUDA(cudaMemsetAsync(work, 0, sizeof(int), st), "reset ray counter");
     if (n_ion == 0) return PETCH_OK;
-    k_ions<<<persistent_blocks((const void*)k_ions, kTB), kTB, 0, st>>>(
+    k_ions<<<persistent_blocks((const void*)k_ions, kTB), kTB, kSmemBytes, st>>>(
         m, to_domain(dom), P, seed, n_ion, work, (float4*)tally4, ang);
     PETCH_LAUNCH_CHECK("k_ions");
     return PETCH_OK;
@@ -482,7 +488,7 @@ extern "C" int petch_trace_neutrals(const void* mesh, int max_tris, int max_vert
     PETCH_LAUNCH_CHECK("k_zero_faces");
     PETCH_CUDA(cudaMemsetAsync(work, 0, sizeof(int), st), "reset ray counter");
     if (n_neu == 0) return PETCH_OK;
-    k_neutrals<<<persistent_blocks((const void*)k_neutrals, kTB), kTB, 0, st>>>(
+    k_neutrals<<<persistent_blocks((const void*)k_neutrals, kTB), kTB, kSmemBytes, st>>>(
         m, to_domain(dom), bare, beta, seed, 0x6e657500u ^ stream_id, n_neu, work, flux);
     PETCH_LAUNCH_CHECK("k_neutrals");
     return PETCH_OK;
@@ -502,7 +508,7 @@ extern "C" int petch_trace_legacy(const void* mesh, int max_tris, int max_verts,
     PETCH_LAUNCH_CHECK("k_zero_faces");
     PETCH_CUDA(cudaMemsetAsync(work, 0, sizeof(int), st), "reset ray counter");
     if (n == 0) return PETCH_OK;
-    k_legacy<<<persistent_blocks((const void*)k_legacy, kTB), kTB, 0, st>>>(
+    k_legacy<<<persistent_blocks((const void*)k_legacy, kTB), kTB, kSmemBytes, st>>>(
         m, to_domain(dom), ion, sigma, sticking, n_reemit, specular, cos_thr, eta, seed,
         ion ? 0x6c696f6eu : 0x6c6e6575u, n, work, flux, angacc);
     PETCH_LAUNCH_CHECK("k_legacy");
@@ -546,7 +552,7 @@ extern "C" int petch_raycast(const void* mesh, int max_tris, int max_verts, cons
     PETCH_REQUIRE(n >= 0, "petch_raycast: n must be >= 0");
     if (n == 0) return PETCH_OK;
     MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
-    k_raycast<<<grid_for(n, kTB, 16), kTB, 0, as_stream(stream)>>>(m, o, d, n, tmax, face, t, work);
+    k_raycast<<<grid_for(n, kTB, 16), kTB, kSmemBytes, as_stream(stream)>>>(m, o, d, n, tmax, face, t, work);
     PETCH_LAUNCH_CHECK("k_raycast");
     return PETCH_OK;
 }

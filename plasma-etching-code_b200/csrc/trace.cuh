@@ -226,6 +226,148 @@ __device__ __forceinline__ HitRec closest_hit(const MeshView& m, int L, const Ra
     return h;
 }
 
+// ---------------------------------------------------------------------------------------------
+// 8-wide quantised BVH traversal (closest hit).  Children are tested together, sorted by entry
+// distance with a fixed 19-comparator network in registers, the nearest is visited next and the
+// others are pushed far-to-near with their entry distance, so popped entries beyond the current
+// closest hit are skipped without a fetch.  The first `nsm` nodes (the top levels, BFS order)
+// are read from shared memory.
+// ---------------------------------------------------------------------------------------------
+constexpr int kWStack = 48;
+constexpr int kSmemNodes = 128;   // 12 KB of the tree top per block
+
+struct Tracer {
+    MeshView m;
+    int WN;                    // wide nodes
+    const float4* snodes;      // shared-memory copy of nodes [0, nsm)
+    int nsm;
+};
+
+__device__ __forceinline__ void cas(float& ka, int& va, float& kb, int& vb) {
+    bool sw = kb < ka;
+    float tk = sw ? kb : ka;
+    int tv = sw ? vb : va;
+    kb = sw ? ka : kb;
+    vb = sw ? va : vb;
+    ka = tk;
+    va = tv;
+}
+
+__device__ __forceinline__ float qbyte(uint32_t lo4, uint32_t hi4, int k) {
+    uint32_t w = (k < 4) ? lo4 : hi4;
+    return (float)((w >> (8 * (k & 3))) & 255u);
+}
+
+__device__ __forceinline__ HitRec closest_hit_wide(const Tracer& T, const Ray& r, float tmax,
+                                                   int* err) {
+    HitRec h{tmax, -1};
+    if (T.WN <= 0) return h;
+    int st_ref[kWStack];
+    float st_t[kWStack];
+    int sp = 0;
+    int cur = 0;
+    const float4* gn = reinterpret_cast<const float4*>(T.m.wnodes);
+    for (int visits = 0; visits < kMaxVisits; ++visits) {
+        if (cur >= 0) {
+            float4 v0, v1, v2, v3, v4, v5;
+            if (cur < T.nsm) {
+                const float4* p = T.snodes + 6 * cur;
+                v0 = p[0]; v1 = p[1]; v2 = p[2]; v3 = p[3]; v4 = p[4]; v5 = p[5];
+            } else {
+                const float4* p = gn + 6 * (long long)cur;
+                v0 = __ldg(p); v1 = __ldg(p + 1); v2 = __ldg(p + 2);
+                v3 = __ldg(p + 3); v4 = __ldg(p + 4); v5 = __ldg(p + 5);
+            }
+            uint32_t meta = __float_as_uint(v0.w);
+            float sx = __int_as_float((int)((meta & 255u) << 23));
+            float sy = __int_as_float((int)(((meta >> 8) & 255u) << 23));
+            float sz = __int_as_float((int)(((meta >> 16) & 255u) << 23));
+            int nc = (int)(meta >> 24);
+            float ax0 = (v0.x - r.o.x) * r.inv.x, ax1 = sx * r.inv.x;
+            float ay0 = (v0.y - r.o.y) * r.inv.y, ay1 = sy * r.inv.y;
+            float az0 = (v0.z - r.o.z) * r.inv.z, az1 = sz * r.inv.z;
+            uint32_t qx0 = __float_as_uint(v1.x), qx1 = __float_as_uint(v1.y);
+            uint32_t qx2 = __float_as_uint(v1.z), qx3 = __float_as_uint(v1.w);
+            uint32_t qy0 = __float_as_uint(v2.x), qy1 = __float_as_uint(v2.y);
+            uint32_t qy2 = __float_as_uint(v2.z), qy3 = __float_as_uint(v2.w);
+            uint32_t qz0 = __float_as_uint(v3.x), qz1 = __float_as_uint(v3.y);
+            uint32_t qz2 = __float_as_uint(v3.z), qz3 = __float_as_uint(v3.w);
+            int ch[8] = {__float_as_int(v4.x), __float_as_int(v4.y), __float_as_int(v4.z),
+                         __float_as_int(v4.w), __float_as_int(v5.x), __float_as_int(v5.y),
+                         __float_as_int(v5.z), __float_as_int(v5.w)};
+            float key[8];
+            int nh = 0;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                float tlx = ax0 + qbyte(qx0, qx1, k) * ax1, thx = ax0 + qbyte(qx2, qx3, k) * ax1;
+                float tly = ay0 + qbyte(qy0, qy1, k) * ay1, thy = ay0 + qbyte(qy2, qy3, k) * ay1;
+                float tlz = az0 + qbyte(qz0, qz1, k) * az1, thz = az0 + qbyte(qz2, qz3, k) * az1;
+                float tn = fmaxf(fmaxf(fminf(tlx, thx), fminf(tly, thy)), fmaxf(fminf(tlz, thz), 0.0f));
+                float tf = fminf(fminf(fmaxf(tlx, thx), fmaxf(tly, thy)), fminf(fmaxf(tlz, thz), h.t));
+                bool hit = (k < nc) && (tn <= tf * 1.00001f + 1.0e-7f);
+                key[k] = hit ? tn : 3.0e38f;
+                nh += hit;
+            }
+            if (nh > 0) {
+                cas(key[0], ch[0], key[1], ch[1]); cas(key[2], ch[2], key[3], ch[3]);
+                cas(key[4], ch[4], key[5], ch[5]); cas(key[6], ch[6], key[7], ch[7]);
+                cas(key[0], ch[0], key[2], ch[2]); cas(key[1], ch[1], key[3], ch[3]);
+                cas(key[4], ch[4], key[6], ch[6]); cas(key[5], ch[5], key[7], ch[7]);
+                cas(key[1], ch[1], key[2], ch[2]); cas(key[5], ch[5], key[6], ch[6]);
+                cas(key[0], ch[0], key[4], ch[4]); cas(key[1], ch[1], key[5], ch[5]);
+                cas(key[2], ch[2], key[6], ch[6]); cas(key[3], ch[3], key[7], ch[7]);
+                cas(key[2], ch[2], key[4], ch[4]); cas(key[3], ch[3], key[5], ch[5]);
+                cas(key[1], ch[1], key[2], ch[2]); cas(key[3], ch[3], key[4], ch[4]);
+                cas(key[5], ch[5], key[6], ch[6]);
+#pragma unroll
+                for (int k = 7; k >= 1; --k)
+                    if (k < nh) {
+                        if (sp < kWStack) {
+                            st_ref[sp] = ch[k];
+                            st_t[sp] = key[k];
+                            ++sp;
+                        } else {
+                            *err |= 1;
+                        }
+                    }
+                cur = ch[0];
+                continue;
+            }
+        } else {
+            int code = -cur - 1;
+            int f0 = code >> 3, f1 = f0 + (code & 7);
+            for (int f = f0; f < f1; ++f)
+                if (hit_triangle(r, tri_v(T.m.tri, f, 0), tri_v(T.m.tri, f, 1), tri_v(T.m.tri, f, 2), h.t))
+                    h.f = f;
+        }
+        bool found = false;
+        while (sp > 0) {
+            --sp;
+            if (st_t[sp] <= h.t) {
+                cur = st_ref[sp];
+                found = true;
+                break;
+            }
+        }
+        if (!found) return h;
+    }
+    *err |= 1;
+    return h;
+}
+
+// Stage the top of the wide tree in shared memory (call from every thread of the block).
+__device__ __forceinline__ Tracer make_tracer(const MeshView& m, float4* smem) {
+    Tracer T;
+    T.m = m;
+    T.WN = m.hdr[HDR_WN];
+    T.nsm = min(T.WN, kSmemNodes);
+    const float4* g = reinterpret_cast<const float4*>(m.wnodes);
+    for (int i = threadIdx.x; i < 6 * T.nsm; i += blockDim.x) smem[i] = __ldg(g + i);
+    __syncthreads();
+    T.snodes = smem;
+    return T;
+}
+
 // Unit winding normal of face f (normalize(cross(b - a, c - a)), as Warp's query normal).
 __device__ __forceinline__ float3 face_normal(const MeshView& m, int f) {
     float3 a = tri_v(m.tri, f, 0), b = tri_v(m.tri, f, 1), c = tri_v(m.tri, f, 2);

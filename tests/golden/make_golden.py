@@ -187,7 +187,11 @@ def _mean_se(fn, seeds):
 
 def flux():
     """Monte-Carlo kernels of the reference (shim-executed) on small meshes: per-face means and
-    standard errors over independent seeds."""
+    standard errors over independent seeds.  Sources come from the reference's host path
+    (_source3d with sampling='pseudo', threed.py:410-438), whose random stream is independent of
+    the trace kernel's.  (On its CUDA path the reference seeds _gen_source and the trace kernel
+    with the same (seed, thread) stream, so a ray's first sticking / re-emission draws repeat its
+    source draws; that correlation is not reproduced.)"""
     out = {}
     wp = t3.wp
     rng = np.random.default_rng(11)
@@ -208,15 +212,20 @@ def flux():
         n = 6000
         par = dict(t3.PAR)
 
+        def src(kind, sd, sigma):
+            o, d = t3._source3d(kind, n, Lx, Ly, z_src, sigma, 'pseudo',
+                                np.random.default_rng(sd), sd)
+            return wp.array(o, dtype=wp.vec3), wp.array(d, dtype=wp.vec3)
+
         def neutral(sd):
-            o, d = t3.gen_source_gpu('neutral', n, Lx, Ly, z_src, 0.0, sd)
+            o, d = src('neutral', sd, 0.0)
             f = wp.zeros(F, dtype=float)
             wp.launch(t3._trace3d_cov_rr, dim=n, inputs=[mesh.id, o, d, wp.array(bare), 0.7, sd, f,
                                                          Lx, Ly, Lz, periodic])
             return f.numpy() / n
 
         def ion(sd):
-            o, d = t3.gen_source_gpu('ion', n, Lx, Ly, z_src, par['ion_ang_sigma'], sd)
+            o, d = src('ion', sd, par['ion_ang_sigma'])
             arrs = [wp.zeros(F, dtype=float) for _ in range(5)]
             inflect, minang, n_l = par['inflectAngle'], par['minAngle'], par['n_l']
             A_en = 1.0 / (1.0 + n_l * (1.5707963 / inflect - 1.0))
@@ -228,7 +237,7 @@ def flux():
             return np.stack([a.numpy() for a in arrs]) / n
 
         def legacy(sd):
-            o, d = t3.gen_source_gpu('neutral', n, Lx, Ly, z_src, 0.0, sd)
+            o, d = src('neutral', sd, 0.0)
             f, a = wp.zeros(F, dtype=float), wp.zeros(F, dtype=float)
             wp.launch(t3._trace3d, dim=n, inputs=[mesh.id, o, d, 0.2, 12, sd, 0, 0.34, 0.8, f, a])
             return np.stack([f.numpy(), a.numpy()]) / n

@@ -28,52 +28,47 @@ def _mesh(key, gold):
     return m, geo, phi
 
 
-def _chi2(x, se_x, g, se_g):
-    v = se_x ** 2 + se_g ** 2
-    k = v > 0
-    z2 = (x[k] - g[k]) ** 2 / v[k]
-    return float(z2.mean()), float(np.sqrt(z2.max()))
-
-
-def _cuda_mean_se(fn, seeds):
-    runs = np.stack([fn(s) for s in seeds])
-    return runs.mean(0), runs.std(0, ddof=1) / np.sqrt(len(seeds))
+def _z2(x, g, sg):
+    """x: a high-ray-count device estimate; g, sg: the reference kernel's 8-seed mean and
+    standard error.  Without a systematic difference z = (x - g) / sg is Student-t with 7 degrees
+    of freedom: E[z^2] = 1.4, median(z^2) = 0.49."""
+    k = sg > 0
+    z2 = (x[k] - g[k]) ** 2 / sg[k] ** 2
+    return float(np.median(z2)), float(z2.mean())
 
 
 @pytest.mark.parametrize("key", ["hole", "trench"])
 def test_neutral_vs_reference_kernel(gold, key):
     m, geo, _ = _mesh(key, gold)
-    n = 500_000
-    x, sx = _cuda_mean_se(lambda s: cuda_neutrals(m, geo, gold[f"{key}_bare"], 0.7, s, n) / n,
-                          range(1, 9))
-    chi, zmax = _chi2(x, sx, gold[f"{key}_neutral_mean"], gold[f"{key}_neutral_se"])
-    assert chi < 1.6, (chi, zmax)
+    n = 8_000_000
+    x = cuda_neutrals(m, geo, gold[f"{key}_bare"], 0.7, 1, n) / n
+    med, mean = _z2(x, gold[f"{key}_neutral_mean"], gold[f"{key}_neutral_se"])
+    assert med < 0.75 and mean < 2.2, (med, mean)
     assert x.sum() == pytest.approx(gold[f"{key}_neutral_mean"].sum(), rel=0.03)
 
 
 @pytest.mark.parametrize("key", ["hole", "trench"])
 def test_ion_vs_reference_kernel(gold, key):
     m, geo, _ = _mesh(key, gold)
-    n = 500_000
+    n = 8_000_000
     par = dict(params.PAR)
-    x, sx = _cuda_mean_se(lambda s: cuda_ions(m, geo, par, s, n).T / n, range(1, 9))
+    x = cuda_ions(m, geo, par, 1, n).T / n
     g, sg = gold[f"{key}_ion_mean"], gold[f"{key}_ion_se"]
     for q in range(5):
-        chi, zmax = _chi2(x[q], sx[q], g[q], sg[q])
-        assert chi < 1.6, (q, chi, zmax)
+        med, mean = _z2(x[q], g[q], sg[q])
+        assert med < 0.75 and mean < 2.2, (q, med, mean)
         assert x[q].sum() == pytest.approx(g[q].sum(), rel=0.03)
 
 
 @pytest.mark.parametrize("key", ["hole", "trench"])
 def test_legacy_vs_reference_kernel(gold, key):
     m, geo, _ = _mesh(key, gold)
-    n = 500_000
-    x, sx = _cuda_mean_se(lambda s: np.stack(cuda_legacy(m, dict(geo, periodic_y=0), 0, 0.0, 0.2,
-                                                         12, 0, s, n)) / n, range(1, 9))
+    n = 8_000_000
+    x = np.stack(cuda_legacy(m, dict(geo, periodic_y=0), 0, 0.0, 0.2, 12, 0, 1, n)) / n
     g, sg = gold[f"{key}_legacy_mean"], gold[f"{key}_legacy_se"]
     for q in range(2):
-        chi, zmax = _chi2(x[q], sx[q], g[q], sg[q])
-        assert chi < 1.6, (q, chi, zmax)
+        med, mean = _z2(x[q], g[q], sg[q])
+        assert med < 0.75 and mean < 2.2, (q, med, mean)
 
 
 def _rel_l2(a, b):

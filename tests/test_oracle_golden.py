@@ -123,3 +123,60 @@ def test_depth_metrics_match_reference(sf, key):
     got = [t3.center_depth_3d(g), t3.max_depth_3d(g), t3.center_depth_3d(g, half=0.4)]
     np.testing.assert_allclose(got, sf[f"depth_{key}"], rtol=0, atol=1e-12)
     assert orc.depth3d(g, phi) == pytest.approx(sf[f"depth_{key}"][0], abs=1e-12)
+
+
+# ------------------------------- Monte-Carlo kernels (statistical) -------------------------------
+@pytest.fixture(scope="module")
+def fx():
+    return np.load(os.path.join(GOLDEN, "flux.npz"))
+
+
+def _fx_mesh_geo(fx, key):
+    m = orc.mesh_from_arrays(fx[f"{key}_verts"], fx[f"{key}_faces"])
+    Lx, Ly, Lz, dx, periodic = fx[f"{key}_geo"]
+    return m, dict(Lx=Lx, Ly=Ly, Lz=Lz, dx=dx, periodic_y=int(periodic))
+
+
+def _z2_ok(x, g, sg):
+    """x: a high-ray-count estimate (its own noise negligible); g, sg: the reference kernel's
+    8-seed mean and standard error.  Without a systematic difference z = (x - g) / sg follows
+    Student-t with 7 degrees of freedom: E[z^2] = 1.4, median(z^2) = 0.49."""
+    k = sg > 0
+    z2 = (x[k] - g[k]) ** 2 / sg[k] ** 2
+    return float(np.median(z2)), float(z2.mean())
+
+
+@pytest.mark.parametrize("key", ["hole", "trench"])
+def test_oracle_neutral_estimator_matches_reference_kernel(fx, key):
+    m, geo = _fx_mesh_geo(fx, key)
+    n = 1_000_000
+    x = orc.trace_neutrals(m, geo, geo, fx[f"{key}_bare"], 0.7, 5, n) / n
+    med, mean = _z2_ok(x, fx[f"{key}_neutral_mean"], fx[f"{key}_neutral_se"])
+    assert med < 0.75 and mean < 2.2, (med, mean)
+    assert x.sum() == pytest.approx(fx[f"{key}_neutral_mean"].sum(), rel=0.03)
+
+
+@pytest.mark.parametrize("key", ["hole", "trench"])
+def test_oracle_ion_estimator_matches_reference_kernel(fx, key):
+    import petch_b200.params as P
+    m, geo = _fx_mesh_geo(fx, key)
+    par = dict(P.PAR, periodic_y=geo['periodic_y'])
+    n = 1_000_000
+    x = orc.trace_ions(m, geo, par, 5, n).T / n
+    g, sg = fx[f"{key}_ion_mean"], fx[f"{key}_ion_se"]
+    for q in range(5):
+        med, mean = _z2_ok(x[q], g[q], sg[q])
+        assert med < 0.75 and mean < 2.2, (q, med, mean)
+        assert x[q].sum() == pytest.approx(g[q].sum(), rel=0.03), q
+
+
+@pytest.mark.parametrize("key", ["hole", "trench"])
+def test_oracle_legacy_estimator_matches_reference_kernel(fx, key):
+    m, geo = _fx_mesh_geo(fx, key)
+    n = 1_000_000
+    x = np.stack(orc.trace_legacy(m, dict(geo, periodic_y=0), geo, 0, 0.0, 0.2, 12, 0, 0.34, 0.8,
+                                  5, n)) / n
+    g, sg = fx[f"{key}_legacy_mean"], fx[f"{key}_legacy_se"]
+    for q in range(2):
+        med, mean = _z2_ok(x[q], g[q], sg[q])
+        assert med < 0.75 and mean < 2.2, (q, med, mean)
