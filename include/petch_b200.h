@@ -127,6 +127,12 @@ typedef struct petch_ion_params {  /* the float32 arguments of _trace3d_ion_yiel
     float sigma;        /* ion angular spread of the source (par['ion_ang_sigma']) */
 } petch_ion_params;
 
+/* Tracer configuration for this process (the autotuner's knobs): bvh_width 2 (binary LBVH,
+ * default) or 8 (quantised 8-wide BVH); steps_per_round = traversal steps each warp runs for all
+ * its lanes between shading / refill rounds (default 8).  Applies to later trace / raycast
+ * calls. */
+int petch_tracer_config(int bvh_width, int steps_per_round);
+
 /* Replaces _gen_source + _trace3d_ion_yield (petch/threed.py:441-458, 599-712): n_ion ions
  * generated and traced on the device.  tally4 (16-byte aligned float4[max_tris]) receives per
  * face (sputter, ion-enhanced, passivation, arrival) and ang the cos-weighted arrival; both are

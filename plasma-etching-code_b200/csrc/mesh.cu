@@ -325,15 +325,19 @@ __global__ void __launch_bounds__(kB) k_face_geometry(MeshView m, FaceParams fp)
         double cr[3] = {u[1] * w[2] - u[2] * w[1], u[2] * w[0] - u[0] * w[2], u[0] * w[1] - u[1] * w[0]};
         double area = 0.5 * sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
         m.area[f] = (float)fmax(area, 1.0e-9);
-        float uf[3] = {bf[0] - af[0], bf[1] - af[1], bf[2] - af[2]};
-        float wf[3] = {cf[0] - af[0], cf[1] - af[1], cf[2] - af[2]};
-        float n[3] = {uf[1] * wf[2] - uf[2] * wf[1], uf[2] * wf[0] - uf[0] * wf[2],
-                      uf[0] * wf[1] - uf[1] * wf[0]};
-        float ln = sqrtf(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
-        float inv = ln > 0.0f ? 1.0f / ln : 0.0f;
+        // IEEE float32 without contraction (the normal of near-degenerate faces is sensitive
+        // to fused multiply-adds): normalize(cross(b - a, c - a)) on the float32 vertices
+        float uf[3] = {__fsub_rn(bf[0], af[0]), __fsub_rn(bf[1], af[1]), __fsub_rn(bf[2], af[2])};
+        float wf[3] = {__fsub_rn(cf[0], af[0]), __fsub_rn(cf[1], af[1]), __fsub_rn(cf[2], af[2])};
+        float n[3] = {__fsub_rn(__fmul_rn(uf[1], wf[2]), __fmul_rn(uf[2], wf[1])),
+                      __fsub_rn(__fmul_rn(uf[2], wf[0]), __fmul_rn(uf[0], wf[2])),
+                      __fsub_rn(__fmul_rn(uf[0], wf[1]), __fmul_rn(uf[1], wf[0]))};
+        float ln = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(n[0], n[0]), __fmul_rn(n[1], n[1])),
+                                        __fmul_rn(n[2], n[2])));
+        float inv = ln > 0.0f ? __fdiv_rn(1.0f, ln) : 0.0f;
         double cen[3];
         for (int q = 0; q < 3; ++q) {
-            m.normal[3 * f + q] = n[q] * inv;
+            m.normal[3 * f + q] = __fmul_rn(n[q], inv);
             cen[q] = (a[q] + b[q] + c[q]) / 3.0;
             m.centroid[3 * f + q] = (float)cen[q];
         }

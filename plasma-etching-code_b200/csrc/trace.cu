@@ -16,39 +16,15 @@ namespace {
 constexpr int kTB = 128;
 constexpr unsigned kFull = 0xffffffffu;
 
+// Tracer configuration (process-wide host state, set by petch_tracer_config): BVH width and
+// traversal steps per warp round.
+int g_bvh_width = 2;
+int g_steps = 8;
+
 struct Domain {
     float lx, ly, lz, z_src;
     int periodic;
 };
-
-// _apply_bc (threed.py:289-349) fused with the bounce query: with periodic lateral boundaries, a
-// ray that misses the surface and leaves through x or y before the open top re-enters at the
-// opposite face with the same direction (<= 256 wraps, then one last query, as the reference's
-// loop followed by the kernel's own query).  `o` is updated to the origin the hit is measured from.
-__device__ __forceinline__ HitRec query_bc(const Tracer& T, float3& o, float3 d, const Domain& D,
-                                           int* err) {
-    if (!D.periodic) return closest_hit_wide(T, make_ray(o, d), 1.0e6f, err);
-    for (int w = 0; w < 256; ++w) {
-        HitRec h = closest_hit_wide(T, make_ray(o, d), 1.0e6f, err);
-        if (h.f >= 0) return h;
-        float tx = 1.0e30f, ty = 1.0e30f, tz = 1.0e30f;
-        if (d.x > 1.0e-9f) tx = (D.lx - o.x) / d.x;
-        if (d.x < -1.0e-9f) tx = (0.0f - o.x) / d.x;
-        if (d.y > 1.0e-9f) ty = (D.ly - o.y) / d.y;
-        if (d.y < -1.0e-9f) ty = (0.0f - o.y) / d.y;
-        if (d.z > 1.0e-9f) tz = (D.lz - o.z) / d.z;
-        if (tx < tz && tx < ty && tx > 1.0e-7f) {
-            float hy = o.y + tx * d.y, hz = o.z + tx * d.z;
-            o = make_float3(d.x < 0.0f ? D.lx - 1.0e-4f : 1.0e-4f, hy, hz);
-        } else if (ty < tz && ty < 1.0e29f && ty > 1.0e-7f) {
-            float hx = o.x + ty * d.x, hz = o.z + ty * d.z;
-            o = make_float3(hx, d.y < 0.0f ? D.ly - 1.0e-4f : 1.0e-4f, hz);
-        } else {
-            return h;   // escapes through the open top
-        }
-    }
-    return closest_hit_wide(T, make_ray(o, d), 1.0e6f, err);
-}
 
 // _gen_source (threed.py:441-458): origin uniform on [0,Lx]x[0,Ly] at z_src; ion direction from
 // a Gaussian tilt (sigma) in x and y, neutral direction cosine-distributed about -z.
@@ -97,9 +73,30 @@ __device__ __forceinline__ bool refill(int& ray, int n, int* counter) {
     return false;
 }
 
+// _apply_bc's wrap (threed.py:311-346): a ray that missed leaves through x or y before the open
+// top -> re-enter at the opposite face with the same direction; false if it escapes the top.
+__device__ __forceinline__ bool periodic_wrap(const Domain& D, float3& o, float3 d) {
+    float tx = 1.0e30f, ty = 1.0e30f, tz = 1.0e30f;
+    if (d.x > 1.0e-9f) tx = (D.lx - o.x) / d.x;
+    if (d.x < -1.0e-9f) tx = (0.0f - o.x) / d.x;
+    if (d.y > 1.0e-9f) ty = (D.ly - o.y) / d.y;
+    if (d.y < -1.0e-9f) ty = (0.0f - o.y) / d.y;
+    if (d.z > 1.0e-9f) tz = (D.lz - o.z) / d.z;
+    if (tx < tz && tx < ty && tx > 1.0e-7f) {
+        float hy = o.y + tx * d.y, hz = o.z + tx * d.z;
+        o = make_float3(d.x < 0.0f ? D.lx - 1.0e-4f : 1.0e-4f, hy, hz);
+        return true;
+    }
+    if (ty < tz && ty < 1.0e29f && ty > 1.0e-7f) {
+        float hx = o.x + ty * d.x, hz = o.z + ty * d.z;
+        o = make_float3(hx, d.y < 0.0f ? D.ly - 1.0e-4f : 1.0e-4f, hz);
+        return true;
+    }
+    return false;
+}
+
 }  // namespace
 }  // namespace petch
-
 
 namespace petch {
 namespace {
@@ -116,229 +113,227 @@ __global__ void k_zero_faces(const int* hdr, int MT, float* a, int na, float* b,
         for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < F * nb; i += gridDim.x * blockDim.x) b[i] = 0.0f;
 }
 
-// _trace3d_ion_yield (threed.py:599-712): per ion E ~ N(meanE, sigmaE) clipped at 0; on every hit
+// Per-ray state carried between queries.
+struct RayState {
+    float w, E;
+    int bounce, wraps;
+};
+
+// _trace3d_cov_rr (threed.py:549-596): deposit the weight on every hit, W *= 1 - bare * beta,
+// stop at W <= 1e-6, Russian roulette below 0.1 (survive with probability W / 0.3 at weight
+// 0.3), cosine re-emission; at most 1024 bounces.
+struct NeutralShader {
+    const float* bare;
+    float beta;
+    float* flux;
+    static constexpr int kMaxBounce = 1024;
+    __device__ __forceinline__ void init(Rng& g, const Domain& D, float3& o, float3& d,
+                                         RayState& s) const {
+        source(g, false, 0.0f, D, o, d);
+        s.w = 1.0f;
+    }
+    __device__ __forceinline__ bool hit(Rng& g, const Tracer& T, int f, float t, float3& o,
+                                        float3& d, RayState& s) const {
+        float3 nrm = face_normal(T.m, f);
+        if (dot3(nrm, d) > 0.0f) nrm = -nrm;
+        atomicAdd(flux + f, s.w);
+        float S = (bare ? __ldg(bare + f) : 1.0f) * beta;
+        s.w = s.w - s.w * S;
+        if (s.w <= 1.0e-6f) return false;
+        if (s.w < 0.1f) {
+            if (g.uniform() < (1.0f - s.w / 0.3f)) return false;
+            s.w = 0.3f;
+        }
+        float3 h = o + t * d;
+        d = cosine_emit(g, nrm);
+        o = h + 1.0e-4f * nrm;
+        return true;
+    }
+};
+
+// _trace3d_ion_yield (threed.py:599-712): E ~ N(meanE, sigmaE) clipped at 0; on every hit
 // deposit the yield-weighted sputter / ion-enhanced / passivation rates, the weight and
-// cos * weight; then angle-dependent sticking, energy loss (<= 4 truncated-normal tries),
-// weight reduction and coned-cosine reflection about the specular axis (<= 64 accept-reject
-// draws); at most 1024 bounces.  tal4[f] = (sp, ie, ip, arr), ang[f] = sum cos * w.
-__global__ void __launch_bounds__(kTB) k_ions(MeshView m, Domain D, IonP P, uint32_t seed, int n,
-                                              int* work, float4* __restrict__ tal4,
-                                              float* __restrict__ ang) {
-    extern __shared__ float4 s_wn[];
-    const Tracer T = make_tracer(m, s_wn);
-    const float PI_2 = 1.5707963f;
-    const float sEsp = sqrtf(P.Eth_sp), sEie = sqrtf(P.Eth_ie), sEp = sqrtf(P.Eth_p);
-    int err = 0;
-    int ray = -1, bounce = 0;
-    Rng g;
-    float3 o, d;
-    float E = 0.0f, w = 0.0f;
-    while (true) {
-        if (refill(ray, n, work)) {
-            g.init(seed, 0x696f6e73u, (uint32_t)ray);
-            source(g, true, P.sigma, D, o, d);
-            E = P.meanE + P.sigmaE * g.normal();
-            if (E < 0.0f) E = 0.0f;
-            w = 1.0f;
-            bounce = 0;
-        }
-        if (__all_sync(kFull, ray == -2)) break;
-        if (ray < 0) continue;
-        // ---- one bounce ----
-        HitRec h = query_bc(T, o, d, D, &err);
-        bool done = true;
-        if (h.f >= 0) {
-            float3 nrm = face_normal(m, h.f);
-            if (dot3(nrm, d) > 0.0f) nrm = -nrm;
-            float cosT = -dot3(d, nrm);
-            cosT = fminf(fmaxf(cosT, 0.0f), 1.0f);
-            float incAng = acosf(cosT);
-            float sqrtE = sqrtf(E);
-            float f_sp = fmaxf((1.0f + P.B_sp * (1.0f - cosT * cosT)) * cosT, 0.0f);
-            float f_ie = 1.0f;
-            if (cosT < 0.5f) f_ie = fmaxf(3.0f - 6.0f * incAng / 3.14159265f, 0.0f);
-            float4 dep = make_float4(P.A_sp * fmaxf(sqrtE - sEsp, 0.0f) * f_sp * w,
-                                     P.A_ie * fmaxf(sqrtE - sEie, 0.0f) * f_ie * w,
-                                     P.A_p * fmaxf(sqrtE - sEp, 0.0f) * f_ie * w, w);
-            atomicAdd(tal4 + h.f, dep);
-            atomicAdd(ang + h.f, cosT * w);
-            float stick = 1.0f;
-            if (incAng > P.thrmin) {
-                float rr = (incAng - P.thrmin) / (P.thrmax - P.thrmin);
-                rr = fminf(fmaxf(rr, 0.0f), 1.0f);
-                stick = 1.0f - rr;
-            }
-            if (stick < 1.0f) {
-                float Eref;
-                if (incAng >= P.inflect)
-                    Eref = 1.0f - (1.0f - P.A_en) * (PI_2 - incAng) / (PI_2 - P.inflect);
-                else
-                    Eref = P.A_en * powf(incAng / P.inflect, P.n_l);
-                float newE = Eref * E;
-                for (int e = 0; e < 4; ++e) {
-                    float cand = Eref * E + 0.1f * E * g.normal();
-                    if (cand >= 0.0f && cand <= E) {
-                        newE = cand;
-                        break;
-                    }
-                }
-                newE = fminf(fmaxf(newE, 0.0f), E);
-                if (newE > P.minE) {
-                    E = newE;
-                    w = w - w * stick;
-                    if (w > 1.0e-4f) {
-                        float3 hit = o + h.t * d;
-                        float3 axis = normalize3(d - (2.0f * dot3(d, nrm)) * nrm);
-                        float3 tt, bb;
-                        if (axis.z < -0.9999999f) {
-                            tt = make_float3(0.0f, -1.0f, 0.0f);
-                            bb = make_float3(-1.0f, 0.0f, 0.0f);
-                        } else {
-                            float aa = 1.0f / (1.0f + axis.z);
-                            float cc = -axis.x * axis.y * aa;
-                            tt = make_float3(1.0f - axis.x * axis.x * aa, cc, -axis.x);
-                            bb = make_float3(cc, 1.0f - axis.y * axis.y * aa, -axis.y);
-                        }
-                        float maxcone = PI_2 - fminf(incAng, P.minang);
-                        float theta = 0.0f;
-                        for (int q = 0; q < 64; ++q) {
-                            float uu = sqrtf(g.uniform());
-                            float ss = sqrtf(fmaxf(1.0f - uu, 0.0f));
-                            theta = maxcone * ss;
-                            if (g.uniform() * theta * uu <= cosf(PI_2 * ss) * sinf(theta)) break;
-                        }
-                        float ph = 6.2831853f * g.uniform();
-                        float st = sinf(theta);
-                        float3 nd = (st * cosf(ph)) * tt + (st * sinf(ph)) * bb + cosf(theta) * axis;
-                        nd = normalize3(nd);
-                        float dn = dot3(nd, nrm);
-                        if (dn <= 0.0f) nd = nd - (2.0f * dn) * nrm;
-                        d = nd;
-                        o = hit + 1.0e-4f * nrm;
-                        done = false;
-                    }
-                }
-            }
-        }
-        if (!done && ++bounce >= 1024) done = true;
-        if (done) ray = -1;
+// cos * weight; then angle-dependent sticking, energy loss (<= 4 truncated-normal tries), weight
+// reduction and coned-cosine reflection about the specular axis (<= 64 accept-reject draws);
+// at most 1024 bounces.  tal4[f] = (sp, ie, ip, arr), ang[f] = sum cos * w.
+struct IonShader {
+    IonP P;
+    float4* tal4;
+    float* ang;
+    static constexpr int kMaxBounce = 1024;
+    __device__ __forceinline__ void init(Rng& g, const Domain& D, float3& o, float3& d,
+                                         RayState& s) const {
+        source(g, true, P.sigma, D, o, d);
+        s.E = fmaxf(P.meanE + P.sigmaE * g.normal(), 0.0f);
+        s.w = 1.0f;
     }
-    if (err) atomicOr(work + 1, err);
-}
+    __device__ __forceinline__ bool hit(Rng& g, const Tracer& T, int f, float t, float3& o,
+                                        float3& d, RayState& s) const {
+        const float PI_2 = 1.5707963f;
+        float3 nrm = face_normal(T.m, f);
+        if (dot3(nrm, d) > 0.0f) nrm = -nrm;
+        float cosT = fminf(fmaxf(-dot3(d, nrm), 0.0f), 1.0f);
+        float incAng = acosf(cosT);
+        float sqrtE = sqrtf(s.E);
+        float f_sp = fmaxf((1.0f + P.B_sp * (1.0f - cosT * cosT)) * cosT, 0.0f);
+        float f_ie = 1.0f;
+        if (cosT < 0.5f) f_ie = fmaxf(3.0f - 6.0f * incAng / 3.14159265f, 0.0f);
+        float w = s.w;
+        atomicAdd(tal4 + f, make_float4(P.A_sp * fmaxf(sqrtE - sqrtf(P.Eth_sp), 0.0f) * f_sp * w,
+                                        P.A_ie * fmaxf(sqrtE - sqrtf(P.Eth_ie), 0.0f) * f_ie * w,
+                                        P.A_p * fmaxf(sqrtE - sqrtf(P.Eth_p), 0.0f) * f_ie * w, w));
+        atomicAdd(ang + f, cosT * w);
+        float stick = 1.0f;
+        if (incAng > P.thrmin) stick = 1.0f - fminf(fmaxf((incAng - P.thrmin) / (P.thrmax - P.thrmin), 0.0f), 1.0f);
+        if (stick >= 1.0f) return false;
+        float Eref = incAng >= P.inflect
+                         ? 1.0f - (1.0f - P.A_en) * (PI_2 - incAng) / (PI_2 - P.inflect)
+                         : P.A_en * powf(incAng / P.inflect, P.n_l);
+        const float E = s.E;
+        float newE = Eref * E;
+        for (int e = 0; e < 4; ++e) {
+            float cand = Eref * E + 0.1f * E * g.normal();
+            if (cand >= 0.0f && cand <= E) {
+                newE = cand;
+                break;
+            }
+        }
+        newE = fminf(fmaxf(newE, 0.0f), E);
+        if (newE <= P.minE) return false;
+        s.E = newE;
+        s.w = w - w * stick;
+        if (s.w <= 1.0e-4f) return false;
+        float3 h = o + t * d;
+        float3 axis = normalize3(d - (2.0f * dot3(d, nrm)) * nrm);
+        float3 tt, bb;
+        if (axis.z < -0.9999999f) {
+            tt = make_float3(0.0f, -1.0f, 0.0f);
+            bb = make_float3(-1.0f, 0.0f, 0.0f);
+        } else {
+            float aa = 1.0f / (1.0f + axis.z);
+            float cc = -axis.x * axis.y * aa;
+            tt = make_float3(1.0f - axis.x * axis.x * aa, cc, -axis.x);
+            bb = make_float3(cc, 1.0f - axis.y * axis.y * aa, -axis.y);
+        }
+        float maxcone = PI_2 - fminf(incAng, P.minang);
+        float theta = 0.0f;
+        for (int q = 0; q < 64; ++q) {
+            float uu = sqrtf(g.uniform());
+            float ss = sqrtf(fmaxf(1.0f - uu, 0.0f));
+            theta = maxcone * ss;
+            if (g.uniform() * theta * uu <= cosf(PI_2 * ss) * sinf(theta)) break;
+        }
+        float ph = 6.2831853f * g.uniform();
+        float st = sinf(theta);
+        float3 nd = normalize3((st * cosf(ph)) * tt + (st * sinf(ph)) * bb + cosf(theta) * axis);
+        float dn = dot3(nd, nrm);
+        if (dn <= 0.0f) nd = nd - (2.0f * dn) * nrm;
+        d = nd;
+        o = h + 1.0e-4f * nrm;
+        return true;
+    }
+};
 
-// _trace3d_cov_rr (threed.py:549-596): weighted neutral, deposit the weight on every hit,
-// W *= 1 - bare[f] * beta, stop at W <= 1e-6, Russian roulette below 0.1 (survive with
-// probability W / 0.3 at weight 0.3), cosine re-emission; at most 1024 bounces.
-__global__ void __launch_bounds__(kTB) k_neutrals(MeshView m, Domain D, const float* __restrict__ bare,
-                                                  float beta, uint32_t seed, uint32_t domain, int n,
-                                                  int* work, float* __restrict__ flux) {
+// _trace3d (threed.py:352-406), the legacy species: specular == 1 deposits (1 - R) and reflects
+// specularly below cos_thr with energy retention eta; otherwise the particle sticks with
+// probability `sticking` or at re-emission n_reemit, depositing w and w * cos.
+struct LegacyShader {
+    int ion, n_reemit, specular;
+    float sigma, sticking, cos_thr, eta;
+    float* flux;
+    float* angacc;
+    static constexpr int kMaxBounce = 1 << 30;
+    __device__ __forceinline__ void init(Rng& g, const Domain& D, float3& o, float3& d,
+                                         RayState& s) const {
+        source(g, ion != 0, sigma, D, o, d);
+        s.w = 1.0f;
+    }
+    __device__ __forceinline__ bool hit(Rng& g, const Tracer& T, int f, float t, float3& o,
+                                        float3& d, RayState& s) const {
+        float3 nrm = face_normal(T.m, f);
+        if (dot3(nrm, d) > 0.0f) nrm = -nrm;
+        float cosang = fmaxf(-dot3(d, nrm), 0.0f);
+        float3 h = o + t * d;
+        if (specular == 1) {
+            if (cosang >= cos_thr || s.bounce == n_reemit) {
+                atomicAdd(flux + f, s.w);
+                atomicAdd(angacc + f, s.w * cosang);
+                return false;
+            }
+            float R = (cos_thr - cosang) / cos_thr;
+            float dep = s.w * (1.0f - R);
+            atomicAdd(flux + f, dep);
+            atomicAdd(angacc + f, dep * cosang);
+            s.w = s.w * R * eta;
+            d = d - (2.0f * dot3(d, nrm)) * nrm;
+        } else {
+            if (g.uniform() < sticking || s.bounce == n_reemit) {
+                atomicAdd(flux + f, s.w);
+                atomicAdd(angacc + f, s.w * cosang);
+                return false;
+            }
+            d = cosine_emit(g, nrm);
+        }
+        o = h + 1.0e-4f * nrm;
+        return true;
+    }
+};
+
+// Persistent tracer.  Each warp loops: refill lanes whose ray ended (one atomic per warp), run
+// up to `steps` traversal steps on every lane with an open query, then resolve the lanes whose
+// query finished -- a miss wraps laterally (periodic domains, <= 256 wraps per bounce, then one
+// final query) or ends the ray; a hit goes to the shader, which deposits and either re-emits
+// (new query) or ends the ray.
+template <class S, bool WIDE>
+__global__ void __launch_bounds__(kTB) k_trace(MeshView m, Domain D, S sh, uint32_t seed,
+                                               uint32_t domain, int n, int steps, int* work) {
     extern __shared__ float4 s_wn[];
-    const Tracer T = make_tracer(m, s_wn);
+    const Tracer T = make_tracer(m, s_wn, WIDE);
+    int st_ref[kWStack];
+    float st_t[kWStack];
     int err = 0;
-    int ray = -1, bounce = 0;
+    int ray = -1, phase = 0;   // phase 1: query open, 2: query finished
+    Query q;
+    RayState rs;
     Rng g;
-    float3 o, d;
-    float w = 0.0f;
     while (true) {
         if (refill(ray, n, work)) {
             g.init(seed, domain, (uint32_t)ray);
-            source(g, false, 0.0f, D, o, d);
-            w = 1.0f;
-            bounce = 0;
+            float3 o, d;
+            sh.init(g, D, o, d, rs);
+            rs.bounce = 0;
+            rs.wraps = 0;
+            query_begin(q, T, o, d, 1.0e6f, WIDE);
+            phase = 1;
         }
         if (__all_sync(kFull, ray == -2)) break;
-        if (ray < 0) continue;
-        HitRec h = query_bc(T, o, d, D, &err);
-        bool done = true;
-        if (h.f >= 0) {
-            float3 nrm = face_normal(m, h.f);
-            if (dot3(nrm, d) > 0.0f) nrm = -nrm;
-            atomicAdd(flux + h.f, w);
-            float S = (bare ? __ldg(bare + h.f) : 1.0f) * beta;
-            w = w - w * S;
-            if (w > 1.0e-6f) {
-                bool alive = true;
-                if (w < 0.1f) {
-                    if (g.uniform() < (1.0f - w / 0.3f)) alive = false;
-                    else w = 0.3f;
-                }
-                if (alive) {
-                    float3 hit = o + h.t * d;
-                    d = cosine_emit(g, nrm);
-                    o = hit + 1.0e-4f * nrm;
-                    done = false;
-                }
+        for (int s = 0; s < steps; ++s) {
+            if (!__any_sync(kFull, phase == 1)) break;
+            if (phase == 1) {
+                bool fin = WIDE ? step_wide(T, q, st_ref, st_t, &err)
+                                : step_binary(T, q, st_ref, st_t, &err);
+                if (fin) phase = 2;
             }
         }
-        if (!done && ++bounce >= 1024) done = true;
-        if (done) ray = -1;
-    }
-    if (err) atomicOr(work + 1, err);
-}
-
-// _trace3d (threed.py:352-406), the legacy first-hit / fixed-re-emission species used when
-// ion_reflection is off: specular == 1 deposits (1 - R) and reflects specularly below cos_thr
-// with energy retention eta; otherwise the particle sticks with probability `sticking` or after
-// n_reemit re-emissions, depositing its weight and weight * cos.
-__global__ void __launch_bounds__(kTB) k_legacy(MeshView m, Domain D, int ion, float sigma,
-                                                float sticking, int n_reemit, int specular,
-                                                float cos_thr, float eta, uint32_t seed,
-                                                uint32_t domain, int n, int* work,
-                                                float* __restrict__ flux, float* __restrict__ angacc) {
-    extern __shared__ float4 s_wn[];
-    const Tracer T = make_tracer(m, s_wn);
-    int err = 0;
-    int ray = -1, bounce = 0;
-    Rng g;
-    float3 o, d;
-    float w = 0.0f;
-    Domain Dn = D;
-    Dn.periodic = 0;
-    while (true) {
-        if (refill(ray, n, work)) {
-            g.init(seed, domain, (uint32_t)ray);
-            source(g, ion != 0, sigma, D, o, d);
-            w = 1.0f;
-            bounce = 0;
-        }
-        if (__all_sync(kFull, ray == -2)) break;
-        if (ray < 0) continue;
-        HitRec h = query_bc(T, o, d, Dn, &err);
-        bool done = true;
-        if (h.f >= 0) {
-            float3 nrm = face_normal(m, h.f);
-            if (dot3(nrm, d) > 0.0f) nrm = -nrm;
-            float cosang = fmaxf(-dot3(d, nrm), 0.0f);
-            if (specular == 1) {
-                if (cosang >= cos_thr || bounce == n_reemit) {
-                    atomicAdd(flux + h.f, w);
-                    atomicAdd(angacc + h.f, w * cosang);
-                } else {
-                    float R = (cos_thr - cosang) / cos_thr;
-                    float dep = w * (1.0f - R);
-                    atomicAdd(flux + h.f, dep);
-                    atomicAdd(angacc + h.f, dep * cosang);
-                    w = w * R * eta;
-                    float3 hit = o + h.t * d;
-                    d = d - (2.0f * dot3(d, nrm)) * nrm;
-                    o = hit + 1.0e-4f * nrm;
-                    done = false;
-                }
+        if (phase == 2) {
+            float3 o = q.r.o, d = q.r.d;
+            bool cont;
+            if (q.f < 0) {
+                cont = D.periodic && rs.wraps < 256 && periodic_wrap(D, o, d);
+                if (cont) ++rs.wraps;
             } else {
-                float u = g.uniform();
-                if (u < sticking || bounce == n_reemit) {
-                    atomicAdd(flux + h.f, w);
-                    atomicAdd(angacc + h.f, w * cosang);
-                } else {
-                    float3 hit = o + h.t * d;
-                    d = cosine_emit(g, nrm);
-                    o = hit + 1.0e-4f * nrm;
-                    done = false;
-                }
+                cont = sh.hit(g, T, q.f, q.t, o, d, rs);
+                rs.wraps = 0;
+                if (cont && ++rs.bounce >= S::kMaxBounce) cont = false;
+            }
+            if (cont) {
+                query_begin(q, T, o, d, 1.0e6f, WIDE);
+                phase = 1;
+            } else {
+                ray = -1;
+                phase = 0;
             }
         }
-        if (!done && ++bounce > n_reemit) done = true;
-        if (done) ray = -1;
     }
     if (err) atomicOr(work + 1, err);
 }
@@ -408,16 +403,21 @@ __global__ void __launch_bounds__(kTB) k_warmstart(MeshView prev, const float* _
 __global__ void __launch_bounds__(kTB) k_raycast(MeshView m, const float* __restrict__ o,
                                                  const float* __restrict__ d, int n, float tmax,
                                                  int* __restrict__ face, float* __restrict__ t,
-                                                 int* work) {
+                                                 int* work, int wide) {
     extern __shared__ float4 s_wn[];
-    const Tracer T = make_tracer(m, s_wn);
+    const Tracer T = make_tracer(m, s_wn, wide);
+    int st_ref[kWStack];
+    float st_t[kWStack];
     int err = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        float3 oo = make_float3(o[3 * i], o[3 * i + 1], o[3 * i + 2]);
-        float3 dd = make_float3(d[3 * i], d[3 * i + 1], d[3 * i + 2]);
-        HitRec h = closest_hit_wide(T, make_ray(oo, dd), tmax, &err);
-        face[i] = h.f;
-        t[i] = h.f >= 0 ? h.t : 0.0f;
+        Query q;
+        query_begin(q, T, make_float3(o[3 * i], o[3 * i + 1], o[3 * i + 2]),
+                    make_float3(d[3 * i], d[3 * i + 1], d[3 * i + 2]), tmax, wide);
+        if (q.cur != kDone)
+            while (!(wide ? step_wide(T, q, st_ref, st_t, &err) : step_binary(T, q, st_ref, st_t, &err))) {
+            }
+        face[i] = q.f;
+        t[i] = q.f >= 0 ? q.t : 0.0f;
     }
     if (err) atomicOr(work + 1, err);
 }
@@ -432,6 +432,7 @@ __global__ void __launch_bounds__(kTB) k_nearest(MeshView m, const float* __rest
 }
 
 constexpr int kSmemBytes = kSmemNodes * 96;
+
 
 int persistent_blocks(const void* kernel, int block) {
     int per_sm = 0;
@@ -456,6 +457,30 @@ static Domain to_domain(const petch_domain* d) {
     return D;
 }
 
+template <class S>
+static int launch_trace(const MeshView& m, const Domain& D, const S& sh, uint32_t seed,
+                        uint32_t domain, int n, int* work, cudaStream_t st, const char* what) {
+    const int steps = g_steps;
+    if (g_bvh_width == 2) {
+        k_trace<S, false><<<persistent_blocks((const void*)k_trace<S, false>, kTB), kTB, kSmemBytes, st>>>(
+            m, D, sh, seed, domain, n, steps, work);
+    } else {
+        k_trace<S, true><<<persistent_blocks((const void*)k_trace<S, true>, kTB), kTB, kSmemBytes, st>>>(
+            m, D, sh, seed, domain, n, steps, work);
+    }
+    PETCH_LAUNCH_CHECK(what);
+    return PETCH_OK;
+}
+
+extern "C" int petch_tracer_config(int bvh_width, int steps_per_round) {
+    PETCH_REQUIRE(bvh_width == 2 || bvh_width == 8, "petch_tracer_config: bvh_width must be 2 or 8");
+    PETCH_REQUIRE(steps_per_round >= 1 && steps_per_round <= 4096,
+                  "petch_tracer_config: steps_per_round must be in [1, 4096]");
+    g_bvh_width = bvh_width;
+    g_steps = steps_per_round;
+    return PETCH_OK;
+}
+
 extern "C" int petch_trace_ions(const void* mesh, int max_tris, int max_verts,
                                 const petch_domain* dom, const petch_ion_params* p, uint32_t seed,
                                 int n_ion, float* tally4, float* ang, int* work, void* stream) {
@@ -464,16 +489,17 @@ extern "C" int petch_trace_ions(const void* mesh, int max_tris, int max_verts,
     PETCH_REQUIRE(((uintptr_t)tally4 & 15) == 0, "petch_trace_ions: tally4 must be 16-byte aligned");
     cudaStream_t st = as_stream(stream);
     MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
-    IonP P{p->meanE, p->sigmaE, p->A_sp, p->Eth_sp, p->B_sp, p->A_ie, p->Eth_ie, p->A_p, p->Eth_p,
-           p->inflect, p->minang, p->n_l, p->A_en, p->minE, p->thrmin, p->thrmax, p->sigma};
+    IonShader sh;
+    sh.P = IonP{p->meanE, p->sigmaE, p->A_sp, p->Eth_sp, p->B_sp, p->A_ie, p->Eth_ie, p->A_p,
+                p->Eth_p, p->inflect, p->minang, p->n_l, p->A_en, p->minE, p->thrmin, p->thrmax,
+                p->sigma};
+    sh.tal4 = (float4*)tally4;
+    sh.ang = ang;
     k_zero_faces<<<grid_for(4LL * max_tris, 256), 256, 0, st>>>(m.hdr, max_tris, tally4, 4, ang, 1);
     PETCH_LAUNCH_CHECK("k_zero_faces");
     PETCH_CUDA(cudaMemsetAsync(work, 0, sizeof(int), st), "reset ray counter");
     if (n_ion == 0) return PETCH_OK;
-    k_ions<<<persistent_blocks((const void*)k_ions, kTB), kTB, kSmemBytes, st>>>(
-        m, to_domain(dom), P, seed, n_ion, work, (float4*)tally4, ang);
-    PETCH_LAUNCH_CHECK("k_ions");
-    return PETCH_OK;
+    return launch_trace(m, to_domain(dom), sh, seed, 0x696f6e73u, n_ion, work, st, "k_trace<ions>");
 }
 
 extern "C" int petch_trace_neutrals(const void* mesh, int max_tris, int max_verts,
@@ -484,14 +510,13 @@ extern "C" int petch_trace_neutrals(const void* mesh, int max_tris, int max_vert
     PETCH_REQUIRE(n_neu >= 0 && max_tris > 0 && max_verts > 0, "petch_trace_neutrals: bad size");
     cudaStream_t st = as_stream(stream);
     MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
+    NeutralShader sh{bare, beta, flux};
     k_zero_faces<<<grid_for(max_tris, 256), 256, 0, st>>>(m.hdr, max_tris, flux, 1, nullptr, 0);
     PETCH_LAUNCH_CHECK("k_zero_faces");
     PETCH_CUDA(cudaMemsetAsync(work, 0, sizeof(int), st), "reset ray counter");
     if (n_neu == 0) return PETCH_OK;
-    k_neutrals<<<persistent_blocks((const void*)k_neutrals, kTB), kTB, kSmemBytes, st>>>(
-        m, to_domain(dom), bare, beta, seed, 0x6e657500u ^ stream_id, n_neu, work, flux);
-    PETCH_LAUNCH_CHECK("k_neutrals");
-    return PETCH_OK;
+    return launch_trace(m, to_domain(dom), sh, seed, 0x6e657500u ^ stream_id, n_neu, work, st,
+                        "k_trace<neutrals>");
 }
 
 extern "C" int petch_trace_legacy(const void* mesh, int max_tris, int max_verts,
@@ -504,15 +529,15 @@ extern "C" int petch_trace_legacy(const void* mesh, int max_tris, int max_verts,
                   "petch_trace_legacy: bad size");
     cudaStream_t st = as_stream(stream);
     MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
+    LegacyShader sh{ion, n_reemit, specular, sigma, sticking, cos_thr, eta, flux, angacc};
     k_zero_faces<<<grid_for(max_tris, 256), 256, 0, st>>>(m.hdr, max_tris, flux, 1, angacc, 1);
     PETCH_LAUNCH_CHECK("k_zero_faces");
     PETCH_CUDA(cudaMemsetAsync(work, 0, sizeof(int), st), "reset ray counter");
     if (n == 0) return PETCH_OK;
-    k_legacy<<<persistent_blocks((const void*)k_legacy, kTB), kTB, kSmemBytes, st>>>(
-        m, to_domain(dom), ion, sigma, sticking, n_reemit, specular, cos_thr, eta, seed,
-        ion ? 0x6c696f6eu : 0x6c6e6575u, n, work, flux, angacc);
-    PETCH_LAUNCH_CHECK("k_legacy");
-    return PETCH_OK;
+    Domain D = to_domain(dom);
+    D.periodic = 0;
+    return launch_trace(m, D, sh, seed, ion ? 0x6c696f6eu : 0x6c6e6575u, n, work, st,
+                        "k_trace<legacy>");
 }
 
 extern "C" int petch_extend_velocity(const void* mesh, int max_tris, int max_verts,
@@ -552,7 +577,8 @@ extern "C" int petch_raycast(const void* mesh, int max_tris, int max_verts, cons
     PETCH_REQUIRE(n >= 0, "petch_raycast: n must be >= 0");
     if (n == 0) return PETCH_OK;
     MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
-    k_raycast<<<grid_for(n, kTB, 16), kTB, kSmemBytes, as_stream(stream)>>>(m, o, d, n, tmax, face, t, work);
+    k_raycast<<<grid_for(n, kTB, 16), kTB, kSmemBytes, as_stream(stream)>>>(m, o, d, n, tmax, face, t, work,
+                                                                          g_bvh_width != 2);
     PETCH_LAUNCH_CHECK("k_raycast");
     return PETCH_OK;
 }

@@ -227,21 +227,50 @@ __device__ __forceinline__ HitRec closest_hit(const MeshView& m, int L, const Ra
 }
 
 // ---------------------------------------------------------------------------------------------
-// 8-wide quantised BVH traversal (closest hit).  Children are tested together, sorted by entry
-// distance with a fixed 19-comparator network in registers, the nearest is visited next and the
-// others are pushed far-to-near with their entry distance, so popped entries beyond the current
-// closest hit are skipped without a fetch.  The first `nsm` nodes (the top levels, BFS order)
-// are read from shared memory.
+// Resumable closest-hit queries.  A Query advances one BVH node or one leaf per step, so a warp
+// can run a bounded number of steps for all its lanes, shade the lanes whose query finished and
+// start new queries, instead of waiting for its slowest lane's whole traversal.
+//
+// Two acceleration structures share the interface:
+//  * 8-wide quantised BVH (WIDE): children tested together, sorted by entry distance with a fixed
+//    19-comparator network in registers; the nearest is visited next, the others pushed
+//    far-to-near with their entry distance (entries beyond the current hit are popped without a
+//    fetch); the first `nsm` nodes (the top levels, BFS order) come from shared memory.
+//  * binary LBVH: both child boxes per node (64 B), near child first.
+// Box planes are decoded in space (p + q * s) before the ray offset is taken, so the slab test
+// keeps the sign of (plane - origin) for rays nearly parallel to a plane.
 // ---------------------------------------------------------------------------------------------
 constexpr int kWStack = 48;
 constexpr int kSmemNodes = 128;   // 12 KB of the tree top per block
+constexpr int kDone = -2147483647 - 1;
 
 struct Tracer {
     MeshView m;
     int WN;                    // wide nodes
-    const float4* snodes;      // shared-memory copy of nodes [0, nsm)
+    int L;                     // binary leaves
+    const float4* snodes;      // shared-memory copy of wide nodes [0, nsm)
     int nsm;
 };
+
+struct Query {
+    Ray r;
+    float t;    // closest hit so far
+    int f;      // its face, -1 if none
+    int cur;    // current node ref (kDone when finished)
+    int sp;     // stack depth
+    int visits;
+};
+
+__device__ __forceinline__ void query_begin(Query& q, const Tracer& T, float3 o, float3 d,
+                                            float tmax, bool wide) {
+    q.r = make_ray(o, d);
+    q.t = tmax;
+    q.f = -1;
+    q.sp = 0;
+    q.visits = 0;
+    if (wide) q.cur = T.WN > 0 ? 0 : kDone;
+    else q.cur = T.L <= 0 ? kDone : (T.L == 1 ? ~0 : 0);
+}
 
 __device__ __forceinline__ void cas(float& ka, int& va, float& kb, int& vb) {
     bool sw = kb < ka;
@@ -258,57 +287,70 @@ __device__ __forceinline__ float qbyte(uint32_t lo4, uint32_t hi4, int k) {
     return (float)((w >> (8 * (k & 3))) & 255u);
 }
 
-__device__ __forceinline__ HitRec closest_hit_wide(const Tracer& T, const Ray& r, float tmax,
-                                                   int* err) {
-    HitRec h{tmax, -1};
-    if (T.WN <= 0) return h;
-    int st_ref[kWStack];
-    float st_t[kWStack];
-    int sp = 0;
-    int cur = 0;
-    const float4* gn = reinterpret_cast<const float4*>(T.m.wnodes);
-    for (int visits = 0; visits < kMaxVisits; ++visits) {
-        if (cur >= 0) {
-            float4 v0, v1, v2, v3, v4, v5;
-            if (cur < T.nsm) {
-                const float4* p = T.snodes + 6 * cur;
-                v0 = p[0]; v1 = p[1]; v2 = p[2]; v3 = p[3]; v4 = p[4]; v5 = p[5];
-            } else {
-                const float4* p = gn + 6 * (long long)cur;
-                v0 = __ldg(p); v1 = __ldg(p + 1); v2 = __ldg(p + 2);
-                v3 = __ldg(p + 3); v4 = __ldg(p + 4); v5 = __ldg(p + 5);
-            }
-            uint32_t meta = __float_as_uint(v0.w);
-            float sx = __int_as_float((int)((meta & 255u) << 23));
-            float sy = __int_as_float((int)(((meta >> 8) & 255u) << 23));
-            float sz = __int_as_float((int)(((meta >> 16) & 255u) << 23));
-            int nc = (int)(meta >> 24);
-            float ax0 = (v0.x - r.o.x) * r.inv.x, ax1 = sx * r.inv.x;
-            float ay0 = (v0.y - r.o.y) * r.inv.y, ay1 = sy * r.inv.y;
-            float az0 = (v0.z - r.o.z) * r.inv.z, az1 = sz * r.inv.z;
-            uint32_t qx0 = __float_as_uint(v1.x), qx1 = __float_as_uint(v1.y);
-            uint32_t qx2 = __float_as_uint(v1.z), qx3 = __float_as_uint(v1.w);
-            uint32_t qy0 = __float_as_uint(v2.x), qy1 = __float_as_uint(v2.y);
-            uint32_t qy2 = __float_as_uint(v2.z), qy3 = __float_as_uint(v2.w);
-            uint32_t qz0 = __float_as_uint(v3.x), qz1 = __float_as_uint(v3.y);
-            uint32_t qz2 = __float_as_uint(v3.z), qz3 = __float_as_uint(v3.w);
-            int ch[8] = {__float_as_int(v4.x), __float_as_int(v4.y), __float_as_int(v4.z),
-                         __float_as_int(v4.w), __float_as_int(v5.x), __float_as_int(v5.y),
-                         __float_as_int(v5.z), __float_as_int(v5.w)};
-            float key[8];
-            int nh = 0;
+// Pop the nearest stacked entry that can still beat the current hit; false if none.
+__device__ __forceinline__ bool query_pop(Query& q, const int* st_ref, const float* st_t) {
+    while (q.sp > 0) {
+        --q.sp;
+        if (st_t[q.sp] <= q.t) {
+            q.cur = st_ref[q.sp];
+            return true;
+        }
+    }
+    q.cur = kDone;
+    return false;
+}
+
+__device__ __forceinline__ void query_leaf(const Tracer& T, Query& q, int f0, int f1) {
+    for (int f = f0; f < f1; ++f)
+        if (hit_triangle(q.r, tri_v(T.m.tri, f, 0), tri_v(T.m.tri, f, 1), tri_v(T.m.tri, f, 2), q.t))
+            q.f = f;
+}
+
+// One step of the 8-wide traversal; returns true once the query has finished.
+__device__ __forceinline__ bool step_wide(const Tracer& T, Query& q, int* st_ref, float* st_t,
+                                          int* err) {
+    if (++q.visits > kMaxVisits) {
+        *err |= 1;
+        q.cur = kDone;
+        return true;
+    }
+    const int cur = q.cur;
+    if (cur >= 0) {
+        float4 v0, v1, v2, v3, v4, v5;
+        if (cur < T.nsm) {
+            const float4* p = T.snodes + 6 * cur;
+            v0 = p[0]; v1 = p[1]; v2 = p[2]; v3 = p[3]; v4 = p[4]; v5 = p[5];
+        } else {
+            const float4* p = reinterpret_cast<const float4*>(T.m.wnodes) + 6 * (long long)cur;
+            v0 = __ldg(p); v1 = __ldg(p + 1); v2 = __ldg(p + 2);
+            v3 = __ldg(p + 3); v4 = __ldg(p + 4); v5 = __ldg(p + 5);
+        }
+        const Ray& r = q.r;
+        uint32_t meta = __float_as_uint(v0.w);
+        float sx = __int_as_float((int)((meta & 255u) << 23));
+        float sy = __int_as_float((int)(((meta >> 8) & 255u) << 23));
+        float sz = __int_as_float((int)(((meta >> 16) & 255u) << 23));
+        int nc = (int)(meta >> 24);
+        int ch[8] = {__float_as_int(v4.x), __float_as_int(v4.y), __float_as_int(v4.z),
+                     __float_as_int(v4.w), __float_as_int(v5.x), __float_as_int(v5.y),
+                     __float_as_int(v5.z), __float_as_int(v5.w)};
+        float key[8];
+        int nh = 0;
 #pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                float tlx = ax0 + qbyte(qx0, qx1, k) * ax1, thx = ax0 + qbyte(qx2, qx3, k) * ax1;
-                float tly = ay0 + qbyte(qy0, qy1, k) * ay1, thy = ay0 + qbyte(qy2, qy3, k) * ay1;
-                float tlz = az0 + qbyte(qz0, qz1, k) * az1, thz = az0 + qbyte(qz2, qz3, k) * az1;
-                float tn = fmaxf(fmaxf(fminf(tlx, thx), fminf(tly, thy)), fmaxf(fminf(tlz, thz), 0.0f));
-                float tf = fminf(fminf(fmaxf(tlx, thx), fmaxf(tly, thy)), fminf(fmaxf(tlz, thz), h.t));
-                bool hit = (k < nc) && (tn <= tf * 1.00001f + 1.0e-7f);
-                key[k] = hit ? tn : 3.0e38f;
-                nh += hit;
-            }
-            if (nh > 0) {
+        for (int k = 0; k < 8; ++k) {
+            float lx = fmaf(qbyte(__float_as_uint(v1.x), __float_as_uint(v1.y), k), sx, v0.x);
+            float hx = fmaf(qbyte(__float_as_uint(v1.z), __float_as_uint(v1.w), k), sx, v0.x);
+            float ly = fmaf(qbyte(__float_as_uint(v2.x), __float_as_uint(v2.y), k), sy, v0.y);
+            float hy = fmaf(qbyte(__float_as_uint(v2.z), __float_as_uint(v2.w), k), sy, v0.y);
+            float lz = fmaf(qbyte(__float_as_uint(v3.x), __float_as_uint(v3.y), k), sz, v0.z);
+            float hz = fmaf(qbyte(__float_as_uint(v3.z), __float_as_uint(v3.w), k), sz, v0.z);
+            float tn;
+            bool hit = (k < nc) && slab(r, lx, hx, ly, hy, lz, hz, q.t, tn);
+            key[k] = hit ? tn : 3.0e38f;
+            nh += hit;
+        }
+        if (nh > 0) {
+            if (nh > 1) {
                 cas(key[0], ch[0], key[1], ch[1]); cas(key[2], ch[2], key[3], ch[3]);
                 cas(key[4], ch[4], key[5], ch[5]); cas(key[6], ch[6], key[7], ch[7]);
                 cas(key[0], ch[0], key[2], ch[2]); cas(key[1], ch[1], key[3], ch[3]);
@@ -322,45 +364,77 @@ __device__ __forceinline__ HitRec closest_hit_wide(const Tracer& T, const Ray& r
 #pragma unroll
                 for (int k = 7; k >= 1; --k)
                     if (k < nh) {
-                        if (sp < kWStack) {
-                            st_ref[sp] = ch[k];
-                            st_t[sp] = key[k];
-                            ++sp;
+                        if (q.sp < kWStack) {
+                            st_ref[q.sp] = ch[k];
+                            st_t[q.sp] = key[k];
+                            ++q.sp;
                         } else {
                             *err |= 1;
                         }
                     }
-                cur = ch[0];
-                continue;
+                q.cur = ch[0];
+            } else {
+                int c = ch[0];
+#pragma unroll
+                for (int k = 1; k < 8; ++k) c = key[k] < 1.0e38f ? ch[k] : c;
+                q.cur = c;
             }
-        } else {
-            int code = -cur - 1;
-            int f0 = code >> 3, f1 = f0 + (code & 7);
-            for (int f = f0; f < f1; ++f)
-                if (hit_triangle(r, tri_v(T.m.tri, f, 0), tri_v(T.m.tri, f, 1), tri_v(T.m.tri, f, 2), h.t))
-                    h.f = f;
+            return false;
         }
-        bool found = false;
-        while (sp > 0) {
-            --sp;
-            if (st_t[sp] <= h.t) {
-                cur = st_ref[sp];
-                found = true;
-                break;
-            }
-        }
-        if (!found) return h;
+    } else {
+        int code = -cur - 1;
+        int f0 = code >> 3;
+        query_leaf(T, q, f0, f0 + (code & 7));
     }
-    *err |= 1;
-    return h;
+    return !query_pop(q, st_ref, st_t);
+}
+
+// One step of the binary traversal; returns true once the query has finished.
+__device__ __forceinline__ bool step_binary(const Tracer& T, Query& q, int* st_ref, float* st_t,
+                                            int* err) {
+    if (++q.visits > kMaxVisits) {
+        *err |= 1;
+        q.cur = kDone;
+        return true;
+    }
+    const int node = q.cur;
+    if (node >= 0) {
+        const float4* n = T.m.nodes + 4 * node;
+        float4 n0 = __ldg(n), n1 = __ldg(n + 1), n2 = __ldg(n + 2), n3 = __ldg(n + 3);
+        float t0, t1;
+        bool h0 = slab(q.r, n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, q.t, t0);
+        bool h1 = slab(q.r, n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, q.t, t1);
+        int c0 = __float_as_int(n3.x), c1 = __float_as_int(n3.y);
+        if (h0 && h1) {
+            bool swap = t1 < t0;
+            if (q.sp < kWStack) {
+                st_ref[q.sp] = swap ? c0 : c1;
+                st_t[q.sp] = swap ? t0 : t1;
+                ++q.sp;
+            } else {
+                *err |= 1;
+            }
+            q.cur = swap ? c1 : c0;
+            return false;
+        }
+        if (h0 || h1) {
+            q.cur = h0 ? c0 : c1;
+            return false;
+        }
+    } else {
+        int l = ~node;
+        query_leaf(T, q, __ldg(T.m.leaf_start + l), __ldg(T.m.leaf_start + l + 1));
+    }
+    return !query_pop(q, st_ref, st_t);
 }
 
 // Stage the top of the wide tree in shared memory (call from every thread of the block).
-__device__ __forceinline__ Tracer make_tracer(const MeshView& m, float4* smem) {
+__device__ __forceinline__ Tracer make_tracer(const MeshView& m, float4* smem, bool wide) {
     Tracer T;
     T.m = m;
     T.WN = m.hdr[HDR_WN];
-    T.nsm = min(T.WN, kSmemNodes);
+    T.L = min(m.hdr[HDR_L], m.MT);
+    T.nsm = wide ? min(T.WN, kSmemNodes) : 0;
     const float4* g = reinterpret_cast<const float4*>(m.wnodes);
     for (int i = threadIdx.x; i < 6 * T.nsm; i += blockDim.x) smem[i] = __ldg(g + i);
     __syncthreads();

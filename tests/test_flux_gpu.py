@@ -109,6 +109,23 @@ def test_ion_vs_oracle_rel_l2(hole):
         assert np.sqrt(max(err ** 2 - 1.5 * noise ** 2, 0.0)) <= 0.02, (q, err, noise)
 
 
+@pytest.mark.parametrize("width,steps", [(2, 2), (2, 64), (8, 4), (8, 64)])
+def test_tracer_configs_agree(width, steps):
+    """Every BVH width / steps-per-round setting is the same estimator (same Philox paths up to
+    float rounding of the traversal order): totals within noise, per-face within 5 %."""
+    phi, geo = small_feature(False)
+    m = cuda_mesh(phi, geo['dx'], geo)
+    from petch_b200 import _lib
+    ref = cuda_neutrals(m, geo, None, 0.7, 7, 1_000_000)
+    try:
+        _lib.call("petch_tracer_config", width, steps)
+        x = cuda_neutrals(m, geo, None, 0.7, 7, 1_000_000)
+    finally:
+        _lib.call("petch_tracer_config", 2, 8)
+    assert _rel_l2(x, ref) < 0.01
+    assert x.sum() == pytest.approx(ref.sum(), rel=1e-3)
+
+
 def test_replay_same_seed_same_paths():
     """Philox streams are keyed by (seed, ray): the same seed reproduces every path; the
     per-face tallies then differ only by float-atomic summation order."""

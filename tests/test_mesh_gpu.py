@@ -63,8 +63,15 @@ def test_sphere_is_closed_and_outward():
     assert abs(m.area[:m.F].double().sum().item() / (4 * np.pi * 1.3 ** 2) - 1) < 5e-3
 
 
+@pytest.fixture(params=[8, 2])
+def width(request):
+    _lib.call("petch_tracer_config", request.param, 16)
+    yield request.param
+    _lib.call("petch_tracer_config", 2, 8)
+
+
 @pytest.mark.parametrize("name", ["sphere", "pit_hole", "config0_seed"])
-def test_raycast_matches_oracle(name):
+def test_raycast_matches_oracle(name, width):
     phi, dx, geo = FIELDS[name]
     m = cuda_mesh(phi, dx, geo)
     o = orc.mesh_build(phi, dx, geo)
