@@ -138,6 +138,8 @@ def run_b200(args):
 
     rays = []
 
+    work_q = []
+
     def after(step, eng, st):
         if step >= W:
             e = torch.cuda.Event(enable_timing=True)
@@ -145,6 +147,7 @@ def run_b200(args):
             ev[step].append(e)
             n_fp = 4 if step == 0 else 1
             rays.append(RAYS + 2 * RAYS * n_fp)
+            work_q.append((st['queries'], st['visits']))
         if step == W + K - 1:
             torch.cuda.synchronize()
             info['launch1'] = _lib.launch_count()
@@ -190,6 +193,14 @@ def run_b200(args):
                         "L2 bound; HBM fraction reported as the contract asks, rays/s beside it"}
         del eng
     mrays = float(np.sum(rays)) * world / total_s / 1e6
+    q_tot = float(sum(a for a, _ in work_q)) * world
+    v_tot = float(sum(b for _, b in work_q)) * world
+    tracer_s = sum(sum(v) for v in kms.values()) / 1e3 if kms else total_s
+    if roof is not None:
+        roof["bvh_queries_per_s"] = q_tot / tracer_s
+        roof["node_visits_per_s"] = v_tot / tracer_s
+        roof["node_fetch_GBps"] = v_tot * 64 / tracer_s / 1e9
+        roof["visits_per_query"] = v_tot / max(q_tot, 1.0)
     out = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": K,
            "warmup": W, "ms_per_step": 1e3 * total_s / K, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 chemistry)",

@@ -136,9 +136,10 @@ int petch_tracer_config(int bvh_width, int steps_per_round);
 /* Replaces _gen_source + _trace3d_ion_yield (petch/threed.py:441-458, 599-712): n_ion ions
  * generated and traced on the device.  tally4 (16-byte aligned float4[max_tris]) receives per
  * face (sputter, ion-enhanced, passivation, arrival) and ang the cos-weighted arrival; both are
- * zeroed first.  work: int[2] device words: [0] ray counter (reset by every trace call), [1] error
- * bits OR-ed by every kernel (1 = traversal bound hit, 2 = active list full) until the caller
- * clears them. */
+ * zeroed first.  work: int[6] device words, 8-byte aligned: [0] ray counter (reset by every trace
+ * call), [1] error bits OR-ed by every kernel (1 = traversal bound hit, 2 = active list full)
+ * until the caller clears them, [2..3] uint64 BVH queries and [4..5] uint64 node + leaf visits,
+ * accumulated by every trace call until the caller clears them. */
 int petch_trace_ions(const void* mesh, int max_tris, int max_verts, const petch_domain* dom,
                      const petch_ion_params* p, uint32_t seed, int n_ion, float* tally4,
                      float* ang, int* work, void* stream);

@@ -292,6 +292,7 @@ __global__ void __launch_bounds__(kTB) k_trace(MeshView m, Domain D, S sh, uint3
     int st_ref[kWStack];
     float st_t[kWStack];
     int err = 0;
+    unsigned long long n_query = 0, n_visit = 0;
     int ray = -1, phase = 0;   // phase 1: query open, 2: query finished
     Query q;
     RayState rs;
@@ -304,6 +305,7 @@ __global__ void __launch_bounds__(kTB) k_trace(MeshView m, Domain D, S sh, uint3
             rs.bounce = 0;
             rs.wraps = 0;
             query_begin(q, T, o, d, 1.0e6f, WIDE);
+            ++n_query;
             phase = 1;
         }
         if (__all_sync(kFull, ray == -2)) break;
@@ -326,8 +328,10 @@ __global__ void __launch_bounds__(kTB) k_trace(MeshView m, Domain D, S sh, uint3
                 rs.wraps = 0;
                 if (cont && ++rs.bounce >= S::kMaxBounce) cont = false;
             }
+            n_visit += q.visits;
             if (cont) {
                 query_begin(q, T, o, d, 1.0e6f, WIDE);
+                ++n_query;
                 phase = 1;
             } else {
                 ray = -1;
@@ -336,6 +340,15 @@ __global__ void __launch_bounds__(kTB) k_trace(MeshView m, Domain D, S sh, uint3
         }
     }
     if (err) atomicOr(work + 1, err);
+    // work[2..3]: queries started, work[4..5]: node + leaf visits (64-bit, warp-reduced)
+    for (int o = 16; o > 0; o >>= 1) {
+        n_query += __shfl_xor_sync(kFull, n_query, o);
+        n_visit += __shfl_xor_sync(kFull, n_visit, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(reinterpret_cast<unsigned long long*>(work + 2), n_query);
+        atomicAdd(reinterpret_cast<unsigned long long*>(work + 4), n_visit);
+    }
 }
 
 struct GridArgs {

@@ -228,8 +228,10 @@ class EtchEngine:
         self.mask_phi = geo['mask_phi_dev']
         self.mask_idx = torch.nonzero(self.mask.view(-1)).view(-1).to(torch.int32)
         self.active = torch.empty(self.ncell, dtype=torch.int32, **dev)
-        self.small = torch.zeros(16, dtype=torch.int32, **dev)   # work(2) stats(2) n_active(1)
-        self.host = torch.zeros(16, dtype=torch.int32).pin_memory()
+        # small[0:6] tracer work words (ray counter, error bits, u64 queries, u64 visits),
+        # small[6:8] rate stats, small[8] band size
+        self.small = torch.zeros(16, dtype=torch.int32, **dev)
+        self.host = torch.zeros(32, dtype=torch.int32).pin_memory()
         self.dom = domain_params(geo, par)
         self.ionp = ion_params(par)
         self.chem = chem_params(par, flags)
@@ -271,7 +273,7 @@ class EtchEngine:
         A_src = float(self.geo['Lx'] * self.geo['Ly'])
         n_smooth = int(par.get('flux_smooth', 1))
         alpha = float(par.get('flux_smooth_alpha', 1.0))
-        work = self.small[0:2]
+        work = self.small[0:6]
         faithful = (flags is not None and getattr(flags, "ion_reflection", False)
                     and getattr(flags, "chemistry", "langmuir") == "belen")
         bare_init = False
@@ -329,7 +331,7 @@ class EtchEngine:
         par, m = self.par, self.mesh
         s = _sp()
         A_src = float(self.geo['Lx'] * self.geo['Ly'])
-        work = self.small[0:2]
+        work = self.small[0:6]
         sF = float(par['s_F'])
         sO = float(par['s_O'])
         if getattr(self.flags, "chemistry", "langmuir") == "belen":
@@ -357,26 +359,28 @@ class EtchEngine:
         m = self.mesh
         s = _sp()
         y = self.yields
-        stats = self.small[2:4]
+        stats = self.small[6:8]
         _lib.call("petch_surface_rate", m.id, m.MT, m.MV, ctypes.byref(self.chem),
                   self.m_i.data_ptr(), self.m_F.data_ptr(), self.m_O.data_ptr(),
                   self.cos_i.data_ptr(), y[0], y[1], y[2], self.V.data_ptr(), stats.data_ptr(), s)
         nx, ny, nz = self.shape
         _lib.call("petch_extend_velocity", m.id, m.MT, m.MV, self.phi.data_ptr(),
                   self.mask.data_ptr(), nx, ny, nz, self.dx, float(band), self.V.data_ptr(),
-                  self.F.data_ptr(), 1, self.active.data_ptr(), self.small[4:5].data_ptr(),
-                  self.ncell, self.small[0:2].data_ptr(), s)
+                  self.F.data_ptr(), 1, self.active.data_ptr(), self.small[8:9].data_ptr(),
+                  self.ncell, self.small[0:6].data_ptr(), s)
 
     def sync_status(self):
         """The step's single device->host read: mesh counts/errors + rate stats + band size."""
         self.host[0:8].copy_(self.mesh.hdr[0:8], non_blocking=True)
-        self.host[8:13].copy_(self.small[0:5], non_blocking=True)
+        self.host[8:17].copy_(self.small[0:9], non_blocking=True)
         torch.cuda.current_stream().synchronize()
         h = self.host.numpy()
+        q = h[10:14].view(np.uint64)
         return dict(F=int(h[0]), V=int(h[1]), L=int(h[2]), mesh_err=int(h[3]),
-                    trace_err=int(h[9]), nonfinite=int(h[10]),
-                    vmax=float(np.array([h[11]], np.int32).view(np.float32)[0]),
-                    n_active=int(h[12]))
+                    trace_err=int(h[9]), queries=int(q[0]), visits=int(q[1]),
+                    nonfinite=int(h[14]),
+                    vmax=float(np.array([h[15]], np.int32).view(np.float32)[0]),
+                    n_active=int(h[16]))
 
     def advect(self, dt_sub, nsub, n_active):
         nx, ny, nz = self.shape

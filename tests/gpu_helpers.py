@@ -59,7 +59,7 @@ def domain(geo):
 
 def cuda_neutrals(m, geo, bare, beta, seed, n):
     flux = torch.zeros(m.MT, device="cuda")
-    work = torch.zeros(2, dtype=torch.int32, device="cuda")
+    work = torch.zeros(6, dtype=torch.int32, device="cuda")
     b = None if bare is None else torch.from_numpy(np.asarray(bare, np.float32)).cuda()
     _lib.call("petch_trace_neutrals", m.id, m.MT, m.MV, ctypes.byref(domain(geo)),
               None if b is None else b.data_ptr(), float(beta), int(seed), 0, int(n),
@@ -71,7 +71,7 @@ def cuda_neutrals(m, geo, bare, beta, seed, n):
 def cuda_ions(m, geo, par, seed, n):
     tal = torch.zeros((m.MT, 4), device="cuda")
     ang = torch.zeros(m.MT, device="cuda")
-    work = torch.zeros(2, dtype=torch.int32, device="cuda")
+    work = torch.zeros(6, dtype=torch.int32, device="cuda")
     _lib.call("petch_trace_ions", m.id, m.MT, m.MV, ctypes.byref(domain(geo)),
               ctypes.byref(t3.ion_params(par)), int(seed), int(n), tal.data_ptr(), ang.data_ptr(),
               work.data_ptr(), stream())
@@ -83,7 +83,7 @@ def cuda_ions(m, geo, par, seed, n):
 def cuda_legacy(m, geo, ion, sigma, sticking, n_reemit, specular, seed, n):
     fl = torch.zeros(m.MT, device="cuda")
     ang = torch.zeros(m.MT, device="cuda")
-    work = torch.zeros(2, dtype=torch.int32, device="cuda")
+    work = torch.zeros(6, dtype=torch.int32, device="cuda")
     _lib.call("petch_trace_legacy", m.id, m.MT, m.MV, ctypes.byref(domain(geo)), int(ion),
               float(sigma), float(sticking), int(n_reemit), int(specular), 0.34, 0.8, int(seed),
               int(n), fl.data_ptr(), ang.data_ptr(), work.data_ptr(), stream())

@@ -85,17 +85,19 @@ def test_raycast_matches_oracle(name, width):
     of, ot = o.raycast(org.astype(np.float64), d.astype(np.float64))
     face = torch.empty(n, dtype=torch.int32, device="cuda")
     t = torch.empty(n, device="cuda")
-    work = torch.zeros(2, dtype=torch.int32, device="cuda")
+    work = torch.zeros(6, dtype=torch.int32, device="cuda")
     org_d, d_d = torch.from_numpy(org).cuda(), torch.from_numpy(d).cuda()   # keep both alive
     _lib.call("petch_raycast", m.id, m.MT, m.MV, org_d.data_ptr(), d_d.data_ptr(), n, 1e6,
               face.data_ptr(), t.data_ptr(), work.data_ptr(), stream())
     cf, ct = face.cpu().numpy(), t.cpu().numpy()
     assert work[1].item() == 0
     same = cf == of
-    assert same.mean() > 0.999, same.mean()
-    # disagreements are exact ties at shared edges/vertices: same distance
+    # every disagreement is an exact tie: a shared edge / vertex, or coincident faces (the seed
+    # field's zero nodes along the mask / substrate interface form a zero-thickness gas sheet
+    # inside the solid, meshed as two coincident layers that only rays started in the solid reach)
+    assert same.mean() > (0.95 if name == "config0_seed" else 0.999), same.mean()
     diff = ~same
-    assert np.all((cf[diff] >= 0) == (of[diff] >= 0))
+    assert np.all((cf >= 0) == (of >= 0))
     np.testing.assert_allclose(ct[diff & (cf >= 0)], ot[diff & (cf >= 0)], rtol=1e-4, atol=1e-5)
     np.testing.assert_allclose(ct[same & (cf >= 0)], ot[same & (cf >= 0)], rtol=1e-4, atol=1e-5)
 
@@ -110,7 +112,7 @@ def test_nearest_face_matches_oracle(name):
     p = rng.uniform(0, np.array(phi.shape) * dx, (n, 3)).astype(np.float32)
     of = o.nearest(p.astype(np.float64))
     face = torch.empty(n, dtype=torch.int32, device="cuda")
-    work = torch.zeros(2, dtype=torch.int32, device="cuda")
+    work = torch.zeros(6, dtype=torch.int32, device="cuda")
     p_d = torch.from_numpy(p).cuda()
     _lib.call("petch_nearest_face", m.id, m.MT, m.MV, p_d.data_ptr(), n, 1e6, face.data_ptr(),
               work.data_ptr(), stream())
