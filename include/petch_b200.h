@@ -79,6 +79,19 @@ int petch_reinit_eik(const float* phi_in, float* phi_out, float* u_a, float* u_b
                      void* stream);
 
 
+/* petch_reinit_eik without caller scratch, for callers that cannot allocate device memory at
+ * all (a host framework that owns the whole device heap and forbids driver allocations, or a
+ * fixed-budget loop that cannot afford an allocation's latency and implicit synchronisation).
+ * No counterpart in the reference (its reinit_fsm allocates Warp arrays on every call).
+ * The two Eikonal scratch grids live in a fixed device array of the library (16 MiB held by
+ * every GPU that loads it, until exit), so the grid may have at most 2,097,152 cells; larger
+ * grids are rejected with PETCH_E_INVALID.  Allocates nothing.  The first call on a device looks
+ * up the array's device address (cudaGetSymbolAddress); make it before any stream capture.
+ * Calls share the array: calls whose kernels overlap on the GPU race.  Same arguments and
+ * results as petch_reinit_eik otherwise. */
+int petch_reinit_eik_noalloc(const float* phi_in, float* phi_out, int nx, int ny, int nz,
+                             double dx, float big, float cap, int n_iter, int mode, void* stream);
+
 /* ------------------------------------------------------------------------------------------ */
 /* Surface mesh + BVH (one caller-allocated device buffer, rebuilt each step)                  */
 /* ------------------------------------------------------------------------------------------ */

@@ -282,3 +282,91 @@ extern "C" int petch_reinit_eik(const float* phi_in, float* phi_out, float* u_a,
     PETCH_LAUNCH_CHECK("k_eik_sweep<final>");
     return PETCH_OK;
 }
+
+// ---------------------------------------------------------------------------------------------
+// Allocation-free reinit.  Some callers cannot allocate device memory at all: a host application
+// or plugin framework that owns the whole device heap and forbids driver allocations, or a
+// fixed-budget real-time loop where an allocation's latency and implicit device synchronisation
+// are not acceptable.  They still own their input and output grids, but cannot provide the two
+// Eikonal scratch grids petch_reinit_eik needs.  This variant keeps that scratch in a fixed
+// file-scope device array instead.
+//
+// The array is part of the library's device image: every GPU that loads the library holds it
+// (16 MiB) until the process exits.  Its host-side name is only a stand-in for the symbol, so
+// the device address is looked up with cudaGetSymbolAddress once per device, on the first call
+// made with that device current; make that first call before any stream capture.  All calls
+// share the one array, so calls whose kernels overlap on the GPU (different streams, threads or
+// processes sharing a context) race on it.  Nothing carries over between calls: the init kernel
+// writes every scratch cell before any sweep reads it.
+// ---------------------------------------------------------------------------------------------
+#include <mutex>
+
+namespace {
+
+constexpr long long kNoAllocMaxCells = 1LL << 21;   // 2,097,152 cells (e.g. 128^3): 8 MiB a grid
+
+__device__ __align__(256) float g_reinit_scratch[2 * kNoAllocMaxCells];
+
+float* g_scratch_addr[64] = {nullptr};
+std::mutex g_scratch_mu;
+
+int reinit_scratch_address(float** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return petch::cuda_fail(e, "petch_reinit_eik_noalloc: cudaGetDevice");
+    if (dev < 0 || dev >= 64) {
+        petch::set_error("petch_reinit_eik_noalloc: device ordinal %d out of range", dev);
+        return PETCH_E_INVALID;
+    }
+    std::lock_guard<std::mutex> lock(g_scratch_mu);
+    if (g_scratch_addr[dev] == nullptr) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_reinit_scratch);
+        if (e != cudaSuccess)
+            return petch::cuda_fail(e, "petch_reinit_eik_noalloc: cudaGetSymbolAddress");
+        g_scratch_addr[dev] = static_cast<float*>(p);
+    }
+    *out = g_scratch_addr[dev];
+    return PETCH_OK;
+}
+
+}  // namespace
+
+extern "C" int petch_reinit_eik_noalloc(const float* phi_in, float* phi_out, int nx, int ny, int nz,
+                                        double dx, float big, float cap, int n_iter, int mode,
+                                        void* stream) {
+    PETCH_REQUIRE(phi_in && phi_out, "petch_reinit_eik_noalloc: null pointer");
+    PETCH_REQUIRE(nx > 0 && ny > 0 && nz > 0 && dx > 0, "petch_reinit_eik_noalloc: bad grid");
+    PETCH_REQUIRE(n_iter >= 1, "petch_reinit_eik_noalloc: n_iter must be >= 1");
+    PETCH_REQUIRE(mode == 0 || mode == 1, "petch_reinit_eik_noalloc: mode must be 0 or 1");
+    const long long cells = (long long)nx * ny * nz;
+    PETCH_REQUIRE(cells <= kNoAllocMaxCells,
+                  "petch_reinit_eik_noalloc: grid of %lld cells exceeds the fixed scratch of %lld "
+                  "cells (use petch_reinit_eik with caller scratch)",
+                  cells, kNoAllocMaxCells);
+    float* base = nullptr;
+    int rc = reinit_scratch_address(&base);
+    if (rc) return rc;
+    float* a = base;
+    float* b = base + kNoAllocMaxCells;
+    Grid g = make_grid(nx, ny, nz);
+    cudaStream_t st = petch::as_stream(stream);
+    int blocks = petch::grid_for(g.n, kBlock);
+    const float dxf = (float)dx, inv_dx = (float)(1.0 / dx);
+    if (mode == 1) k_eik_init<true><<<blocks, kBlock, 0, st>>>(phi_in, a, g, inv_dx, big);
+    else k_eik_init<false><<<blocks, kBlock, 0, st>>>(phi_in, a, g, inv_dx, big);
+    PETCH_LAUNCH_CHECK("k_eik_init");
+    for (int it = 0; it < n_iter - 1; ++it) {
+        k_eik_sweep<false, false><<<blocks, kBlock, 0, st>>>(a, b, nullptr, nullptr, g, dxf, big, cap);
+        PETCH_LAUNCH_CHECK("k_eik_sweep");
+        float* t = a;
+        a = b;
+        b = t;
+    }
+    if (mode == 1)
+        k_eik_sweep<true, true><<<blocks, kBlock, 0, st>>>(a, nullptr, phi_in, phi_out, g, dxf, big, cap);
+    else
+        k_eik_sweep<true, false><<<blocks, kBlock, 0, st>>>(a, nullptr, phi_in, phi_out, g, dxf, big, cap);
+    PETCH_LAUNCH_CHECK("k_eik_sweep<final>");
+    return PETCH_OK;
+}

@@ -53,6 +53,7 @@ SIGNATURES = {
     "petch_seed_level_set": [P, P, I, I, I, D, D, D, D, D, D, I, P],
     "petch_advect": [P, P, P, P, P, I, I, I, F, F, I, P],
     "petch_reinit_eik": [P, P, P, P, I, I, I, D, F, F, I, I, P],
+    "petch_reinit_eik_noalloc": [P, P, I, I, I, D, F, F, I, I, P],
     "petch_mesh_layout": [I, I, LLP, I, LLP],
     "petch_mesh_scratch_bytes": [I, I, I, I, LLP],
     "petch_mesh_build": [P, I, I, I, D, D, D, D, D, D, I, P, I, I, P, L, P],
