@@ -141,16 +141,18 @@ typedef struct petch_ion_params {  /* the float32 arguments of _trace3d_ion_yiel
 } petch_ion_params;
 
 /* Tracer configuration for this process (the autotuner's knobs): bvh_width 2 (binary LBVH,
- * default) or 8 (quantised 8-wide BVH); steps_per_round = traversal steps each warp runs for all
- * its lanes between shading / refill rounds (default 8).  Applies to later trace / raycast
- * calls. */
-int petch_tracer_config(int bvh_width, int steps_per_round);
+ * default) or 8 (quantised 8-wide BVH); each warp runs traversal steps for all its lanes with an
+ * open query, at most steps_per_round (default 64) and only while more than keep_lanes lanes
+ * (0..31, default 12) still have one, between shading / refill rounds; once the ray pool is empty
+ * a warp steps until its last query ends.  Applies to later trace / raycast calls. */
+int petch_tracer_config(int bvh_width, int steps_per_round, int keep_lanes);
 
 /* Replaces _gen_source + _trace3d_ion_yield (petch/threed.py:441-458, 599-712): n_ion ions
  * generated and traced on the device.  tally4 (16-byte aligned float4[max_tris]) receives per
  * face (sputter, ion-enhanced, passivation, arrival) and ang the cos-weighted arrival; both are
  * zeroed first.  work: int[6] device words, 8-byte aligned: [0] ray counter (reset by every trace
- * call), [1] error bits OR-ed by every kernel (1 = traversal bound hit, 2 = active list full)
+ * call), [1] error bits OR-ed by every kernel (1 = traversal bound hit, 2 = active list full,
+ * 4 = tracer round bound hit)
  * until the caller clears them, [2..3] uint64 BVH queries and [4..5] uint64 node + leaf visits,
  * accumulated by every trace call until the caller clears them. */
 int petch_trace_ions(const void* mesh, int max_tris, int max_verts, const petch_domain* dom,

@@ -14,12 +14,17 @@ namespace petch {
 namespace {
 
 constexpr int kTB = 128;
+constexpr int kTraceMinBlocks = 8;   // 8 blocks x 4 warps per SM: <= 64 registers per thread
+constexpr long long kMaxRounds = 1LL << 24;   // per-warp bound on tracer rounds (error bit 4)
 constexpr unsigned kFull = 0xffffffffu;
 
-// Tracer configuration (process-wide host state, set by petch_tracer_config): BVH width and
-// traversal steps per warp round.
+// Tracer configuration (process-wide host state, set by petch_tracer_config): BVH width,
+// traversal steps per warp round, and how many lanes may still be traversing when a warp stops
+// stepping to shade and refill (only while the ray pool has rays).  The defaults were the fastest
+// of a sweep over neutral fluxes on the 8x4x40 trench (bare coverage 0.25 and 0.06).
 int g_bvh_width = 2;
-int g_steps = 8;
+int g_steps = 64;
+int g_keep = 12;
 
 struct Domain {
     float lx, ly, lz, z_src;
@@ -113,6 +118,12 @@ __global__ void k_zero_faces(const int* hdr, int MT, float* a, int na, float* b,
         for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < F * nb; i += gridDim.x * blockDim.x) b[i] = 0.0f;
 }
 
+// The face's unit winding normal as stored by the mesh build (float32, bit-identical to
+// normalize(cross(b - a, c - a)) on the float32 vertices, the normal Warp's query returns).
+__device__ __forceinline__ float3 stored_normal(const MeshView& m, int f) {
+    return make_float3(__ldg(m.normal + 3 * f), __ldg(m.normal + 3 * f + 1), __ldg(m.normal + 3 * f + 2));
+}
+
 // Per-ray state carried between queries.
 struct RayState {
     float w, E;
@@ -134,7 +145,7 @@ struct NeutralShader {
     }
     __device__ __forceinline__ bool hit(Rng& g, const Tracer& T, int f, float t, float3& o,
                                         float3& d, RayState& s) const {
-        float3 nrm = face_normal(T.m, f);
+        float3 nrm = stored_normal(T.m, f);
         if (dot3(nrm, d) > 0.0f) nrm = -nrm;
         atomicAdd(flux + f, s.w);
         float S = (bare ? __ldg(bare + f) : 1.0f) * beta;
@@ -170,7 +181,7 @@ struct IonShader {
     __device__ __forceinline__ bool hit(Rng& g, const Tracer& T, int f, float t, float3& o,
                                         float3& d, RayState& s) const {
         const float PI_2 = 1.5707963f;
-        float3 nrm = face_normal(T.m, f);
+        float3 nrm = stored_normal(T.m, f);
         if (dot3(nrm, d) > 0.0f) nrm = -nrm;
         float cosT = fminf(fmaxf(-dot3(d, nrm), 0.0f), 1.0f);
         float incAng = acosf(cosT);
@@ -250,7 +261,7 @@ struct LegacyShader {
     }
     __device__ __forceinline__ bool hit(Rng& g, const Tracer& T, int f, float t, float3& o,
                                         float3& d, RayState& s) const {
-        float3 nrm = face_normal(T.m, f);
+        float3 nrm = stored_normal(T.m, f);
         if (dot3(nrm, d) > 0.0f) nrm = -nrm;
         float cosang = fmaxf(-dot3(d, nrm), 0.0f);
         float3 h = o + t * d;
@@ -280,13 +291,14 @@ struct LegacyShader {
 };
 
 // Persistent tracer.  Each warp loops: refill lanes whose ray ended (one atomic per warp), run
-// up to `steps` traversal steps on every lane with an open query, then resolve the lanes whose
-// query finished -- a miss wraps laterally (periodic domains, <= 256 wraps per bounce, then one
+// traversal steps on every lane with an open query (up to `steps`, and only while more than
+// `keep` lanes still have one), then resolve the lanes whose query finished -- a miss wraps laterally (periodic domains, <= 256 wraps per bounce, then one
 // final query) or ends the ray; a hit goes to the shader, which deposits and either re-emits
 // (new query) or ends the ray.
 template <class S, bool WIDE>
-__global__ void __launch_bounds__(kTB) k_trace(MeshView m, Domain D, S sh, uint32_t seed,
-                                               uint32_t domain, int n, int steps, int* work) {
+__global__ void __launch_bounds__(kTB, kTraceMinBlocks) k_trace(MeshView m, Domain D, S sh, uint32_t seed,
+                                               uint32_t domain, int n, int steps, int keep,
+                                               int* work) {
     extern __shared__ float4 s_wn[];
     const Tracer T = make_tracer(m, s_wn, WIDE);
     int st_ref[kWStack];
@@ -297,7 +309,12 @@ __global__ void __launch_bounds__(kTB) k_trace(MeshView m, Domain D, S sh, uint3
     Query q;
     RayState rs;
     Rng g;
-    while (true) {
+    bool pool_empty = false;   // warp-uniform: once set, no lane can be refilled any more
+    for (long long round = 0;; ++round) {
+        if (round >= kMaxRounds) {   // last-resort bound (never reached by a valid mesh)
+            err |= 4;
+            break;
+        }
         if (refill(ray, n, work)) {
             g.init(seed, domain, (uint32_t)ray);
             float3 o, d;
@@ -306,11 +323,17 @@ __global__ void __launch_bounds__(kTB) k_trace(MeshView m, Domain D, S sh, uint3
             rs.wraps = 0;
             query_begin(q, T, o, d, 1.0e6f, WIDE);
             ++n_query;
-            phase = 1;
+            phase = q.cur == kDone ? 2 : 1;   // an empty mesh: the query is over at once
         }
         if (__all_sync(kFull, ray == -2)) break;
+        // Traverse while more than `keep` lanes still have an open query (at most `steps` steps),
+        // so lanes that finished early idle only while most of the warp is still busy.  Once the
+        // ray pool is empty no lane can be refilled, so the warp then steps until every query is
+        // done (keep 0): each round makes progress.
+        pool_empty = pool_empty || __any_sync(kFull, ray == -2);
+        const int keep_now = pool_empty ? 0 : keep;
         for (int s = 0; s < steps; ++s) {
-            if (!__any_sync(kFull, phase == 1)) break;
+            if (__popc(__ballot_sync(kFull, phase == 1)) <= keep_now) break;
             if (phase == 1) {
                 bool fin = WIDE ? step_wide(T, q, st_ref, st_t, &err)
                                 : step_binary(T, q, st_ref, st_t, &err);
@@ -332,7 +355,7 @@ __global__ void __launch_bounds__(kTB) k_trace(MeshView m, Domain D, S sh, uint3
             if (cont) {
                 query_begin(q, T, o, d, 1.0e6f, WIDE);
                 ++n_query;
-                phase = 1;
+                phase = q.cur == kDone ? 2 : 1;
             } else {
                 ray = -1;
                 phase = 0;
@@ -473,24 +496,27 @@ static Domain to_domain(const petch_domain* d) {
 template <class S>
 static int launch_trace(const MeshView& m, const Domain& D, const S& sh, uint32_t seed,
                         uint32_t domain, int n, int* work, cudaStream_t st, const char* what) {
-    const int steps = g_steps;
+    const int steps = g_steps, keep = g_keep;
     if (g_bvh_width == 2) {
         k_trace<S, false><<<persistent_blocks((const void*)k_trace<S, false>, kTB), kTB, kSmemBytes, st>>>(
-            m, D, sh, seed, domain, n, steps, work);
+            m, D, sh, seed, domain, n, steps, keep, work);
     } else {
         k_trace<S, true><<<persistent_blocks((const void*)k_trace<S, true>, kTB), kTB, kSmemBytes, st>>>(
-            m, D, sh, seed, domain, n, steps, work);
+            m, D, sh, seed, domain, n, steps, keep, work);
     }
     PETCH_LAUNCH_CHECK(what);
     return PETCH_OK;
 }
 
-extern "C" int petch_tracer_config(int bvh_width, int steps_per_round) {
+extern "C" int petch_tracer_config(int bvh_width, int steps_per_round, int keep_lanes) {
     PETCH_REQUIRE(bvh_width == 2 || bvh_width == 8, "petch_tracer_config: bvh_width must be 2 or 8");
     PETCH_REQUIRE(steps_per_round >= 1 && steps_per_round <= 4096,
                   "petch_tracer_config: steps_per_round must be in [1, 4096]");
+    PETCH_REQUIRE(keep_lanes >= 0 && keep_lanes <= 31,
+                  "petch_tracer_config: keep_lanes must be in [0, 31]");
     g_bvh_width = bvh_width;
     g_steps = steps_per_round;
+    g_keep = keep_lanes;
     return PETCH_OK;
 }
 

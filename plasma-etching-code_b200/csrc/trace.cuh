@@ -309,6 +309,7 @@ __device__ __forceinline__ void query_leaf(const Tracer& T, Query& q, int f0, in
 // One step of the 8-wide traversal; returns true once the query has finished.
 __device__ __forceinline__ bool step_wide(const Tracer& T, Query& q, int* st_ref, float* st_t,
                                           int* err) {
+    if (q.cur == kDone) return true;
     if (++q.visits > kMaxVisits) {
         *err |= 1;
         q.cur = kDone;
@@ -392,6 +393,7 @@ __device__ __forceinline__ bool step_wide(const Tracer& T, Query& q, int* st_ref
 // One step of the binary traversal; returns true once the query has finished.
 __device__ __forceinline__ bool step_binary(const Tracer& T, Query& q, int* st_ref, float* st_t,
                                             int* err) {
+    if (q.cur == kDone) return true;
     if (++q.visits > kMaxVisits) {
         *err |= 1;
         q.cur = kDone;

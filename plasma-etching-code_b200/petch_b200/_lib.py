@@ -69,9 +69,13 @@ SIGNATURES = {
     "petch_surface_rate": [P, I, I, CP, P, P, P, P, P, P, P, P, P, P],
     "petch_advect_sparse": [P, P, P, P, P, I, P, I, I, I, I, F, F, I, P],
     "petch_raycast": [P, I, I, P, P, I, F, P, P, P, P],
-    "petch_tracer_config": [I, I],
+    "petch_tracer_config": [I, I, I],
     "petch_nearest_face": [P, I, I, P, I, F, P, P, P],
 }
+
+# The library's tracer configuration at load (bvh_width, steps_per_round, keep_lanes): what
+# petch_tracer_config restores to.
+TRACER_DEFAULT = (2, 64, 12)
 
 _lib = None
 

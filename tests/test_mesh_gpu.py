@@ -65,9 +65,9 @@ def test_sphere_is_closed_and_outward():
 
 @pytest.fixture(params=[8, 2])
 def width(request):
-    _lib.call("petch_tracer_config", request.param, 16)
+    _lib.call("petch_tracer_config", request.param, 16, 4)
     yield request.param
-    _lib.call("petch_tracer_config", 2, 8)
+    _lib.call("petch_tracer_config", *_lib.TRACER_DEFAULT)
 
 
 @pytest.mark.parametrize("name", ["sphere", "pit_hole", "config0_seed"])
