@@ -260,6 +260,44 @@ int petch_advect_sparse(float* phi, float* tmp, const float* F, const float* mas
                         const int* mask_idx, int n_mask, const int* active, int n_active, int nx,
                         int ny, int nz, float inv_dx, float dt_sub, int nsub, void* stream);
 
+/* ---- deterministic radiosity neutrals (mc_flux_3d_radiosity, petch/threed.py:923-991) ---- */
+
+/* Replaces _gas_normals (petch/threed.py:1553-1568): fn (float[3 * max_tris]) = the face's unit
+ * winding normal, flipped to agree with -grad(phi) at the grid node nearest its centroid
+ * (np.gradient differences: central inside, one-sided at the grid faces). */
+int petch_gas_normals(const void* mesh, int max_tris, int max_verts, const float* phi, int nx,
+                      int ny, int nz, double dx, float* fn, void* stream);
+
+/* Replaces the form-factor cast of mc_flux_3d_radiosity (petch/threed.py:947-956: origins
+ * centroid + 1e-3 fn, _cosine_dirs :1571-1579, _trace_ff :908-920 with _apply_bc's periodic
+ * wrap): n_ff cosine-distributed rays per face, hitface[j * n_ff + k] = first face hit by ray k
+ * of face j, or -1 if it escapes (entries past F * n_ff are -1).  hitface: int[max_tris * n_ff].
+ * Philox stream keyed by (seed, ray).  work: as petch_trace_ions. */
+int petch_trace_ff(const void* mesh, int max_tris, int max_verts, const petch_domain* dom,
+                   const float* fn, uint32_t seed, int n_ff, int* hitface, int* work,
+                   void* stream);
+
+/* Scratch bytes petch_ff_matrix needs for a mesh of max_tris faces and n_ff rays per face. */
+int petch_ff_scratch_bytes(int max_tris, int n_ff, long long* bytes);
+
+/* Replaces the matrix assembly of mc_flux_3d_radiosity (petch/threed.py:957-960): from
+ * petch_trace_ff's hits, sky[i] = escaping rays of face i / n_ff (double[max_tris]) and the CSR
+ * of A[i, j] = F_{j->i}: row_ptr (int[max_tris + 1]) and col (int[max_tris * n_ff]) with one
+ * entry of weight 1 / n_ff per ray (repeated j for repeated hits), entries of a row in ascending
+ * ray order.  No host synchronisation; the result is identical on every run. */
+int petch_ff_matrix(const void* mesh, int max_tris, int max_verts, const int* hitface, int n_ff,
+                    int* row_ptr, int* col, double* sky, void* scratch, long long scratch_bytes,
+                    void* stream);
+
+/* Replaces solve() of mc_flux_3d_radiosity with the Jacobi solver (petch/threed.py:966-985):
+ * for beta in (betaE, betaO): G = sky, then n_iter times G = sky + M G with
+ * M[i, j] = A[i, j] (1 - clip(bare_j beta, 0, 1)), in float64; g_E / g_O = clip(G, 0, 8) as float.
+ * work2: double[4 * max_tris] scratch. */
+int petch_radiosity_solve(const void* mesh, int max_tris, int max_verts, const int* row_ptr,
+                          const int* col, const double* sky, int n_ff, const float* bare,
+                          double betaE, double betaO, int n_iter, float* g_E, float* g_O,
+                          double* work2, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -49,6 +49,7 @@ _SIGS = {
     "orc_trace_ions": ([_P, _P, _P, _U64, _I, _P], None),
     "orc_trace_neutrals": ([_P, _P, _P, _D, _U64, _U64, _I, _P], None),
     "orc_trace_legacy": ([_P, _P, _I, _D, _D, _I, _I, _D, _D, _U64, _I, _P, _P], None),
+    "orc_trace_ff": ([_P, _P, _P, _P, _I, _I, _U64, _P], None),
 }
 
 
@@ -443,6 +444,108 @@ def flux_coupled(mesh, geo, par, flags, n_ion, n_neu, seed, bare_init=None, tt=N
     return m_i, m_F, m_O, cos_i, bare, iy
 
 
+# ------------------------------- radiosity neutrals -------------------------------
+def gas_normals(verts, faces, centroids, phi, dx):
+    """_gas_normals (threed.py:1553-1568): float32 winding normals of the float32 vertices,
+    flipped to agree with -np.gradient(phi) at the rounded, clipped centroid node."""
+    vv = np.asarray(verts, np.float32)[np.asarray(faces)]
+    fn = np.cross(vv[:, 1] - vv[:, 0], vv[:, 2] - vv[:, 0])
+    fn = fn / (np.linalg.norm(fn, axis=1, keepdims=True) + np.float32(1e-12))
+    gx, gy, gz = np.gradient(np.asarray(phi, np.float64), dx)
+    c = np.asarray(centroids, np.float64)
+    ix = np.clip((c[:, 0] / dx).round().astype(int), 0, gx.shape[0] - 1)
+    iy = np.clip((c[:, 1] / dx).round().astype(int), 0, gx.shape[1] - 1)
+    iz = np.clip((c[:, 2] / dx).round().astype(int), 0, gx.shape[2] - 1)
+    into_gas = -np.stack([gx[ix, iy, iz], gy[ix, iy, iz], gz[ix, iy, iz]], axis=1)
+    flip = np.sum(fn * into_gas, axis=1) < 0.0
+    fn[flip] *= -1.0
+    return fn
+
+
+def trace_ff(mesh, geo, par, fn, centroids, n_ff, seed):
+    """The form-factor cast (threed.py:947-956 + _trace_ff :908-920): int[F * n_ff] first-hit
+    faces, -1 for escapes; ray k of face j at index j * n_ff + k."""
+    F = len(fn)
+    hit = np.empty(F * n_ff, np.int32)
+    if F:
+        lib().orc_trace_ff(mesh.h, _p(_dom(geo, par)), _p(_f64(fn)), _p(_f64(centroids)), F,
+                           int(n_ff), int(seed) & (2**64 - 1), _p(hit))
+    return hit
+
+
+def ff_matrix(hit, F, n_ff):
+    """D (sky view) and the CSR A[i, j] = F_{j->i} of mc_flux_3d_radiosity (threed.py:957-960)."""
+    import scipy.sparse as sp
+    hit = np.asarray(hit)
+    src = np.repeat(np.arange(F), n_ff)
+    esc = hit < 0
+    D = np.bincount(src[esc], minlength=F).astype(np.float64) / n_ff
+    j = src[~esc]
+    i = hit[~esc]
+    Aff = sp.coo_matrix((np.full(len(i), 1.0 / n_ff), (i, j)), shape=(F, F)).tocsr()
+    return D, Aff
+
+
+def radiosity_solve(Aff, D, bare, beta, n_iter=40):
+    """solve() of mc_flux_3d_radiosity with the Jacobi solver (threed.py:966-985)."""
+    s = np.clip(bare * beta, 0.0, 1.0)
+    M = Aff.multiply((1.0 - s)[None, :]).tocsr()
+    G = D.copy()
+    for _ in range(n_iter):
+        G = D + M.dot(G)
+    return np.clip(G, 0.0, 8.0)
+
+
+def radiosity_ions(mesh, geo, par, flags, n_ion, seed):
+    """_ions_deterministic (threed.py:994-1029): (m_i, cos_i, ion_yield-or-None), unsmoothed."""
+    A_src = geo['Lx'] * geo['Ly']
+    A = np.maximum(mesh.area, 1e-9)
+    faithful = getattr(flags, "ion_reflection", False) and getattr(flags, "chemistry", "langmuir") == "belen"
+    if faithful:
+        tal = trace_ions(mesh, geo, par, seed * 9 + 1, n_ion)
+        norm = A_src / n_ion
+        iy = tuple((tal[:, q] / A) * norm for q in range(3))
+        fi, ai = tal[:, 3], tal[:, 4]
+        m_i = (fi / A) * norm
+    else:
+        fi, ai = trace_legacy(mesh, geo, par, 1, par['ion_ang_sigma'], 1.0, 0, 0, 0.34, 0.8,
+                              seed * 9 + 1, n_ion)
+        iy = None
+        m_i = np.clip((fi / A) / (n_ion / A_src), 0.0, 1.5)
+    cos_i = np.where(fi > 0, ai / np.maximum(fi, 1e-9), 0.0)
+    return m_i, cos_i, iy
+
+
+def radiosity_fixed_point(D, Aff, m_i, cos_i, iy, par, flags, n_fp=4, n_iter=40):
+    """The coverage <-> radiosity fixed point of mc_flux_3d_radiosity (threed.py:986-990)."""
+    F = len(D)
+    bare = np.ones(F)
+    betaE, betaO = par.get('betaE', 0.7), par.get('betaO', 1.0)
+    ya = getattr(flags, "yield_angular", "cosine")
+    m_F = m_O = np.zeros(F)
+    for _ in range(n_fp):
+        m_F = radiosity_solve(Aff, D, bare, betaE, n_iter)
+        m_O = radiosity_solve(Aff, D, bare, betaO, n_iter)
+        thF, thO = belen_coverages(m_i, m_F, m_O, cos_i, par, ya, iy)
+        bare = np.clip(1.0 - thF - thO, 0.0, 1.0)
+    return m_F, m_O
+
+
+def flux_radiosity(mesh, geo, phi, par, flags, n_ion, seed, n_ff=64, tt=None):
+    """mc_flux_3d_radiosity (threed.py:923-991) on the oracle mesh: (m_i, m_F, m_O, cos_i,
+    ion_yield-or-None)."""
+    tt = {} if tt is None else tt
+    tt.setdefault('trace', 0.0)
+    t0 = time.time()
+    m_i, cos_i, iy = radiosity_ions(mesh, geo, par, flags, n_ion, seed)
+    fn = gas_normals(mesh.verts, mesh.faces, mesh.centroid, phi, geo['dx'])
+    hit = trace_ff(mesh, geo, par, fn, mesh.centroid, n_ff, seed)
+    tt['trace'] += time.time() - t0
+    D, Aff = ff_matrix(hit, mesh.F, n_ff)
+    m_F, m_O = radiosity_fixed_point(D, Aff, m_i, cos_i, iy, par, flags)
+    return m_i, m_F, m_O, cos_i, iy
+
+
 # ------------------------------- the loop -------------------------------
 def depth3d(geo, phi, half=1.0):
     """_depth3d (threed.py:1798-1834)."""
@@ -473,8 +576,8 @@ def depth3d(geo, phi, half=1.0):
 def run_etch_3d(Lx, Ly, Lz, dx, trench_width, mask_th, sub_top, t_end, n_steps, hole, par, flags,
                 n_ion, n_neu, seed_offset=0, record_depth_every=0, max_seconds=None, steps=None,
                 stage_times=None):
-    """run_etch_3d (threed.py:1643-1795) with the oracle's stages (coverage-coupled MC path, FSM
-    reinit, nearest-face extension).  Runs `steps` (default n_steps) steps of the n_steps
+    """run_etch_3d (threed.py:1643-1795) with the oracle's stages (coverage-coupled MC path or
+    radiosity neutrals, FSM reinit, nearest-face extension).  Runs `steps` (default n_steps) steps of the n_steps
     schedule.  Returns (phi, depth_history, stats); stage_times (list) receives one dict of stage
     seconds per step."""
     nx, ny, nz = int(round(Lx / dx)), int(round(Ly / dx)), int(round(Lz / dx))
@@ -497,14 +600,18 @@ def run_etch_3d(Lx, Ly, Lz, dx, trench_width, mask_th, sub_top, t_end, n_steps, 
         mesh = mesh_build(phi, dx, geo)
         st['mesh'] = time.time() - ta
         ta = time.time()
-        bi = None
-        if warm and prev is not None:
-            pm, pb = prev
-            q = pm.nearest(mesh.centroid.astype(np.float32).astype(np.float64))
-            bi = np.where(q >= 0, pb[np.maximum(q, 0)], 1.0)
-        m_i, m_F, m_O, cos_i, bare, iy = flux_coupled(mesh, geo, par, flags, n_ion, n_neu,
-                                                      step + seed_offset, bi, tt=st)
-        prev = (mesh, bare)
+        if getattr(flags, "neutral_transport", "mc") == "radiosity":
+            m_i, m_F, m_O, cos_i, iy = flux_radiosity(mesh, geo, phi, par, flags, n_ion,
+                                                      step + seed_offset, tt=st)
+        else:
+            bi = None
+            if warm and prev is not None:
+                pm, pb = prev
+                q = pm.nearest(mesh.centroid.astype(np.float32).astype(np.float64))
+                bi = np.where(q >= 0, pb[np.maximum(q, 0)], 1.0)
+            m_i, m_F, m_O, cos_i, bare, iy = flux_coupled(mesh, geo, par, flags, n_ion, n_neu,
+                                                          step + seed_offset, bi, tt=st)
+            prev = (mesh, bare)
         V = surface_rate(m_i, m_F, m_O, cos_i, mesh.fmask, par,
                          getattr(flags, "chemistry", "langmuir"),
                          getattr(flags, "yield_angular", "cosine"), iy)

@@ -4,6 +4,7 @@
 //   Russian-roulette neut.: _trace3d_cov_rr        petch/threed.py:549-596
 //   faithful ion          : _trace3d_ion_yield     petch/threed.py:599-712
 //   legacy species        : _trace3d               petch/threed.py:352-406
+//   form-factor rays      : _trace_ff + emission   petch/threed.py:908-920, 947-956, 1571-1579
 // The random stream is this file's own (SplitMix64 counter hash per (seed, domain, ray)), not the
 // device's Philox and not Warp's: these are oracles of the same estimator, checked statistically.
 // Parity pin: tests/golden/flux.npz holds per-face means of the reference's own kernels (executed
@@ -325,6 +326,26 @@ void orc_trace_legacy(void* mesh, const double* dom, int ion, double sigma, doub
                 for (int q = 0; q < 3; ++q) o[q] = hit[q] + 1e-4 * nr[q];
             }
         }
+    }
+}
+
+// mc_flux_3d_radiosity's form-factor cast: ray k of face j leaves centroid_j + 1e-3 * fn_j in a
+// cosine direction about fn_j (the _cosine_dirs tangent frame), wraps laterally like _apply_bc,
+// and hit[j * n_ff + k] = its first hit face or -1.  fn, centroid: double[3 * F].
+void orc_trace_ff(void* mesh, const double* dom, const double* fn, const double* centroid, int F,
+                  int n_ff, uint64_t seed, int* hit) {
+    const Mesh* m = (const Mesh*)mesh;
+    Dom D{dom[0], dom[1], dom[2], dom[3], (int)dom[4]};
+    const long long n = (long long)F * n_ff;
+#pragma omp parallel for schedule(dynamic, 256)
+    for (long long p = 0; p < n; ++p) {
+        const int j = (int)(p / n_ff);
+        Rng g(seed, 0x66666600ULL, (uint64_t)p);
+        double o[3], d[3];
+        for (int q = 0; q < 3; ++q) o[q] = centroid[3 * j + q] + 1e-3 * fn[3 * j + q];
+        cosine_emit(g, fn + 3 * j, d);
+        orc::HitD h = query(m, o, d, D);
+        hit[p] = h.f;
     }
 }
 

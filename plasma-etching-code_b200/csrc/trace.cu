@@ -127,7 +127,7 @@ __device__ __forceinline__ float3 stored_normal(const MeshView& m, int f) {
 // Per-ray state carried between queries.
 struct RayState {
     float w, E;
-    int bounce, wraps;
+    int bounce, wraps, id;
 };
 
 // _trace3d_cov_rr (threed.py:549-596): deposit the weight on every hit, W *= 1 - bare * beta,
@@ -138,8 +138,9 @@ struct NeutralShader {
     float beta;
     float* flux;
     static constexpr int kMaxBounce = 1024;
-    __device__ __forceinline__ void init(Rng& g, const Domain& D, float3& o, float3& d,
-                                         RayState& s) const {
+    __device__ __forceinline__ int count(const MeshView&, int n) const { return n; }
+    __device__ __forceinline__ void init(Rng& g, const Tracer&, const Domain& D, int, float3& o,
+                                         float3& d, RayState& s) const {
         source(g, false, 0.0f, D, o, d);
         s.w = 1.0f;
     }
@@ -172,8 +173,9 @@ struct IonShader {
     float4* tal4;
     float* ang;
     static constexpr int kMaxBounce = 1024;
-    __device__ __forceinline__ void init(Rng& g, const Domain& D, float3& o, float3& d,
-                                         RayState& s) const {
+    __device__ __forceinline__ int count(const MeshView&, int n) const { return n; }
+    __device__ __forceinline__ void init(Rng& g, const Tracer&, const Domain& D, int, float3& o,
+                                         float3& d, RayState& s) const {
         source(g, true, P.sigma, D, o, d);
         s.E = fmaxf(P.meanE + P.sigmaE * g.normal(), 0.0f);
         s.w = 1.0f;
@@ -254,8 +256,9 @@ struct LegacyShader {
     float* flux;
     float* angacc;
     static constexpr int kMaxBounce = 1 << 30;
-    __device__ __forceinline__ void init(Rng& g, const Domain& D, float3& o, float3& d,
-                                         RayState& s) const {
+    __device__ __forceinline__ int count(const MeshView&, int n) const { return n; }
+    __device__ __forceinline__ void init(Rng& g, const Tracer&, const Domain& D, int, float3& o,
+                                         float3& d, RayState& s) const {
         source(g, ion != 0, sigma, D, o, d);
         s.w = 1.0f;
     }
@@ -290,6 +293,36 @@ struct LegacyShader {
     }
 };
 
+// _trace_ff + the emission of mc_flux_3d_radiosity (threed.py:908-920, 947-956): ray p leaves
+// face j = p / n_ff from centroid + 1e-3 * n_gas in a cosine direction about the into-gas normal
+// (the tangent frame of _cosine_dirs, threed.py:1571-1579); its first hit face is recorded (the
+// entries stay -1 for rays that escape to the open top).  Only F * n_ff rays exist.
+struct FormFactorShader {
+    const float* fn;     // into-gas unit normals, float[3 * MT]
+    int n_ff;
+    int* hitface;
+    static constexpr int kMaxBounce = 1;
+    __device__ __forceinline__ int count(const MeshView& m, int n) const {
+        const long long F = min(m.hdr[HDR_F], m.MT);
+        return (int)min((long long)n, F * n_ff);
+    }
+    __device__ __forceinline__ void init(Rng& g, const Tracer& T, const Domain&, int ray,
+                                         float3& o, float3& d, RayState& s) const {
+        const int j = ray / n_ff;
+        const float3 n = make_float3(__ldg(fn + 3 * j), __ldg(fn + 3 * j + 1), __ldg(fn + 3 * j + 2));
+        const float3 c = make_float3(__ldg(T.m.centroid + 3 * j), __ldg(T.m.centroid + 3 * j + 1),
+                                     __ldg(T.m.centroid + 3 * j + 2));
+        o = c + 1.0e-3f * n;
+        d = cosine_emit(g, n);
+        s.w = 1.0f;
+    }
+    __device__ __forceinline__ bool hit(Rng&, const Tracer&, int f, float, float3&, float3&,
+                                        RayState& s) const {
+        hitface[s.id] = f;
+        return false;
+    }
+};
+
 // Persistent tracer.  Each warp loops: refill lanes whose ray ended (one atomic per warp), run
 // traversal steps on every lane with an open query (up to `steps`, and only while more than
 // `keep` lanes still have one), then resolve the lanes whose query finished -- a miss wraps laterally (periodic domains, <= 256 wraps per bounce, then one
@@ -301,6 +334,7 @@ __global__ void __launch_bounds__(kTB, kTraceMinBlocks) k_trace(MeshView m, Doma
                                                int* work) {
     extern __shared__ float4 s_wn[];
     const Tracer T = make_tracer(m, s_wn, WIDE);
+    n = sh.count(m, n);
     int st_ref[kWStack];
     float st_t[kWStack];
     int err = 0;
@@ -318,7 +352,8 @@ __global__ void __launch_bounds__(kTB, kTraceMinBlocks) k_trace(MeshView m, Doma
         if (refill(ray, n, work)) {
             g.init(seed, domain, (uint32_t)ray);
             float3 o, d;
-            sh.init(g, D, o, d, rs);
+            rs.id = ray;
+            sh.init(g, T, D, ray, o, d, rs);
             rs.bounce = 0;
             rs.wraps = 0;
             query_begin(q, T, o, d, 1.0e6f, WIDE);
@@ -556,6 +591,23 @@ extern "C" int petch_trace_neutrals(const void* mesh, int max_tris, int max_vert
     if (n_neu == 0) return PETCH_OK;
     return launch_trace(m, to_domain(dom), sh, seed, 0x6e657500u ^ stream_id, n_neu, work, st,
                         "k_trace<neutrals>");
+}
+
+extern "C" int petch_trace_ff(const void* mesh, int max_tris, int max_verts,
+                              const petch_domain* dom, const float* fn, uint32_t seed, int n_ff,
+                              int* hitface, int* work, void* stream) {
+    PETCH_REQUIRE(mesh && dom && fn && hitface && work, "petch_trace_ff: null pointer");
+    PETCH_REQUIRE(max_tris > 0 && max_verts > 0 && n_ff >= 1 &&
+                      (long long)max_tris * n_ff < (1LL << 31),
+                  "petch_trace_ff: max_tris * n_ff must be in [1, 2^31)");
+    cudaStream_t st = as_stream(stream);
+    MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
+    FormFactorShader sh{fn, n_ff, hitface};
+    PETCH_CUDA(cudaMemsetAsync(hitface, 0xff, sizeof(int) * (size_t)max_tris * n_ff, st),
+               "hitface = -1");
+    PETCH_CUDA(cudaMemsetAsync(work, 0, sizeof(int), st), "reset ray counter");
+    return launch_trace(m, to_domain(dom), sh, seed, 0x66666600u, max_tris * n_ff, work, st,
+                        "k_trace<form factors>");
 }
 
 extern "C" int petch_trace_legacy(const void* mesh, int max_tris, int max_verts,

@@ -71,6 +71,11 @@ SIGNATURES = {
     "petch_raycast": [P, I, I, P, P, I, F, P, P, P, P],
     "petch_tracer_config": [I, I, I],
     "petch_nearest_face": [P, I, I, P, I, F, P, P, P],
+    "petch_gas_normals": [P, I, I, P, I, I, I, D, P, P],
+    "petch_trace_ff": [P, I, I, DP, P, U, I, P, P, P],
+    "petch_ff_scratch_bytes": [I, I, LLP],
+    "petch_ff_matrix": [P, I, I, P, I, P, P, P, P, L, P],
+    "petch_radiosity_solve": [P, I, I, P, P, P, I, P, D, D, I, P, P, P, P],
 }
 
 # The library's tracer configuration at load (bvh_width, steps_per_round, keep_lanes): what

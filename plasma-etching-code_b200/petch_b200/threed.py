@@ -210,24 +210,14 @@ def _unsupported(flags, par):
 # --------------------------------------------------------------------------------------------
 # the engine: all buffers of one run
 # --------------------------------------------------------------------------------------------
-class EtchEngine:
-    """Device state of one etch run on an (nx, ny, nz) grid."""
+class FluxEngine:
+    """Per-face device buffers and the flux stages of one mesh capacity (the part of the loop
+    between the mesh and the surface rate): mc_flux_3d_coupled, mc_flux_3d and
+    mc_flux_3d_radiosity on a DeviceMesh."""
 
-    def __init__(self, geo, par, flags, max_tris=None):
+    def __init__(self, geo, par, flags, max_tris):
         self.geo, self.par, self.flags = geo, par, flags
-        self.shape = tuple(int(s) for s in geo['phi_dev'].shape)
-        self.ncell = int(np.prod(self.shape))
-        self.dx = float(geo['dx'])
         dev = dict(device="cuda")
-        self.phi = geo['phi_dev']
-        self.tmp = torch.empty_like(self.phi)
-        self.ua = torch.empty_like(self.phi)
-        self.ub = torch.empty_like(self.phi)
-        self.F = torch.zeros_like(self.phi)
-        self.mask = geo['mask_dev']
-        self.mask_phi = geo['mask_phi_dev']
-        self.mask_idx = torch.nonzero(self.mask.view(-1)).view(-1).to(torch.int32)
-        self.active = torch.empty(self.ncell, dtype=torch.int32, **dev)
         # small[0:6] tracer work words (ray counter, error bits, u64 queries, u64 visits),
         # small[6:8] rate stats, small[8] band size
         self.small = torch.zeros(16, dtype=torch.int32, **dev)
@@ -235,7 +225,7 @@ class EtchEngine:
         self.dom = domain_params(geo, par)
         self.ionp = ion_params(par)
         self.chem = chem_params(par, flags)
-        self._alloc_faces(max_tris or default_capacity(self.shape))
+        self._alloc_faces(max_tris)
         self.prev = None          # (mesh, bare) of the previous step for the warm start
         self.ktimer = _NoTimer()  # set to an EventTimer to time individual trace launches
 
@@ -243,8 +233,6 @@ class EtchEngine:
         self.MT = int(MT)
         dev = dict(device="cuda", dtype=torch.float32)
         self.mesh = DeviceMesh(self.MT)
-        self.scratch = torch.empty(mesh_scratch_bytes(self.shape, self.MT), dtype=torch.uint8,
-                                   device="cuda")
         MT = self.MT
         self.tal4 = torch.empty((MT, 4), **dev)
         self.ang = torch.empty(MT, **dev)
@@ -257,17 +245,17 @@ class EtchEngine:
         self.bare = torch.empty(MT, **dev)
         self.V = torch.empty(MT, **dev)
         self.tmp5 = torch.empty(5 * MT, **dev)
+        self.rad = None           # radiosity buffers, allocated on first use
 
     def grow(self, need):
         MT = max(int(need * 1.5), 2 * self.MT)
         self._alloc_faces(MT)
 
-    # ---- stages ----
-    def build_mesh(self):
-        self.mesh.build(self.phi, self.dx, self.geo, self.scratch)
-
-    def flux_coupled(self, n_ion, n_neu, seed, warm):
-        """mc_flux_3d_coupled (threed.py:740-905) on the device."""
+    # ---- flux stages ----
+    def flux_coupled(self, n_ion, n_neu, seed, warm, bare_init=None):
+        """mc_flux_3d_coupled (threed.py:740-905) on the device.  The coverage starts from the
+        previous step's (warm, nearest face) or from bare_init (a device float[F] the caller
+        supplies), else cold at 1."""
         par, flags, m = self.par, self.flags, self.mesh
         s = _sp()
         A_src = float(self.geo['Lx'] * self.geo['Ly'])
@@ -276,12 +264,16 @@ class EtchEngine:
         work = self.small[0:6]
         faithful = (flags is not None and getattr(flags, "ion_reflection", False)
                     and getattr(flags, "chemistry", "langmuir") == "belen")
-        bare_init = False
-        if warm and self.prev is not None:
+        seeded = False
+        if bare_init is not None:
+            F = int(bare_init.numel())
+            self.bare[:F].copy_(bare_init.clamp(0.0, 1.0))
+            seeded = True
+        elif warm and self.prev is not None:
             pm, pb = self.prev
             _lib.call("petch_warmstart", pm.id, pm.MT, pm.MV, pb.data_ptr(), m.id, m.MT, m.MV,
                       self.bare.data_ptr(), work.data_ptr(), s)
-            bare_init = True
+            seeded = True
         if faithful:
             self.ktimer.start("k_ions")
             _lib.call("petch_trace_ions", m.id, m.MT, m.MV, ctypes.byref(self.dom),
@@ -305,8 +297,8 @@ class EtchEngine:
                       float(A_src / n_ion), 0.0, 1.5, 1, n_smooth, alpha, self.m_i.data_ptr(),
                       self.tmp5.data_ptr(), self.tmp5[m.MT:].data_ptr(), s)
             yields = (None, None, None)
-        n_fp = int(par.get('n_fp', 1 if bare_init else 4))
-        if not bare_init:
+        n_fp = int(par.get('n_fp', 1 if seeded else 4))
+        if not seeded:
             self.bare.fill_(1.0)
         betaE, betaO = float(par.get('betaE', 0.7)), float(par.get('betaO', 1.0))
         for it in range(n_fp):
@@ -354,6 +346,119 @@ class EtchEngine:
                       float(A_src / n_neu), 0.0, 4.0, 1, 0, 1.0, out.data_ptr(),
                       self.tmp5.data_ptr(), self.tmp5[m.MT:].data_ptr(), s)
         self.yields = (None, None, None)
+
+    def _radiosity_buffers(self, n_ff):
+        r = self.rad
+        if r is None or r['n_ff'] != n_ff:
+            MT = self.MT
+            nb = ctypes.c_longlong()
+            _lib.call("petch_ff_scratch_bytes", MT, int(n_ff), ctypes.byref(nb))
+            i32 = dict(device="cuda", dtype=torch.int32)
+            f64 = dict(device="cuda", dtype=torch.float64)
+            r = dict(n_ff=int(n_ff), fn=torch.empty((MT, 3), device="cuda"),
+                     hit=torch.empty(MT * n_ff, **i32), col=torch.empty(MT * n_ff, **i32),
+                     row_ptr=torch.empty(MT + 1, **i32), sky=torch.empty(MT, **f64),
+                     work2=torch.empty(4 * MT, **f64),
+                     scratch=torch.empty(int(nb.value), dtype=torch.uint8, device="cuda"))
+            self.rad = r
+        return r
+
+    def flux_radiosity(self, phi, n_ion, seed, n_ff=64, n_fp=4, n_iter=40):
+        """mc_flux_3d_radiosity (threed.py:923-991) on the device: ions as _ions_deterministic
+        (unsmoothed), into-gas normals from phi, n_ff form-factor rays per face, the CSR form
+        factor matrix, then n_fp rounds of the two-species Jacobi solve and the Belen coverage
+        update, starting from bare = 1."""
+        par, flags, m = self.par, self.flags, self.mesh
+        if par.get('radiosity_solver', 'jacobi') != 'jacobi':
+            raise NotImplementedError("only the Jacobi radiosity solver is provided")
+        s = _sp()
+        A_src = float(self.geo['Lx'] * self.geo['Ly'])
+        work = self.small[0:6]
+        faithful = (flags is not None and getattr(flags, "ion_reflection", False)
+                    and getattr(flags, "chemistry", "langmuir") == "belen")
+        self.ktimer.start("k_ions")
+        if faithful:
+            _lib.call("petch_trace_ions", m.id, m.MT, m.MV, ctypes.byref(self.dom),
+                      ctypes.byref(self.ionp), int(seed * 9 + 1) & 0xffffffff, int(n_ion),
+                      self.tal4.data_ptr(), self.ang.data_ptr(), work.data_ptr(), s)
+            _lib.call("petch_ion_post", m.id, m.MT, m.MV, self.tal4.data_ptr(), self.ang.data_ptr(),
+                      float(A_src / n_ion), 0, 1.0, self.y[0].data_ptr(), self.y[1].data_ptr(),
+                      self.y[2].data_ptr(), self.m_i.data_ptr(), self.cos_i.data_ptr(),
+                      self.tmp5.data_ptr(), s)
+            yields = (self.y[0].data_ptr(), self.y[1].data_ptr(), self.y[2].data_ptr())
+        else:
+            _lib.call("petch_trace_legacy", m.id, m.MT, m.MV, ctypes.byref(self.dom), 1,
+                      float(par['ion_ang_sigma']), 1.0, 0, 0, 0.34, 0.8,
+                      int(seed * 9 + 1) & 0xffffffff, int(n_ion), self.flux.data_ptr(),
+                      self.ang.data_ptr(), work.data_ptr(), s)
+            _lib.call("petch_cos_ratio", m.id, m.MT, m.MV, self.flux.data_ptr(),
+                      self.ang.data_ptr(), self.cos_i.data_ptr(), s)
+            _lib.call("petch_norm_smooth", m.id, m.MT, m.MV, self.flux.data_ptr(),
+                      float(A_src / n_ion), 0.0, 1.5, 1, 0, 1.0, self.m_i.data_ptr(),
+                      self.tmp5.data_ptr(), self.tmp5[m.MT:].data_ptr(), s)
+            yields = (None, None, None)
+        self.ktimer.stop("k_ions")
+        r = self._radiosity_buffers(n_ff)
+        nx, ny, nz = phi.shape
+        _lib.call("petch_gas_normals", m.id, m.MT, m.MV, phi.data_ptr(), nx, ny, nz,
+                  float(self.geo['dx']), r['fn'].data_ptr(), s)
+        self.ktimer.start("k_ff")
+        _lib.call("petch_trace_ff", m.id, m.MT, m.MV, ctypes.byref(self.dom), r['fn'].data_ptr(),
+                  int(seed) & 0xffffffff, int(n_ff), r['hit'].data_ptr(), work.data_ptr(), s)
+        self.ktimer.stop("k_ff")
+        self.radiosity_from_hits(r['hit'], n_ff, yields, n_fp, n_iter)
+        self.yields = yields
+
+    def radiosity_from_hits(self, hit, n_ff, yields, n_fp=4, n_iter=40):
+        """The deterministic part of mc_flux_3d_radiosity from form-factor hits already on the
+        device (int[MT * n_ff]): matrix assembly, then the coverage <-> radiosity fixed point
+        into m_F, m_O and bare (m_i, cos_i and the yields must be in place)."""
+        m = self.mesh
+        s = _sp()
+        r = self._radiosity_buffers(n_ff)
+        _lib.call("petch_ff_matrix", m.id, m.MT, m.MV, hit.data_ptr(), int(n_ff),
+                  r['row_ptr'].data_ptr(), r['col'].data_ptr(), r['sky'].data_ptr(),
+                  r['scratch'].data_ptr(), r['scratch'].numel(), s)
+        self.bare.fill_(1.0)
+        betaE, betaO = float(self.par.get('betaE', 0.7)), float(self.par.get('betaO', 1.0))
+        for _ in range(n_fp):
+            self.ktimer.start("k_rad_solve")
+            _lib.call("petch_radiosity_solve", m.id, m.MT, m.MV, r['row_ptr'].data_ptr(),
+                      r['col'].data_ptr(), r['sky'].data_ptr(), int(n_ff), self.bare.data_ptr(),
+                      betaE, betaO, int(n_iter), self.m_F.data_ptr(), self.m_O.data_ptr(),
+                      r['work2'].data_ptr(), s)
+            self.ktimer.stop("k_rad_solve")
+            _lib.call("petch_belen_bare", m.id, m.MT, m.MV, ctypes.byref(self.chem),
+                      self.m_i.data_ptr(), self.m_F.data_ptr(), self.m_O.data_ptr(),
+                      self.cos_i.data_ptr(), yields[1], yields[2], self.bare.data_ptr(), s)
+
+
+class EtchEngine(FluxEngine):
+    """Device state of one etch run on an (nx, ny, nz) grid."""
+
+    def __init__(self, geo, par, flags, max_tris=None):
+        self.shape = tuple(int(s) for s in geo['phi_dev'].shape)
+        self.ncell = int(np.prod(self.shape))
+        self.dx = float(geo['dx'])
+        dev = dict(device="cuda")
+        self.phi = geo['phi_dev']
+        self.tmp = torch.empty_like(self.phi)
+        self.ua = torch.empty_like(self.phi)
+        self.ub = torch.empty_like(self.phi)
+        self.F = torch.zeros_like(self.phi)
+        self.mask = geo['mask_dev']
+        self.mask_phi = geo['mask_phi_dev']
+        self.mask_idx = torch.nonzero(self.mask.view(-1)).view(-1).to(torch.int32)
+        self.active = torch.empty(self.ncell, dtype=torch.int32, **dev)
+        super().__init__(geo, par, flags, max_tris or default_capacity(self.shape))
+
+    def _alloc_faces(self, MT):
+        super()._alloc_faces(MT)
+        self.scratch = torch.empty(mesh_scratch_bytes(self.shape, self.MT), dtype=torch.uint8,
+                                   device="cuda")
+
+    def build_mesh(self):
+        self.mesh.build(self.phi, self.dx, self.geo, self.scratch)
 
     def rate_and_extend(self, band):
         m = self.mesh
@@ -449,8 +554,6 @@ def run_etch_3d(Lx=10.0, Ly=4.0, Lz=14.0, dx=0.4, trench_width=4.0, mask_th=2.0,
     if surf_smooth and surf_smooth > 0.0:
         raise NotImplementedError("surf_smooth is not implemented")
     nt = getattr(flags, "neutral_transport", "mc")
-    if nt == "radiosity":
-        raise NotImplementedError("neutral_transport='radiosity' is not implemented yet")
     hooks = hooks or {}
     mc_par = par
     if getattr(flags, "chemistry", "langmuir") == "belen":
@@ -490,7 +593,9 @@ def run_etch_3d(Lx=10.0, Ly=4.0, Lz=14.0, dx=0.4, trench_width=4.0, mask_th=2.0,
         else:
             n_ion_s, n_neu_s = n_ion, n_neu
         st_timer.start("flux")
-        if coupled:
+        if nt == "radiosity":
+            eng.flux_radiosity(eng.phi, n_ion_s, seed)
+        elif coupled:
             eng.flux_coupled(n_ion_s, n_neu_s, seed, warm)
         else:
             eng.par = mc_par
@@ -525,7 +630,7 @@ def run_etch_3d(Lx=10.0, Ly=4.0, Lz=14.0, dx=0.4, trench_width=4.0, mask_th=2.0,
             st_timer.start("reinit")
             eng.reinit(band + 2.0 * dx)
             st_timer.stop("reinit")
-        eng.end_step(warm and coupled)
+        eng.end_step(warm and coupled and nt != "radiosity")
         st['nsub'] = nsub
         if record_depth_every and (step % record_depth_every == 0 or step == n_steps - 1):
             g2 = _host_geo(geo, eng.phi)
@@ -625,7 +730,76 @@ def max_depth_3d(geo):
 
 def extract_mesh_3d(phi, dx, geo=None):
     """extract_mesh_3d (threed.py:62-69): (verts f32, faces i32, centroids f64, areas f64) from
-    the device marching cubes (areas floored at 1e-9 as every consumer applies)."""
+    the device marching cubes."""
+    return extract_mesh_3d_device(phi, dx, geo)[1]
+
+
+# --------------------------------------------------------------------------------------------
+# drop-in flux functions on a DeviceMesh
+# --------------------------------------------------------------------------------------------
+def _flux_engine(mesh, geo, par, flags):
+    fe = FluxEngine(geo, par, flags, mesh.MT)
+    fe.mesh = mesh                       # the caller's mesh (same face capacity)
+    return fe
+
+
+def _host(t, F):
+    return t[:F].double().cpu().numpy()
+
+
+def mc_flux_3d_coupled(mesh, verts, faces, areas, geo, par, n_ion=20000, n_neu=20000, seed=0,
+                       sampling="pseudo", flags=None, n_fp=4, bare_init=None):
+    """mc_flux_3d_coupled (threed.py:740-905) on a DeviceMesh (from extract_mesh_3d_device):
+    returns numpy (m_i, m_F, m_O, cos_i, bare) and, on the faithful-ion path, sets
+    par['_ion_yield'] like the reference.  Sources are device Philox streams whatever `sampling`
+    says (the reference's CUDA path also generates them on the device); n_fp is unused there too
+    (4 rounds cold, 1 from bare_init).  verts / faces / areas describe the same mesh and are not
+    read."""
+    F = mesh.n_faces()
+    fe = _flux_engine(mesh, geo, par, flags)
+    b0 = None
+    if bare_init is not None:
+        b0 = torch.as_tensor(np.asarray(bare_init, np.float32), device="cuda")
+    fe.flux_coupled(int(n_ion), int(n_neu), int(seed), False, bare_init=b0)
+    _raise_trace_errors(fe)
+    _set_ion_yield(fe, par, F)
+    return (_host(fe.m_i, F), _host(fe.m_F, F), _host(fe.m_O, F), _host(fe.cos_i, F),
+            _host(fe.bare, F))
+
+
+def mc_flux_3d_radiosity(mesh, verts, faces, centroids, areas, geo, par, n_ion=20000, n_ff=64,
+                         seed=0, flags=None, n_fp=4):
+    """mc_flux_3d_radiosity (threed.py:923-991) on a DeviceMesh: returns numpy
+    (m_i, m_F, m_O, cos_i) and sets or clears par['_ion_yield'] like the reference.  geo['phi']
+    (host or device) is the level set the mesh was extracted from (for the into-gas normals)."""
+    F = mesh.n_faces()
+    fe = _flux_engine(mesh, geo, par, flags)
+    phi = geo['phi']
+    phi = (phi if isinstance(phi, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(phi)))
+    phi = phi.to("cuda", torch.float32).contiguous()
+    fe.flux_radiosity(phi, int(n_ion), int(seed), n_ff=int(n_ff), n_fp=int(n_fp))
+    _raise_trace_errors(fe)
+    _set_ion_yield(fe, par, F)
+    return _host(fe.m_i, F), _host(fe.m_F, F), _host(fe.m_O, F), _host(fe.cos_i, F)
+
+
+def _raise_trace_errors(fe):
+    err = int(fe.small[1].item())
+    if err:
+        raise RuntimeError(f"device traversal limit hit (error bits {err})")
+
+
+def _set_ion_yield(fe, par, F):
+    if fe.yields[0] is None:
+        par.pop('_ion_yield', None)
+    else:
+        par['_ion_yield'] = tuple(_host(fe.y[q], F) for q in range(3))
+
+
+def extract_mesh_3d_device(phi, dx, geo=None):
+    """extract_mesh_3d_gpu + wp.Mesh (threed.py:75-100, 1674-1675) in one: the DeviceMesh (the
+    handle every flux function takes as `mesh`) and its host arrays (verts f32, faces i32,
+    centroids f64, areas f64)."""
     phi_t = phi if isinstance(phi, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(phi))
     phi_t = phi_t.to("cuda", torch.float32).contiguous()
     shape = tuple(phi_t.shape)
@@ -639,4 +813,4 @@ def extract_mesh_3d(phi, dx, geo=None):
         if c['err'] & (MESH_ERR_TRI_OVERFLOW | MESH_ERR_VERT_OVERFLOW | MESH_ERR_HASH_FULL):
             MT = 2 * max(MT, c['F'], c['V'])
             continue
-        return mesh.host_arrays()
+        return mesh, mesh.host_arrays()

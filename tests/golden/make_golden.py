@@ -4,7 +4,7 @@ warp-lang replaced by warp_shim.py (a CPU stand-in: see its docstring for what i
 
 Run in a checkout that has the reference at /root/reference (or $PETCH_REFERENCE):
 
-    python tests/golden/make_golden.py [group ...]      # groups: levelset surface flux
+    python tests/golden/make_golden.py [group ...]   # groups: levelset surface flux radiosity
 
 The fixtures are committed; tests read only the .npz files, never the reference.
 """
@@ -251,7 +251,76 @@ def flux():
     np.savez_compressed(os.path.join(HERE, "flux.npz"), **out)
 
 
-GROUPS = {"levelset": levelset, "surface": surface, "flux": flux}
+def radiosity():
+    """mc_flux_3d_radiosity (threed.py:923-991) run unmodified on small meshes.  For one seed per
+    case the form-factor hits of its _trace_ff launch are recorded with the ion results, so the
+    deterministic part (matrix assembly, Jacobi solves, coverage fixed point) can be replayed
+    exactly; over 8 seeds the per-face means and standard errors of (m_i, m_F, m_O) pin the
+    estimator statistically.  _gas_normals is recorded on the same meshes."""
+    out = {}
+    wp = t3.wp
+    real_launch = wp.launch
+    rec = {}
+
+    def launch(k, dim, device=None, inputs=()):
+        real_launch(k, dim, device=device, inputs=inputs)
+        if k is t3._trace_ff:
+            rec['hit'] = np.asarray(inputs[3]).astype(np.int32).copy()
+
+    wp.launch = launch
+    try:
+        cases = (("hole", True, True), ("trench", False, True), ("hole_legacy", True, False))
+        for key, hole, faithful in cases:
+            m, geo, phi = _small_mesh(hole, nx=10, ny=10, nz=14, dx=0.3)
+            verts = m.verts.astype(np.float32)
+            faces = m.faces
+            v64 = verts.astype(np.float64)[faces]
+            centroids = v64.mean(axis=1)
+            areas = 0.5 * np.linalg.norm(np.cross(v64[:, 1] - v64[:, 0], v64[:, 2] - v64[:, 0]),
+                                         axis=1)
+            geo = dict(geo, phi=phi.astype(np.float64))
+            mesh = wp.Mesh(points=wp.array(verts, dtype=wp.vec3),
+                           indices=wp.array(faces.flatten(), dtype=wp.int32))
+            par = dict(t3.PAR, periodic_y=0 if hole else 1)
+            flags = t3.DEFAULT_FLAGS.__class__(
+                chemistry="belen" if faithful else "langmuir", yield_angular="viennaps",
+                ion_reflection=faithful, coverage_sticking=True, neutral_transport="radiosity")
+            out[f"{key}_verts"], out[f"{key}_faces"] = verts, faces
+            out[f"{key}_phi"] = phi.astype(np.float32)
+            out[f"{key}_geo"] = np.array([geo['Lx'], geo['Ly'], geo['Lz'], geo['dx'],
+                                          par['periodic_y']])
+            out[f"{key}_gas_normals"] = t3._gas_normals(verts, faces, centroids, geo)
+            n_ion = 3000
+
+            def run(sd):
+                p = dict(par)
+                t0 = time.time()
+                r = t3.mc_flux_3d_radiosity(mesh, verts, faces, centroids, areas, geo, p,
+                                            n_ion=n_ion, n_ff=64, seed=sd, flags=flags)
+                print(f"  {key} seed {sd}: {time.time() - t0:.1f}s", flush=True)
+                return r, p
+
+            (m_i, m_F, m_O, cos_i), p = run(100)
+            out[f"{key}_hit"] = rec['hit']
+            out[f"{key}_m_i"], out[f"{key}_cos_i"] = m_i, cos_i
+            out[f"{key}_m_F"], out[f"{key}_m_O"] = m_F, m_O
+            if faithful:
+                out[f"{key}_ion_yield"] = np.stack(p['_ion_yield'])
+            if key == "hole_legacy":
+                continue
+
+            def stats(sd):
+                (mi, mF, mO, _), _ = run(sd)
+                return np.stack([mi, mF, mO])
+
+            mean, se = _mean_se(stats, range(200, 208))
+            out[f"{key}_mean"], out[f"{key}_se"] = mean, se
+    finally:
+        wp.launch = real_launch
+    np.savez_compressed(os.path.join(HERE, "radiosity.npz"), **out)
+
+
+GROUPS = {"levelset": levelset, "surface": surface, "flux": flux, "radiosity": radiosity}
 
 if __name__ == "__main__":
     for g in (sys.argv[1:] or list(GROUPS)):
