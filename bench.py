@@ -102,24 +102,17 @@ def peaks():
     return 6650.0, "fallback"
 
 
-# ------------------------------------------------------------------------------------------
-def run_b200(args):
+def timed_run(par, flags, W, K, world, rank, local, dist):
+    """W untimed + K timed steps of the workload with `flags`; per-step CUDA events on the compute
+    stream, 256 MB L2 flush before each timed step (outside the interval), trace-kernel events,
+    launch counts and clocks over the timed region.  Time = max over ranks."""
     import torch
-    import torch.distributed as dist
     from petch_b200 import _lib, threed as t3
-
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
-    par, flags = sf6o2()
-    W, K = args.warmup, min(args.steps, N_STEPS - args.warmup)
     flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda")   # 256 MB > L2
     ev = {}
     info = {}
     ktimer = t3.EventTimer()
+    radiosity = getattr(flags, "neutral_transport", "mc") == "radiosity"
 
     def before(step, eng):
         if step == W:
@@ -137,7 +130,6 @@ def run_b200(args):
             ev[step] = [e]
 
     rays = []
-
     work_q = []
 
     def after(step, eng, st):
@@ -145,8 +137,11 @@ def run_b200(args):
             e = torch.cuda.Event(enable_timing=True)
             e.record()
             ev[step].append(e)
-            n_fp = 4 if step == 0 else 1
-            rays.append(RAYS + 2 * RAYS * n_fp)
+            if radiosity:                     # ions + n_ff = 64 form-factor rays per face
+                rays.append(RAYS + 64 * st['F'])
+            else:                             # ions + F and O neutrals per fixed-point round
+                n_fp = 4 if step == 0 else 1
+                rays.append(RAYS + 2 * RAYS * n_fp)
             work_q.append((st['queries'], st['visits']))
         if step == W + K - 1:
             torch.cuda.synchronize()
@@ -168,7 +163,46 @@ def run_b200(args):
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dist.all_reduce(launches, op=dist.ReduceOp.SUM)
-    total_s = float(t.item())
+    return dict(geo=geo, kms=kms, info=info, rays=rays, work_q=work_q, total_s=float(t.item()),
+                launches=int(launches.item()))
+
+
+def radiosity_summary(par, flags, W, K, world, rank, local, dist):
+    """The workload's second run (neutral_transport='radiosity'): steps/s, rays/s (ions + form
+    factor rays) and per-step kernel times."""
+    from petch_b200 import params
+    fl = params.Flags(**{**flags.__dict__, "neutral_transport": "radiosity"})
+    r = timed_run(par, fl, W, K, world, rank, local, dist)
+    total_s = r['total_s']
+    return {"value": world * K / total_s, "unit": "steps/s", "ms_per_step": 1e3 * total_s / K,
+            "steps": K, "warmup": W,
+            "mrays_per_s": float(np.sum(r['rays'])) * world / total_s / 1e6,
+            "rays_per_step": int(np.mean(r['rays'])), "faces_last_step": r['info']['F'],
+            "kernel_ms_per_step": {k: float(np.sum(v)) / K for k, v in r['kms'].items()},
+            "gpu_launches": r['launches'], "clocks": r['info'].get('clk'),
+            "stage_seconds": dict(r['geo']['timings']),
+            "workload": "the same trench, neutral_transport='radiosity' (64 form-factor rays per "
+                        "face, 4 coverage rounds of 40 Jacobi sweeps, 2^22 ions), seed 0"}
+
+
+# ------------------------------------------------------------------------------------------
+def run_b200(args):
+    import torch
+    import torch.distributed as dist
+    from petch_b200 import _lib, threed as t3
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    par, flags = sf6o2()
+    W, K = args.warmup, min(args.steps, N_STEPS - args.warmup)
+    r = timed_run(par, flags, W, K, world, rank, local, dist)
+    geo, kms, info, rays, work_q = r['geo'], r['kms'], r['info'], r['rays'], r['work_q']
+    total_s = r['total_s']
+    launches = r['launches']
     value = world * K / total_s
     # ---- roofline of the dominant kernel (live CUDA events over the timed region) ----
     dom_name = max(kms, key=lambda k: sum(kms[k])) if kms else None
@@ -207,8 +241,10 @@ def run_b200(args):
            "data": "synthetic (analytic trench geometry, Philox rays)",
            "config": config_dict(world, args), "mrays_per_s": mrays,
            "primary_rays_per_step": int(np.mean(rays)),
-           "gpu_launches": int(launches.item()), "roofline": roof,
+           "gpu_launches": launches, "roofline": roof,
            "clocks": info.get('clk'), "stage_seconds": {k: v for k, v in geo['timings'].items()}}
+    if not args.no_radiosity:
+        out["radiosity"] = radiosity_summary(par, flags, W, K, world, rank, local, dist)
     if rank == 0 and not args.no_e2e:
         out["e2e"] = e2e(args, par, flags)
     if rank == 0 and not args.no_cpu_baseline:
@@ -311,6 +347,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-radiosity", action="store_true")
     args = ap.parse_args()
     if args.warmup < 0 or args.steps < 1 or args.warmup >= N_STEPS:
         raise SystemExit("need 0 <= warmup < 100 and steps >= 1")
