@@ -184,6 +184,15 @@ int petch_extend_velocity(const void* mesh, int max_tris, int max_verts, const f
                           const float* V, float* Fs, int fold_mask, int* active, int* n_active,
                           int max_active, int* work, void* stream);
 
+/* Replaces extend_velocity_3d (petch/threed.py:1310-1321, run_etch_3d's extend != "gpu"): as
+ * petch_extend_velocity but each band cell takes V of the face with the nearest CENTROID (the
+ * reference's cKDTree over centroids); exact ties go to the lower face index. */
+int petch_extend_velocity_centroid(const void* mesh, int max_tris, int max_verts, const float* phi,
+                                   const uint8_t* mask, int nx, int ny, int nz, double dx,
+                                   double band, const float* V, float* Fs, int fold_mask,
+                                   int* active, int* n_active, int max_active, int* work,
+                                   void* stream);
+
 /* Replaces gpu_warmstart_bare + _nearest_face_cov (petch/threed.py:1619-1639): bare[f] =
  * clip(prev_bare[nearest face of the previous mesh to centroid f], 0, 1), 1 if none. */
 int petch_warmstart(const void* prev_mesh, int prev_max_tris, int prev_max_verts,
@@ -259,6 +268,22 @@ int petch_surface_rate(const void* mesh, int max_tris, int max_verts, const petc
 int petch_advect_sparse(float* phi, float* tmp, const float* F, const float* mask_phi,
                         const int* mask_idx, int n_mask, const int* active, int n_active, int nx,
                         int ny, int nz, float inv_dx, float dt_sub, int nsub, void* stream);
+
+/* Replaces reinit_gpu + _reinit_iter (petch/threed.py:1349-1418, reinit_method="gpu"): n_iter
+ * forward-Euler sweeps (step 0.3 dx) of phi_tau + sgn(phi0)(|grad phi| - 1) = 0 with the
+ * Russo-Smereka sub-cell target phi0 / max(|grad phi0|, 0.5) clipped to +-1.8 dx at interface
+ * cells (sign change with a face neighbour).  phi0, tmp: scratch grids; phi_out may equal phi_in. */
+int petch_reinit_pde(const float* phi_in, float* phi_out, float* phi0, float* tmp, int nx, int ny,
+                     int nz, double dx, int n_iter, void* stream);
+
+/* Replaces run_etch_3d's surf_smooth step (petch/threed.py:1779-1782):
+ * phi = scipy.ndimage.gaussian_filter(phi, sigma) (axes 0, 1, 2 in turn; weights
+ * exp(-t^2 / (2 sigma^2)) normalised over |t| <= int(truncate * sigma + 0.5) <= 64; 'reflect'
+ * boundaries; double accumulation), then phi[mask] = mask_phi[mask] when mask is not NULL.
+ * tmp_a, tmp_b: scratch grids. */
+int petch_gaussian_smooth(float* phi, float* tmp_a, float* tmp_b, const uint8_t* mask,
+                          const float* mask_phi, int nx, int ny, int nz, double sigma,
+                          double truncate, void* stream);
 
 /* ---- deterministic radiosity neutrals (mc_flux_3d_radiosity, petch/threed.py:923-991) ---- */
 

@@ -11,10 +11,15 @@ Reference lines followed (paths within the reference project):
   angular_factors / _yields / _ied_yield   petch/chemistry.py:10-59
   run_etch_3d          petch/threed.py:1643-1795   CFL, band, seeds, warm start
   extend_velocity_gpu  petch/threed.py:1333-1346 ; faces_in_mask :1608-1616
+  extend_velocity_3d   petch/threed.py:1310-1321   nearest centroid (the same cKDTree call)
+  reinit_gpu           petch/threed.py:1349-1418   Russo-Smereka PDE sweeps
+  surf_smooth          petch/threed.py:1779-1782   the same scipy gaussian_filter call
+  mc_flux_3d_radiosity petch/threed.py:923-1029    _gas_normals :1553-1568, _cosine_dirs :1571-1579
   _depth3d / max_depth_3d petch/threed.py:1798-1869
 Parity pinning: level-set stages and the per-face arithmetic against tests/golden/*.npz made by
 running the reference's own code (tests/golden/make_golden.py); Monte-Carlo stages statistically
-against the reference kernels' per-face means (tests/golden/flux.npz).  Marching cubes and the seed
+against the reference kernels' per-face means (tests/golden/flux.npz, radiosity.npz); the
+radiosity fixed point exactly from the reference's recorded form-factor hits.  Marching cubes and the seed
 distance (skfmm) are third-party in the reference: parity unpinned there.
 """
 import ctypes
@@ -444,6 +449,76 @@ def flux_coupled(mesh, geo, par, flags, n_ion, n_neu, seed, bare_init=None, tt=N
     return m_i, m_F, m_O, cos_i, bare, iy
 
 
+# ------------------------------- run_etch_3d options -------------------------------
+def reinit_pde(phi, dx, n_iter=24):
+    """reinit_gpu / _reinit_iter (threed.py:1349-1418) in float32 numpy: n_iter forward-Euler
+    sweeps of step 0.3 dx, Russo-Smereka sub-cell target at interface cells."""
+    f = np.float32
+    a = np.asarray(phi, np.float32).copy()
+    phi0 = a.copy()
+    inv = f(1.0 / dx)
+    dtau = f(0.3 * dx)
+
+    def nb(x):
+        p = np.pad(x, 1, mode="edge")
+        return (p[:-2, 1:-1, 1:-1], p[2:, 1:-1, 1:-1], p[1:-1, :-2, 1:-1], p[1:-1, 2:, 1:-1],
+                p[1:-1, 1:-1, :-2], p[1:-1, 1:-1, 2:])
+
+    o_xm, o_xp, o_ym, o_yp, o_zm, o_zp = nb(phi0)
+    s0 = phi0
+    interface = ((s0 * o_xm < 0) | (s0 * o_xp < 0) | (s0 * o_ym < 0) | (s0 * o_yp < 0)
+                 | (s0 * o_zm < 0) | (s0 * o_zp < 0))
+    gx0 = (o_xp - o_xm) * f(0.5) * inv
+    gy0 = (o_yp - o_ym) * f(0.5) * inv
+    gz0 = (o_zp - o_zm) * f(0.5) * inv
+    grad0 = np.maximum(np.sqrt(gx0 * gx0 + gy0 * gy0 + gz0 * gz0), f(0.5))
+    dxl = f(1.0) / inv
+    D = np.clip(s0 / grad0, f(-1.8) * dxl, f(1.8) * dxl)
+    sgn0 = np.where(s0 < 0, f(-1.0), f(1.0))
+    sgn = s0 / np.sqrt(s0 * s0 + f(0.25) / (inv * inv))
+    for _ in range(n_iter):
+        xm, xp, ym, yp, zm, zp = nb(a)
+        Dxm, Dxp = (a - xm) * inv, (xp - a) * inv
+        Dym, Dyp = (a - ym) * inv, (yp - a) * inv
+        Dzm, Dzp = (a - zm) * inv, (zp - a) * inv
+        pos = sgn > 0
+        gx = np.where(pos, np.maximum(np.maximum(Dxm, 0), -np.minimum(Dxp, 0)),
+                      np.maximum(-np.minimum(Dxm, 0), np.maximum(Dxp, 0)))
+        gy = np.where(pos, np.maximum(np.maximum(Dym, 0), -np.minimum(Dyp, 0)),
+                      np.maximum(-np.minimum(Dym, 0), np.maximum(Dyp, 0)))
+        gz = np.where(pos, np.maximum(np.maximum(Dzm, 0), -np.minimum(Dzp, 0)),
+                      np.maximum(-np.minimum(Dzm, 0), np.maximum(Dzp, 0)))
+        G = np.sqrt(gx * gx + gy * gy + gz * gz)
+        bulk = a - dtau * sgn * (G - f(1.0))
+        front = a - dtau * inv * (sgn0 * np.abs(a) - D)
+        a = np.where(interface, front, bulk).astype(np.float32)
+    return a
+
+
+def gaussian_smooth(phi, sigma, mask=None, mask_phi=None):
+    """run_etch_3d's surf_smooth step (threed.py:1779-1782): the same scipy call, then the mask
+    re-pin."""
+    from scipy.ndimage import gaussian_filter
+    out = gaussian_filter(np.asarray(phi, np.float64), sigma)
+    if mask is not None:
+        out[mask] = np.asarray(mask_phi, np.float64)[mask]
+    return out
+
+
+def extend_nearest_centroid(V, centroids, phi, dx, band):
+    """extend_velocity_3d (threed.py:1310-1321): band cells take V of the nearest centroid."""
+    from scipy.spatial import cKDTree
+    Fs = np.zeros(phi.shape)
+    bm = np.abs(phi) < band
+    ii, jj, kk = np.where(bm)
+    if len(centroids) == 0 or len(ii) == 0:
+        return Fs
+    pts = np.stack([ii * dx, jj * dx, kk * dx], axis=1)
+    _, idx = cKDTree(centroids).query(pts)
+    Fs[ii, jj, kk] = np.asarray(V)[idx]
+    return Fs
+
+
 # ------------------------------- radiosity neutrals -------------------------------
 def gas_normals(verts, faces, centroids, phi, dx):
     """_gas_normals (threed.py:1553-1568): float32 winding normals of the float32 vertices,
@@ -575,7 +650,7 @@ def depth3d(geo, phi, half=1.0):
 
 def run_etch_3d(Lx, Ly, Lz, dx, trench_width, mask_th, sub_top, t_end, n_steps, hole, par, flags,
                 n_ion, n_neu, seed_offset=0, record_depth_every=0, max_seconds=None, steps=None,
-                stage_times=None):
+                stage_times=None, reinit_method="fsm", extend="gpu", surf_smooth=0.0):
     """run_etch_3d (threed.py:1643-1795) with the oracle's stages (coverage-coupled MC path or
     radiosity neutrals, FSM reinit, nearest-face extension).  Runs `steps` (default n_steps) steps of the n_steps
     schedule.  Returns (phi, depth_history, stats); stage_times (list) receives one dict of stage
@@ -623,7 +698,9 @@ def run_etch_3d(Lx, Ly, Lz, dx, trench_width, mask_th, sub_top, t_end, n_steps, 
         pts = np.stack([geo['xs'][ii], geo['ys'][jj], geo['zs'][kk]], axis=1)
         pts = pts.astype(np.float32).astype(np.float64)
         Fs = np.zeros(phi.shape)
-        if len(pts) and mesh.F:
+        if extend != "gpu":
+            Fs = extend_nearest_centroid(V, mesh.centroid, phi.astype(np.float64), dx, band)
+        elif len(pts) and mesh.F:
             q = mesh.nearest(pts)
             Fs[ii, jj, kk] = np.where(q >= 0, V[np.maximum(q, 0)], 0.0)
         st['extend'] = time.time() - ta
@@ -634,7 +711,12 @@ def run_etch_3d(Lx, Ly, Lz, dx, trench_width, mask_th, sub_top, t_end, n_steps, 
         phi = advect(phi, Fs.astype(np.float32), mask, mask_phi, 1.0 / dx, dt / nsub, nsub)
         st['advect'] = time.time() - ta
         ta = time.time()
-        phi = reinit(phi.astype(np.float32), dx, band + 2.0 * dx).astype(np.float32)
+        if reinit_method == "gpu":
+            phi = reinit_pde(phi.astype(np.float32), dx)
+        else:
+            phi = reinit(phi.astype(np.float32), dx, band + 2.0 * dx).astype(np.float32)
+        if surf_smooth and surf_smooth > 0.0:
+            phi = gaussian_smooth(phi, surf_smooth, mask, mask_phi).astype(np.float32)
         st['reinit'] = time.time() - ta
         st['nsub'] = nsub
         if stage_times is not None:

@@ -114,12 +114,15 @@ __global__ void k_ff_sky(const int* __restrict__ hdr, int MT, const int* __restr
         D[i] = (double)esc[i] / (double)n_ff;
 }
 
-// One Jacobi iteration for both species, one warp per row i:
+// One Jacobi iteration for both species, a group of kG lanes per row i (32 / kG rows per warp):
 //   G_i = D_i + (1 / n_ff) * sum over the row's entries j of x_j,
 // where x_j = (1 - s_j) G_j from the previous iteration (x = y_in), or (1 - s_j) D_j on the first
 // (y_in == nullptr), s = clip(bare * beta, 0, 1).  The last iteration writes clip(G, 0, 8) as
-// float; the others write x_i = (1 - s_i) G_i for the next.  Lanes take entries in a fixed order
-// and reduce with a fixed butterfly, so every run sums in the same order.
+// float; the others write x_i = (1 - s_i) G_i for the next.  Lane q of a group sums entries
+// q, q + kG, q + 2 kG, ... and the group reduces with a fixed butterfly, so every run sums in the
+// same order.
+constexpr int kG = 8;
+
 __global__ void __launch_bounds__(kRB) k_rad_iter(const int* __restrict__ hdr, int MT,
                                                   const int* __restrict__ row_ptr,
                                                   const int* __restrict__ col,
@@ -130,28 +133,37 @@ __global__ void __launch_bounds__(kRB) k_rad_iter(const int* __restrict__ hdr, i
                                                   double2* __restrict__ y_out, float* __restrict__ gE,
                                                   float* __restrict__ gO) {
     const int F = min(hdr[HDR_F], MT);
-    const int lane = threadIdx.x & 31;
-    const int warps = (gridDim.x * blockDim.x) >> 5;
-    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < F; i += warps) {
-        const int e0 = row_ptr[i], e1 = row_ptr[i + 1];
+    const int sub = threadIdx.x & (kG - 1);
+    const int groups = (gridDim.x * blockDim.x) / kG;
+    // every lane of a warp runs the same number of trips (the warp's groups share the loop
+    // bound), so the butterfly below always has the full warp converged
+    const int first = (blockIdx.x * blockDim.x + threadIdx.x) / kG;
+    const int warp_first = first - ((threadIdx.x & 31) / kG);
+    for (int base = warp_first; base < F; base += groups) {
+        const int i = base + ((threadIdx.x & 31) / kG);
         double sE = 0.0, sO = 0.0;
-        for (int e = e0 + lane; e < e1; e += 32) {
-            const int j = __ldg(col + e);
+        if (i < F) {
+            const int e0 = row_ptr[i], e1 = row_ptr[i + 1];
             if (y_in) {
-                const double2 x = y_in[j];
-                sE += x.x;
-                sO += x.y;
+                for (int e = e0 + sub; e < e1; e += kG) {
+                    const double2 x = y_in[__ldg(col + e)];
+                    sE += x.x;
+                    sO += x.y;
+                }
             } else {
-                const double b = (double)__ldg(bare + j), dj = __ldg(D + j);
-                sE += (1.0 - fmin(fmax(b * betaE, 0.0), 1.0)) * dj;
-                sO += (1.0 - fmin(fmax(b * betaO, 0.0), 1.0)) * dj;
+                for (int e = e0 + sub; e < e1; e += kG) {
+                    const int j = __ldg(col + e);
+                    const double b = (double)__ldg(bare + j), dj = __ldg(D + j);
+                    sE += (1.0 - fmin(fmax(b * betaE, 0.0), 1.0)) * dj;
+                    sO += (1.0 - fmin(fmax(b * betaO, 0.0), 1.0)) * dj;
+                }
             }
         }
-        for (int o = 16; o > 0; o >>= 1) {
+        for (int o = kG / 2; o > 0; o >>= 1) {
             sE += __shfl_xor_sync(0xffffffffu, sE, o);
             sO += __shfl_xor_sync(0xffffffffu, sO, o);
         }
-        if (lane == 0) {
+        if (sub == 0 && i < F) {
             const double GE = D[i] + inv_nff * sE, GO = D[i] + inv_nff * sO;
             if (gE) {
                 gE[i] = (float)fmin(fmax(GE, 0.0), 8.0);
@@ -301,7 +313,7 @@ extern "C" int petch_radiosity_solve(const void* mesh, int max_tris, int max_ver
     double2* ya = reinterpret_cast<double2*>(work2);
     double2* yb = ya + max_tris;
     const double2* yin = nullptr;
-    const int blocks = grid_for((long long)max_tris * 32, kRB);
+    const int blocks = grid_for((long long)max_tris * kG, kRB);
     for (int it = 0; it < n_iter; ++it) {
         const bool last = it == n_iter - 1;
         double2* yout = (it & 1) ? yb : ya;

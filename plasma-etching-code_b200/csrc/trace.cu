@@ -420,6 +420,7 @@ struct GridArgs {
 // reference's 1e6 if nothing is found there); all other cells get 0.  With fold != 0, mask cells
 // are written as -1 (the advection's pinned-cell marker) and band cells with F > 0 are listed in
 // `active` for the sparse advection.
+template <bool CENTROID>
 __global__ void __launch_bounds__(kTB) k_extend(MeshView m, GridArgs G, const float* __restrict__ phi,
                                                 const uint8_t* __restrict__ mask,
                                                 const float* __restrict__ V, float* __restrict__ Fs,
@@ -439,8 +440,8 @@ __global__ void __launch_bounds__(kTB) k_extend(MeshView m, GridArgs G, const fl
             int i = (int)(r / G.ny);
             int j = (int)(r - (long long)i * G.ny);
             float3 p = make_float3((float)(i * G.dx), (float)(j * G.dx), (float)(k * G.dx));
-            int f = nearest_face(m, L, p, r_near * r_near, &err);
-            if (f < 0) f = nearest_face(m, L, p, 1.0e12f, &err);
+            int f = nearest_prim<CENTROID>(m, L, p, r_near * r_near, &err);
+            if (f < 0) f = nearest_prim<CENTROID>(m, L, p, 1.0e12f, &err);
             if (f >= 0) out = V[f];
         }
         if (pinned) out = -1.0f;
@@ -631,11 +632,10 @@ extern "C" int petch_trace_legacy(const void* mesh, int max_tris, int max_verts,
                         "k_trace<legacy>");
 }
 
-extern "C" int petch_extend_velocity(const void* mesh, int max_tris, int max_verts,
-                                     const float* phi, const uint8_t* mask, int nx, int ny, int nz,
-                                     double dx, double band, const float* V, float* Fs, int fold_mask,
-                                     int* active, int* n_active, int max_active, int* work,
-                                     void* stream) {
+static int extend_velocity(const void* mesh, int max_tris, int max_verts, const float* phi,
+                           const uint8_t* mask, int nx, int ny, int nz, double dx, double band,
+                           const float* V, float* Fs, int fold_mask, int* active, int* n_active,
+                           int max_active, int* work, void* stream, bool centroid) {
     PETCH_REQUIRE(mesh && phi && V && Fs && work, "petch_extend_velocity: null pointer");
     PETCH_REQUIRE(nx > 0 && ny > 0 && nz > 0 && dx > 0, "petch_extend_velocity: bad grid");
     PETCH_REQUIRE(!fold_mask || !active || n_active, "petch_extend_velocity: n_active is null");
@@ -643,10 +643,34 @@ extern "C" int petch_extend_velocity(const void* mesh, int max_tris, int max_ver
     MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
     GridArgs G{nx, ny, nz, (long long)ny * nz, (long long)nx * ny * nz, dx, band};
     if (fold_mask && active) PETCH_CUDA(cudaMemsetAsync(n_active, 0, sizeof(int), st), "memset n_active");
-    k_extend<<<grid_for(G.n, kTB, 16), kTB, 0, st>>>(m, G, phi, mask, V, Fs, fold_mask, active,
-                                                     n_active, max_active, work);
+    if (centroid) {
+        k_extend<true><<<grid_for(G.n, kTB, 16), kTB, 0, st>>>(m, G, phi, mask, V, Fs, fold_mask,
+                                                               active, n_active, max_active, work);
+    } else {
+        k_extend<false><<<grid_for(G.n, kTB, 16), kTB, 0, st>>>(m, G, phi, mask, V, Fs, fold_mask,
+                                                                active, n_active, max_active, work);
+    }
     PETCH_LAUNCH_CHECK("k_extend");
     return PETCH_OK;
+}
+
+extern "C" int petch_extend_velocity(const void* mesh, int max_tris, int max_verts,
+                                     const float* phi, const uint8_t* mask, int nx, int ny, int nz,
+                                     double dx, double band, const float* V, float* Fs, int fold_mask,
+                                     int* active, int* n_active, int max_active, int* work,
+                                     void* stream) {
+    return extend_velocity(mesh, max_tris, max_verts, phi, mask, nx, ny, nz, dx, band, V, Fs,
+                           fold_mask, active, n_active, max_active, work, stream, false);
+}
+
+extern "C" int petch_extend_velocity_centroid(const void* mesh, int max_tris, int max_verts,
+                                              const float* phi, const uint8_t* mask, int nx,
+                                              int ny, int nz, double dx, double band,
+                                              const float* V, float* Fs, int fold_mask,
+                                              int* active, int* n_active, int max_active,
+                                              int* work, void* stream) {
+    return extend_velocity(mesh, max_tris, max_verts, phi, mask, nx, ny, nz, dx, band, V, Fs,
+                           fold_mask, active, n_active, max_active, work, stream, true);
 }
 
 extern "C" int petch_warmstart(const void* prev_mesh, int prev_max_tris, int prev_max_verts,

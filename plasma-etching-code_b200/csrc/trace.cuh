@@ -497,7 +497,11 @@ __device__ __forceinline__ float box_d2(float3 p, float lx, float hx, float ly, 
 }
 
 // Nearest face to p within sqrt(r2max); ties go to the lower face index.  Returns -1 if none.
-__device__ __forceinline__ int nearest_face(const MeshView& m, int L, float3 p, float r2max,
+// Nearest face to p within sqrt(r2max): by distance to the triangle (CENTROID false, the
+// mesh_query_point contract) or to the face centroid (CENTROID true, a KD-tree over centroids);
+// exact ties go to the lower face index.  Node boxes bound the triangles, hence their centroids.
+template <bool CENTROID>
+__device__ __forceinline__ int nearest_prim(const MeshView& m, int L, float3 p, float r2max,
                                             int* err) {
     int best = -1;
     float bd = r2max;
@@ -530,7 +534,14 @@ __device__ __forceinline__ int nearest_face(const MeshView& m, int L, float3 p, 
             int l = ~node;
             int f0 = __ldg(m.leaf_start + l), f1 = __ldg(m.leaf_start + l + 1);
             for (int f = f0; f < f1; ++f) {
-                float d2 = point_tri_d2(p, tri_v(m.tri, f, 0), tri_v(m.tri, f, 1), tri_v(m.tri, f, 2));
+                float d2;
+                if (CENTROID) {
+                    float3 c = make_float3(__ldg(m.centroid + 3 * f), __ldg(m.centroid + 3 * f + 1),
+                                           __ldg(m.centroid + 3 * f + 2));
+                    d2 = dot3(p - c, p - c);
+                } else {
+                    d2 = point_tri_d2(p, tri_v(m.tri, f, 0), tri_v(m.tri, f, 1), tri_v(m.tri, f, 2));
+                }
                 if (d2 < bd || (d2 == bd && (best < 0 || f < best))) {
                     bd = d2;
                     best = f;
@@ -542,6 +553,11 @@ __device__ __forceinline__ int nearest_face(const MeshView& m, int L, float3 p, 
     }
     *err |= 1;
     return best;
+}
+
+__device__ __forceinline__ int nearest_face(const MeshView& m, int L, float3 p, float r2max,
+                                            int* err) {
+    return nearest_prim<false>(m, L, p, r2max, err);
 }
 
 }  // namespace petch

@@ -78,3 +78,35 @@ def advect_3d_gpu(phi, Fspeed, mask, mask_phi, dx, dt, nsub):
     m = _dev(mask, torch.uint8)
     out = advect_dev(p, _dev(Fspeed), m, _dev(mask_phi), dx, dt, nsub)
     return out.double().cpu().numpy() if host else out
+
+
+def reinit_pde_dev(phi, dx, n_iter=24, out=None, scratch=None, stream=None):
+    """reinit_gpu on a CUDA float32 grid (threed.py:1399-1418): n_iter Russo-Smereka PDE sweeps."""
+    nx, ny, nz = phi.shape
+    if out is None:
+        out = torch.empty_like(phi)
+    if scratch is None:
+        scratch = (torch.empty_like(phi), torch.empty_like(phi))
+    _lib.call("petch_reinit_pde", _lib.ptr(phi), _lib.ptr(out), _lib.ptr(scratch[0]),
+              _lib.ptr(scratch[1]), nx, ny, nz, float(dx), int(n_iter), _lib.stream_ptr(stream))
+    return out
+
+
+def gaussian_smooth_dev(phi, sigma, mask=None, mask_phi=None, truncate=4.0, scratch=None,
+                        stream=None):
+    """In place: scipy.ndimage.gaussian_filter(phi, sigma) then phi[mask] = mask_phi[mask]
+    (run_etch_3d's surf_smooth, threed.py:1779-1782) on a CUDA float32 grid."""
+    nx, ny, nz = phi.shape
+    if scratch is None:
+        scratch = (torch.empty_like(phi), torch.empty_like(phi))
+    _lib.call("petch_gaussian_smooth", _lib.ptr(phi), _lib.ptr(scratch[0]), _lib.ptr(scratch[1]),
+              _lib.ptr(mask), _lib.ptr(mask_phi), nx, ny, nz, float(sigma), float(truncate),
+              _lib.stream_ptr(stream))
+    return phi
+
+
+def reinit_gpu(phi_np, dx, n_iter=24):
+    """Drop-in for threed.reinit_gpu (numpy in -> float64 numpy out; tensors stay on the device)."""
+    host = not isinstance(phi_np, torch.Tensor)
+    out = reinit_pde_dev(_dev(phi_np), dx, n_iter)
+    return out.double().cpu().numpy() if host else out

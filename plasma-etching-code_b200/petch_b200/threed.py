@@ -24,7 +24,8 @@ import torch
 
 from . import _lib
 from .chemistry import _yields
-from .levelset import grid_shape, reinit_fsm_dev, seed_field
+from .levelset import (gaussian_smooth_dev, grid_shape, reinit_fsm_dev, reinit_pde_dev,
+                       seed_field)
 from .params import DEFAULT_FLAGS, PAR
 
 SEGMENTS = ("hdr", "vnode", "verts", "faces", "tri", "area", "normal", "centroid", "fmask", "nbr",
@@ -460,7 +461,9 @@ class EtchEngine(FluxEngine):
     def build_mesh(self):
         self.mesh.build(self.phi, self.dx, self.geo, self.scratch)
 
-    def rate_and_extend(self, band):
+    def rate_and_extend(self, band, centroid=False):
+        """surface_rate, then the velocity extension into the band: nearest face
+        (extend_velocity_gpu) or nearest centroid (extend_velocity_3d, centroid=True)."""
         m = self.mesh
         s = _sp()
         y = self.yields
@@ -469,7 +472,8 @@ class EtchEngine(FluxEngine):
                   self.m_i.data_ptr(), self.m_F.data_ptr(), self.m_O.data_ptr(),
                   self.cos_i.data_ptr(), y[0], y[1], y[2], self.V.data_ptr(), stats.data_ptr(), s)
         nx, ny, nz = self.shape
-        _lib.call("petch_extend_velocity", m.id, m.MT, m.MV, self.phi.data_ptr(),
+        fn = "petch_extend_velocity_centroid" if centroid else "petch_extend_velocity"
+        _lib.call(fn, m.id, m.MT, m.MV, self.phi.data_ptr(),
                   self.mask.data_ptr(), nx, ny, nz, self.dx, float(band), self.V.data_ptr(),
                   self.F.data_ptr(), 1, self.active.data_ptr(), self.small[8:9].data_ptr(),
                   self.ncell, self.small[0:6].data_ptr(), s)
@@ -494,8 +498,14 @@ class EtchEngine(FluxEngine):
                   int(self.mask_idx.numel()), self.active.data_ptr(), int(n_active), nx, ny, nz,
                   float(1.0 / self.dx), float(dt_sub), int(nsub), _sp())
 
-    def reinit(self, band_r):
-        reinit_fsm_dev(self.phi, self.dx, band_r, out=self.phi, scratch=(self.ua, self.ub))
+    def reinit(self, band_r, method="fsm"):
+        if method == "gpu":
+            reinit_pde_dev(self.phi, self.dx, out=self.phi, scratch=(self.ua, self.ub))
+        else:
+            reinit_fsm_dev(self.phi, self.dx, band_r, out=self.phi, scratch=(self.ua, self.ub))
+
+    def smooth(self, sigma):
+        gaussian_smooth_dev(self.phi, sigma, self.mask, self.mask_phi, scratch=(self.ua, self.ub))
 
     def end_step(self, warm):
         """Keep this step's mesh + coverage for the next step's warm start."""
@@ -539,8 +549,11 @@ def run_etch_3d(Lx=10.0, Ly=4.0, Lz=14.0, dx=0.4, trench_width=4.0, mask_th=2.0,
     `geo` dict (numpy phi / mask, `timings` per stage from CUDA events, optional depth_history /
     frames).
 
-    reinit_method: every method runs the Jacobi Godunov-Eikonal reinit ('fsm'); the reference's
-    skfmm / PDE variants are CPU or legacy paths.  extend must be 'gpu' (nearest face).
+    reinit_method: 'gpu' runs the Russo-Smereka PDE reinit (reinit_gpu); every other method runs
+    the Jacobi Godunov-Eikonal reinit ('fsm'; the reference's skfmm variants are CPU paths).
+    extend: 'gpu' takes V of the nearest face (extend_velocity_gpu), anything else V of the
+    nearest centroid (extend_velocity_3d).  surf_smooth > 0 applies the Gaussian smoothing and
+    mask re-pin after each reinit.
     Extensions: phi_init (host or device initial level set, replacing the seed field; the mask
     and mask_phi still come from the geometry), max_tris (initial face capacity, grown on
     demand), hooks (dict of callables: before_step(step, eng), after_step(step, eng, status))."""
@@ -549,10 +562,6 @@ def run_etch_3d(Lx=10.0, Ly=4.0, Lz=14.0, dx=0.4, trench_width=4.0, mask_th=2.0,
     if flags is None:
         flags = DEFAULT_FLAGS
     _unsupported(flags, par)
-    if extend != "gpu":
-        raise NotImplementedError("only the nearest-face ('gpu') velocity extension is provided")
-    if surf_smooth and surf_smooth > 0.0:
-        raise NotImplementedError("surf_smooth is not implemented")
     nt = getattr(flags, "neutral_transport", "mc")
     hooks = hooks or {}
     mc_par = par
@@ -603,7 +612,7 @@ def run_etch_3d(Lx=10.0, Ly=4.0, Lz=14.0, dx=0.4, trench_width=4.0, mask_th=2.0,
             eng.par = par
         st_timer.stop("flux")
         st_timer.start("extend")
-        eng.rate_and_extend(band)
+        eng.rate_and_extend(band, centroid=extend != "gpu")
         st_timer.stop("extend")
         st = eng.sync_status()
         if st['mesh_err'] & (MESH_ERR_TRI_OVERFLOW | MESH_ERR_VERT_OVERFLOW | MESH_ERR_HASH_FULL):
@@ -628,8 +637,10 @@ def run_etch_3d(Lx=10.0, Ly=4.0, Lz=14.0, dx=0.4, trench_width=4.0, mask_th=2.0,
         st_timer.stop("advect")
         if (step + 1) % reinit_every == 0 or step == n_steps - 1:
             st_timer.start("reinit")
-            eng.reinit(band + 2.0 * dx)
+            eng.reinit(band + 2.0 * dx, "gpu" if reinit_method == "gpu" else "fsm")
             st_timer.stop("reinit")
+        if surf_smooth and surf_smooth > 0.0:
+            eng.smooth(float(surf_smooth))
         eng.end_step(warm and coupled and nt != "radiosity")
         st['nsub'] = nsub
         if record_depth_every and (step % record_depth_every == 0 or step == n_steps - 1):

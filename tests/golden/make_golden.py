@@ -4,7 +4,7 @@ warp-lang replaced by warp_shim.py (a CPU stand-in: see its docstring for what i
 
 Run in a checkout that has the reference at /root/reference (or $PETCH_REFERENCE):
 
-    python tests/golden/make_golden.py [group ...]   # groups: levelset surface flux radiosity
+    python tests/golden/make_golden.py [group ...]   # groups: levelset surface flux radiosity options
 
 The fixtures are committed; tests read only the .npz files, never the reference.
 """
@@ -320,7 +320,37 @@ def radiosity():
     np.savez_compressed(os.path.join(HERE, "radiosity.npz"), **out)
 
 
-GROUPS = {"levelset": levelset, "surface": surface, "flux": flux, "radiosity": radiosity}
+def options():
+    """run_etch_3d's non-default level-set options on the reference's own functions: the PDE
+    reinit (reinit_gpu, reinit_method='gpu') and the nearest-centroid extension
+    (extend_velocity_3d, extend != 'gpu')."""
+    out = {}
+    rng = np.random.default_rng(99)
+    for name, nx, ny, nz, dx, Lx, Ly, sub_top, mask_th, width, hole in (
+            ("hole", 12, 12, 16, 0.25, 3.0, 3.0, 2.5, 0.75, 1.5, True),
+            ("trench", 14, 6, 16, 0.15, 2.1, 0.9, 1.5, 0.3, 0.9, False)):
+        phi_a, _ = _csg(nx, ny, nz, dx, Lx, Ly, sub_top, mask_th, width, hole)
+        phi_a = (phi_a + rng.normal(0.0, 0.02 * dx, phi_a.shape)).astype(np.float32)
+        out[f"{name}_pde_in"] = phi_a
+        out[f"{name}_pde_dx"] = np.array([dx])
+        t0 = time.time()
+        out[f"{name}_pde_out"] = t3.reinit_gpu(phi_a.astype(np.float64), dx)
+        print(f"  reinit_gpu {name}: {time.time() - t0:.1f}s", flush=True)
+    m, geo, phi = _small_mesh(True)
+    v64 = m.verts.astype(np.float32).astype(np.float64)[m.faces]
+    centroids = v64.mean(axis=1)
+    V = rng.uniform(0.0, 2.0, len(m.faces))
+    band = 4 * geo['dx']
+    g = dict(geo, phi=phi.astype(np.float64))
+    out["ext_phi"], out["ext_centroids"], out["ext_V"] = phi, centroids, V
+    out["ext_verts"], out["ext_faces"] = m.verts.astype(np.float32), m.faces
+    out["ext_args"] = np.array([geo['dx'], band])
+    out["ext_Fs"] = t3.extend_velocity_3d(V, centroids, g, band)
+    np.savez_compressed(os.path.join(HERE, "options.npz"), **out)
+
+
+GROUPS = {"levelset": levelset, "surface": surface, "flux": flux, "radiosity": radiosity,
+          "options": options}
 
 if __name__ == "__main__":
     for g in (sys.argv[1:] or list(GROUPS)):
