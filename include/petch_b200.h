@@ -285,6 +285,30 @@ int petch_gaussian_smooth(float* phi, float* tmp_a, float* tmp_b, const uint8_t*
                           const float* mask_phi, int nx, int ny, int nz, double sigma,
                           double truncate, void* stream);
 
+/* ---- etch-product redeposition (mc_redep_3d, petch/threed.py:1582-1605) ---- */
+
+/* CUB scratch bytes petch_trace_redep needs for max_tris faces. */
+int petch_redep_scratch_bytes(int max_tris, long long* bytes);
+
+/* Replaces mc_redep_3d's emission and trace (petch/threed.py:1590-1604): n product particles,
+ * each leaving face j with probability w_j / sum(w), w = max(V * area, 0) (cdf: double[max_tris]
+ * receives the inclusive prefix of w), from centroid + 1e-3 fn in a cosine direction about fn
+ * (petch_gas_normals), traced like _trace3d_cov_rr with bare = 1 and beta = s_redep and no
+ * lateral wrap; flux (float[max_tris], zeroed first) = deposited weight per face.  Philox stream
+ * keyed by (seed, particle).  No particles are traced when sum(w) <= 0.  work: as
+ * petch_trace_ions. */
+int petch_trace_redep(const void* mesh, int max_tris, int max_verts, const petch_domain* dom,
+                      const float* fn, const float* V, float s_redep, uint32_t seed, int n,
+                      float* flux, double* cdf, void* scratch, long long scratch_bytes, int* work,
+                      void* stream);
+
+/* Replaces mc_redep_3d's normalisation and run_etch_3d's use of it (petch/threed.py:1605, 1743):
+ * Rf = flux * (sum(w) / n) / area (written to Rf if not NULL), V = max(V - k_redep * Rf, 0), and,
+ * if stats is not NULL, stats[1] = float bits of the new max(V) (as petch_surface_rate). */
+int petch_redep_apply(const void* mesh, int max_tris, int max_verts, const float* flux,
+                      const double* cdf, int n, float k_redep, float* V, float* Rf, int* stats,
+                      void* stream);
+
 /* ---- deterministic radiosity neutrals (mc_flux_3d_radiosity, petch/threed.py:923-991) ---- */
 
 /* Replaces _gas_normals (petch/threed.py:1553-1568): fn (float[3 * max_tris]) = the face's unit

@@ -15,6 +15,7 @@ Reference lines followed (paths within the reference project):
   reinit_gpu           petch/threed.py:1349-1418   Russo-Smereka PDE sweeps
   surf_smooth          petch/threed.py:1779-1782   the same scipy gaussian_filter call
   mc_flux_3d_radiosity petch/threed.py:923-1029    _gas_normals :1553-1568, _cosine_dirs :1571-1579
+  mc_redep_3d          petch/threed.py:1582-1605   wired as run_etch_3d :1730-1743
   _depth3d / max_depth_3d petch/threed.py:1798-1869
 Parity pinning: level-set stages and the per-face arithmetic against tests/golden/*.npz made by
 running the reference's own code (tests/golden/make_golden.py); Monte-Carlo stages statistically
@@ -55,6 +56,7 @@ _SIGS = {
     "orc_trace_neutrals": ([_P, _P, _P, _D, _U64, _U64, _I, _P], None),
     "orc_trace_legacy": ([_P, _P, _I, _D, _D, _I, _I, _D, _D, _U64, _I, _P, _P], None),
     "orc_trace_ff": ([_P, _P, _P, _P, _I, _I, _U64, _P], None),
+    "orc_trace_redep": ([_P, _P, _P, _P, _I, _D, _U64, _I, _P], None),
 }
 
 
@@ -519,6 +521,23 @@ def extend_nearest_centroid(V, centroids, phi, dx, band):
     return Fs
 
 
+# ------------------------------- redeposition -------------------------------
+def redep(mesh, fn, src_flux, n_redep, s_redep, seed):
+    """mc_redep_3d (threed.py:1582-1605): redeposited flux density per face."""
+    F = mesh.F
+    if F == 0:
+        return np.zeros(0)
+    w = np.maximum(np.asarray(src_flux, np.float64) * mesh.area, 0.0)
+    tot = float(w.sum())
+    if tot <= 0.0:
+        return np.zeros(F)
+    cdf = np.cumsum(w)
+    fl = np.zeros(F)
+    lib().orc_trace_redep(mesh.h, _p(_f64(fn)), _p(_f64(mesh.centroid)), _p(cdf), F,
+                          float(s_redep), int(seed) & (2**64 - 1), int(n_redep), _p(fl))
+    return (fl * (tot / n_redep)) / np.maximum(mesh.area, 1e-9)
+
+
 # ------------------------------- radiosity neutrals -------------------------------
 def gas_normals(verts, faces, centroids, phi, dx):
     """_gas_normals (threed.py:1553-1568): float32 winding normals of the float32 vertices,
@@ -691,6 +710,10 @@ def run_etch_3d(Lx, Ly, Lz, dx, trench_width, mask_th, sub_top, t_end, n_steps, 
                          getattr(flags, "chemistry", "langmuir"),
                          getattr(flags, "yield_angular", "cosine"), iy)
         V = np.nan_to_num(V, nan=0.0, posinf=0.0, neginf=0.0).astype(np.float32).astype(np.float64)
+        if getattr(flags, "redeposition", False):
+            fn = gas_normals(mesh.verts, mesh.faces, mesh.centroid, phi, dx)
+            Rf = redep(mesh, fn, V, n_neu, par.get('s_redep', 0.5), step)
+            V = np.maximum(V - par.get('k_redep', 1.0) * Rf, 0.0)
         st['flux_rate'] = time.time() - ta
         ta = time.time()
         bandm = np.abs(phi.astype(np.float64)) < band

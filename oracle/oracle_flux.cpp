@@ -5,6 +5,7 @@
 //   faithful ion          : _trace3d_ion_yield     petch/threed.py:599-712
 //   legacy species        : _trace3d               petch/threed.py:352-406
 //   form-factor rays      : _trace_ff + emission   petch/threed.py:908-920, 947-956, 1571-1579
+//   redeposition          : mc_redep_3d            petch/threed.py:1582-1605
 // The random stream is this file's own (SplitMix64 counter hash per (seed, domain, ray)), not the
 // device's Philox and not Warp's: these are oracles of the same estimator, checked statistically.
 // Parity pin: tests/golden/flux.npz holds per-face means of the reference's own kernels (executed
@@ -346,6 +347,49 @@ void orc_trace_ff(void* mesh, const double* dom, const double* fn, const double*
         cosine_emit(g, fn + 3 * j, d);
         orc::HitD h = query(m, o, d, D);
         hit[p] = h.f;
+    }
+}
+
+// mc_redep_3d's emission + trace: particle p leaves face j with probability cdf-weighted
+// (cdf: inclusive prefix of w = max(V * area, 0), double[F]) from centroid_j + 1e-3 fn_j in a
+// cosine direction about fn_j, then moves like _trace3d_cov_rr with bare = 1, beta = s_redep and
+// no lateral wrap.  flux: double[F] deposited weight (caller zeroes).
+void orc_trace_redep(void* mesh, const double* fn, const double* centroid, const double* cdf,
+                     int F, double s_redep, uint64_t seed, int n, double* flux) {
+    const Mesh* m = (const Mesh*)mesh;
+    if (F <= 0 || !(cdf[F - 1] > 0.0)) return;
+    Dom D{1.0, 1.0, 1.0, 0.0, 0};
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int p = 0; p < n; ++p) {
+        Rng g(seed, 0x72656470ULL, (uint64_t)p);
+        const double target = g.uniform() * cdf[F - 1];
+        int lo = 0, hi = F - 1;
+        while (lo < hi) {
+            int mid = (lo + hi) / 2;
+            if (cdf[mid] > target) hi = mid;
+            else lo = mid + 1;
+        }
+        const int j = lo;
+        double o[3], d[3];
+        for (int q = 0; q < 3; ++q) o[q] = centroid[3 * j + q] + 1e-3 * fn[3 * j + q];
+        cosine_emit(g, fn + 3 * j, d);
+        double w = 1.0;
+        for (int bounce = 0; bounce < 1024; ++bounce) {
+            orc::HitD h = query(m, o, d, D);
+            if (h.f < 0) break;
+            double nr[3];
+            oriented_normal(m, h.f, d, nr);
+            add(flux, h.f, w);
+            w = w - w * s_redep;
+            if (w <= 1e-6) break;
+            if (w < 0.1) {
+                if (g.uniform() < (1.0 - w / 0.3)) break;
+                w = 0.3;
+            }
+            double hit[3] = {o[0] + h.t * d[0], o[1] + h.t * d[1], o[2] + h.t * d[2]};
+            cosine_emit(g, nr, d);
+            for (int q = 0; q < 3; ++q) o[q] = hit[q] + 1e-4 * nr[q];
+        }
     }
 }
 

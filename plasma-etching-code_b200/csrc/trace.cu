@@ -6,6 +6,7 @@
 // the long bounce tails of the Russian-roulette and reflected-ion paths instead of idling behind
 // their longest ray.  Sources are generated in-kernel from the ray's Philox stream; there are no
 // origin/direction arrays.
+#include <cub/cub.cuh>
 #include "common.cuh"
 #include "mesh.cuh"
 #include "trace.cuh"
@@ -323,6 +324,71 @@ struct FormFactorShader {
     }
 };
 
+// mc_redep_3d (threed.py:1582-1605): etch product leaves face j with probability
+// w_j / sum(w), w = max(V * area, 0) (cdf: inclusive float64 prefix of w), from centroid + 1e-3 n_gas
+// in a cosine direction about the into-gas normal, then moves like a Russian-roulette neutral
+// that sticks with probability s_redep everywhere (bare = 1, beta = s_redep).
+struct RedepShader {
+    NeutralShader rr;
+    const double* cdf;
+    const float* fn;
+    static constexpr int kMaxBounce = NeutralShader::kMaxBounce;
+    __device__ __forceinline__ int count(const MeshView& m, int n) const {
+        const int F = min(m.hdr[HDR_F], m.MT);
+        return (F > 0 && cdf[F - 1] > 0.0) ? n : 0;
+    }
+    __device__ __forceinline__ void init(Rng& g, const Tracer& T, const Domain&, int, float3& o,
+                                         float3& d, RayState& s) const {
+        const int F = min(T.m.hdr[HDR_F], T.m.MT);
+        const uint32_t a = g.next_u32() >> 5, b = g.next_u32() >> 6;   // 27 + 26 bits
+        const double u = ((double)a * 67108864.0 + (double)b) * (1.0 / 9007199254740992.0);
+        const double target = u * cdf[F - 1];
+        int lo = 0, hi = F - 1;                  // first j with cdf[j] > target
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (cdf[mid] > target) hi = mid;
+            else lo = mid + 1;
+        }
+        const int j = lo;
+        const float3 n = make_float3(__ldg(fn + 3 * j), __ldg(fn + 3 * j + 1), __ldg(fn + 3 * j + 2));
+        const float3 c = make_float3(__ldg(T.m.centroid + 3 * j), __ldg(T.m.centroid + 3 * j + 1),
+                                     __ldg(T.m.centroid + 3 * j + 2));
+        o = c + 1.0e-3f * n;
+        d = cosine_emit(g, n);
+        s.w = 1.0f;
+    }
+    __device__ __forceinline__ bool hit(Rng& g, const Tracer& T, int f, float t, float3& o,
+                                        float3& d, RayState& s) const {
+        return rr.hit(g, T, f, t, o, d, s);
+    }
+};
+
+// w_j = max(V_j * area_j, 0) in float64 (the CDF's input); scanned in place afterwards.
+__global__ void k_redep_weights(MeshView m, const float* __restrict__ V, double* __restrict__ w) {
+    const int F = min(m.hdr[HDR_F], m.MT);
+    for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < m.MT; f += gridDim.x * blockDim.x)
+        w[f] = f < F ? fmax((double)V[f] * (double)m.area[f], 0.0) : 0.0;
+}
+
+// Rf = flux * (sum(w) / n) / area; V = max(V - k_redep * Rf, 0); stats[1] = bits of max V.
+__global__ void k_redep_apply(MeshView m, const float* __restrict__ flux,
+                              const double* __restrict__ cdf, int n, float k_redep,
+                              float* __restrict__ V, float* __restrict__ Rf, int* stats) {
+    const int F = min(m.hdr[HDR_F], m.MT);
+    const double tot = F > 0 ? cdf[F - 1] : 0.0;
+    float vmax = 0.0f;
+    for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < F; f += gridDim.x * blockDim.x) {
+        float r = 0.0f;
+        if (tot > 0.0 && n > 0) r = (float)((double)flux[f] * (tot / n) / (double)m.area[f]);
+        if (Rf) Rf[f] = r;
+        const float v = fmaxf(V[f] - k_redep * r, 0.0f);
+        V[f] = v;
+        vmax = fmaxf(vmax, v);
+    }
+    for (int o = 16; o > 0; o >>= 1) vmax = fmaxf(vmax, __shfl_xor_sync(kFull, vmax, o));
+    if ((threadIdx.x & 31) == 0 && stats) atomicMax(stats + 1, __float_as_int(vmax));
+}
+
 // Persistent tracer.  Each warp loops: refill lanes whose ray ended (one atomic per warp), run
 // traversal steps on every lane with an open query (up to `steps`, and only while more than
 // `keep` lanes still have one), then resolve the lanes whose query finished -- a miss wraps laterally (periodic domains, <= 256 wraps per bounce, then one
@@ -609,6 +675,55 @@ extern "C" int petch_trace_ff(const void* mesh, int max_tris, int max_verts,
     PETCH_CUDA(cudaMemsetAsync(work, 0, sizeof(int), st), "reset ray counter");
     return launch_trace(m, to_domain(dom), sh, seed, 0x66666600u, max_tris * n_ff, work, st,
                         "k_trace<form factors>");
+}
+
+extern "C" int petch_redep_scratch_bytes(int max_tris, long long* bytes) {
+    PETCH_REQUIRE(bytes && max_tris > 0, "petch_redep_scratch_bytes: bad argument");
+    size_t b = 0;
+    PETCH_CUDA(cub::DeviceScan::InclusiveSum(nullptr, b, (double*)nullptr, (double*)nullptr,
+                                             max_tris),
+               "petch_redep_scratch_bytes: scan size query");
+    *bytes = (long long)b;
+    return PETCH_OK;
+}
+
+extern "C" int petch_trace_redep(const void* mesh, int max_tris, int max_verts,
+                                 const petch_domain* dom, const float* fn, const float* V,
+                                 float s_redep, uint32_t seed, int n, float* flux, double* cdf,
+                                 void* scratch, long long scratch_bytes, int* work, void* stream) {
+    PETCH_REQUIRE(mesh && dom && fn && V && flux && cdf && scratch && work,
+                  "petch_trace_redep: null pointer");
+    PETCH_REQUIRE(n >= 0 && max_tris > 0 && max_verts > 0, "petch_trace_redep: bad size");
+    cudaStream_t st = as_stream(stream);
+    MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
+    k_redep_weights<<<grid_for(max_tris, 256), 256, 0, st>>>(m, V, cdf);
+    PETCH_LAUNCH_CHECK("k_redep_weights");
+    size_t b = (size_t)scratch_bytes;
+    PETCH_CUDA(cub::DeviceScan::InclusiveSum(scratch, b, cdf, cdf, max_tris, st), "redep cdf scan");
+    k_zero_faces<<<grid_for(max_tris, 256), 256, 0, st>>>(m.hdr, max_tris, flux, 1, nullptr, 0);
+    PETCH_LAUNCH_CHECK("k_zero_faces");
+    PETCH_CUDA(cudaMemsetAsync(work, 0, sizeof(int), st), "reset ray counter");
+    if (n == 0) return PETCH_OK;
+    RedepShader sh;
+    sh.rr = NeutralShader{nullptr, s_redep, flux};
+    sh.cdf = cdf;
+    sh.fn = fn;
+    Domain D = to_domain(dom);
+    D.periodic = 0;                      // mc_redep_3d traces without the lateral wrap
+    return launch_trace(m, D, sh, seed, 0x72656470u, n, work, st, "k_trace<redeposition>");
+}
+
+extern "C" int petch_redep_apply(const void* mesh, int max_tris, int max_verts, const float* flux,
+                                 const double* cdf, int n, float k_redep, float* V, float* Rf,
+                                 int* stats, void* stream) {
+    PETCH_REQUIRE(mesh && flux && cdf && V, "petch_redep_apply: null pointer");
+    PETCH_REQUIRE(n >= 0 && max_tris > 0, "petch_redep_apply: bad size");
+    cudaStream_t st = as_stream(stream);
+    MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
+    if (stats) PETCH_CUDA(cudaMemsetAsync(stats + 1, 0, sizeof(int), st), "reset max V");
+    k_redep_apply<<<grid_for(max_tris, 256), 256, 0, st>>>(m, flux, cdf, n, k_redep, V, Rf, stats);
+    PETCH_LAUNCH_CHECK("k_redep_apply");
+    return PETCH_OK;
 }
 
 extern "C" int petch_trace_legacy(const void* mesh, int max_tris, int max_verts,

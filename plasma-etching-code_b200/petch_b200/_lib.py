@@ -79,6 +79,9 @@ SIGNATURES = {
     "petch_extend_velocity_centroid": [P, I, I, P, P, I, I, I, D, D, P, P, I, P, P, I, P, P],
     "petch_reinit_pde": [P, P, P, P, I, I, I, D, I, P],
     "petch_gaussian_smooth": [P, P, P, P, P, I, I, I, D, D, P],
+    "petch_redep_scratch_bytes": [I, LLP],
+    "petch_trace_redep": [P, I, I, DP, P, P, F, U, I, P, P, P, L, P, P],
+    "petch_redep_apply": [P, I, I, P, P, I, F, P, P, P, P],
 }
 
 # The library's tracer configuration at load (bvh_width, steps_per_round, keep_lanes): what

@@ -200,8 +200,6 @@ def _unsupported(flags, par):
         raise NotImplementedError(f"neutral_transport={nt!r} is outside this engine's scope")
     if getattr(flags, "surface_charging", False) or getattr(flags, "floor_charge_throttle", False):
         raise NotImplementedError("surface charging models are outside this engine's scope")
-    if getattr(flags, "redeposition", False):
-        raise NotImplementedError("redeposition is not implemented yet")
     if par.get('cov_transport', 'rr') != 'rr':
         raise NotImplementedError("only the Russian-roulette coverage transport (cov_transport='rr')")
     if par.get('charge_alpha', 0.0) > 0.0 and getattr(flags, "surface_charging", False):
@@ -461,9 +459,10 @@ class EtchEngine(FluxEngine):
     def build_mesh(self):
         self.mesh.build(self.phi, self.dx, self.geo, self.scratch)
 
-    def rate_and_extend(self, band, centroid=False):
-        """surface_rate, then the velocity extension into the band: nearest face
-        (extend_velocity_gpu) or nearest centroid (extend_velocity_3d, centroid=True)."""
+    def rate_and_extend(self, band, centroid=False, redep=None):
+        """surface_rate, the optional redeposition correction (redep = (n particles, seed)), then
+        the velocity extension into the band: nearest face (extend_velocity_gpu) or nearest
+        centroid (extend_velocity_3d, centroid=True)."""
         m = self.mesh
         s = _sp()
         y = self.yields
@@ -471,12 +470,41 @@ class EtchEngine(FluxEngine):
         _lib.call("petch_surface_rate", m.id, m.MT, m.MV, ctypes.byref(self.chem),
                   self.m_i.data_ptr(), self.m_F.data_ptr(), self.m_O.data_ptr(),
                   self.cos_i.data_ptr(), y[0], y[1], y[2], self.V.data_ptr(), stats.data_ptr(), s)
+        if redep is not None:
+            self.redeposition(*redep)
         nx, ny, nz = self.shape
         fn = "petch_extend_velocity_centroid" if centroid else "petch_extend_velocity"
         _lib.call(fn, m.id, m.MT, m.MV, self.phi.data_ptr(),
                   self.mask.data_ptr(), nx, ny, nz, self.dx, float(band), self.V.data_ptr(),
                   self.F.data_ptr(), 1, self.active.data_ptr(), self.small[8:9].data_ptr(),
                   self.ncell, self.small[0:6].data_ptr(), s)
+
+    def redeposition(self, n, seed):
+        """mc_redep_3d + run_etch_3d's V = max(V - k_redep * Rf, 0) (threed.py:1582-1605,
+        1730-1743), with the into-gas normals of the current level set."""
+        m, par = self.mesh, self.par
+        s = _sp()
+        if getattr(self, "redep", None) is None or self.redep['MT'] != self.MT:
+            nb = ctypes.c_longlong()
+            _lib.call("petch_redep_scratch_bytes", self.MT, ctypes.byref(nb))
+            self.redep = dict(MT=self.MT, fn=torch.empty((self.MT, 3), device="cuda"),
+                              cdf=torch.empty(self.MT, dtype=torch.float64, device="cuda"),
+                              Rf=torch.empty(self.MT, device="cuda"),
+                              scratch=torch.empty(max(int(nb.value), 1), dtype=torch.uint8,
+                                                  device="cuda"))
+        r = self.redep
+        nx, ny, nz = self.shape
+        _lib.call("petch_gas_normals", m.id, m.MT, m.MV, self.phi.data_ptr(), nx, ny, nz, self.dx,
+                  r['fn'].data_ptr(), s)
+        self.ktimer.start("k_redep")
+        _lib.call("petch_trace_redep", m.id, m.MT, m.MV, ctypes.byref(self.dom), r['fn'].data_ptr(),
+                  self.V.data_ptr(), float(par.get('s_redep', 0.5)), int(seed) & 0xffffffff,
+                  int(n), self.flux.data_ptr(), r['cdf'].data_ptr(), r['scratch'].data_ptr(),
+                  r['scratch'].numel(), self.small[0:6].data_ptr(), s)
+        self.ktimer.stop("k_redep")
+        _lib.call("petch_redep_apply", m.id, m.MT, m.MV, self.flux.data_ptr(), r['cdf'].data_ptr(),
+                  int(n), float(par.get('k_redep', 1.0)), self.V.data_ptr(), r['Rf'].data_ptr(),
+                  self.small[6:8].data_ptr(), s)
 
     def sync_status(self):
         """The step's single device->host read: mesh counts/errors + rate stats + band size."""
@@ -584,6 +612,7 @@ def run_etch_3d(Lx=10.0, Ly=4.0, Lz=14.0, dx=0.4, trench_width=4.0, mask_th=2.0,
                    nsub_max=0)
     warm = getattr(flags, "warm_start_coverage", False)
     coupled = getattr(flags, "coverage_sticking", False)
+    redepo = getattr(flags, "redeposition", False)
     eng = EtchEngine(geo, par, flags, max_tris=max_tris)
     st_timer = EventTimer()
     step = 0
@@ -612,7 +641,8 @@ def run_etch_3d(Lx=10.0, Ly=4.0, Lz=14.0, dx=0.4, trench_width=4.0, mask_th=2.0,
             eng.par = par
         st_timer.stop("flux")
         st_timer.start("extend")
-        eng.rate_and_extend(band, centroid=extend != "gpu")
+        eng.rate_and_extend(band, centroid=extend != "gpu",
+                            redep=(n_neu, step) if redepo else None)
         st_timer.stop("extend")
         st = eng.sync_status()
         if st['mesh_err'] & (MESH_ERR_TRI_OVERFLOW | MESH_ERR_VERT_OVERFLOW | MESH_ERR_HASH_FULL):

@@ -4,7 +4,7 @@ warp-lang replaced by warp_shim.py (a CPU stand-in: see its docstring for what i
 
 Run in a checkout that has the reference at /root/reference (or $PETCH_REFERENCE):
 
-    python tests/golden/make_golden.py [group ...]   # groups: levelset surface flux radiosity options
+    python tests/golden/make_golden.py [group ...]   # groups: levelset surface flux radiosity options redep
 
 The fixtures are committed; tests read only the .npz files, never the reference.
 """
@@ -349,8 +349,46 @@ def options():
     np.savez_compressed(os.path.join(HERE, "options.npz"), **out)
 
 
+def redep():
+    """mc_redep_3d (threed.py:1582-1605) run unmodified on small meshes: per-face means and
+    standard errors of the redeposited flux density over 8 seeds, for a random source rate with
+    some non-etching faces."""
+    out = {}
+    wp = t3.wp
+    rng = np.random.default_rng(21)
+    for key, hole in (("hole", True), ("trench", False)):
+        m, geo, phi = _small_mesh(hole, nx=10, ny=10, nz=14, dx=0.3)
+        verts = m.verts.astype(np.float32)
+        faces = m.faces
+        v64 = verts.astype(np.float64)[faces]
+        centroids = v64.mean(axis=1)
+        areas = 0.5 * np.linalg.norm(np.cross(v64[:, 1] - v64[:, 0], v64[:, 2] - v64[:, 0]),
+                                     axis=1)
+        geo = dict(geo, phi=phi.astype(np.float64))
+        fn = t3._gas_normals(verts, faces, centroids, geo)
+        mesh = wp.Mesh(points=wp.array(verts, dtype=wp.vec3),
+                       indices=wp.array(faces.flatten(), dtype=wp.int32))
+        V = rng.uniform(0.0, 2.0, len(faces))
+        V[rng.random(len(faces)) < 0.3] = 0.0
+        out[f"{key}_verts"], out[f"{key}_faces"], out[f"{key}_phi"] = verts, faces, phi
+        out[f"{key}_V"], out[f"{key}_gas_normals"] = V, fn
+        out[f"{key}_geo"] = np.array([geo['Lx'], geo['Ly'], geo['Lz'], geo['dx']])
+        n = 4000
+
+        def run(sd):
+            t0 = time.time()
+            r = t3.mc_redep_3d(mesh, centroids, areas, fn, V, n_redep=n, s_redep=0.5, seed=sd)
+            print(f"  {key} seed {sd}: {time.time() - t0:.1f}s", flush=True)
+            return r
+
+        mean, se = _mean_se(run, range(100, 108))
+        out[f"{key}_mean"], out[f"{key}_se"] = mean, se
+        out[f"{key}_n"] = np.array([n])
+    np.savez_compressed(os.path.join(HERE, "redep.npz"), **out)
+
+
 GROUPS = {"levelset": levelset, "surface": surface, "flux": flux, "radiosity": radiosity,
-          "options": options}
+          "options": options, "redep": redep}
 
 if __name__ == "__main__":
     for g in (sys.argv[1:] or list(GROUPS)):
