@@ -141,7 +141,7 @@ typedef struct petch_ion_params {  /* the float32 arguments of _trace3d_ion_yiel
 } petch_ion_params;
 
 /* Tracer configuration for this process (the autotuner's knobs): bvh_width 2 (binary LBVH,
- * default) or 8 (quantised 8-wide BVH); each warp runs traversal steps for all its lanes with an
+ * default) or 8 (quantised 8-wide BVH, built only by mesh builds made while it is configured); each warp runs traversal steps for all its lanes with an
  * open query, at most steps_per_round (default 64) and only while more than keep_lanes lanes
  * (0..31, default 12) still have one, between shading / refill rounds; once the ray pool is empty
  * a warp steps until its last query ends.  Applies to later trace / raycast calls. */
@@ -152,7 +152,8 @@ int petch_tracer_config(int bvh_width, int steps_per_round, int keep_lanes);
  * face (sputter, ion-enhanced, passivation, arrival) and ang the cos-weighted arrival; both are
  * zeroed first.  work: int[6] device words, 8-byte aligned: [0] ray counter (reset by every trace
  * call), [1] error bits OR-ed by every kernel (1 = traversal bound hit, 2 = active list full,
- * 4 = tracer round bound hit)
+ * 4 = tracer round bound hit, 8 = BVH width 8 configured but the mesh was built without the
+ * 8-wide tree)
  * until the caller clears them, [2..3] uint64 BVH queries and [4..5] uint64 node + leaf visits,
  * accumulated by every trace call until the caller clears them. */
 int petch_trace_ions(const void* mesh, int max_tris, int max_verts, const petch_domain* dom,
@@ -284,6 +285,74 @@ int petch_reinit_pde(const float* phi_in, float* phi_out, float* phi0, float* tm
 int petch_gaussian_smooth(float* phi, float* tmp_a, float* tmp_b, const uint8_t* mask,
                           const float* mask_phi, int nx, int ny, int nz, double sigma,
                           double truncate, void* stream);
+
+/* ---- batched tracing (many independent instances in one launch) ---- */
+
+/* Caches the host-side device queries the launchers use (SM count, resident blocks of the
+ * persistent tracers) for the current device, so that calls made while a stream is being
+ * captured into a CUDA graph issue no driver queries.  Call once per device before capturing. */
+int petch_prepare_device(void);
+
+/* One instance of a batched trace: its mesh buffer (laid out by petch_mesh_layout with the
+ * batch's max_tris / max_verts), domain, ion parameters (kind 0), coverage (kind 1; NULL = 1),
+ * outputs and ray count.  out: kind 0 the tally4 of petch_trace_ions (float4[max_tris], 16-byte
+ * aligned), kind 1 the flux of petch_trace_neutrals (float[max_tris]); ang: kind 0 only. */
+typedef struct petch_batch_item {
+    const void* mesh;
+    petch_domain dom;
+    petch_ion_params ion;
+    const float* bare;
+    float* out;
+    float* ang;
+    int n_rays;
+    uint32_t seed;       /* added to *step before the seed multiplier */
+} petch_batch_item;
+
+/* No single reference counterpart: runs petch_trace_ions (kind 0) or petch_trace_neutrals
+ * (kind 1, coverage-weighted with beta) for up to 64 instances in ONE persistent launch with one
+ * global ray queue, zeroing each instance's outputs first.  Ray r of instance b uses the Philox
+ * stream of ray r in the single-instance call with seed (*step + items[b].seed) * seed_mul +
+ * seed_add (step: device int, NULL = 0), so the result equals the per-instance calls up to the
+ * order of float atomic additions.  The seed is read on the device: the call can be captured in
+ * a CUDA graph and replayed step after step.  items: host array (copied into the launch).
+ * work: as petch_trace_ions, shared by the batch. */
+int petch_trace_batch(int kind, const petch_batch_item* items, int B, int max_tris, int max_verts,
+                      float beta, const int* step, uint32_t seed_mul, uint32_t seed_add,
+                      int* work, void* stream);
+
+/* One instance's level-set state for the batched stages. */
+typedef struct petch_batch_grid {
+    float* phi;              /* level set (in / out) */
+    float* tmp;              /* advection ping-pong grid */
+    float* ua;               /* reinit scratch grids */
+    float* ub;
+    const float* F;          /* extended speed, -1 on mask cells (petch_extend_velocity fold_mask) */
+    const float* mask_phi;
+    const int* mask_idx;     /* the mask cells (F == -1) */
+    int n_mask;
+    const int* active;       /* band cells with F > 0 and their count (petch_extend_velocity) */
+    const int* n_active;
+    int max_active;
+    int nx, ny, nz;
+    double dx;
+    double dt;               /* the etch step, t_end / n_steps */
+    const int* stats;        /* petch_surface_rate's stats: [1] = float bits of max V */
+    const int* hdr;          /* the mesh header: [0] = face count */
+    int* sub;                /* out, int[2]: [0] substeps, [1] float bits of dt / nsub */
+} petch_batch_grid;
+
+/* Replaces, for B <= 64 instances at once, run_etch_3d's CFL substep count and advect_3d_gpu
+ * (petch/threed.py:1750-1764, 1262-1307) as petch_advect_sparse does them: nsub from stats and
+ * hdr on the device, then a fixed sequence of 160 substep launches in which instance b steps
+ * while s < nsub_b.  Results equal per-instance petch_advect_sparse calls.  Graph-capturable. */
+int petch_batch_advect(const petch_batch_grid* grids, int B, void* stream);
+
+/* Replaces, for B <= 64 instances with the same dx, reinit_fsm (petch/threed.py:1515-1537) as
+ * petch_reinit_eik mode 0 with band = band_r, in place on each phi.  Graph-capturable. */
+int petch_batch_reinit(const petch_batch_grid* grids, int B, double band_r, void* stream);
+
+/* *step += 1 on the device (the step counter petch_trace_batch seeds from). */
+int petch_batch_step_advance(int* step, void* stream);
 
 /* ---- etch-product redeposition (mc_redep_3d, petch/threed.py:1582-1605) ---- */
 

@@ -7,6 +7,7 @@
 // reinit loops (three or four grids) stays resident in the 126 MB L2 for grids up to ~8M cells,
 // so the repeated sweeps inside one etch step mostly run at L2 rather than HBM bandwidth.
 #include "common.cuh"
+#include "levelset.cuh"
 
 namespace {
 
@@ -109,101 +110,28 @@ __global__ void __launch_bounds__(kBlock) k_advect(const float* __restrict__ phi
     }
 }
 
-// Godunov solution of |grad U| = 1 from the three upwind neighbour minima (threed.py:1421-1452):
-// sort ascending, then take the 1-, 2- or 3-term root while it stays below the next neighbour.
-__device__ __forceinline__ float eik_solve(float a1, float a2, float a3, float dx) {
-    float t;
-    if (a1 > a2) { t = a1; a1 = a2; a2 = t; }
-    if (a2 > a3) { t = a2; a2 = a3; a3 = t; }
-    if (a1 > a2) { t = a1; a1 = a2; a2 = t; }
-    float x = a1 + dx;
-    if (x <= a2) return x;
-    float d2 = 2.0f * dx * dx - (a1 - a2) * (a1 - a2);
-    d2 = fmaxf(d2, 0.0f);
-    x = 0.5f * (a1 + a2 + sqrtf(d2));
-    if (x <= a3) return x;
-    float s1 = a1 + a2 + a3;
-    float s2 = a1 * a1 + a2 * a2 + a3 * a3;
-    float d3 = s1 * s1 - 3.0f * (s2 - dx * dx);
-    d3 = fmaxf(d3, 0.0f);
-    return (s1 + sqrtf(d3)) / 3.0f;
-}
-
-// Frozen cells carry their distance with the sign bit set (U >= 0 everywhere else).
-__device__ __forceinline__ bool frozen(float u) { return signbit(u); }
-
-// _eik_init (threed.py:1455-1479): interface cells (a face neighbour, index-clamped, of opposite
-// sign) get the sub-cell distance min(|phi0| / max(|grad phi0|, 0.5), 1.8 dx) and are frozen.
-// SEED (the skfmm.distance stand-in used for the initial field): nodes where phi0 is exactly 0
-// lie on the front and are frozen at distance 0, as fast marching treats them.
 template <bool SEED>
 __global__ void __launch_bounds__(kBlock) k_eik_init(const float* __restrict__ phi0,
                                                      float* __restrict__ U, Grid g, float inv_dx,
                                                      float big) {
+    const petch::LGrid lg = petch::make_lgrid(g.nx, g.ny, g.nz);
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.n;
-         c += (long long)gridDim.x * blockDim.x) {
-        int i, j, k;
-        split(g, c, i, j, k);
-        float v = phi0[c];
-        float oxm = phi0[i >= 1 ? c - g.plane : c];
-        float oxp = phi0[i <= g.nx - 2 ? c + g.plane : c];
-        float oym = phi0[j >= 1 ? c - g.nz : c];
-        float oyp = phi0[j <= g.ny - 2 ? c + g.nz : c];
-        float ozm = phi0[k >= 1 ? c - 1 : c];
-        float ozp = phi0[k <= g.nz - 2 ? c + 1 : c];
-        bool iface = (v * oxm < 0.0f) || (v * oxp < 0.0f) || (v * oym < 0.0f) ||
-                     (v * oyp < 0.0f) || (v * ozm < 0.0f) || (v * ozp < 0.0f);
-        if (SEED && v == 0.0f) {
-            U[c] = -0.0f;
-        } else if (iface) {
-            float gx = (oxp - oxm) * 0.5f * inv_dx;
-            float gy = (oyp - oym) * 0.5f * inv_dx;
-            float gz = (ozp - ozm) * 0.5f * inv_dx;
-            float grad0 = fmaxf(sqrtf(gx * gx + gy * gy + gz * gz), 0.5f);
-            float dxl = 1.0f / inv_dx;
-            float D = fminf(fabsf(v) / grad0, 1.8f * dxl);
-            U[c] = copysignf(D, -1.0f);
-        } else {
-            U[c] = big;
-        }
-    }
+         c += (long long)gridDim.x * blockDim.x)
+        U[c] = petch::eik_init_cell<SEED>(phi0, c, lg, inv_dx, big);
 }
 
-// _eik_jacobi (threed.py:1482-1512); FINAL additionally writes sign(phi_in) * min(U, cap)
-// (reinit_fsm's finalisation, threed.py:1535-1537) instead of U.
 template <bool FINAL, bool SEED>
 __global__ void __launch_bounds__(kBlock) k_eik_sweep(const float* __restrict__ Uin,
                                                       float* __restrict__ Uout,
                                                       const float* __restrict__ phi_in,
                                                       float* __restrict__ phi_out, Grid g,
                                                       float dx, float big, float cap) {
+    const petch::LGrid lg = petch::make_lgrid(g.nx, g.ny, g.nz);
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.n;
          c += (long long)gridDim.x * blockDim.x) {
-        float u = Uin[c];
-        float un;
-        if (frozen(u)) {
-            un = FINAL ? fabsf(u) : u;
-        } else {
-            int i, j, k;
-            split(g, c, i, j, k);
-            float um = (i >= 1) ? fabsf(Uin[c - g.plane]) : big;
-            float up = (i <= g.nx - 2) ? fabsf(Uin[c + g.plane]) : big;
-            float ax = fminf(um, up);
-            um = (j >= 1) ? fabsf(Uin[c - g.nz]) : big;
-            up = (j <= g.ny - 2) ? fabsf(Uin[c + g.nz]) : big;
-            float ay = fminf(um, up);
-            um = (k >= 1) ? fabsf(Uin[c - 1]) : big;
-            up = (k <= g.nz - 2) ? fabsf(Uin[c + 1]) : big;
-            float az = fminf(um, up);
-            un = fminf(u, eik_solve(ax, ay, az, dx));
-        }
-        if (FINAL) {
-            float s = phi_in[c];
-            float sg = s < 0.0f ? -1.0f : (SEED && s == 0.0f ? 0.0f : 1.0f);
-            phi_out[c] = sg * fminf(un, cap) + 0.0f;
-        } else {
-            Uout[c] = un;
-        }
+        const float v = petch::eik_sweep_cell<FINAL, SEED>(Uin, c, lg, dx, big, cap, phi_in);
+        if (FINAL) phi_out[c] = v;
+        else Uout[c] = v;
     }
 }
 

@@ -1,0 +1,143 @@
+// Per-cell level-set updates shared by the single-grid kernels (levelset.cu, surface.cu) and
+// the batched kernels (batch.cu), so that every path computes bit-identical values.
+#pragma once
+#include <cstdint>
+
+namespace petch {
+
+struct LGrid {
+    int nx, ny, nz;
+    long long plane;  // ny * nz
+    long long n;      // nx * ny * nz
+};
+
+__host__ __device__ inline LGrid make_lgrid(int nx, int ny, int nz) {
+    LGrid g;
+    g.nx = nx;
+    g.ny = ny;
+    g.nz = nz;
+    g.plane = (long long)ny * nz;
+    g.n = g.plane * nx;
+    return g;
+}
+
+__device__ __forceinline__ void lsplit(const LGrid& g, long long c, int& i, int& j, int& k) {
+    long long r = c / g.nz;
+    k = (int)(c - r * g.nz);
+    i = (int)(r / g.ny);
+    j = (int)(r - (long long)i * g.ny);
+}
+
+// One first-order Godunov upwind substep of cell c with speed f (threed.py:1262-1292): a zero
+// one-sided difference at the domain faces.
+__device__ __forceinline__ float advect_cell(const float* __restrict__ phi, long long c,
+                                             const LGrid& g, float inv_dx, float f, float dt) {
+    int i, j, k;
+    lsplit(g, c, i, j, k);
+    const float v = phi[c];
+    float dm, dp, t, s;
+    float gg = 0.0f;
+    dm = (i >= 1) ? (v - phi[c - g.plane]) * inv_dx : 0.0f;
+    dp = (i <= g.nx - 2) ? (phi[c + g.plane] - v) * inv_dx : 0.0f;
+    t = fmaxf(dm, 0.0f);
+    s = fminf(dp, 0.0f);
+    gg += t * t + s * s;
+    dm = (j >= 1) ? (v - phi[c - g.nz]) * inv_dx : 0.0f;
+    dp = (j <= g.ny - 2) ? (phi[c + g.nz] - v) * inv_dx : 0.0f;
+    t = fmaxf(dm, 0.0f);
+    s = fminf(dp, 0.0f);
+    gg += t * t + s * s;
+    dm = (k >= 1) ? (v - phi[c - 1]) * inv_dx : 0.0f;
+    dp = (k <= g.nz - 2) ? (phi[c + 1] - v) * inv_dx : 0.0f;
+    t = fmaxf(dm, 0.0f);
+    s = fminf(dp, 0.0f);
+    gg += t * t + s * s;
+    return v - dt * f * sqrtf(gg);
+}
+
+// Godunov solution of |grad U| = 1 from the three upwind neighbour minima (threed.py:1421-1452):
+// sort ascending, then take the 1-, 2- or 3-term root while it stays below the next neighbour.
+__device__ __forceinline__ float eik_solve(float a1, float a2, float a3, float dx) {
+    float t;
+    if (a1 > a2) { t = a1; a1 = a2; a2 = t; }
+    if (a2 > a3) { t = a2; a2 = a3; a3 = t; }
+    if (a1 > a2) { t = a1; a1 = a2; a2 = t; }
+    float x = a1 + dx;
+    if (x <= a2) return x;
+    float d2 = 2.0f * dx * dx - (a1 - a2) * (a1 - a2);
+    d2 = fmaxf(d2, 0.0f);
+    x = 0.5f * (a1 + a2 + sqrtf(d2));
+    if (x <= a3) return x;
+    float s1 = a1 + a2 + a3;
+    float s2 = a1 * a1 + a2 * a2 + a3 * a3;
+    float d3 = s1 * s1 - 3.0f * (s2 - dx * dx);
+    d3 = fmaxf(d3, 0.0f);
+    return (s1 + sqrtf(d3)) / 3.0f;
+}
+
+// Frozen cells carry their distance with the sign bit set (U >= 0 everywhere else).
+__device__ __forceinline__ bool frozen(float u) { return signbit(u); }
+
+// _eik_init (threed.py:1455-1479) for cell c: interface cells (a face neighbour, index-clamped,
+// of opposite sign) get the sub-cell distance min(|phi0| / max(|grad phi0|, 0.5), 1.8 dx),
+// frozen; others `big`.  SEED: nodes where phi0 is exactly 0 are frozen at distance 0.
+template <bool SEED>
+__device__ __forceinline__ float eik_init_cell(const float* __restrict__ phi0, long long c,
+                                               const LGrid& g, float inv_dx, float big) {
+    int i, j, k;
+    lsplit(g, c, i, j, k);
+    float v = phi0[c];
+    float oxm = phi0[i >= 1 ? c - g.plane : c];
+    float oxp = phi0[i <= g.nx - 2 ? c + g.plane : c];
+    float oym = phi0[j >= 1 ? c - g.nz : c];
+    float oyp = phi0[j <= g.ny - 2 ? c + g.nz : c];
+    float ozm = phi0[k >= 1 ? c - 1 : c];
+    float ozp = phi0[k <= g.nz - 2 ? c + 1 : c];
+    bool iface = (v * oxm < 0.0f) || (v * oxp < 0.0f) || (v * oym < 0.0f) ||
+                 (v * oyp < 0.0f) || (v * ozm < 0.0f) || (v * ozp < 0.0f);
+    if (SEED && v == 0.0f) return -0.0f;
+    if (iface) {
+        float gx = (oxp - oxm) * 0.5f * inv_dx;
+        float gy = (oyp - oym) * 0.5f * inv_dx;
+        float gz = (ozp - ozm) * 0.5f * inv_dx;
+        float grad0 = fmaxf(sqrtf(gx * gx + gy * gy + gz * gz), 0.5f);
+        float dxl = 1.0f / inv_dx;
+        float D = fminf(fabsf(v) / grad0, 1.8f * dxl);
+        return copysignf(D, -1.0f);
+    }
+    return big;
+}
+
+// One Jacobi sweep of _eik_jacobi (threed.py:1482-1512) for cell c; FINAL returns
+// sign(phi_in) * min(U, cap) (reinit_fsm's finalisation, threed.py:1535-1537) instead of U.
+template <bool FINAL, bool SEED>
+__device__ __forceinline__ float eik_sweep_cell(const float* __restrict__ Uin, long long c,
+                                                const LGrid& g, float dx, float big, float cap,
+                                                const float* __restrict__ phi_in) {
+    float u = Uin[c];
+    float un;
+    if (frozen(u)) {
+        un = FINAL ? fabsf(u) : u;
+    } else {
+        int i, j, k;
+        lsplit(g, c, i, j, k);
+        float um = (i >= 1) ? fabsf(Uin[c - g.plane]) : big;
+        float up = (i <= g.nx - 2) ? fabsf(Uin[c + g.plane]) : big;
+        float ax = fminf(um, up);
+        um = (j >= 1) ? fabsf(Uin[c - g.nz]) : big;
+        up = (j <= g.ny - 2) ? fabsf(Uin[c + g.nz]) : big;
+        float ay = fminf(um, up);
+        um = (k >= 1) ? fabsf(Uin[c - 1]) : big;
+        up = (k <= g.nz - 2) ? fabsf(Uin[c + 1]) : big;
+        float az = fminf(um, up);
+        un = fminf(u, eik_solve(ax, ay, az, dx));
+    }
+    if (FINAL) {
+        float s = phi_in[c];
+        float sg = s < 0.0f ? -1.0f : (SEED && s == 0.0f ? 0.0f : 1.0f);
+        return sg * fminf(un, cap) + 0.0f;
+    }
+    return un;
+}
+
+}  // namespace petch

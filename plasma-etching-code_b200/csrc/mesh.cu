@@ -845,6 +845,12 @@ extern "C" int petch_mesh_build(const float* phi, int nx, int ny, int nz, double
     PETCH_LAUNCH_CHECK("k_bvh_internal");
     k_bvh_refit<<<fb, kB, 0, st>>>(m);
     PETCH_LAUNCH_CHECK("k_bvh_refit");
+    if (!wide_bvh_enabled()) {
+        // no 8-wide tree: WN = 0 and WLEVELS = -1 mark it absent for the wide traversal
+        PETCH_CUDA(cudaMemsetAsync(m.hdr + HDR_WN, 0, sizeof(int), st), "memset wide count");
+        PETCH_CUDA(cudaMemsetAsync(m.hdr + HDR_WLEVELS, 0xff, sizeof(int), st), "memset wide levels");
+        return PETCH_OK;
+    }
     k_wide_init<<<1, 1, 0, st>>>(m);
     PETCH_LAUNCH_CHECK("k_wide_init");
     int wb = grid_for(max_tris / 4 + 1, 128);

@@ -94,4 +94,7 @@ struct MeshView {
 
 MeshView mesh_view(void* base, int max_tris, int max_verts);
 
+// Whether mesh builds add the 8-wide BVH (the tracer configuration's BVH width is 8).
+bool wide_bvh_enabled();
+
 }  // namespace petch

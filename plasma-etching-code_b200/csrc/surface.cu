@@ -9,6 +9,7 @@
 //     (threed.py:1723-1728) and the CFL maximum (threed.py:1750).
 // Chemistry runs in float64 like the reference's numpy host code; flux arrays are float32.
 #include "common.cuh"
+#include "levelset.cuh"
 #include "mesh.cuh"
 
 namespace petch {
@@ -231,30 +232,10 @@ __global__ void __launch_bounds__(kSB) k_advect_list(const float* __restrict__ p
                                                      const float* __restrict__ F,
                                                      const int* __restrict__ idx, int n, AGrid g,
                                                      float inv_dx, float dt) {
+    const LGrid lg = make_lgrid(g.nx, g.ny, g.nz);
     for (int s = blockIdx.x * kSB + threadIdx.x; s < n; s += gridDim.x * kSB) {
         long long c = idx[s];
-        long long r = c / g.nz;
-        int k = (int)(c - r * g.nz);
-        int i = (int)(r / g.ny);
-        int j = (int)(r - (long long)i * g.ny);
-        float v = phi[c];
-        float dm, dp, t, q, gg = 0.0f;
-        dm = (i >= 1) ? (v - phi[c - g.plane]) * inv_dx : 0.0f;
-        dp = (i <= g.nx - 2) ? (phi[c + g.plane] - v) * inv_dx : 0.0f;
-        t = fmaxf(dm, 0.0f);
-        q = fminf(dp, 0.0f);
-        gg += t * t + q * q;
-        dm = (j >= 1) ? (v - phi[c - g.nz]) * inv_dx : 0.0f;
-        dp = (j <= g.ny - 2) ? (phi[c + g.nz] - v) * inv_dx : 0.0f;
-        t = fmaxf(dm, 0.0f);
-        q = fminf(dp, 0.0f);
-        gg += t * t + q * q;
-        dm = (k >= 1) ? (v - phi[c - 1]) * inv_dx : 0.0f;
-        dp = (k <= g.nz - 2) ? (phi[c + 1] - v) * inv_dx : 0.0f;
-        t = fmaxf(dm, 0.0f);
-        q = fminf(dp, 0.0f);
-        gg += t * t + q * q;
-        out[c] = v - dt * F[c] * sqrtf(gg);
+        out[c] = advect_cell(phi, c, lg, inv_dx, F[c], dt);
     }
 }
 

@@ -7,6 +7,9 @@
 // their longest ray.  Sources are generated in-kernel from the ray's Philox stream; there are no
 // origin/direction arrays.
 #include <cub/cub.cuh>
+#include <map>
+#include <mutex>
+#include <utility>
 #include "common.cuh"
 #include "mesh.cuh"
 #include "trace.cuh"
@@ -26,6 +29,12 @@ constexpr unsigned kFull = 0xffffffffu;
 int g_bvh_width = 2;
 int g_steps = 64;
 int g_keep = 12;
+
+}  // namespace
+
+bool wide_bvh_enabled() { return g_bvh_width == 8; }
+
+namespace {
 
 struct Domain {
     float lx, ly, lz, z_src;
@@ -134,6 +143,25 @@ struct RayState {
 // _trace3d_cov_rr (threed.py:549-596): deposit the weight on every hit, W *= 1 - bare * beta,
 // stop at W <= 1e-6, Russian roulette below 0.1 (survive with probability W / 0.3 at weight
 // 0.3), cosine re-emission; at most 1024 bounces.
+__device__ __forceinline__ bool neutral_hit(const float* bare, float beta, float* flux, Rng& g,
+                                            const Tracer& T, int f, float t, float3& o, float3& d,
+                                            RayState& s) {
+    float3 nrm = stored_normal(T.m, f);
+    if (dot3(nrm, d) > 0.0f) nrm = -nrm;
+    atomicAdd(flux + f, s.w);
+    float S = (bare ? __ldg(bare + f) : 1.0f) * beta;
+    s.w = s.w - s.w * S;
+    if (s.w <= 1.0e-6f) return false;
+    if (s.w < 0.1f) {
+        if (g.uniform() < (1.0f - s.w / 0.3f)) return false;
+        s.w = 0.3f;
+    }
+    float3 h = o + t * d;
+    d = cosine_emit(g, nrm);
+    o = h + 1.0e-4f * nrm;
+    return true;
+}
+
 struct NeutralShader {
     const float* bare;
     float beta;
@@ -147,20 +175,7 @@ struct NeutralShader {
     }
     __device__ __forceinline__ bool hit(Rng& g, const Tracer& T, int f, float t, float3& o,
                                         float3& d, RayState& s) const {
-        float3 nrm = stored_normal(T.m, f);
-        if (dot3(nrm, d) > 0.0f) nrm = -nrm;
-        atomicAdd(flux + f, s.w);
-        float S = (bare ? __ldg(bare + f) : 1.0f) * beta;
-        s.w = s.w - s.w * S;
-        if (s.w <= 1.0e-6f) return false;
-        if (s.w < 0.1f) {
-            if (g.uniform() < (1.0f - s.w / 0.3f)) return false;
-            s.w = 0.3f;
-        }
-        float3 h = o + t * d;
-        d = cosine_emit(g, nrm);
-        o = h + 1.0e-4f * nrm;
-        return true;
+        return neutral_hit(bare, beta, flux, g, T, f, t, o, d, s);
     }
 };
 
@@ -169,6 +184,73 @@ struct NeutralShader {
 // cos * weight; then angle-dependent sticking, energy loss (<= 4 truncated-normal tries), weight
 // reduction and coned-cosine reflection about the specular axis (<= 64 accept-reject draws);
 // at most 1024 bounces.  tal4[f] = (sp, ie, ip, arr), ang[f] = sum cos * w.
+__device__ __forceinline__ bool ion_hit(const IonP& P, float4* tal4, float* ang, Rng& g,
+                                        const Tracer& T, int f, float t, float3& o, float3& d,
+                                        RayState& s) {
+    const float PI_2 = 1.5707963f;
+    float3 nrm = stored_normal(T.m, f);
+    if (dot3(nrm, d) > 0.0f) nrm = -nrm;
+    float cosT = fminf(fmaxf(-dot3(d, nrm), 0.0f), 1.0f);
+    float incAng = acosf(cosT);
+    float sqrtE = sqrtf(s.E);
+    float f_sp = fmaxf((1.0f + P.B_sp * (1.0f - cosT * cosT)) * cosT, 0.0f);
+    float f_ie = 1.0f;
+    if (cosT < 0.5f) f_ie = fmaxf(3.0f - 6.0f * incAng / 3.14159265f, 0.0f);
+    float w = s.w;
+    atomicAdd(tal4 + f, make_float4(P.A_sp * fmaxf(sqrtE - sqrtf(P.Eth_sp), 0.0f) * f_sp * w,
+                                    P.A_ie * fmaxf(sqrtE - sqrtf(P.Eth_ie), 0.0f) * f_ie * w,
+                                    P.A_p * fmaxf(sqrtE - sqrtf(P.Eth_p), 0.0f) * f_ie * w, w));
+    atomicAdd(ang + f, cosT * w);
+    float stick = 1.0f;
+    if (incAng > P.thrmin) stick = 1.0f - fminf(fmaxf((incAng - P.thrmin) / (P.thrmax - P.thrmin), 0.0f), 1.0f);
+    if (stick >= 1.0f) return false;
+    float Eref = incAng >= P.inflect
+                     ? 1.0f - (1.0f - P.A_en) * (PI_2 - incAng) / (PI_2 - P.inflect)
+                     : P.A_en * powf(incAng / P.inflect, P.n_l);
+    const float E = s.E;
+    float newE = Eref * E;
+    for (int e = 0; e < 4; ++e) {
+        float cand = Eref * E + 0.1f * E * g.normal();
+        if (cand >= 0.0f && cand <= E) {
+            newE = cand;
+            break;
+        }
+    }
+    newE = fminf(fmaxf(newE, 0.0f), E);
+    if (newE <= P.minE) return false;
+    s.E = newE;
+    s.w = w - w * stick;
+    if (s.w <= 1.0e-4f) return false;
+    float3 h = o + t * d;
+    float3 axis = normalize3(d - (2.0f * dot3(d, nrm)) * nrm);
+    float3 tt, bb;
+    if (axis.z < -0.9999999f) {
+        tt = make_float3(0.0f, -1.0f, 0.0f);
+        bb = make_float3(-1.0f, 0.0f, 0.0f);
+    } else {
+        float aa = 1.0f / (1.0f + axis.z);
+        float cc = -axis.x * axis.y * aa;
+        tt = make_float3(1.0f - axis.x * axis.x * aa, cc, -axis.x);
+        bb = make_float3(cc, 1.0f - axis.y * axis.y * aa, -axis.y);
+    }
+    float maxcone = PI_2 - fminf(incAng, P.minang);
+    float theta = 0.0f;
+    for (int q = 0; q < 64; ++q) {
+        float uu = sqrtf(g.uniform());
+        float ss = sqrtf(fmaxf(1.0f - uu, 0.0f));
+        theta = maxcone * ss;
+        if (g.uniform() * theta * uu <= cosf(PI_2 * ss) * sinf(theta)) break;
+    }
+    float ph = 6.2831853f * g.uniform();
+    float st = sinf(theta);
+    float3 nd = normalize3((st * cosf(ph)) * tt + (st * sinf(ph)) * bb + cosf(theta) * axis);
+    float dn = dot3(nd, nrm);
+    if (dn <= 0.0f) nd = nd - (2.0f * dn) * nrm;
+    d = nd;
+    o = h + 1.0e-4f * nrm;
+    return true;
+}
+
 struct IonShader {
     IonP P;
     float4* tal4;
@@ -183,68 +265,7 @@ struct IonShader {
     }
     __device__ __forceinline__ bool hit(Rng& g, const Tracer& T, int f, float t, float3& o,
                                         float3& d, RayState& s) const {
-        const float PI_2 = 1.5707963f;
-        float3 nrm = stored_normal(T.m, f);
-        if (dot3(nrm, d) > 0.0f) nrm = -nrm;
-        float cosT = fminf(fmaxf(-dot3(d, nrm), 0.0f), 1.0f);
-        float incAng = acosf(cosT);
-        float sqrtE = sqrtf(s.E);
-        float f_sp = fmaxf((1.0f + P.B_sp * (1.0f - cosT * cosT)) * cosT, 0.0f);
-        float f_ie = 1.0f;
-        if (cosT < 0.5f) f_ie = fmaxf(3.0f - 6.0f * incAng / 3.14159265f, 0.0f);
-        float w = s.w;
-        atomicAdd(tal4 + f, make_float4(P.A_sp * fmaxf(sqrtE - sqrtf(P.Eth_sp), 0.0f) * f_sp * w,
-                                        P.A_ie * fmaxf(sqrtE - sqrtf(P.Eth_ie), 0.0f) * f_ie * w,
-                                        P.A_p * fmaxf(sqrtE - sqrtf(P.Eth_p), 0.0f) * f_ie * w, w));
-        atomicAdd(ang + f, cosT * w);
-        float stick = 1.0f;
-        if (incAng > P.thrmin) stick = 1.0f - fminf(fmaxf((incAng - P.thrmin) / (P.thrmax - P.thrmin), 0.0f), 1.0f);
-        if (stick >= 1.0f) return false;
-        float Eref = incAng >= P.inflect
-                         ? 1.0f - (1.0f - P.A_en) * (PI_2 - incAng) / (PI_2 - P.inflect)
-                         : P.A_en * powf(incAng / P.inflect, P.n_l);
-        const float E = s.E;
-        float newE = Eref * E;
-        for (int e = 0; e < 4; ++e) {
-            float cand = Eref * E + 0.1f * E * g.normal();
-            if (cand >= 0.0f && cand <= E) {
-                newE = cand;
-                break;
-            }
-        }
-        newE = fminf(fmaxf(newE, 0.0f), E);
-        if (newE <= P.minE) return false;
-        s.E = newE;
-        s.w = w - w * stick;
-        if (s.w <= 1.0e-4f) return false;
-        float3 h = o + t * d;
-        float3 axis = normalize3(d - (2.0f * dot3(d, nrm)) * nrm);
-        float3 tt, bb;
-        if (axis.z < -0.9999999f) {
-            tt = make_float3(0.0f, -1.0f, 0.0f);
-            bb = make_float3(-1.0f, 0.0f, 0.0f);
-        } else {
-            float aa = 1.0f / (1.0f + axis.z);
-            float cc = -axis.x * axis.y * aa;
-            tt = make_float3(1.0f - axis.x * axis.x * aa, cc, -axis.x);
-            bb = make_float3(cc, 1.0f - axis.y * axis.y * aa, -axis.y);
-        }
-        float maxcone = PI_2 - fminf(incAng, P.minang);
-        float theta = 0.0f;
-        for (int q = 0; q < 64; ++q) {
-            float uu = sqrtf(g.uniform());
-            float ss = sqrtf(fmaxf(1.0f - uu, 0.0f));
-            theta = maxcone * ss;
-            if (g.uniform() * theta * uu <= cosf(PI_2 * ss) * sinf(theta)) break;
-        }
-        float ph = 6.2831853f * g.uniform();
-        float st = sinf(theta);
-        float3 nd = normalize3((st * cosf(ph)) * tt + (st * sinf(ph)) * bb + cosf(theta) * axis);
-        float dn = dot3(nd, nrm);
-        if (dn <= 0.0f) nd = nd - (2.0f * dn) * nrm;
-        d = nd;
-        o = h + 1.0e-4f * nrm;
-        return true;
+        return ion_hit(P, tal4, ang, g, T, f, t, o, d, s);
     }
 };
 
@@ -404,6 +425,10 @@ __global__ void __launch_bounds__(kTB, kTraceMinBlocks) k_trace(MeshView m, Doma
     int st_ref[kWStack];
     float st_t[kWStack];
     int err = 0;
+    if (WIDE && T.L > 0 && m.hdr[HDR_WLEVELS] < 0) {   // mesh built without the 8-wide tree
+        err = 8;
+        n = 0;
+    }
     unsigned long long n_query = 0, n_visit = 0;
     int ray = -1, phase = 0;   // phase 1: query open, 2: query finished
     Query q;
@@ -465,6 +490,188 @@ __global__ void __launch_bounds__(kTB, kTraceMinBlocks) k_trace(MeshView m, Doma
     }
     if (err) atomicOr(work + 1, err);
     // work[2..3]: queries started, work[4..5]: node + leaf visits (64-bit, warp-reduced)
+    for (int o = 16; o > 0; o >>= 1) {
+        n_query += __shfl_xor_sync(kFull, n_query, o);
+        n_visit += __shfl_xor_sync(kFull, n_visit, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(reinterpret_cast<unsigned long long*>(work + 2), n_query);
+        atomicAdd(reinterpret_cast<unsigned long long*>(work + 4), n_visit);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Batched tracing: one persistent launch over the rays of up to kMaxBatch independent instances
+// (feature / recipe pairs), each with its own mesh buffer (all laid out for the same capacities),
+// domain, ion parameters and output tallies.  Rays are drawn from ONE global queue; ray r of
+// instance b has the Philox key ((step + seed_b) * seed_mul + seed_add, domain) and counter r,
+// exactly the stream the single-instance launch gives it, so a batched step reproduces the
+// per-instance steps' paths.  The instance table is a kernel parameter copied into shared memory;
+// each lane resolves its ray's instance when it takes the ray.
+// ---------------------------------------------------------------------------------------------
+constexpr int kMaxBatch = 64;
+
+struct BatchItem {
+    const char* mesh;
+    Domain D;
+    IonP P;
+    const float* bare;
+    float* out;
+    float* ang;
+    int ray_start;
+    uint32_t seed;
+};
+
+struct BatchTable {
+    BatchItem it[kMaxBatch];
+    int B;
+    int total;
+};
+
+struct MeshOffsets {
+    long long off[SEG_COUNT];
+};
+
+__device__ __forceinline__ MeshView view_at(const char* base, const MeshOffsets& L, int MT, int MV) {
+    MeshView v;
+    char* b = const_cast<char*>(base);
+    v.hdr = (int*)(b + L.off[SEG_HDR]);
+    v.vnode = (float*)(b + L.off[SEG_VNODE]);
+    v.verts = (float*)(b + L.off[SEG_VERTS]);
+    v.faces = (int*)(b + L.off[SEG_FACES]);
+    v.tri = (float4*)(b + L.off[SEG_TRI]);
+    v.area = (float*)(b + L.off[SEG_AREA]);
+    v.normal = (float*)(b + L.off[SEG_NORMAL]);
+    v.centroid = (float*)(b + L.off[SEG_CENTROID]);
+    v.fmask = (uint8_t*)(b + L.off[SEG_FMASK]);
+    v.nbr = (int*)(b + L.off[SEG_NBR]);
+    v.nbrw = (float*)(b + L.off[SEG_NBRW]);
+    v.leaf_code = (uint32_t*)(b + L.off[SEG_LEAF_CODE]);
+    v.leaf_start = (int*)(b + L.off[SEG_LEAF_START]);
+    v.nodes = (float4*)(b + L.off[SEG_NODES]);
+    v.parent = (int*)(b + L.off[SEG_PARENT]);
+    v.flags = (int*)(b + L.off[SEG_FLAGS]);
+    v.wnodes = (WNode*)(b + L.off[SEG_WNODES]);
+    v.wfront = (int2*)(b + L.off[SEG_WFRONT]);
+    v.MT = MT;
+    v.MV = MV;
+    return v;
+}
+
+// Zero each instance's tallies on its live faces (blockIdx.y = instance).
+__global__ void k_zero_batch(BatchTable tab, MeshOffsets L, int MT, int MV, int per_face) {
+    const int b = blockIdx.y;
+    if (b >= tab.B) return;
+    const BatchItem& it = tab.it[b];
+    const int F = min(((const int*)(it.mesh + L.off[SEG_HDR]))[HDR_F], MT);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < F * per_face; i += gridDim.x * blockDim.x)
+        it.out[i] = 0.0f;
+    if (it.ang)
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < F; i += gridDim.x * blockDim.x)
+            it.ang[i] = 0.0f;
+}
+
+template <bool ION>
+__global__ void __launch_bounds__(kTB, kTraceMinBlocks) k_trace_batch(BatchTable tab, MeshOffsets L,
+                                                                     int MT, int MV, float beta,
+                                                                     const int* step,
+                                                                     uint32_t seed_mul,
+                                                                     uint32_t seed_add,
+                                                                     uint32_t domain, int steps,
+                                                                     int keep, int* work) {
+    __shared__ BatchItem s_it[kMaxBatch];
+    __shared__ int s_start[kMaxBatch + 1];
+    for (int i = threadIdx.x; i < tab.B; i += blockDim.x) {
+        s_it[i] = tab.it[i];
+        s_start[i] = tab.it[i].ray_start;
+    }
+    if (threadIdx.x == 0) s_start[tab.B] = tab.total;
+    __syncthreads();
+    const int n = tab.total;
+    const uint32_t stepv = step ? (uint32_t)*step : 0u;
+    int st_ref[kWStack];
+    float st_t[kWStack];
+    int err = 0;
+    unsigned long long n_query = 0, n_visit = 0;
+    int ray = -1, phase = 0, inst = 0;
+    Query q;
+    RayState rs;
+    Rng g;
+    Tracer T;
+    T.WN = 0;
+    T.nsm = 0;
+    T.snodes = nullptr;
+    T.L = 0;
+    T.m = view_at(s_it[0].mesh, L, MT, MV);
+    bool pool_empty = false;
+    for (long long round = 0;; ++round) {
+        if (round >= kMaxRounds) {
+            err |= 4;
+            break;
+        }
+        if (refill(ray, n, work)) {
+            int lo = 0, hi = tab.B - 1;           // last instance whose range starts at or before ray
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (s_start[mid] <= ray) lo = mid;
+                else hi = mid - 1;
+            }
+            inst = lo;
+            const BatchItem& it = s_it[inst];
+            T.m = view_at(it.mesh, L, MT, MV);
+            T.L = min(T.m.hdr[HDR_L], MT);
+            const uint32_t local = (uint32_t)(ray - it.ray_start);
+            g.init((stepv + it.seed) * seed_mul + seed_add, domain, local);
+            float3 o, d;
+            if (ION) {
+                source(g, true, it.P.sigma, it.D, o, d);
+                rs.E = fmaxf(it.P.meanE + it.P.sigmaE * g.normal(), 0.0f);
+            } else {
+                source(g, false, 0.0f, it.D, o, d);
+            }
+            rs.w = 1.0f;
+            rs.bounce = 0;
+            rs.wraps = 0;
+            rs.id = ray;
+            query_begin(q, T, o, d, 1.0e6f, false);
+            ++n_query;
+            phase = q.cur == kDone ? 2 : 1;
+        }
+        if (__all_sync(kFull, ray == -2)) break;
+        pool_empty = pool_empty || __any_sync(kFull, ray == -2);
+        const int keep_now = pool_empty ? 0 : keep;
+        for (int s = 0; s < steps; ++s) {
+            if (__popc(__ballot_sync(kFull, phase == 1)) <= keep_now) break;
+            if (phase == 1) {
+                if (step_binary(T, q, st_ref, st_t, &err)) phase = 2;
+            }
+        }
+        if (phase == 2) {
+            const BatchItem& it = s_it[inst];
+            float3 o = q.r.o, d = q.r.d;
+            bool cont;
+            if (q.f < 0) {
+                cont = it.D.periodic && rs.wraps < 256 && periodic_wrap(it.D, o, d);
+                if (cont) ++rs.wraps;
+            } else {
+                cont = ION ? ion_hit(it.P, reinterpret_cast<float4*>(it.out), it.ang, g, T, q.f,
+                                     q.t, o, d, rs)
+                           : neutral_hit(it.bare, beta, it.out, g, T, q.f, q.t, o, d, rs);
+                rs.wraps = 0;
+                if (cont && ++rs.bounce >= 1024) cont = false;
+            }
+            n_visit += q.visits;
+            if (cont) {
+                query_begin(q, T, o, d, 1.0e6f, false);
+                ++n_query;
+                phase = q.cur == kDone ? 2 : 1;
+            } else {
+                ray = -1;
+                phase = 0;
+            }
+        }
+    }
+    if (err) atomicOr(work + 1, err);
     for (int o = 16; o > 0; o >>= 1) {
         n_query += __shfl_xor_sync(kFull, n_query, o);
         n_visit += __shfl_xor_sync(kFull, n_visit, o);
@@ -547,10 +754,13 @@ __global__ void __launch_bounds__(kTB) k_raycast(MeshView m, const float* __rest
     int st_ref[kWStack];
     float st_t[kWStack];
     int err = 0;
+    const bool missing = wide && T.L > 0 && m.hdr[HDR_WLEVELS] < 0;   // no 8-wide tree built
+    if (missing) err = 8;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         Query q;
         query_begin(q, T, make_float3(o[3 * i], o[3 * i + 1], o[3 * i + 2]),
                     make_float3(d[3 * i], d[3 * i + 1], d[3 * i + 2]), tmax, wide);
+        if (missing) q.cur = kDone;
         if (q.cur != kDone)
             while (!(wide ? step_wide(T, q, st_ref, st_t, &err) : step_binary(T, q, st_ref, st_t, &err))) {
             }
@@ -572,12 +782,24 @@ __global__ void __launch_bounds__(kTB) k_nearest(MeshView m, const float* __rest
 constexpr int kSmemBytes = kSmemNodes * 96;
 
 
-int persistent_blocks(const void* kernel, int block) {
+// Resident blocks per SM x SMs for a persistent launch, cached per (kernel, device) so that calls
+// made during stream capture issue no driver queries.
+int persistent_blocks(const void* kernel, int block, size_t dyn_smem = kSmemBytes) {
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, int> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(mu);
+    auto key = std::make_pair(kernel, dev);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, kSmemBytes) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, dyn_smem) != cudaSuccess ||
         per_sm < 1)
         per_sm = 1;
-    return per_sm * sm_count();
+    const int blocks = per_sm * sm_count();
+    cache[key] = blocks;
+    return blocks;
 }
 
 }  // namespace
@@ -675,6 +897,72 @@ extern "C" int petch_trace_ff(const void* mesh, int max_tris, int max_verts,
     PETCH_CUDA(cudaMemsetAsync(work, 0, sizeof(int), st), "reset ray counter");
     return launch_trace(m, to_domain(dom), sh, seed, 0x66666600u, max_tris * n_ff, work, st,
                         "k_trace<form factors>");
+}
+
+extern "C" int petch_prepare_device(void) {
+    sm_count();
+    persistent_blocks((const void*)k_trace_batch<true>, kTB, 0);
+    persistent_blocks((const void*)k_trace_batch<false>, kTB, 0);
+    persistent_blocks((const void*)k_trace<IonShader, false>, kTB);
+    persistent_blocks((const void*)k_trace<NeutralShader, false>, kTB);
+    persistent_blocks((const void*)k_trace<LegacyShader, false>, kTB);
+    persistent_blocks((const void*)k_trace<FormFactorShader, false>, kTB);
+    persistent_blocks((const void*)k_trace<RedepShader, false>, kTB);
+    PETCH_CUDA(cudaGetLastError(), "petch_prepare_device");
+    return PETCH_OK;
+}
+
+extern "C" int petch_trace_batch(int kind, const petch_batch_item* items, int B, int max_tris,
+                                 int max_verts, float beta, const int* step, uint32_t seed_mul,
+                                 uint32_t seed_add, int* work, void* stream) {
+    PETCH_REQUIRE(items && work, "petch_trace_batch: null pointer");
+    PETCH_REQUIRE(kind == 0 || kind == 1, "petch_trace_batch: kind must be 0 (ions) or 1 (neutrals)");
+    PETCH_REQUIRE(B >= 1 && B <= kMaxBatch, "petch_trace_batch: 1 <= B <= %d", kMaxBatch);
+    PETCH_REQUIRE(max_tris > 0 && max_verts > 0, "petch_trace_batch: bad capacities");
+    BatchTable tab;
+    long long total = 0;
+    for (int b = 0; b < B; ++b) {
+        const petch_batch_item& x = items[b];
+        PETCH_REQUIRE(x.mesh && x.out && x.n_rays >= 0, "petch_trace_batch: item %d incomplete", b);
+        PETCH_REQUIRE(kind == 1 || (x.ang && ((uintptr_t)x.out & 15) == 0),
+                      "petch_trace_batch: ion item %d needs ang and a 16-byte aligned tally", b);
+        BatchItem& it = tab.it[b];
+        it.mesh = (const char*)x.mesh;
+        it.D = to_domain(&x.dom);
+        const petch_ion_params& p = x.ion;
+        it.P = IonP{p.meanE, p.sigmaE, p.A_sp, p.Eth_sp, p.B_sp, p.A_ie, p.Eth_ie, p.A_p, p.Eth_p,
+                    p.inflect, p.minang, p.n_l, p.A_en, p.minE, p.thrmin, p.thrmax, p.sigma};
+        it.bare = x.bare;
+        it.out = x.out;
+        it.ang = kind == 0 ? x.ang : nullptr;
+        it.ray_start = (int)total;
+        it.seed = x.seed;
+        total += x.n_rays;
+    }
+    PETCH_REQUIRE(total < (1LL << 31), "petch_trace_batch: more than 2^31 - 1 rays");
+    tab.B = B;
+    tab.total = (int)total;
+    MeshOffsets L;
+    const MeshLayout ml = mesh_layout(max_tris, max_verts);
+    for (int i = 0; i < SEG_COUNT; ++i) L.off[i] = ml.off[i];
+    cudaStream_t st = as_stream(stream);
+    dim3 zg(grid_for(4LL * max_tris, 256, 2), B);
+    k_zero_batch<<<zg, 256, 0, st>>>(tab, L, max_tris, max_verts, kind == 0 ? 4 : 1);
+    PETCH_LAUNCH_CHECK("k_zero_batch");
+    PETCH_CUDA(cudaMemsetAsync(work, 0, sizeof(int), st), "reset ray counter");
+    if (total == 0) return PETCH_OK;
+    const uint32_t domain = kind == 0 ? 0x696f6e73u : 0x6e657500u;
+    if (kind == 0) {
+        k_trace_batch<true><<<persistent_blocks((const void*)k_trace_batch<true>, kTB, 0), kTB, 0, st>>>(
+            tab, L, max_tris, max_verts, beta, step, seed_mul, seed_add, domain, g_steps, g_keep,
+            work);
+    } else {
+        k_trace_batch<false><<<persistent_blocks((const void*)k_trace_batch<false>, kTB, 0), kTB, 0, st>>>(
+            tab, L, max_tris, max_verts, beta, step, seed_mul, seed_add, domain, g_steps, g_keep,
+            work);
+    }
+    PETCH_LAUNCH_CHECK("k_trace_batch");
+    return PETCH_OK;
 }
 
 extern "C" int petch_redep_scratch_bytes(int max_tris, long long* bytes) {

@@ -41,6 +41,24 @@ class ChemParams(ctypes.Structure):
                                  "Yp", "B_sp")] + [("yield_angular", I), ("chemistry", I)]
 
 
+class BatchItem(ctypes.Structure):
+    """petch_batch_item."""
+    _fields_ = [("mesh", ctypes.c_void_p), ("dom", Domain), ("ion", IonParams),
+                ("bare", ctypes.c_void_p), ("out", ctypes.c_void_p), ("ang", ctypes.c_void_p),
+                ("n_rays", ctypes.c_int), ("seed", ctypes.c_uint32)]
+
+
+class BatchGrid(ctypes.Structure):
+    """petch_batch_grid."""
+    _fields_ = [("phi", ctypes.c_void_p), ("tmp", ctypes.c_void_p), ("ua", ctypes.c_void_p),
+                ("ub", ctypes.c_void_p), ("F", ctypes.c_void_p), ("mask_phi", ctypes.c_void_p),
+                ("mask_idx", ctypes.c_void_p), ("n_mask", ctypes.c_int),
+                ("active", ctypes.c_void_p), ("n_active", ctypes.c_void_p),
+                ("max_active", ctypes.c_int), ("nx", ctypes.c_int), ("ny", ctypes.c_int),
+                ("nz", ctypes.c_int), ("dx", ctypes.c_double), ("dt", ctypes.c_double),
+                ("stats", ctypes.c_void_p), ("hdr", ctypes.c_void_p), ("sub", ctypes.c_void_p)]
+
+
 DP = ctypes.POINTER(Domain)
 IP = ctypes.POINTER(IonParams)
 CP = ctypes.POINTER(ChemParams)
@@ -82,6 +100,11 @@ SIGNATURES = {
     "petch_redep_scratch_bytes": [I, LLP],
     "petch_trace_redep": [P, I, I, DP, P, P, F, U, I, P, P, P, L, P, P],
     "petch_redep_apply": [P, I, I, P, P, I, F, P, P, P, P],
+    "petch_trace_batch": [I, P, I, I, I, F, P, U, U, P, P],
+    "petch_prepare_device": [],
+    "petch_batch_advect": [P, I, P],
+    "petch_batch_reinit": [P, I, D, P],
+    "petch_batch_step_advance": [P, P],
 }
 
 # The library's tracer configuration at load (bvh_width, steps_per_round, keep_lanes): what

@@ -2,6 +2,7 @@
 (tests/golden/flux.npz, shim-executed) with a chi-square test on the per-face differences, and
 (b) the FP64 oracle at high ray counts with the criterion per-face relative L2 <= 2% (plus the
 measured noise floor).  Different random streams on all three sides: estimator parity."""
+import ctypes
 import os
 
 import numpy as np
@@ -10,7 +11,8 @@ import torch
 
 import oracle.oracle as orc
 from conftest import GOLDEN
-from gpu_helpers import cuda_ions, cuda_legacy, cuda_mesh, cuda_neutrals, small_feature
+from gpu_helpers import (cuda_ions, cuda_legacy, cuda_mesh, cuda_neutrals, domain, small_feature,
+                         stream)
 from petch_b200 import params
 
 pytestmark = pytest.mark.gpu
@@ -116,16 +118,33 @@ def test_tracer_configs_agree(width, steps, keep):
     paths up to float rounding of the traversal order): totals within noise, per-face within
     1 %."""
     phi, geo = small_feature(False)
-    m = cuda_mesh(phi, geo['dx'], geo)
     from petch_b200 import _lib
-    ref = cuda_neutrals(m, geo, None, 0.7, 7, 1_000_000)
     try:
         _lib.call("petch_tracer_config", width, steps, keep)
+        m = cuda_mesh(phi, geo['dx'], geo)      # the 8-wide tree is built only when configured
         x = cuda_neutrals(m, geo, None, 0.7, 7, 1_000_000)
     finally:
         _lib.call("petch_tracer_config", *_lib.TRACER_DEFAULT)
+    ref = cuda_neutrals(m, geo, None, 0.7, 7, 1_000_000)
     assert _rel_l2(x, ref) < 0.01
     assert x.sum() == pytest.approx(ref.sum(), rel=1e-3)
+
+
+def test_wide_traversal_without_wide_tree_fails_loudly():
+    """A mesh built under the default (binary) configuration has no 8-wide tree: tracing it with
+    width 8 sets error bit 8 instead of silently missing every face."""
+    phi, geo = small_feature(False)
+    m = cuda_mesh(phi, geo['dx'], geo)
+    from petch_b200 import _lib
+    work = torch.zeros(6, dtype=torch.int32, device="cuda")
+    flux = torch.zeros(m.MT, device="cuda")
+    try:
+        _lib.call("petch_tracer_config", 8, 8, 0)
+        _lib.call("petch_trace_neutrals", m.id, m.MT, m.MV, ctypes.byref(domain(geo)), None, 0.7,
+                  1, 0, 1000, flux.data_ptr(), work.data_ptr(), stream())
+    finally:
+        _lib.call("petch_tracer_config", *_lib.TRACER_DEFAULT)
+    assert work[1].item() & 8
 
 
 def test_replay_same_seed_same_paths():
