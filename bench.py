@@ -185,6 +185,67 @@ def radiosity_summary(par, flags, W, K, world, rank, local, dist):
                         "face, 4 coverage rounds of 40 Jacobi sweeps, 2^22 ions), seed 0"}
 
 
+BATCH_N, BATCH_STEPS, BATCH_RAYS, BATCH_T_END, BATCH_PLAIN_SAMPLE = 64, 30, 1 << 20, 3.0, 16
+
+
+def batched_summary(world, rank, dist):
+    """The batched forward: 64 ragged holes (diameter U[2,8] um, mask U[1,3] um, extent d + 8 um,
+    dx 0.25, 24 um grid height; ion energy, F / ion and O / F ratios drawn per instance, seed 0),
+    30 steps, 2^20 rays per species per step per instance, each step one CUDA graph replay;
+    beside it the plain per-instance loop (run_etch_3d one instance after another) on the first
+    16 instances.  Values are instance-steps/s; device time from CUDA events, max over ranks."""
+    import torch
+    from petch_b200 import params, threed as t3
+    from petch_b200.batch import BatchEngine, hole_batch_specs
+    fl = params.Flags(chemistry="belen", yield_angular="viennaps", coverage_sticking=True,
+                      ion_reflection=True, warm_start_coverage=True)
+    specs = hole_batch_specs(BATCH_N, seed=0)
+    eng = BatchEngine(specs, fl, n_ion=BATCH_RAYS, n_neu=BATCH_RAYS, t_end=BATCH_T_END,
+                      n_steps=BATCH_STEPS, seed_offset=1000 * rank)
+    launches = eng.capture()
+    flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda")
+    flush.fill_(1.0)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = Clocks(int(os.environ.get("LOCAL_RANK", "0")))
+    sec = eng.run()
+    clocks = clk.stop()
+    depths = eng.depths()
+    n_plain = BATCH_PLAIN_SAMPLE
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    plain_depths = []
+    for sp in specs[:n_plain]:
+        par = dict(params.PAR, **sp['par'])
+        g = t3.run_etch_3d(Lx=sp['Lx'], Ly=sp['Ly'], Lz=sp['Lz'], dx=sp['dx'],
+                           trench_width=sp['trench_width'], mask_th=sp['mask_th'],
+                           sub_top=sp['sub_top'], hole=True, t_end=BATCH_T_END,
+                           n_steps=BATCH_STEPS, par=par, flags=fl, n_ion=BATCH_RAYS,
+                           n_neu=BATCH_RAYS, reinit_method="fsm", verbose=False,
+                           seed_offset=1000 * rank)
+        plain_depths.append(t3.center_depth_3d(g))
+    e1.record()
+    torch.cuda.synchronize()
+    plain_s = e0.elapsed_time(e1) / 1e3
+    t = torch.tensor([sec, plain_s], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    sec, plain_s = float(t[0].item()), float(t[1].item())
+    dd = np.abs(np.array(depths[:n_plain]) - np.array(plain_depths))
+    return {"value": world * BATCH_N * BATCH_STEPS / sec, "unit": "instance-steps/s",
+            "seconds": sec, "instances": BATCH_N, "steps": BATCH_STEPS,
+            "rays_per_species": BATCH_RAYS,
+            "plain_loop": {"value": world * n_plain * BATCH_STEPS / plain_s,
+                           "unit": "instance-steps/s", "seconds": plain_s,
+                           "sample": f"first {n_plain} instances, run_etch_3d one after another"},
+            "graph_launches_per_step": launches, "clocks": clocks,
+            "max_depth_diff_vs_plain_um": float(dd.max()),
+            "workload": "64 ragged holes (configs: batched forward), 30 steps, 2^20 rays per "
+                        "species, each step one CUDA graph, seed 0",
+            "l2": "256 MB flush before the timed run; instances' working sets exceed L2"}
+
+
 # ------------------------------------------------------------------------------------------
 def run_b200(args):
     import torch
@@ -245,6 +306,8 @@ def run_b200(args):
            "clocks": info.get('clk'), "stage_seconds": {k: v for k, v in geo['timings'].items()}}
     if not args.no_radiosity:
         out["radiosity"] = radiosity_summary(par, flags, W, K, world, rank, local, dist)
+    if not args.no_batched:
+        out["batched"] = batched_summary(world, rank, dist)
     if rank == 0 and not args.no_e2e:
         out["e2e"] = e2e(args, par, flags)
     if rank == 0 and not args.no_cpu_baseline:
@@ -348,6 +411,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-radiosity", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
     args = ap.parse_args()
     if args.warmup < 0 or args.steps < 1 or args.warmup >= N_STEPS:
         raise SystemExit("need 0 <= warmup < 100 and steps >= 1")
