@@ -416,6 +416,78 @@ int petch_radiosity_solve(const void* mesh, int max_tris, int max_verts, const i
                           double betaE, double betaO, int n_iter, float* g_E, float* g_O,
                           double* work2, void* stream);
 
+/* ---- recipe gradient: tangent (forward-mode) versions of the step's stages ----
+ * No reference counterpart (the reference has no loop gradient).  Each call computes the
+ * primal result exactly as its plain counterpart and the derivatives of it along 3 directions
+ * (the recipe parameters theta_k), taking the primal's branches: ray hits, sticking / roulette
+ * and energy-acceptance decisions, upwind and min / max selections, clamps and nearest faces are
+ * held fixed (the pathwise derivative; visibility-boundary terms are not included).  Tangent
+ * arrays are direction-major: direction k of a field of n entries starts at k * n. */
+
+/* petch_trace_ions plus dtal[3][max_tris] = d(sputter, ion-enhanced, passivation tallies) /
+ * d(mean ion energy) along the same paths. */
+int petch_trace_ions_tangent(const void* mesh, int max_tris, int max_verts,
+                             const petch_domain* dom, const petch_ion_params* p, uint32_t seed,
+                             int n_ion, float* tally4, float* ang, float* dtal, int* work,
+                             void* stream);
+
+/* petch_trace_neutrals plus dflux[3][max_tris], the tallies' tangents given the coverage
+ * tangents dbare[3][max_tris] (NULL = 0). */
+int petch_trace_neutrals_tangent(const void* mesh, int max_tris, int max_verts,
+                                 const petch_domain* dom, const float* bare, const float* dbare,
+                                 float beta, uint32_t seed, uint32_t stream_id, int n_neu,
+                                 float* flux, float* dflux, int* work, void* stream);
+
+/* Tangent of petch_norm_smooth (blend_last_only = 0) or of petch_ion_post's smoothing
+ * (blend_last_only = 1, clip = 0): dout[3][max_tris] from dfl[3][max_tris] (fl: the primal
+ * tally, for the clamp).  tmp_a, tmp_b: float[max_tris]. */
+int petch_norm_smooth_tangent(const void* mesh, int max_tris, int max_verts, const float* fl,
+                              const float* dfl, float scale, float lo, float hi, int clip,
+                              int n_smooth, float alpha, int blend_last_only, float* dout,
+                              float* tmp_a, float* tmp_b, void* stream);
+
+/* petch_belen_bare (faithful-ion yields) in float64 dual arithmetic: bare and dbare[3][MT] from
+ * the tangents of m_F, m_O, y_ie, y_ip ([3][MT] each, NULL = 0) and dOflux[3] (host). */
+int petch_belen_bare_tangent(const void* mesh, int max_tris, int max_verts,
+                             const petch_chem_params* p, const double* dOflux, const float* m_F,
+                             const float* dm_F, const float* m_O, const float* dm_O,
+                             const float* y_ie, const float* dy_ie, const float* y_ip,
+                             const float* dy_ip, float* bare, float* dbare, void* stream);
+
+/* petch_surface_rate (Belen chemistry, faithful-ion yields) in float64 dual arithmetic: V and
+ * dV[3][MT]; dOflux[3], drate[3]: d Oflux / d theta_k and d rate_scale / d theta_k (host). */
+int petch_surface_rate_tangent(const void* mesh, int max_tris, int max_verts,
+                               const petch_chem_params* p, const double* dOflux,
+                               const double* drate, const float* m_F, const float* dm_F,
+                               const float* m_O, const float* dm_O, const float* y_sp,
+                               const float* dy_sp, const float* y_ie, const float* dy_ie,
+                               const float* y_ip, const float* dy_ip, float* V, float* dV,
+                               int* stats, void* stream);
+
+/* dF[3][n] = dV[3][max_tris] of the nearest face on cells with |phi| < band (the choice
+ * petch_extend_velocity makes), 0 elsewhere. */
+int petch_extend_tangent(const void* mesh, int max_tris, int max_verts, const float* phi, int nx,
+                         int ny, int nz, double dx, double band, const float* dV, float* dF,
+                         int* work, void* stream);
+
+/* dbare[3][MT] of the warm start (petch_warmstart): the previous mesh's nearest-face tangent,
+ * 0 where the copied coverage is clamped. */
+int petch_warmstart_tangent(const void* prev_mesh, int prev_max_tris, int prev_max_verts,
+                            const float* prev_bare, const float* prev_dbare, const void* mesh,
+                            int max_tris, int max_verts, float* dbare, int* work, void* stream);
+
+/* petch_advect (mask array) with tangents: phi / dphi[3][n] advanced nsub substeps with F /
+ * dF[3][n]; tmp, dtmp: ping-pong scratch of the same sizes. */
+int petch_advect_tangent(float* phi, float* tmp, float* dphi, float* dtmp, const float* F,
+                         const float* dF, const uint8_t* mask, const float* mask_phi, int nx,
+                         int ny, int nz, float inv_dx, float dt_sub, int nsub, void* stream);
+
+/* petch_reinit_eik (mode 0, in place) with tangents of phi ([3][n]); u_a, u_b: float[n],
+ * du_a, du_b: float[3][n] scratch. */
+int petch_reinit_tangent(float* phi, float* dphi, float* u_a, float* u_b, float* du_a, float* du_b,
+                         int nx, int ny, int nz, double dx, float big, float cap, int n_iter,
+                         void* stream);
+
 #ifdef __cplusplus
 }
 #endif

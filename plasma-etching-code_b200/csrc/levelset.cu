@@ -74,6 +74,7 @@ __global__ void __launch_bounds__(kBlock) k_advect(const float* __restrict__ phi
                                                    const uint8_t* __restrict__ mask,
                                                    const float* __restrict__ mask_phi, Grid g,
                                                    float inv_dx, float dt) {
+    const petch::LGrid lg = petch::make_lgrid(g.nx, g.ny, g.nz);
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.n;
          c += (long long)gridDim.x * blockDim.x) {
         float f = F[c];
@@ -87,26 +88,7 @@ __global__ void __launch_bounds__(kBlock) k_advect(const float* __restrict__ phi
             out[c] = v;
             continue;
         }
-        int i, j, k;
-        split(g, c, i, j, k);
-        float dm, dp, t;
-        float gg = 0.0f;
-        dm = (i >= 1) ? (v - phi[c - g.plane]) * inv_dx : 0.0f;
-        dp = (i <= g.nx - 2) ? (phi[c + g.plane] - v) * inv_dx : 0.0f;
-        t = fmaxf(dm, 0.0f);
-        float s = fminf(dp, 0.0f);
-        gg += t * t + s * s;
-        dm = (j >= 1) ? (v - phi[c - g.nz]) * inv_dx : 0.0f;
-        dp = (j <= g.ny - 2) ? (phi[c + g.nz] - v) * inv_dx : 0.0f;
-        t = fmaxf(dm, 0.0f);
-        s = fminf(dp, 0.0f);
-        gg += t * t + s * s;
-        dm = (k >= 1) ? (v - phi[c - 1]) * inv_dx : 0.0f;
-        dp = (k <= g.nz - 2) ? (phi[c + 1] - v) * inv_dx : 0.0f;
-        t = fmaxf(dm, 0.0f);
-        s = fminf(dp, 0.0f);
-        gg += t * t + s * s;
-        out[c] = v - dt * f * sqrtf(gg);
+        out[c] = petch::advect_cell(phi, c, lg, inv_dx, f, dt);
     }
 }
 

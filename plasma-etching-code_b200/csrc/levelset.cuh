@@ -29,30 +29,27 @@ __device__ __forceinline__ void lsplit(const LGrid& g, long long c, int& i, int&
 }
 
 // One first-order Godunov upwind substep of cell c with speed f (threed.py:1262-1292): a zero
-// one-sided difference at the domain faces.
+// one-sided difference at the domain faces.  Every operation is rounded on its own (no fused
+// multiply-add), so every kernel that advects -- dense, band list, batched, tangent -- produces
+// the same bits.
 __device__ __forceinline__ float advect_cell(const float* __restrict__ phi, long long c,
                                              const LGrid& g, float inv_dx, float f, float dt) {
     int i, j, k;
     lsplit(g, c, i, j, k);
     const float v = phi[c];
-    float dm, dp, t, s;
+    const long long st[3] = {g.plane, (long long)g.nz, 1};
+    const int pos[3] = {i, j, k};
+    const int ext[3] = {g.nx, g.ny, g.nz};
     float gg = 0.0f;
-    dm = (i >= 1) ? (v - phi[c - g.plane]) * inv_dx : 0.0f;
-    dp = (i <= g.nx - 2) ? (phi[c + g.plane] - v) * inv_dx : 0.0f;
-    t = fmaxf(dm, 0.0f);
-    s = fminf(dp, 0.0f);
-    gg += t * t + s * s;
-    dm = (j >= 1) ? (v - phi[c - g.nz]) * inv_dx : 0.0f;
-    dp = (j <= g.ny - 2) ? (phi[c + g.nz] - v) * inv_dx : 0.0f;
-    t = fmaxf(dm, 0.0f);
-    s = fminf(dp, 0.0f);
-    gg += t * t + s * s;
-    dm = (k >= 1) ? (v - phi[c - 1]) * inv_dx : 0.0f;
-    dp = (k <= g.nz - 2) ? (phi[c + 1] - v) * inv_dx : 0.0f;
-    t = fmaxf(dm, 0.0f);
-    s = fminf(dp, 0.0f);
-    gg += t * t + s * s;
-    return v - dt * f * sqrtf(gg);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float dm = pos[a] >= 1 ? __fmul_rn(__fsub_rn(v, phi[c - st[a]]), inv_dx) : 0.0f;
+        const float dp = pos[a] <= ext[a] - 2 ? __fmul_rn(__fsub_rn(phi[c + st[a]], v), inv_dx) : 0.0f;
+        const float t = fmaxf(dm, 0.0f);
+        const float s = fminf(dp, 0.0f);
+        gg = __fadd_rn(gg, __fadd_rn(__fmul_rn(t, t), __fmul_rn(s, s)));
+    }
+    return __fsub_rn(v, __fmul_rn(__fmul_rn(dt, f), __fsqrt_rn(gg)));
 }
 
 // Godunov solution of |grad U| = 1 from the three upwind neighbour minima (threed.py:1421-1452):

@@ -9,6 +9,7 @@
 //     (threed.py:1723-1728) and the CFL maximum (threed.py:1750).
 // Chemistry runs in float64 like the reference's numpy host code; flux arrays are float32.
 #include "common.cuh"
+#include "dual.cuh"
 #include "levelset.cuh"
 #include "mesh.cuh"
 
@@ -186,6 +187,134 @@ __global__ void __launch_bounds__(kSB) k_rate(MeshView m, Chem c, const float* _
     if ((threadIdx.x & 31) == 0) {
         if (bad) atomicAdd(stats, bad);
         atomicMax(stats + 1, __float_as_int(fmaxf(vmax, 0.0f)));
+    }
+}
+
+// ---- tangent (forward-mode) versions for the recipe gradient: the primal values bit for bit,
+// plus N = 3 directional derivatives; tangent arrays are direction-major ([3][MT]) ----
+constexpr int kND = 3;
+using DD = Dual<double, kND>;
+
+__device__ __forceinline__ DD ddload(const float* v, const float* d, int f, long long MT) {
+    DD r;
+    r.v = (double)v[f];
+#pragma unroll
+    for (int k = 0; k < kND; ++k) r.d[k] = d ? (double)d[f + k * MT] : 0.0;
+    return r;
+}
+
+struct ParamTan {
+    double dOflux[kND];      // d Oflux / d theta_k
+    double drate[kND];       // d rate_scale / d theta_k
+};
+
+__device__ __forceinline__ DD dparam(double v, const double* d) {
+    DD r;
+    r.v = v;
+#pragma unroll
+    for (int k = 0; k < kND; ++k) r.d[k] = d[k];
+    return r;
+}
+
+// k_belen_bare with the faithful-ion yields, in dual arithmetic.
+__global__ void __launch_bounds__(kSB) k_belen_bare_tan(MeshView m, Chem c, ParamTan pt,
+                                                        const float* __restrict__ m_F,
+                                                        const float* __restrict__ dm_F,
+                                                        const float* __restrict__ m_O,
+                                                        const float* __restrict__ dm_O,
+                                                        const float* __restrict__ y_ie,
+                                                        const float* __restrict__ dy_ie,
+                                                        const float* __restrict__ y_ip,
+                                                        const float* __restrict__ dy_ip,
+                                                        float* __restrict__ bare,
+                                                        float* __restrict__ dbare) {
+    const int F = min(m.hdr[HDR_F], m.MT);
+    const long long MT = m.MT;
+    const double eps = 1e-9;
+    const DD Oflux = dparam(c.Oflux, pt.dOflux);
+    for (int f = blockIdx.x * kSB + threadIdx.x; f < F; f += gridDim.x * kSB) {
+        const DD GY_ie = c.ionFlux * ddload(y_ie, dy_ie, f, MT);
+        const DD GY_p = c.ionFlux * ddload(y_ip, dy_ip, f, MT);
+        const DD GbE = c.Fflux * ddload(m_F, dm_F, f, MT) + eps;
+        const DD GbP = Oflux * ddload(m_O, dm_O, f, MT) + eps;
+        const DD a = (c.k_sigma + 2.0 * GY_ie) / GbE;
+        const DD b = (c.beta_sigma + GY_p) / GbP;
+        const DD thF = 1.0 / (1.0 + a * (1.0 + 1.0 / (b + eps)));
+        const DD thO = 1.0 / (1.0 + b * (1.0 + 1.0 / (a + eps)));
+        const DD x = 1.0 - thF - thO;
+        const bool inside = x.v > 0.0 && x.v < 1.0;
+        bare[f] = (float)fmin(fmax(x.v, 0.0), 1.0);
+#pragma unroll
+        for (int k = 0; k < kND; ++k) dbare[f + k * MT] = inside ? (float)x.d[k] : 0.0f;
+    }
+}
+
+// k_rate (Belen chemistry, faithful-ion yields) in dual arithmetic; stats as k_rate.
+__global__ void __launch_bounds__(kSB) k_rate_tan(MeshView m, Chem c, ParamTan pt,
+                                                  const float* __restrict__ m_F,
+                                                  const float* __restrict__ dm_F,
+                                                  const float* __restrict__ m_O,
+                                                  const float* __restrict__ dm_O,
+                                                  const float* __restrict__ y_sp,
+                                                  const float* __restrict__ dy_sp,
+                                                  const float* __restrict__ y_ie,
+                                                  const float* __restrict__ dy_ie,
+                                                  const float* __restrict__ y_ip,
+                                                  const float* __restrict__ dy_ip,
+                                                  float* __restrict__ V, float* __restrict__ dV,
+                                                  int* stats) {
+    const int F = min(m.hdr[HDR_F], m.MT);
+    const long long MT = m.MT;
+    const double eps = 1e-9;
+    const DD Oflux = dparam(c.Oflux, pt.dOflux);
+    const DD rs = dparam(c.rate_scale, pt.drate);
+    int bad = 0;
+    float vmax_ = 0.0f;
+    for (int f = blockIdx.x * kSB + threadIdx.x; f < F; f += gridDim.x * kSB) {
+        const DD GY_ie = c.ionFlux * ddload(y_ie, dy_ie, f, MT);
+        const DD GY_p = c.ionFlux * ddload(y_ip, dy_ip, f, MT);
+        const DD sputter = c.ionFlux * ddload(y_sp, dy_sp, f, MT);
+        const DD ion_enh = GY_ie;
+        const DD GbE = c.Fflux * ddload(m_F, dm_F, f, MT) / c.fnorm_E + eps;
+        const DD GbP = Oflux * ddload(m_O, dm_O, f, MT) / c.fnorm_O + eps;
+        const DD a = (c.k_sigma + 2.0 * GY_ie) / GbE;
+        const DD b = (c.beta_sigma + GY_p) / GbP;
+        const DD thF = 1.0 / (1.0 + a * (1.0 + 1.0 / (b + eps)));
+        const DD rate = c.k_sigma * thF / 4.0 + sputter + thF * ion_enh;
+        DD v = (1.0 / c.rho) * rate * rs;
+        if (m.fmask[f]) v = dconst<double, kND>(0.0);
+        float vf = (float)v.v;
+        bool ok = isfinite(v.v) && isfinite(vf);
+        if (!ok) {
+            ++bad;
+            vf = 0.0f;
+        }
+        V[f] = vf;
+#pragma unroll
+        for (int k = 0; k < kND; ++k) dV[f + k * MT] = ok ? (float)v.d[k] : 0.0f;
+        vmax_ = fmaxf(vmax_, vf);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        vmax_ = fmaxf(vmax_, __shfl_xor_sync(0xffffffffu, vmax_, o));
+        bad += __shfl_xor_sync(0xffffffffu, bad, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (bad) atomicAdd(stats, bad);
+        atomicMax(stats + 1, __float_as_int(fmaxf(vmax_, 0.0f)));
+    }
+}
+
+// Tangent of clamp((fl / A) * scale, lo, hi): d(out) = (d fl / A) * scale inside the clamp.
+__global__ void __launch_bounds__(kSB) k_norm_tan(MeshView m, const float* __restrict__ fl,
+                                                  const float* __restrict__ dfl, float scale,
+                                                  float lo, float hi, int clip,
+                                                  float* __restrict__ dout) {
+    const int F = min(m.hdr[HDR_F], m.MT);
+    for (int f = blockIdx.x * kSB + threadIdx.x; f < F; f += gridDim.x * kSB) {
+        const float A = m.area[f];
+        const float v = (fl[f] / A) * scale;
+        const bool inside = !clip || (v > lo && v < hi);
+        dout[f] = inside ? (dfl[f] / A) * scale : 0.0f;
     }
 }
 
@@ -401,5 +530,90 @@ extern "C" int petch_advect_sparse(float* phi, float* tmp, const float* F, const
         k_copy_list<<<ba, kSB, 0, st>>>(phi, a, active, n_active);
         PETCH_LAUNCH_CHECK("k_copy_list");
     }
+    return PETCH_OK;
+}
+
+static ParamTan param_tan(const double* dOflux, const double* drate) {
+    ParamTan pt;
+    for (int k = 0; k < kND; ++k) {
+        pt.dOflux[k] = dOflux ? dOflux[k] : 0.0;
+        pt.drate[k] = drate ? drate[k] : 0.0;
+    }
+    return pt;
+}
+
+extern "C" int petch_norm_smooth_tangent(const void* mesh, int max_tris, int max_verts,
+                                         const float* fl, const float* dfl, float scale, float lo,
+                                         float hi, int clip, int n_smooth, float alpha,
+                                         int blend_last_only, float* dout, float* tmp_a,
+                                         float* tmp_b, void* stream) {
+    PETCH_REQUIRE(mesh && fl && dfl && dout && tmp_a && tmp_b,
+                  "petch_norm_smooth_tangent: null pointer");
+    cudaStream_t st = as_stream(stream);
+    MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
+    const int b = grid_for(max_tris, kSB);
+    const long long MT = max_tris;
+    for (int k = 0; k < kND; ++k) {
+        float* out = dout + k * MT;
+        const bool smooth = n_smooth > 0 && alpha > 0.0f;
+        k_norm_tan<<<b, kSB, 0, st>>>(m, fl, dfl + k * MT, scale, lo, hi, clip, smooth ? tmp_a : out);
+        PETCH_LAUNCH_CHECK("k_norm_tan");
+        if (!smooth) continue;
+        // the primal's smoothing passes on the tangent (the smoothing is linear): each pass
+        // blended with its own input (petch_norm_smooth) or only the last pass blended with the
+        // raw field (petch_ion_post, blend_last_only)
+        const float* raw = tmp_a;
+        const float* src = tmp_a;
+        for (int it = 0; it < n_smooth; ++it) {
+            const bool last = it == n_smooth - 1;
+            float* dst;
+            if (blend_last_only)      // as petch_ion_post: the raw field stays intact to the end
+                dst = ((n_smooth - 1 - it) % 2 == 0) ? out : tmp_b;
+            else                      // as petch_norm_smooth
+                dst = last ? out : (src == tmp_a ? tmp_b : tmp_a);
+            const float* blend = blend_last_only ? raw : src;
+            const float a = blend_last_only ? (last ? alpha : 1.0f) : alpha;
+            k_smooth<<<b, kSB, 0, st>>>(m, src, blend, a, dst);
+            PETCH_LAUNCH_CHECK("k_smooth");
+            src = dst;
+        }
+    }
+    return PETCH_OK;
+}
+
+extern "C" int petch_belen_bare_tangent(const void* mesh, int max_tris, int max_verts,
+                                        const petch_chem_params* p, const double* dOflux,
+                                        const float* m_F, const float* dm_F, const float* m_O,
+                                        const float* dm_O, const float* y_ie, const float* dy_ie,
+                                        const float* y_ip, const float* dy_ip, float* bare,
+                                        float* dbare, void* stream) {
+    PETCH_REQUIRE(mesh && p && m_F && m_O && y_ie && y_ip && bare && dbare,
+                  "petch_belen_bare_tangent: null pointer");
+    MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
+    k_belen_bare_tan<<<grid_for(max_tris, kSB), kSB, 0, as_stream(stream)>>>(
+        m, to_chem(p), param_tan(dOflux, nullptr), m_F, dm_F, m_O, dm_O, y_ie, dy_ie, y_ip, dy_ip,
+        bare, dbare);
+    PETCH_LAUNCH_CHECK("k_belen_bare_tan");
+    return PETCH_OK;
+}
+
+extern "C" int petch_surface_rate_tangent(const void* mesh, int max_tris, int max_verts,
+                                          const petch_chem_params* p, const double* dOflux,
+                                          const double* drate, const float* m_F, const float* dm_F,
+                                          const float* m_O, const float* dm_O, const float* y_sp,
+                                          const float* dy_sp, const float* y_ie,
+                                          const float* dy_ie, const float* y_ip,
+                                          const float* dy_ip, float* V, float* dV, int* stats,
+                                          void* stream) {
+    PETCH_REQUIRE(mesh && p && m_F && m_O && y_sp && y_ie && y_ip && V && dV && stats,
+                  "petch_surface_rate_tangent: null pointer");
+    PETCH_REQUIRE(p->chemistry == 1, "petch_surface_rate_tangent: Belen chemistry only");
+    cudaStream_t st = as_stream(stream);
+    MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
+    PETCH_CUDA(cudaMemsetAsync(stats, 0, 2 * sizeof(int), st), "memset stats");
+    k_rate_tan<<<grid_for(max_tris, kSB), kSB, 0, st>>>(m, to_chem(p), param_tan(dOflux, drate), m_F,
+                                                        dm_F, m_O, dm_O, y_sp, dy_sp, y_ie, dy_ie,
+                                                        y_ip, dy_ip, V, dV, stats);
+    PETCH_LAUNCH_CHECK("k_rate_tan");
     return PETCH_OK;
 }

@@ -138,6 +138,8 @@ __device__ __forceinline__ float3 stored_normal(const MeshView& m, int f) {
 struct RayState {
     float w, E;
     int bounce, wraps, id;
+    float dE;        // tangent of E w.r.t. the mean ion energy (tangent shaders only)
+    float dw[3];     // tangents of the neutral weight (tangent shaders only)
 };
 
 // _trace3d_cov_rr (threed.py:549-596): deposit the weight on every hit, W *= 1 - bare * beta,
@@ -154,6 +156,41 @@ __device__ __forceinline__ bool neutral_hit(const float* bare, float beta, float
     if (s.w <= 1.0e-6f) return false;
     if (s.w < 0.1f) {
         if (g.uniform() < (1.0f - s.w / 0.3f)) return false;
+        s.w = 0.3f;
+    }
+    float3 h = o + t * d;
+    d = cosine_emit(g, nrm);
+    o = h + 1.0e-4f * nrm;
+    return true;
+}
+
+// neutral_hit with weight tangents: d(deposit) = dw, dw' = dw (1 - S) - w dS with
+// dS = dbare * beta (dbare[0..2][MT]); the roulette decisions are those of the primal path.
+__device__ __forceinline__ bool neutral_hit_tan(const float* bare, const float* dbare, float beta,
+                                                float* flux, float* dflux, Rng& g, const Tracer& T,
+                                                int f, float t, float3& o, float3& d, RayState& s) {
+    float3 nrm = stored_normal(T.m, f);
+    if (dot3(nrm, d) > 0.0f) nrm = -nrm;
+    const long long MT = T.m.MT;
+    atomicAdd(flux + f, s.w);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) atomicAdd(dflux + k * MT + f, s.dw[k]);
+    float S = (bare ? __ldg(bare + f) : 1.0f) * beta;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float dS = dbare ? __ldg(dbare + k * MT + f) * beta : 0.0f;
+        s.dw[k] = s.dw[k] - (s.dw[k] * S + s.w * dS);
+    }
+    s.w = s.w - s.w * S;
+    if (s.w <= 1.0e-6f) return false;
+    if (s.w < 0.1f) {
+        if (g.uniform() < (1.0f - s.w / 0.3f)) return false;
+        // the survivor stands for weight w with probability w / 0.3: with that probability held
+        // fixed, its weight 0.3 = w / p has tangent dw / p = dw * 0.3 / w (an unbiased estimate of
+        // the derivative of the expected deposits)
+        const float r = 0.3f / s.w;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) s.dw[k] *= r;
         s.w = 0.3f;
     }
     float3 h = o + t * d;
@@ -184,9 +221,13 @@ struct NeutralShader {
 // cos * weight; then angle-dependent sticking, energy loss (<= 4 truncated-normal tries), weight
 // reduction and coned-cosine reflection about the specular axis (<= 64 accept-reject draws);
 // at most 1024 bounces.  tal4[f] = (sp, ie, ip, arr), ang[f] = sum cos * w.
+// TAN: also accumulate d(sputter, ion-enhanced, passivation tallies) / d(mean ion energy) into
+// dtal[0..2][MT] along the same path (hits, sticking and energy-acceptance decisions fixed) and
+// carry dE / dE_mean through the energy losses.
+template <bool TAN = false>
 __device__ __forceinline__ bool ion_hit(const IonP& P, float4* tal4, float* ang, Rng& g,
                                         const Tracer& T, int f, float t, float3& o, float3& d,
-                                        RayState& s) {
+                                        RayState& s, float* dtal = nullptr) {
     const float PI_2 = 1.5707963f;
     float3 nrm = stored_normal(T.m, f);
     if (dot3(nrm, d) > 0.0f) nrm = -nrm;
@@ -201,6 +242,13 @@ __device__ __forceinline__ bool ion_hit(const IonP& P, float4* tal4, float* ang,
                                     P.A_ie * fmaxf(sqrtE - sqrtf(P.Eth_ie), 0.0f) * f_ie * w,
                                     P.A_p * fmaxf(sqrtE - sqrtf(P.Eth_p), 0.0f) * f_ie * w, w));
     atomicAdd(ang + f, cosT * w);
+    if (TAN) {
+        const long long MT = T.m.MT;
+        const float dsq = s.E > 0.0f ? 0.5f * s.dE / sqrtE : 0.0f;
+        if (sqrtE > sqrtf(P.Eth_sp)) atomicAdd(dtal + f, P.A_sp * dsq * f_sp * w);
+        if (sqrtE > sqrtf(P.Eth_ie)) atomicAdd(dtal + MT + f, P.A_ie * dsq * f_ie * w);
+        if (sqrtE > sqrtf(P.Eth_p)) atomicAdd(dtal + 2 * MT + f, P.A_p * dsq * f_ie * w);
+    }
     float stick = 1.0f;
     if (incAng > P.thrmin) stick = 1.0f - fminf(fmaxf((incAng - P.thrmin) / (P.thrmax - P.thrmin), 0.0f), 1.0f);
     if (stick >= 1.0f) return false;
@@ -209,15 +257,21 @@ __device__ __forceinline__ bool ion_hit(const IonP& P, float4* tal4, float* ang,
                      : P.A_en * powf(incAng / P.inflect, P.n_l);
     const float E = s.E;
     float newE = Eref * E;
+    float slope = Eref;                      // d newE / d E on the taken branch
     for (int e = 0; e < 4; ++e) {
-        float cand = Eref * E + 0.1f * E * g.normal();
+        const float z = g.normal();
+        float cand = Eref * E + 0.1f * E * z;
         if (cand >= 0.0f && cand <= E) {
             newE = cand;
+            slope = Eref + 0.1f * z;
             break;
         }
     }
+    if (newE < 0.0f) slope = 0.0f;
+    if (newE > E) slope = 1.0f;
     newE = fminf(fmaxf(newE, 0.0f), E);
     if (newE <= P.minE) return false;
+    if (TAN) s.dE = slope * s.dE;
     s.E = newE;
     s.w = w - w * stick;
     if (s.w <= 1.0e-4f) return false;
@@ -312,6 +366,47 @@ struct LegacyShader {
         }
         o = h + 1.0e-4f * nrm;
         return true;
+    }
+};
+
+// Tangent versions of the ion and neutral shaders (the primal tallies plus their tangents).
+struct IonTanShader {
+    IonP P;
+    float4* tal4;
+    float* ang;
+    float* dtal;            // [3][MT]: d(sp, ie, ip) / d(mean ion energy)
+    static constexpr int kMaxBounce = 1024;
+    __device__ __forceinline__ int count(const MeshView&, int n) const { return n; }
+    __device__ __forceinline__ void init(Rng& g, const Tracer&, const Domain& D, int, float3& o,
+                                         float3& d, RayState& s) const {
+        source(g, true, P.sigma, D, o, d);
+        s.E = fmaxf(P.meanE + P.sigmaE * g.normal(), 0.0f);
+        s.dE = s.E > 0.0f ? 1.0f : 0.0f;
+        s.w = 1.0f;
+    }
+    __device__ __forceinline__ bool hit(Rng& g, const Tracer& T, int f, float t, float3& o,
+                                        float3& d, RayState& s) const {
+        return ion_hit<true>(P, tal4, ang, g, T, f, t, o, d, s, dtal);
+    }
+};
+
+struct NeutralTanShader {
+    const float* bare;
+    const float* dbare;     // [3][MT]
+    float beta;
+    float* flux;
+    float* dflux;           // [3][MT]
+    static constexpr int kMaxBounce = 1024;
+    __device__ __forceinline__ int count(const MeshView&, int n) const { return n; }
+    __device__ __forceinline__ void init(Rng& g, const Tracer&, const Domain& D, int, float3& o,
+                                         float3& d, RayState& s) const {
+        source(g, false, 0.0f, D, o, d);
+        s.w = 1.0f;
+        s.dw[0] = s.dw[1] = s.dw[2] = 0.0f;
+    }
+    __device__ __forceinline__ bool hit(Rng& g, const Tracer& T, int f, float t, float3& o,
+                                        float3& d, RayState& s) const {
+        return neutral_hit_tan(bare, dbare, beta, flux, dflux, g, T, f, t, o, d, s);
     }
 };
 
@@ -1012,6 +1107,52 @@ extern "C" int petch_redep_apply(const void* mesh, int max_tris, int max_verts, 
     k_redep_apply<<<grid_for(max_tris, 256), 256, 0, st>>>(m, flux, cdf, n, k_redep, V, Rf, stats);
     PETCH_LAUNCH_CHECK("k_redep_apply");
     return PETCH_OK;
+}
+
+extern "C" int petch_trace_ions_tangent(const void* mesh, int max_tris, int max_verts,
+                                        const petch_domain* dom, const petch_ion_params* p,
+                                        uint32_t seed, int n_ion, float* tally4, float* ang,
+                                        float* dtal, int* work, void* stream) {
+    PETCH_REQUIRE(mesh && dom && p && tally4 && ang && dtal && work,
+                  "petch_trace_ions_tangent: null pointer");
+    PETCH_REQUIRE(n_ion >= 0 && max_tris > 0 && max_verts > 0, "petch_trace_ions_tangent: bad size");
+    PETCH_REQUIRE(((uintptr_t)tally4 & 15) == 0, "petch_trace_ions_tangent: tally4 alignment");
+    cudaStream_t st = as_stream(stream);
+    MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
+    IonTanShader sh;
+    sh.P = IonP{p->meanE, p->sigmaE, p->A_sp, p->Eth_sp, p->B_sp, p->A_ie, p->Eth_ie, p->A_p,
+                p->Eth_p, p->inflect, p->minang, p->n_l, p->A_en, p->minE, p->thrmin, p->thrmax,
+                p->sigma};
+    sh.tal4 = (float4*)tally4;
+    sh.ang = ang;
+    sh.dtal = dtal;
+    k_zero_faces<<<grid_for(4LL * max_tris, 256), 256, 0, st>>>(m.hdr, max_tris, tally4, 4, ang, 1);
+    PETCH_LAUNCH_CHECK("k_zero_faces");
+    PETCH_CUDA(cudaMemsetAsync(dtal, 0, sizeof(float) * 3 * (size_t)max_tris, st), "zero dtal");
+    PETCH_CUDA(cudaMemsetAsync(work, 0, sizeof(int), st), "reset ray counter");
+    if (n_ion == 0) return PETCH_OK;
+    return launch_trace(m, to_domain(dom), sh, seed, 0x696f6e73u, n_ion, work, st,
+                        "k_trace<ions, tangent>");
+}
+
+extern "C" int petch_trace_neutrals_tangent(const void* mesh, int max_tris, int max_verts,
+                                            const petch_domain* dom, const float* bare,
+                                            const float* dbare, float beta, uint32_t seed,
+                                            uint32_t stream_id, int n_neu, float* flux,
+                                            float* dflux, int* work, void* stream) {
+    PETCH_REQUIRE(mesh && dom && flux && dflux && work, "petch_trace_neutrals_tangent: null pointer");
+    PETCH_REQUIRE(n_neu >= 0 && max_tris > 0 && max_verts > 0,
+                  "petch_trace_neutrals_tangent: bad size");
+    cudaStream_t st = as_stream(stream);
+    MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
+    NeutralTanShader sh{bare, dbare, beta, flux, dflux};
+    k_zero_faces<<<grid_for(max_tris, 256), 256, 0, st>>>(m.hdr, max_tris, flux, 1, nullptr, 0);
+    PETCH_LAUNCH_CHECK("k_zero_faces");
+    PETCH_CUDA(cudaMemsetAsync(dflux, 0, sizeof(float) * 3 * (size_t)max_tris, st), "zero dflux");
+    PETCH_CUDA(cudaMemsetAsync(work, 0, sizeof(int), st), "reset ray counter");
+    if (n_neu == 0) return PETCH_OK;
+    return launch_trace(m, to_domain(dom), sh, seed, 0x6e657500u ^ stream_id, n_neu, work, st,
+                        "k_trace<neutrals, tangent>");
 }
 
 extern "C" int petch_trace_legacy(const void* mesh, int max_tris, int max_verts,

@@ -102,6 +102,15 @@ SIGNATURES = {
     "petch_redep_apply": [P, I, I, P, P, I, F, P, P, P, P],
     "petch_trace_batch": [I, P, I, I, I, F, P, U, U, P, P],
     "petch_prepare_device": [],
+    "petch_trace_ions_tangent": [P, I, I, DP, IP, U, I, P, P, P, P, P],
+    "petch_trace_neutrals_tangent": [P, I, I, DP, P, P, F, U, U, I, P, P, P, P],
+    "petch_norm_smooth_tangent": [P, I, I, P, P, F, F, F, I, I, F, I, P, P, P, P],
+    "petch_belen_bare_tangent": [P, I, I, CP, P, P, P, P, P, P, P, P, P, P, P, P],
+    "petch_surface_rate_tangent": [P, I, I, CP, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P],
+    "petch_extend_tangent": [P, I, I, P, I, I, I, D, D, P, P, P, P],
+    "petch_warmstart_tangent": [P, I, I, P, P, P, I, I, P, P, P],
+    "petch_advect_tangent": [P, P, P, P, P, P, P, P, I, I, I, F, F, I, P],
+    "petch_reinit_tangent": [P, P, P, P, P, P, I, I, I, D, F, F, I, P],
     "petch_batch_advect": [P, I, P],
     "petch_batch_reinit": [P, I, D, P],
     "petch_batch_step_advance": [P, P],
