@@ -246,6 +246,100 @@ def batched_summary(world, rank, dist):
             "l2": "256 MB flush before the timed run; instances' working sets exceed L2"}
 
 
+DIFF_STEPS, DIFF_SEEDS = 20, 8
+
+
+def _loss_fn(target):
+    def loss(p):
+        ok = np.isfinite(p) & np.isfinite(target)
+        return float(np.mean((p[ok] - target[ok]) ** 2)), ok
+    return loss
+
+
+def _grad_check(cfg, theta0, theta_t, seeds, h_rel, radial_profile, run):
+    """Mean over seeds of dLoss/dtheta from the tangents and of the central difference with
+    relative step h_rel on the same seeds (common random numbers)."""
+    phi_t, _, g_t, _ = run(theta_t, seed_offset=1, **cfg)
+    loss = _loss_fn(radial_profile(phi_t, g_t)[0])
+    target = radial_profile(phi_t, g_t)[0]
+    g_tan, g_fd = np.zeros(3), np.zeros((len(seeds), 3))
+    losses = []
+    for i, s in enumerate(seeds):
+        phi, dphi, geo, _ = run(theta0, seed_offset=s, **cfg)
+        p, J = radial_profile(phi, geo, dphi)
+        L, ok = loss(p)
+        losses.append(L)
+        g_tan += 2.0 * np.mean((p[ok] - target[ok])[:, None] * np.nan_to_num(J[ok]), axis=0)
+        for k in range(3):
+            h = h_rel * theta0[k]
+            tp, tm = theta0.copy(), theta0.copy()
+            tp[k] += h
+            tm[k] -= h
+            Lp = loss(radial_profile(run(tp, seed_offset=s, **cfg)[0], geo)[0])[0]
+            Lm = loss(radial_profile(run(tm, seed_offset=s, **cfg)[0], geo)[0])[0]
+            g_fd[i, k] = (Lp - Lm) / (2 * h)
+    names = ("Emean", "O_F", "rate_scale")
+    return {"loss": float(np.mean(losses)),
+            "grad_tangent": dict(zip(names, map(float, g_tan / len(seeds)))),
+            "grad_fd": dict(zip(names, map(float, g_fd.mean(0)))),
+            "grad_fd_stderr": dict(zip(names, map(float, g_fd.std(0, ddof=1) / np.sqrt(len(seeds))))),
+            "fd_step_rel": h_rel, "seeds": len(seeds)}
+
+
+def differentiation_summary():
+    """The recipe gradient (forward-mode tangents of every stage; mesh, hit topology and random
+    decisions held fixed) with deterministic tallies.
+      cost: the tangent run's device time over the plain forward run's on the config-0 hole
+        (extent 14, dx 0.25, diameter 6, mask 2, depth 18, 30000 rays per species, the first 20
+        steps of the 40-step 3.0 schedule);
+      config3: dLoss/dtheta there (loss = MSE of the 32-bin radial depth profile against the
+        profile at (150 eV, O/F 0.2, rate_scale 1.1, seed 1); theta0 = (100, 0.1, 1.0)), tangent
+        beside central differences with relative step 1e-3, 8 seeds;
+      slope_check: a sub-limit etch (rate_scale 0.05; at 1.0 the front moves at the narrow-band
+        limit and the profile hardly depends on theta), tangent beside the seed-averaged slope of
+        the loss (relative step 0.1, common random numbers, 32 seeds)."""
+    import torch
+    from petch_b200 import _lib, params, threed as t3
+    from petch_b200.adjoint import apply_theta, radial_profile, run_etch_3d_tangent
+    _lib.set_deterministic(8 * 16 * 131072)
+    try:
+        fl = params.Flags(chemistry="belen", yield_angular="viennaps", coverage_sticking=True,
+                          ion_reflection=True, warm_start_coverage=True)
+        geo_kw = dict(Lx=14.0, Ly=14.0, Lz=24.0, dx=0.25, trench_width=6.0, mask_th=2.0,
+                      sub_top=18.0, hole=True)
+        cfg = dict(geo_kw, t_end=1.5, n_steps=DIFF_STEPS, flags=fl, n_ion=30000, n_neu=30000)
+        theta0 = np.array([100.0, 0.1, 1.0])
+        run_etch_3d_tangent(theta0, seed_offset=0, **cfg)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        t3.run_etch_3d(**geo_kw, t_end=1.5, n_steps=DIFF_STEPS,
+                       par=apply_theta(dict(params.PAR), theta0), flags=fl, n_ion=30000,
+                       n_neu=30000, reinit_method="fsm", verbose=False)
+        e1.record()
+        torch.cuda.synchronize()
+        fwd = e0.elapsed_time(e1) / 1e3
+        _, _, _, tan = run_etch_3d_tangent(theta0, seed_offset=0, **cfg)
+        c3 = _grad_check(cfg, theta0, np.array([150.0, 0.2, 1.1]), range(100, 100 + DIFF_SEEDS),
+                         1e-3, radial_profile, run_etch_3d_tangent)
+        small = dict(Lx=8.0, Ly=8.0, Lz=12.0, dx=0.25, trench_width=4.0, mask_th=1.0,
+                     sub_top=8.0, hole=True, t_end=0.6, n_steps=6, flags=fl, n_ion=30000,
+                     n_neu=30000)
+        sc = _grad_check(small, np.array([100.0, 0.1, 0.05]), np.array([150.0, 0.2, 0.055]),
+                         range(200, 232), 0.1, radial_profile, run_etch_3d_tangent)
+    finally:
+        _lib.set_deterministic(0)
+    return {"bwd_fwd_ratio": tan / fwd, "forward_s": fwd, "tangent_run_s": tan,
+            "config3": dict(c3, workload="config-0 hole, 20 steps of the 40-step 3.0 schedule, "
+                            "30000 rays per species, theta0 = (100 eV, 0.1, 1.0), target "
+                            "(150, 0.2, 1.1) seed 1"),
+            "slope_check": dict(sc, workload="8 x 8 x 12 um hole, diameter 4, mask 1, 6 steps "
+                                "of 0.1, 30000 rays, theta0 = (100 eV, 0.1, 0.05), target "
+                                "(150, 0.2, 0.055) seed 1"),
+            "method": "forward-mode tangents (3 directions) through every stage; deterministic "
+                      "tallies; mesh, hit topology and random decisions held fixed (the fluxes' "
+                      "surface-shape feedback is not differentiated)"}
+
+
 # ------------------------------------------------------------------------------------------
 def run_b200(args):
     import torch
@@ -308,6 +402,8 @@ def run_b200(args):
         out["radiosity"] = radiosity_summary(par, flags, W, K, world, rank, local, dist)
     if not args.no_batched:
         out["batched"] = batched_summary(world, rank, dist)
+    if rank == 0 and not args.no_diff:
+        out["differentiation"] = differentiation_summary()
     if rank == 0 and not args.no_e2e:
         out["e2e"] = e2e(args, par, flags)
     if rank == 0 and not args.no_cpu_baseline:
@@ -412,6 +508,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-radiosity", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-diff", action="store_true")
     args = ap.parse_args()
     if args.warmup < 0 or args.steps < 1 or args.warmup >= N_STEPS:
         raise SystemExit("need 0 <= warmup < 100 and steps >= 1")

@@ -286,6 +286,17 @@ int petch_gaussian_smooth(float* phi, float* tmp_a, float* tmp_b, const uint8_t*
                           const float* mask_phi, int nx, int ny, int nz, double sigma,
                           double truncate, void* stream);
 
+/* Deterministic tallies (no reference counterpart).  With a scratch registered, every tracing
+ * entry point accumulates its per-face tallies as 64-bit fixed-point integers (units of 2^-32,
+ * carved from the scratch, converted to the float outputs at the end of the call): integer sums
+ * do not depend on the order in which rays deposit, so with the Philox streams fixed a run is
+ * reproducible bit for bit.  Deposits are rounded to 2^-32 (far below the 1e-6 weight floor of
+ * the Russian roulette).  The scratch must hold 8 bytes per tally entry of the largest call
+ * (ions: 5 * max_tris, 8 * max_tris with tangents; batches: per instance) plus 256-byte
+ * alignment per array; calls fail with PETCH_E_INVALID otherwise.  NULL switches back to float
+ * atomics.  Process-wide state: calls on several streams at once share the scratch and race. */
+int petch_set_deterministic(void* scratch, long long scratch_bytes);
+
 /* ---- batched tracing (many independent instances in one launch) ---- */
 
 /* Caches the host-side device queries the launchers use (SM count, resident blocks of the

@@ -30,6 +30,13 @@ int g_bvh_width = 2;
 int g_steps = 64;
 int g_keep = 12;
 
+// Deterministic tallies (petch_set_deterministic): caller-registered scratch for 64-bit
+// fixed-point accumulators; NULL = float atomics.
+void* g_det_scratch = nullptr;
+long long g_det_bytes = 0;
+
+constexpr float kTallyScale = 4294967296.0f;      // 2^32: one unit = 2^-32
+
 }  // namespace
 
 bool wide_bvh_enabled() { return g_bvh_width == 8; }
@@ -128,6 +135,18 @@ __global__ void k_zero_faces(const int* hdr, int MT, float* a, int na, float* b,
         for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < F * nb; i += gridDim.x * blockDim.x) b[i] = 0.0f;
 }
 
+
+// One deposit into a tally.  det == 0: float atomic add into out[i].  det != 0: out is an int64
+// accumulator array (same indexing) and v is added in units of 2^-32 -- integer sums do not
+// depend on the order of the additions, so the result is the same on every run.
+__device__ __forceinline__ void tally(float* out, long long i, float v, int det) {
+    if (det)
+        atomicAdd(reinterpret_cast<unsigned long long*>(out) + i,
+                  (unsigned long long)__float2ll_rn(v * kTallyScale));
+    else
+        atomicAdd(out + i, v);
+}
+
 // The face's unit winding normal as stored by the mesh build (float32, bit-identical to
 // normalize(cross(b - a, c - a)) on the float32 vertices, the normal Warp's query returns).
 __device__ __forceinline__ float3 stored_normal(const MeshView& m, int f) {
@@ -147,10 +166,10 @@ struct RayState {
 // 0.3), cosine re-emission; at most 1024 bounces.
 __device__ __forceinline__ bool neutral_hit(const float* bare, float beta, float* flux, Rng& g,
                                             const Tracer& T, int f, float t, float3& o, float3& d,
-                                            RayState& s) {
+                                            RayState& s, int det) {
     float3 nrm = stored_normal(T.m, f);
     if (dot3(nrm, d) > 0.0f) nrm = -nrm;
-    atomicAdd(flux + f, s.w);
+    tally(flux, f, s.w, det);
     float S = (bare ? __ldg(bare + f) : 1.0f) * beta;
     s.w = s.w - s.w * S;
     if (s.w <= 1.0e-6f) return false;
@@ -168,13 +187,14 @@ __device__ __forceinline__ bool neutral_hit(const float* bare, float beta, float
 // dS = dbare * beta (dbare[0..2][MT]); the roulette decisions are those of the primal path.
 __device__ __forceinline__ bool neutral_hit_tan(const float* bare, const float* dbare, float beta,
                                                 float* flux, float* dflux, Rng& g, const Tracer& T,
-                                                int f, float t, float3& o, float3& d, RayState& s) {
+                                                int f, float t, float3& o, float3& d, RayState& s,
+                                                int det) {
     float3 nrm = stored_normal(T.m, f);
     if (dot3(nrm, d) > 0.0f) nrm = -nrm;
     const long long MT = T.m.MT;
-    atomicAdd(flux + f, s.w);
+    tally(flux, f, s.w, det);
 #pragma unroll
-    for (int k = 0; k < 3; ++k) atomicAdd(dflux + k * MT + f, s.dw[k]);
+    for (int k = 0; k < 3; ++k) tally(dflux, k * MT + f, s.dw[k], det);
     float S = (bare ? __ldg(bare + f) : 1.0f) * beta;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -203,6 +223,7 @@ struct NeutralShader {
     const float* bare;
     float beta;
     float* flux;
+    int det;
     static constexpr int kMaxBounce = 1024;
     __device__ __forceinline__ int count(const MeshView&, int n) const { return n; }
     __device__ __forceinline__ void init(Rng& g, const Tracer&, const Domain& D, int, float3& o,
@@ -212,7 +233,7 @@ struct NeutralShader {
     }
     __device__ __forceinline__ bool hit(Rng& g, const Tracer& T, int f, float t, float3& o,
                                         float3& d, RayState& s) const {
-        return neutral_hit(bare, beta, flux, g, T, f, t, o, d, s);
+        return neutral_hit(bare, beta, flux, g, T, f, t, o, d, s, det);
     }
 };
 
@@ -227,7 +248,7 @@ struct NeutralShader {
 template <bool TAN = false>
 __device__ __forceinline__ bool ion_hit(const IonP& P, float4* tal4, float* ang, Rng& g,
                                         const Tracer& T, int f, float t, float3& o, float3& d,
-                                        RayState& s, float* dtal = nullptr) {
+                                        RayState& s, int det, float* dtal = nullptr) {
     const float PI_2 = 1.5707963f;
     float3 nrm = stored_normal(T.m, f);
     if (dot3(nrm, d) > 0.0f) nrm = -nrm;
@@ -238,16 +259,25 @@ __device__ __forceinline__ bool ion_hit(const IonP& P, float4* tal4, float* ang,
     float f_ie = 1.0f;
     if (cosT < 0.5f) f_ie = fmaxf(3.0f - 6.0f * incAng / 3.14159265f, 0.0f);
     float w = s.w;
-    atomicAdd(tal4 + f, make_float4(P.A_sp * fmaxf(sqrtE - sqrtf(P.Eth_sp), 0.0f) * f_sp * w,
-                                    P.A_ie * fmaxf(sqrtE - sqrtf(P.Eth_ie), 0.0f) * f_ie * w,
-                                    P.A_p * fmaxf(sqrtE - sqrtf(P.Eth_p), 0.0f) * f_ie * w, w));
-    atomicAdd(ang + f, cosT * w);
+    const float4 dep = make_float4(P.A_sp * fmaxf(sqrtE - sqrtf(P.Eth_sp), 0.0f) * f_sp * w,
+                                   P.A_ie * fmaxf(sqrtE - sqrtf(P.Eth_ie), 0.0f) * f_ie * w,
+                                   P.A_p * fmaxf(sqrtE - sqrtf(P.Eth_p), 0.0f) * f_ie * w, w);
+    if (det) {
+        float* t4 = reinterpret_cast<float*>(tal4);
+        tally(t4, 4LL * f, dep.x, det);
+        tally(t4, 4LL * f + 1, dep.y, det);
+        tally(t4, 4LL * f + 2, dep.z, det);
+        tally(t4, 4LL * f + 3, dep.w, det);
+    } else {
+        atomicAdd(tal4 + f, dep);
+    }
+    tally(ang, f, cosT * w, det);
     if (TAN) {
         const long long MT = T.m.MT;
         const float dsq = s.E > 0.0f ? 0.5f * s.dE / sqrtE : 0.0f;
-        if (sqrtE > sqrtf(P.Eth_sp)) atomicAdd(dtal + f, P.A_sp * dsq * f_sp * w);
-        if (sqrtE > sqrtf(P.Eth_ie)) atomicAdd(dtal + MT + f, P.A_ie * dsq * f_ie * w);
-        if (sqrtE > sqrtf(P.Eth_p)) atomicAdd(dtal + 2 * MT + f, P.A_p * dsq * f_ie * w);
+        if (sqrtE > sqrtf(P.Eth_sp)) tally(dtal, f, P.A_sp * dsq * f_sp * w, det);
+        if (sqrtE > sqrtf(P.Eth_ie)) tally(dtal, MT + f, P.A_ie * dsq * f_ie * w, det);
+        if (sqrtE > sqrtf(P.Eth_p)) tally(dtal, 2 * MT + f, P.A_p * dsq * f_ie * w, det);
     }
     float stick = 1.0f;
     if (incAng > P.thrmin) stick = 1.0f - fminf(fmaxf((incAng - P.thrmin) / (P.thrmax - P.thrmin), 0.0f), 1.0f);
@@ -309,6 +339,7 @@ struct IonShader {
     IonP P;
     float4* tal4;
     float* ang;
+    int det;
     static constexpr int kMaxBounce = 1024;
     __device__ __forceinline__ int count(const MeshView&, int n) const { return n; }
     __device__ __forceinline__ void init(Rng& g, const Tracer&, const Domain& D, int, float3& o,
@@ -319,7 +350,7 @@ struct IonShader {
     }
     __device__ __forceinline__ bool hit(Rng& g, const Tracer& T, int f, float t, float3& o,
                                         float3& d, RayState& s) const {
-        return ion_hit(P, tal4, ang, g, T, f, t, o, d, s);
+        return ion_hit(P, tal4, ang, g, T, f, t, o, d, s, det);
     }
 };
 
@@ -331,6 +362,7 @@ struct LegacyShader {
     float sigma, sticking, cos_thr, eta;
     float* flux;
     float* angacc;
+    int det;
     static constexpr int kMaxBounce = 1 << 30;
     __device__ __forceinline__ int count(const MeshView&, int n) const { return n; }
     __device__ __forceinline__ void init(Rng& g, const Tracer&, const Domain& D, int, float3& o,
@@ -346,20 +378,20 @@ struct LegacyShader {
         float3 h = o + t * d;
         if (specular == 1) {
             if (cosang >= cos_thr || s.bounce == n_reemit) {
-                atomicAdd(flux + f, s.w);
-                atomicAdd(angacc + f, s.w * cosang);
+                tally(flux, f, s.w, det);
+                tally(angacc, f, s.w * cosang, det);
                 return false;
             }
             float R = (cos_thr - cosang) / cos_thr;
             float dep = s.w * (1.0f - R);
-            atomicAdd(flux + f, dep);
-            atomicAdd(angacc + f, dep * cosang);
+            tally(flux, f, dep, det);
+            tally(angacc, f, dep * cosang, det);
             s.w = s.w * R * eta;
             d = d - (2.0f * dot3(d, nrm)) * nrm;
         } else {
             if (g.uniform() < sticking || s.bounce == n_reemit) {
-                atomicAdd(flux + f, s.w);
-                atomicAdd(angacc + f, s.w * cosang);
+                tally(flux, f, s.w, det);
+                tally(angacc, f, s.w * cosang, det);
                 return false;
             }
             d = cosine_emit(g, nrm);
@@ -375,6 +407,7 @@ struct IonTanShader {
     float4* tal4;
     float* ang;
     float* dtal;            // [3][MT]: d(sp, ie, ip) / d(mean ion energy)
+    int det;
     static constexpr int kMaxBounce = 1024;
     __device__ __forceinline__ int count(const MeshView&, int n) const { return n; }
     __device__ __forceinline__ void init(Rng& g, const Tracer&, const Domain& D, int, float3& o,
@@ -386,7 +419,7 @@ struct IonTanShader {
     }
     __device__ __forceinline__ bool hit(Rng& g, const Tracer& T, int f, float t, float3& o,
                                         float3& d, RayState& s) const {
-        return ion_hit<true>(P, tal4, ang, g, T, f, t, o, d, s, dtal);
+        return ion_hit<true>(P, tal4, ang, g, T, f, t, o, d, s, det, dtal);
     }
 };
 
@@ -396,6 +429,7 @@ struct NeutralTanShader {
     float beta;
     float* flux;
     float* dflux;           // [3][MT]
+    int det;
     static constexpr int kMaxBounce = 1024;
     __device__ __forceinline__ int count(const MeshView&, int n) const { return n; }
     __device__ __forceinline__ void init(Rng& g, const Tracer&, const Domain& D, int, float3& o,
@@ -406,7 +440,7 @@ struct NeutralTanShader {
     }
     __device__ __forceinline__ bool hit(Rng& g, const Tracer& T, int f, float t, float3& o,
                                         float3& d, RayState& s) const {
-        return neutral_hit_tan(bare, dbare, beta, flux, dflux, g, T, f, t, o, d, s);
+        return neutral_hit_tan(bare, dbare, beta, flux, dflux, g, T, f, t, o, d, s, det);
     }
 };
 
@@ -673,7 +707,7 @@ __global__ void __launch_bounds__(kTB, kTraceMinBlocks) k_trace_batch(BatchTable
                                                                      uint32_t seed_mul,
                                                                      uint32_t seed_add,
                                                                      uint32_t domain, int steps,
-                                                                     int keep, int* work) {
+                                                                     int keep, int det, int* work) {
     __shared__ BatchItem s_it[kMaxBatch];
     __shared__ int s_start[kMaxBatch + 1];
     for (int i = threadIdx.x; i < tab.B; i += blockDim.x) {
@@ -750,8 +784,8 @@ __global__ void __launch_bounds__(kTB, kTraceMinBlocks) k_trace_batch(BatchTable
                 if (cont) ++rs.wraps;
             } else {
                 cont = ION ? ion_hit(it.P, reinterpret_cast<float4*>(it.out), it.ang, g, T, q.f,
-                                     q.t, o, d, rs)
-                           : neutral_hit(it.bare, beta, it.out, g, T, q.f, q.t, o, d, rs);
+                                     q.t, o, d, rs, det)
+                           : neutral_hit(it.bare, beta, it.out, g, T, q.f, q.t, o, d, rs, det);
                 rs.wraps = 0;
                 if (cont && ++rs.bounce >= 1024) cont = false;
             }
@@ -775,6 +809,14 @@ __global__ void __launch_bounds__(kTB, kTraceMinBlocks) k_trace_batch(BatchTable
         atomicAdd(reinterpret_cast<unsigned long long*>(work + 2), n_query);
         atomicAdd(reinterpret_cast<unsigned long long*>(work + 4), n_visit);
     }
+}
+
+// Deterministic tallies back to float: out[i] = acc[i] * 2^-32.
+__global__ void k_acc_to_float(const long long* __restrict__ acc, float* __restrict__ out,
+                               long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        out[i] = (float)((double)acc[i] * (1.0 / 4294967296.0));
 }
 
 struct GridArgs {
@@ -912,6 +954,54 @@ static Domain to_domain(const petch_domain* d) {
     return D;
 }
 
+// Accumulators of one deterministic trace call, carved from the registered scratch.
+struct DetArena {
+    char* base = static_cast<char*>(g_det_scratch);
+    long long cap = g_det_bytes, used = 0;
+    bool on() const { return base != nullptr; }
+    long long* take(long long count) {
+        const long long bytes = ((8 * count) + 255) & ~255LL;
+        if (used + bytes > cap) return nullptr;
+        long long* p = reinterpret_cast<long long*>(base + used);
+        used += bytes;
+        return p;
+    }
+};
+
+static int acc_zero(long long* acc, long long n, cudaStream_t st) {
+    PETCH_CUDA(cudaMemsetAsync(acc, 0, sizeof(long long) * (size_t)n, st), "zero tally accumulators");
+    return PETCH_OK;
+}
+
+static int acc_convert(const long long* acc, float* out, long long n, cudaStream_t st) {
+    k_acc_to_float<<<grid_for(n, 256), 256, 0, st>>>(acc, out, n);
+    PETCH_LAUNCH_CHECK("k_acc_to_float");
+    return PETCH_OK;
+}
+
+#define PETCH_DET_TAKE(var, count)                                                           \
+    long long* var = arena.take(count);                                                      \
+    PETCH_REQUIRE(var, "deterministic tallies: the registered scratch (%lld bytes) is too small", \
+                  g_det_bytes);                                                              \
+    do {                                                                                     \
+        int _rc = acc_zero(var, count, st);                                                  \
+        if (_rc) return _rc;                                                                 \
+    } while (0)
+
+#define PETCH_DET_CONVERT(var, out, count)                                                   \
+    do {                                                                                     \
+        int _rc = acc_convert(var, out, count, st);                                          \
+        if (_rc) return _rc;                                                                 \
+    } while (0)
+
+extern "C" int petch_set_deterministic(void* scratch, long long scratch_bytes) {
+    PETCH_REQUIRE(scratch == nullptr || scratch_bytes >= 256,
+                  "petch_set_deterministic: scratch too small");
+    g_det_scratch = scratch;
+    g_det_bytes = scratch ? scratch_bytes : 0;
+    return PETCH_OK;
+}
+
 template <class S>
 static int launch_trace(const MeshView& m, const Domain& D, const S& sh, uint32_t seed,
                         uint32_t domain, int n, int* work, cudaStream_t st, const char* what) {
@@ -953,11 +1043,24 @@ extern "C" int petch_trace_ions(const void* mesh, int max_tris, int max_verts,
                 p->sigma};
     sh.tal4 = (float4*)tally4;
     sh.ang = ang;
+    sh.det = 0;
     k_zero_faces<<<grid_for(4LL * max_tris, 256), 256, 0, st>>>(m.hdr, max_tris, tally4, 4, ang, 1);
     PETCH_LAUNCH_CHECK("k_zero_faces");
     PETCH_CUDA(cudaMemsetAsync(work, 0, sizeof(int), st), "reset ray counter");
     if (n_ion == 0) return PETCH_OK;
-    return launch_trace(m, to_domain(dom), sh, seed, 0x696f6e73u, n_ion, work, st, "k_trace<ions>");
+    DetArena arena;
+    if (!arena.on())
+        return launch_trace(m, to_domain(dom), sh, seed, 0x696f6e73u, n_ion, work, st, "k_trace<ions>");
+    PETCH_DET_TAKE(a_t, 4LL * max_tris);
+    PETCH_DET_TAKE(a_a, (long long)max_tris);
+    sh.tal4 = reinterpret_cast<float4*>(a_t);
+    sh.ang = reinterpret_cast<float*>(a_a);
+    sh.det = 1;
+    int rc = launch_trace(m, to_domain(dom), sh, seed, 0x696f6e73u, n_ion, work, st, "k_trace<ions>");
+    if (rc) return rc;
+    PETCH_DET_CONVERT(a_t, tally4, 4LL * max_tris);
+    PETCH_DET_CONVERT(a_a, ang, (long long)max_tris);
+    return PETCH_OK;
 }
 
 extern "C" int petch_trace_neutrals(const void* mesh, int max_tris, int max_verts,
@@ -968,13 +1071,23 @@ extern "C" int petch_trace_neutrals(const void* mesh, int max_tris, int max_vert
     PETCH_REQUIRE(n_neu >= 0 && max_tris > 0 && max_verts > 0, "petch_trace_neutrals: bad size");
     cudaStream_t st = as_stream(stream);
     MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
-    NeutralShader sh{bare, beta, flux};
+    NeutralShader sh{bare, beta, flux, 0};
     k_zero_faces<<<grid_for(max_tris, 256), 256, 0, st>>>(m.hdr, max_tris, flux, 1, nullptr, 0);
     PETCH_LAUNCH_CHECK("k_zero_faces");
     PETCH_CUDA(cudaMemsetAsync(work, 0, sizeof(int), st), "reset ray counter");
     if (n_neu == 0) return PETCH_OK;
-    return launch_trace(m, to_domain(dom), sh, seed, 0x6e657500u ^ stream_id, n_neu, work, st,
-                        "k_trace<neutrals>");
+    DetArena arena;
+    if (!arena.on())
+        return launch_trace(m, to_domain(dom), sh, seed, 0x6e657500u ^ stream_id, n_neu, work, st,
+                            "k_trace<neutrals>");
+    PETCH_DET_TAKE(a_f, (long long)max_tris);
+    sh.flux = reinterpret_cast<float*>(a_f);
+    sh.det = 1;
+    int rc = launch_trace(m, to_domain(dom), sh, seed, 0x6e657500u ^ stream_id, n_neu, work, st,
+                          "k_trace<neutrals>");
+    if (rc) return rc;
+    PETCH_DET_CONVERT(a_f, flux, (long long)max_tris);
+    return PETCH_OK;
 }
 
 extern "C" int petch_trace_ff(const void* mesh, int max_tris, int max_verts,
@@ -1047,16 +1160,39 @@ extern "C" int petch_trace_batch(int kind, const petch_batch_item* items, int B,
     PETCH_CUDA(cudaMemsetAsync(work, 0, sizeof(int), st), "reset ray counter");
     if (total == 0) return PETCH_OK;
     const uint32_t domain = kind == 0 ? 0x696f6e73u : 0x6e657500u;
+    DetArena arena;
+    const int det = arena.on() ? 1 : 0;
+    const long long per_out = (kind == 0 ? 4LL : 1LL) * max_tris;
+    long long* acc_out[kMaxBatch] = {};
+    long long* acc_ang[kMaxBatch] = {};
+    if (det) {
+        for (int b = 0; b < B; ++b) {
+            PETCH_DET_TAKE(ao, per_out);
+            acc_out[b] = ao;
+            tab.it[b].out = reinterpret_cast<float*>(ao);
+            if (kind == 0) {
+                PETCH_DET_TAKE(aa, (long long)max_tris);
+                acc_ang[b] = aa;
+                tab.it[b].ang = reinterpret_cast<float*>(aa);
+            }
+        }
+    }
     if (kind == 0) {
         k_trace_batch<true><<<persistent_blocks((const void*)k_trace_batch<true>, kTB, 0), kTB, 0, st>>>(
             tab, L, max_tris, max_verts, beta, step, seed_mul, seed_add, domain, g_steps, g_keep,
-            work);
+            det, work);
     } else {
         k_trace_batch<false><<<persistent_blocks((const void*)k_trace_batch<false>, kTB, 0), kTB, 0, st>>>(
             tab, L, max_tris, max_verts, beta, step, seed_mul, seed_add, domain, g_steps, g_keep,
-            work);
+            det, work);
     }
     PETCH_LAUNCH_CHECK("k_trace_batch");
+    if (det) {
+        for (int b = 0; b < B; ++b) {
+            PETCH_DET_CONVERT(acc_out[b], items[b].out, per_out);
+            if (kind == 0) PETCH_DET_CONVERT(acc_ang[b], items[b].ang, (long long)max_tris);
+        }
+    }
     return PETCH_OK;
 }
 
@@ -1088,12 +1224,21 @@ extern "C" int petch_trace_redep(const void* mesh, int max_tris, int max_verts,
     PETCH_CUDA(cudaMemsetAsync(work, 0, sizeof(int), st), "reset ray counter");
     if (n == 0) return PETCH_OK;
     RedepShader sh;
-    sh.rr = NeutralShader{nullptr, s_redep, flux};
+    sh.rr = NeutralShader{nullptr, s_redep, flux, 0};
     sh.cdf = cdf;
     sh.fn = fn;
     Domain D = to_domain(dom);
     D.periodic = 0;                      // mc_redep_3d traces without the lateral wrap
-    return launch_trace(m, D, sh, seed, 0x72656470u, n, work, st, "k_trace<redeposition>");
+    DetArena arena;
+    if (!arena.on())
+        return launch_trace(m, D, sh, seed, 0x72656470u, n, work, st, "k_trace<redeposition>");
+    PETCH_DET_TAKE(a_f, (long long)max_tris);
+    sh.rr.flux = reinterpret_cast<float*>(a_f);
+    sh.rr.det = 1;
+    int rc = launch_trace(m, D, sh, seed, 0x72656470u, n, work, st, "k_trace<redeposition>");
+    if (rc) return rc;
+    PETCH_DET_CONVERT(a_f, flux, (long long)max_tris);
+    return PETCH_OK;
 }
 
 extern "C" int petch_redep_apply(const void* mesh, int max_tris, int max_verts, const float* flux,
@@ -1126,13 +1271,30 @@ extern "C" int petch_trace_ions_tangent(const void* mesh, int max_tris, int max_
     sh.tal4 = (float4*)tally4;
     sh.ang = ang;
     sh.dtal = dtal;
+    sh.det = 0;
     k_zero_faces<<<grid_for(4LL * max_tris, 256), 256, 0, st>>>(m.hdr, max_tris, tally4, 4, ang, 1);
     PETCH_LAUNCH_CHECK("k_zero_faces");
     PETCH_CUDA(cudaMemsetAsync(dtal, 0, sizeof(float) * 3 * (size_t)max_tris, st), "zero dtal");
     PETCH_CUDA(cudaMemsetAsync(work, 0, sizeof(int), st), "reset ray counter");
     if (n_ion == 0) return PETCH_OK;
-    return launch_trace(m, to_domain(dom), sh, seed, 0x696f6e73u, n_ion, work, st,
-                        "k_trace<ions, tangent>");
+    DetArena arena;
+    if (!arena.on())
+        return launch_trace(m, to_domain(dom), sh, seed, 0x696f6e73u, n_ion, work, st,
+                            "k_trace<ions, tangent>");
+    PETCH_DET_TAKE(a_t, 4LL * max_tris);
+    PETCH_DET_TAKE(a_a, (long long)max_tris);
+    PETCH_DET_TAKE(a_d, 3LL * max_tris);
+    sh.tal4 = reinterpret_cast<float4*>(a_t);
+    sh.ang = reinterpret_cast<float*>(a_a);
+    sh.dtal = reinterpret_cast<float*>(a_d);
+    sh.det = 1;
+    int rc = launch_trace(m, to_domain(dom), sh, seed, 0x696f6e73u, n_ion, work, st,
+                          "k_trace<ions, tangent>");
+    if (rc) return rc;
+    PETCH_DET_CONVERT(a_t, tally4, 4LL * max_tris);
+    PETCH_DET_CONVERT(a_a, ang, (long long)max_tris);
+    PETCH_DET_CONVERT(a_d, dtal, 3LL * max_tris);
+    return PETCH_OK;
 }
 
 extern "C" int petch_trace_neutrals_tangent(const void* mesh, int max_tris, int max_verts,
@@ -1145,14 +1307,27 @@ extern "C" int petch_trace_neutrals_tangent(const void* mesh, int max_tris, int 
                   "petch_trace_neutrals_tangent: bad size");
     cudaStream_t st = as_stream(stream);
     MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
-    NeutralTanShader sh{bare, dbare, beta, flux, dflux};
+    NeutralTanShader sh{bare, dbare, beta, flux, dflux, 0};
     k_zero_faces<<<grid_for(max_tris, 256), 256, 0, st>>>(m.hdr, max_tris, flux, 1, nullptr, 0);
     PETCH_LAUNCH_CHECK("k_zero_faces");
     PETCH_CUDA(cudaMemsetAsync(dflux, 0, sizeof(float) * 3 * (size_t)max_tris, st), "zero dflux");
     PETCH_CUDA(cudaMemsetAsync(work, 0, sizeof(int), st), "reset ray counter");
     if (n_neu == 0) return PETCH_OK;
-    return launch_trace(m, to_domain(dom), sh, seed, 0x6e657500u ^ stream_id, n_neu, work, st,
-                        "k_trace<neutrals, tangent>");
+    DetArena arena;
+    if (!arena.on())
+        return launch_trace(m, to_domain(dom), sh, seed, 0x6e657500u ^ stream_id, n_neu, work, st,
+                            "k_trace<neutrals, tangent>");
+    PETCH_DET_TAKE(a_f, (long long)max_tris);
+    PETCH_DET_TAKE(a_d, 3LL * max_tris);
+    sh.flux = reinterpret_cast<float*>(a_f);
+    sh.dflux = reinterpret_cast<float*>(a_d);
+    sh.det = 1;
+    int rc = launch_trace(m, to_domain(dom), sh, seed, 0x6e657500u ^ stream_id, n_neu, work, st,
+                          "k_trace<neutrals, tangent>");
+    if (rc) return rc;
+    PETCH_DET_CONVERT(a_f, flux, (long long)max_tris);
+    PETCH_DET_CONVERT(a_d, dflux, 3LL * max_tris);
+    return PETCH_OK;
 }
 
 extern "C" int petch_trace_legacy(const void* mesh, int max_tris, int max_verts,
@@ -1165,15 +1340,28 @@ extern "C" int petch_trace_legacy(const void* mesh, int max_tris, int max_verts,
                   "petch_trace_legacy: bad size");
     cudaStream_t st = as_stream(stream);
     MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
-    LegacyShader sh{ion, n_reemit, specular, sigma, sticking, cos_thr, eta, flux, angacc};
+    LegacyShader sh{ion, n_reemit, specular, sigma, sticking, cos_thr, eta, flux, angacc, 0};
     k_zero_faces<<<grid_for(max_tris, 256), 256, 0, st>>>(m.hdr, max_tris, flux, 1, angacc, 1);
     PETCH_LAUNCH_CHECK("k_zero_faces");
     PETCH_CUDA(cudaMemsetAsync(work, 0, sizeof(int), st), "reset ray counter");
     if (n == 0) return PETCH_OK;
     Domain D = to_domain(dom);
     D.periodic = 0;
-    return launch_trace(m, D, sh, seed, ion ? 0x6c696f6eu : 0x6c6e6575u, n, work, st,
-                        "k_trace<legacy>");
+    DetArena arena;
+    if (!arena.on())
+        return launch_trace(m, D, sh, seed, ion ? 0x6c696f6eu : 0x6c6e6575u, n, work, st,
+                            "k_trace<legacy>");
+    PETCH_DET_TAKE(a_f, (long long)max_tris);
+    PETCH_DET_TAKE(a_a, (long long)max_tris);
+    sh.flux = reinterpret_cast<float*>(a_f);
+    sh.angacc = reinterpret_cast<float*>(a_a);
+    sh.det = 1;
+    int rc = launch_trace(m, D, sh, seed, ion ? 0x6c696f6eu : 0x6c6e6575u, n, work, st,
+                          "k_trace<legacy>");
+    if (rc) return rc;
+    PETCH_DET_CONVERT(a_f, flux, (long long)max_tris);
+    PETCH_DET_CONVERT(a_a, angacc, (long long)max_tris);
+    return PETCH_OK;
 }
 
 static int extend_velocity(const void* mesh, int max_tris, int max_verts, const float* phi,

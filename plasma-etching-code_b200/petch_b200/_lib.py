@@ -102,6 +102,7 @@ SIGNATURES = {
     "petch_redep_apply": [P, I, I, P, P, I, F, P, P, P, P],
     "petch_trace_batch": [I, P, I, I, I, F, P, U, U, P, P],
     "petch_prepare_device": [],
+    "petch_set_deterministic": [P, L],
     "petch_trace_ions_tangent": [P, I, I, DP, IP, U, I, P, P, P, P, P],
     "petch_trace_neutrals_tangent": [P, I, I, DP, P, P, F, U, U, I, P, P, P, P],
     "petch_norm_smooth_tangent": [P, I, I, P, P, F, F, F, I, I, F, I, P, P, P, P],
@@ -119,6 +120,23 @@ SIGNATURES = {
 # The library's tracer configuration at load (bvh_width, steps_per_round, keep_lanes): what
 # petch_tracer_config restores to.
 TRACER_DEFAULT = (2, 64, 12)
+
+_det_scratch = None
+
+
+def set_deterministic(max_entries):
+    """Deterministic (order-independent, bit-reproducible) tallies for every later trace call,
+    with device scratch for max_entries tally entries (8 bytes each; a batch of B instances of
+    capacity MT needs about 5 * B * MT); max_entries = 0 switches back to float atomics."""
+    import torch
+    global _det_scratch
+    if max_entries <= 0:
+        call("petch_set_deterministic", None, 0)
+        _det_scratch = None
+        return
+    nbytes = 8 * int(max_entries) + 256 * 64
+    _det_scratch = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    call("petch_set_deterministic", _det_scratch.data_ptr(), nbytes)
 
 _lib = None
 
