@@ -427,6 +427,33 @@ int petch_radiosity_solve(const void* mesh, int max_tris, int max_verts, const i
                           double betaE, double betaO, int n_iter, float* g_E, float* g_O,
                           double* work2, void* stream);
 
+/* ---- DDA neutral transport (deterministic discrete ordinates) ----
+ * Replaces dda_neutral_flux (petch/dda.py:132-188) as called by mc_flux_3d_dda
+ * (petch/threed.py:1211-1244).  petch_dda_prepare marches every (face, direction) ray of
+ * _dda_gather_kernel (dda.py:26-96) once through the occupancy grid and records where it ends
+ * (a solid cell, an escape at z >= z_top, or nothing after max_steps), computes the direct view,
+ * each face's solid-side wall cell round(centroid - 0.7 dx n) and the cells of the one-cell
+ * dilation; petch_dda_solve then runs n_reemit re-emission passes plus the Aitken extrapolation
+ * for both sticking fields s = clip(bare * betaE / betaO, 0, 1) from those records.  March and
+ * gather sums in float32, the cell re-emission, dilation and extrapolation in float64, every sum in
+ * the reference's order: bit-reproducible.
+ * Grid: phi float[nx*ny*nz] (phi > 0 solid), node i at x = i dx.  Faces: n_faces is a DEVICE int
+ * (the live count, clamped to max_faces; a mesh header's HDR_F word works), origins / normals
+ * float[3*max_faces] (surface points and unit into-gas normals), areas float[max_faces].
+ * Directions: dirs float[3*n_dirs], weights float[n_dirs] (fib_sphere(2 * dda_n_dir): unit
+ * weights).  z_top and max_steps as dda.py:137-151 computes them.  The scratch holds the whole
+ * prepared geometry (copies of normals, areas, directions included); petch_dda_solve reads only it,
+ * bare float[max_faces], and writes flux_E / flux_O float[max_faces]. */
+int petch_dda_scratch_bytes(int max_faces, int nx, int ny, int nz, int n_dirs, long long* bytes);
+int petch_dda_prepare(const float* phi, int nx, int ny, int nz, double dx, double z_top,
+                      int max_steps, int periodic_y, const int* n_faces, int max_faces,
+                      const float* origins, const float* normals, const float* areas,
+                      const float* dirs, const float* weights, int n_dirs, void* scratch,
+                      long long scratch_bytes, void* stream);
+int petch_dda_solve(int max_faces, int nx, int ny, int nz, int n_dirs, const float* bare,
+                    double betaE, double betaO, int n_reemit, void* scratch,
+                    long long scratch_bytes, float* flux_E, float* flux_O, void* stream);
+
 /* ---- recipe gradient: tangent (forward-mode) versions of the step's stages ----
  * No reference counterpart (the reference has no loop gradient).  Each call computes the
  * primal result exactly as its plain counterpart and the derivatives of it along 3 directions

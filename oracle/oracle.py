@@ -16,12 +16,16 @@ Reference lines followed (paths within the reference project):
   surf_smooth          petch/threed.py:1779-1782   the same scipy gaussian_filter call
   mc_flux_3d_radiosity petch/threed.py:923-1029    _gas_normals :1553-1568, _cosine_dirs :1571-1579
   mc_redep_3d          petch/threed.py:1582-1605   wired as run_etch_3d :1730-1743
+  dda_neutral_flux     petch/dda.py:26-188         gather kernel (oracle_dda.cpp), fib_sphere,
+                       wall cells, dilation, Aitken; mc_flux_3d_dda petch/threed.py:1211-1244
   _depth3d / max_depth_3d petch/threed.py:1798-1869
 Parity pinning: level-set stages and the per-face arithmetic against tests/golden/*.npz made by
 running the reference's own code (tests/golden/make_golden.py); Monte-Carlo stages statistically
 against the reference kernels' per-face means (tests/golden/flux.npz, radiosity.npz); the
-radiosity fixed point exactly from the reference's recorded form-factor hits.  Marching cubes and the seed
-distance (skfmm) are third-party in the reference: parity unpinned there.
+radiosity fixed point exactly from the reference's recorded form-factor hits; the DDA gather
+and dda_neutral_flux exactly against tests/golden/dda.npz (float64 evaluation, as the fixture
+ran).  Marching cubes and the seed distance (skfmm) are third-party in the reference: parity
+unpinned there.
 """
 import ctypes
 import glob
@@ -57,6 +61,8 @@ _SIGS = {
     "orc_trace_legacy": ([_P, _P, _I, _D, _D, _I, _I, _D, _D, _U64, _I, _P, _P], None),
     "orc_trace_ff": ([_P, _P, _P, _P, _I, _I, _U64, _P], None),
     "orc_trace_redep": ([_P, _P, _P, _P, _I, _D, _U64, _I, _P], None),
+    "orc_dda_gather": ([_P, _I, _I, _I, _P, _P, _P, _P, _I, _P, _D, _D, _D, _I, _I, _I, _I, _P],
+                       None),
 }
 
 
@@ -66,7 +72,8 @@ def build(force=False):
     newest = max(os.path.getmtime(s) for s in srcs)
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
         tmp = LIB + f".{os.getpid()}.tmp"
-        cmd = ["g++", "-O2", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-o", tmp, *srcs]
+        cmd = ["g++", "-O2", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-ffp-contract=off",
+               "-o", tmp, *srcs]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("oracle build failed:\n" + r.stderr)
@@ -640,6 +647,137 @@ def flux_radiosity(mesh, geo, phi, par, flags, n_ion, seed, n_ff=64, tt=None):
     return m_i, m_F, m_O, cos_i, iy
 
 
+# ------------------------------- DDA neutrals -------------------------------
+def fib_sphere(n):
+    """fib_sphere (dda.py:120-129): n Fibonacci directions on the full sphere, unit weights."""
+    i = np.arange(n) + 0.5
+    z = 1.0 - 2.0 * i / n
+    r = np.sqrt(np.maximum(1.0 - z * z, 0.0))
+    gold = np.pi * (1.0 + 5.0 ** 0.5)
+    theta = gold * i
+    return np.stack([r * np.cos(theta), r * np.sin(theta), z], axis=1), np.ones(n)
+
+
+def dda_gather(phi, dx, origins, normals, dirs, weights, remit, z_top, src_top, max_steps,
+               periodic_y=0, f32=False):
+    """One launch of _dda_gather_kernel (dda.py:26-96): the arriving flux per origin.  The
+    arrays are rounded to float32 as the reference uploads them; f32 evaluates in float32 (the
+    device's arithmetic), else in float64 (the golden fixture's)."""
+    phi = np.ascontiguousarray(phi, np.float32)
+    nx, ny, nz = phi.shape
+    r32 = lambda a: np.ascontiguousarray(np.asarray(a, np.float32), np.float64)  # noqa: E731
+    o, n, d, w = r32(origins), r32(normals), r32(dirs), r32(weights)
+    rem = r32(np.ravel(remit))
+    N = len(o)
+    out = np.zeros(N)
+    if N:
+        lib().orc_dda_gather(_p(phi), nx, ny, nz, _p(o), _p(n), _p(d), _p(w), len(d), _p(rem),
+                             float(dx), float(z_top), float(src_top), int(max_steps),
+                             int(periodic_y), N, int(bool(f32)), _p(out))
+    return out
+
+
+def dda_wall_cells(centroids, normals, dx, shape):
+    """The solid-side cell of each face (dda.py:143-149): round(centroid - 0.7 dx n)."""
+    nx, ny, nz = shape
+    spos = np.asarray(centroids, np.float64) - 0.7 * dx * np.asarray(normals, np.float64)
+    inv = 1.0 / dx
+    six = np.clip((spos[:, 0] * inv + 0.5).astype(np.int64), 0, nx - 1)
+    siy = np.clip((spos[:, 1] * inv + 0.5).astype(np.int64), 0, ny - 1)
+    siz = np.clip((spos[:, 2] * inv + 0.5).astype(np.int64), 0, nz - 1)
+    return (six * ny + siy) * nz + siz
+
+
+def dda_neutral_flux(phi, dx, zs, centroids, normals, s_face, n_dir=64, n_reemit=12, z_top=None,
+                     face_areas=None, periodic_y=0, f32=False):
+    """dda_neutral_flux (dda.py:132-188): the direct view, then n_reemit passes of
+    vf = direct + gather(area-weighted cell re-emission (1 - s) vf, dilated once into unseeded
+    solid neighbours), then Aitken extrapolation of the last three iterates."""
+    phi = np.asarray(phi)
+    nx, ny, nz = phi.shape
+    F = len(centroids)
+    if z_top is None:
+        z_top = zs[-1] - 0.5 * dx
+    dirs, weights = fib_sphere(2 * n_dir)
+    wall_cell = dda_wall_cells(centroids, normals, dx, phi.shape)
+    max_steps = (int((z_top - zs[0]) / dx) + 4) * (3 if periodic_y else 1)
+
+    def gather(remit, src):
+        return dda_gather(phi, dx, centroids, normals, dirs, weights, remit, z_top, src,
+                          max_steps, periodic_y, f32)
+
+    direct = gather(np.zeros(nx * ny * nz), 1.0)
+    vf = direct.copy()
+    alpha = np.clip(1.0 - np.asarray(s_face, float), 0.0, 1.0)
+    A_face = np.asarray(face_areas, float) if face_areas is not None else np.ones(F)
+    cell_area = np.zeros(nx * ny * nz)
+    np.add.at(cell_area, wall_cell, A_face)
+    solid = phi > 0.0
+    seeded = np.zeros((nx, ny, nz), bool)
+    seeded.ravel()[wall_cell] = True
+    need = solid & ~seeded
+    prev2 = prev1 = None
+    for _ in range(max(1, n_reemit)):
+        remit = np.zeros(nx * ny * nz)
+        np.add.at(remit, wall_cell, A_face * alpha * np.maximum(vf, 0.0))
+        remit /= np.maximum(cell_area, 1e-12)
+        R = remit.reshape(nx, ny, nz)
+        num = np.zeros_like(R)
+        cnt = np.zeros_like(R)
+        for ax in (0, 1, 2):
+            for sh in (1, -1):
+                num += np.where(np.roll(seeded, sh, axis=ax), np.roll(R, sh, axis=ax), 0.0)
+                cnt += np.roll(seeded, sh, axis=ax)
+        fill = need & (cnt > 0)
+        R[fill] = num[fill] / cnt[fill]
+        prev2, prev1 = prev1, vf
+        vf = direct + gather(R.ravel(), 0.0)
+    if prev2 is not None:
+        d1 = vf - prev1
+        d0 = prev1 - prev2
+        big = np.abs(d0) > 1e-12
+        r = np.where(big, d1 / np.where(big, d0, 1.0), 0.0)
+        r = np.clip(r, 0.0, 0.995)
+        vf = vf + d1 * r / (1.0 - r)
+    return np.clip(np.maximum(vf, 0.0), 0.0, 8.0)
+
+
+def dda_fixed_point(phi, dx, zs, centroids, fn, areas, m_i, cos_i, iy, par, flags, n_fp=4,
+                    f32=False):
+    """The coverage <-> DDA fixed point of mc_flux_3d_dda (threed.py:1234-1243)."""
+    F = len(centroids)
+    A = np.maximum(areas, 1e-9)
+    betaE, betaO = par.get('betaE', 0.7), par.get('betaO', 1.0)
+    n_dir, n_re = int(par.get('dda_n_dir', 64)), int(par.get('dda_n_reemit', 12))
+    per = int(par.get('periodic_y', 0))
+    ya = getattr(flags, "yield_angular", "cosine")
+    bare = np.ones(F)
+    m_F = m_O = np.zeros(F)
+    for _ in range(n_fp):
+        m_F = dda_neutral_flux(phi, dx, zs, centroids, fn, np.clip(bare * betaE, 0.0, 1.0), n_dir,
+                               n_re, face_areas=A, periodic_y=per, f32=f32)
+        m_O = dda_neutral_flux(phi, dx, zs, centroids, fn, np.clip(bare * betaO, 0.0, 1.0), n_dir,
+                               n_re, face_areas=A, periodic_y=per, f32=f32)
+        thF, thO = belen_coverages(m_i, m_F, m_O, cos_i, par, ya, iy)
+        bare = np.clip(1.0 - thF - thO, 0.0, 1.0)
+    return m_F, m_O
+
+
+def flux_dda(mesh, geo, phi, par, flags, n_ion, seed, tt=None):
+    """mc_flux_3d_dda (threed.py:1211-1244) on the oracle mesh: (m_i, m_F, m_O, cos_i,
+    ion_yield-or-None); the DDA in float32 arithmetic (the device's)."""
+    tt = {} if tt is None else tt
+    tt.setdefault('trace', 0.0)
+    t0 = time.time()
+    m_i, cos_i, iy = radiosity_ions(mesh, geo, par, flags, n_ion, seed)
+    tt['trace'] += time.time() - t0
+    fn = gas_normals(mesh.verts, mesh.faces, mesh.centroid, phi, geo['dx'])
+    zs = np.arange(np.asarray(phi).shape[2]) * geo['dx']
+    m_F, m_O = dda_fixed_point(phi, geo['dx'], zs, mesh.centroid, fn, mesh.area, m_i, cos_i, iy,
+                               par, flags, f32=True)
+    return m_i, m_F, m_O, cos_i, iy
+
+
 # ------------------------------- the loop -------------------------------
 def depth3d(geo, phi, half=1.0):
     """_depth3d (threed.py:1798-1834)."""
@@ -670,8 +808,8 @@ def depth3d(geo, phi, half=1.0):
 def run_etch_3d(Lx, Ly, Lz, dx, trench_width, mask_th, sub_top, t_end, n_steps, hole, par, flags,
                 n_ion, n_neu, seed_offset=0, record_depth_every=0, max_seconds=None, steps=None,
                 stage_times=None, reinit_method="fsm", extend="gpu", surf_smooth=0.0):
-    """run_etch_3d (threed.py:1643-1795) with the oracle's stages (coverage-coupled MC path or
-    radiosity neutrals, FSM reinit, nearest-face extension).  Runs `steps` (default n_steps) steps of the n_steps
+    """run_etch_3d (threed.py:1643-1795) with the oracle's stages (coverage-coupled MC path,
+    radiosity or DDA neutrals, FSM reinit, nearest-face extension).  Runs `steps` (default n_steps) steps of the n_steps
     schedule.  Returns (phi, depth_history, stats); stage_times (list) receives one dict of stage
     seconds per step."""
     nx, ny, nz = int(round(Lx / dx)), int(round(Ly / dx)), int(round(Lz / dx))
@@ -697,6 +835,9 @@ def run_etch_3d(Lx, Ly, Lz, dx, trench_width, mask_th, sub_top, t_end, n_steps, 
         if getattr(flags, "neutral_transport", "mc") == "radiosity":
             m_i, m_F, m_O, cos_i, iy = flux_radiosity(mesh, geo, phi, par, flags, n_ion,
                                                       step + seed_offset, tt=st)
+        elif getattr(flags, "neutral_transport", "mc") == "dda":
+            m_i, m_F, m_O, cos_i, iy = flux_dda(mesh, geo, phi, par, flags, n_ion,
+                                                step + seed_offset, tt=st)
         else:
             bi = None
             if warm and prev is not None:

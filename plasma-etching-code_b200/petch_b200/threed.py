@@ -196,7 +196,7 @@ def chem_params(par, flags):
 
 def _unsupported(flags, par):
     nt = getattr(flags, "neutral_transport", "mc")
-    if nt in ("knudsen", "dda"):
+    if nt == "knudsen":
         raise NotImplementedError(f"neutral_transport={nt!r} is outside this engine's scope")
     if getattr(flags, "surface_charging", False) or getattr(flags, "floor_charge_throttle", False):
         raise NotImplementedError("surface charging models are outside this engine's scope")
@@ -245,6 +245,7 @@ class FluxEngine:
         self.V = torch.empty(MT, **dev)
         self.tmp5 = torch.empty(5 * MT, **dev)
         self.rad = None           # radiosity buffers, allocated on first use
+        self.dda = None           # DDA solver and its normals, allocated on first use
 
     def grow(self, need):
         MT = max(int(need * 1.5), 2 * self.MT)
@@ -362,14 +363,11 @@ class FluxEngine:
             self.rad = r
         return r
 
-    def flux_radiosity(self, phi, n_ion, seed, n_ff=64, n_fp=4, n_iter=40):
-        """mc_flux_3d_radiosity (threed.py:923-991) on the device: ions as _ions_deterministic
-        (unsmoothed), into-gas normals from phi, n_ff form-factor rays per face, the CSR form
-        factor matrix, then n_fp rounds of the two-species Jacobi solve and the Belen coverage
-        update, starting from bare = 1."""
+    def _ions_deterministic(self, n_ion, seed):
+        """_ions_deterministic (threed.py:994-1029), the ion launch of the deterministic-neutral
+        paths (radiosity, DDA): faithful ViennaPS reflection (yields, m_i, cos_i, unsmoothed) or
+        the legacy first-hit ion (m_i clipped at 1.5).  Returns the yield pointers (or Nones)."""
         par, flags, m = self.par, self.flags, self.mesh
-        if par.get('radiosity_solver', 'jacobi') != 'jacobi':
-            raise NotImplementedError("only the Jacobi radiosity solver is provided")
         s = _sp()
         A_src = float(self.geo['Lx'] * self.geo['Ly'])
         work = self.small[0:6]
@@ -397,6 +395,19 @@ class FluxEngine:
                       self.tmp5.data_ptr(), self.tmp5[m.MT:].data_ptr(), s)
             yields = (None, None, None)
         self.ktimer.stop("k_ions")
+        return yields
+
+    def flux_radiosity(self, phi, n_ion, seed, n_ff=64, n_fp=4, n_iter=40):
+        """mc_flux_3d_radiosity (threed.py:923-991) on the device: ions as _ions_deterministic
+        (unsmoothed), into-gas normals from phi, n_ff form-factor rays per face, the CSR form
+        factor matrix, then n_fp rounds of the two-species Jacobi solve and the Belen coverage
+        update, starting from bare = 1."""
+        par, flags, m = self.par, self.flags, self.mesh
+        if par.get('radiosity_solver', 'jacobi') != 'jacobi':
+            raise NotImplementedError("only the Jacobi radiosity solver is provided")
+        s = _sp()
+        work = self.small[0:6]
+        yields = self._ions_deterministic(n_ion, seed)
         r = self._radiosity_buffers(n_ff)
         nx, ny, nz = phi.shape
         _lib.call("petch_gas_normals", m.id, m.MT, m.MV, phi.data_ptr(), nx, ny, nz,
@@ -427,6 +438,53 @@ class FluxEngine:
                       betaE, betaO, int(n_iter), self.m_F.data_ptr(), self.m_O.data_ptr(),
                       r['work2'].data_ptr(), s)
             self.ktimer.stop("k_rad_solve")
+            _lib.call("petch_belen_bare", m.id, m.MT, m.MV, ctypes.byref(self.chem),
+                      self.m_i.data_ptr(), self.m_F.data_ptr(), self.m_O.data_ptr(),
+                      self.cos_i.data_ptr(), yields[1], yields[2], self.bare.data_ptr(), s)
+
+
+    def flux_dda(self, phi, n_ion, seed, n_fp=4):
+        """mc_flux_3d_dda (threed.py:1211-1244) on the device: ions as _ions_deterministic, the
+        into-gas normals, the DDA rays marched once for this mesh, then n_fp rounds of the
+        two-species DDA solve (par dda_n_dir directions per hemisphere, dda_n_reemit passes) and
+        the Belen coverage update, starting from bare = 1."""
+        yields = self._ions_deterministic(n_ion, seed)
+        self.dda_prepare(phi)
+        self.dda_fixed_point(yields, n_fp)
+        self.yields = yields
+
+    def dda_prepare(self, phi):
+        """Into-gas normals and the DDA march for the current mesh on the level set phi."""
+        from .dda import DDASolver
+        m = self.mesh
+        s = _sp()
+        n_dir = int(self.par.get('dda_n_dir', 64))
+        shape = tuple(phi.shape)
+        if self.dda is None or not self.dda[0].fits(m.MT, shape, n_dir):
+            self.dda = (DDASolver(m.MT, shape, n_dir), torch.empty((m.MT, 3), device="cuda"))
+        solver, fn = self.dda
+        nx, ny, nz = shape
+        dx = float(self.geo['dx'])
+        _lib.call("petch_gas_normals", m.id, m.MT, m.MV, phi.data_ptr(), nx, ny, nz, dx,
+                  fn.data_ptr(), s)
+        self.ktimer.start("k_dda_march")
+        solver.prepare(phi, dx, m.id, m.centroid, fn, m.area, int(self.par.get('periodic_y', 0)),
+                       stream=s)
+        self.ktimer.stop("k_dda_march")
+
+    def dda_fixed_point(self, yields, n_fp=4):
+        """The coverage <-> DDA fixed point (threed.py:1234-1243) on the prepared rays (m_i,
+        cos_i and the yields must be in place)."""
+        m = self.mesh
+        s = _sp()
+        solver = self.dda[0]
+        n_re = int(self.par.get('dda_n_reemit', 12))
+        betaE, betaO = float(self.par.get('betaE', 0.7)), float(self.par.get('betaO', 1.0))
+        self.bare.fill_(1.0)
+        for _ in range(n_fp):
+            self.ktimer.start("k_dda_solve")
+            solver.solve(self.bare, betaE, betaO, n_re, self.m_F, self.m_O, stream=s)
+            self.ktimer.stop("k_dda_solve")
             _lib.call("petch_belen_bare", m.id, m.MT, m.MV, ctypes.byref(self.chem),
                       self.m_i.data_ptr(), self.m_F.data_ptr(), self.m_O.data_ptr(),
                       self.cos_i.data_ptr(), yields[1], yields[2], self.bare.data_ptr(), s)
@@ -633,6 +691,8 @@ def run_etch_3d(Lx=10.0, Ly=4.0, Lz=14.0, dx=0.4, trench_width=4.0, mask_th=2.0,
         st_timer.start("flux")
         if nt == "radiosity":
             eng.flux_radiosity(eng.phi, n_ion_s, seed)
+        elif nt == "dda":
+            eng.flux_dda(eng.phi, n_ion_s, seed)
         elif coupled:
             eng.flux_coupled(n_ion_s, n_neu_s, seed, warm)
         else:
@@ -671,7 +731,7 @@ def run_etch_3d(Lx=10.0, Ly=4.0, Lz=14.0, dx=0.4, trench_width=4.0, mask_th=2.0,
             st_timer.stop("reinit")
         if surf_smooth and surf_smooth > 0.0:
             eng.smooth(float(surf_smooth))
-        eng.end_step(warm and coupled and nt != "radiosity")
+        eng.end_step(warm and coupled and nt not in ("radiosity", "dda"))
         st['nsub'] = nsub
         if record_depth_every and (step % record_depth_every == 0 or step == n_steps - 1):
             g2 = _host_geo(geo, eng.phi)
@@ -819,6 +879,23 @@ def mc_flux_3d_radiosity(mesh, verts, faces, centroids, areas, geo, par, n_ion=2
     phi = (phi if isinstance(phi, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(phi)))
     phi = phi.to("cuda", torch.float32).contiguous()
     fe.flux_radiosity(phi, int(n_ion), int(seed), n_ff=int(n_ff), n_fp=int(n_fp))
+    _raise_trace_errors(fe)
+    _set_ion_yield(fe, par, F)
+    return _host(fe.m_i, F), _host(fe.m_F, F), _host(fe.m_O, F), _host(fe.cos_i, F)
+
+
+def mc_flux_3d_dda(mesh, verts, faces, centroids, areas, geo, par, n_ion=20000, seed=0,
+                   flags=None, n_fp=4):
+    """mc_flux_3d_dda (threed.py:1211-1244) on a DeviceMesh: returns numpy (m_i, m_F, m_O,
+    cos_i) and sets or clears par['_ion_yield'] like the reference.  geo['phi'] (host or device)
+    is the level set the mesh was extracted from; verts / faces / centroids / areas describe the
+    same mesh and are not read."""
+    F = mesh.n_faces()
+    fe = _flux_engine(mesh, geo, par, flags)
+    phi = geo['phi']
+    phi = (phi if isinstance(phi, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(phi)))
+    phi = phi.to("cuda", torch.float32).contiguous()
+    fe.flux_dda(phi, int(n_ion), int(seed), n_fp=int(n_fp))
     _raise_trace_errors(fe)
     _set_ion_yield(fe, par, F)
     return _host(fe.m_i, F), _host(fe.m_F, F), _host(fe.m_O, F), _host(fe.cos_i, F)

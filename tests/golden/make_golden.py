@@ -4,7 +4,7 @@ warp-lang replaced by warp_shim.py (a CPU stand-in: see its docstring for what i
 
 Run in a checkout that has the reference at /root/reference (or $PETCH_REFERENCE):
 
-    python tests/golden/make_golden.py [group ...]   # groups: levelset surface flux radiosity options redep
+    python tests/golden/make_golden.py [group ...]   # groups: levelset surface flux radiosity options redep dda
 
 The fixtures are committed; tests read only the .npz files, never the reference.
 """
@@ -387,8 +387,94 @@ def redep():
     np.savez_compressed(os.path.join(HERE, "redep.npz"), **out)
 
 
+def dda():
+    """The DDA neutral transport (petch/dda.py, wired as mc_flux_3d_dda, threed.py:1211-1244) run
+    unmodified on small meshes: single launches of _dda_gather_kernel (the direct view with a zero
+    re-emission field, and one pass over a random re-emission field), dda_neutral_flux for a random
+    sticking field at several direction / iteration counts, and mc_flux_3d_dda itself with its
+    ion results recorded so the deterministic part can be replayed."""
+    import petch.dda as dda_mod
+    out = {}
+    wp = t3.wp
+    rng = np.random.default_rng(77)
+    for key, hole in (("hole", True), ("trench", False)):
+        m, geo, phi = _small_mesh(hole, nx=10, ny=10, nz=14, dx=0.3)
+        nx, ny, nz = phi.shape
+        dx = geo['dx']
+        periodic = 0 if hole else 1
+        verts = m.verts.astype(np.float32)
+        faces = m.faces
+        v64 = verts.astype(np.float64)[faces]
+        centroids = v64.mean(axis=1)
+        areas = 0.5 * np.linalg.norm(np.cross(v64[:, 1] - v64[:, 0], v64[:, 2] - v64[:, 0]),
+                                     axis=1)
+        geo = dict(geo, phi=phi.astype(np.float64))
+        fn = t3._gas_normals(verts, faces, centroids, geo)
+        F = len(faces)
+        out[f"{key}_verts"], out[f"{key}_faces"], out[f"{key}_phi"] = verts, faces, phi
+        out[f"{key}_centroids"], out[f"{key}_areas"], out[f"{key}_gas_normals"] = (
+            centroids, areas, fn)
+        out[f"{key}_geo"] = np.array([geo['Lx'], geo['Ly'], geo['Lz'], dx, periodic])
+        zs = geo['zs']
+        z_top = zs[-1] - 0.5 * dx
+        max_steps = (int((z_top - zs[0]) / dx) + 4) * (3 if periodic else 1)
+
+        # single launches of the gather kernel with the 128-direction sphere (dda_n_dir = 64)
+        dirs, w = dda_mod.fib_sphere(128)
+        out[f"{key}_dirs"] = dirs
+        remit = np.zeros(nx * ny * nz)
+        solid = (phi > 0).ravel()
+        remit[solid] = rng.uniform(0.0, 1.0, int(solid.sum()))
+        out[f"{key}_remit"] = remit
+
+        def gather(rem, src):
+            o = wp.zeros(F, dtype=wp.float32)
+            wp.launch(dda_mod._dda_gather_kernel, dim=F,
+                      inputs=[wp.array(np.ascontiguousarray(phi, dtype=np.float32)),
+                              wp.array(centroids.astype(np.float32), dtype=wp.vec3),
+                              wp.array(fn.astype(np.float32), dtype=wp.vec3),
+                              wp.array(dirs.astype(np.float32), dtype=wp.vec3),
+                              wp.array(w.astype(np.float32)),
+                              wp.array(rem.astype(np.float32)), float(dx), float(z_top),
+                              float(src), int(max_steps), nx, ny, nz, periodic, o])
+            return o.numpy().astype(np.float64)
+
+        t0 = time.time()
+        out[f"{key}_direct"] = gather(np.zeros(nx * ny * nz), 1.0)
+        out[f"{key}_remit_pass"] = gather(remit, 0.0)
+        print(f"  {key} gathers: {time.time() - t0:.1f}s", flush=True)
+
+        # dda_neutral_flux for a random sticking field
+        s_face = rng.uniform(0.05, 1.0, F)
+        out[f"{key}_s_face"] = s_face
+        for n_dir, n_re in ((16, 12), (8, 1), (8, 2), (8, 5)):
+            t0 = time.time()
+            out[f"{key}_flux_{n_dir}_{n_re}"] = dda_mod.dda_neutral_flux(
+                phi, dx, zs, centroids, fn, s_face, n_dir=n_dir, n_reemit=n_re,
+                face_areas=np.maximum(areas, 1e-9), periodic_y=periodic)
+            print(f"  {key} dda_neutral_flux({n_dir}, {n_re}): {time.time() - t0:.1f}s",
+                  flush=True)
+
+        # mc_flux_3d_dda: faithful ions, 16 directions, 12 re-emission passes, 4 coverage rounds
+        mesh = wp.Mesh(points=wp.array(verts, dtype=wp.vec3),
+                       indices=wp.array(faces.flatten(), dtype=wp.int32))
+        par = dict(t3.PAR, periodic_y=periodic, dda_n_dir=8, dda_n_reemit=12)
+        flags = t3.DEFAULT_FLAGS.__class__(chemistry="belen", yield_angular="viennaps",
+                                           ion_reflection=True, coverage_sticking=True,
+                                           neutral_transport="dda")
+        p = dict(par)
+        t0 = time.time()
+        m_i, m_F, m_O, cos_i = t3.mc_flux_3d_dda(mesh, verts, faces, centroids, areas, geo, p,
+                                                 n_ion=3000, seed=100, flags=flags)
+        print(f"  {key} mc_flux_3d_dda: {time.time() - t0:.1f}s", flush=True)
+        out[f"{key}_m_i"], out[f"{key}_cos_i"] = m_i, cos_i
+        out[f"{key}_m_F"], out[f"{key}_m_O"] = m_F, m_O
+        out[f"{key}_ion_yield"] = np.stack(p['_ion_yield'])
+    np.savez_compressed(os.path.join(HERE, "dda.npz"), **out)
+
+
 GROUPS = {"levelset": levelset, "surface": surface, "flux": flux, "radiosity": radiosity,
-          "options": options, "redep": redep}
+          "options": options, "redep": redep, "dda": dda}
 
 if __name__ == "__main__":
     for g in (sys.argv[1:] or list(GROUPS)):
