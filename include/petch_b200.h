@@ -454,6 +454,62 @@ int petch_dda_solve(int max_faces, int nx, int ny, int nz, int n_dirs, const flo
                     double betaE, double betaO, int n_reemit, void* scratch,
                     long long scratch_bytes, float* flux_E, float* flux_O, void* stream);
 
+/* ---- Knudsen 1-D conductance tail (mc_flux_3d_knudsen, petch/threed.py:1149-1208) ----
+ * petch_knudsen_prepare replaces slice_geometry (petch/knudsen.py:29-68) and the per-face part of
+ * knudsen_face_flux (knudsen.py:188-241) that depends only on the geometry: per z-slice below
+ * sub_top the gas area and perimeter of phi (hole; trench = 1: mean open x-width and 2), the
+ * chain of valid slices with their conductances, each face's slice (its rounded centroid height,
+ * snapped to the nearest valid slice), and the floor faces (into-gas n_z > 0.7, below sub_top,
+ * within half_width + 2 dx of the axis (cx, cy); half_width < 0: no footprint filter) grouped by
+ * slice.  Faces: n_faces a DEVICE int (clamped to max_faces), centroids / normals float[3 * max_faces].
+ * petch_knudsen_solve runs one coverage round for both sticking fields
+ * s = clip(bare' * betaE / betaO, 0, 1), bare' = min(bare, mean of bare over the open-field faces)
+ * when sink_field != 0 (knudsen_sink = 'field'): the slice sinks 0.25 s A (per unit length Ly for a
+ * trench), the conductance chain (conductance_profile, knudsen.py:91-150) with loss scale
+ * wall_loss_scale, or, front_loss != 0, the passivation-linked per-slice scale of
+ * _front_loss_scale (knudsen.py:165-185; W the feature width), and writes flux_E / flux_O
+ * (float[max_faces]).  petch_knudsen_profile solves the chain of the prepared geometry for a
+ * caller's sink slice_loss (double[nz], device) and loss scale (loss_scale double[nz] device, or
+ * NULL for the scalar) into profile (double[nz], device); petch_knudsen_slices copies out the slice
+ * areas and perimeters. */
+int petch_knudsen_scratch_bytes(int max_faces, int nz, long long* bytes);
+int petch_knudsen_prepare(const float* phi, int nx, int ny, int nz, double dx, double sub_top,
+                          int trench, const int* n_faces, int max_faces, const float* centroids,
+                          const float* normals, double cx, double cy, double half_width,
+                          void* scratch, long long scratch_bytes, void* stream);
+int petch_knudsen_solve(int max_faces, int nz, const float* bare, const float* areas, double betaE,
+                        double betaO, int sink_field, double Ly, double wall_loss_scale,
+                        int front_loss, double W, double band_W, double pass_frac, double ar_pass,
+                        void* scratch, long long scratch_bytes, float* flux_E, float* flux_O,
+                        void* stream);
+int petch_knudsen_profile(int max_faces, int nz, const double* slice_loss, const double* loss_scale,
+                          double wall_loss_scale, void* scratch, long long scratch_bytes,
+                          double* profile, void* stream);
+int petch_knudsen_slices(int max_faces, int nz, const void* scratch, long long scratch_bytes,
+                         double* area, double* perimeter, void* stream);
+
+/* ---- floor-charging hooks (_apply_hg_charging, petch/threed.py:1046-1110;
+ * _apply_floor_charge_throttle, :1112-1147) ----
+ * Face classes: in the feature = within `band` of the axis (hole: hypot(x - cx, y - cy); trench:
+ * |x - cx|) and below sub_top; floor = in the feature with into-gas n_z > 0.7.
+ * petch_charging_floor_stats writes stats (double[5], device): floor faces, the lowest floor
+ * centroid z, sum of m_i A over the floor (m_i may be NULL: 0), and the count and summed area of the
+ * foot (in the feature, n_z <= 0.7, z <= that lowest z + foot_h).  petch_charging_apply multiplies
+ * the floor's m_i, y_sp, y_ie, y_p by q4[0..3] and adds add3[0..2] to y_sp, y_ie, y_p of the
+ * non-floor in-feature faces with z <= z_foot (q4, add3: HOST arrays; any of the float arrays may
+ * be NULL).  petch_zero_below zeroes values[f] where the centroid z <= z_top (run_etch_3d's
+ * redeposition foot cleaning, threed.py:1733-1741). */
+int petch_charging_floor_stats(const int* n_faces, int max_faces, const float* centroids,
+                               const float* normals, const float* areas, const float* m_i,
+                               double cx, double cy, double band, int hole, double sub_top,
+                               double foot_h, double* stats, void* stream);
+int petch_charging_apply(const int* n_faces, int max_faces, const float* centroids,
+                         const float* normals, double cx, double cy, double band, int hole,
+                         double sub_top, const double* q4, const double* add3, double z_foot,
+                         float* m_i, float* y_sp, float* y_ie, float* y_p, void* stream);
+int petch_zero_below(const int* n_faces, int max_faces, const float* centroids, double z_top,
+                     float* values, void* stream);
+
 /* ---- recipe gradient: tangent (forward-mode) versions of the step's stages ----
  * No reference counterpart (the reference has no loop gradient).  Each call computes the
  * primal result exactly as its plain counterpart and the derivatives of it along 3 directions

@@ -410,10 +410,11 @@ def surface_rate(m_i, m_F, m_O, cos_i, is_mask, par, chemistry, yield_angular, i
     return V
 
 
-def flux_coupled(mesh, geo, par, flags, n_ion, n_neu, seed, bare_init=None, tt=None):
-    """mc_flux_3d_coupled (faithful-ion / legacy-ion branches, RR neutrals) on the oracle mesh.
-    Returns (m_i, m_F, m_O, cos_i, bare, ion_yield-or-None).  tt: optional dict that accumulates
-    the seconds spent in the ray tracers under key 'trace'."""
+def flux_coupled(mesh, geo, par, flags, n_ion, n_neu, seed, bare_init=None, tt=None, phi=None):
+    """mc_flux_3d_coupled (faithful-ion / legacy-ion branches, RR neutrals, the optional floor
+    throttle) on the oracle mesh.  Returns (m_i, m_F, m_O, cos_i, bare, ion_yield-or-None).  tt:
+    optional dict that accumulates the seconds spent in the ray tracers under key 'trace'; phi:
+    the level set (for the throttle's into-gas normals)."""
     tt = {} if tt is None else tt
     tt.setdefault('trace', 0.0)
 
@@ -443,6 +444,10 @@ def flux_coupled(mesh, geo, par, flags, n_ion, n_neu, seed, bare_init=None, tt=N
                        0.8, seed * 9 + 1, n_ion)
         cos_i = np.where(fi > 0, ai / np.where(fi > 0, fi, 1.0), 0.0)
         m_i = sm(np.clip((fi / A) * (A_src / n_ion), 0.0, 1.5))
+    if getattr(flags, "floor_charge_throttle", False):
+        fn = gas_normals(mesh.verts, mesh.faces, mesh.centroid, phi, geo['dx'])
+        c32 = np.asarray(mesh.verts, np.float32)[mesh.faces].mean(axis=1)
+        m_i, iy = floor_throttle(m_i, iy, c32, fn[:, 2], geo)
     n_fp = int(par.get('n_fp', 1 if bare_init is not None else 4))
     bare = np.ones(mesh.F) if bare_init is None else np.clip(np.asarray(bare_init, float), 0.0, 1.0)
     betaE, betaO = par.get('betaE', 0.7), par.get('betaO', 1.0)
@@ -778,6 +783,267 @@ def flux_dda(mesh, geo, phi, par, flags, n_ion, seed, tt=None):
     return m_i, m_F, m_O, cos_i, iy
 
 
+# ------------------------------- Knudsen tail -------------------------------
+def kn_slice_geometry(phi, zs, dx, sub_top, trench):
+    """slice_geometry (knudsen.py:29-68): per z-slice below sub_top, the gas area and the
+    sidewall perimeter.  Hole: area = gas cells dx^2, perimeter = max(gas/solid cell faces in
+    the slice, 1) dx.  Trench: area = mean open x-width over the y-rows with any gas,
+    perimeter = 2."""
+    gas = np.asarray(phi) < 0.0
+    nz = gas.shape[2]
+    area, perim = np.zeros(nz), np.zeros(nz)
+    for k in np.flatnonzero(np.asarray(zs) < sub_top):
+        g = gas[:, :, k]
+        if trench:
+            w = g.sum(axis=0) * dx
+            w = w[w > 0.0]
+            if w.size:
+                area[k], perim[k] = float(w.mean()), 2.0
+        elif g.any():
+            area[k] = float(g.sum()) * dx * dx
+            nf = np.count_nonzero(g[1:, :] != g[:-1, :]) + np.count_nonzero(g[:, 1:] != g[:, :-1])
+            perim[k] = max(float(nf) * dx, dx)
+    return area, perim
+
+
+def kn_thomas(lower, diag, upper, rhs):
+    """The guarded Thomas algorithm of knudsen.py:71-88."""
+    n = len(diag)
+    if n == 0:
+        return np.zeros(0)
+    b, d = np.array(diag, float), np.array(rhs, float)
+    for i in range(1, n):
+        w = lower[i - 1] / max(b[i - 1], 1.0e-30)
+        b[i] -= w * upper[i - 1]
+        d[i] -= w * d[i - 1]
+    x = np.zeros(n)
+    x[-1] = d[-1] / max(b[-1], 1.0e-30)
+    for i in range(n - 2, -1, -1):
+        x[i] = (d[i] - upper[i] * x[i + 1]) / max(b[i], 1.0e-30)
+    return x
+
+
+def kn_profile(phi, zs, dx, sub_top, trench, slice_loss, loss_scale):
+    """conductance_profile (knudsen.py:91-150): the neutral concentration per slice from the
+    chain of valid slices, opening first: conductance (2/3) r a / dx with r = max(2a/p, dx),
+    harmonic-mean links between adjacent slices, unit concentration through the opening's own
+    conductance, sink loss_scale * slice_loss.  1 outside the chain."""
+    area, perim = kn_slice_geometry(phi, zs, dx, sub_top, trench)
+    valid = (np.asarray(zs) < sub_top) & (area > 0.0) & (perim > 0.0)
+    prof = np.ones(len(area))
+    if not valid.any():
+        return prof
+    idx = np.flatnonzero(valid)[::-1]
+    a, p = area[idx], perim[idx]
+    r = np.maximum(2.0 * a / np.maximum(p, 1.0e-30), dx)
+    cond = (2.0 / 3.0) * r * a / dx
+    ls = np.asarray(loss_scale, float)
+    scale = np.maximum(float(ls), 0.0) if ls.ndim == 0 else np.maximum(ls[idx], 0.0)
+    sink = scale * np.maximum(np.asarray(slice_loss)[idx], 0.0)
+    m = len(idx)
+    diag = np.array(sink, float) * np.ones(m)
+    lower, upper, rhs = np.zeros(max(m - 1, 0)), np.zeros(max(m - 1, 0)), np.zeros(m)
+    diag[0] += cond[0]
+    rhs[0] += cond[0]
+    for i in range(m - 1):
+        g = 0.0
+        if abs(idx[i + 1] - idx[i]) == 1:
+            g = 2.0 * cond[i] * cond[i + 1] / max(cond[i] + cond[i + 1], 1.0e-30)
+        diag[i] += g
+        diag[i + 1] += g
+        upper[i] = -g
+        lower[i] = -g
+    prof[idx] = np.clip(kn_thomas(lower, np.maximum(diag, 1.0e-30), upper, rhs), 0.0, 1.0)
+    return prof
+
+
+def kn_front_scale(zs, sub_top, W, wls, band_W, pass_frac, ar_pass):
+    """_front_loss_scale (knudsen.py:165-185): wls (f + (1 - f) exp(-max(AR - band, 0) / ar))
+    per slice, AR = max(sub_top - z, 0) / W."""
+    ar = np.maximum((sub_top - np.asarray(zs)) / max(W, 1.0e-9), 0.0)
+    g = np.exp(-np.maximum(ar - band_W, 0.0) / max(ar_pass, 1.0e-9))
+    return max(float(wls), 0.0) * (pass_frac + (1.0 - pass_frac) * g)
+
+
+def kn_face_flux(phi, zs, dx, sub_top, trench, centroids, gas_nz, A, Ly, s_face, wls,
+                 center=None, half_width=None, front_loss=False, band_W=8.0, pass_frac=0.5,
+                 ar_pass=15.0):
+    """knudsen_face_flux (knudsen.py:188-241): each face's slice (rounded centroid height,
+    snapped to the nearest valid slice, ties to the lower), the floor faces (into-gas n_z > 0.7)
+    below sub_top inside the footprint add 0.25 s A to their slice's sink (per unit trench
+    length), and every face below sub_top takes its slice's concentration; 1 elsewhere."""
+    zs = np.asarray(zs)
+    nz = np.asarray(phi).shape[2]
+    area, perim = kn_slice_geometry(phi, zs, dx, sub_top, trench)
+    vz = np.flatnonzero((zs < sub_top) & (area > 0.0) & (perim > 0.0))
+    c = np.asarray(centroids, float)
+    iz = np.clip(np.round((c[:, 2] - zs[0]) / dx).astype(int), 0, nz - 1)
+    if vz.size == 0:
+        snap = np.full(len(c), -1)
+    else:
+        pos = np.searchsorted(vz, iz)
+        hi, lo = vz[np.clip(pos, 0, vz.size - 1)], vz[np.clip(pos - 1, 0, vz.size - 1)]
+        snap = np.where(np.abs(hi - iz) < np.abs(lo - iz), hi, lo)
+    below = c[:, 2] < sub_top
+    inside = np.ones(len(c), bool)
+    if center is not None and half_width is not None:
+        band = half_width + 2.0 * dx
+        if trench:
+            inside = np.abs(c[:, 0] - center[0]) <= band
+        else:
+            inside = np.hypot(c[:, 0] - center[0], c[:, 1] - center[1]) <= band
+    loss = np.zeros(nz)
+    sel = below & inside & (snap >= 0) & (np.asarray(gas_nz) > 0.7)
+    if sel.any():
+        np.add.at(loss, snap[sel], 0.25 * (np.clip(np.asarray(s_face, float)[sel], 0.0, 1.0)
+                                           * np.asarray(A, float)[sel]))
+        if trench:
+            loss /= max(float(Ly), 1.0e-30)
+    scale = wls
+    if front_loss:
+        W = 2.0 * float(half_width) if half_width is not None else dx
+        scale = kn_front_scale(zs[:nz], sub_top, W, wls, band_W, pass_frac, ar_pass)
+    prof = kn_profile(phi, zs, dx, sub_top, trench, loss, scale)
+    m = np.ones(len(c))
+    take = (snap >= 0) & below
+    m[take] = prof[snap[take]]
+    return np.clip(m, 0.0, 8.0)
+
+
+# Floor-charging tables (the reference's data, restated): the Hwang-Giapis published values
+# (charging2d.py:1511-1518), petch's own first-principles table (charging_general.py:1038-1041)
+# and the de Boer deep-AR throttle (charging_general.py:1070-1071).
+HG_AR = np.array([0.0, 1.0, 1.2, 1.6, 2.0, 2.6, 3.0, 3.6, 4.0])
+HG_Q = np.array([1.0, 0.59, 0.55, 0.47, 0.40, 0.34, 0.30, 0.26, 0.22])
+HG_VF = np.array([0.0, 8.0, 10.0, 15.0, 19.0, 25.0, 28.0, 31.0, 33.0])
+HG_E = np.array([0.0, 15.0, 16.5, 17.5, 20.0, 23.0, 25.0, 26.5, 27.5])
+PT_AR = np.array([1.0, 2.0, 3.0, 4.0])
+PT_Q = np.array([0.704, 0.491, 0.406, 0.349])
+PT_VF = np.array([9.5, 19.2, 27.7, 34.0])
+PT_E = np.array([16.6, 14.2, 18.8, 21.6])
+TH_AR = np.array([0.0, 1.0, 2.0, 3.0, 4.0, 8.0, 15.0, 25.0])
+TH_Q = np.array([1.0, 0.704, 0.491, 0.406, 0.349, 0.25, 0.60, 0.50])
+
+
+def _footprint_floor(centroids, gas_nz, geo):
+    """The in-feature faces below sub_top (within half the width + 2 dx of the axis) and those
+    of them facing up (n_z > 0.7)."""
+    c = np.asarray(centroids, float)
+    cx0, cy0 = 0.5 * geo['Lx'], 0.5 * geo['Ly']
+    hw = 0.5 * geo['trench_width'] + 2.0 * geo['dx']
+    if geo.get('hole', False):
+        inside = np.hypot(c[:, 0] - cx0, c[:, 1] - cy0) <= hw
+    else:
+        inside = np.abs(c[:, 0] - cx0) <= hw
+    below = c[:, 2] < geo['sub_top']
+    return inside & below, inside & below & (np.asarray(gas_nz) > 0.7)
+
+
+def hg_charging(m_i, iy, par, mode, centroids, gas_nz, A, geo):
+    """_apply_hg_charging (threed.py:1046-1110): returns (m_i, (sp, ie, ip)).  The floor flux
+    keeps the fraction Q(AR) with yields at Emean - V_f; the removed flux lands on the sidewall
+    foot (0.3 W, at least 2 dx, above the deepest floor face) with the yields of E_defl."""
+    if mode not in ("hg", "petch") or iy is None:
+        return m_i, iy
+    feat, floor = _footprint_floor(centroids, gas_nz, geo)
+    if not floor.any():
+        return m_i, iy
+    c = np.asarray(centroids, float)
+    W = geo['trench_width']
+    AR = float(geo['sub_top'] - c[floor, 2].min()) / max(W, 1e-9)
+    tab = (HG_AR, HG_Q, HG_VF, HG_E) if mode == "hg" else (PT_AR, PT_Q, PT_VF, PT_E)
+    Q, Vf, Ed = (float(np.interp(AR, tab[0], t)) for t in tab[1:])
+    sp, ie, ip = (np.array(a, float) for a in iy)
+    y0 = yields(par)
+    yv = yields(dict(par, Emean=max(par['Emean'] - Vf, 0.0)))
+    r = [yv[q] / y0[q] if y0[q] > 0 else 0.0 for q in range(3)]      # (ie, sp, p)
+    defl = float((m_i[floor] * A[floor]).sum()) * (1.0 - Q)
+    ie[floor] *= Q * r[0]
+    sp[floor] *= Q * r[1]
+    ip[floor] *= Q * r[2]
+    m_i = np.array(m_i, float)
+    m_i[floor] *= Q
+    zf = float(c[floor, 2].min())
+    foot = feat & (np.asarray(gas_nz) <= 0.7) & (c[:, 2] <= zf + max(0.3 * W, 2.0 * geo['dx']))
+    if foot.any() and defl > 0.0:
+        fd = defl / max(float(A[foot].sum()), 1e-12)
+        sE = np.sqrt(Ed)
+        ie[foot] += fd * par['A_ie'] * max(sE - np.sqrt(par['Eth_ie']), 0.0)
+        sp[foot] += fd * par['A_sp'] * max(sE - np.sqrt(par['Eth_sp']), 0.0)
+        ip[foot] += fd * par['A_p'] * max(sE - np.sqrt(par['Eth_p']), 0.0)
+    return m_i, (sp, ie, ip)
+
+
+def floor_throttle(m_i, iy, centroids, gas_nz, geo):
+    """_apply_floor_charge_throttle (threed.py:1112-1147): the floor faces' ion flux (and
+    yields) times Q(AR) of the deep-AR throttle table (1 below AR 0, 0.5 above AR 25).  The
+    reference averages the float32 vertices itself, so its depth sub_top - z_min is a float32
+    subtraction (numpy's Python-scalar rule); `centroids` are those float32 means."""
+    _, floor = _footprint_floor(centroids, gas_nz, geo)
+    if not floor.any():
+        return m_i, iy
+    zmin = np.float32(np.asarray(centroids, np.float32)[floor, 2].min())
+    AR = float(np.float32(geo['sub_top']) - zmin) / max(geo['trench_width'], 1e-9)
+    Q = float(np.clip(np.interp(AR, TH_AR, TH_Q, left=1.0, right=float(TH_Q[-1])), 0.0, 1.0))
+    m_i = np.array(m_i, float)
+    m_i[floor] *= Q
+    if iy is not None:
+        iy = tuple(np.array(a, float) for a in iy)
+        for a in iy:
+            a[floor] *= Q
+    return m_i, iy
+
+
+def knudsen_fixed_point(phi, geo, centroids, fn, A, m_i, cos_i, iy, par, flags, n_fp=4):
+    """The coverage <-> Knudsen fixed point of mc_flux_3d_knudsen (threed.py:1184-1207),
+    starting from bare = 1; 'field' sinks clamp bare at the open-field faces' mean."""
+    dx, sub_top = geo['dx'], geo['sub_top']
+    zs = np.arange(np.asarray(phi).shape[2]) * dx
+    trench = not geo.get('hole', False)
+    c = np.asarray(centroids, float)
+    gas_nz = np.asarray(fn)[:, 2]
+    A = np.maximum(A, 1e-9)
+    betaE, betaO = par.get('betaE', 0.7), par.get('betaO', 1.0)
+    wls = float(par.get('knudsen_wall_loss_scale', 1.85))
+    kw = dict(center=(0.5 * geo['Lx'], 0.5 * geo['Ly']),
+              half_width=0.5 * float(geo.get('trench_width', geo['Lx'])),
+              front_loss=bool(getattr(flags, 'knudsen_front_loss', False)),
+              band_W=float(par.get('knudsen_front_band_W', 8.0)),
+              pass_frac=float(par.get('knudsen_passive_frac', 0.5)),
+              ar_pass=float(par.get('knudsen_front_ar_pass', 15.0)))
+    ya = getattr(flags, "yield_angular", "cosine")
+    field = c[:, 2] > sub_top - 0.5 * dx
+    bare = np.ones(len(c))
+    m_F = m_O = np.zeros(len(c))
+    for _ in range(n_fp):
+        sb = bare
+        if par.get('knudsen_sink', 'local') == 'field' and field.any():
+            sb = np.minimum(bare, float(np.mean(bare[field])))
+        m_F = kn_face_flux(phi, zs, dx, sub_top, trench, c, gas_nz, A, geo['Ly'],
+                           np.clip(sb * betaE, 0.0, 1.0), wls, **kw)
+        m_O = kn_face_flux(phi, zs, dx, sub_top, trench, c, gas_nz, A, geo['Ly'],
+                           np.clip(sb * betaO, 0.0, 1.0), wls, **kw)
+        thF, thO = belen_coverages(m_i, m_F, m_O, cos_i, par, ya, iy)
+        bare = np.clip(1.0 - thF - thO, 0.0, 1.0)
+    return m_F, m_O
+
+
+def flux_knudsen(mesh, geo, phi, par, flags, n_ion, seed, tt=None):
+    """mc_flux_3d_knudsen (threed.py:1149-1208) on the oracle mesh: (m_i, m_F, m_O, cos_i,
+    ion_yield-or-None), with the floor-charging closure for surface_charging hg / petch."""
+    tt = {} if tt is None else tt
+    tt.setdefault('trace', 0.0)
+    t0 = time.time()
+    m_i, cos_i, iy = radiosity_ions(mesh, geo, par, flags, n_ion, seed)
+    tt['trace'] += time.time() - t0
+    fn = gas_normals(mesh.verts, mesh.faces, mesh.centroid, phi, geo['dx'])
+    A = np.maximum(mesh.area, 1e-9)
+    m_i, iy = hg_charging(m_i, iy, par, getattr(flags, "surface_charging", False),
+                          mesh.centroid, fn[:, 2], A, geo)
+    m_F, m_O = knudsen_fixed_point(phi, geo, mesh.centroid, fn, A, m_i, cos_i, iy, par, flags)
+    return m_i, m_F, m_O, cos_i, iy
+
+
 # ------------------------------- the loop -------------------------------
 def depth3d(geo, phi, half=1.0):
     """_depth3d (threed.py:1798-1834)."""
@@ -838,6 +1104,9 @@ def run_etch_3d(Lx, Ly, Lz, dx, trench_width, mask_th, sub_top, t_end, n_steps, 
         elif getattr(flags, "neutral_transport", "mc") == "dda":
             m_i, m_F, m_O, cos_i, iy = flux_dda(mesh, geo, phi, par, flags, n_ion,
                                                 step + seed_offset, tt=st)
+        elif getattr(flags, "neutral_transport", "mc") == "knudsen":
+            m_i, m_F, m_O, cos_i, iy = flux_knudsen(mesh, geo, phi, par, flags, n_ion,
+                                                    step + seed_offset, tt=st)
         else:
             bi = None
             if warm and prev is not None:
@@ -845,7 +1114,7 @@ def run_etch_3d(Lx, Ly, Lz, dx, trench_width, mask_th, sub_top, t_end, n_steps, 
                 q = pm.nearest(mesh.centroid.astype(np.float32).astype(np.float64))
                 bi = np.where(q >= 0, pb[np.maximum(q, 0)], 1.0)
             m_i, m_F, m_O, cos_i, bare, iy = flux_coupled(mesh, geo, par, flags, n_ion, n_neu,
-                                                          step + seed_offset, bi, tt=st)
+                                                          step + seed_offset, bi, tt=st, phi=phi)
             prev = (mesh, bare)
         V = surface_rate(m_i, m_F, m_O, cos_i, mesh.fmask, par,
                          getattr(flags, "chemistry", "langmuir"),

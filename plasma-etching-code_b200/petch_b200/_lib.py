@@ -97,6 +97,14 @@ SIGNATURES = {
     "petch_dda_scratch_bytes": [I, I, I, I, I, LLP],
     "petch_dda_prepare": [P, I, I, I, D, D, I, I, P, I, P, P, P, P, P, I, P, L, P],
     "petch_dda_solve": [I, I, I, I, I, P, D, D, I, P, L, P, P, P],
+    "petch_knudsen_scratch_bytes": [I, I, LLP],
+    "petch_knudsen_prepare": [P, I, I, I, D, D, I, P, I, P, P, D, D, D, P, L, P],
+    "petch_knudsen_solve": [I, I, P, P, D, D, I, D, D, I, D, D, D, D, P, L, P, P, P],
+    "petch_knudsen_profile": [I, I, P, P, D, P, L, P, P],
+    "petch_knudsen_slices": [I, I, P, L, P, P, P],
+    "petch_charging_floor_stats": [P, I, P, P, P, P, D, D, D, I, D, D, P, P],
+    "petch_charging_apply": [P, I, P, P, D, D, D, I, D, P, P, D, P, P, P, P, P],
+    "petch_zero_below": [P, I, P, D, P, P],
     "petch_extend_velocity_centroid": [P, I, I, P, P, I, I, I, D, D, P, P, I, P, P, I, P, P],
     "petch_reinit_pde": [P, P, P, P, I, I, I, D, I, P],
     "petch_gaussian_smooth": [P, P, P, P, P, I, I, I, D, D, P],

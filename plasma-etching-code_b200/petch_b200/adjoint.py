@@ -198,6 +198,8 @@ def run_etch_3d_tangent(theta, Lx, Ly, Lz, dx, trench_width, mask_th, sub_top, t
     if getattr(flags, "neutral_transport", "mc") != "mc" or getattr(flags, "redeposition", False):
         raise NotImplementedError("the recipe gradient follows Monte-Carlo neutrals without "
                                   "redeposition")
+    if getattr(flags, "floor_charge_throttle", False):
+        raise NotImplementedError("the recipe gradient does not include the floor-charging throttle")
     torch.cuda.init()
     geo = make_trench_3d(Lx, Ly, Lz, dx, trench_width, mask_th, sub_top, hole=hole, host=False)
     geo['mask_th'] = mask_th

@@ -82,7 +82,7 @@ class BatchEngine:
                 and getattr(flags, "chemistry", "langmuir") == "belen"):
             raise NotImplementedError("the batched step runs the coverage-coupled SF6/O2 path with "
                                       "faithful ions (belen, ion_reflection, coverage_sticking)")
-        for flag in ("redeposition",):
+        for flag in ("redeposition", "floor_charge_throttle"):
             if getattr(flags, flag, False):
                 raise NotImplementedError(f"{flag} is not part of the batched step")
         if getattr(flags, "neutral_transport", "mc") != "mc":

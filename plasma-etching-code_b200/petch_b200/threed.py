@@ -196,14 +196,13 @@ def chem_params(par, flags):
 
 def _unsupported(flags, par):
     nt = getattr(flags, "neutral_transport", "mc")
-    if nt == "knudsen":
-        raise NotImplementedError(f"neutral_transport={nt!r} is outside this engine's scope")
-    if getattr(flags, "surface_charging", False) or getattr(flags, "floor_charge_throttle", False):
-        raise NotImplementedError("surface charging models are outside this engine's scope")
+    if (getattr(flags, "surface_charging", False) and par.get('charge_alpha', 0.0) > 0.0
+            and nt not in ("radiosity", "dda", "knudsen")
+            and getattr(flags, "coverage_sticking", False)):
+        raise NotImplementedError("the electron-shadowing charging model (charge_alpha > 0) is "
+                                  "outside this engine's scope")
     if par.get('cov_transport', 'rr') != 'rr':
         raise NotImplementedError("only the Russian-roulette coverage transport (cov_transport='rr')")
-    if par.get('charge_alpha', 0.0) > 0.0 and getattr(flags, "surface_charging", False):
-        raise NotImplementedError("surface charging models are outside this engine's scope")
 
 
 # --------------------------------------------------------------------------------------------
@@ -245,17 +244,21 @@ class FluxEngine:
         self.V = torch.empty(MT, **dev)
         self.tmp5 = torch.empty(5 * MT, **dev)
         self.rad = None           # radiosity buffers, allocated on first use
-        self.dda = None           # DDA solver and its normals, allocated on first use
+        self.dda = None           # DDA solver, allocated on first use
+        self.kn = None            # Knudsen solver, allocated on first use
+        self.fn = None            # into-gas normals, allocated on first use
 
     def grow(self, need):
         MT = max(int(need * 1.5), 2 * self.MT)
         self._alloc_faces(MT)
 
     # ---- flux stages ----
-    def flux_coupled(self, n_ion, n_neu, seed, warm, bare_init=None):
+    def flux_coupled(self, n_ion, n_neu, seed, warm, bare_init=None, phi=None):
         """mc_flux_3d_coupled (threed.py:740-905) on the device.  The coverage starts from the
         previous step's (warm, nearest face) or from bare_init (a device float[F] the caller
-        supplies), else cold at 1."""
+        supplies), else cold at 1.  flags.floor_charge_throttle scales the floor's ion results
+        before the fixed point (_apply_floor_charge_throttle); it needs the level set phi (the
+        engine's own when not given)."""
         par, flags, m = self.par, self.flags, self.mesh
         s = _sp()
         A_src = float(self.geo['Lx'] * self.geo['Ly'])
@@ -297,6 +300,13 @@ class FluxEngine:
                       float(A_src / n_ion), 0.0, 1.5, 1, n_smooth, alpha, self.m_i.data_ptr(),
                       self.tmp5.data_ptr(), self.tmp5[m.MT:].data_ptr(), s)
             yields = (None, None, None)
+        if flags is not None and getattr(flags, "floor_charge_throttle", False):
+            from .charging import apply_floor_throttle
+            phi = phi if phi is not None else getattr(self, "phi", None)
+            if phi is None:
+                raise ValueError("floor_charge_throttle needs the level set the mesh came from")
+            self.yields = yields
+            self.charging = apply_floor_throttle(self, self.gas_normals(phi))
         n_fp = int(par.get('n_fp', 1 if seeded else 4))
         if not seeded:
             self.bare.fill_(1.0)
@@ -453,6 +463,17 @@ class FluxEngine:
         self.dda_fixed_point(yields, n_fp)
         self.yields = yields
 
+    def gas_normals(self, phi):
+        """_gas_normals (threed.py:1553-1568) of the current mesh on the level set phi, into a
+        [MT, 3] device buffer of the engine."""
+        m = self.mesh
+        if self.fn is None or self.fn.shape[0] != m.MT:
+            self.fn = torch.empty((m.MT, 3), device="cuda")
+        nx, ny, nz = phi.shape
+        _lib.call("petch_gas_normals", m.id, m.MT, m.MV, phi.data_ptr(), nx, ny, nz,
+                  float(self.geo['dx']), self.fn.data_ptr(), _sp())
+        return self.fn
+
     def dda_prepare(self, phi):
         """Into-gas normals and the DDA march for the current mesh on the level set phi."""
         from .dda import DDASolver
@@ -460,13 +481,11 @@ class FluxEngine:
         s = _sp()
         n_dir = int(self.par.get('dda_n_dir', 64))
         shape = tuple(phi.shape)
-        if self.dda is None or not self.dda[0].fits(m.MT, shape, n_dir):
-            self.dda = (DDASolver(m.MT, shape, n_dir), torch.empty((m.MT, 3), device="cuda"))
-        solver, fn = self.dda
-        nx, ny, nz = shape
+        if self.dda is None or not self.dda.fits(m.MT, shape, n_dir):
+            self.dda = DDASolver(m.MT, shape, n_dir)
+        solver = self.dda
+        fn = self.gas_normals(phi)
         dx = float(self.geo['dx'])
-        _lib.call("petch_gas_normals", m.id, m.MT, m.MV, phi.data_ptr(), nx, ny, nz, dx,
-                  fn.data_ptr(), s)
         self.ktimer.start("k_dda_march")
         solver.prepare(phi, dx, m.id, m.centroid, fn, m.area, int(self.par.get('periodic_y', 0)),
                        stream=s)
@@ -477,7 +496,7 @@ class FluxEngine:
         cos_i and the yields must be in place)."""
         m = self.mesh
         s = _sp()
-        solver = self.dda[0]
+        solver = self.dda
         n_re = int(self.par.get('dda_n_reemit', 12))
         betaE, betaO = float(self.par.get('betaE', 0.7)), float(self.par.get('betaO', 1.0))
         self.bare.fill_(1.0)
@@ -485,6 +504,58 @@ class FluxEngine:
             self.ktimer.start("k_dda_solve")
             solver.solve(self.bare, betaE, betaO, n_re, self.m_F, self.m_O, stream=s)
             self.ktimer.stop("k_dda_solve")
+            _lib.call("petch_belen_bare", m.id, m.MT, m.MV, ctypes.byref(self.chem),
+                      self.m_i.data_ptr(), self.m_F.data_ptr(), self.m_O.data_ptr(),
+                      self.cos_i.data_ptr(), yields[1], yields[2], self.bare.data_ptr(), s)
+
+
+    def flux_knudsen(self, phi, n_ion, seed, n_fp=4):
+        """mc_flux_3d_knudsen (threed.py:1149-1208) on the device: ions as _ions_deterministic,
+        the floor-charging closure for flags.surface_charging = "hg" / "petch" (_apply_hg_charging),
+        then n_fp rounds of the two-species Knudsen solve and the Belen coverage update, starting
+        from bare = 1."""
+        from .charging import apply_hg_charging
+        yields = self._ions_deterministic(n_ion, seed)
+        self.yields = yields
+        fn = self.gas_normals(phi)
+        self.charging = apply_hg_charging(self, fn, getattr(self.flags, "surface_charging", False))
+        self.knudsen_prepare(phi, fn)
+        self.knudsen_fixed_point(yields, n_fp)
+
+    def knudsen_prepare(self, phi, fn):
+        """Slice geometry of phi and the per-face slice data of the current mesh."""
+        from .knudsen import KnudsenSolver
+        m, geo = self.mesh, self.geo
+        nz = phi.shape[2]
+        if self.kn is None or not self.kn.fits(m.MT, nz):
+            self.kn = KnudsenSolver(m.MT, nz)
+        hw = 0.5 * float(geo.get('trench_width', geo['Lx']))
+        self.ktimer.start("k_kn_prepare")
+        self.kn.prepare(phi, float(geo['dx']), float(geo['sub_top']), not geo.get('hole', False),
+                        m.id, m.centroid, fn, center=(0.5 * geo['Lx'], 0.5 * geo['Ly']),
+                        half_width=hw, stream=_sp())
+        self.ktimer.stop("k_kn_prepare")
+
+    def knudsen_fixed_point(self, yields, n_fp=4):
+        """The coverage <-> Knudsen fixed point (threed.py:1184-1207) on the prepared geometry
+        (m_i, cos_i and the yields must be in place)."""
+        m, par, geo = self.mesh, self.par, self.geo
+        s = _sp()
+        betaE, betaO = float(par.get('betaE', 0.7)), float(par.get('betaO', 1.0))
+        wls = float(par.get('knudsen_wall_loss_scale', 1.85))
+        front = None
+        if getattr(self.flags, 'knudsen_front_loss', False):
+            W = 2.0 * 0.5 * float(geo.get('trench_width', geo['Lx']))
+            front = (W, float(par.get('knudsen_front_band_W', 8.0)),
+                     float(par.get('knudsen_passive_frac', 0.5)),
+                     float(par.get('knudsen_front_ar_pass', 15.0)))
+        field = par.get('knudsen_sink', 'local') == 'field'
+        self.bare.fill_(1.0)
+        for _ in range(n_fp):
+            self.ktimer.start("k_kn_solve")
+            self.kn.solve(self.bare, m.area, betaE, betaO, float(geo['Ly']), wls, self.m_F,
+                          self.m_O, sink_field=field, front=front, stream=s)
+            self.ktimer.stop("k_kn_solve")
             _lib.call("petch_belen_bare", m.id, m.MT, m.MV, ctypes.byref(self.chem),
                       self.m_i.data_ptr(), self.m_F.data_ptr(), self.m_O.data_ptr(),
                       self.cos_i.data_ptr(), yields[1], yields[2], self.bare.data_ptr(), s)
@@ -518,9 +589,10 @@ class EtchEngine(FluxEngine):
         self.mesh.build(self.phi, self.dx, self.geo, self.scratch)
 
     def rate_and_extend(self, band, centroid=False, redep=None):
-        """surface_rate, the optional redeposition correction (redep = (n particles, seed)), then
-        the velocity extension into the band: nearest face (extend_velocity_gpu) or nearest
-        centroid (extend_velocity_3d, centroid=True)."""
+        """surface_rate, the optional redeposition correction (redep = (n particles, seed) or
+        (n, seed, z_clean): no redeposit on faces with centroid z <= z_clean), then the velocity
+        extension into the band: nearest face (extend_velocity_gpu) or nearest centroid
+        (extend_velocity_3d, centroid=True)."""
         m = self.mesh
         s = _sp()
         y = self.yields
@@ -537,9 +609,10 @@ class EtchEngine(FluxEngine):
                   self.F.data_ptr(), 1, self.active.data_ptr(), self.small[8:9].data_ptr(),
                   self.ncell, self.small[0:6].data_ptr(), s)
 
-    def redeposition(self, n, seed):
+    def redeposition(self, n, seed, z_clean=None):
         """mc_redep_3d + run_etch_3d's V = max(V - k_redep * Rf, 0) (threed.py:1582-1605,
-        1730-1743), with the into-gas normals of the current level set."""
+        1730-1743), with the into-gas normals of the current level set; Rf = 0 on faces with
+        centroid z <= z_clean (the charging foot cleaning, threed.py:1733-1741)."""
         m, par = self.mesh, self.par
         s = _sp()
         if getattr(self, "redep", None) is None or self.redep['MT'] != self.MT:
@@ -560,6 +633,9 @@ class EtchEngine(FluxEngine):
                   int(n), self.flux.data_ptr(), r['cdf'].data_ptr(), r['scratch'].data_ptr(),
                   r['scratch'].numel(), self.small[0:6].data_ptr(), s)
         self.ktimer.stop("k_redep")
+        if z_clean is not None:
+            _lib.call("petch_zero_below", m.id, m.MT, m.centroid.data_ptr(), float(z_clean),
+                      self.flux.data_ptr(), s)
         _lib.call("petch_redep_apply", m.id, m.MT, m.MV, self.flux.data_ptr(), r['cdf'].data_ptr(),
                   int(n), float(par.get('k_redep', 1.0)), self.V.data_ptr(), r['Rf'].data_ptr(),
                   self.small[6:8].data_ptr(), s)
@@ -693,6 +769,8 @@ def run_etch_3d(Lx=10.0, Ly=4.0, Lz=14.0, dx=0.4, trench_width=4.0, mask_th=2.0,
             eng.flux_radiosity(eng.phi, n_ion_s, seed)
         elif nt == "dda":
             eng.flux_dda(eng.phi, n_ion_s, seed)
+        elif nt == "knudsen":
+            eng.flux_knudsen(eng.phi, n_ion_s, seed)
         elif coupled:
             eng.flux_coupled(n_ion_s, n_neu_s, seed, warm)
         else:
@@ -701,8 +779,13 @@ def run_etch_3d(Lx=10.0, Ly=4.0, Lz=14.0, dx=0.4, trench_width=4.0, mask_th=2.0,
             eng.par = par
         st_timer.stop("flux")
         st_timer.start("extend")
-        eng.rate_and_extend(band, centroid=extend != "gpu",
-                            redep=(n_neu, step) if redepo else None)
+        redep = None
+        if redepo:
+            redep = (n_neu, step)
+            if getattr(flags, "surface_charging", False) and etch_stop_z is not None:
+                foot_h = max(0.3 * trench_width, 2.0 * dx)
+                redep = (n_neu, step, float(etch_stop_z) + foot_h)
+        eng.rate_and_extend(band, centroid=extend != "gpu", redep=redep)
         st_timer.stop("extend")
         st = eng.sync_status()
         if st['mesh_err'] & (MESH_ERR_TRI_OVERFLOW | MESH_ERR_VERT_OVERFLOW | MESH_ERR_HASH_FULL):
@@ -731,7 +814,7 @@ def run_etch_3d(Lx=10.0, Ly=4.0, Lz=14.0, dx=0.4, trench_width=4.0, mask_th=2.0,
             st_timer.stop("reinit")
         if surf_smooth and surf_smooth > 0.0:
             eng.smooth(float(surf_smooth))
-        eng.end_step(warm and coupled and nt not in ("radiosity", "dda"))
+        eng.end_step(warm and coupled and nt == "mc")
         st['nsub'] = nsub
         if record_depth_every and (step % record_depth_every == 0 or step == n_steps - 1):
             g2 = _host_geo(geo, eng.phi)
@@ -861,7 +944,13 @@ def mc_flux_3d_coupled(mesh, verts, faces, areas, geo, par, n_ion=20000, n_neu=2
     b0 = None
     if bare_init is not None:
         b0 = torch.as_tensor(np.asarray(bare_init, np.float32), device="cuda")
-    fe.flux_coupled(int(n_ion), int(n_neu), int(seed), False, bare_init=b0)
+    phi = None
+    if flags is not None and getattr(flags, "floor_charge_throttle", False):
+        phi = geo['phi']
+        phi = (phi if isinstance(phi, torch.Tensor)
+               else torch.from_numpy(np.ascontiguousarray(phi)))
+        phi = phi.to("cuda", torch.float32).contiguous()
+    fe.flux_coupled(int(n_ion), int(n_neu), int(seed), False, bare_init=b0, phi=phi)
     _raise_trace_errors(fe)
     _set_ion_yield(fe, par, F)
     return (_host(fe.m_i, F), _host(fe.m_F, F), _host(fe.m_O, F), _host(fe.cos_i, F),
@@ -896,6 +985,23 @@ def mc_flux_3d_dda(mesh, verts, faces, centroids, areas, geo, par, n_ion=20000, 
     phi = (phi if isinstance(phi, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(phi)))
     phi = phi.to("cuda", torch.float32).contiguous()
     fe.flux_dda(phi, int(n_ion), int(seed), n_fp=int(n_fp))
+    _raise_trace_errors(fe)
+    _set_ion_yield(fe, par, F)
+    return _host(fe.m_i, F), _host(fe.m_F, F), _host(fe.m_O, F), _host(fe.cos_i, F)
+
+
+def mc_flux_3d_knudsen(mesh, verts, faces, centroids, areas, geo, par, n_ion=20000, seed=0,
+                       flags=None, n_fp=4):
+    """mc_flux_3d_knudsen (threed.py:1149-1208) on a DeviceMesh: returns numpy (m_i, m_F, m_O,
+    cos_i) and sets or clears par['_ion_yield'] like the reference.  geo carries phi (host or
+    device), Lx, Ly, Lz, dx, sub_top, trench_width and hole; verts / faces / centroids / areas
+    describe the same mesh and are not read."""
+    F = mesh.n_faces()
+    fe = _flux_engine(mesh, geo, par, flags)
+    phi = geo['phi']
+    phi = (phi if isinstance(phi, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(phi)))
+    phi = phi.to("cuda", torch.float32).contiguous()
+    fe.flux_knudsen(phi, int(n_ion), int(seed), n_fp=int(n_fp))
     _raise_trace_errors(fe)
     _set_ion_yield(fe, par, F)
     return _host(fe.m_i, F), _host(fe.m_F, F), _host(fe.m_O, F), _host(fe.cos_i, F)

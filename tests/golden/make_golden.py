@@ -4,7 +4,7 @@ warp-lang replaced by warp_shim.py (a CPU stand-in: see its docstring for what i
 
 Run in a checkout that has the reference at /root/reference (or $PETCH_REFERENCE):
 
-    python tests/golden/make_golden.py [group ...]   # groups: levelset surface flux radiosity options redep dda
+    python tests/golden/make_golden.py [group ...]   # groups: levelset surface flux radiosity options redep dda knudsen
 
 The fixtures are committed; tests read only the .npz files, never the reference.
 """
@@ -473,8 +473,122 @@ def dda():
     np.savez_compressed(os.path.join(HERE, "dda.npz"), **out)
 
 
+def knudsen():
+    """The Knudsen conductance tail (petch/knudsen.py, wired as mc_flux_3d_knudsen,
+    threed.py:1149-1208) and the charging hooks (_apply_hg_charging :1046-1110,
+    _apply_floor_charge_throttle :1112-1147) run unmodified on small meshes: slice geometry,
+    conductance profiles for random sinks (scalar and per-slice loss scales), knudsen_face_flux
+    with and without the footprint filter and the front loss, mc_flux_3d_knudsen with recorded
+    ions (local and field sinks, with and without surface_charging), and both hooks on recorded
+    inputs."""
+    import petch.knudsen as kn
+    out = {}
+    wp = t3.wp
+    rng = np.random.default_rng(31)
+    for key, hole, deep in (("hole", True, False), ("trench", False, False),
+                            ("hole_deep", True, True), ("trench_deep", False, True)):
+        nz = 22 if deep else 14
+        m, geo, phi = _small_mesh(hole, nx=10, ny=10, nz=nz, dx=0.3)
+        if deep:                       # a deeper pit: material minus {r < w/2, z > 0.45}
+            orc = _oracle()
+            nx, ny = 10, 10
+            dx, Lx, Ly = 0.3, 3.0, 3.0
+            sub_top = 5.4
+            phi_a, _ = orc.seed(nx, ny, nz, dx, Lx, Ly, sub_top, 0.75, 1.5, hole)
+            X, Y, Z = np.meshgrid(np.arange(nx) * dx, np.arange(ny) * dx, np.arange(nz) * dx,
+                                  indexing="ij")
+            r = np.sqrt((X - Lx / 2) ** 2 + (Y - Ly / 2) ** 2) if hole else np.abs(X - Lx / 2)
+            phi_a = np.minimum(phi_a, np.maximum(r - 0.75, 0.45 - Z))
+            phi = orc.reinit(phi_a.astype(np.float32), dx, 6 * dx).astype(np.float32)
+            geo = dict(geo, sub_top=sub_top, Lz=nz * dx, zs=np.arange(nz) * dx,
+                       phi=phi.astype(np.float64))
+            m = orc.mesh_build(phi, dx, geo)
+        dx, sub_top = geo['dx'], geo['sub_top']
+        periodic = 0 if hole else 1
+        shape = "via" if hole else "trench"
+        verts = m.verts.astype(np.float32)
+        faces = m.faces
+        v64 = verts.astype(np.float64)[faces]
+        centroids = v64.mean(axis=1)
+        areas = 0.5 * np.linalg.norm(np.cross(v64[:, 1] - v64[:, 0], v64[:, 2] - v64[:, 0]),
+                                     axis=1)
+        geo = dict(geo, phi=phi.astype(np.float64))
+        fn = t3._gas_normals(verts, faces, centroids, geo)
+        F = len(faces)
+        zs = geo['zs']
+        A = np.maximum(areas, 1e-9)
+        out[f"{key}_verts"], out[f"{key}_faces"], out[f"{key}_phi"] = verts, faces, phi
+        out[f"{key}_centroids"], out[f"{key}_areas"], out[f"{key}_gas_normals"] = (
+            centroids, areas, fn)
+        out[f"{key}_geo"] = np.array([geo['Lx'], geo['Ly'], geo['Lz'], dx, periodic, sub_top,
+                                      geo['trench_width']])
+        area, perim = kn.slice_geometry(phi.astype(np.float64), zs, dx, sub_top, shape)
+        out[f"{key}_slice_area"], out[f"{key}_slice_perim"] = area, perim
+        loss = rng.uniform(0.0, 0.3, nz) * (rng.random(nz) < 0.7)
+        out[f"{key}_loss"] = loss
+        out[f"{key}_profile_scalar"] = kn.conductance_profile(phi.astype(np.float64), zs, dx,
+                                                              sub_top, shape, loss, 1.85)
+        ls = rng.uniform(0.5, 3.0, nz)
+        out[f"{key}_ls"] = ls
+        out[f"{key}_profile_array"] = kn.conductance_profile(phi.astype(np.float64), zs, dx,
+                                                             sub_top, shape, loss, ls)
+        s_face = rng.uniform(0.0, 1.0, F)
+        out[f"{key}_s_face"] = s_face
+        ctr = (0.5 * geo['Lx'], 0.5 * geo['Ly'])
+        hw = 0.5 * geo['trench_width']
+        kw = dict(center=ctr, half_width=hw)
+        out[f"{key}_kff_plain"] = kn.knudsen_face_flux(phi.astype(np.float64), zs, dx, sub_top,
+                                                       shape, centroids, fn[:, 2], A, geo['Ly'],
+                                                       s_face, 2.9)
+        out[f"{key}_kff_foot"] = kn.knudsen_face_flux(phi.astype(np.float64), zs, dx, sub_top,
+                                                      shape, centroids, fn[:, 2], A, geo['Ly'],
+                                                      s_face, 2.9, **kw)
+        out[f"{key}_kff_front"] = kn.knudsen_face_flux(phi.astype(np.float64), zs, dx, sub_top,
+                                                       shape, centroids, fn[:, 2], A, geo['Ly'],
+                                                       s_face, 2.0, front_loss=True, band_W=1.0,
+                                                       pass_frac=0.3, ar_pass=0.7, **kw)
+
+        mesh = wp.Mesh(points=wp.array(verts, dtype=wp.vec3),
+                       indices=wp.array(faces.flatten(), dtype=wp.int32))
+        runs = (("local", dict(), dict()), ("field", dict(knudsen_sink='field'), dict()),
+                ("front", dict(knudsen_front_band_W=1.0, knudsen_passive_frac=0.3,
+                               knudsen_front_ar_pass=0.7), dict(knudsen_front_loss=True)),
+                ("hg", dict(), dict(surface_charging="hg")),
+                ("petch", dict(), dict(surface_charging="petch")))
+        for name, pkw, fkw in runs:
+            par = dict(t3.PAR, periodic_y=periodic, **pkw)
+            flags = t3.DEFAULT_FLAGS.__class__(chemistry="belen", yield_angular="viennaps",
+                                               ion_reflection=True, coverage_sticking=True,
+                                               neutral_transport="knudsen", **fkw)
+            p = dict(par)
+            t0 = time.time()
+            m_i, m_F, m_O, cos_i = t3.mc_flux_3d_knudsen(mesh, verts, faces, centroids, areas,
+                                                         geo, p, n_ion=3000, seed=100,
+                                                         flags=flags)
+            print(f"  {key} mc_flux_3d_knudsen[{name}]: {time.time() - t0:.1f}s", flush=True)
+            out[f"{key}_{name}_m_i"], out[f"{key}_{name}_cos_i"] = m_i, cos_i
+            out[f"{key}_{name}_m_F"], out[f"{key}_{name}_m_O"] = m_F, m_O
+            out[f"{key}_{name}_ion_yield"] = np.stack(p['_ion_yield'])
+
+        # the hooks on recorded inputs
+        m_i = rng.uniform(0.0, 1.5, F)
+        iy = tuple(rng.uniform(0.0, 3.0, F) for _ in range(3))
+        out[f"{key}_hook_m_i"], out[f"{key}_hook_iy"] = m_i, np.stack(iy)
+        for mode in ("hg", "petch"):
+            par = dict(t3.PAR, _ion_yield=iy)
+            flags = t3.DEFAULT_FLAGS.__class__(chemistry="belen", surface_charging=mode)
+            mi2 = t3._apply_hg_charging(m_i, par, flags, centroids, fn[:, 2], A, geo)
+            out[f"{key}_{mode}_hook_m_i"] = mi2
+            out[f"{key}_{mode}_hook_iy"] = np.stack(par['_ion_yield'])
+        par = dict(t3.PAR, _ion_yield=iy)
+        mi2 = t3._apply_floor_charge_throttle(m_i, par, verts, faces, geo)
+        out[f"{key}_throttle_m_i"] = mi2
+        out[f"{key}_throttle_iy"] = np.stack(par['_ion_yield'])
+    np.savez_compressed(os.path.join(HERE, "knudsen.npz"), **out)
+
+
 GROUPS = {"levelset": levelset, "surface": surface, "flux": flux, "radiosity": radiosity,
-          "options": options, "redep": redep, "dda": dda}
+          "options": options, "redep": redep, "dda": dda, "knudsen": knudsen}
 
 if __name__ == "__main__":
     for g in (sys.argv[1:] or list(GROUPS)):
