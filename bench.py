@@ -102,17 +102,18 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def timed_run(par, flags, W, K, world, rank, local, dist):
+def timed_run(par, flags, W, K, world, rank, local, dist, prefix=False):
     """W untimed + K timed steps of the workload with `flags`; per-step CUDA events on the compute
     stream, 256 MB L2 flush before each timed step (outside the interval), trace-kernel events,
-    launch counts and clocks over the timed region.  Time = max over ranks."""
+    launch counts and clocks over the timed region.  Time = max over ranks.  prefix: run only the
+    first W + K steps of the 100-step schedule (same step length and seeds)."""
     import torch
     from petch_b200 import _lib, threed as t3
     flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda")   # 256 MB > L2
     ev = {}
     info = {}
     ktimer = t3.EventTimer()
-    radiosity = getattr(flags, "neutral_transport", "mc") == "radiosity"
+    nt = getattr(flags, "neutral_transport", "mc")
 
     def before(step, eng):
         if step == W:
@@ -137,8 +138,10 @@ def timed_run(par, flags, W, K, world, rank, local, dist):
             e = torch.cuda.Event(enable_timing=True)
             e.record()
             ev[step].append(e)
-            if radiosity:                     # ions + n_ff = 64 form-factor rays per face
+            if nt == "radiosity":             # ions + n_ff = 64 form-factor rays per face
                 rays.append(RAYS + 64 * st['F'])
+            elif nt in ("dda", "knudsen"):    # ions (deterministic neutrals)
+                rays.append(RAYS)
             else:                             # ions + F and O neutrals per fixed-point round
                 n_fp = 4 if step == 0 else 1
                 rays.append(RAYS + 2 * RAYS * n_fp)
@@ -150,7 +153,9 @@ def timed_run(par, flags, W, K, world, rank, local, dist):
             info['clk'] = info['clocks'].stop()
             info['F'] = st['F']
 
-    geo = t3.run_etch_3d(**WORKLOAD, t_end=T_END, n_steps=W + K if W + K < N_STEPS else N_STEPS,
+    n_run = W + K if W + K < N_STEPS else N_STEPS
+    t_end = T_END * n_run / N_STEPS if prefix else T_END
+    geo = t3.run_etch_3d(**WORKLOAD, t_end=t_end, n_steps=n_run,
                          par=par, flags=flags, n_ion=RAYS, n_neu=RAYS, reinit_method="fsm",
                          verbose=False, seed_offset=1000 * rank, max_tris=1 << 20,
                          hooks=dict(before_step=before, after_step=after))
@@ -183,6 +188,80 @@ def radiosity_summary(par, flags, W, K, world, rank, local, dist):
             "stage_seconds": dict(r['geo']['timings']),
             "workload": "the same trench, neutral_transport='radiosity' (64 form-factor rays per "
                         "face, 4 coverage rounds of 40 Jacobi sweeps, 2^22 ions), seed 0"}
+
+
+TR_W, TR_K = 3, 10
+
+
+def transports_summary(par, flags, world, rank, local, dist):
+    """The deterministic neutral transports on the same trench: the first 13 steps of the 100-step
+    schedule (3 untimed, 10 timed) with neutral_transport 'dda' (dda_n_dir 64: 128 directions,
+    12 re-emission passes) and 'knudsen' (1-D conductance tail), ions as the MC run."""
+    from petch_b200 import params
+    out = {}
+    for nt in ("dda", "knudsen"):
+        fl = params.Flags(**{**flags.__dict__, "neutral_transport": nt})
+        r = timed_run(par, fl, TR_W, TR_K, world, rank, local, dist, prefix=True)
+        total_s = r['total_s']
+        out[nt] = {"value": world * TR_K / total_s, "unit": "steps/s",
+                   "ms_per_step": 1e3 * total_s / TR_K, "steps": TR_K, "warmup": TR_W,
+                   "faces_last_step": r['info']['F'],
+                   "kernel_ms_per_step": {k: float(np.sum(v)) / TR_K for k, v in r['kms'].items()},
+                   "gpu_launches": r['launches'], "clocks": r['info'].get('clk'),
+                   "stage_seconds": dict(r['geo']['timings'])}
+    out["workload"] = ("the headline trench, steps 3..12 of its 100-step schedule, "
+                       "neutral_transport dda / knudsen, 2^22 ions, seed 0")
+    return out
+
+
+# The reference's own published loop-speed runs (scripts/vps_sweep.py:42-50; RTX 3090 results in
+# box_results/vps_sweep_result.json and README "Headline numbers"): hole diameter, published wall
+# seconds for 40 steps (sweep, re-measured), published centre depth.
+PUB_GEO = dict(Lx=14.0, Ly=14.0, Lz=24.0, dx=0.25, mask_th=2.0, sub_top=18.0, hole=True,
+               t_end=3.0)
+PUB_RUNS = ((4.0, 1.3016, 0.90, 7.75), (6.0, 1.6117, 1.01, 10.25), (8.0, 1.8242, 1.17, 10.25))
+PUB_RATES = (0.10, 0.15, 0.20, 0.25, 0.30)
+
+
+def published_config_summary():
+    """The reference's published full-loop speed configuration run through the public API:
+    Ø4/6/8 um holes, extent 14 um, dx 0.25, 40 steps over 3.0, 30k rays, warm coverage start
+    (n_fp = 1), FSM reinit, default flags plus coverage_sticking / warm_start_coverage (legacy
+    first-hit ions).  As the reference's sweep does, each diameter tries rate_scale in
+    0.10..0.30 and keeps the run whose depth is closest to the published one; wall-clock seconds
+    of run_etch_3d (host arithmetic included, as the published figures) after one warm-up run."""
+    import torch
+    from petch_b200 import params, threed as t3
+    par0 = dict(params.PAR, betaE=0.7, n_fp=1)
+    flags = params.Flags(coverage_sticking=True, sampling="sobol", warm_start_coverage=True)
+    kw = dict(dx=PUB_GEO['dx'], n_steps=40, flags=flags, n_ion=30000, n_neu=30000,
+              reinit_method="fsm", verbose=False,
+              **{k: v for k, v in PUB_GEO.items() if k != 'dx'})
+    t3.run_etch_3d(trench_width=6.0, par=dict(par0, rate_scale=0.08), **dict(kw, n_steps=4))
+    rows = []
+    for diam, pub_s, pub_s2, pub_depth in PUB_RUNS:
+        best = None
+        for r in PUB_RATES:
+            torch.cuda.synchronize()
+            t0 = time.time()
+            g = t3.run_etch_3d(trench_width=diam, par=dict(par0, rate_scale=r), **kw)
+            torch.cuda.synchronize()
+            wall = time.time() - t0
+            depth = t3.center_depth_3d(g)
+            g.pop('engine', None)
+            if best is None or abs(depth - pub_depth) < abs(best[1] - pub_depth):
+                best = (wall, depth, r)
+        wall, depth, r = best
+        rows.append({"diameter_um": diam, "rate_scale": r, "wall_s": wall,
+                     "steps_per_s": 40.0 / wall, "depth_um": depth,
+                     "published_wall_s": pub_s, "published_steps_per_s": 40.0 / pub_s,
+                     "published_wall_s_remeasured": pub_s2, "published_depth_um": pub_depth,
+                     "speedup_vs_published": pub_s / wall,
+                     "speedup_vs_published_remeasured": pub_s2 / wall})
+    return {"runs": rows, "unit": "steps/s (wall clock, public API)",
+            "reference_hardware": "RTX 3090 (published; cross-hardware comparison)",
+            "workload": "hole sweep of scripts/vps_sweep.py: extent 14, dx 0.25, Lz 24, mask 2, "
+                        "sub_top 18, 40 steps over 3.0, 30k rays, n_fp 1, warm start, fsm"}
 
 
 BATCH_N, BATCH_STEPS, BATCH_RAYS, BATCH_T_END, BATCH_PLAIN_SAMPLE = 64, 30, 1 << 20, 3.0, 16
@@ -400,10 +479,14 @@ def run_b200(args):
            "clocks": info.get('clk'), "stage_seconds": {k: v for k, v in geo['timings'].items()}}
     if not args.no_radiosity:
         out["radiosity"] = radiosity_summary(par, flags, W, K, world, rank, local, dist)
+    if not args.no_transports:
+        out["transports"] = transports_summary(par, flags, world, rank, local, dist)
     if not args.no_batched:
         out["batched"] = batched_summary(world, rank, dist)
     if rank == 0 and not args.no_diff:
         out["differentiation"] = differentiation_summary()
+    if rank == 0 and not args.no_published:
+        out["published_config"] = published_config_summary()
     if rank == 0 and not args.no_e2e:
         out["e2e"] = e2e(args, par, flags)
     if rank == 0 and not args.no_cpu_baseline:
@@ -509,6 +592,8 @@ def main():
     ap.add_argument("--no-radiosity", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-diff", action="store_true")
+    ap.add_argument("--no-published", action="store_true")
+    ap.add_argument("--no-transports", action="store_true")
     args = ap.parse_args()
     if args.warmup < 0 or args.steps < 1 or args.warmup >= N_STEPS:
         raise SystemExit("need 0 <= warmup < 100 and steps >= 1")
