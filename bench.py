@@ -94,6 +94,19 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def rank_reduce(values, op, dist, world):
+    """Reduce per-rank float64 values over the ranks (op "max" or "sum"; the device follows the
+    process group's backend); world == 1 returns them unchanged."""
+    vals = [float(v) for v in values]
+    if world <= 1:
+        return vals
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor(vals, dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return [float(v) for v in t.cpu().tolist()]
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -163,13 +176,10 @@ def timed_run(par, flags, W, K, world, rank, local, dist, prefix=False):
     step_ms = [ev[s][0].elapsed_time(ev[s][1]) for s in sorted(ev)]
     total_s = float(np.sum(step_ms)) / 1e3
     kms = ktimer.totals_ms()
-    t = torch.tensor([total_s], dtype=torch.float64, device="cuda")
-    launches = torch.tensor([info['launch1'] - info['launch0']], dtype=torch.int64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dist.all_reduce(launches, op=dist.ReduceOp.SUM)
-    return dict(geo=geo, kms=kms, info=info, rays=rays, work_q=work_q, total_s=float(t.item()),
-                launches=int(launches.item()))
+    (total_s,) = rank_reduce([total_s], "max", dist, world)
+    (launches,) = rank_reduce([info['launch1'] - info['launch0']], "sum", dist, world)
+    return dict(geo=geo, kms=kms, info=info, rays=rays, work_q=work_q, total_s=total_s,
+                launches=int(launches))
 
 
 def radiosity_summary(par, flags, W, K, world, rank, local, dist):
@@ -307,10 +317,7 @@ def batched_summary(world, rank, dist):
     e1.record()
     torch.cuda.synchronize()
     plain_s = e0.elapsed_time(e1) / 1e3
-    t = torch.tensor([sec, plain_s], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    sec, plain_s = float(t[0].item()), float(t[1].item())
+    sec, plain_s = rank_reduce([sec, plain_s], "max", dist, world)
     dd = np.abs(np.array(depths[:n_plain]) - np.array(plain_depths))
     return {"value": world * BATCH_N * BATCH_STEPS / sec, "unit": "instance-steps/s",
             "seconds": sec, "instances": BATCH_N, "steps": BATCH_STEPS,

@@ -331,6 +331,22 @@ int petch_trace_batch(int kind, const petch_batch_item* items, int B, int max_tr
                       float beta, const int* step, uint32_t seed_mul, uint32_t seed_add,
                       int* work, void* stream);
 
+/* Tangent outputs of one instance for petch_trace_batch_tangent: dout = d(sputter, ion-enhanced,
+ * passivation tallies) / d(mean ion energy) [3][max_tris] (kind 0) or d(flux) [3][max_tris] along
+ * the three recipe directions (kind 1); dbare = the coverage tangents [3][max_tris] (kind 1; NULL
+ * = 0). */
+typedef struct petch_batch_tangent {
+    float* dout;
+    const float* dbare;
+} petch_batch_tangent;
+
+/* petch_trace_batch carrying tangents: the batched form of petch_trace_ions_tangent (kind 0) and
+ * petch_trace_neutrals_tangent (kind 1); tans: host array parallel to items. */
+int petch_trace_batch_tangent(int kind, const petch_batch_item* items,
+                              const petch_batch_tangent* tans, int B, int max_tris, int max_verts,
+                              float beta, const int* step, uint32_t seed_mul, uint32_t seed_add,
+                              int* work, void* stream);
+
 /* One instance's level-set state for the batched stages. */
 typedef struct petch_batch_grid {
     float* phi;              /* level set (in / out) */
@@ -361,6 +377,28 @@ int petch_batch_advect(const petch_batch_grid* grids, int B, void* stream);
 /* Replaces, for B <= 64 instances with the same dx, reinit_fsm (petch/threed.py:1515-1537) as
  * petch_reinit_eik mode 0 with band = band_r, in place on each phi.  Graph-capturable. */
 int petch_batch_reinit(const petch_batch_grid* grids, int B, double band_r, void* stream);
+
+/* The tangent state of one instance for the batched tangent stages (direction-major [3][n]
+ * arrays of the instance's n = nx*ny*nz cells). */
+typedef struct petch_batch_tangent_grid {
+    float* dphi;                 /* level-set tangents (in / out) */
+    float* dtmp;                 /* advection ping-pong */
+    const float* dF;             /* speed tangents (petch_extend_tangent) */
+    const unsigned char* mask;   /* 1 on mask cells: pinned to mask_phi, tangent 0 */
+    float* du_a;                 /* reinit scratch */
+    float* du_b;
+} petch_batch_tangent_grid;
+
+/* petch_batch_advect carrying tangents: the CFL substep count on the device, then 160 substep
+ * launches of petch_advect_tangent's dense dual update over all instances (instance b steps while
+ * s < nsub_b).  Values equal per-instance petch_advect_tangent calls.  Graph-capturable. */
+int petch_batch_advect_tangent(const petch_batch_grid* grids,
+                               const petch_batch_tangent_grid* tans, int B, void* stream);
+
+/* petch_batch_reinit carrying tangents (petch_reinit_tangent per instance, same dx for all). */
+int petch_batch_reinit_tangent(const petch_batch_grid* grids,
+                               const petch_batch_tangent_grid* tans, int B, double band_r,
+                               void* stream);
 
 /* *step += 1 on the device (the step counter petch_trace_batch seeds from). */
 int petch_batch_step_advance(int* step, void* stream);

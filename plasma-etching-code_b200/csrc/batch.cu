@@ -51,14 +51,7 @@ __global__ void k_b_nsub(BTable t) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= t.B) return;
     const BGrid& x = t.it[b];
-    const int F = x.hdr[HDR_F];
-    float vmx = F > 0 ? __int_as_float(x.stats[1]) : 0.0f;
-    double V = isfinite(vmx) ? (double)vmx : 0.0;
-    V = fmax(V, 1e-6);
-    double q = ceil(V * x.dt / (0.4 * x.dx));
-    int nsub = (int)fmin(fmax(q, 1.0), (double)kMaxSub);
-    x.sub[0] = nsub;
-    x.sub[1] = __float_as_int((float)(x.dt / nsub));
+    cfl_substeps(x.hdr[HDR_F], x.stats, x.dt, x.dx, x.sub);
 }
 
 // tmp = phi with the mask cells pinned (the first substep's write target).

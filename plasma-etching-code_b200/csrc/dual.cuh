@@ -7,6 +7,34 @@
 
 namespace petch {
 
+// Elementary float operations, each rounded on its own on the device (no fused multiply-add), so
+// an expression gives the same bits in every kernel that inlines it; double keeps the plain
+// operators (the chemistry duals follow the plain double kernels' code generation).
+__host__ __device__ inline float rn_add(float a, float b) {
+#ifdef __CUDA_ARCH__
+    return __fadd_rn(a, b);
+#else
+    return a + b;
+#endif
+}
+__host__ __device__ inline float rn_sub(float a, float b) {
+#ifdef __CUDA_ARCH__
+    return __fsub_rn(a, b);
+#else
+    return a - b;
+#endif
+}
+__host__ __device__ inline float rn_mul(float a, float b) {
+#ifdef __CUDA_ARCH__
+    return __fmul_rn(a, b);
+#else
+    return a * b;
+#endif
+}
+__host__ __device__ inline double rn_add(double a, double b) { return a + b; }
+__host__ __device__ inline double rn_sub(double a, double b) { return a - b; }
+__host__ __device__ inline double rn_mul(double a, double b) { return a * b; }
+
 template <class S, int N>
 struct Dual {
     S v;
@@ -30,9 +58,9 @@ __host__ __device__ inline Dual<S, N> dconst(S v) {
         _Pragma("unroll") for (int k = 0; k < N; ++k) r.d[k] = DER;                              \
         return r;                                                                                \
     }
-PETCH_DUAL_BINOP(+, a.v + b.v, a.d[k] + b.d[k])
-PETCH_DUAL_BINOP(-, a.v - b.v, a.d[k] - b.d[k])
-PETCH_DUAL_BINOP(*, a.v * b.v, a.d[k] * b.v + a.v * b.d[k])
+PETCH_DUAL_BINOP(+, rn_add(a.v, b.v), rn_add(a.d[k], b.d[k]))
+PETCH_DUAL_BINOP(-, rn_sub(a.v, b.v), rn_sub(a.d[k], b.d[k]))
+PETCH_DUAL_BINOP(*, rn_mul(a.v, b.v), rn_add(rn_mul(a.d[k], b.v), rn_mul(a.v, b.d[k])))
 #undef PETCH_DUAL_BINOP
 
 template <class S, int N>
@@ -41,7 +69,7 @@ __host__ __device__ inline Dual<S, N> operator/(const Dual<S, N>& a, const Dual<
     r.v = a.v / b.v;
     const S ib = S(1) / b.v;
 #pragma unroll
-    for (int k = 0; k < N; ++k) r.d[k] = (a.d[k] - r.v * b.d[k]) * ib;
+    for (int k = 0; k < N; ++k) r.d[k] = rn_mul(rn_sub(a.d[k], rn_mul(r.v, b.d[k])), ib);
     return r;
 }
 
@@ -66,9 +94,9 @@ __host__ __device__ inline Dual<S, N> operator-(S a, const Dual<S, N>& b) { retu
 template <class S, int N>
 __host__ __device__ inline Dual<S, N> operator*(const Dual<S, N>& a, S b) {
     Dual<S, N> r;
-    r.v = a.v * b;
+    r.v = rn_mul(a.v, b);
 #pragma unroll
-    for (int k = 0; k < N; ++k) r.d[k] = a.d[k] * b;
+    for (int k = 0; k < N; ++k) r.d[k] = rn_mul(a.d[k], b);
     return r;
 }
 template <class S, int N>
@@ -120,7 +148,7 @@ __host__ __device__ inline Dual<S, N> vsqrt(const Dual<S, N>& a) {
     r.v = sqrt(a.v);
     const S g = r.v > S(0) ? S(0.5) / r.v : S(0);
 #pragma unroll
-    for (int k = 0; k < N; ++k) r.d[k] = a.d[k] * g;
+    for (int k = 0; k < N; ++k) r.d[k] = rn_mul(a.d[k], g);
     return r;
 }
 

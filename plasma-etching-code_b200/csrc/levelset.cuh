@@ -54,22 +54,24 @@ __device__ __forceinline__ float advect_cell(const float* __restrict__ phi, long
 
 // Godunov solution of |grad U| = 1 from the three upwind neighbour minima (threed.py:1421-1452):
 // sort ascending, then take the 1-, 2- or 3-term root while it stays below the next neighbour.
+// Each operation rounded on its own, in the order the tangent kernels' dual version uses.
 __device__ __forceinline__ float eik_solve(float a1, float a2, float a3, float dx) {
     float t;
     if (a1 > a2) { t = a1; a1 = a2; a2 = t; }
     if (a2 > a3) { t = a2; a2 = a3; a3 = t; }
     if (a1 > a2) { t = a1; a1 = a2; a2 = t; }
-    float x = a1 + dx;
+    float x = __fadd_rn(a1, dx);
     if (x <= a2) return x;
-    float d2 = 2.0f * dx * dx - (a1 - a2) * (a1 - a2);
+    const float t12 = __fsub_rn(a1, a2);
+    float d2 = __fsub_rn(__fmul_rn(__fmul_rn(2.0f, dx), dx), __fmul_rn(t12, t12));
     d2 = fmaxf(d2, 0.0f);
-    x = 0.5f * (a1 + a2 + sqrtf(d2));
+    x = __fmul_rn(__fadd_rn(__fadd_rn(a1, a2), __fsqrt_rn(d2)), 0.5f);
     if (x <= a3) return x;
-    float s1 = a1 + a2 + a3;
-    float s2 = a1 * a1 + a2 * a2 + a3 * a3;
-    float d3 = s1 * s1 - 3.0f * (s2 - dx * dx);
+    const float s1 = __fadd_rn(__fadd_rn(a1, a2), a3);
+    const float s2 = __fadd_rn(__fadd_rn(__fmul_rn(a1, a1), __fmul_rn(a2, a2)), __fmul_rn(a3, a3));
+    float d3 = __fsub_rn(__fmul_rn(s1, s1), __fmul_rn(3.0f, __fsub_rn(s2, __fmul_rn(dx, dx))));
     d3 = fmaxf(d3, 0.0f);
-    return (s1 + sqrtf(d3)) / 3.0f;
+    return __fdiv_rn(__fadd_rn(s1, __fsqrt_rn(d3)), 3.0f);
 }
 
 // Frozen cells carry their distance with the sign bit set (U >= 0 everywhere else).
@@ -94,12 +96,13 @@ __device__ __forceinline__ float eik_init_cell(const float* __restrict__ phi0, l
                  (v * oyp < 0.0f) || (v * ozm < 0.0f) || (v * ozp < 0.0f);
     if (SEED && v == 0.0f) return -0.0f;
     if (iface) {
-        float gx = (oxp - oxm) * 0.5f * inv_dx;
-        float gy = (oyp - oym) * 0.5f * inv_dx;
-        float gz = (ozp - ozm) * 0.5f * inv_dx;
-        float grad0 = fmaxf(sqrtf(gx * gx + gy * gy + gz * gz), 0.5f);
-        float dxl = 1.0f / inv_dx;
-        float D = fminf(fabsf(v) / grad0, 1.8f * dxl);
+        const float gx = __fmul_rn(__fmul_rn(__fsub_rn(oxp, oxm), 0.5f), inv_dx);
+        const float gy = __fmul_rn(__fmul_rn(__fsub_rn(oyp, oym), 0.5f), inv_dx);
+        const float gz = __fmul_rn(__fmul_rn(__fsub_rn(ozp, ozm), 0.5f), inv_dx);
+        const float gg = __fadd_rn(__fadd_rn(__fmul_rn(gx, gx), __fmul_rn(gy, gy)), __fmul_rn(gz, gz));
+        const float grad0 = fmaxf(__fsqrt_rn(gg), 0.5f);
+        const float dxl = __fdiv_rn(1.0f, inv_dx);
+        const float D = fminf(__fdiv_rn(fabsf(v), grad0), __fmul_rn(1.8f, dxl));
         return copysignf(D, -1.0f);
     }
     return big;
@@ -132,9 +135,23 @@ __device__ __forceinline__ float eik_sweep_cell(const float* __restrict__ Uin, l
     if (FINAL) {
         float s = phi_in[c];
         float sg = s < 0.0f ? -1.0f : (SEED && s == 0.0f ? 0.0f : 1.0f);
-        return sg * fminf(un, cap) + 0.0f;
+        return __fadd_rn(__fmul_rn(sg, fminf(un, cap)), 0.0f);
     }
     return un;
+}
+
+// run_etch_3d's CFL substep count (threed.py:1750-1756) from the device-side rate statistics:
+// nsub = clamp(ceil(Vmax dt / (0.4 dx)), 1, 160), Vmax = max(max V if finite (0 without faces),
+// 1e-6); sub[0] = nsub, sub[1] = float bits of float(dt / nsub).
+__device__ __forceinline__ void cfl_substeps(int n_faces, const int* stats, double dt, double dx,
+                                             int* sub) {
+    const float vmx = n_faces > 0 ? __int_as_float(stats[1]) : 0.0f;
+    double V = isfinite(vmx) ? (double)vmx : 0.0;
+    V = fmax(V, 1e-6);
+    const double q = ceil(V * dt / (0.4 * dx));
+    const int nsub = (int)fmin(fmax(q, 1.0), 160.0);
+    sub[0] = nsub;
+    sub[1] = __float_as_int((float)(dt / nsub));
 }
 
 }  // namespace petch

@@ -6,6 +6,7 @@
 //   * Eikonal reinit: init, Jacobi sweeps, finalisation (reinit_fsm, threed.py:1421-1537);
 //   * velocity extension (extend_velocity_gpu, threed.py:1324-1346): dF = dV[nearest face];
 //   * coverage warm start (gpu_warmstart_bare, threed.py:1619-1639).
+#include <cmath>
 #include "common.cuh"
 #include "dual.cuh"
 #include "levelset.cuh"
@@ -35,24 +36,22 @@ __device__ __forceinline__ void dstore(float* __restrict__ v, float* __restrict_
     for (int k = 0; k < ND; ++k) d[c + k * n] = x.d[k];
 }
 
-// One substep of the mask-array advection with tangents (values equal petch_advect's).
-__global__ void __launch_bounds__(kTanB) k_advect_tan(const float* __restrict__ phi,
-                                                      const float* __restrict__ dphi,
-                                                      float* __restrict__ out,
-                                                      float* __restrict__ dout,
-                                                      const float* __restrict__ F,
-                                                      const float* __restrict__ dF,
-                                                      const uint8_t* __restrict__ mask,
-                                                      const float* __restrict__ mask_phi, LGrid g,
-                                                      float inv_dx, float dt) {
+// One cell of a mask-array advection substep with tangents (the value equals petch_advect's).
+__device__ __forceinline__ void advect_tan_cell(const float* __restrict__ phi,
+                                                const float* __restrict__ dphi,
+                                                float* __restrict__ out, float* __restrict__ dout,
+                                                const float* __restrict__ F,
+                                                const float* __restrict__ dF,
+                                                const uint8_t* __restrict__ mask,
+                                                const float* __restrict__ mask_phi, const LGrid& g,
+                                                float inv_dx, float dt, long long c) {
     const long long n = g.n;
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
-         c += (long long)gridDim.x * blockDim.x) {
+    {
         if (mask[c]) {
             out[c] = mask_phi[c];
 #pragma unroll
             for (int k = 0; k < ND; ++k) dout[c + k * n] = 0.0f;
-            continue;
+            return;
         }
         const D3 v = dload(phi, dphi, c, n);
         const D3 f = dload(F, dF, c, n);
@@ -78,6 +77,20 @@ __global__ void __launch_bounds__(kTanB) k_advect_tan(const float* __restrict__ 
     }
 }
 
+__global__ void __launch_bounds__(kTanB) k_advect_tan(const float* __restrict__ phi,
+                                                      const float* __restrict__ dphi,
+                                                      float* __restrict__ out,
+                                                      float* __restrict__ dout,
+                                                      const float* __restrict__ F,
+                                                      const float* __restrict__ dF,
+                                                      const uint8_t* __restrict__ mask,
+                                                      const float* __restrict__ mask_phi, LGrid g,
+                                                      float inv_dx, float dt) {
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.n;
+         c += (long long)gridDim.x * blockDim.x)
+        advect_tan_cell(phi, dphi, out, dout, F, dF, mask, mask_phi, g, inv_dx, dt, c);
+}
+
 // eik_solve with tangents (same sort and branch structure as the primal).
 __device__ __forceinline__ D3 eik_solve_tan(D3 a1, D3 a2, D3 a3, float dx) {
     D3 t;
@@ -97,14 +110,13 @@ __device__ __forceinline__ D3 eik_solve_tan(D3 a1, D3 a2, D3 a3, float dx) {
     return (s1 + vsqrt(d3)) / 3.0f;
 }
 
-__global__ void __launch_bounds__(kTanB) k_eik_init_tan(const float* __restrict__ phi0,
-                                                        const float* __restrict__ dphi0,
-                                                        float* __restrict__ U,
-                                                        float* __restrict__ dU, LGrid g,
-                                                        float inv_dx, float big) {
+__device__ __forceinline__ void eik_init_tan_cell(const float* __restrict__ phi0,
+                                                  const float* __restrict__ dphi0,
+                                                  float* __restrict__ U, float* __restrict__ dU,
+                                                  const LGrid& g, float inv_dx, float big,
+                                                  long long c) {
     const long long n = g.n;
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
-         c += (long long)gridDim.x * blockDim.x) {
+    {
         int i, j, k;
         lsplit(g, c, i, j, k);
         const D3 v = dload(phi0, dphi0, c, n);
@@ -133,18 +145,27 @@ __global__ void __launch_bounds__(kTanB) k_eik_init_tan(const float* __restrict_
     }
 }
 
+__global__ void __launch_bounds__(kTanB) k_eik_init_tan(const float* __restrict__ phi0,
+                                                        const float* __restrict__ dphi0,
+                                                        float* __restrict__ U,
+                                                        float* __restrict__ dU, LGrid g,
+                                                        float inv_dx, float big) {
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.n;
+         c += (long long)gridDim.x * blockDim.x)
+        eik_init_tan_cell(phi0, dphi0, U, dU, g, inv_dx, big, c);
+}
+
 template <bool FINAL>
-__global__ void __launch_bounds__(kTanB) k_eik_sweep_tan(const float* __restrict__ Uin,
-                                                         const float* __restrict__ dUin,
-                                                         float* __restrict__ Uout,
-                                                         float* __restrict__ dUout,
-                                                         const float* __restrict__ phi_in,
-                                                         float* __restrict__ phi_out,
-                                                         float* __restrict__ dphi_out, LGrid g,
-                                                         float dx, float big, float cap) {
+__device__ __forceinline__ void eik_sweep_tan_cell(const float* __restrict__ Uin,
+                                                   const float* __restrict__ dUin,
+                                                   float* __restrict__ Uout,
+                                                   float* __restrict__ dUout,
+                                                   const float* __restrict__ phi_in,
+                                                   float* __restrict__ phi_out,
+                                                   float* __restrict__ dphi_out, const LGrid& g,
+                                                   float dx, float big, float cap, long long c) {
     const long long n = g.n;
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
-         c += (long long)gridDim.x * blockDim.x) {
+    {
         const D3 u = dload(Uin, dUin, c, n);
         D3 un;
         if (frozen(u.v)) {
@@ -175,6 +196,21 @@ __global__ void __launch_bounds__(kTanB) k_eik_sweep_tan(const float* __restrict
             dstore(Uout, dUout, c, n, un);
         }
     }
+}
+
+template <bool FINAL>
+__global__ void __launch_bounds__(kTanB) k_eik_sweep_tan(const float* __restrict__ Uin,
+                                                         const float* __restrict__ dUin,
+                                                         float* __restrict__ Uout,
+                                                         float* __restrict__ dUout,
+                                                         const float* __restrict__ phi_in,
+                                                         float* __restrict__ phi_out,
+                                                         float* __restrict__ dphi_out, LGrid g,
+                                                         float dx, float big, float cap) {
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.n;
+         c += (long long)gridDim.x * blockDim.x)
+        eik_sweep_tan_cell<FINAL>(Uin, dUin, Uout, dUout, phi_in, phi_out, dphi_out, g, dx, big,
+                                  cap, c);
 }
 
 struct TGrid {
@@ -227,6 +263,146 @@ __global__ void __launch_bounds__(kTanB) k_warmstart_tan(MeshView prev,
         for (int k = 0; k < ND; ++k) dbare[f + k * MT] = pass ? prev_dbare[q + k * PMT] : 0.0f;
     }
     if (err) atomicOr(work + 1, err);
+}
+
+// ---- batched tangent level-set stages: blockIdx.y selects the instance ----
+constexpr int kTMaxInst = 64;
+
+struct TBItem {
+    float* phi;
+    float* tmp;
+    float* ua;
+    float* ub;
+    const float* F;
+    const float* mask_phi;
+    float* dphi;
+    float* dtmp;
+    float* dua;
+    float* dub;
+    const float* dF;
+    const uint8_t* mask;
+    LGrid g;
+    double dx, dt;
+    const int* stats;
+    const int* hdr;
+    int* sub;
+};
+
+struct TBTable {
+    TBItem it[kTMaxInst];
+    int B;
+};
+
+__global__ void k_bt_nsub(TBTable t) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= t.B) return;
+    const TBItem& x = t.it[b];
+    cfl_substeps(x.hdr[HDR_F], x.stats, x.dt, x.dx, x.sub);
+}
+
+// Substep s of every instance with s < nsub (dense, mask array; buffers of parity s into the
+// other).
+__global__ void __launch_bounds__(kTanB) k_bt_adv(TBTable t, int s) {
+    const int b = blockIdx.y;
+    if (b >= t.B) return;
+    const TBItem& x = t.it[b];
+    if (s >= x.sub[0]) return;
+    const float* a = (s & 1) ? x.tmp : x.phi;
+    const float* da = (s & 1) ? x.dtmp : x.dphi;
+    float* o = (s & 1) ? x.phi : x.tmp;
+    float* dout = (s & 1) ? x.dphi : x.dtmp;
+    const float inv_dx = (float)(1.0 / x.dx);
+    const float dt = __int_as_float(x.sub[1]);
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < x.g.n;
+         c += (long long)gridDim.x * blockDim.x)
+        advect_tan_cell(a, da, o, dout, x.F, x.dF, x.mask, x.mask_phi, x.g, inv_dx, dt, c);
+}
+
+// After an odd number of substeps the state lives in tmp / dtmp: copy it back.
+__global__ void k_bt_adv_finish(TBTable t) {
+    const int b = blockIdx.y;
+    if (b >= t.B) return;
+    const TBItem& x = t.it[b];
+    if ((x.sub[0] & 1) == 0) return;
+    const long long n = x.g.n;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
+         c += (long long)gridDim.x * blockDim.x) {
+        x.phi[c] = x.tmp[c];
+#pragma unroll
+        for (int k = 0; k < ND; ++k) x.dphi[c + k * n] = x.dtmp[c + k * n];
+    }
+}
+
+__global__ void __launch_bounds__(kTanB) k_bt_eik_init(TBTable t, double band_r) {
+    const int b = blockIdx.y;
+    if (b >= t.B) return;
+    const TBItem& x = t.it[b];
+    const float inv_dx = (float)(1.0 / x.dx);
+    const float big = (float)(band_r + 4.0 * x.dx);
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < x.g.n;
+         c += (long long)gridDim.x * blockDim.x)
+        eik_init_tan_cell(x.phi, x.dphi, x.ua, x.dua, x.g, inv_dx, big, c);
+}
+
+template <bool FINAL>
+__global__ void __launch_bounds__(kTanB) k_bt_eik_sweep(TBTable t, double band_r, int parity) {
+    const int b = blockIdx.y;
+    if (b >= t.B) return;
+    const TBItem& x = t.it[b];
+    const float* in = parity ? x.ub : x.ua;
+    const float* din = parity ? x.dub : x.dua;
+    float* out = parity ? x.ua : x.ub;
+    float* dout = parity ? x.dua : x.dub;
+    const float dxf = (float)x.dx;
+    const float big = (float)(band_r + 4.0 * x.dx), cap = (float)(band_r + x.dx);
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < x.g.n;
+         c += (long long)gridDim.x * blockDim.x) {
+        if (FINAL)
+            eik_sweep_tan_cell<true>(in, din, nullptr, nullptr, x.phi, x.phi, x.dphi, x.g, dxf, big,
+                                     cap, c);
+        else
+            eik_sweep_tan_cell<false>(in, din, out, dout, nullptr, nullptr, nullptr, x.g, dxf, big,
+                                      cap, c);
+    }
+}
+
+int make_ttable(const petch_batch_grid* grids, const petch_batch_tangent_grid* tans, int B,
+                TBTable* t, long long* max_cells, const char* who) {
+    PETCH_REQUIRE(grids && tans, "%s: null table", who);
+    PETCH_REQUIRE(B >= 1 && B <= kTMaxInst, "%s: 1 <= B <= %d", who, kTMaxInst);
+    t->B = B;
+    long long mc = 0;
+    for (int b = 0; b < B; ++b) {
+        const petch_batch_grid& s = grids[b];
+        const petch_batch_tangent_grid& d = tans[b];
+        PETCH_REQUIRE(s.phi && s.tmp && s.ua && s.ub && s.F && s.mask_phi && s.stats && s.hdr &&
+                          s.sub && d.dphi && d.dtmp && d.dF && d.mask && d.du_a && d.du_b,
+                      "%s: instance %d incomplete", who, b);
+        PETCH_REQUIRE(s.nx > 0 && s.ny > 0 && s.nz > 0 && s.dx > 0.0 && s.dt >= 0.0,
+                      "%s: instance %d has a bad size", who, b);
+        TBItem& x = t->it[b];
+        x.phi = s.phi;
+        x.tmp = s.tmp;
+        x.ua = s.ua;
+        x.ub = s.ub;
+        x.F = s.F;
+        x.mask_phi = s.mask_phi;
+        x.dphi = d.dphi;
+        x.dtmp = d.dtmp;
+        x.dua = d.du_a;
+        x.dub = d.du_b;
+        x.dF = d.dF;
+        x.mask = d.mask;
+        x.g = make_lgrid(s.nx, s.ny, s.nz);
+        x.dx = s.dx;
+        x.dt = s.dt;
+        x.stats = s.stats;
+        x.hdr = s.hdr;
+        x.sub = s.sub;
+        if (x.g.n > mc) mc = x.g.n;
+    }
+    *max_cells = mc;
+    return PETCH_OK;
 }
 
 }  // namespace
@@ -311,5 +487,51 @@ extern "C" int petch_warmstart_tangent(const void* prev_mesh, int prev_max_tris,
                                                                               prev_dbare, m, dbare,
                                                                               work);
     PETCH_LAUNCH_CHECK("k_warmstart_tan");
+    return PETCH_OK;
+}
+
+extern "C" int petch_batch_advect_tangent(const petch_batch_grid* grids,
+                                          const petch_batch_tangent_grid* tans, int B,
+                                          void* stream) {
+    TBTable t;
+    long long mc = 0;
+    int rc = make_ttable(grids, tans, B, &t, &mc, "petch_batch_advect_tangent");
+    if (rc) return rc;
+    cudaStream_t st = as_stream(stream);
+    k_bt_nsub<<<1, kTMaxInst, 0, st>>>(t);
+    PETCH_LAUNCH_CHECK("k_bt_nsub");
+    dim3 gc(grid_for(mc, kTanB, 2), B);
+    for (int s = 0; s < 160; ++s) {
+        k_bt_adv<<<gc, kTanB, 0, st>>>(t, s);
+        PETCH_LAUNCH_CHECK("k_bt_adv");
+    }
+    k_bt_adv_finish<<<gc, kTanB, 0, st>>>(t);
+    PETCH_LAUNCH_CHECK("k_bt_adv_finish");
+    return PETCH_OK;
+}
+
+extern "C" int petch_batch_reinit_tangent(const petch_batch_grid* grids,
+                                          const petch_batch_tangent_grid* tans, int B,
+                                          double band_r, void* stream) {
+    TBTable t;
+    long long mc = 0;
+    int rc = make_ttable(grids, tans, B, &t, &mc, "petch_batch_reinit_tangent");
+    if (rc) return rc;
+    const double dx = grids[0].dx;
+    for (int b = 1; b < B; ++b)
+        PETCH_REQUIRE(grids[b].dx == dx, "petch_batch_reinit_tangent: all grids need the same dx");
+    const int n_iter = (int)std::ceil(band_r / dx) + 4;
+    cudaStream_t st = as_stream(stream);
+    dim3 gc(grid_for(mc, kTanB, 2), B);
+    k_bt_eik_init<<<gc, kTanB, 0, st>>>(t, band_r);
+    PETCH_LAUNCH_CHECK("k_bt_eik_init");
+    int parity = 0;
+    for (int it = 0; it < n_iter - 1; ++it) {
+        k_bt_eik_sweep<false><<<gc, kTanB, 0, st>>>(t, band_r, parity);
+        PETCH_LAUNCH_CHECK("k_bt_eik_sweep");
+        parity ^= 1;
+    }
+    k_bt_eik_sweep<true><<<gc, kTanB, 0, st>>>(t, band_r, parity);
+    PETCH_LAUNCH_CHECK("k_bt_eik_sweep<final>");
     return PETCH_OK;
 }

@@ -18,7 +18,11 @@ namespace petch {
 namespace {
 
 constexpr int kTB = 128;
-constexpr int kTraceMinBlocks = 8;   // 8 blocks x 4 warps per SM: <= 64 registers per thread
+#ifndef PETCH_TRACE_MIN_BLOCKS
+#define PETCH_TRACE_MIN_BLOCKS 8
+#endif
+// resident blocks of the persistent tracers per SM (8 x 4 warps: <= 64 registers per thread)
+constexpr int kTraceMinBlocks = PETCH_TRACE_MIN_BLOCKS;
 constexpr long long kMaxRounds = 1LL << 24;   // per-warp bound on tracer rounds (error bit 4)
 constexpr unsigned kFull = 0xffffffffu;
 
@@ -651,8 +655,16 @@ struct BatchItem {
     uint32_t seed;
 };
 
+// Tangent outputs of a batched tangent trace: dout = d(ion tallies) [3][MT] or d(neutral flux)
+// [3][MT]; dbare = the coverage tangents [3][MT] (neutrals; NULL = 0).
+struct BatchTan {
+    float* dout;
+    const float* dbare;
+};
+
 struct BatchTable {
     BatchItem it[kMaxBatch];
+    BatchTan tn[kMaxBatch];
     int B;
     int total;
 };
@@ -687,8 +699,9 @@ __device__ __forceinline__ MeshView view_at(const char* base, const MeshOffsets&
     return v;
 }
 
-// Zero each instance's tallies on its live faces (blockIdx.y = instance).
-__global__ void k_zero_batch(BatchTable tab, MeshOffsets L, int MT, int MV, int per_face) {
+// Zero each instance's tallies on its live faces (blockIdx.y = instance), and with tan the three
+// tangent directions of dout.
+__global__ void k_zero_batch(BatchTable tab, MeshOffsets L, int MT, int MV, int per_face, int tan) {
     const int b = blockIdx.y;
     if (b >= tab.B) return;
     const BatchItem& it = tab.it[b];
@@ -698,9 +711,14 @@ __global__ void k_zero_batch(BatchTable tab, MeshOffsets L, int MT, int MV, int 
     if (it.ang)
         for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < F; i += gridDim.x * blockDim.x)
             it.ang[i] = 0.0f;
+    if (tan)
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < F; i += gridDim.x * blockDim.x)
+            for (int k = 0; k < 3; ++k) tab.tn[b].dout[i + (long long)k * MT] = 0.0f;
 }
 
-template <bool ION>
+// KIND: 0 ions, 1 neutrals, 2 ions with energy tangents, 3 neutrals with weight tangents (the
+// single-instance tangent shaders' hit functions, outputs per instance from tab.tn).
+template <int KIND>
 __global__ void __launch_bounds__(kTB, kTraceMinBlocks) k_trace_batch(BatchTable tab, MeshOffsets L,
                                                                      int MT, int MV, float beta,
                                                                      const int* step,
@@ -708,10 +726,14 @@ __global__ void __launch_bounds__(kTB, kTraceMinBlocks) k_trace_batch(BatchTable
                                                                      uint32_t seed_add,
                                                                      uint32_t domain, int steps,
                                                                      int keep, int det, int* work) {
+    constexpr bool ION = KIND == 0 || KIND == 2;
+    constexpr bool TAN = KIND >= 2;
     __shared__ BatchItem s_it[kMaxBatch];
+    __shared__ BatchTan s_tn[kMaxBatch];
     __shared__ int s_start[kMaxBatch + 1];
     for (int i = threadIdx.x; i < tab.B; i += blockDim.x) {
         s_it[i] = tab.it[i];
+        s_tn[i] = tab.tn[i];
         s_start[i] = tab.it[i].ray_start;
     }
     if (threadIdx.x == 0) s_start[tab.B] = tab.total;
@@ -755,8 +777,10 @@ __global__ void __launch_bounds__(kTB, kTraceMinBlocks) k_trace_batch(BatchTable
             if (ION) {
                 source(g, true, it.P.sigma, it.D, o, d);
                 rs.E = fmaxf(it.P.meanE + it.P.sigmaE * g.normal(), 0.0f);
+                if (TAN) rs.dE = rs.E > 0.0f ? 1.0f : 0.0f;
             } else {
                 source(g, false, 0.0f, it.D, o, d);
+                if (TAN) rs.dw[0] = rs.dw[1] = rs.dw[2] = 0.0f;
             }
             rs.w = 1.0f;
             rs.bounce = 0;
@@ -783,9 +807,17 @@ __global__ void __launch_bounds__(kTB, kTraceMinBlocks) k_trace_batch(BatchTable
                 cont = it.D.periodic && rs.wraps < 256 && periodic_wrap(it.D, o, d);
                 if (cont) ++rs.wraps;
             } else {
-                cont = ION ? ion_hit(it.P, reinterpret_cast<float4*>(it.out), it.ang, g, T, q.f,
-                                     q.t, o, d, rs, det)
-                           : neutral_hit(it.bare, beta, it.out, g, T, q.f, q.t, o, d, rs, det);
+                if (KIND == 0)
+                    cont = ion_hit(it.P, reinterpret_cast<float4*>(it.out), it.ang, g, T, q.f, q.t,
+                                   o, d, rs, det);
+                else if (KIND == 1)
+                    cont = neutral_hit(it.bare, beta, it.out, g, T, q.f, q.t, o, d, rs, det);
+                else if (KIND == 2)
+                    cont = ion_hit<true>(it.P, reinterpret_cast<float4*>(it.out), it.ang, g, T,
+                                         q.f, q.t, o, d, rs, det, s_tn[inst].dout);
+                else
+                    cont = neutral_hit_tan(it.bare, s_tn[inst].dbare, beta, it.out,
+                                           s_tn[inst].dout, g, T, q.f, q.t, o, d, rs, det);
                 rs.wraps = 0;
                 if (cont && ++rs.bounce >= 1024) cont = false;
             }
@@ -1109,8 +1141,10 @@ extern "C" int petch_trace_ff(const void* mesh, int max_tris, int max_verts,
 
 extern "C" int petch_prepare_device(void) {
     sm_count();
-    persistent_blocks((const void*)k_trace_batch<true>, kTB, 0);
-    persistent_blocks((const void*)k_trace_batch<false>, kTB, 0);
+    persistent_blocks((const void*)k_trace_batch<0>, kTB, 0);
+    persistent_blocks((const void*)k_trace_batch<1>, kTB, 0);
+    persistent_blocks((const void*)k_trace_batch<2>, kTB, 0);
+    persistent_blocks((const void*)k_trace_batch<3>, kTB, 0);
     persistent_blocks((const void*)k_trace<IonShader, false>, kTB);
     persistent_blocks((const void*)k_trace<NeutralShader, false>, kTB);
     persistent_blocks((const void*)k_trace<LegacyShader, false>, kTB);
@@ -1120,20 +1154,33 @@ extern "C" int petch_prepare_device(void) {
     return PETCH_OK;
 }
 
-extern "C" int petch_trace_batch(int kind, const petch_batch_item* items, int B, int max_tris,
-                                 int max_verts, float beta, const int* step, uint32_t seed_mul,
-                                 uint32_t seed_add, int* work, void* stream) {
-    PETCH_REQUIRE(items && work, "petch_trace_batch: null pointer");
-    PETCH_REQUIRE(kind == 0 || kind == 1, "petch_trace_batch: kind must be 0 (ions) or 1 (neutrals)");
-    PETCH_REQUIRE(B >= 1 && B <= kMaxBatch, "petch_trace_batch: 1 <= B <= %d", kMaxBatch);
-    PETCH_REQUIRE(max_tris > 0 && max_verts > 0, "petch_trace_batch: bad capacities");
+namespace {
+
+template <int KIND>
+void launch_batch(const BatchTable& tab, const MeshOffsets& L, int max_tris, int max_verts,
+                  float beta, const int* step, uint32_t seed_mul, uint32_t seed_add,
+                  uint32_t domain, int det, int* work, cudaStream_t st) {
+    k_trace_batch<KIND><<<persistent_blocks((const void*)k_trace_batch<KIND>, kTB, 0), kTB, 0, st>>>(
+        tab, L, max_tris, max_verts, beta, step, seed_mul, seed_add, domain, g_steps, g_keep, det,
+        work);
+}
+
+// kind: 0 ions, 1 neutrals, 2 ions with energy tangents, 3 neutrals with weight tangents.
+int trace_batch(int kind, const petch_batch_item* items, const petch_batch_tangent* tans, int B,
+                int max_tris, int max_verts, float beta, const int* step, uint32_t seed_mul,
+                uint32_t seed_add, int* work, void* stream, const char* who) {
+    PETCH_REQUIRE(items && work, "%s: null pointer", who);
+    PETCH_REQUIRE(B >= 1 && B <= kMaxBatch, "%s: 1 <= B <= %d", who, kMaxBatch);
+    PETCH_REQUIRE(max_tris > 0 && max_verts > 0, "%s: bad capacities", who);
+    const bool ion = kind == 0 || kind == 2, tan = kind >= 2;
+    PETCH_REQUIRE(!tan || tans, "%s: null tangent table", who);
     BatchTable tab;
     long long total = 0;
     for (int b = 0; b < B; ++b) {
         const petch_batch_item& x = items[b];
-        PETCH_REQUIRE(x.mesh && x.out && x.n_rays >= 0, "petch_trace_batch: item %d incomplete", b);
-        PETCH_REQUIRE(kind == 1 || (x.ang && ((uintptr_t)x.out & 15) == 0),
-                      "petch_trace_batch: ion item %d needs ang and a 16-byte aligned tally", b);
+        PETCH_REQUIRE(x.mesh && x.out && x.n_rays >= 0, "%s: item %d incomplete", who, b);
+        PETCH_REQUIRE(!ion || (x.ang && ((uintptr_t)x.out & 15) == 0),
+                      "%s: ion item %d needs ang and a 16-byte aligned tally", who, b);
         BatchItem& it = tab.it[b];
         it.mesh = (const char*)x.mesh;
         it.D = to_domain(&x.dom);
@@ -1142,12 +1189,19 @@ extern "C" int petch_trace_batch(int kind, const petch_batch_item* items, int B,
                     p.inflect, p.minang, p.n_l, p.A_en, p.minE, p.thrmin, p.thrmax, p.sigma};
         it.bare = x.bare;
         it.out = x.out;
-        it.ang = kind == 0 ? x.ang : nullptr;
+        it.ang = ion ? x.ang : nullptr;
         it.ray_start = (int)total;
         it.seed = x.seed;
+        tab.tn[b].dout = nullptr;
+        tab.tn[b].dbare = nullptr;
+        if (tan) {
+            PETCH_REQUIRE(tans[b].dout, "%s: tangent item %d has no output", who, b);
+            tab.tn[b].dout = tans[b].dout;
+            tab.tn[b].dbare = ion ? nullptr : tans[b].dbare;
+        }
         total += x.n_rays;
     }
-    PETCH_REQUIRE(total < (1LL << 31), "petch_trace_batch: more than 2^31 - 1 rays");
+    PETCH_REQUIRE(total < (1LL << 31), "%s: more than 2^31 - 1 rays", who);
     tab.B = B;
     tab.total = (int)total;
     MeshOffsets L;
@@ -1155,45 +1209,70 @@ extern "C" int petch_trace_batch(int kind, const petch_batch_item* items, int B,
     for (int i = 0; i < SEG_COUNT; ++i) L.off[i] = ml.off[i];
     cudaStream_t st = as_stream(stream);
     dim3 zg(grid_for(4LL * max_tris, 256, 2), B);
-    k_zero_batch<<<zg, 256, 0, st>>>(tab, L, max_tris, max_verts, kind == 0 ? 4 : 1);
+    k_zero_batch<<<zg, 256, 0, st>>>(tab, L, max_tris, max_verts, ion ? 4 : 1, tan ? 1 : 0);
     PETCH_LAUNCH_CHECK("k_zero_batch");
     PETCH_CUDA(cudaMemsetAsync(work, 0, sizeof(int), st), "reset ray counter");
     if (total == 0) return PETCH_OK;
-    const uint32_t domain = kind == 0 ? 0x696f6e73u : 0x6e657500u;
+    const uint32_t domain = ion ? 0x696f6e73u : 0x6e657500u;
     DetArena arena;
     const int det = arena.on() ? 1 : 0;
-    const long long per_out = (kind == 0 ? 4LL : 1LL) * max_tris;
+    const long long per_out = (ion ? 4LL : 1LL) * max_tris;
     long long* acc_out[kMaxBatch] = {};
     long long* acc_ang[kMaxBatch] = {};
+    long long* acc_d[kMaxBatch] = {};
     if (det) {
         for (int b = 0; b < B; ++b) {
             PETCH_DET_TAKE(ao, per_out);
             acc_out[b] = ao;
             tab.it[b].out = reinterpret_cast<float*>(ao);
-            if (kind == 0) {
+            if (ion) {
                 PETCH_DET_TAKE(aa, (long long)max_tris);
                 acc_ang[b] = aa;
                 tab.it[b].ang = reinterpret_cast<float*>(aa);
             }
+            if (tan) {
+                PETCH_DET_TAKE(ad, 3LL * max_tris);
+                acc_d[b] = ad;
+                tab.tn[b].dout = reinterpret_cast<float*>(ad);
+            }
         }
     }
-    if (kind == 0) {
-        k_trace_batch<true><<<persistent_blocks((const void*)k_trace_batch<true>, kTB, 0), kTB, 0, st>>>(
-            tab, L, max_tris, max_verts, beta, step, seed_mul, seed_add, domain, g_steps, g_keep,
-            det, work);
-    } else {
-        k_trace_batch<false><<<persistent_blocks((const void*)k_trace_batch<false>, kTB, 0), kTB, 0, st>>>(
-            tab, L, max_tris, max_verts, beta, step, seed_mul, seed_add, domain, g_steps, g_keep,
-            det, work);
+    switch (kind) {
+        case 0: launch_batch<0>(tab, L, max_tris, max_verts, beta, step, seed_mul, seed_add, domain, det, work, st); break;
+        case 1: launch_batch<1>(tab, L, max_tris, max_verts, beta, step, seed_mul, seed_add, domain, det, work, st); break;
+        case 2: launch_batch<2>(tab, L, max_tris, max_verts, beta, step, seed_mul, seed_add, domain, det, work, st); break;
+        default: launch_batch<3>(tab, L, max_tris, max_verts, beta, step, seed_mul, seed_add, domain, det, work, st); break;
     }
     PETCH_LAUNCH_CHECK("k_trace_batch");
     if (det) {
         for (int b = 0; b < B; ++b) {
             PETCH_DET_CONVERT(acc_out[b], items[b].out, per_out);
-            if (kind == 0) PETCH_DET_CONVERT(acc_ang[b], items[b].ang, (long long)max_tris);
+            if (ion) PETCH_DET_CONVERT(acc_ang[b], items[b].ang, (long long)max_tris);
+            if (tan) PETCH_DET_CONVERT(acc_d[b], tans[b].dout, 3LL * max_tris);
         }
     }
     return PETCH_OK;
+}
+
+}  // namespace
+
+extern "C" int petch_trace_batch(int kind, const petch_batch_item* items, int B, int max_tris,
+                                 int max_verts, float beta, const int* step, uint32_t seed_mul,
+                                 uint32_t seed_add, int* work, void* stream) {
+    PETCH_REQUIRE(kind == 0 || kind == 1, "petch_trace_batch: kind must be 0 (ions) or 1 (neutrals)");
+    return trace_batch(kind, items, nullptr, B, max_tris, max_verts, beta, step, seed_mul,
+                       seed_add, work, stream, "petch_trace_batch");
+}
+
+extern "C" int petch_trace_batch_tangent(int kind, const petch_batch_item* items,
+                                         const petch_batch_tangent* tans, int B, int max_tris,
+                                         int max_verts, float beta, const int* step,
+                                         uint32_t seed_mul, uint32_t seed_add, int* work,
+                                         void* stream) {
+    PETCH_REQUIRE(kind == 0 || kind == 1,
+                  "petch_trace_batch_tangent: kind must be 0 (ions) or 1 (neutrals)");
+    return trace_batch(kind + 2, items, tans, B, max_tris, max_verts, beta, step, seed_mul,
+                       seed_add, work, stream, "petch_trace_batch_tangent");
 }
 
 extern "C" int petch_redep_scratch_bytes(int max_tris, long long* bytes) {

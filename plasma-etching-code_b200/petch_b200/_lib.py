@@ -59,6 +59,17 @@ class BatchGrid(ctypes.Structure):
                 ("stats", ctypes.c_void_p), ("hdr", ctypes.c_void_p), ("sub", ctypes.c_void_p)]
 
 
+class BatchTangent(ctypes.Structure):
+    """petch_batch_tangent."""
+    _fields_ = [("dout", ctypes.c_void_p), ("dbare", ctypes.c_void_p)]
+
+
+class BatchTangentGrid(ctypes.Structure):
+    """petch_batch_tangent_grid."""
+    _fields_ = [("dphi", ctypes.c_void_p), ("dtmp", ctypes.c_void_p), ("dF", ctypes.c_void_p),
+                ("mask", ctypes.c_void_p), ("du_a", ctypes.c_void_p), ("du_b", ctypes.c_void_p)]
+
+
 DP = ctypes.POINTER(Domain)
 IP = ctypes.POINTER(IonParams)
 CP = ctypes.POINTER(ChemParams)
@@ -126,6 +137,9 @@ SIGNATURES = {
     "petch_batch_advect": [P, I, P],
     "petch_batch_reinit": [P, I, D, P],
     "petch_batch_step_advance": [P, P],
+    "petch_trace_batch_tangent": [I, P, P, I, I, I, F, P, U, U, P, P],
+    "petch_batch_advect_tangent": [P, P, I, P],
+    "petch_batch_reinit_tangent": [P, P, I, D, P],
 }
 
 # The library's tracer configuration at load (bvh_width, steps_per_round, keep_lanes): what

@@ -238,17 +238,19 @@ def run_etch_3d_tangent(theta, Lx, Ly, Lz, dx, trench_width, mask_th, sub_top, t
 
 
 def radial_profile(phi, geo, dphi=None, n_bins=32):
-    """Zero-level-set depth profile of a hole: per column (i, j), the depth below sub_top of the
-    lowest zero crossing of the gas run connected to the top of the grid (linear interpolation
-    between the last gas node and the solid node under it; the grid floor if the run reaches it),
-    averaged over n_bins equal radial bins of the column's distance from the hole axis (out to
-    min(Lx, Ly) / 2).  Returns (profile[n_bins], jac[n_bins, 3] or None); empty bins are NaN."""
+    """Zero-level-set depth profile of a hole (geo['hole'] true or absent) or a trench: per column
+    (i, j), the depth below sub_top of the lowest zero crossing of the gas run connected to the top
+    of the grid (linear interpolation between the last gas node and the solid node under it; the
+    grid floor if the run reaches it), averaged over n_bins equal bins of the column's distance
+    from the hole axis (out to min(Lx, Ly) / 2) or from the trench's mid-plane x = Lx / 2 (out to
+    Lx / 2).  Returns (profile[n_bins], jac[n_bins, 3] or None); empty bins are NaN."""
     phi = np.asarray(phi, np.float64)
     dx = geo['dx']
     nx, ny, nz = phi.shape
     xs, ys = np.arange(nx) * dx, np.arange(ny) * dx
     cx, cy = geo['Lx'] / 2.0, geo['Ly'] / 2.0
-    rmax = min(geo['Lx'], geo['Ly']) / 2.0
+    hole = geo.get('hole', True)
+    rmax = min(geo['Lx'], geo['Ly']) / 2.0 if hole else geo['Lx'] / 2.0
     gas = phi < 0
     # lowest gas node of the top-connected run: cumulative "all gas from the top"
     run = np.flip(np.cumprod(np.flip(gas, axis=2), axis=2), axis=2).astype(bool)
@@ -258,7 +260,7 @@ def radial_profile(phi, geo, dphi=None, n_bins=32):
     cnt = np.zeros(n_bins)
     jac = np.zeros((n_bins, ND)) if dphi is not None else None
     X, Y = np.meshgrid(xs - cx, ys - cy, indexing="ij")
-    R = np.hypot(X, Y)
+    R = np.hypot(X, Y) if hole else np.abs(X)
     b = np.floor(R / rmax * n_bins).astype(int)
     for i in range(nx):
         for j in range(ny):
