@@ -274,6 +274,73 @@ def published_config_summary():
                         "sub_top 18, 40 steps over 3.0, 30k rays, n_fp 1, warm start, fsm"}
 
 
+INV_N, INV_STEPS, INV_RAYS, INV_T_END, INV_PLAIN = 32, 20, 1 << 16, 0.5, 2
+
+
+def inverse_design_summary(world, rank, dist, iters):
+    """The batched inverse design: 32 periodic trenches (width U[1, 4] um, mask 1 um, dx 0.125,
+    substrate deep enough for aspect ratio 10), per-instance recipes drawn as the ragged forward
+    batch's, targets from the same simulator at recipes perturbed by U[-20 %, 20 %] (seed offset
+    1), 20 etch steps per forward + tangent pass, Adam on (ion energy, O/F, rate_scale).  `iters`
+    Adam iterations of the batched loop (instances sharded over ranks, losses all-gathered) against
+    the per-instance loop (run_etch_3d_tangent one instance after another) on a sample; both
+    follow the same Philox paths and tally deterministically, so their gradients are equal."""
+    import torch
+    from petch_b200 import _lib, inverse, params
+    flags = params.Flags(chemistry="belen", yield_angular="viennaps", coverage_sticking=True,
+                         ion_reflection=True, warm_start_coverage=True)
+    kw = dict(n_ion=INV_RAYS, n_neu=INV_RAYS, t_end=INV_T_END, n_steps=INV_STEPS)
+    specs, th0 = inverse.trench_batch_specs(INV_N, seed=0)
+    # deterministic tallies in both loops: the batched and the per-instance gradients are then
+    # the same numbers (one estimator, one set of paths), so "equal gradient error" holds exactly
+    from petch_b200.levelset import grid_shape
+    from petch_b200.threed import default_capacity
+    MT = max(default_capacity(grid_shape(s['Lx'], s['Ly'], s['Lz'], s['dx'])) for s in specs)
+    rng = np.random.default_rng(0)
+    th_t = th0 * (1.0 + rng.uniform(-0.2, 0.2, th0.shape))
+    targets = inverse.target_profiles(specs, th_t, flags, **kw)
+    _lib.set_deterministic(8 * len(inverse.shard(INV_N, world, rank)) * MT + (1 << 20))
+    grads = []
+    orig = inverse.loss_and_grad
+
+    def spy(prof, jac, target):
+        L, g = orig(prof, jac, target)
+        grads.append(g)
+        return L, g
+
+    inverse.loss_and_grad = spy
+    try:
+        torch.cuda.synchronize()
+        out = inverse.batched_inverse_design(specs, th0, targets, flags, n_iter=iters, world=world,
+                                             rank=rank, **kw)
+    finally:
+        inverse.loss_and_grad = orig
+    mine = inverse.shard(INV_N, world, rank)
+    torch.cuda.synchronize()
+    plain = [inverse.plain_inverse_design(specs[b], th0[b], targets[b], flags, n_iter=1,
+                                          max_tris=MT, **kw) for b in mine[:INV_PLAIN]]
+    _lib.set_deterministic(0)
+    plain_s = sum(p['seconds'] for p in plain)
+    sec, fwd, plain_s = rank_reduce([out['seconds'], out['forward_seconds'], plain_s], "max", dist,
+                                    world)
+    g_b = np.array(grads[:len(plain)])
+    g_p = np.array([p['grads'][0] for p in plain])
+    rel = float(np.max(np.abs(g_b - g_p)) / max(np.max(np.abs(g_p)), 1e-30))
+    loss = out['loss']
+    return {"value": INV_N * iters / sec, "unit": "instance-iterations/s", "seconds": sec,
+            "device_forward_seconds": fwd, "iterations": iters, "instances": INV_N,
+            "plain_loop": {"value": world * len(plain) / plain_s, "unit": "instance-iterations/s",
+                           "seconds": plain_s,
+                           "sample": f"{len(plain)} instances per rank, run_etch_3d_tangent"},
+            "gradient_rel_diff_vs_plain": rel,
+            "mean_loss_per_iteration": [float(np.nanmean(r)) for r in loss],
+            "workload": "32 periodic trenches (width U[1,4] um, mask 1 um, dx 0.125, AR-10 "
+                        "substrate), recipes as the ragged batch, targets at +-20% recipes seed 1, "
+                        "20 steps over 0.5 per pass, 2^16 rays per species per instance, Adam "
+                        "lr 0.05 on normalised (energy, O/F, rate_scale), deterministic tallies, "
+                        "seed 0"}
+
+
 BATCH_N, BATCH_STEPS, BATCH_RAYS, BATCH_T_END, BATCH_PLAIN_SAMPLE = 64, 30, 1 << 20, 3.0, 16
 
 
@@ -492,6 +559,8 @@ def run_b200(args):
         out["batched"] = batched_summary(world, rank, dist)
     if rank == 0 and not args.no_diff:
         out["differentiation"] = differentiation_summary()
+    if not args.no_inverse:
+        out["inverse_design"] = inverse_design_summary(world, rank, dist, args.inverse_iters)
     if rank == 0 and not args.no_published:
         out["published_config"] = published_config_summary()
     if rank == 0 and not args.no_e2e:
@@ -601,6 +670,8 @@ def main():
     ap.add_argument("--no-diff", action="store_true")
     ap.add_argument("--no-published", action="store_true")
     ap.add_argument("--no-transports", action="store_true")
+    ap.add_argument("--no-inverse", action="store_true")
+    ap.add_argument("--inverse-iters", type=int, default=3)
     args = ap.parse_args()
     if args.warmup < 0 or args.steps < 1 or args.warmup >= N_STEPS:
         raise SystemExit("need 0 <= warmup < 100 and steps >= 1")

@@ -492,6 +492,20 @@ int petch_dda_solve(int max_faces, int nx, int ny, int nz, int n_dirs, const flo
                     double betaE, double betaO, int n_reemit, void* scratch,
                     long long scratch_bytes, float* flux_E, float* flux_O, void* stream);
 
+/* petch_extend_velocity (nearest face) and petch_extend_tangent in one pass: the same nearest-face
+ * query gives Fs and dF (dV, dF: [3][max_tris] and [3][nx*ny*nz] tangents). */
+int petch_extend_velocity_dual(const void* mesh, int max_tris, int max_verts, const float* phi,
+                               const unsigned char* mask, int nx, int ny, int nz, double dx,
+                               double band, const float* V, const float* dV, float* Fs, float* dF,
+                               int fold_mask, int* active, int* n_active, int max_active,
+                               int* work, void* stream);
+
+/* petch_warmstart and petch_warmstart_tangent in one pass (one nearest-face query per face). */
+int petch_warmstart_dual(const void* prev_mesh, int prev_max_tris, int prev_max_verts,
+                         const float* prev_bare, const float* prev_dbare, const void* mesh,
+                         int max_tris, int max_verts, float* bare, float* dbare, int* work,
+                         void* stream);
+
 /* ---- Knudsen 1-D conductance tail (mc_flux_3d_knudsen, petch/threed.py:1149-1208) ----
  * petch_knudsen_prepare replaces slice_geometry (petch/knudsen.py:29-68) and the per-face part of
  * knudsen_face_flux (knudsen.py:188-241) that depends only on the geometry: per z-slice below

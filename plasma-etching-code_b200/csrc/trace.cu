@@ -861,13 +861,15 @@ struct GridArgs {
 // velocity of the nearest face (search radius first limited to band + 2 dx, widened to the
 // reference's 1e6 if nothing is found there); all other cells get 0.  With fold != 0, mask cells
 // are written as -1 (the advection's pinned-cell marker) and band cells with F > 0 are listed in
-// `active` for the sparse advection.
+// `active` for the sparse advection.  With dV (tangents [3][MT]) the same nearest face also gives
+// dF[c + k n] = dV[f + k MT] on the band (0 elsewhere), as petch_extend_tangent.
 template <bool CENTROID>
 __global__ void __launch_bounds__(kTB) k_extend(MeshView m, GridArgs G, const float* __restrict__ phi,
                                                 const uint8_t* __restrict__ mask,
                                                 const float* __restrict__ V, float* __restrict__ Fs,
                                                 int fold, int* active, int* n_active, int max_active,
-                                                int* work) {
+                                                int* work, const float* __restrict__ dV = nullptr,
+                                                float* __restrict__ dF = nullptr) {
     const int L = min(m.hdr[HDR_L], m.MT);
     int err = 0;
     const float r_near = (float)(G.band + 2.0 * G.dx);
@@ -876,6 +878,7 @@ __global__ void __launch_bounds__(kTB) k_extend(MeshView m, GridArgs G, const fl
         float v = phi[c];
         bool pinned = fold && mask && mask[c];
         float out = 0.0f;
+        float dout[3] = {0.0f, 0.0f, 0.0f};
         if ((double)fabsf(v) < G.band) {
             long long r = c / G.nz;
             int k = (int)(c - r * G.nz);
@@ -884,10 +887,16 @@ __global__ void __launch_bounds__(kTB) k_extend(MeshView m, GridArgs G, const fl
             float3 p = make_float3((float)(i * G.dx), (float)(j * G.dx), (float)(k * G.dx));
             int f = nearest_prim<CENTROID>(m, L, p, r_near * r_near, &err);
             if (f < 0) f = nearest_prim<CENTROID>(m, L, p, 1.0e12f, &err);
-            if (f >= 0) out = V[f];
+            if (f >= 0) {
+                out = V[f];
+                if (dV)
+                    for (int q = 0; q < 3; ++q) dout[q] = dV[f + (long long)q * m.MT];
+            }
         }
         if (pinned) out = -1.0f;
         Fs[c] = out;
+        if (dF)
+            for (int q = 0; q < 3; ++q) dF[c + q * G.n] = dout[q];
         if (fold && active && out > 0.0f) {
             int s = atomicAdd(n_active, 1);
             if (s < max_active) active[s] = (int)c;
@@ -900,8 +909,12 @@ __global__ void __launch_bounds__(kTB) k_extend(MeshView m, GridArgs G, const fl
 // _nearest_face_cov + gpu_warmstart_bare (threed.py:1619-1639): each new face centroid takes
 // the coverage of the nearest face of the previous mesh (1.0 if none), clipped to [0, 1] as
 // mc_flux_3d_coupled does with bare_init.
+// With prev_dbare (tangents [3][prev MT]) also dbare = the nearest face's tangents where its
+// coverage is strictly inside (0, 1) (the clip's derivative), 0 elsewhere, as petch_warmstart_tangent.
 __global__ void __launch_bounds__(kTB) k_warmstart(MeshView prev, const float* __restrict__ prev_bare,
-                                                   MeshView cur, float* __restrict__ bare, int* work) {
+                                                   MeshView cur, float* __restrict__ bare, int* work,
+                                                   const float* __restrict__ prev_dbare = nullptr,
+                                                   float* __restrict__ dbare = nullptr) {
     const int Lp = min(prev.hdr[HDR_L], prev.MT);
     const int F = min(cur.hdr[HDR_F], cur.MT);
     int err = 0;
@@ -910,6 +923,11 @@ __global__ void __launch_bounds__(kTB) k_warmstart(MeshView prev, const float* _
         int q = nearest_face(prev, Lp, p, 1.0e12f, &err);
         float b = q >= 0 ? prev_bare[q] : 1.0f;
         bare[f] = fminf(fmaxf(b, 0.0f), 1.0f);
+        if (dbare) {
+            const bool pass = q >= 0 && prev_bare[q] > 0.0f && prev_bare[q] < 1.0f;
+            for (int k = 0; k < 3; ++k)
+                dbare[f + (long long)k * cur.MT] = pass ? prev_dbare[q + (long long)k * prev.MT] : 0.0f;
+        }
     }
     if (err) atomicOr(work + 1, err);
 }
@@ -1446,7 +1464,8 @@ extern "C" int petch_trace_legacy(const void* mesh, int max_tris, int max_verts,
 static int extend_velocity(const void* mesh, int max_tris, int max_verts, const float* phi,
                            const uint8_t* mask, int nx, int ny, int nz, double dx, double band,
                            const float* V, float* Fs, int fold_mask, int* active, int* n_active,
-                           int max_active, int* work, void* stream, bool centroid) {
+                           int max_active, int* work, void* stream, bool centroid,
+                           const float* dV = nullptr, float* dF = nullptr) {
     PETCH_REQUIRE(mesh && phi && V && Fs && work, "petch_extend_velocity: null pointer");
     PETCH_REQUIRE(nx > 0 && ny > 0 && nz > 0 && dx > 0, "petch_extend_velocity: bad grid");
     PETCH_REQUIRE(!fold_mask || !active || n_active, "petch_extend_velocity: n_active is null");
@@ -1459,7 +1478,8 @@ static int extend_velocity(const void* mesh, int max_tris, int max_verts, const 
                                                                active, n_active, max_active, work);
     } else {
         k_extend<false><<<grid_for(G.n, kTB, 16), kTB, 0, st>>>(m, G, phi, mask, V, Fs, fold_mask,
-                                                                active, n_active, max_active, work);
+                                                                active, n_active, max_active, work,
+                                                                dV, dF);
     }
     PETCH_LAUNCH_CHECK("k_extend");
     return PETCH_OK;
@@ -1472,6 +1492,17 @@ extern "C" int petch_extend_velocity(const void* mesh, int max_tris, int max_ver
                                      void* stream) {
     return extend_velocity(mesh, max_tris, max_verts, phi, mask, nx, ny, nz, dx, band, V, Fs,
                            fold_mask, active, n_active, max_active, work, stream, false);
+}
+
+extern "C" int petch_extend_velocity_dual(const void* mesh, int max_tris, int max_verts,
+                                          const float* phi, const uint8_t* mask, int nx, int ny,
+                                          int nz, double dx, double band, const float* V,
+                                          const float* dV, float* Fs, float* dF, int fold_mask,
+                                          int* active, int* n_active, int max_active, int* work,
+                                          void* stream) {
+    PETCH_REQUIRE(dV && dF, "petch_extend_velocity_dual: null pointer");
+    return extend_velocity(mesh, max_tris, max_verts, phi, mask, nx, ny, nz, dx, band, V, Fs,
+                           fold_mask, active, n_active, max_active, work, stream, false, dV, dF);
 }
 
 extern "C" int petch_extend_velocity_centroid(const void* mesh, int max_tris, int max_verts,
@@ -1492,6 +1523,21 @@ extern "C" int petch_warmstart(const void* prev_mesh, int prev_max_tris, int pre
     MeshView pm = mesh_view(const_cast<void*>(prev_mesh), prev_max_tris, prev_max_verts);
     MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
     k_warmstart<<<grid_for(max_tris, kTB), kTB, 0, st>>>(pm, prev_bare, m, bare, work);
+    PETCH_LAUNCH_CHECK("k_warmstart");
+    return PETCH_OK;
+}
+
+extern "C" int petch_warmstart_dual(const void* prev_mesh, int prev_max_tris, int prev_max_verts,
+                                    const float* prev_bare, const float* prev_dbare,
+                                    const void* mesh, int max_tris, int max_verts, float* bare,
+                                    float* dbare, int* work, void* stream) {
+    PETCH_REQUIRE(prev_mesh && prev_bare && prev_dbare && mesh && bare && dbare && work,
+                  "petch_warmstart_dual: null pointer");
+    cudaStream_t st = as_stream(stream);
+    MeshView pm = mesh_view(const_cast<void*>(prev_mesh), prev_max_tris, prev_max_verts);
+    MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
+    k_warmstart<<<grid_for(max_tris, kTB), kTB, 0, st>>>(pm, prev_bare, m, bare, work, prev_dbare,
+                                                        dbare);
     PETCH_LAUNCH_CHECK("k_warmstart");
     return PETCH_OK;
 }

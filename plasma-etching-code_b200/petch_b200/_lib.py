@@ -140,6 +140,8 @@ SIGNATURES = {
     "petch_trace_batch_tangent": [I, P, P, I, I, I, F, P, U, U, P, P],
     "petch_batch_advect_tangent": [P, P, I, P],
     "petch_batch_reinit_tangent": [P, P, I, D, P],
+    "petch_extend_velocity_dual": [P, I, I, P, P, I, I, I, D, D, P, P, P, P, I, P, P, I, P, P],
+    "petch_warmstart_dual": [P, I, I, P, P, P, I, I, P, P, P, P],
 }
 
 # The library's tracer configuration at load (bvh_width, steps_per_round, keep_lanes): what

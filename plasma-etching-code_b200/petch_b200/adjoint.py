@@ -103,11 +103,9 @@ class TangentEngine(EtchEngine):
         seeded = False
         if warm and self.prev is not None:
             pm, pb = self.prev
-            _lib.call("petch_warmstart", pm.id, pm.MT, pm.MV, pb.data_ptr(), m.id, m.MT, m.MV,
-                      self.bare.data_ptr(), work.data_ptr(), s)
-            _lib.call("petch_warmstart_tangent", pm.id, pm.MT, pm.MV, pb.data_ptr(),
-                      self.prev_dbare.data_ptr(), m.id, m.MT, m.MV, self.dbare.data_ptr(),
-                      work.data_ptr(), s)
+            _lib.call("petch_warmstart_dual", pm.id, pm.MT, pm.MV, pb.data_ptr(),
+                      self.prev_dbare.data_ptr(), m.id, m.MT, m.MV, self.bare.data_ptr(),
+                      self.dbare.data_ptr(), work.data_ptr(), s)
             seeded = True
         _lib.call("petch_trace_ions_tangent", m.id, m.MT, m.MV, ctypes.byref(self.dom),
                   ctypes.byref(self.ionp), int(seed * 9 + 1) & 0xffffffff, int(n_ion),
@@ -159,12 +157,10 @@ class TangentEngine(EtchEngine):
                   self.y[2].data_ptr(), self.dy[2].data_ptr(), self.V.data_ptr(),
                   self.dV.data_ptr(), self.small[6:8].data_ptr(), s)
         nx, ny, nz = self.shape
-        _lib.call("petch_extend_velocity", m.id, m.MT, m.MV, self.phi.data_ptr(),
+        _lib.call("petch_extend_velocity_dual", m.id, m.MT, m.MV, self.phi.data_ptr(),
                   self.mask.data_ptr(), nx, ny, nz, self.dx, float(band), self.V.data_ptr(),
-                  self.F.data_ptr(), 1, self.active.data_ptr(), self.small[8:9].data_ptr(),
-                  self.ncell, self.small[0:6].data_ptr(), s)
-        _lib.call("petch_extend_tangent", m.id, m.MT, m.MV, self.phi.data_ptr(), nx, ny, nz,
-                  self.dx, float(band), self.dV.data_ptr(), self.dF.data_ptr(),
+                  self.dV.data_ptr(), self.F.data_ptr(), self.dF.data_ptr(), 1,
+                  self.active.data_ptr(), self.small[8:9].data_ptr(), self.ncell,
                   self.small[0:6].data_ptr(), s)
 
     def advect_tangent(self, dt_sub, nsub):

@@ -5,12 +5,14 @@ instance follows run_etch_3d_tangent (the forward-mode recipe gradient of the co
 SF6/O2 loop, petch/threed.py:1643-1795 with faithful ions, warm-started coverage, nearest-face
 extension and the FSM reinit); the instances advance together as BatchEngine's do:
 
-    per instance: marching cubes + BVH, warm start of the coverage and of its tangents
+    per instance: marching cubes + BVH, warm start of the coverage and its tangents (one
+        nearest-face query per face)
     ions of ALL instances with energy tangents: one persistent launch (petch_trace_batch_tangent)
     per instance: ion normalisation + smoothing, the yields' tangents
     coverage fixed point: F and O neutrals of all instances with weight tangents, one launch each;
         per instance normalisation + smoothing (+ tangents), Belen coverage update with duals
-    per instance: surface rate with duals, velocity extension and its tangent
+    per instance: surface rate with duals, velocity extension and its tangent (one nearest-face
+        query per band cell)
     all instances: CFL substeps on the device and the dual advection (petch_batch_advect_tangent),
         the dual Eikonal reinit (petch_batch_reinit_tangent), the step counter
 No host synchronisation inside a step, so each step is captured in a CUDA graph and replayed.
@@ -247,11 +249,10 @@ class BatchTangentEngine:
         if not cold:
             for x in self.inst:
                 pm, cm = x.meshes[prev], x.meshes[cur]
-                _lib.call("petch_warmstart", pm.id, pm.MT, pm.MV, x.bares[prev].data_ptr(), cm.id,
-                          cm.MT, cm.MV, x.bares[cur].data_ptr(), x.fe.small.data_ptr(), s)
-                _lib.call("petch_warmstart_tangent", pm.id, pm.MT, pm.MV,
-                          x.bares[prev].data_ptr(), x.dbares[prev].data_ptr(), cm.id, cm.MT,
-                          cm.MV, x.dbares[cur].data_ptr(), x.fe.small.data_ptr(), s)
+                _lib.call("petch_warmstart_dual", pm.id, pm.MT, pm.MV, x.bares[prev].data_ptr(),
+                          x.dbares[prev].data_ptr(), cm.id, cm.MT, cm.MV,
+                          x.bares[cur].data_ptr(), x.dbares[cur].data_ptr(),
+                          x.fe.small.data_ptr(), s)
         items, tans = self._items(True, cur)
         _lib.call("petch_trace_batch_tangent", 0, items, tans, B, MT, MV, 0.0,
                   self.step_dev.data_ptr(), 9, 1, self.work.data_ptr(), s)
@@ -304,13 +305,10 @@ class BatchTangentEngine:
                       x.dy[2].data_ptr(), fe.V.data_ptr(), x.dV.data_ptr(),
                       fe.small[6:8].data_ptr(), s)
             nx, ny, nz = x.shape
-            _lib.call("petch_extend_velocity", m.id, m.MT, m.MV, x.phi.data_ptr(),
+            _lib.call("petch_extend_velocity_dual", m.id, m.MT, m.MV, x.phi.data_ptr(),
                       x.mask.data_ptr(), nx, ny, nz, x.dx, float(self.band), fe.V.data_ptr(),
-                      x.F.data_ptr(), 1, x.active.data_ptr(), fe.small[8:9].data_ptr(), x.ncell,
-                      fe.small[0:6].data_ptr(), s)
-            _lib.call("petch_extend_tangent", m.id, m.MT, m.MV, x.phi.data_ptr(), nx, ny, nz,
-                      x.dx, float(self.band), x.dV.data_ptr(), x.dF.data_ptr(),
-                      fe.small[0:6].data_ptr(), s)
+                      x.dV.data_ptr(), x.F.data_ptr(), x.dF.data_ptr(), 1, x.active.data_ptr(),
+                      fe.small[8:9].data_ptr(), x.ncell, fe.small[0:6].data_ptr(), s)
         grids, tg = self._grids(cur)
         _lib.call("petch_batch_advect_tangent", grids, tg, B, s)
         _lib.call("petch_batch_reinit_tangent", grids, tg, B, float(self.band + 2.0 * self.dx), s)

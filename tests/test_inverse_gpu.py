@@ -108,3 +108,62 @@ def test_bad_tables_fail_loudly():
                   eng.work.data_ptr(), torch.cuda.current_stream().cuda_stream)
     with pytest.raises(NotImplementedError):
         inverse.BatchTangentEngine(specs, petch.Flags(chemistry="belen", coverage_sticking=True))
+
+
+def test_fused_extension_and_warm_start_equal_the_separate_calls():
+    """petch_extend_velocity_dual / petch_warmstart_dual give the same numbers as the primal call
+    followed by its tangent call."""
+    from gpu_helpers import cuda_mesh, small_feature, stream
+    phi, geo = small_feature(True, nx=12, ny=12, nz=16, dx=0.25)
+    m1 = cuda_mesh(phi, 0.25, geo)
+    phi2 = phi.copy()
+    phi2[:, :, 6:] -= 0.05
+    m2 = cuda_mesh(phi2, 0.25, geo, MT=m1.MT)
+    MT = m1.MT
+    rng = np.random.default_rng(0)
+    g = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda()  # noqa: E731
+    V = g(rng.uniform(0, 2, MT))
+    dV = g(rng.normal(size=(3, MT)))
+    phid = g(phi2)
+    nx, ny, nz = phi.shape
+    n = phi.size
+    mask = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    pb = g(rng.uniform(-0.2, 1.2, MT))                   # coverages outside [0, 1] included
+    pdb = g(rng.normal(size=(3, MT)))
+    outs = []
+    for dual in (False, True):
+        Fs = torch.full((n,), 7.0, device="cuda")
+        dF = torch.full((3, n), 7.0, device="cuda")
+        act = torch.zeros(n, dtype=torch.int32, device="cuda")
+        na = torch.zeros(1, dtype=torch.int32, device="cuda")
+        work = torch.zeros(6, dtype=torch.int32, device="cuda")
+        if dual:
+            _lib.call("petch_extend_velocity_dual", m2.id, MT, m2.MV, phid.data_ptr(),
+                      mask.data_ptr(), nx, ny, nz, 0.25, 1.0, V.data_ptr(), dV.data_ptr(),
+                      Fs.data_ptr(), dF.data_ptr(), 1, act.data_ptr(), na.data_ptr(), n,
+                      work.data_ptr(), stream())
+        else:
+            _lib.call("petch_extend_velocity", m2.id, MT, m2.MV, phid.data_ptr(), mask.data_ptr(),
+                      nx, ny, nz, 0.25, 1.0, V.data_ptr(), Fs.data_ptr(), 1, act.data_ptr(),
+                      na.data_ptr(), n, work.data_ptr(), stream())
+            _lib.call("petch_extend_tangent", m2.id, MT, m2.MV, phid.data_ptr(), nx, ny, nz, 0.25,
+                      1.0, dV.data_ptr(), dF.data_ptr(), work.data_ptr(), stream())
+        bare = torch.full((MT,), 7.0, device="cuda")
+        dbare = torch.full((3, MT), 7.0, device="cuda")
+        if dual:
+            _lib.call("petch_warmstart_dual", m1.id, MT, m1.MV, pb.data_ptr(), pdb.data_ptr(),
+                      m2.id, MT, m2.MV, bare.data_ptr(), dbare.data_ptr(), work.data_ptr(),
+                      stream())
+        else:
+            _lib.call("petch_warmstart", m1.id, MT, m1.MV, pb.data_ptr(), m2.id, MT, m2.MV,
+                      bare.data_ptr(), work.data_ptr(), stream())
+            _lib.call("petch_warmstart_tangent", m1.id, MT, m1.MV, pb.data_ptr(), pdb.data_ptr(),
+                      m2.id, MT, m2.MV, dbare.data_ptr(), work.data_ptr(), stream())
+        F2 = m2.F
+        outs.append((Fs.clone(), dF.clone(), bare[:F2].clone(), dbare[:, :F2].clone(),
+                     int(na.item())))
+        assert int(work[1].item()) == 0
+    a, b = outs
+    for x, y in zip(a[:4], b[:4]):
+        assert torch.equal(x, y)
+    assert a[4] == b[4] and a[4] > 0
