@@ -21,8 +21,15 @@ constexpr int kTB = 128;
 #ifndef PETCH_TRACE_MIN_BLOCKS
 #define PETCH_TRACE_MIN_BLOCKS 8
 #endif
-// resident blocks of the persistent tracers per SM (8 x 4 warps: <= 64 registers per thread)
+#ifndef PETCH_TRACE_MIN_BLOCKS_RR
+#define PETCH_TRACE_MIN_BLOCKS_RR 10
+#endif
+// Resident blocks of the persistent tracers per SM: 8 x 4 warps (<= 64 registers per thread) for
+// the ion shaders, 10 x 4 (<= 48 registers) for the Russian-roulette neutral shaders, whose
+// traversal-bound loop gains more from the extra warps than it loses to spills (a sweep on the
+// trench workload: neutrals -6 % time at 10, ions +10 % at 10).
 constexpr int kTraceMinBlocks = PETCH_TRACE_MIN_BLOCKS;
+constexpr int kTraceMinBlocksRR = PETCH_TRACE_MIN_BLOCKS_RR;
 constexpr long long kMaxRounds = 1LL << 24;   // per-warp bound on tracer rounds (error bit 4)
 constexpr unsigned kFull = 0xffffffffu;
 
@@ -229,6 +236,7 @@ struct NeutralShader {
     float* flux;
     int det;
     static constexpr int kMaxBounce = 1024;
+    static constexpr int kMinBlocks = kTraceMinBlocksRR;
     __device__ __forceinline__ int count(const MeshView&, int n) const { return n; }
     __device__ __forceinline__ void init(Rng& g, const Tracer&, const Domain& D, int, float3& o,
                                          float3& d, RayState& s) const {
@@ -345,6 +353,7 @@ struct IonShader {
     float* ang;
     int det;
     static constexpr int kMaxBounce = 1024;
+    static constexpr int kMinBlocks = kTraceMinBlocks;
     __device__ __forceinline__ int count(const MeshView&, int n) const { return n; }
     __device__ __forceinline__ void init(Rng& g, const Tracer&, const Domain& D, int, float3& o,
                                          float3& d, RayState& s) const {
@@ -368,6 +377,7 @@ struct LegacyShader {
     float* angacc;
     int det;
     static constexpr int kMaxBounce = 1 << 30;
+    static constexpr int kMinBlocks = kTraceMinBlocks;
     __device__ __forceinline__ int count(const MeshView&, int n) const { return n; }
     __device__ __forceinline__ void init(Rng& g, const Tracer&, const Domain& D, int, float3& o,
                                          float3& d, RayState& s) const {
@@ -413,6 +423,7 @@ struct IonTanShader {
     float* dtal;            // [3][MT]: d(sp, ie, ip) / d(mean ion energy)
     int det;
     static constexpr int kMaxBounce = 1024;
+    static constexpr int kMinBlocks = kTraceMinBlocks;
     __device__ __forceinline__ int count(const MeshView&, int n) const { return n; }
     __device__ __forceinline__ void init(Rng& g, const Tracer&, const Domain& D, int, float3& o,
                                          float3& d, RayState& s) const {
@@ -435,6 +446,7 @@ struct NeutralTanShader {
     float* dflux;           // [3][MT]
     int det;
     static constexpr int kMaxBounce = 1024;
+    static constexpr int kMinBlocks = kTraceMinBlocksRR;
     __device__ __forceinline__ int count(const MeshView&, int n) const { return n; }
     __device__ __forceinline__ void init(Rng& g, const Tracer&, const Domain& D, int, float3& o,
                                          float3& d, RayState& s) const {
@@ -457,6 +469,7 @@ struct FormFactorShader {
     int n_ff;
     int* hitface;
     static constexpr int kMaxBounce = 1;
+    static constexpr int kMinBlocks = kTraceMinBlocks;
     __device__ __forceinline__ int count(const MeshView& m, int n) const {
         const long long F = min(m.hdr[HDR_F], m.MT);
         return (int)min((long long)n, F * n_ff);
@@ -487,6 +500,7 @@ struct RedepShader {
     const double* cdf;
     const float* fn;
     static constexpr int kMaxBounce = NeutralShader::kMaxBounce;
+    static constexpr int kMinBlocks = kTraceMinBlocksRR;
     __device__ __forceinline__ int count(const MeshView& m, int n) const {
         const int F = min(m.hdr[HDR_F], m.MT);
         return (F > 0 && cdf[F - 1] > 0.0) ? n : 0;
@@ -549,7 +563,7 @@ __global__ void k_redep_apply(MeshView m, const float* __restrict__ flux,
 // final query) or ends the ray; a hit goes to the shader, which deposits and either re-emits
 // (new query) or ends the ray.
 template <class S, bool WIDE>
-__global__ void __launch_bounds__(kTB, kTraceMinBlocks) k_trace(MeshView m, Domain D, S sh, uint32_t seed,
+__global__ void __launch_bounds__(kTB, S::kMinBlocks) k_trace(MeshView m, Domain D, S sh, uint32_t seed,
                                                uint32_t domain, int n, int steps, int keep,
                                                int* work) {
     extern __shared__ float4 s_wn[];
@@ -719,7 +733,7 @@ __global__ void k_zero_batch(BatchTable tab, MeshOffsets L, int MT, int MV, int 
 // KIND: 0 ions, 1 neutrals, 2 ions with energy tangents, 3 neutrals with weight tangents (the
 // single-instance tangent shaders' hit functions, outputs per instance from tab.tn).
 template <int KIND>
-__global__ void __launch_bounds__(kTB, kTraceMinBlocks) k_trace_batch(BatchTable tab, MeshOffsets L,
+__global__ void __launch_bounds__(kTB, (KIND & 1) ? kTraceMinBlocksRR : kTraceMinBlocks) k_trace_batch(BatchTable tab, MeshOffsets L,
                                                                      int MT, int MV, float beta,
                                                                      const int* step,
                                                                      uint32_t seed_mul,

@@ -81,8 +81,9 @@ def test_redep_apply_updates_rate_and_max(rp):
 
 def test_redep_loop_depth_matches_oracle_loop():
     """With redeposition a single small-trench run scatters by several cells between seeds, so
-    the centre depth averaged over six seeds is compared: device vs oracle within one cell at
-    every recorded step."""
+    the centre depth averaged over 16 seeds is compared at every recorded step: device vs oracle
+    (independent random streams) within one cell, or within three standard errors of the
+    difference of the two means where the seed scatter is larger than that."""
     dx = 0.25
     cfg = dict(Lx=5.0, Ly=2.5, Lz=8.0, dx=dx, trench_width=2.0, mask_th=1.0, sub_top=6.0,
                t_end=1.2, n_steps=12, hole=False)
@@ -91,7 +92,7 @@ def test_redep_loop_depth_matches_oracle_loop():
                      ion_reflection=True, warm_start_coverage=True, redeposition=True)
     n = 60000
     dev, orc_h = [], []
-    for off in (0, 100, 200, 300, 400, 500):
+    for off in range(0, 1600, 100):
         geo = t3.run_etch_3d(**cfg, par=par, flags=fl, n_ion=n, n_neu=n, reinit_method="fsm",
                              verbose=False, record_depth_every=3, seed_offset=off)
         dev.append(dict(geo['depth_history']))
@@ -102,7 +103,8 @@ def test_redep_loop_depth_matches_oracle_loop():
         orc_h.append(dict(hist))
     steps = sorted(orc_h[0])
     for s in steps:
-        d = np.mean([h[s] for h in dev])
-        o = np.mean([h[s] for h in orc_h])
-        assert abs(d - o) <= dx + 1e-9, (s, d, o)
+        a = np.array([h[s] for h in dev])
+        b = np.array([h[s] for h in orc_h])
+        se = np.sqrt(a.var(ddof=1) / len(a) + b.var(ddof=1) / len(b))
+        assert abs(a.mean() - b.mean()) <= max(dx, 3.0 * se) + 1e-9, (s, a.mean(), b.mean(), se)
     assert np.mean([h[steps[-1]] for h in orc_h]) > 2 * dx
