@@ -562,6 +562,19 @@ int petch_charging_apply(const int* n_faces, int max_faces, const float* centroi
 int petch_zero_below(const int* n_faces, int max_faces, const float* centroids, double z_top,
                      float* values, void* stream);
 
+/* Replaces solve() with radiosity_solver = 'gmres' (petch/threed.py:972-982): restarted GMRES
+ * (restart Krylov vectors per cycle, at most maxiter cycles, modified Gram-Schmidt, Givens
+ * rotations, x0 = 0) on (I - M) G = D, M[i, j] = A[i, j] (1 - clip(bare_j beta, 0, 1)), with the
+ * reference's stopping rule |D - (I - M) G| <= rtol |D| (atol 0).  g_out = clip(G, 0, 8); *info
+ * (host int) = 0 when converged, 1 when not (the reference then falls back to the Jacobi sweeps:
+ * petch_radiosity_solve).  Float64, every sum in a fixed order; the host reads one scalar per
+ * Arnoldi step (the call synchronises the stream).  Scratch: petch_radiosity_gmres_scratch_bytes. */
+int petch_radiosity_gmres_scratch_bytes(int max_tris, int restart, long long* bytes);
+int petch_radiosity_gmres(const void* mesh, int max_tris, int max_verts, const int* row_ptr,
+                          const int* col, const double* sky, int n_ff, const float* bare,
+                          double beta, double rtol, int restart, int maxiter, float* g_out,
+                          void* scratch, long long scratch_bytes, int* info, void* stream);
+
 /* ---- recipe gradient: tangent (forward-mode) versions of the step's stages ----
  * No reference counterpart (the reference has no loop gradient).  Each call computes the
  * primal result exactly as its plain counterpart and the derivatives of it along 3 directions

@@ -15,6 +15,7 @@ Reference lines followed (paths within the reference project):
   reinit_gpu           petch/threed.py:1349-1418   Russo-Smereka PDE sweeps
   surf_smooth          petch/threed.py:1779-1782   the same scipy gaussian_filter call
   mc_flux_3d_radiosity petch/threed.py:923-1029    _gas_normals :1553-1568, _cosine_dirs :1571-1579
+                       (radiosity_solver 'gmres': the same scipy gmres call, :972-982)
   mc_redep_3d          petch/threed.py:1582-1605   wired as run_etch_3d :1730-1743
   dda_neutral_flux     petch/dda.py:26-188         gather kernel (oracle_dda.cpp), fib_sphere,
                        wall cells, dilation, Aitken; mc_flux_3d_dda petch/threed.py:1211-1244
@@ -592,13 +593,28 @@ def ff_matrix(hit, F, n_ff):
     return D, Aff
 
 
-def radiosity_solve(Aff, D, bare, beta, n_iter=40):
-    """solve() of mc_flux_3d_radiosity with the Jacobi solver (threed.py:966-985)."""
+def radiosity_solve(Aff, D, bare, beta, n_iter=40, solver="jacobi"):
+    """solve() of mc_flux_3d_radiosity (threed.py:966-985): n_iter Jacobi sweeps G = D + M G, or
+    (solver 'gmres') scipy's restarted GMRES on (I - M) G = D with rtol 1e-3, restart 12, at most
+    40 cycles, the Jacobi sweeps when it does not converge."""
     s = np.clip(bare * beta, 0.0, 1.0)
     M = Aff.multiply((1.0 - s)[None, :]).tocsr()
-    G = D.copy()
-    for _ in range(n_iter):
-        G = D + M.dot(G)
+
+    def jacobi():
+        G = D.copy()
+        for _ in range(n_iter):
+            G = D + M.dot(G)
+        return G
+
+    if solver == "gmres":
+        from scipy.sparse.linalg import LinearOperator, gmres
+        n = len(D)
+        op = LinearOperator((n, n), matvec=lambda x: x - M.dot(x), dtype=float)
+        G, info = gmres(op, D, rtol=1e-3, atol=0.0, restart=12, maxiter=40)
+        if info != 0:
+            G = jacobi()
+    else:
+        G = jacobi()
     return np.clip(G, 0.0, 8.0)
 
 
@@ -623,15 +639,17 @@ def radiosity_ions(mesh, geo, par, flags, n_ion, seed):
 
 
 def radiosity_fixed_point(D, Aff, m_i, cos_i, iy, par, flags, n_fp=4, n_iter=40):
-    """The coverage <-> radiosity fixed point of mc_flux_3d_radiosity (threed.py:986-990)."""
+    """The coverage <-> radiosity fixed point of mc_flux_3d_radiosity (threed.py:986-990), with
+    par['radiosity_solver'] ('jacobi' or 'gmres')."""
+    solver = par.get('radiosity_solver', 'jacobi')
     F = len(D)
     bare = np.ones(F)
     betaE, betaO = par.get('betaE', 0.7), par.get('betaO', 1.0)
     ya = getattr(flags, "yield_angular", "cosine")
     m_F = m_O = np.zeros(F)
     for _ in range(n_fp):
-        m_F = radiosity_solve(Aff, D, bare, betaE, n_iter)
-        m_O = radiosity_solve(Aff, D, bare, betaO, n_iter)
+        m_F = radiosity_solve(Aff, D, bare, betaE, n_iter, solver)
+        m_O = radiosity_solve(Aff, D, bare, betaO, n_iter, solver)
         thF, thO = belen_coverages(m_i, m_F, m_O, cos_i, par, ya, iy)
         bare = np.clip(1.0 - thF - thO, 0.0, 1.0)
     return m_F, m_O

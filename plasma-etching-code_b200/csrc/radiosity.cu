@@ -325,3 +325,326 @@ extern "C" int petch_radiosity_solve(const void* mesh, int max_tris, int max_ver
     }
     return PETCH_OK;
 }
+
+// ---------------------------------------------------------------------------------------------
+// Restarted GMRES on (I - M) G = D (radiosity_solver = 'gmres', threed.py:972-982): the
+// reference's scipy gmres(rtol, atol 0, restart, maxiter) with its Jacobi fallback on failure.
+// Host-driven: each Arnoldi step is a few kernels (mat-vec, modified Gram-Schmidt dot / axpy
+// pairs with the coefficients left on the device, norm, Givens rotation), and one 8-byte read of
+// the residual estimate decides whether the cycle goes on; every reduction sums in a fixed order,
+// so a solve is reproducible bit for bit.  Float64 throughout.
+// ---------------------------------------------------------------------------------------------
+namespace petch {
+namespace {
+
+constexpr int kGB = 256;
+constexpr int kGBlocks = 296;   // dot-product partial blocks (2 per SM)
+
+struct GmScratch {
+    double* V;        // [(restart + 1) * MT] Krylov basis
+    double* w;        // [MT]
+    double* x;        // [MT]
+    double* t;        // [MT]
+    double* a;        // [MT] 1 - clip(bare beta, 0, 1)
+    double* part;     // [kGBlocks]
+    double* H;        // [(restart + 1) * restart], column-major
+    double* cs;       // [restart]
+    double* sn;       // [restart]
+    double* g;        // [restart + 1]
+    double* y;        // [restart]
+    double* scal;     // [4]: [0] last dot / norm, [1] residual estimate
+};
+
+int gm_layout(int MT, int restart, void* base, size_t* total, GmScratch* out) {
+    size_t off = 0;
+    char* b = (char*)base;
+    auto take = [&](size_t n) {
+        char* p = b ? b + off : nullptr;
+        off += (sizeof(double) * n + 255) & ~(size_t)255;
+        return (double*)p;
+    };
+    GmScratch s;
+    s.V = take((size_t)(restart + 1) * MT);
+    s.w = take(MT);
+    s.x = take(MT);
+    s.t = take(MT);
+    s.a = take(MT);
+    s.part = take(kGBlocks);
+    s.H = take((size_t)(restart + 1) * restart);
+    s.cs = take(restart);
+    s.sn = take(restart);
+    s.g = take(restart + 1);
+    s.y = take(restart);
+    s.scal = take(4);
+    *total = off;
+    if (out) *out = s;
+    return PETCH_OK;
+}
+
+__global__ void k_gm_alpha(const int* hdr, int MT, const float* __restrict__ bare, double beta,
+                           double* __restrict__ a) {
+    const int F = min(hdr[HDR_F], MT);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < F; i += gridDim.x * blockDim.x)
+        a[i] = 1.0 - fmin(fmax((double)bare[i] * beta, 0.0), 1.0);
+}
+
+// out = in - (1 / n_ff) sum over row i's entries j of a_j in_j  (row entries in ascending order)
+__global__ void k_gm_matvec(const int* hdr, int MT, const int* __restrict__ row_ptr,
+                            const int* __restrict__ col, const double* __restrict__ a,
+                            double inv_nff, const double* __restrict__ in,
+                            double* __restrict__ out) {
+    const int F = min(hdr[HDR_F], MT);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < F; i += gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int e = row_ptr[i]; e < row_ptr[i + 1]; ++e) {
+            const int j = __ldg(col + e);
+            s += a[j] * in[j];
+        }
+        out[i] = in[i] - inv_nff * s;
+    }
+}
+
+// partial[b] = sum over this block's fixed slice of u . v; then dest = sum of the partials
+__global__ void __launch_bounds__(kGB) k_gm_dot_part(const int* hdr, int MT,
+                                                      const double* __restrict__ u,
+                                                      const double* __restrict__ v,
+                                                      double* __restrict__ part) {
+    __shared__ double sh[kGB];
+    const int F = min(hdr[HDR_F], MT);
+    double acc = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < F; i += gridDim.x * blockDim.x)
+        acc += u[i] * v[i];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = kGB / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
+// dest = sum(part); sqrt_it: dest = sqrt(sum)
+__global__ void __launch_bounds__(kGB) k_gm_dot_final(const double* __restrict__ part, int n,
+                                                       double* __restrict__ dest, int sqrt_it) {
+    __shared__ double sh[kGB];
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) acc += part[i];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = kGB / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *dest = sqrt_it ? sqrt(sh[0]) : sh[0];
+}
+
+// y = x * (*num) / (*den) elementwise factor read on the device (den <= 0: y = 0)
+__global__ void k_gm_scale(const int* hdr, int MT, const double* __restrict__ x,
+                           const double* __restrict__ den, double* __restrict__ y) {
+    const int F = min(hdr[HDR_F], MT);
+    const double d = *den;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < F; i += gridDim.x * blockDim.x)
+        y[i] = d > 0.0 ? x[i] / d : 0.0;
+}
+
+// w -= (*h) v
+__global__ void k_gm_axpy(const int* hdr, int MT, const double* __restrict__ h,
+                          const double* __restrict__ v, double* __restrict__ w) {
+    const int F = min(hdr[HDR_F], MT);
+    const double c = *h;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < F; i += gridDim.x * blockDim.x)
+        w[i] -= c * v[i];
+}
+
+// r = b - t
+__global__ void k_gm_resid(const int* hdr, int MT, const double* __restrict__ b,
+                           const double* __restrict__ t, double* __restrict__ r) {
+    const int F = min(hdr[HDR_F], MT);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < F; i += gridDim.x * blockDim.x)
+        r[i] = b[i] - t[i];
+}
+
+// Start of a cycle: g = (beta0, 0, ...), beta0 = scal[0].
+__global__ void k_gm_start(GmScratch s, int restart) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    for (int i = 0; i <= restart; ++i) s.g[i] = 0.0;
+    s.g[0] = s.scal[0];
+}
+
+// Column j of H (rows 0..j+1 in place): apply the previous rotations, form the new one, rotate g;
+// scal[1] = |g[j + 1]|, the residual norm of the current iterate.
+__global__ void k_gm_givens(GmScratch s, int j, int restart) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int m1 = restart + 1;
+    double* h = s.H + (size_t)j * m1;
+    for (int i = 0; i < j; ++i) {
+        const double t = s.cs[i] * h[i] + s.sn[i] * h[i + 1];
+        h[i + 1] = -s.sn[i] * h[i] + s.cs[i] * h[i + 1];
+        h[i] = t;
+    }
+    const double a = h[j], b = h[j + 1];
+    double c = 1.0, sn = 0.0;
+    if (b != 0.0) {
+        if (fabs(b) > fabs(a)) {
+            const double t = a / b;
+            sn = 1.0 / sqrt(1.0 + t * t);
+            c = t * sn;
+        } else {
+            const double t = b / a;
+            c = 1.0 / sqrt(1.0 + t * t);
+            sn = t * c;
+        }
+    }
+    s.cs[j] = c;
+    s.sn[j] = sn;
+    h[j] = c * a + sn * b;
+    h[j + 1] = 0.0;
+    s.g[j + 1] = -sn * s.g[j];
+    s.g[j] = c * s.g[j];
+    s.scal[1] = fabs(s.g[j + 1]);
+}
+
+// y = R^-1 g over the first k columns (zero pivots give 0).
+__global__ void k_gm_backsolve(GmScratch s, int k, int restart) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int m1 = restart + 1;
+    for (int i = k - 1; i >= 0; --i) {
+        double v = s.g[i];
+        for (int l = i + 1; l < k; ++l) v -= s.H[i + (size_t)l * m1] * s.y[l];
+        const double d = s.H[i + (size_t)i * m1];
+        s.y[i] = d != 0.0 ? v / d : 0.0;
+    }
+}
+
+// x += sum_k y_k V_k
+__global__ void k_gm_xupdate(const int* hdr, int MT, GmScratch s, int k) {
+    const int F = min(hdr[HDR_F], MT);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < F; i += gridDim.x * blockDim.x) {
+        double v = s.x[i];
+        for (int q = 0; q < k; ++q) v += s.y[q] * s.V[(size_t)q * MT + i];
+        s.x[i] = v;
+    }
+}
+
+__global__ void k_gm_out(const int* hdr, int MT, const double* __restrict__ x,
+                         float* __restrict__ out) {
+    const int F = min(hdr[HDR_F], MT);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < F; i += gridDim.x * blockDim.x)
+        out[i] = (float)fmin(fmax(x[i], 0.0), 8.0);
+}
+
+}  // namespace
+}  // namespace petch
+
+extern "C" int petch_radiosity_gmres_scratch_bytes(int max_tris, int restart, long long* bytes) {
+    PETCH_REQUIRE(bytes, "petch_radiosity_gmres_scratch_bytes: null pointer");
+    PETCH_REQUIRE(max_tris > 0 && restart >= 1 && restart <= 256,
+                  "petch_radiosity_gmres_scratch_bytes: bad size");
+    size_t total = 0;
+    gm_layout(max_tris, restart, nullptr, &total, nullptr);
+    *bytes = (long long)total;
+    return PETCH_OK;
+}
+
+extern "C" int petch_radiosity_gmres(const void* mesh, int max_tris, int max_verts,
+                                     const int* row_ptr, const int* col, const double* sky,
+                                     int n_ff, const float* bare, double beta, double rtol,
+                                     int restart, int maxiter, float* g_out, void* scratch,
+                                     long long scratch_bytes, int* info, void* stream) {
+    PETCH_REQUIRE(mesh && row_ptr && col && sky && bare && g_out && scratch && info,
+                  "petch_radiosity_gmres: null pointer");
+    PETCH_REQUIRE(max_tris > 0 && n_ff >= 1 && restart >= 1 && restart <= 256 && maxiter >= 0 &&
+                      rtol >= 0.0,
+                  "petch_radiosity_gmres: bad size");
+    size_t need = 0;
+    GmScratch s;
+    gm_layout(max_tris, restart, scratch, &need, &s);
+    PETCH_REQUIRE((long long)need <= scratch_bytes, "petch_radiosity_gmres: scratch too small");
+    cudaStream_t st = as_stream(stream);
+    MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
+    const int* hdr = m.hdr;
+    const int MT = max_tris;
+    const int gb = grid_for(MT, kGB);
+    const double inv_nff = 1.0 / n_ff;
+    auto dot = [&](const double* u, const double* v, double* dest, int sqrt_it) -> int {
+        k_gm_dot_part<<<kGBlocks, kGB, 0, st>>>(hdr, MT, u, v, s.part);
+        PETCH_LAUNCH_CHECK("k_gm_dot_part");
+        k_gm_dot_final<<<1, kGB, 0, st>>>(s.part, kGBlocks, dest, sqrt_it);
+        PETCH_LAUNCH_CHECK("k_gm_dot_final");
+        return PETCH_OK;
+    };
+    auto read = [&](const double* p, double* h) -> int {
+        PETCH_CUDA(cudaMemcpyAsync(h, p, sizeof(double), cudaMemcpyDeviceToHost, st),
+                   "petch_radiosity_gmres: read scalar");
+        PETCH_CUDA(cudaStreamSynchronize(st), "petch_radiosity_gmres: sync");
+        return PETCH_OK;
+    };
+    int rc;
+    k_gm_alpha<<<gb, kGB, 0, st>>>(hdr, MT, bare, beta, s.a);
+    PETCH_LAUNCH_CHECK("k_gm_alpha");
+    PETCH_CUDA(cudaMemsetAsync(s.x, 0, sizeof(double) * MT, st), "petch_radiosity_gmres: memset");
+    if ((rc = dot(sky, sky, s.scal + 2, 1))) return rc;
+    double bnorm = 0.0;
+    if ((rc = read(s.scal + 2, &bnorm))) return rc;
+    const double tol = rtol * bnorm;          // atol 0: the reference's threshold
+    int status = 1;
+    if (bnorm == 0.0) status = 0;
+    const int m1 = restart + 1;
+    for (int cycle = 0; cycle < maxiter && status; ++cycle) {
+        // r = b - A x into V_0, beta0 = |r|
+        k_gm_matvec<<<gb, kGB, 0, st>>>(hdr, MT, row_ptr, col, s.a, inv_nff, s.x, s.t);
+        PETCH_LAUNCH_CHECK("k_gm_matvec");
+        k_gm_resid<<<gb, kGB, 0, st>>>(hdr, MT, sky, s.t, s.w);
+        PETCH_LAUNCH_CHECK("k_gm_resid");
+        if ((rc = dot(s.w, s.w, s.scal, 1))) return rc;
+        double beta0 = 0.0;
+        if ((rc = read(s.scal, &beta0))) return rc;
+        if (beta0 <= tol) {
+            status = 0;
+            break;
+        }
+        k_gm_scale<<<gb, kGB, 0, st>>>(hdr, MT, s.w, s.scal, s.V);
+        PETCH_LAUNCH_CHECK("k_gm_scale");
+        k_gm_start<<<1, 32, 0, st>>>(s, restart);
+        PETCH_LAUNCH_CHECK("k_gm_start");
+        int k = 0;
+        for (int j = 0; j < restart; ++j) {
+            double* vj = s.V + (size_t)j * MT;
+            k_gm_matvec<<<gb, kGB, 0, st>>>(hdr, MT, row_ptr, col, s.a, inv_nff, vj, s.w);
+            PETCH_LAUNCH_CHECK("k_gm_matvec");
+            double* hj = s.H + (size_t)j * m1;
+            for (int i = 0; i <= j; ++i) {         // modified Gram-Schmidt
+                if ((rc = dot(s.w, s.V + (size_t)i * MT, hj + i, 0))) return rc;
+                k_gm_axpy<<<gb, kGB, 0, st>>>(hdr, MT, hj + i, s.V + (size_t)i * MT, s.w);
+                PETCH_LAUNCH_CHECK("k_gm_axpy");
+            }
+            if ((rc = dot(s.w, s.w, hj + j + 1, 1))) return rc;
+            k_gm_scale<<<gb, kGB, 0, st>>>(hdr, MT, s.w, hj + j + 1, s.V + (size_t)(j + 1) * MT);
+            PETCH_LAUNCH_CHECK("k_gm_scale");
+            k_gm_givens<<<1, 32, 0, st>>>(s, j, restart);
+            PETCH_LAUNCH_CHECK("k_gm_givens");
+            k = j + 1;
+            double est = 0.0;
+            if ((rc = read(s.scal + 1, &est))) return rc;
+            if (est <= tol) break;
+        }
+        k_gm_backsolve<<<1, 32, 0, st>>>(s, k, restart);
+        PETCH_LAUNCH_CHECK("k_gm_backsolve");
+        k_gm_xupdate<<<gb, kGB, 0, st>>>(hdr, MT, s, k);
+        PETCH_LAUNCH_CHECK("k_gm_xupdate");
+    }
+    if (status) {   // the iterate after the last cycle may have converged: check it as scipy does
+        k_gm_matvec<<<gb, kGB, 0, st>>>(hdr, MT, row_ptr, col, s.a, inv_nff, s.x, s.t);
+        PETCH_LAUNCH_CHECK("k_gm_matvec");
+        k_gm_resid<<<gb, kGB, 0, st>>>(hdr, MT, sky, s.t, s.w);
+        PETCH_LAUNCH_CHECK("k_gm_resid");
+        if ((rc = dot(s.w, s.w, s.scal, 1))) return rc;
+        double r = 0.0;
+        if ((rc = read(s.scal, &r))) return rc;
+        if (r <= tol) status = 0;
+    }
+    k_gm_out<<<gb, kGB, 0, st>>>(hdr, MT, s.x, g_out);
+    PETCH_LAUNCH_CHECK("k_gm_out");
+    *info = status;
+    return PETCH_OK;
+}

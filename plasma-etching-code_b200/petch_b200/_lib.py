@@ -105,6 +105,8 @@ SIGNATURES = {
     "petch_ff_scratch_bytes": [I, I, LLP],
     "petch_ff_matrix": [P, I, I, P, I, P, P, P, P, L, P],
     "petch_radiosity_solve": [P, I, I, P, P, P, I, P, D, D, I, P, P, P, P],
+    "petch_radiosity_gmres_scratch_bytes": [I, I, LLP],
+    "petch_radiosity_gmres": [P, I, I, P, P, P, I, P, D, D, I, I, P, P, L, P, P],
     "petch_dda_scratch_bytes": [I, I, I, I, I, LLP],
     "petch_dda_prepare": [P, I, I, I, D, D, I, I, P, I, P, P, P, P, P, I, P, L, P],
     "petch_dda_solve": [I, I, I, I, I, P, D, D, I, P, L, P, P, P],

@@ -411,10 +411,9 @@ class FluxEngine:
         """mc_flux_3d_radiosity (threed.py:923-991) on the device: ions as _ions_deterministic
         (unsmoothed), into-gas normals from phi, n_ff form-factor rays per face, the CSR form
         factor matrix, then n_fp rounds of the two-species Jacobi solve and the Belen coverage
-        update, starting from bare = 1."""
+        update, starting from bare = 1; par['radiosity_solver'] 'gmres' solves each species by
+        restarted GMRES (anything else: the Jacobi sweeps, as the reference)."""
         par, flags, m = self.par, self.flags, self.mesh
-        if par.get('radiosity_solver', 'jacobi') != 'jacobi':
-            raise NotImplementedError("only the Jacobi radiosity solver is provided")
         s = _sp()
         work = self.small[0:6]
         yields = self._ions_deterministic(n_ion, seed)
@@ -441,17 +440,44 @@ class FluxEngine:
                   r['scratch'].data_ptr(), r['scratch'].numel(), s)
         self.bare.fill_(1.0)
         betaE, betaO = float(self.par.get('betaE', 0.7)), float(self.par.get('betaO', 1.0))
+        gmres = self.par.get('radiosity_solver', 'jacobi') == 'gmres'
         for _ in range(n_fp):
             self.ktimer.start("k_rad_solve")
-            _lib.call("petch_radiosity_solve", m.id, m.MT, m.MV, r['row_ptr'].data_ptr(),
-                      r['col'].data_ptr(), r['sky'].data_ptr(), int(n_ff), self.bare.data_ptr(),
-                      betaE, betaO, int(n_iter), self.m_F.data_ptr(), self.m_O.data_ptr(),
-                      r['work2'].data_ptr(), s)
+            if gmres:
+                for beta, out in ((betaE, self.m_F), (betaO, self.m_O)):
+                    self._radiosity_gmres(r, n_ff, beta, n_iter, out)
+            else:
+                _lib.call("petch_radiosity_solve", m.id, m.MT, m.MV, r['row_ptr'].data_ptr(),
+                          r['col'].data_ptr(), r['sky'].data_ptr(), int(n_ff),
+                          self.bare.data_ptr(), betaE, betaO, int(n_iter), self.m_F.data_ptr(),
+                          self.m_O.data_ptr(), r['work2'].data_ptr(), s)
             self.ktimer.stop("k_rad_solve")
             _lib.call("petch_belen_bare", m.id, m.MT, m.MV, ctypes.byref(self.chem),
                       self.m_i.data_ptr(), self.m_F.data_ptr(), self.m_O.data_ptr(),
                       self.cos_i.data_ptr(), yields[1], yields[2], self.bare.data_ptr(), s)
 
+
+    def _radiosity_gmres(self, r, n_ff, beta, n_iter, out, rtol=1e-3, restart=12, maxiter=40):
+        """One species of solve() with radiosity_solver='gmres' (threed.py:972-982): restarted
+        GMRES on (I - M) G = D into out; the Jacobi sweeps when it does not converge."""
+        m = self.mesh
+        s = _sp()
+        if r.get('gm') is None or r['gm'][0] != restart:
+            nb = ctypes.c_longlong()
+            _lib.call("petch_radiosity_gmres_scratch_bytes", m.MT, int(restart), ctypes.byref(nb))
+            r['gm'] = (restart, torch.empty(int(nb.value), dtype=torch.uint8, device="cuda"))
+        scr = r['gm'][1]
+        info = ctypes.c_int(0)
+        _lib.call("petch_radiosity_gmres", m.id, m.MT, m.MV, r['row_ptr'].data_ptr(),
+                  r['col'].data_ptr(), r['sky'].data_ptr(), int(n_ff), self.bare.data_ptr(),
+                  float(beta), float(rtol), int(restart), int(maxiter), out.data_ptr(),
+                  scr.data_ptr(), scr.numel(), ctypes.byref(info), s)
+        if info.value != 0:
+            _lib.call("petch_radiosity_solve", m.id, m.MT, m.MV, r['row_ptr'].data_ptr(),
+                      r['col'].data_ptr(), r['sky'].data_ptr(), int(n_ff), self.bare.data_ptr(),
+                      float(beta), float(beta), int(n_iter), out.data_ptr(),
+                      self.tmp5.data_ptr(), r['work2'].data_ptr(), s)
+        return info.value
 
     def flux_dda(self, phi, n_ion, seed, n_fp=4):
         """mc_flux_3d_dda (threed.py:1211-1244) on the device: ions as _ions_deterministic, the

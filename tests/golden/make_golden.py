@@ -4,7 +4,7 @@ warp-lang replaced by warp_shim.py (a CPU stand-in: see its docstring for what i
 
 Run in a checkout that has the reference at /root/reference (or $PETCH_REFERENCE):
 
-    python tests/golden/make_golden.py [group ...]   # groups: levelset surface flux radiosity options redep dda knudsen
+    python tests/golden/make_golden.py [group ...]   # groups: levelset surface flux radiosity options redep dda knudsen gmres
 
 The fixtures are committed; tests read only the .npz files, never the reference.
 """
@@ -587,8 +587,60 @@ def knudsen():
     np.savez_compressed(os.path.join(HERE, "knudsen.npz"), **out)
 
 
+def gmres():
+    """mc_flux_3d_radiosity with radiosity_solver='gmres' (threed.py:964-985: scipy's gmres on
+    (I - M) G = D, rtol 1e-3, restart 12, maxiter 40, Jacobi on failure) on the radiosity group's
+    meshes at its recorded seed: the form-factor hits and ion results are recorded with the
+    solution, so the solve can be replayed."""
+    out = {}
+    wp = t3.wp
+    real_launch = wp.launch
+    rec = {}
+
+    def launch(k, dim, device=None, inputs=()):
+        real_launch(k, dim, device=device, inputs=inputs)
+        if k is t3._trace_ff:
+            rec['hit'] = np.asarray(inputs[3]).astype(np.int32).copy()
+
+    wp.launch = launch
+    try:
+        for key, hole in (("hole", True), ("trench", False)):
+            m, geo, phi = _small_mesh(hole, nx=10, ny=10, nz=14, dx=0.3)
+            verts = m.verts.astype(np.float32)
+            faces = m.faces
+            v64 = verts.astype(np.float64)[faces]
+            centroids = v64.mean(axis=1)
+            areas = 0.5 * np.linalg.norm(np.cross(v64[:, 1] - v64[:, 0], v64[:, 2] - v64[:, 0]),
+                                         axis=1)
+            geo = dict(geo, phi=phi.astype(np.float64))
+            mesh = wp.Mesh(points=wp.array(verts, dtype=wp.vec3),
+                           indices=wp.array(faces.flatten(), dtype=wp.int32))
+            for bE, tag in ((0.7, "a"), (0.05, "b")):    # b: high albedo, where Jacobi lags
+                par = dict(t3.PAR, periodic_y=0 if hole else 1, radiosity_solver="gmres",
+                           betaE=bE)
+                flags = t3.DEFAULT_FLAGS.__class__(chemistry="belen", yield_angular="viennaps",
+                                                   ion_reflection=True, coverage_sticking=True,
+                                                   neutral_transport="radiosity")
+                p = dict(par)
+                t0 = time.time()
+                m_i, m_F, m_O, cos_i = t3.mc_flux_3d_radiosity(mesh, verts, faces, centroids,
+                                                               areas, geo, p, n_ion=3000, n_ff=64,
+                                                               seed=100, flags=flags)
+                print(f"  {key}/{tag} gmres: {time.time() - t0:.1f}s", flush=True)
+                out[f"{key}_{tag}_hit"] = rec['hit']
+                out[f"{key}_{tag}_m_i"], out[f"{key}_{tag}_cos_i"] = m_i, cos_i
+                out[f"{key}_{tag}_m_F"], out[f"{key}_{tag}_m_O"] = m_F, m_O
+                out[f"{key}_{tag}_ion_yield"] = np.stack(p['_ion_yield'])
+                out[f"{key}_{tag}_betaE"] = np.array([bE])
+            out[f"{key}_verts"], out[f"{key}_faces"] = verts, faces
+            out[f"{key}_phi"] = phi.astype(np.float32)
+    finally:
+        wp.launch = real_launch
+    np.savez_compressed(os.path.join(HERE, "gmres.npz"), **out)
+
+
 GROUPS = {"levelset": levelset, "surface": surface, "flux": flux, "radiosity": radiosity,
-          "options": options, "redep": redep, "dda": dda, "knudsen": knudsen}
+          "options": options, "redep": redep, "dda": dda, "knudsen": knudsen, "gmres": gmres}
 
 if __name__ == "__main__":
     for g in (sys.argv[1:] or list(GROUPS)):
