@@ -176,6 +176,14 @@ int petch_trace_legacy(const void* mesh, int max_tris, int max_verts, const petc
                        float cos_thr, float eta, uint32_t seed, int n, float* flux, float* angacc,
                        int* work, void* stream);
 
+/* Replaces the electron trace of mc_flux_3d_coupled's surface-charging block
+ * (petch/threed.py:852-856: _src('ion', ..., e_ang_sigma) + _trace3d_cov_rr with bare = 1,
+ * beta = 1): n electrons from the Gaussian-angle source (tilt sigma), each depositing weight 1
+ * on the face it first reaches; lateral wrap as the domain says.  flux float[max_tris], zeroed
+ * first. */
+int petch_trace_electrons(const void* mesh, int max_tris, int max_verts, const petch_domain* dom,
+                          float sigma, uint32_t seed, int n, float* flux, int* work, void* stream);
+
 /* Replaces extend_velocity_gpu + _extend_kernel (petch/threed.py:1324-1346): Fs = V[nearest face]
  * on cells with |phi| < band, else 0.  fold_mask = 1: mask cells get -1 (petch_advect's pinned
  * marker, mask may not be NULL) and band cells with Fs > 0 are appended to active (if not NULL;
@@ -561,6 +569,14 @@ int petch_charging_apply(const int* n_faces, int max_faces, const float* centroi
                          float* m_i, float* y_sp, float* y_ie, float* y_p, void* stream);
 int petch_zero_below(const int* n_faces, int max_faces, const float* centroids, double z_top,
                      float* values, void* stream);
+
+/* Replaces the charging factor of mc_flux_3d_coupled (petch/threed.py:862-868): with
+ * sh_e = clip(m_e / max(ref_e, 1e-6), 0, 1) and sh_i likewise from m_i and ref_i, every face's
+ * m_i (in place) is multiplied by 1 - alpha clip(1 - sh_e / max(sh_i, 1e-3), 0, 1).  ref_i,
+ * ref_e: the 90th percentiles of m_i and m_e over the faces above 1e-6 (1 when none), computed
+ * by the caller.  Float64 arithmetic. */
+int petch_electron_shadow(const int* n_faces, int max_faces, const float* m_e, double ref_i,
+                          double ref_e, double alpha, float* m_i, void* stream);
 
 /* Replaces solve() with radiosity_solver = 'gmres' (petch/threed.py:972-982): restarted GMRES
  * (restart Krylov vectors per cycle, at most maxiter cycles, modified Gram-Schmidt, Givens

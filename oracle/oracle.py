@@ -60,6 +60,7 @@ _SIGS = {
     "orc_trace_ions": ([_P, _P, _P, _U64, _I, _P], None),
     "orc_trace_neutrals": ([_P, _P, _P, _D, _U64, _U64, _I, _P], None),
     "orc_trace_legacy": ([_P, _P, _I, _D, _D, _I, _I, _D, _D, _U64, _I, _P, _P], None),
+    "orc_trace_electrons": ([_P, _P, _D, _U64, _I, _P], None),
     "orc_trace_ff": ([_P, _P, _P, _P, _I, _I, _U64, _P], None),
     "orc_trace_redep": ([_P, _P, _P, _P, _I, _D, _U64, _I, _P], None),
     "orc_dda_gather": ([_P, _I, _I, _I, _P, _P, _P, _P, _I, _P, _D, _D, _D, _I, _I, _I, _I, _P],
@@ -303,6 +304,14 @@ def trace_legacy(mesh, geo, par, ion, sigma, sticking, n_reemit, specular, cos_t
     return fl, ang
 
 
+def trace_electrons(mesh, geo, par, sigma, seed, n):
+    """The electron trace of mc_flux_3d_coupled's charging block (threed.py:852-856)."""
+    fl = np.zeros(mesh.F, np.float64)
+    lib().orc_trace_electrons(mesh.h, _p(_dom(geo, par)), float(sigma), int(seed) & (2**64 - 1),
+                              int(n), _p(fl))
+    return fl
+
+
 # ------------------------------- per-face arithmetic (numpy) -------------------------------
 def smooth(flux, normals, pairs, n_iter=1, alpha=1.0):
     """smooth_flux (threed.py:129-148), np.add.at pair scatter."""
@@ -411,11 +420,38 @@ def surface_rate(m_i, m_F, m_O, cos_i, is_mask, par, chemistry, yield_angular, i
     return V
 
 
+def open_field_level(x):
+    """np.percentile(x[x > 1e-6], 90), 1.0 when no face is above 1e-6 (threed.py:862-863)."""
+    x = np.asarray(x, np.float64)
+    live = x[x > 1e-6]
+    return float(np.percentile(live, 90)) if live.size else 1.0
+
+
+def electron_shadow(m_i, m_e, alpha):
+    """The charging factor of mc_flux_3d_coupled (threed.py:862-868): each flux relative to its
+    open-field level, clipped to [0, 1]; m_i times 1 - alpha clip(1 - sh_e / max(sh_i, 1e-3), 0, 1).
+    Returns (m_i scaled, ref_i, ref_e)."""
+    m_i = np.asarray(m_i, np.float64)
+    m_e = np.asarray(m_e, np.float64)
+    ref_i, ref_e = open_field_level(m_i), open_field_level(m_e)
+    sh_e = np.clip(m_e / max(ref_e, 1e-6), 0.0, 1.0)
+    sh_i = np.clip(m_i / max(ref_i, 1e-6), 0.0, 1.0)
+    f = 1.0 - alpha * np.clip(1.0 - sh_e / np.maximum(sh_i, 1e-3), 0.0, 1.0)
+    return m_i * f, ref_i, ref_e
+
+
+def electron_flux(fe, A, A_src, n_neu, par, sm):
+    """m_e of the charging block (threed.py:857-859): the normalised electron arrival times eFlux,
+    clipped to [0, 8], smoothed like the other fluxes."""
+    return sm(np.clip((fe / A) / (n_neu / A_src) * par.get('eFlux', 1.0), 0.0, 8.0))
+
+
 def flux_coupled(mesh, geo, par, flags, n_ion, n_neu, seed, bare_init=None, tt=None, phi=None):
-    """mc_flux_3d_coupled (faithful-ion / legacy-ion branches, RR neutrals, the optional floor
-    throttle) on the oracle mesh.  Returns (m_i, m_F, m_O, cos_i, bare, ion_yield-or-None).  tt:
-    optional dict that accumulates the seconds spent in the ray tracers under key 'trace'; phi:
-    the level set (for the throttle's into-gas normals)."""
+    """mc_flux_3d_coupled (faithful-ion / legacy-ion branches, the optional electron-shadowing
+    charge model, RR neutrals, the optional floor throttle) on the oracle mesh.  Returns (m_i,
+    m_F, m_O, cos_i, bare, ion_yield-or-None).  tt: optional dict that accumulates the seconds
+    spent in the ray tracers under key 'trace'; phi: the level set (for the throttle's into-gas
+    normals)."""
     tt = {} if tt is None else tt
     tt.setdefault('trace', 0.0)
 
@@ -445,6 +481,11 @@ def flux_coupled(mesh, geo, par, flags, n_ion, n_neu, seed, bare_init=None, tt=N
                        0.8, seed * 9 + 1, n_ion)
         cos_i = np.where(fi > 0, ai / np.where(fi > 0, fi, 1.0), 0.0)
         m_i = sm(np.clip((fi / A) * (A_src / n_ion), 0.0, 1.5))
+    alpha_c = float(par.get('charge_alpha', 0.0))
+    if getattr(flags, "surface_charging", False) and alpha_c > 0.0:
+        fe = timed(trace_electrons, mesh, geo, par, par.get('e_ang_sigma', 0.5), seed * 9 + 7,
+                   n_neu)
+        m_i, _, _ = electron_shadow(m_i, electron_flux(fe, A, A_src, n_neu, par, sm), alpha_c)
     if getattr(flags, "floor_charge_throttle", False):
         fn = gas_normals(mesh.verts, mesh.faces, mesh.centroid, phi, geo['dx'])
         c32 = np.asarray(mesh.verts, np.float32)[mesh.faces].mean(axis=1)

@@ -283,6 +283,23 @@ void orc_trace_neutrals(void* mesh, const double* dom, const double* bare, doubl
     }
 }
 
+// The electron trace of mc_flux_3d_coupled's charging block (threed.py:852-856): the ion-type
+// source with tilt sigma, _trace3d_cov_rr with bare = 1 and beta = 1 -> weight 1 on the first face
+// reached, with the domain's lateral wrap.  flux double[F] (caller zeroes).
+void orc_trace_electrons(void* mesh, const double* dom, double sigma, uint64_t seed, int n,
+                         double* flux) {
+    const Mesh* m = (const Mesh*)mesh;
+    Dom D{dom[0], dom[1], dom[2], dom[3], (int)dom[4]};
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int p = 0; p < n; ++p) {
+        Rng g(seed, 0x656c6563ULL, (uint64_t)p);
+        double o[3], d[3];
+        source(g, true, sigma, D, o, d);
+        orc::HitD h = query(m, o, d, D);
+        if (h.f >= 0) add(flux, h.f, 1.0);
+    }
+}
+
 // _trace3d: flux, angacc double[F] (caller zeroes); no lateral wrap.
 void orc_trace_legacy(void* mesh, const double* dom, int ion, double sigma, double sticking,
                       int n_reemit, int specular, double cos_thr, double eta, uint64_t seed, int n,

@@ -1,13 +1,14 @@
-// Floor-charging hooks on the per-face ion results: the Hwang-Giapis closure
+// Charging hooks on the per-face ion results: the Hwang-Giapis closure
 // (_apply_hg_charging, petch/threed.py:1046-1110) and the deep-AR floor throttle
-// (_apply_floor_charge_throttle, petch/threed.py:1112-1147).
+// (_apply_floor_charge_throttle, petch/threed.py:1112-1147), and the electron-shadowing factor of
+// mc_flux_3d_coupled (threed.py:847-868; k_electron_shadow below).
 //
-// Both act on the same face classes: inside the feature footprint (within half the feature width
-// + 2 dx of its axis), below sub_top, and either facing up (into-gas n_z > 0.7: the floor) or not
-// (the sidewall; the HG "foot" is the part within foot_h of the deepest floor face).  The
-// aspect-ratio tables they interpolate are host arithmetic on four numbers; the device gives those
-// numbers (petch_charging_floor_stats, one block, fixed-order reductions) and applies the result
-// to every face (petch_charging_apply).
+// The first two act on the same face classes: inside the feature footprint (within half the
+// feature width + 2 dx of its axis), below sub_top, and either facing up (into-gas n_z > 0.7: the
+// floor) or not (the sidewall; the HG "foot" is the part within foot_h of the deepest floor
+// face).  The aspect-ratio tables they interpolate are host arithmetic on four numbers; the device
+// gives those numbers (petch_charging_floor_stats, one block, fixed-order reductions) and applies
+// the result to every face (petch_charging_apply).
 #include "common.cuh"
 #include "petch_b200.h"
 
@@ -122,10 +123,40 @@ __global__ void k_zero_below(const int* __restrict__ n_faces, int MF, const floa
         if ((double)cen[3 * f + 2] <= z_top) v[f] = 0.0f;
 }
 
+// The electron-shadowing factor (threed.py:862-867): each flux is taken relative to its own
+// open-field level (ref: the 90th percentile of its faces above 1e-6), clipped to [0, 1]; the ion
+// result of a face is scaled by f = 1 - alpha clip(1 - sh_e / max(sh_i, 1e-3), 0, 1).  Float64,
+// every product and difference rounded on its own (no contraction), as numpy evaluates it.
+__global__ void k_electron_shadow(const int* __restrict__ n_faces, int MF,
+                                  const float* __restrict__ m_e, double ref_i, double ref_e,
+                                  double alpha, float* __restrict__ m_i) {
+    const int F = min(max(*n_faces, 0), MF);
+    const double ri = fmax(ref_i, 1e-6), re = fmax(ref_e, 1e-6);
+    for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < F; f += gridDim.x * blockDim.x) {
+        const double mi = m_i[f];
+        const double sh_e = fmin(fmax((double)m_e[f] / re, 0.0), 1.0);
+        const double sh_i = fmin(fmax(mi / ri, 0.0), 1.0);
+        const double gap = fmin(fmax(__dsub_rn(1.0, sh_e / fmax(sh_i, 1e-3)), 0.0), 1.0);
+        const double fc = __dsub_rn(1.0, __dmul_rn(alpha, gap));
+        m_i[f] = (float)__dmul_rn(mi, fc);
+    }
+}
+
 }  // namespace
 }  // namespace petch
 
 using namespace petch;
+
+extern "C" int petch_electron_shadow(const int* n_faces, int max_faces, const float* m_e,
+                                     double ref_i, double ref_e, double alpha, float* m_i,
+                                     void* stream) {
+    PETCH_REQUIRE(n_faces && m_e && m_i, "petch_electron_shadow: null pointer");
+    PETCH_REQUIRE(max_faces > 0, "petch_electron_shadow: bad face capacity");
+    k_electron_shadow<<<grid_for(max_faces, 256), 256, 0, as_stream(stream)>>>(
+        n_faces, max_faces, m_e, ref_i, ref_e, alpha, m_i);
+    PETCH_LAUNCH_CHECK("k_electron_shadow");
+    return PETCH_OK;
+}
 
 extern "C" int petch_zero_below(const int* n_faces, int max_faces, const float* centroids,
                                 double z_top, float* values, void* stream) {

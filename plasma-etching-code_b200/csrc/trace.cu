@@ -249,6 +249,29 @@ struct NeutralShader {
     }
 };
 
+// The electron trace of the electron-shadowing charging model (threed.py:847-857):
+// _trace3d_cov_rr with bare = 1 and beta = 1 on rays from the ion-type (Gaussian angle, sigma =
+// e_ang_sigma) source, so every electron sticks where it first lands and deposits weight 1; the
+// lateral wrap follows the domain.
+struct ElectronShader {
+    float sigma;
+    float* flux;
+    int det;
+    static constexpr int kMaxBounce = 1;
+    static constexpr int kMinBlocks = kTraceMinBlocksRR;
+    __device__ __forceinline__ int count(const MeshView&, int n) const { return n; }
+    __device__ __forceinline__ void init(Rng& g, const Tracer&, const Domain& D, int, float3& o,
+                                         float3& d, RayState& s) const {
+        source(g, true, sigma, D, o, d);
+        s.w = 1.0f;
+    }
+    __device__ __forceinline__ bool hit(Rng&, const Tracer&, int f, float, float3&, float3&,
+                                        RayState& s) const {
+        tally(flux, f, s.w, det);
+        return false;
+    }
+};
+
 // _trace3d_ion_yield (threed.py:599-712): E ~ N(meanE, sigmaE) clipped at 0; on every hit
 // deposit the yield-weighted sputter / ion-enhanced / passivation rates, the weight and
 // cos * weight; then angle-dependent sticking, energy loss (<= 4 truncated-normal tries), weight
@@ -1149,6 +1172,32 @@ extern "C" int petch_trace_neutrals(const void* mesh, int max_tris, int max_vert
     sh.det = 1;
     int rc = launch_trace(m, to_domain(dom), sh, seed, 0x6e657500u ^ stream_id, n_neu, work, st,
                           "k_trace<neutrals>");
+    if (rc) return rc;
+    PETCH_DET_CONVERT(a_f, flux, (long long)max_tris);
+    return PETCH_OK;
+}
+
+extern "C" int petch_trace_electrons(const void* mesh, int max_tris, int max_verts,
+                                     const petch_domain* dom, float sigma, uint32_t seed, int n,
+                                     float* flux, int* work, void* stream) {
+    PETCH_REQUIRE(mesh && dom && flux && work, "petch_trace_electrons: null pointer");
+    PETCH_REQUIRE(n >= 0 && max_tris > 0 && max_verts > 0, "petch_trace_electrons: bad size");
+    cudaStream_t st = as_stream(stream);
+    MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
+    ElectronShader sh{sigma, flux, 0};
+    k_zero_faces<<<grid_for(max_tris, 256), 256, 0, st>>>(m.hdr, max_tris, flux, 1, nullptr, 0);
+    PETCH_LAUNCH_CHECK("k_zero_faces");
+    PETCH_CUDA(cudaMemsetAsync(work, 0, sizeof(int), st), "reset ray counter");
+    if (n == 0) return PETCH_OK;
+    DetArena arena;
+    if (!arena.on())
+        return launch_trace(m, to_domain(dom), sh, seed, 0x656c6563u, n, work, st,
+                            "k_trace<electrons>");
+    PETCH_DET_TAKE(a_f, (long long)max_tris);
+    sh.flux = reinterpret_cast<float*>(a_f);
+    sh.det = 1;
+    int rc = launch_trace(m, to_domain(dom), sh, seed, 0x656c6563u, n, work, st,
+                          "k_trace<electrons>");
     if (rc) return rc;
     PETCH_DET_CONVERT(a_f, flux, (long long)max_tris);
     return PETCH_OK;

@@ -89,6 +89,7 @@ SIGNATURES = {
     "petch_trace_ions": [P, I, I, DP, IP, U, I, P, P, P, P],
     "petch_trace_neutrals": [P, I, I, DP, P, F, U, U, I, P, P, P],
     "petch_trace_legacy": [P, I, I, DP, I, F, F, I, I, F, F, U, I, P, P, P, P],
+    "petch_trace_electrons": [P, I, I, DP, F, U, I, P, P, P],
     "petch_extend_velocity": [P, I, I, P, P, I, I, I, D, D, P, P, I, P, P, I, P, P],
     "petch_warmstart": [P, I, I, P, P, I, I, P, P, P],
     "petch_norm_smooth": [P, I, I, P, F, F, F, I, I, F, P, P, P, P],
@@ -118,6 +119,7 @@ SIGNATURES = {
     "petch_charging_floor_stats": [P, I, P, P, P, P, D, D, D, I, D, D, P, P],
     "petch_charging_apply": [P, I, P, P, D, D, D, I, D, P, P, D, P, P, P, P, P],
     "petch_zero_below": [P, I, P, D, P, P],
+    "petch_electron_shadow": [P, I, P, D, D, D, P, P],
     "petch_extend_velocity_centroid": [P, I, I, P, P, I, I, I, D, D, P, P, I, P, P, I, P, P],
     "petch_reinit_pde": [P, P, P, P, I, I, I, D, I, P],
     "petch_gaussian_smooth": [P, P, P, P, P, I, I, I, D, D, P],

@@ -196,6 +196,9 @@ def run_etch_3d_tangent(theta, Lx, Ly, Lz, dx, trench_width, mask_th, sub_top, t
                                   "redeposition")
     if getattr(flags, "floor_charge_throttle", False):
         raise NotImplementedError("the recipe gradient does not include the floor-charging throttle")
+    if getattr(flags, "surface_charging", False) and float(par.get('charge_alpha', 0.0)) > 0.0:
+        raise NotImplementedError("the recipe gradient does not include the electron-shadowing "
+                                  "charge model")
     torch.cuda.init()
     geo = make_trench_3d(Lx, Ly, Lz, dx, trench_width, mask_th, sub_top, hole=hole, host=False)
     geo['mask_th'] = mask_th

@@ -87,6 +87,10 @@ class BatchEngine:
                 raise NotImplementedError(f"{flag} is not part of the batched step")
         if getattr(flags, "neutral_transport", "mc") != "mc":
             raise NotImplementedError("the batched step runs Monte-Carlo neutrals")
+        alphas = [float(dict(PAR, **sp.get('par', {})).get('charge_alpha', 0.0)) for sp in specs]
+        if getattr(flags, "surface_charging", False) and max(alphas) > 0.0:
+            raise NotImplementedError("the electron-shadowing charge model is not part of the "
+                                      "batched step")
         dxs = {float(s['dx']) for s in specs}
         if len(dxs) != 1:
             raise ValueError("all instances need the same dx")

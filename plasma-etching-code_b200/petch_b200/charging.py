@@ -130,3 +130,41 @@ def apply_floor_throttle(fe, normals):
     present = fe.yields[0] is not None
     _apply(fe, normals, (Q, Q, Q, Q), (0.0, 0.0, 0.0), -np.inf, present)
     return dict(AR=AR, Q=Q, n_floor=int(n_floor), z_floor=zmin)
+
+
+def open_field_level(x):
+    """np.percentile(x[x > 1e-6], 90) in float64, 1.0 when no face is above 1e-6: the open-field
+    reference level of a flux (threed.py:862-863)."""
+    x = np.asarray(x, np.float64)
+    live = x[x > 1e-6]
+    return float(np.percentile(live, 90)) if live.size else 1.0
+
+
+def apply_electron_shadow(fe, n_neu, seed):
+    """The surface-charging block of mc_flux_3d_coupled (threed.py:847-868) on a FluxEngine's
+    device results, for flags.surface_charging truthy and charge_alpha > 0: n_neu electrons from
+    the Gaussian-angle source (e_ang_sigma) land with unit sticking; m_e = their normalised
+    arrival (times eFlux, clipped at 8, smoothed like the other fluxes); the host takes the two
+    open-field levels from one read of m_i and m_e; one kernel multiplies m_i by the charging
+    factor.  The yields are left as they are, as in the reference.  Returns the levels used."""
+    par, geo, m = fe.par, fe.geo, fe.mesh
+    s = torch.cuda.current_stream().cuda_stream
+    if getattr(fe, "m_e", None) is None or fe.m_e.numel() != fe.MT:
+        fe.m_e = torch.empty(fe.MT, device="cuda", dtype=torch.float32)
+    A_src = float(geo['Lx'] * geo['Ly'])
+    n_smooth = int(par.get('flux_smooth', 1))
+    sm_alpha = float(par.get('flux_smooth_alpha', 1.0))
+    work = fe.small[0:6]
+    _lib.call("petch_trace_electrons", m.id, m.MT, m.MV, ctypes.byref(fe.dom),
+              float(par.get('e_ang_sigma', 0.5)), int(seed * 9 + 7) & 0xffffffff, int(n_neu),
+              fe.flux.data_ptr(), work.data_ptr(), s)
+    _lib.call("petch_norm_smooth", m.id, m.MT, m.MV, fe.flux.data_ptr(),
+              float(A_src / n_neu * float(par.get('eFlux', 1.0))), 0.0, 8.0, 1, n_smooth,
+              sm_alpha, fe.m_e.data_ptr(), fe.tmp5.data_ptr(), fe.tmp5[m.MT:].data_ptr(), s)
+    F = m.n_faces()
+    ref_i = open_field_level(fe.m_i[:F].cpu().numpy())
+    ref_e = open_field_level(fe.m_e[:F].cpu().numpy())
+    alpha = float(par.get('charge_alpha', 0.0))
+    _lib.call("petch_electron_shadow", m.id, m.MT, fe.m_e.data_ptr(), ref_i, ref_e, alpha,
+              fe.m_i.data_ptr(), s)
+    return dict(ref_i=ref_i, ref_e=ref_e, alpha=alpha)

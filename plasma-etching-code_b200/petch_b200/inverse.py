@@ -152,6 +152,10 @@ class BatchTangentEngine:
                 raise NotImplementedError(f"{flag} is not part of the batched gradient")
         if getattr(flags, "neutral_transport", "mc") != "mc":
             raise NotImplementedError("the batched gradient follows Monte-Carlo neutrals")
+        alphas = [float(dict(PAR, **sp.get('par', {})).get('charge_alpha', 0.0)) for sp in specs]
+        if getattr(flags, "surface_charging", False) and max(alphas) > 0.0:
+            raise NotImplementedError("the electron-shadowing charge model is not part of the "
+                                      "batched gradient")
         dxs = {float(s['dx']) for s in specs}
         if len(dxs) != 1:
             raise ValueError("all instances need the same dx")

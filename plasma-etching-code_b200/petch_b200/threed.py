@@ -195,12 +195,6 @@ def chem_params(par, flags):
 
 
 def _unsupported(flags, par):
-    nt = getattr(flags, "neutral_transport", "mc")
-    if (getattr(flags, "surface_charging", False) and par.get('charge_alpha', 0.0) > 0.0
-            and nt not in ("radiosity", "dda", "knudsen")
-            and getattr(flags, "coverage_sticking", False)):
-        raise NotImplementedError("the electron-shadowing charging model (charge_alpha > 0) is "
-                                  "outside this engine's scope")
     if par.get('cov_transport', 'rr') != 'rr':
         raise NotImplementedError("only the Russian-roulette coverage transport (cov_transport='rr')")
 
@@ -300,6 +294,10 @@ class FluxEngine:
                       float(A_src / n_ion), 0.0, 1.5, 1, n_smooth, alpha, self.m_i.data_ptr(),
                       self.tmp5.data_ptr(), self.tmp5[m.MT:].data_ptr(), s)
             yields = (None, None, None)
+        if (flags is not None and getattr(flags, "surface_charging", False)
+                and float(par.get('charge_alpha', 0.0)) > 0.0):
+            from .charging import apply_electron_shadow
+            self.electron = apply_electron_shadow(self, n_neu, seed)
         if flags is not None and getattr(flags, "floor_charge_throttle", False):
             from .charging import apply_floor_throttle
             phi = phi if phi is not None else getattr(self, "phi", None)

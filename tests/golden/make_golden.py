@@ -4,7 +4,7 @@ warp-lang replaced by warp_shim.py (a CPU stand-in: see its docstring for what i
 
 Run in a checkout that has the reference at /root/reference (or $PETCH_REFERENCE):
 
-    python tests/golden/make_golden.py [group ...]   # groups: levelset surface flux radiosity options redep dda knudsen gmres
+    python tests/golden/make_golden.py [group ...]   # groups: levelset surface flux radiosity options redep dda knudsen gmres electron
 
 The fixtures are committed; tests read only the .npz files, never the reference.
 """
@@ -639,8 +639,96 @@ def gmres():
     np.savez_compressed(os.path.join(HERE, "gmres.npz"), **out)
 
 
+def electron():
+    """The electron-shadowing charge model of mc_flux_3d_coupled (threed.py:847-868) run
+    unmodified: (1) its electron trace (_source3d('ion', ..., e_ang_sigma) + _trace3d_cov_rr with
+    bare = 1, beta = 1) over 8 seeds, per-face mean and standard error; (2) mc_flux_3d_coupled with
+    surface_charging and charge_alpha > 0 (faithful and legacy ions), with every trace launch's
+    tallies recorded, so the normalisation, the charging factor and the coverage fixed point can
+    be replayed exactly from them."""
+    out = {}
+    wp = t3.wp
+    real_launch = wp.launch
+    rec = []
+
+    def launch(k, dim, device=None, inputs=()):
+        real_launch(k, dim, device=device, inputs=inputs)
+        if k is t3._trace3d_cov_rr:
+            rec.append(("rr", int(inputs[5]), float(inputs[4]), np.asarray(inputs[6]).copy()))
+        elif k is t3._trace3d_ion_yield:
+            rec.append(("ion", int(inputs[3]), 0.0,
+                        np.stack([np.asarray(a).copy() for a in inputs[-5:]])))
+        elif k is t3._trace3d:
+            rec.append(("legacy", int(inputs[5]), 0.0,
+                        np.stack([np.asarray(a).copy() for a in inputs[-2:]])))
+
+    for hole in (True, False):
+        key = "hole" if hole else "trench"
+        m, geo, phi = _small_mesh(hole, nx=10, ny=10, nz=14, dx=0.3)
+        verts = m.verts.astype(np.float32)
+        faces = m.faces
+        F = len(faces)
+        v64 = verts.astype(np.float64)[faces]
+        areas = 0.5 * np.linalg.norm(np.cross(v64[:, 1] - v64[:, 0], v64[:, 2] - v64[:, 0]),
+                                     axis=1)
+        mesh = wp.Mesh(points=wp.array(verts, dtype=wp.vec3),
+                       indices=wp.array(faces.flatten(), dtype=wp.int32))
+        Lx, Ly, Lz = geo['Lx'], geo['Ly'], geo['Lz']
+        periodic = 0 if hole else 1
+        out[f"{key}_verts"], out[f"{key}_faces"], out[f"{key}_areas"] = verts, faces, areas
+        out[f"{key}_geo"] = np.array([Lx, Ly, Lz, geo['dx'], periodic])
+        n = 6000
+
+        def etrace(sd):
+            o, d = t3._source3d('ion', n, Lx, Ly, Lz - geo['dx'], 0.5, 'pseudo',
+                                np.random.default_rng(sd), sd)
+            f = wp.zeros(F, dtype=float)
+            wp.launch(t3._trace3d_cov_rr, dim=n, inputs=[
+                mesh.id, wp.array(o, dtype=wp.vec3), wp.array(d, dtype=wp.vec3),
+                wp.array(np.ones(F, np.float32), dtype=float), 1.0, sd, f, Lx, Ly, Lz, periodic])
+            return f.numpy() / n
+
+        t0 = time.time()
+        mean, se = _mean_se(etrace, range(100, 108))
+        print(f"  {key} electrons: {time.time() - t0:.1f}s", flush=True)
+        out[f"{key}_electron_mean"], out[f"{key}_electron_se"] = mean, se
+        out[f"{key}_electron_n"] = np.array([n * 8])
+
+        wp.launch = launch
+        try:
+            for tag, faithful in (("faithful", True), ("legacy", False)):
+                par = dict(t3.PAR, periodic_y=periodic, charge_alpha=0.6, eFlux=1.3)
+                flags = t3.DEFAULT_FLAGS.__class__(
+                    chemistry="belen", yield_angular="viennaps", ion_reflection=faithful,
+                    coverage_sticking=True, surface_charging=True)
+                rec.clear()
+                p = dict(par)
+                t0 = time.time()
+                m_i, m_F, m_O, cos_i, bare = t3.mc_flux_3d_coupled(
+                    mesh, verts, faces, areas, geo, p, n_ion=3000, n_neu=3000, seed=100,
+                    flags=flags)
+                print(f"  {key} mc_flux_3d_coupled[{tag}]: {time.time() - t0:.1f}s", flush=True)
+                kinds = [r[0] for r in rec]
+                seeds = [r[1] for r in rec]
+                assert kinds[0] == ("ion" if faithful else "legacy") and seeds[1] == 100 * 9 + 7
+                out[f"{key}_{tag}_ion_raw"] = rec[0][3]
+                out[f"{key}_{tag}_electron_raw"] = rec[1][3]
+                out[f"{key}_{tag}_neutral_raw"] = np.stack([r[3] for r in rec[2:]])
+                out[f"{key}_{tag}_neutral_seed"] = np.array(seeds[2:])
+                out[f"{key}_{tag}_neutral_beta"] = np.array([r[2] for r in rec[2:]])
+                out[f"{key}_{tag}_m_i"], out[f"{key}_{tag}_m_F"] = m_i, m_F
+                out[f"{key}_{tag}_m_O"], out[f"{key}_{tag}_cos_i"] = m_O, cos_i
+                out[f"{key}_{tag}_bare"] = bare
+                if faithful:
+                    out[f"{key}_{tag}_ion_yield"] = np.stack(p['_ion_yield'])
+        finally:
+            wp.launch = real_launch
+    np.savez_compressed(os.path.join(HERE, "electron.npz"), **out)
+
+
 GROUPS = {"levelset": levelset, "surface": surface, "flux": flux, "radiosity": radiosity,
-          "options": options, "redep": redep, "dda": dda, "knudsen": knudsen, "gmres": gmres}
+          "options": options, "redep": redep, "dda": dda, "knudsen": knudsen, "gmres": gmres,
+          "electron": electron}
 
 if __name__ == "__main__":
     for g in (sys.argv[1:] or list(GROUPS)):
