@@ -294,6 +294,14 @@ int petch_gaussian_smooth(float* phi, float* tmp_a, float* tmp_b, const uint8_t*
                           const float* mask_phi, int nx, int ny, int nz, double sigma,
                           double truncate, void* stream);
 
+/* The column scan of the depth metrics (_depth3d / max_depth_3d, petch/threed.py:1798-1869):
+ * for each column cols[2c], cols[2c+1] (= i, j; device ints) of phi (nx, ny, nz; z fastest),
+ * k_out[c] = the index of the lowest cell of the gas run (phi < 0) that reaches the top cell, -1
+ * when the top cell is not gas, -2 when (i, j) lies outside the grid.  The caller takes zs[k]
+ * and the median / percentile. */
+int petch_column_floors(const float* phi, int nx, int ny, int nz, const int* cols, int n_cols,
+                        int* k_out, void* stream);
+
 /* Deterministic tallies (no reference counterpart).  With a scratch registered, every tracing
  * entry point accumulates its per-face tallies as 64-bit fixed-point integers (units of 2^-32,
  * carved from the scratch, converted to the float outputs at the end of the call): integer sums

@@ -122,9 +122,55 @@ __global__ void __launch_bounds__(kLB) k_gauss_pass(const float* __restrict__ in
     }
 }
 
+// The floor of a column for the depth metrics (threed.py:1822-1830): column (i, j) of phi is the
+// contiguous run phi[(i ny + j) nz + k], k = 0..nz-1.  A column whose top cell is not gas
+// (phi < 0) has no floor (-1); otherwise the floor is the lowest cell of the gas run that reaches
+// the top: one above the highest non-gas cell, 0 when every cell is gas.  One warp per column
+// scans 32 cells at a time from the top; the first chunk holding a non-gas cell ends the scan.
+// A column index outside the grid gives -2.
+__global__ void k_column_floors(const float* __restrict__ phi, int nx, int ny, int nz,
+                                const int* __restrict__ cols, int n_cols, int* __restrict__ k_out) {
+    const int lane = threadIdx.x & 31;
+    const int c = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+    if (c >= n_cols) return;
+    const int i = cols[2 * c], j = cols[2 * c + 1];
+    if (i < 0 || i >= nx || j < 0 || j >= ny) {
+        if (lane == 0) k_out[c] = -2;
+        return;
+    }
+    const float* col = phi + ((long long)i * ny + j) * nz;
+    if (!(col[nz - 1] < 0.0f)) {
+        if (lane == 0) k_out[c] = -1;
+        return;
+    }
+    int k = 0;
+    for (int start = nz - 1; start >= 0; start -= 32) {
+        const int idx = start - lane;
+        const bool solid = idx >= 0 && !(col[idx] < 0.0f);
+        const unsigned m = __ballot_sync(0xffffffffu, solid);
+        if (m) {
+            k = start - (__ffs(m) - 1) + 1;
+            break;
+        }
+    }
+    if (lane == 0) k_out[c] = k;
+}
+
 }  // namespace
 
 using namespace petch;
+
+extern "C" int petch_column_floors(const float* phi, int nx, int ny, int nz, const int* cols,
+                                   int n_cols, int* k_out, void* stream) {
+    PETCH_REQUIRE(phi && (n_cols == 0 || (cols && k_out)), "petch_column_floors: null pointer");
+    PETCH_REQUIRE(nx > 0 && ny > 0 && nz > 0 && n_cols >= 0, "petch_column_floors: bad size");
+    if (n_cols == 0) return PETCH_OK;
+    const long long threads = 32LL * n_cols;
+    k_column_floors<<<(unsigned)((threads + 255) / 256), 256, 0, as_stream(stream)>>>(
+        phi, nx, ny, nz, cols, n_cols, k_out);
+    PETCH_LAUNCH_CHECK("k_column_floors");
+    return PETCH_OK;
+}
 
 extern "C" int petch_reinit_pde(const float* phi_in, float* phi_out, float* phi0, float* tmp,
                                 int nx, int ny, int nz, double dx, int n_iter, void* stream) {

@@ -120,6 +120,7 @@ SIGNATURES = {
     "petch_charging_apply": [P, I, P, P, D, D, D, I, D, P, P, D, P, P, P, P, P],
     "petch_zero_below": [P, I, P, D, P, P],
     "petch_electron_shadow": [P, I, P, D, D, D, P, P],
+    "petch_column_floors": [P, I, I, I, P, I, P, P],
     "petch_extend_velocity_centroid": [P, I, I, P, P, I, I, I, D, D, P, P, I, P, P, I, P, P],
     "petch_reinit_pde": [P, P, P, P, I, I, I, D, I, P],
     "petch_gaussian_smooth": [P, P, P, P, P, I, I, I, D, D, P],

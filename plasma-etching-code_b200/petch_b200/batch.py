@@ -29,7 +29,7 @@ import torch
 from . import _lib
 from .params import DEFAULT_FLAGS, PAR
 from .threed import (MESH_ERR_HASH_FULL, MESH_ERR_TRI_OVERFLOW, MESH_ERR_VERT_OVERFLOW, DeviceMesh,
-                     FluxEngine, _depth3d, _host_geo, _sp, default_capacity, make_trench_3d,
+                     FluxEngine, _depth3d, _sp, default_capacity, make_trench_3d,
                      mesh_scratch_bytes)
 
 MAX_BATCH = 64
@@ -263,7 +263,7 @@ class BatchEngine:
 
     def _record_depths(self):
         for b, x in enumerate(self.inst):
-            self.depth_history[b].append((self.steps_done, _depth3d(_host_geo(x.geo, x.phi))))
+            self.depth_history[b].append((self.steps_done, _depth3d(dict(x.geo, phi=x.phi))))
 
     def check(self):
         """Raise on device-side errors (mesh capacity, traversal limits) after a run."""
@@ -281,7 +281,7 @@ class BatchEngine:
 
     def depths(self):
         """Centre depth (_depth3d) of every instance now."""
-        return [_depth3d(_host_geo(x.geo, x.phi)) for x in self.inst]
+        return [_depth3d(dict(x.geo, phi=x.phi)) for x in self.inst]
 
     def phis(self):
         return [x.phi.double().cpu().numpy() for x in self.inst]

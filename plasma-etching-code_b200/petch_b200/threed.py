@@ -841,17 +841,16 @@ def run_etch_3d(Lx=10.0, Ly=4.0, Lz=14.0, dx=0.4, trench_width=4.0, mask_th=2.0,
         eng.end_step(warm and coupled and nt == "mc")
         st['nsub'] = nsub
         if record_depth_every and (step % record_depth_every == 0 or step == n_steps - 1):
-            g2 = _host_geo(geo, eng.phi)
-            geo.setdefault('depth_history', []).append((step + 1, _depth3d(g2)))
+            d_now = _depth3d(dict(geo, phi=eng.phi))
+            geo.setdefault('depth_history', []).append((step + 1, d_now))
             if record_frames:
                 jc = eng.shape[1] // 2
                 geo.setdefault('frames', []).append(
-                    dict(step=step + 1, t=(step + 1) / n_steps * t_end, depth=_depth3d(g2),
-                         phi_xz=g2['phi'][:, jc, :].copy()))
+                    dict(step=step + 1, t=(step + 1) / n_steps * t_end, depth=d_now,
+                         phi_xz=eng.phi[:, jc, :].double().cpu().numpy()))
         if verbose and step % 5 == 0:
-            g2 = _host_geo(geo, eng.phi)
-            print(f"  step {step:3d}/{n_steps}  faces {st['F']:5d}  depth ~ {_depth3d(g2):5.2f}  "
-                  f"Vmax {Vmax:.3f}")
+            print(f"  step {step:3d}/{n_steps}  faces {st['F']:5d}  "
+                  f"depth ~ {_depth3d(dict(geo, phi=eng.phi)):5.2f}  Vmax {Vmax:.3f}")
         if 'after_step' in hooks:
             hooks['after_step'](step, eng, st)
         step += 1
@@ -868,45 +867,63 @@ def run_etch_3d(Lx=10.0, Ly=4.0, Lz=14.0, dx=0.4, trench_width=4.0, mask_th=2.0,
     return geo
 
 
-def _host_geo(geo, phi_dev):
-    g = dict(geo)
-    g['phi'] = phi_dev.double().cpu().numpy()
-    return g
+# ---- depth metrics (threed.py:1798-1869) ----
+def _floor_indices(phi, ii, jj):
+    """For each column (ii[c], jj[c]) of phi: the index of the lowest cell of the gas run
+    (phi < 0) that reaches the top cell, -1 when the top cell is not gas (threed.py:1822-1830).
+    A device phi is scanned on the device (petch_column_floors) and only the indices come back;
+    a host phi is scanned with numpy."""
+    ii = np.asarray(ii, np.int64).ravel()
+    jj = np.asarray(jj, np.int64).ravel()
+    if isinstance(phi, torch.Tensor):
+        nx, ny, nz = phi.shape
+        if len(ii) == 0:
+            return np.zeros(0, np.int64)
+        src = phi if phi.dtype == torch.float32 else phi.float()
+        src = src.contiguous()
+        cols = torch.from_numpy(np.stack([ii, jj], axis=1).astype(np.int32)).to(src.device)
+        out = torch.empty(len(ii), dtype=torch.int32, device=src.device)
+        _lib.call("petch_column_floors", src.data_ptr(), nx, ny, nz, cols.data_ptr(), len(ii),
+                  out.data_ptr(), _sp())
+        k = out.cpu().numpy().astype(np.int64)
+        if (k == -2).any():
+            raise ValueError("depth metric: a column index lies outside the grid")
+        return k
+    phi = np.asarray(phi)
+    nz = phi.shape[2]
+    gas = phi[ii, jj, :] < 0
+    solid = ~gas
+    k = np.where(solid.any(axis=1), nz - np.argmax(solid[:, ::-1], axis=1), 0)
+    return np.where(gas[:, nz - 1], k, -1)
 
 
-# ---- depth metrics (threed.py:1798-1869): host post-processing of the final level set ----
-def _column_floor(phi, i, j):
-    col = phi[i, j, :] < 0
-    k = len(col) - 1
-    if not col[k]:
-        return None
-    while k > 0 and col[k - 1]:
-        k -= 1
-    return k
-
-
-def _depth3d(geo, half=1.0):
-    """center_depth_3d: sub_top - median floor over the central columns inside the opening."""
-    phi, xs, ys, zs = geo['phi'], geo['xs'], geo['ys'], geo['zs']
+def center_columns(geo, half=1.0):
+    """The columns (i, j) center_depth_3d samples: inside the opening, within `half` of the axis
+    (threed.py:1805-1820)."""
+    xs, ys = geo['xs'], geo['ys']
     cx, cy = geo['Lx'] / 2, geo['Ly'] / 2
     r_feat = geo.get('trench_width', 2.0) / 2.0 - geo['dx']
     hx = max(min(half, r_feat), geo['dx'])
     ic = np.where(np.abs(xs - cx) <= hx)[0]
     if geo.get('hole', False):
         jc = np.where(np.abs(ys - cy) <= hx)[0]
-        inside = lambda i, j: (xs[i] - cx) ** 2 + (ys[j] - cy) ** 2 <= r_feat ** 2  # noqa: E731
     else:
         jc = np.where(np.abs(ys - cy) <= half)[0]
-        inside = lambda i, j: True  # noqa: E731
-    floors = []
-    for i in ic:
-        for j in jc:
-            if not inside(i, j):
-                continue
-            k = _column_floor(phi, i, j)
-            if k is not None:
-                floors.append(zs[k])
-    if not floors:
+    I, J = np.meshgrid(ic, jc, indexing="ij")
+    I, J = I.ravel(), J.ravel()
+    if geo.get('hole', False):
+        keep = (xs[I] - cx) ** 2 + (ys[J] - cy) ** 2 <= r_feat ** 2
+        I, J = I[keep], J[keep]
+    return I, J
+
+
+def _depth3d(geo, half=1.0):
+    """center_depth_3d: sub_top - median floor over the central columns inside the opening.
+    geo['phi'] may be a host array or the engine's device level set."""
+    I, J = center_columns(geo, half)
+    k = _floor_indices(geo['phi'], I, J)
+    floors = geo['zs'][k[k >= 0]]
+    if floors.size == 0:
         return 0.0
     return float(geo['sub_top'] - np.median(floors))
 
@@ -922,16 +939,12 @@ def max_depth_3d(geo):
     r = geo.get('trench_width', 4.0) / 2.0
     if geo.get('hole', False):
         ii, jj = np.where((xs[:, None] - cx) ** 2 + (ys[None, :] - cy) ** 2 <= (r + geo['dx']) ** 2)
-        cols = list(zip(ii, jj))
     else:
         ix = np.where(np.abs(xs - cx) <= r + geo['dx'])[0]
-        cols = [(i, j) for i in ix for j in range(len(ys))]
-    floors = []
-    for i, j in cols:
-        k = _column_floor(phi, i, j)
-        if k is not None:
-            floors.append(zs[k])
-    if not floors:
+        ii, jj = np.meshgrid(ix, np.arange(len(ys)), indexing="ij")
+    k = _floor_indices(phi, ii, jj)
+    floors = zs[k[k >= 0]]
+    if floors.size == 0:
         return 0.0
     return float(geo['sub_top'] - np.percentile(floors, 5))
 
