@@ -522,8 +522,8 @@ def run_b200(args):
         per = np.mean(kms[dom_name]) / 1e3
         # algorithmic HBM bytes per launch: read the surface once (tracer triangles 48 B, BVH
         # node 64 B per leaf, leaf start 4 B, coverage 4 B per face) and write the tallies once
-        # (4 B per face for neutrals, 20 B for ions)
-        tally = 20 if dom_name == "k_ions" else 4
+        # (ions: 20 B per face; neutrals: both species of a round in one launch, 2 x 4 B)
+        tally = 20 if dom_name == "k_ions" else 8
         algo = F * (48 + 4 + tally) + F * (64 + 4)
         roof = {"kernel": dom_name, "bound": "hbm", "achieved": algo / per / 1e9, "peak": hbm,
                 "unit": "GB/s", "frac": (algo / per / 1e9) / hbm, "traffic": None,

@@ -168,6 +168,18 @@ int petch_trace_neutrals(const void* mesh, int max_tris, int max_verts, const pe
                          const float* bare, float beta, uint32_t seed, uint32_t stream_id,
                          int n_neu, float* flux, int* work, void* stream);
 
+/* Replaces the two _trace3d_cov_rr launches of one coverage round (petch/threed.py:898-902: the F
+ * species with betaE, the O species with betaO, on the same coverage) with ONE launch: rays
+ * [0, n_neu) follow petch_trace_neutrals with (beta_a, seed_a), rays [n_neu, 2 n_neu) with
+ * (beta_b, seed_b), both with stream_id; ray r of each species draws the same Philox stream as in
+ * the single-species call, so each flux equals that call's up to the order of float atomic
+ * additions (exactly, with deterministic tallies).  flux_a, flux_b: float[max_tris], distinct,
+ * zeroed first; n_neu <= 2^30. */
+int petch_trace_neutral_pair(const void* mesh, int max_tris, int max_verts,
+                             const petch_domain* dom, const float* bare, float beta_a,
+                             float beta_b, uint32_t seed_a, uint32_t seed_b, uint32_t stream_id,
+                             int n_neu, float* flux_a, float* flux_b, int* work, void* stream);
+
 /* Replaces _trace3d (petch/threed.py:352-406), the legacy species of mc_flux_3d and the
  * non-faithful ion of mc_flux_3d_coupled: first-hit / specular ions (ion = 1, source tilt sigma)
  * or neutrals with fixed sticking and n_reemit diffuse re-emissions; no lateral wrap. */

@@ -249,6 +249,37 @@ struct NeutralShader {
     }
 };
 
+// Both neutral species of one coverage round in one launch (threed.py:898-902: the F trace with
+// betaE and seed s_a, then the O trace with betaO and seed s_b, on the same coverage): rays
+// [0, n) are species a, rays [n, 2n) species b.  Ray r of a species draws the Philox stream of ray
+// r in the single-species launch with that species' seed, so each tally equals its own launch's
+// up to the order of float atomic additions (and exactly with deterministic tallies); one launch
+// has one tail instead of two.
+struct NeutralPairShader {
+    const float* bare;
+    float beta_a, beta_b;
+    float* flux_a;
+    float* flux_b;
+    uint32_t seed_b, domain;
+    int n;
+    int det;
+    static constexpr int kMaxBounce = 1024;
+    static constexpr int kMinBlocks = kTraceMinBlocksRR;
+    __device__ __forceinline__ int count(const MeshView&, int n2) const { return n2; }
+    __device__ __forceinline__ void init(Rng& g, const Tracer&, const Domain& D, int ray, float3& o,
+                                         float3& d, RayState& s) const {
+        if (ray >= n) g.init(seed_b, domain, (uint32_t)(ray - n));
+        source(g, false, 0.0f, D, o, d);
+        s.w = 1.0f;
+    }
+    __device__ __forceinline__ bool hit(Rng& g, const Tracer& T, int f, float t, float3& o,
+                                        float3& d, RayState& s) const {
+        const bool b = s.id >= n;
+        return neutral_hit(bare, b ? beta_b : beta_a, b ? flux_b : flux_a, g, T, f, t, o, d, s,
+                           det);
+    }
+};
+
 // The electron trace of the electron-shadowing charging model (threed.py:847-857):
 // _trace3d_cov_rr with bare = 1 and beta = 1 on rays from the ion-type (Gaussian angle, sigma =
 // e_ang_sigma) source, so every electron sticks where it first lands and deposits weight 1; the
@@ -1174,6 +1205,40 @@ extern "C" int petch_trace_neutrals(const void* mesh, int max_tris, int max_vert
                           "k_trace<neutrals>");
     if (rc) return rc;
     PETCH_DET_CONVERT(a_f, flux, (long long)max_tris);
+    return PETCH_OK;
+}
+
+extern "C" int petch_trace_neutral_pair(const void* mesh, int max_tris, int max_verts,
+                                        const petch_domain* dom, const float* bare, float beta_a,
+                                        float beta_b, uint32_t seed_a, uint32_t seed_b,
+                                        uint32_t stream_id, int n_neu, float* flux_a,
+                                        float* flux_b, int* work, void* stream) {
+    PETCH_REQUIRE(mesh && dom && flux_a && flux_b && work, "petch_trace_neutral_pair: null pointer");
+    PETCH_REQUIRE(flux_a != flux_b, "petch_trace_neutral_pair: flux_a and flux_b must differ");
+    PETCH_REQUIRE(n_neu >= 0 && n_neu <= (1 << 30) && max_tris > 0 && max_verts > 0,
+                  "petch_trace_neutral_pair: bad size");
+    cudaStream_t st = as_stream(stream);
+    MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
+    const uint32_t domain = 0x6e657500u ^ stream_id;
+    NeutralPairShader sh{bare, beta_a, beta_b, flux_a, flux_b, seed_b, domain, n_neu, 0};
+    k_zero_faces<<<grid_for(max_tris, 256), 256, 0, st>>>(m.hdr, max_tris, flux_a, 1, flux_b, 1);
+    PETCH_LAUNCH_CHECK("k_zero_faces");
+    PETCH_CUDA(cudaMemsetAsync(work, 0, sizeof(int), st), "reset ray counter");
+    if (n_neu == 0) return PETCH_OK;
+    DetArena arena;
+    if (!arena.on())
+        return launch_trace(m, to_domain(dom), sh, seed_a, domain, 2 * n_neu, work, st,
+                            "k_trace<neutral pair>");
+    PETCH_DET_TAKE(a_a, (long long)max_tris);
+    PETCH_DET_TAKE(a_b, (long long)max_tris);
+    sh.flux_a = reinterpret_cast<float*>(a_a);
+    sh.flux_b = reinterpret_cast<float*>(a_b);
+    sh.det = 1;
+    int rc = launch_trace(m, to_domain(dom), sh, seed_a, domain, 2 * n_neu, work, st,
+                          "k_trace<neutral pair>");
+    if (rc) return rc;
+    PETCH_DET_CONVERT(a_a, flux_a, (long long)max_tris);
+    PETCH_DET_CONVERT(a_b, flux_b, (long long)max_tris);
     return PETCH_OK;
 }
 

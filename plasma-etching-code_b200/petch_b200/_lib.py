@@ -90,6 +90,7 @@ SIGNATURES = {
     "petch_trace_neutrals": [P, I, I, DP, P, F, U, U, I, P, P, P],
     "petch_trace_legacy": [P, I, I, DP, I, F, F, I, I, F, F, U, I, P, P, P, P],
     "petch_trace_electrons": [P, I, I, DP, F, U, I, P, P, P],
+    "petch_trace_neutral_pair": [P, I, I, DP, P, F, F, U, U, U, I, P, P, P, P],
     "petch_extend_velocity": [P, I, I, P, P, I, I, I, D, D, P, P, I, P, P, I, P, P],
     "petch_warmstart": [P, I, I, P, P, I, I, P, P, P],
     "petch_norm_smooth": [P, I, I, P, F, F, F, I, I, F, P, P, P, P],

@@ -309,15 +309,17 @@ class FluxEngine:
         if not seeded:
             self.bare.fill_(1.0)
         betaE, betaO = float(par.get('betaE', 0.7)), float(par.get('betaO', 1.0))
+        flux_o = self.tmp5[2 * m.MT:3 * m.MT]
         for it in range(n_fp):
-            for beta, out, sd in ((betaE, self.m_F, seed * 9 + 2 + 2 * it),
-                                  (betaO, self.m_O, seed * 9 + 3 + 2 * it)):
-                self.ktimer.start("k_neutrals")
-                _lib.call("petch_trace_neutrals", m.id, m.MT, m.MV, ctypes.byref(self.dom),
-                          self.bare.data_ptr(), beta, int(sd) & 0xffffffff, 0, int(n_neu),
-                          self.flux.data_ptr(), work.data_ptr(), s)
-                self.ktimer.stop("k_neutrals")
-                _lib.call("petch_norm_smooth", m.id, m.MT, m.MV, self.flux.data_ptr(),
+            # both species of the round in one launch (F: betaE, seed*9+2+2it; O: betaO, +3+2it)
+            self.ktimer.start("k_neutrals")
+            _lib.call("petch_trace_neutral_pair", m.id, m.MT, m.MV, ctypes.byref(self.dom),
+                      self.bare.data_ptr(), betaE, betaO, int(seed * 9 + 2 + 2 * it) & 0xffffffff,
+                      int(seed * 9 + 3 + 2 * it) & 0xffffffff, 0, int(n_neu),
+                      self.flux.data_ptr(), flux_o.data_ptr(), work.data_ptr(), s)
+            self.ktimer.stop("k_neutrals")
+            for fl, out in ((self.flux, self.m_F), (flux_o, self.m_O)):
+                _lib.call("petch_norm_smooth", m.id, m.MT, m.MV, fl.data_ptr(),
                           float(A_src / n_neu), 0.0, 8.0, 1, n_smooth, alpha, out.data_ptr(),
                           self.tmp5.data_ptr(), self.tmp5[m.MT:].data_ptr(), s)
             _lib.call("petch_belen_bare", m.id, m.MT, m.MV, ctypes.byref(self.chem),

@@ -157,3 +157,56 @@ def test_replay_same_seed_same_paths():
     c = cuda_neutrals(m, geo, None, 0.7, 4, 200_000)
     np.testing.assert_allclose(a, b, rtol=1e-5, atol=1e-3)
     assert np.abs(a - c).max() > 1.0
+
+
+@pytest.mark.parametrize("hole", [True, False])
+def test_neutral_pair_equals_two_single_launches(hole):
+    """petch_trace_neutral_pair (both species of a coverage round in one launch) gives each
+    species exactly the tally of its own petch_trace_neutrals launch with deterministic tallies
+    (same Philox paths), and the same up to float summation order without them."""
+    from petch_b200 import _lib
+    phi, geo = small_feature(hole)
+    m = cuda_mesh(phi, geo['dx'], geo)
+    rng = np.random.default_rng(2)
+    bare = torch.from_numpy(rng.uniform(0.1, 1.0, m.MT).astype(np.float32)).cuda()
+    n = 300_000
+    dom = domain(geo)
+
+    def single(beta, seed):
+        flux = torch.zeros(m.MT, device="cuda")
+        work = torch.zeros(6, dtype=torch.int32, device="cuda")
+        _lib.call("petch_trace_neutrals", m.id, m.MT, m.MV, ctypes.byref(dom), bare.data_ptr(),
+                  beta, seed, 0, n, flux.data_ptr(), work.data_ptr(), stream())
+        assert work[1].item() == 0
+        return flux[:m.F].cpu().numpy()
+
+    def pair(count=n):
+        fa = torch.full((m.MT,), 5.0, device="cuda")
+        fb = torch.full((m.MT,), 5.0, device="cuda")
+        work = torch.zeros(6, dtype=torch.int32, device="cuda")
+        _lib.call("petch_trace_neutral_pair", m.id, m.MT, m.MV, ctypes.byref(dom),
+                  bare.data_ptr(), 0.7, 1.0, 11, 12, 0, count, fa.data_ptr(), fb.data_ptr(),
+                  work.data_ptr(), stream())
+        assert work[1].item() == 0
+        return fa[:m.F].cpu().numpy(), fb[:m.F].cpu().numpy()
+
+    _lib.set_deterministic(64 << 20)
+    try:
+        a, b = single(0.7, 11), single(1.0, 12)
+        pa, pb = pair()
+    finally:
+        _lib.set_deterministic(0)
+    np.testing.assert_array_equal(pa, a)
+    np.testing.assert_array_equal(pb, b)
+    assert np.abs(a - b).max() > 1.0                      # two different species
+    qa, qb = pair()
+    np.testing.assert_allclose(qa, a, rtol=1e-5, atol=1e-3)
+    np.testing.assert_allclose(qb, b, rtol=1e-5, atol=1e-3)
+    za, zb = pair(0)
+    assert za.max() == 0.0 and zb.max() == 0.0
+    with pytest.raises(_lib.PetchError, match="must differ"):
+        f = torch.zeros(m.MT, device="cuda")
+        _lib.call("petch_trace_neutral_pair", m.id, m.MT, m.MV, ctypes.byref(dom), None, 0.7, 1.0,
+                  1, 2, 0, 10, f.data_ptr(), f.data_ptr(), torch.zeros(6, dtype=torch.int32,
+                                                                    device="cuda").data_ptr(),
+                  stream())
