@@ -22,14 +22,21 @@ constexpr int kTB = 128;
 #define PETCH_TRACE_MIN_BLOCKS 8
 #endif
 #ifndef PETCH_TRACE_MIN_BLOCKS_RR
-#define PETCH_TRACE_MIN_BLOCKS_RR 10
+#define PETCH_TRACE_MIN_BLOCKS_RR 12
 #endif
-// Resident blocks of the persistent tracers per SM: 8 x 4 warps (<= 64 registers per thread) for
-// the ion shaders, 10 x 4 (<= 48 registers) for the Russian-roulette neutral shaders, whose
-// traversal-bound loop gains more from the extra warps than it loses to spills (a sweep on the
-// trench workload: neutrals -6 % time at 10, ions +10 % at 10).
+#ifndef PETCH_TRACE_MIN_BLOCKS_RR_TAN
+#define PETCH_TRACE_MIN_BLOCKS_RR_TAN 10
+#endif
+// Resident blocks of the persistent tracers per SM (the binary-traversal launches use no shared
+// memory, so registers alone set them): 8 x 4 warps (<= 64 registers per thread) for the ion
+// shaders; 12 x 4 (<= 40 registers) for the single-instance Russian-roulette neutral shaders,
+// whose traversal-bound loop gains more from the extra warps than it loses to spills (trench
+// workload: 10 -> 12 blocks 1.8 % faster, 16 blocks at 32 registers 12 % slower); 10 x 4
+// (<= 48 registers) for the neutral tangent shader and the batched neutral kinds, which carry
+// more per-ray state.
 constexpr int kTraceMinBlocks = PETCH_TRACE_MIN_BLOCKS;
 constexpr int kTraceMinBlocksRR = PETCH_TRACE_MIN_BLOCKS_RR;
+constexpr int kTraceMinBlocksRRTan = PETCH_TRACE_MIN_BLOCKS_RR_TAN;
 constexpr long long kMaxRounds = 1LL << 24;   // per-warp bound on tracer rounds (error bit 4)
 constexpr unsigned kFull = 0xffffffffu;
 
@@ -500,7 +507,7 @@ struct NeutralTanShader {
     float* dflux;           // [3][MT]
     int det;
     static constexpr int kMaxBounce = 1024;
-    static constexpr int kMinBlocks = kTraceMinBlocksRR;
+    static constexpr int kMinBlocks = kTraceMinBlocksRRTan;
     __device__ __forceinline__ int count(const MeshView&, int n) const { return n; }
     __device__ __forceinline__ void init(Rng& g, const Tracer&, const Domain& D, int, float3& o,
                                          float3& d, RayState& s) const {
@@ -787,7 +794,7 @@ __global__ void k_zero_batch(BatchTable tab, MeshOffsets L, int MT, int MV, int 
 // KIND: 0 ions, 1 neutrals, 2 ions with energy tangents, 3 neutrals with weight tangents (the
 // single-instance tangent shaders' hit functions, outputs per instance from tab.tn).
 template <int KIND>
-__global__ void __launch_bounds__(kTB, (KIND & 1) ? kTraceMinBlocksRR : kTraceMinBlocks) k_trace_batch(BatchTable tab, MeshOffsets L,
+__global__ void __launch_bounds__(kTB, (KIND & 1) ? kTraceMinBlocksRRTan : kTraceMinBlocks) k_trace_batch(BatchTable tab, MeshOffsets L,
                                                                      int MT, int MV, float beta,
                                                                      const int* step,
                                                                      uint32_t seed_mul,
@@ -1125,7 +1132,9 @@ static int launch_trace(const MeshView& m, const Domain& D, const S& sh, uint32_
                         uint32_t domain, int n, int* work, cudaStream_t st, const char* what) {
     const int steps = g_steps, keep = g_keep;
     if (g_bvh_width == 2) {
-        k_trace<S, false><<<persistent_blocks((const void*)k_trace<S, false>, kTB), kTB, kSmemBytes, st>>>(
+        // binary traversal reads no tree from shared memory: launching without the 12 KB of the
+        // wide tree's top leaves the L1 / shared split and the resident blocks to the registers
+        k_trace<S, false><<<persistent_blocks((const void*)k_trace<S, false>, kTB, 0), kTB, 0, st>>>(
             m, D, sh, seed, domain, n, steps, keep, work);
     } else {
         k_trace<S, true><<<persistent_blocks((const void*)k_trace<S, true>, kTB), kTB, kSmemBytes, st>>>(
@@ -1291,11 +1300,13 @@ extern "C" int petch_prepare_device(void) {
     persistent_blocks((const void*)k_trace_batch<1>, kTB, 0);
     persistent_blocks((const void*)k_trace_batch<2>, kTB, 0);
     persistent_blocks((const void*)k_trace_batch<3>, kTB, 0);
-    persistent_blocks((const void*)k_trace<IonShader, false>, kTB);
-    persistent_blocks((const void*)k_trace<NeutralShader, false>, kTB);
-    persistent_blocks((const void*)k_trace<LegacyShader, false>, kTB);
-    persistent_blocks((const void*)k_trace<FormFactorShader, false>, kTB);
-    persistent_blocks((const void*)k_trace<RedepShader, false>, kTB);
+    persistent_blocks((const void*)k_trace<IonShader, false>, kTB, 0);
+    persistent_blocks((const void*)k_trace<NeutralShader, false>, kTB, 0);
+    persistent_blocks((const void*)k_trace<NeutralPairShader, false>, kTB, 0);
+    persistent_blocks((const void*)k_trace<ElectronShader, false>, kTB, 0);
+    persistent_blocks((const void*)k_trace<LegacyShader, false>, kTB, 0);
+    persistent_blocks((const void*)k_trace<FormFactorShader, false>, kTB, 0);
+    persistent_blocks((const void*)k_trace<RedepShader, false>, kTB, 0);
     PETCH_CUDA(cudaGetLastError(), "petch_prepare_device");
     return PETCH_OK;
 }
