@@ -359,6 +359,15 @@ int petch_trace_batch(int kind, const petch_batch_item* items, int B, int max_tr
                       float beta, const int* step, uint32_t seed_mul, uint32_t seed_add,
                       int* work, void* stream);
 
+/* petch_trace_batch for both neutral species of a coverage round in ONE launch (the batched
+ * counterpart of petch_trace_neutral_pair): item b's rays [0, n_rays) follow kind 1 with beta_a
+ * and seed_add_a into items[b].out, rays [n_rays, 2 n_rays) with beta_b and seed_add_b into
+ * items[b].ang (the second flux, float[max_tris], distinct from out); each species' ray r draws
+ * the Philox stream of ray r of its own kind-1 launch.  n_rays <= 2^29 per item. */
+int petch_trace_batch_pair(const petch_batch_item* items, int B, int max_tris, int max_verts,
+                           float beta_a, float beta_b, const int* step, uint32_t seed_mul,
+                           uint32_t seed_add_a, uint32_t seed_add_b, int* work, void* stream);
+
 /* Tangent outputs of one instance for petch_trace_batch_tangent: dout = d(sputter, ion-enhanced,
  * passivation tallies) / d(mean ion energy) [3][max_tris] (kind 0) or d(flux) [3][max_tris] along
  * the three recipe directions (kind 1); dbare = the coverage tangents [3][max_tris] (kind 1; NULL
@@ -374,6 +383,17 @@ int petch_trace_batch_tangent(int kind, const petch_batch_item* items,
                               const petch_batch_tangent* tans, int B, int max_tris, int max_verts,
                               float beta, const int* step, uint32_t seed_mul, uint32_t seed_add,
                               int* work, void* stream);
+
+/* petch_trace_batch_pair with the weight tangents of petch_trace_batch_tangent kind 1: item b's
+ * rays [0, n_rays) (beta_a, seed_add_a) deposit into items[b].out and tans_a[b].dout, rays
+ * [n_rays, 2 n_rays) (beta_b, seed_add_b) into items[b].ang and tans_b[b].dout; tans_a[b].dbare
+ * is the coverage tangent both species read (tans_b[b].dbare is not read). */
+int petch_trace_batch_pair_tangent(const petch_batch_item* items,
+                                   const petch_batch_tangent* tans_a,
+                                   const petch_batch_tangent* tans_b, int B, int max_tris,
+                                   int max_verts, float beta_a, float beta_b, const int* step,
+                                   uint32_t seed_mul, uint32_t seed_add_a, uint32_t seed_add_b,
+                                   int* work, void* stream);
 
 /* One instance's level-set state for the batched stages. */
 typedef struct petch_batch_grid {
@@ -632,6 +652,18 @@ int petch_trace_neutrals_tangent(const void* mesh, int max_tris, int max_verts,
                                  const petch_domain* dom, const float* bare, const float* dbare,
                                  float beta, uint32_t seed, uint32_t stream_id, int n_neu,
                                  float* flux, float* dflux, int* work, void* stream);
+
+/* petch_trace_neutral_pair with the weight tangents of petch_trace_neutrals_tangent: both
+ * species of a coverage round in one launch (rays [0, n_neu): beta_a, seed_a into flux_a /
+ * dflux_a; rays [n_neu, 2 n_neu): beta_b, seed_b into flux_b / dflux_b), each equal to its own
+ * tangent launch up to the order of float atomic additions (exactly, with deterministic tallies).
+ * dbare, dflux_*: [3][max_tris]; outputs zeroed first; n_neu <= 2^30. */
+int petch_trace_neutral_pair_tangent(const void* mesh, int max_tris, int max_verts,
+                                     const petch_domain* dom, const float* bare,
+                                     const float* dbare, float beta_a, float beta_b,
+                                     uint32_t seed_a, uint32_t seed_b, uint32_t stream_id,
+                                     int n_neu, float* flux_a, float* dflux_a, float* flux_b,
+                                     float* dflux_b, int* work, void* stream);
 
 /* Tangent of petch_norm_smooth (blend_last_only = 0) or of petch_ion_post's smoothing
  * (blend_last_only = 1, clip = 0): dout[3][max_tris] from dfl[3][max_tris] (fl: the primal

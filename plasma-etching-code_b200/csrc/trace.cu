@@ -31,9 +31,9 @@ constexpr int kTB = 128;
 // memory, so registers alone set them): 8 x 4 warps (<= 64 registers per thread) for the ion
 // shaders; 12 x 4 (<= 40 registers) for the single-instance Russian-roulette neutral shaders,
 // whose traversal-bound loop gains more from the extra warps than it loses to spills (trench
-// workload: 10 -> 12 blocks 1.8 % faster, 16 blocks at 32 registers 12 % slower); 10 x 4
-// (<= 48 registers) for the neutral tangent shader and the batched neutral kinds, which carry
-// more per-ray state.
+// workload: 10 -> 12 blocks 1.8 % faster, 16 blocks at 32 registers 12 % slower) and the batched
+// neutral kinds (64 ragged holes: +1.7 %); 10 x 4 (<= 48 registers) for the neutral tangent
+// shaders, which carry three weight tangents per ray.
 constexpr int kTraceMinBlocks = PETCH_TRACE_MIN_BLOCKS;
 constexpr int kTraceMinBlocksRR = PETCH_TRACE_MIN_BLOCKS_RR;
 constexpr int kTraceMinBlocksRRTan = PETCH_TRACE_MIN_BLOCKS_RR_TAN;
@@ -521,6 +521,37 @@ struct NeutralTanShader {
     }
 };
 
+// NeutralPairShader with weight tangents: both species of a coverage round in one launch, each
+// carrying d(weight) / d(theta) along its path (the species' own beta scales dbare).
+struct NeutralTanPairShader {
+    const float* bare;
+    const float* dbare;     // [3][MT]
+    float beta_a, beta_b;
+    float* flux_a;
+    float* dflux_a;         // [3][MT]
+    float* flux_b;
+    float* dflux_b;         // [3][MT]
+    uint32_t seed_b, domain;
+    int n;
+    int det;
+    static constexpr int kMaxBounce = 1024;
+    static constexpr int kMinBlocks = kTraceMinBlocksRRTan;
+    __device__ __forceinline__ int count(const MeshView&, int n2) const { return n2; }
+    __device__ __forceinline__ void init(Rng& g, const Tracer&, const Domain& D, int ray, float3& o,
+                                         float3& d, RayState& s) const {
+        if (ray >= n) g.init(seed_b, domain, (uint32_t)(ray - n));
+        source(g, false, 0.0f, D, o, d);
+        s.w = 1.0f;
+        s.dw[0] = s.dw[1] = s.dw[2] = 0.0f;
+    }
+    __device__ __forceinline__ bool hit(Rng& g, const Tracer& T, int f, float t, float3& o,
+                                        float3& d, RayState& s) const {
+        const bool b = s.id >= n;
+        return neutral_hit_tan(bare, dbare, b ? beta_b : beta_a, b ? flux_b : flux_a,
+                               b ? dflux_b : dflux_a, g, T, f, t, o, d, s, det);
+    }
+};
+
 // _trace_ff + the emission of mc_flux_3d_radiosity (threed.py:908-920, 947-956): ray p leaves
 // face j = p / n_ff from centroid + 1e-3 * n_gas in a cosine direction about the into-gas normal
 // (the tangent frame of _cosine_dirs, threed.py:1571-1579); its first hit face is recorded (the
@@ -714,8 +745,8 @@ __global__ void __launch_bounds__(kTB, S::kMinBlocks) k_trace(MeshView m, Domain
 // domain, ion parameters and output tallies.  Rays are drawn from ONE global queue; ray r of
 // instance b has the Philox key ((step + seed_b) * seed_mul + seed_add, domain) and counter r,
 // exactly the stream the single-instance launch gives it, so a batched step reproduces the
-// per-instance steps' paths.  The instance table is a kernel parameter copied into shared memory;
-// each lane resolves its ray's instance when it takes the ray.
+// per-instance steps' paths.  The instance table is a kernel parameter, read from the parameter
+// space; each lane resolves its ray's instance when it takes the ray.
 // ---------------------------------------------------------------------------------------------
 constexpr int kMaxBatch = 64;
 
@@ -740,6 +771,7 @@ struct BatchTan {
 struct BatchTable {
     BatchItem it[kMaxBatch];
     BatchTan tn[kMaxBatch];
+    float* dout2[kMaxBatch];   // kind 5: the second species' weight tangents [3][MT]
     int B;
     int total;
 };
@@ -789,30 +821,33 @@ __global__ void k_zero_batch(BatchTable tab, MeshOffsets L, int MT, int MV, int 
     if (tan)
         for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < F; i += gridDim.x * blockDim.x)
             for (int k = 0; k < 3; ++k) tab.tn[b].dout[i + (long long)k * MT] = 0.0f;
+    if (tab.dout2[b])
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < F; i += gridDim.x * blockDim.x)
+            for (int k = 0; k < 3; ++k) tab.dout2[b][i + (long long)k * MT] = 0.0f;
 }
 
 // KIND: 0 ions, 1 neutrals, 2 ions with energy tangents, 3 neutrals with weight tangents (the
-// single-instance tangent shaders' hit functions, outputs per instance from tab.tn).
+// single-instance tangent shaders' hit functions, outputs per instance from tab.tn), 4 both
+// neutral species of a coverage round: an item's rays [0, n) follow kind 1 with (beta, seed_add)
+// into out, rays [n, 2n) with (beta2, seed_add2) into ang, each species' ray r on the Philox
+// stream of ray r of its own kind-1 launch; 5 the same with the weight tangents of kind 3 (the
+// second species' into dout2).
 template <int KIND>
-__global__ void __launch_bounds__(kTB, (KIND & 1) ? kTraceMinBlocksRRTan : kTraceMinBlocks) k_trace_batch(BatchTable tab, MeshOffsets L,
-                                                                     int MT, int MV, float beta,
-                                                                     const int* step,
-                                                                     uint32_t seed_mul,
-                                                                     uint32_t seed_add,
-                                                                     uint32_t domain, int steps,
-                                                                     int keep, int det, int* work) {
+__global__ void __launch_bounds__(kTB, (KIND == 1 || KIND == 4) ? kTraceMinBlocksRR
+                                    : ((KIND == 3 || KIND == 5) ? kTraceMinBlocksRRTan
+                                                                : kTraceMinBlocks))
+k_trace_batch(BatchTable tab, MeshOffsets L, int MT, int MV, float beta, float beta2,
+              const int* step, uint32_t seed_mul, uint32_t seed_add, uint32_t seed_add2,
+              uint32_t domain, int steps, int keep, int det, int* work) {
     constexpr bool ION = KIND == 0 || KIND == 2;
-    constexpr bool TAN = KIND >= 2;
-    __shared__ BatchItem s_it[kMaxBatch];
-    __shared__ BatchTan s_tn[kMaxBatch];
-    __shared__ int s_start[kMaxBatch + 1];
-    for (int i = threadIdx.x; i < tab.B; i += blockDim.x) {
-        s_it[i] = tab.it[i];
-        s_tn[i] = tab.tn[i];
-        s_start[i] = tab.it[i].ray_start;
-    }
-    if (threadIdx.x == 0) s_start[tab.B] = tab.total;
-    __syncthreads();
+    constexpr bool TAN = KIND == 2 || KIND == 3 || KIND == 5;
+    constexpr bool PAIR = KIND == 4 || KIND == 5;
+    // The instance table is read where it lies, in the kernel's parameter space: a warp's lanes
+    // mostly hold rays of one instance (the queue hands out consecutive ray ids), so the reads are
+    // near-uniform, and no shared memory is taken from the L1.
+    const BatchItem* s_it = tab.it;
+    const BatchTan* s_tn = tab.tn;
+    auto s_start = [&](int i) { return i < tab.B ? tab.it[i].ray_start : tab.total; };
     const int n = tab.total;
     const uint32_t stepv = step ? (uint32_t)*step : 0u;
     int st_ref[kWStack];
@@ -839,15 +874,23 @@ __global__ void __launch_bounds__(kTB, (KIND & 1) ? kTraceMinBlocksRRTan : kTrac
             int lo = 0, hi = tab.B - 1;           // last instance whose range starts at or before ray
             while (lo < hi) {
                 const int mid = (lo + hi + 1) >> 1;
-                if (s_start[mid] <= ray) lo = mid;
+                if (s_start(mid) <= ray) lo = mid;
                 else hi = mid - 1;
             }
             inst = lo;
             const BatchItem& it = s_it[inst];
             T.m = view_at(it.mesh, L, MT, MV);
             T.L = min(T.m.hdr[HDR_L], MT);
-            const uint32_t local = (uint32_t)(ray - it.ray_start);
-            g.init((stepv + it.seed) * seed_mul + seed_add, domain, local);
+            uint32_t local = (uint32_t)(ray - it.ray_start);
+            uint32_t sadd = seed_add;
+            if (PAIR) {
+                const uint32_t nb = (uint32_t)(s_start(inst + 1) - it.ray_start) >> 1;
+                if (local >= nb) {
+                    local -= nb;
+                    sadd = seed_add2;
+                }
+            }
+            g.init((stepv + it.seed) * seed_mul + sadd, domain, local);
             float3 o, d;
             if (ION) {
                 source(g, true, it.P.sigma, it.D, o, d);
@@ -890,7 +933,19 @@ __global__ void __launch_bounds__(kTB, (KIND & 1) ? kTraceMinBlocksRRTan : kTrac
                 else if (KIND == 2)
                     cont = ion_hit<true>(it.P, reinterpret_cast<float4*>(it.out), it.ang, g, T,
                                          q.f, q.t, o, d, rs, det, s_tn[inst].dout);
-                else
+                else if (KIND == 4) {
+                    const int nb = (s_start(inst + 1) - it.ray_start) >> 1;
+                    const bool second = rs.id - it.ray_start >= nb;
+                    cont = neutral_hit(it.bare, second ? beta2 : beta, second ? it.ang : it.out,
+                                       g, T, q.f, q.t, o, d, rs, det);
+                } else if (KIND == 5) {
+                    const int nb = (s_start(inst + 1) - it.ray_start) >> 1;
+                    const bool second = rs.id - it.ray_start >= nb;
+                    cont = neutral_hit_tan(it.bare, s_tn[inst].dbare, second ? beta2 : beta,
+                                           second ? it.ang : it.out,
+                                           second ? tab.dout2[inst] : s_tn[inst].dout, g, T, q.f,
+                                           q.t, o, d, rs, det);
+                } else
                     cont = neutral_hit_tan(it.bare, s_tn[inst].dbare, beta, it.out,
                                            s_tn[inst].dout, g, T, q.f, q.t, o, d, rs, det);
                 rs.wraps = 0;
@@ -1300,6 +1355,8 @@ extern "C" int petch_prepare_device(void) {
     persistent_blocks((const void*)k_trace_batch<1>, kTB, 0);
     persistent_blocks((const void*)k_trace_batch<2>, kTB, 0);
     persistent_blocks((const void*)k_trace_batch<3>, kTB, 0);
+    persistent_blocks((const void*)k_trace_batch<4>, kTB, 0);
+    persistent_blocks((const void*)k_trace_batch<5>, kTB, 0);
     persistent_blocks((const void*)k_trace<IonShader, false>, kTB, 0);
     persistent_blocks((const void*)k_trace<NeutralShader, false>, kTB, 0);
     persistent_blocks((const void*)k_trace<NeutralPairShader, false>, kTB, 0);
@@ -1315,21 +1372,26 @@ namespace {
 
 template <int KIND>
 void launch_batch(const BatchTable& tab, const MeshOffsets& L, int max_tris, int max_verts,
-                  float beta, const int* step, uint32_t seed_mul, uint32_t seed_add,
-                  uint32_t domain, int det, int* work, cudaStream_t st) {
+                  float beta, float beta2, const int* step, uint32_t seed_mul, uint32_t seed_add,
+                  uint32_t seed_add2, uint32_t domain, int det, int* work, cudaStream_t st) {
     k_trace_batch<KIND><<<persistent_blocks((const void*)k_trace_batch<KIND>, kTB, 0), kTB, 0, st>>>(
-        tab, L, max_tris, max_verts, beta, step, seed_mul, seed_add, domain, g_steps, g_keep, det,
-        work);
+        tab, L, max_tris, max_verts, beta, beta2, step, seed_mul, seed_add, seed_add2, domain,
+        g_steps, g_keep, det, work);
 }
 
-// kind: 0 ions, 1 neutrals, 2 ions with energy tangents, 3 neutrals with weight tangents.
+// kind: 0 ions, 1 neutrals, 2 ions with energy tangents, 3 neutrals with weight tangents,
+// 4 both neutral species of a round (the second species' flux in the item's ang), 5 kind 4 with
+// weight tangents (the second species' in tans2[b].dout).
 int trace_batch(int kind, const petch_batch_item* items, const petch_batch_tangent* tans, int B,
-                int max_tris, int max_verts, float beta, const int* step, uint32_t seed_mul,
-                uint32_t seed_add, int* work, void* stream, const char* who) {
+                int max_tris, int max_verts, float beta, float beta2, const int* step,
+                uint32_t seed_mul, uint32_t seed_add, uint32_t seed_add2, int* work, void* stream,
+                const char* who, const petch_batch_tangent* tans2 = nullptr) {
     PETCH_REQUIRE(items && work, "%s: null pointer", who);
     PETCH_REQUIRE(B >= 1 && B <= kMaxBatch, "%s: 1 <= B <= %d", who, kMaxBatch);
     PETCH_REQUIRE(max_tris > 0 && max_verts > 0, "%s: bad capacities", who);
-    const bool ion = kind == 0 || kind == 2, tan = kind >= 2;
+    const bool ion = kind == 0 || kind == 2, tan = kind == 2 || kind == 3 || kind == 5;
+    const bool pair = kind == 4 || kind == 5;
+    PETCH_REQUIRE(kind != 5 || tans2, "%s: null second tangent table", who);
     PETCH_REQUIRE(!tan || tans, "%s: null tangent table", who);
     BatchTable tab;
     long long total = 0;
@@ -1338,6 +1400,8 @@ int trace_batch(int kind, const petch_batch_item* items, const petch_batch_tange
         PETCH_REQUIRE(x.mesh && x.out && x.n_rays >= 0, "%s: item %d incomplete", who, b);
         PETCH_REQUIRE(!ion || (x.ang && ((uintptr_t)x.out & 15) == 0),
                       "%s: ion item %d needs ang and a 16-byte aligned tally", who, b);
+        PETCH_REQUIRE(!pair || (x.ang && x.ang != x.out && x.n_rays <= (1 << 29)),
+                      "%s: pair item %d needs a second flux (ang) and n_rays <= 2^29", who, b);
         BatchItem& it = tab.it[b];
         it.mesh = (const char*)x.mesh;
         it.D = to_domain(&x.dom);
@@ -1346,17 +1410,23 @@ int trace_batch(int kind, const petch_batch_item* items, const petch_batch_tange
                     p.inflect, p.minang, p.n_l, p.A_en, p.minE, p.thrmin, p.thrmax, p.sigma};
         it.bare = x.bare;
         it.out = x.out;
-        it.ang = ion ? x.ang : nullptr;
+        it.ang = (ion || pair) ? x.ang : nullptr;
         it.ray_start = (int)total;
         it.seed = x.seed;
         tab.tn[b].dout = nullptr;
         tab.tn[b].dbare = nullptr;
+        tab.dout2[b] = nullptr;
         if (tan) {
             PETCH_REQUIRE(tans[b].dout, "%s: tangent item %d has no output", who, b);
             tab.tn[b].dout = tans[b].dout;
             tab.tn[b].dbare = ion ? nullptr : tans[b].dbare;
         }
-        total += x.n_rays;
+        if (kind == 5) {
+            PETCH_REQUIRE(tans2[b].dout && tans2[b].dout != tans[b].dout,
+                          "%s: item %d needs a distinct second tangent output", who, b);
+            tab.dout2[b] = tans2[b].dout;
+        }
+        total += pair ? 2LL * x.n_rays : (long long)x.n_rays;
     }
     PETCH_REQUIRE(total < (1LL << 31), "%s: more than 2^31 - 1 rays", who);
     tab.B = B;
@@ -1377,12 +1447,13 @@ int trace_batch(int kind, const petch_batch_item* items, const petch_batch_tange
     long long* acc_out[kMaxBatch] = {};
     long long* acc_ang[kMaxBatch] = {};
     long long* acc_d[kMaxBatch] = {};
+    long long* acc_d2[kMaxBatch] = {};
     if (det) {
         for (int b = 0; b < B; ++b) {
             PETCH_DET_TAKE(ao, per_out);
             acc_out[b] = ao;
             tab.it[b].out = reinterpret_cast<float*>(ao);
-            if (ion) {
+            if (ion || pair) {
                 PETCH_DET_TAKE(aa, (long long)max_tris);
                 acc_ang[b] = aa;
                 tab.it[b].ang = reinterpret_cast<float*>(aa);
@@ -1392,20 +1463,32 @@ int trace_batch(int kind, const petch_batch_item* items, const petch_batch_tange
                 acc_d[b] = ad;
                 tab.tn[b].dout = reinterpret_cast<float*>(ad);
             }
+            if (kind == 5) {
+                PETCH_DET_TAKE(ad2, 3LL * max_tris);
+                acc_d2[b] = ad2;
+                tab.dout2[b] = reinterpret_cast<float*>(ad2);
+            }
         }
     }
+#define PETCH_LB(K)                                                                            \
+    launch_batch<K>(tab, L, max_tris, max_verts, beta, beta2, step, seed_mul, seed_add, seed_add2, \
+                    domain, det, work, st)
     switch (kind) {
-        case 0: launch_batch<0>(tab, L, max_tris, max_verts, beta, step, seed_mul, seed_add, domain, det, work, st); break;
-        case 1: launch_batch<1>(tab, L, max_tris, max_verts, beta, step, seed_mul, seed_add, domain, det, work, st); break;
-        case 2: launch_batch<2>(tab, L, max_tris, max_verts, beta, step, seed_mul, seed_add, domain, det, work, st); break;
-        default: launch_batch<3>(tab, L, max_tris, max_verts, beta, step, seed_mul, seed_add, domain, det, work, st); break;
+        case 0: PETCH_LB(0); break;
+        case 1: PETCH_LB(1); break;
+        case 2: PETCH_LB(2); break;
+        case 3: PETCH_LB(3); break;
+        case 4: PETCH_LB(4); break;
+        default: PETCH_LB(5); break;
     }
+#undef PETCH_LB
     PETCH_LAUNCH_CHECK("k_trace_batch");
     if (det) {
         for (int b = 0; b < B; ++b) {
             PETCH_DET_CONVERT(acc_out[b], items[b].out, per_out);
-            if (ion) PETCH_DET_CONVERT(acc_ang[b], items[b].ang, (long long)max_tris);
+            if (ion || pair) PETCH_DET_CONVERT(acc_ang[b], items[b].ang, (long long)max_tris);
             if (tan) PETCH_DET_CONVERT(acc_d[b], tans[b].dout, 3LL * max_tris);
+            if (kind == 5) PETCH_DET_CONVERT(acc_d2[b], tans2[b].dout, 3LL * max_tris);
         }
     }
     return PETCH_OK;
@@ -1417,8 +1500,16 @@ extern "C" int petch_trace_batch(int kind, const petch_batch_item* items, int B,
                                  int max_verts, float beta, const int* step, uint32_t seed_mul,
                                  uint32_t seed_add, int* work, void* stream) {
     PETCH_REQUIRE(kind == 0 || kind == 1, "petch_trace_batch: kind must be 0 (ions) or 1 (neutrals)");
-    return trace_batch(kind, items, nullptr, B, max_tris, max_verts, beta, step, seed_mul,
-                       seed_add, work, stream, "petch_trace_batch");
+    return trace_batch(kind, items, nullptr, B, max_tris, max_verts, beta, beta, step, seed_mul,
+                       seed_add, seed_add, work, stream, "petch_trace_batch");
+}
+
+extern "C" int petch_trace_batch_pair(const petch_batch_item* items, int B, int max_tris,
+                                      int max_verts, float beta_a, float beta_b, const int* step,
+                                      uint32_t seed_mul, uint32_t seed_add_a, uint32_t seed_add_b,
+                                      int* work, void* stream) {
+    return trace_batch(4, items, nullptr, B, max_tris, max_verts, beta_a, beta_b, step, seed_mul,
+                       seed_add_a, seed_add_b, work, stream, "petch_trace_batch_pair");
 }
 
 extern "C" int petch_trace_batch_tangent(int kind, const petch_batch_item* items,
@@ -1428,8 +1519,20 @@ extern "C" int petch_trace_batch_tangent(int kind, const petch_batch_item* items
                                          void* stream) {
     PETCH_REQUIRE(kind == 0 || kind == 1,
                   "petch_trace_batch_tangent: kind must be 0 (ions) or 1 (neutrals)");
-    return trace_batch(kind + 2, items, tans, B, max_tris, max_verts, beta, step, seed_mul,
-                       seed_add, work, stream, "petch_trace_batch_tangent");
+    return trace_batch(kind + 2, items, tans, B, max_tris, max_verts, beta, beta, step, seed_mul,
+                       seed_add, seed_add, work, stream, "petch_trace_batch_tangent");
+}
+
+extern "C" int petch_trace_batch_pair_tangent(const petch_batch_item* items,
+                                              const petch_batch_tangent* tans_a,
+                                              const petch_batch_tangent* tans_b, int B,
+                                              int max_tris, int max_verts, float beta_a,
+                                              float beta_b, const int* step, uint32_t seed_mul,
+                                              uint32_t seed_add_a, uint32_t seed_add_b, int* work,
+                                              void* stream) {
+    return trace_batch(5, items, tans_a, B, max_tris, max_verts, beta_a, beta_b, step, seed_mul,
+                       seed_add_a, seed_add_b, work, stream, "petch_trace_batch_pair_tangent",
+                       tans_b);
 }
 
 extern "C" int petch_redep_scratch_bytes(int max_tris, long long* bytes) {
@@ -1530,6 +1633,53 @@ extern "C" int petch_trace_ions_tangent(const void* mesh, int max_tris, int max_
     PETCH_DET_CONVERT(a_t, tally4, 4LL * max_tris);
     PETCH_DET_CONVERT(a_a, ang, (long long)max_tris);
     PETCH_DET_CONVERT(a_d, dtal, 3LL * max_tris);
+    return PETCH_OK;
+}
+
+extern "C" int petch_trace_neutral_pair_tangent(const void* mesh, int max_tris, int max_verts,
+                                                const petch_domain* dom, const float* bare,
+                                                const float* dbare, float beta_a, float beta_b,
+                                                uint32_t seed_a, uint32_t seed_b,
+                                                uint32_t stream_id, int n_neu, float* flux_a,
+                                                float* dflux_a, float* flux_b, float* dflux_b,
+                                                int* work, void* stream) {
+    PETCH_REQUIRE(mesh && dom && flux_a && dflux_a && flux_b && dflux_b && work,
+                  "petch_trace_neutral_pair_tangent: null pointer");
+    PETCH_REQUIRE(flux_a != flux_b && dflux_a != dflux_b,
+                  "petch_trace_neutral_pair_tangent: the two species' outputs must differ");
+    PETCH_REQUIRE(n_neu >= 0 && n_neu <= (1 << 30) && max_tris > 0 && max_verts > 0,
+                  "petch_trace_neutral_pair_tangent: bad size");
+    cudaStream_t st = as_stream(stream);
+    MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
+    const uint32_t domain = 0x6e657500u ^ stream_id;
+    NeutralTanPairShader sh{bare, dbare, beta_a, beta_b, flux_a, dflux_a, flux_b, dflux_b,
+                            seed_b, domain, n_neu, 0};
+    k_zero_faces<<<grid_for(max_tris, 256), 256, 0, st>>>(m.hdr, max_tris, flux_a, 1, flux_b, 1);
+    PETCH_LAUNCH_CHECK("k_zero_faces");
+    PETCH_CUDA(cudaMemsetAsync(dflux_a, 0, sizeof(float) * 3 * (size_t)max_tris, st), "zero dflux");
+    PETCH_CUDA(cudaMemsetAsync(dflux_b, 0, sizeof(float) * 3 * (size_t)max_tris, st), "zero dflux");
+    PETCH_CUDA(cudaMemsetAsync(work, 0, sizeof(int), st), "reset ray counter");
+    if (n_neu == 0) return PETCH_OK;
+    DetArena arena;
+    if (!arena.on())
+        return launch_trace(m, to_domain(dom), sh, seed_a, domain, 2 * n_neu, work, st,
+                            "k_trace<neutral pair, tangent>");
+    PETCH_DET_TAKE(a_fa, (long long)max_tris);
+    PETCH_DET_TAKE(a_da, 3LL * max_tris);
+    PETCH_DET_TAKE(a_fb, (long long)max_tris);
+    PETCH_DET_TAKE(a_db, 3LL * max_tris);
+    sh.flux_a = reinterpret_cast<float*>(a_fa);
+    sh.dflux_a = reinterpret_cast<float*>(a_da);
+    sh.flux_b = reinterpret_cast<float*>(a_fb);
+    sh.dflux_b = reinterpret_cast<float*>(a_db);
+    sh.det = 1;
+    int rc = launch_trace(m, to_domain(dom), sh, seed_a, domain, 2 * n_neu, work, st,
+                          "k_trace<neutral pair, tangent>");
+    if (rc) return rc;
+    PETCH_DET_CONVERT(a_fa, flux_a, (long long)max_tris);
+    PETCH_DET_CONVERT(a_da, dflux_a, 3LL * max_tris);
+    PETCH_DET_CONVERT(a_fb, flux_b, (long long)max_tris);
+    PETCH_DET_CONVERT(a_db, dflux_b, 3LL * max_tris);
     return PETCH_OK;
 }
 

@@ -129,10 +129,12 @@ SIGNATURES = {
     "petch_trace_redep": [P, I, I, DP, P, P, F, U, I, P, P, P, L, P, P],
     "petch_redep_apply": [P, I, I, P, P, I, F, P, P, P, P],
     "petch_trace_batch": [I, P, I, I, I, F, P, U, U, P, P],
+    "petch_trace_batch_pair": [P, I, I, I, F, F, P, U, U, U, P, P],
     "petch_prepare_device": [],
     "petch_set_deterministic": [P, L],
     "petch_trace_ions_tangent": [P, I, I, DP, IP, U, I, P, P, P, P, P],
     "petch_trace_neutrals_tangent": [P, I, I, DP, P, P, F, U, U, I, P, P, P, P],
+    "petch_trace_neutral_pair_tangent": [P, I, I, DP, P, P, F, F, U, U, U, I, P, P, P, P, P, P],
     "petch_norm_smooth_tangent": [P, I, I, P, P, F, F, F, I, I, F, I, P, P, P, P],
     "petch_belen_bare_tangent": [P, I, I, CP, P, P, P, P, P, P, P, P, P, P, P, P],
     "petch_surface_rate_tangent": [P, I, I, CP, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P],
@@ -144,6 +146,7 @@ SIGNATURES = {
     "petch_batch_reinit": [P, I, D, P],
     "petch_batch_step_advance": [P, P],
     "petch_trace_batch_tangent": [I, P, P, I, I, I, F, P, U, U, P, P],
+    "petch_trace_batch_pair_tangent": [P, P, P, I, I, I, F, F, P, U, U, U, P, P],
     "petch_batch_advect_tangent": [P, P, I, P],
     "petch_batch_reinit_tangent": [P, P, I, D, P],
     "petch_extend_velocity_dual": [P, I, I, P, P, I, I, I, D, D, P, P, P, P, I, P, P, I, P, P],

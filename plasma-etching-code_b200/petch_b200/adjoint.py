@@ -68,6 +68,7 @@ class TangentEngine(EtchEngine):
         self.dm_O = torch.zeros((ND, MT), **dev)
         self.dbare = torch.zeros((ND, MT), **dev)
         self.dflux = torch.empty((ND, MT), **dev)
+        self.dflux_o = torch.empty((ND, MT), **dev)      # the O species of a paired round
         self.dV = torch.zeros((ND, MT), **dev)
         self.ttmp = torch.empty((2, MT), **dev)
 
@@ -126,18 +127,22 @@ class TangentEngine(EtchEngine):
             self.bare.fill_(1.0)
             self.dbare.zero_()
         betaE, betaO = float(par.get('betaE', 0.7)), float(par.get('betaO', 1.0))
+        flux_o = self.tmp5[2 * MT:3 * MT]
         for it in range(n_fp):
-            for beta, out, dout, sd in ((betaE, self.m_F, self.dm_F, seed * 9 + 2 + 2 * it),
-                                        (betaO, self.m_O, self.dm_O, seed * 9 + 3 + 2 * it)):
-                _lib.call("petch_trace_neutrals_tangent", m.id, m.MT, m.MV, ctypes.byref(self.dom),
-                          self.bare.data_ptr(), self.dbare.data_ptr(), beta,
-                          int(sd) & 0xffffffff, 0, int(n_neu), self.flux.data_ptr(),
-                          self.dflux.data_ptr(), work.data_ptr(), s)
-                _lib.call("petch_norm_smooth", m.id, m.MT, m.MV, self.flux.data_ptr(),
+            # both species of the round in one launch (F: betaE, seed*9+2+2it; O: betaO, +3+2it)
+            _lib.call("petch_trace_neutral_pair_tangent", m.id, m.MT, m.MV, ctypes.byref(self.dom),
+                      self.bare.data_ptr(), self.dbare.data_ptr(), betaE, betaO,
+                      int(seed * 9 + 2 + 2 * it) & 0xffffffff,
+                      int(seed * 9 + 3 + 2 * it) & 0xffffffff, 0, int(n_neu),
+                      self.flux.data_ptr(), self.dflux.data_ptr(), flux_o.data_ptr(),
+                      self.dflux_o.data_ptr(), work.data_ptr(), s)
+            for fl, dfl, out, dout in ((self.flux, self.dflux, self.m_F, self.dm_F),
+                                       (flux_o, self.dflux_o, self.m_O, self.dm_O)):
+                _lib.call("petch_norm_smooth", m.id, m.MT, m.MV, fl.data_ptr(),
                           float(A_src / n_neu), 0.0, 8.0, 1, n_smooth, alpha, out.data_ptr(),
                           self.tmp5.data_ptr(), self.tmp5[MT:].data_ptr(), s)
-                _lib.call("petch_norm_smooth_tangent", m.id, m.MT, m.MV, self.flux.data_ptr(),
-                          self.dflux.data_ptr(), float(A_src / n_neu), 0.0, 8.0, 1, n_smooth,
+                _lib.call("petch_norm_smooth_tangent", m.id, m.MT, m.MV, fl.data_ptr(),
+                          dfl.data_ptr(), float(A_src / n_neu), 0.0, 8.0, 1, n_smooth,
                           alpha, 0, dout.data_ptr(), self.ttmp[0].data_ptr(),
                           self.ttmp[1].data_ptr(), s)
             _lib.call("petch_belen_bare_tangent", m.id, m.MT, m.MV, ctypes.byref(self.chem),

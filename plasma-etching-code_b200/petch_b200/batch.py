@@ -181,16 +181,20 @@ class BatchEngine:
             for x in self.inst:
                 x.bares[cur].fill_(1.0)
         for it in range(n_fp):
-            for beta, name, add in ((self.betaE, "m_F", 2 + 2 * it), (self.betaO, "m_O", 3 + 2 * it)):
-                _lib.call("petch_trace_batch", 1, self._items(1, cur), B, MT, MV, beta,
-                          self.step_dev.data_ptr(), 9, add, self.work.data_ptr(), s)
-                for x in self.inst:
-                    m, fe = x.meshes[cur], x.fe
-                    A_src = float(x.geo['Lx'] * x.geo['Ly'])
-                    _lib.call("petch_norm_smooth", m.id, m.MT, m.MV, fe.flux.data_ptr(),
+            # both species of the round in one launch: F (betaE, +2+2it) into fe.flux, O (betaO,
+            # +3+2it) into the third slice of fe.tmp5
+            items = self._items(1, cur)
+            for b, x in enumerate(self.inst):
+                items[b].ang = x.fe.tmp5[2 * MT:3 * MT].data_ptr()
+            _lib.call("petch_trace_batch_pair", items, B, MT, MV, self.betaE, self.betaO,
+                      self.step_dev.data_ptr(), 9, 2 + 2 * it, 3 + 2 * it, self.work.data_ptr(), s)
+            for x in self.inst:
+                m, fe = x.meshes[cur], x.fe
+                A_src = float(x.geo['Lx'] * x.geo['Ly'])
+                for fl, out in ((fe.flux, fe.m_F), (fe.tmp5[2 * MT:3 * MT], fe.m_O)):
+                    _lib.call("petch_norm_smooth", m.id, m.MT, m.MV, fl.data_ptr(),
                               float(A_src / self.n_neu), 0.0, 8.0, 1, self.n_smooth, self.alpha,
-                              getattr(fe, name).data_ptr(), fe.tmp5.data_ptr(),
-                              fe.tmp5[m.MT:].data_ptr(), s)
+                              out.data_ptr(), fe.tmp5.data_ptr(), fe.tmp5[m.MT:].data_ptr(), s)
             for x in self.inst:
                 m, fe = x.meshes[cur], x.fe
                 _lib.call("petch_belen_bare", m.id, m.MT, m.MV, ctypes.byref(fe.chem),

@@ -9,7 +9,7 @@ extension and the FSM reinit); the instances advance together as BatchEngine's d
         nearest-face query per face)
     ions of ALL instances with energy tangents: one persistent launch (petch_trace_batch_tangent)
     per instance: ion normalisation + smoothing, the yields' tangents
-    coverage fixed point: F and O neutrals of all instances with weight tangents, one launch each;
+    coverage fixed point: F and O neutrals of all instances with weight tangents, one launch;
         per instance normalisation + smoothing (+ tangents), Belen coverage update with duals
     per instance: surface rate with duals, velocity extension and its tangent (one nearest-face
         query per band cell)
@@ -107,6 +107,7 @@ class _TInst:
         self.dm_F = torch.zeros((ND, MT), **dev)
         self.dm_O = torch.zeros((ND, MT), **dev)
         self.dflux = torch.empty((ND, MT), **dev)
+        self.dflux_o = torch.empty((ND, MT), **dev)      # the O species of a paired round
         self.dV = torch.zeros((ND, MT), **dev)
         self.ttmp = torch.empty((2, MT), **dev)
         self.scratch = torch.empty(mesh_scratch_bytes(self.shape, MT), dtype=torch.uint8,
@@ -278,20 +279,26 @@ class BatchTangentEngine:
                 x.bares[cur].fill_(1.0)
                 x.dbares[cur].zero_()
         for it in range(n_fp):
-            for beta, name, add in ((self.betaE, "F", 2 + 2 * it), (self.betaO, "O", 3 + 2 * it)):
-                items, tans = self._items(False, cur)
-                _lib.call("petch_trace_batch_tangent", 1, items, tans, B, MT, MV, beta,
-                          self.step_dev.data_ptr(), 9, add, self.work.data_ptr(), s)
-                for x in self.inst:
-                    m, fe = x.meshes[cur], x.fe
-                    norm = float(x.geo['Lx'] * x.geo['Ly'] / self.n_neu)
-                    out = fe.m_F if name == "F" else fe.m_O
-                    dout = x.dm_F if name == "F" else x.dm_O
-                    _lib.call("petch_norm_smooth", m.id, m.MT, m.MV, fe.flux.data_ptr(), norm, 0.0,
+            # both species of the round with their tangents in one launch: F (betaE, +2+2it) into
+            # fe.flux / x.dflux, O (betaO, +3+2it) into fe.tmp5's third slice / x.dflux_o
+            items, tans = self._items(False, cur)
+            tans_o = (_lib.BatchTangent * B)()
+            for b, x in enumerate(self.inst):
+                items[b].ang = x.fe.tmp5[2 * MT:3 * MT].data_ptr()
+                tans_o[b].dout = x.dflux_o.data_ptr()
+            _lib.call("petch_trace_batch_pair_tangent", items, tans, tans_o, B, MT, MV,
+                      self.betaE, self.betaO, self.step_dev.data_ptr(), 9, 2 + 2 * it, 3 + 2 * it,
+                      self.work.data_ptr(), s)
+            for x in self.inst:
+                m, fe = x.meshes[cur], x.fe
+                norm = float(x.geo['Lx'] * x.geo['Ly'] / self.n_neu)
+                for fl, dfl, out, dout in ((fe.flux, x.dflux, fe.m_F, x.dm_F),
+                                           (fe.tmp5[2 * MT:3 * MT], x.dflux_o, fe.m_O, x.dm_O)):
+                    _lib.call("petch_norm_smooth", m.id, m.MT, m.MV, fl.data_ptr(), norm, 0.0,
                               8.0, 1, self.n_smooth, self.alpha, out.data_ptr(),
                               fe.tmp5.data_ptr(), fe.tmp5[MT:].data_ptr(), s)
-                    _lib.call("petch_norm_smooth_tangent", m.id, m.MT, m.MV, fe.flux.data_ptr(),
-                              x.dflux.data_ptr(), norm, 0.0, 8.0, 1, self.n_smooth, self.alpha, 0,
+                    _lib.call("petch_norm_smooth_tangent", m.id, m.MT, m.MV, fl.data_ptr(),
+                              dfl.data_ptr(), norm, 0.0, 8.0, 1, self.n_smooth, self.alpha, 0,
                               dout.data_ptr(), x.ttmp[0].data_ptr(), x.ttmp[1].data_ptr(), s)
             for x in self.inst:
                 m, fe = x.meshes[cur], x.fe

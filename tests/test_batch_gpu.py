@@ -142,3 +142,44 @@ def test_batch_rejects_unsupported_configurations():
     bad = [dict(specs[0]), dict(specs[0], dx=0.2)]
     with pytest.raises(ValueError):
         BatchEngine(bad, petch.Flags(**FLAGS))
+
+
+def test_batched_pair_equals_per_instance_single_launches():
+    """petch_trace_batch_pair (both neutral species of every instance in one launch) against the
+    per-instance single-species tracers with the seeds the batch derives: bit-equal with
+    deterministic tallies."""
+    feats = [small_feature(True), small_feature(False), small_feature(True, nx=12, ny=12, nz=16)]
+    MT = 65536
+    meshes = [cuda_mesh(phi, geo['dx'], geo, MT=MT) for phi, geo in feats]
+    rng = np.random.default_rng(6)
+    step = torch.tensor([5], dtype=torch.int32, device="cuda")
+    work = torch.zeros(6, dtype=torch.int32, device="cuda")
+    n = 100_000
+    bares = [torch.from_numpy(rng.uniform(0.2, 1.0, MT).astype(np.float32)).cuda() for _ in meshes]
+    fa = [torch.full((MT,), 3.0, device="cuda") for _ in meshes]
+    fb = [torch.full((MT,), 3.0, device="cuda") for _ in meshes]
+    items = (_lib.BatchItem * 3)()
+    for b, (m, (phi, geo)) in enumerate(zip(meshes, feats)):
+        it = items[b]
+        it.mesh, it.dom, it.ion = m.id, domain(geo), t3.ion_params(dict(petch.PAR))
+        it.bare, it.out, it.ang = bares[b].data_ptr(), fa[b].data_ptr(), fb[b].data_ptr()
+        it.n_rays, it.seed = n + 500 * b, 7 * b
+    _lib.set_deterministic(64 << 20)
+    try:
+        _lib.call("petch_trace_batch_pair", items, 3, MT, MT, 0.7, 1.0, step.data_ptr(), 9, 2, 3,
+                  work.data_ptr(), stream())
+        assert work[1].item() == 0
+        for b, (m, (phi, geo)) in enumerate(zip(meshes, feats)):
+            for beta, add, got in ((0.7, 2, fa[b]), (1.0, 3, fb[b])):
+                flux = torch.zeros(MT, device="cuda")
+                _lib.call("petch_trace_neutrals", m.id, m.MT, m.MV, ctypes.byref(domain(geo)),
+                          bares[b].data_ptr(), beta, (5 + 7 * b) * 9 + add, 0, n + 500 * b,
+                          flux.data_ptr(), work.data_ptr(), stream())
+                assert torch.equal(got[:m.F], flux[:m.F]), (b, beta)
+                assert flux[:m.F].abs().max().item() > 0.0
+    finally:
+        _lib.set_deterministic(0)
+    items[0].ang = items[0].out
+    with pytest.raises(_lib.PetchError, match="second flux"):
+        _lib.call("petch_trace_batch_pair", items, 3, MT, MT, 0.7, 1.0, None, 9, 2, 3,
+                  work.data_ptr(), stream())
