@@ -174,7 +174,7 @@ int petch_trace_neutrals(const void* mesh, int max_tris, int max_verts, const pe
  * (beta_b, seed_b), both with stream_id; ray r of each species draws the same Philox stream as in
  * the single-species call, so each flux equals that call's up to the order of float atomic
  * additions (exactly, with deterministic tallies).  flux_a, flux_b: float[max_tris], distinct,
- * zeroed first; n_neu <= 2^30. */
+ * zeroed first; n_neu < 2^30. */
 int petch_trace_neutral_pair(const void* mesh, int max_tris, int max_verts,
                              const petch_domain* dom, const float* bare, float beta_a,
                              float beta_b, uint32_t seed_a, uint32_t seed_b, uint32_t stream_id,
@@ -657,7 +657,7 @@ int petch_trace_neutrals_tangent(const void* mesh, int max_tris, int max_verts,
  * species of a coverage round in one launch (rays [0, n_neu): beta_a, seed_a into flux_a /
  * dflux_a; rays [n_neu, 2 n_neu): beta_b, seed_b into flux_b / dflux_b), each equal to its own
  * tangent launch up to the order of float atomic additions (exactly, with deterministic tallies).
- * dbare, dflux_*: [3][max_tris]; outputs zeroed first; n_neu <= 2^30. */
+ * dbare, dflux_*: [3][max_tris]; outputs zeroed first; n_neu < 2^30. */
 int petch_trace_neutral_pair_tangent(const void* mesh, int max_tris, int max_verts,
                                      const petch_domain* dom, const float* bare,
                                      const float* dbare, float beta_a, float beta_b,

@@ -1279,7 +1279,7 @@ extern "C" int petch_trace_neutral_pair(const void* mesh, int max_tris, int max_
                                         float* flux_b, int* work, void* stream) {
     PETCH_REQUIRE(mesh && dom && flux_a && flux_b && work, "petch_trace_neutral_pair: null pointer");
     PETCH_REQUIRE(flux_a != flux_b, "petch_trace_neutral_pair: flux_a and flux_b must differ");
-    PETCH_REQUIRE(n_neu >= 0 && n_neu <= (1 << 30) && max_tris > 0 && max_verts > 0,
+    PETCH_REQUIRE(n_neu >= 0 && n_neu < (1 << 30) && max_tris > 0 && max_verts > 0,
                   "petch_trace_neutral_pair: bad size");
     cudaStream_t st = as_stream(stream);
     MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
@@ -1647,7 +1647,7 @@ extern "C" int petch_trace_neutral_pair_tangent(const void* mesh, int max_tris, 
                   "petch_trace_neutral_pair_tangent: null pointer");
     PETCH_REQUIRE(flux_a != flux_b && dflux_a != dflux_b,
                   "petch_trace_neutral_pair_tangent: the two species' outputs must differ");
-    PETCH_REQUIRE(n_neu >= 0 && n_neu <= (1 << 30) && max_tris > 0 && max_verts > 0,
+    PETCH_REQUIRE(n_neu >= 0 && n_neu < (1 << 30) && max_tris > 0 && max_verts > 0,
                   "petch_trace_neutral_pair_tangent: bad size");
     cudaStream_t st = as_stream(stream);
     MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
