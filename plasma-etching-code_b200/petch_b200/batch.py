@@ -33,6 +33,7 @@ from .threed import (MESH_ERR_HASH_FULL, MESH_ERR_TRI_OVERFLOW, MESH_ERR_VERT_OV
                      mesh_scratch_bytes)
 
 MAX_BATCH = 64
+LANES = 8          # side streams for the per-instance kernels of a batched step
 
 
 class _Instance:
@@ -115,6 +116,7 @@ class BatchEngine:
         self.alpha = float(p0.get('flux_smooth_alpha', 1.0))
         self.step_dev = torch.zeros(1, dtype=torch.int32, device="cuda")
         self.work = torch.zeros(8, dtype=torch.int32, device="cuda")
+        self.lanes = [torch.cuda.Stream() for _ in range(min(LANES, B))]
         self.graphs = None
         self.steps_done = 0
         self.depth_history = [[] for _ in self.inst]
@@ -153,33 +155,74 @@ class BatchEngine:
             t.sub = x.sub.data_ptr()
         return g
 
+    def _each(self, fn):
+        """fn(x) for every instance, instance b on side stream b % len(self.lanes), forked from
+        and joined back into the current stream: the small per-instance kernels of different
+        instances overlap (parallel branches of the captured step graph).  Each instance's chain
+        touches only its own buffers."""
+        main = torch.cuda.current_stream()
+        for ln in self.lanes:
+            ln.wait_stream(main)
+        for b, x in enumerate(self.inst):
+            with torch.cuda.stream(self.lanes[b % len(self.lanes)]):
+                fn(x)
+        for ln in self.lanes:
+            main.wait_stream(ln)
+
     def _step(self, cold, cur):
         s = _sp()
         prev = 1 - cur
         MT = self.MT
         B = len(self.inst)
         MV = self.inst[0].meshes[cur].MV
-        for x in self.inst:
+        n_fp = int(self.inst[0].par.get('n_fp', 4 if cold else 1))
+
+        def surface(x):
             x.fe.small.zero_()
             x.meshes[cur].build(x.phi, x.dx, x.geo, x.scratch)
-        if not cold:
-            for x in self.inst:
+            if not cold:
                 pm, cm = x.meshes[prev], x.meshes[cur]
                 _lib.call("petch_warmstart", pm.id, pm.MT, pm.MV, x.bares[prev].data_ptr(), cm.id,
-                          cm.MT, cm.MV, x.bares[cur].data_ptr(), x.fe.small.data_ptr(), s)
-        _lib.call("petch_trace_batch", 0, self._items(0, cur), B, MT, MV, 0.0,
-                  self.step_dev.data_ptr(), 9, 1, self.work.data_ptr(), s)
-        for x in self.inst:
+                          cm.MT, cm.MV, x.bares[cur].data_ptr(), x.fe.small.data_ptr(), _sp())
+            else:
+                x.bares[cur].fill_(1.0)
+
+        def ion_post(x):
             m, fe = x.meshes[cur], x.fe
             A_src = float(x.geo['Lx'] * x.geo['Ly'])
             _lib.call("petch_ion_post", m.id, m.MT, m.MV, fe.tal4.data_ptr(), fe.ang.data_ptr(),
                       float(A_src / self.n_ion), self.n_smooth, self.alpha, fe.y[0].data_ptr(),
                       fe.y[1].data_ptr(), fe.y[2].data_ptr(), fe.m_i.data_ptr(),
-                      fe.cos_i.data_ptr(), fe.tmp5.data_ptr(), s)
-        n_fp = int(self.inst[0].par.get('n_fp', 4 if cold else 1))
-        if cold:
-            for x in self.inst:
-                x.bares[cur].fill_(1.0)
+                      fe.cos_i.data_ptr(), fe.tmp5.data_ptr(), _sp())
+
+        def coverage(x):
+            m, fe = x.meshes[cur], x.fe
+            A_src = float(x.geo['Lx'] * x.geo['Ly'])
+            for fl, out in ((fe.flux, fe.m_F), (fe.tmp5[2 * MT:3 * MT], fe.m_O)):
+                _lib.call("petch_norm_smooth", m.id, m.MT, m.MV, fl.data_ptr(),
+                          float(A_src / self.n_neu), 0.0, 8.0, 1, self.n_smooth, self.alpha,
+                          out.data_ptr(), fe.tmp5.data_ptr(), fe.tmp5[m.MT:].data_ptr(), _sp())
+            _lib.call("petch_belen_bare", m.id, m.MT, m.MV, ctypes.byref(fe.chem),
+                      fe.m_i.data_ptr(), fe.m_F.data_ptr(), fe.m_O.data_ptr(),
+                      fe.cos_i.data_ptr(), fe.y[1].data_ptr(), fe.y[2].data_ptr(),
+                      x.bares[cur].data_ptr(), _sp())
+
+        def rate_extend(x):
+            m, fe = x.meshes[cur], x.fe
+            _lib.call("petch_surface_rate", m.id, m.MT, m.MV, ctypes.byref(fe.chem),
+                      fe.m_i.data_ptr(), fe.m_F.data_ptr(), fe.m_O.data_ptr(), fe.cos_i.data_ptr(),
+                      fe.y[0].data_ptr(), fe.y[1].data_ptr(), fe.y[2].data_ptr(), fe.V.data_ptr(),
+                      fe.small[6:8].data_ptr(), _sp())
+            nx, ny, nz = x.shape
+            _lib.call("petch_extend_velocity", m.id, m.MT, m.MV, x.phi.data_ptr(),
+                      x.mask.data_ptr(), nx, ny, nz, x.dx, float(self.band), fe.V.data_ptr(),
+                      x.F.data_ptr(), 1, x.active.data_ptr(), fe.small[8:9].data_ptr(), x.ncell,
+                      fe.small[0:6].data_ptr(), _sp())
+
+        self._each(surface)
+        _lib.call("petch_trace_batch", 0, self._items(0, cur), B, MT, MV, 0.0,
+                  self.step_dev.data_ptr(), 9, 1, self.work.data_ptr(), s)
+        self._each(ion_post)
         for it in range(n_fp):
             # both species of the round in one launch: F (betaE, +2+2it) into fe.flux, O (betaO,
             # +3+2it) into the third slice of fe.tmp5
@@ -188,30 +231,8 @@ class BatchEngine:
                 items[b].ang = x.fe.tmp5[2 * MT:3 * MT].data_ptr()
             _lib.call("petch_trace_batch_pair", items, B, MT, MV, self.betaE, self.betaO,
                       self.step_dev.data_ptr(), 9, 2 + 2 * it, 3 + 2 * it, self.work.data_ptr(), s)
-            for x in self.inst:
-                m, fe = x.meshes[cur], x.fe
-                A_src = float(x.geo['Lx'] * x.geo['Ly'])
-                for fl, out in ((fe.flux, fe.m_F), (fe.tmp5[2 * MT:3 * MT], fe.m_O)):
-                    _lib.call("petch_norm_smooth", m.id, m.MT, m.MV, fl.data_ptr(),
-                              float(A_src / self.n_neu), 0.0, 8.0, 1, self.n_smooth, self.alpha,
-                              out.data_ptr(), fe.tmp5.data_ptr(), fe.tmp5[m.MT:].data_ptr(), s)
-            for x in self.inst:
-                m, fe = x.meshes[cur], x.fe
-                _lib.call("petch_belen_bare", m.id, m.MT, m.MV, ctypes.byref(fe.chem),
-                          fe.m_i.data_ptr(), fe.m_F.data_ptr(), fe.m_O.data_ptr(),
-                          fe.cos_i.data_ptr(), fe.y[1].data_ptr(), fe.y[2].data_ptr(),
-                          x.bares[cur].data_ptr(), s)
-        for x in self.inst:
-            m, fe = x.meshes[cur], x.fe
-            _lib.call("petch_surface_rate", m.id, m.MT, m.MV, ctypes.byref(fe.chem),
-                      fe.m_i.data_ptr(), fe.m_F.data_ptr(), fe.m_O.data_ptr(), fe.cos_i.data_ptr(),
-                      fe.y[0].data_ptr(), fe.y[1].data_ptr(), fe.y[2].data_ptr(), fe.V.data_ptr(),
-                      fe.small[6:8].data_ptr(), s)
-            nx, ny, nz = x.shape
-            _lib.call("petch_extend_velocity", m.id, m.MT, m.MV, x.phi.data_ptr(),
-                      x.mask.data_ptr(), nx, ny, nz, x.dx, float(self.band), fe.V.data_ptr(),
-                      x.F.data_ptr(), 1, x.active.data_ptr(), fe.small[8:9].data_ptr(), x.ncell,
-                      fe.small[0:6].data_ptr(), s)
+            self._each(coverage)
+        self._each(rate_extend)
         grids = self._grids(cur)
         _lib.call("petch_batch_advect", grids, B, s)
         _lib.call("petch_batch_reinit", grids, B, float(self.band + 2.0 * self.dx), s)

@@ -38,6 +38,7 @@ from .threed import (MESH_ERR_HASH_FULL, MESH_ERR_TRI_OVERFLOW, MESH_ERR_VERT_OV
                      mesh_scratch_bytes)
 
 MAX_BATCH = 64
+LANES = 8          # side streams for the per-instance kernels of a batched step
 
 
 def trench_batch_specs(n=32, seed=0, dx=0.125, aspect=10.0, mask=1.0, Ly_cells=8, margin=2.0,
@@ -182,6 +183,7 @@ class BatchTangentEngine:
         self.alpha = float(p0.get('flux_smooth_alpha', 1.0))
         self.step_dev = torch.zeros(1, dtype=torch.int32, device="cuda")
         self.work = torch.zeros(8, dtype=torch.int32, device="cuda")
+        self.lanes = [torch.cuda.Stream() for _ in range(min(LANES, len(self.inst)))]
         self.graphs = None
         self.steps_done = 0
 
@@ -242,42 +244,89 @@ class BatchTangentEngine:
             d.mask, d.du_a, d.du_b = x.mask_u8.data_ptr(), x.du_a.data_ptr(), x.du_b.data_ptr()
         return g, t
 
+    def _each(self, fn):
+        """fn(x) for every instance on side stream b % len(self.lanes) (forked from and joined
+        back into the current stream), so the small per-instance kernels of different instances
+        overlap; each instance's chain touches only its own buffers."""
+        main = torch.cuda.current_stream()
+        for ln in self.lanes:
+            ln.wait_stream(main)
+        for b, x in enumerate(self.inst):
+            with torch.cuda.stream(self.lanes[b % len(self.lanes)]):
+                fn(x)
+        for ln in self.lanes:
+            main.wait_stream(ln)
+
     def _step(self, cold, cur):
         s = _sp()
         prev = 1 - cur
         B = len(self.inst)
         MT = self.MT
         MV = self.inst[0].meshes[cur].MV
-        for x in self.inst:
+        n_fp = int(self.inst[0].base_par.get('n_fp', 4 if cold else 1))
+
+        def surface(x):
             x.fe.small.zero_()
             x.meshes[cur].build(x.phi, x.dx, x.geo, x.scratch)
-        if not cold:
-            for x in self.inst:
+            if not cold:
                 pm, cm = x.meshes[prev], x.meshes[cur]
                 _lib.call("petch_warmstart_dual", pm.id, pm.MT, pm.MV, x.bares[prev].data_ptr(),
                           x.dbares[prev].data_ptr(), cm.id, cm.MT, cm.MV,
                           x.bares[cur].data_ptr(), x.dbares[cur].data_ptr(),
-                          x.fe.small.data_ptr(), s)
-        items, tans = self._items(True, cur)
-        _lib.call("petch_trace_batch_tangent", 0, items, tans, B, MT, MV, 0.0,
-                  self.step_dev.data_ptr(), 9, 1, self.work.data_ptr(), s)
-        for x in self.inst:
+                          x.fe.small.data_ptr(), _sp())
+            else:
+                x.bares[cur].fill_(1.0)
+                x.dbares[cur].zero_()
+
+        def ion_post(x):
             m, fe = x.meshes[cur], x.fe
             norm = float(x.geo['Lx'] * x.geo['Ly'] / self.n_ion)
             _lib.call("petch_ion_post", m.id, m.MT, m.MV, fe.tal4.data_ptr(), fe.ang.data_ptr(),
                       norm, self.n_smooth, self.alpha, fe.y[0].data_ptr(), fe.y[1].data_ptr(),
                       fe.y[2].data_ptr(), fe.m_i.data_ptr(), fe.cos_i.data_ptr(),
-                      fe.tmp5.data_ptr(), s)
+                      fe.tmp5.data_ptr(), _sp())
             for q in range(3):                  # d y_q: direction 0 only (ion energy)
                 x.dtal_in[0].copy_(x.dtal[q])
                 _lib.call("petch_norm_smooth_tangent", m.id, m.MT, m.MV, x.dtal_in.data_ptr(),
                           x.dtal_in.data_ptr(), norm, 0.0, 0.0, 0, self.n_smooth, self.alpha, 1,
-                          x.dy[q].data_ptr(), x.ttmp[0].data_ptr(), x.ttmp[1].data_ptr(), s)
-        n_fp = int(self.inst[0].base_par.get('n_fp', 4 if cold else 1))
-        if cold:
-            for x in self.inst:
-                x.bares[cur].fill_(1.0)
-                x.dbares[cur].zero_()
+                          x.dy[q].data_ptr(), x.ttmp[0].data_ptr(), x.ttmp[1].data_ptr(), _sp())
+
+        def coverage(x):
+            m, fe = x.meshes[cur], x.fe
+            norm = float(x.geo['Lx'] * x.geo['Ly'] / self.n_neu)
+            for fl, dfl, out, dout in ((fe.flux, x.dflux, fe.m_F, x.dm_F),
+                                       (fe.tmp5[2 * MT:3 * MT], x.dflux_o, fe.m_O, x.dm_O)):
+                _lib.call("petch_norm_smooth", m.id, m.MT, m.MV, fl.data_ptr(), norm, 0.0,
+                          8.0, 1, self.n_smooth, self.alpha, out.data_ptr(),
+                          fe.tmp5.data_ptr(), fe.tmp5[MT:].data_ptr(), _sp())
+                _lib.call("petch_norm_smooth_tangent", m.id, m.MT, m.MV, fl.data_ptr(),
+                          dfl.data_ptr(), norm, 0.0, 8.0, 1, self.n_smooth, self.alpha, 0,
+                          dout.data_ptr(), x.ttmp[0].data_ptr(), x.ttmp[1].data_ptr(), _sp())
+            _lib.call("petch_belen_bare_tangent", m.id, m.MT, m.MV, ctypes.byref(fe.chem),
+                      x.dOflux, fe.m_F.data_ptr(), x.dm_F.data_ptr(), fe.m_O.data_ptr(),
+                      x.dm_O.data_ptr(), fe.y[1].data_ptr(), x.dy[1].data_ptr(),
+                      fe.y[2].data_ptr(), x.dy[2].data_ptr(), x.bares[cur].data_ptr(),
+                      x.dbares[cur].data_ptr(), _sp())
+
+        def rate_extend(x):
+            m, fe = x.meshes[cur], x.fe
+            _lib.call("petch_surface_rate_tangent", m.id, m.MT, m.MV, ctypes.byref(fe.chem),
+                      x.dOflux, x.drate, fe.m_F.data_ptr(), x.dm_F.data_ptr(), fe.m_O.data_ptr(),
+                      x.dm_O.data_ptr(), fe.y[0].data_ptr(), x.dy[0].data_ptr(),
+                      fe.y[1].data_ptr(), x.dy[1].data_ptr(), fe.y[2].data_ptr(),
+                      x.dy[2].data_ptr(), fe.V.data_ptr(), x.dV.data_ptr(),
+                      fe.small[6:8].data_ptr(), _sp())
+            nx, ny, nz = x.shape
+            _lib.call("petch_extend_velocity_dual", m.id, m.MT, m.MV, x.phi.data_ptr(),
+                      x.mask.data_ptr(), nx, ny, nz, x.dx, float(self.band), fe.V.data_ptr(),
+                      x.dV.data_ptr(), x.F.data_ptr(), x.dF.data_ptr(), 1, x.active.data_ptr(),
+                      fe.small[8:9].data_ptr(), x.ncell, fe.small[0:6].data_ptr(), _sp())
+
+        self._each(surface)
+        items, tans = self._items(True, cur)
+        _lib.call("petch_trace_batch_tangent", 0, items, tans, B, MT, MV, 0.0,
+                  self.step_dev.data_ptr(), 9, 1, self.work.data_ptr(), s)
+        self._each(ion_post)
         for it in range(n_fp):
             # both species of the round with their tangents in one launch: F (betaE, +2+2it) into
             # fe.flux / x.dflux, O (betaO, +3+2it) into fe.tmp5's third slice / x.dflux_o
@@ -289,37 +338,8 @@ class BatchTangentEngine:
             _lib.call("petch_trace_batch_pair_tangent", items, tans, tans_o, B, MT, MV,
                       self.betaE, self.betaO, self.step_dev.data_ptr(), 9, 2 + 2 * it, 3 + 2 * it,
                       self.work.data_ptr(), s)
-            for x in self.inst:
-                m, fe = x.meshes[cur], x.fe
-                norm = float(x.geo['Lx'] * x.geo['Ly'] / self.n_neu)
-                for fl, dfl, out, dout in ((fe.flux, x.dflux, fe.m_F, x.dm_F),
-                                           (fe.tmp5[2 * MT:3 * MT], x.dflux_o, fe.m_O, x.dm_O)):
-                    _lib.call("petch_norm_smooth", m.id, m.MT, m.MV, fl.data_ptr(), norm, 0.0,
-                              8.0, 1, self.n_smooth, self.alpha, out.data_ptr(),
-                              fe.tmp5.data_ptr(), fe.tmp5[MT:].data_ptr(), s)
-                    _lib.call("petch_norm_smooth_tangent", m.id, m.MT, m.MV, fl.data_ptr(),
-                              dfl.data_ptr(), norm, 0.0, 8.0, 1, self.n_smooth, self.alpha, 0,
-                              dout.data_ptr(), x.ttmp[0].data_ptr(), x.ttmp[1].data_ptr(), s)
-            for x in self.inst:
-                m, fe = x.meshes[cur], x.fe
-                _lib.call("petch_belen_bare_tangent", m.id, m.MT, m.MV, ctypes.byref(fe.chem),
-                          x.dOflux, fe.m_F.data_ptr(), x.dm_F.data_ptr(), fe.m_O.data_ptr(),
-                          x.dm_O.data_ptr(), fe.y[1].data_ptr(), x.dy[1].data_ptr(),
-                          fe.y[2].data_ptr(), x.dy[2].data_ptr(), x.bares[cur].data_ptr(),
-                          x.dbares[cur].data_ptr(), s)
-        for x in self.inst:
-            m, fe = x.meshes[cur], x.fe
-            _lib.call("petch_surface_rate_tangent", m.id, m.MT, m.MV, ctypes.byref(fe.chem),
-                      x.dOflux, x.drate, fe.m_F.data_ptr(), x.dm_F.data_ptr(), fe.m_O.data_ptr(),
-                      x.dm_O.data_ptr(), fe.y[0].data_ptr(), x.dy[0].data_ptr(),
-                      fe.y[1].data_ptr(), x.dy[1].data_ptr(), fe.y[2].data_ptr(),
-                      x.dy[2].data_ptr(), fe.V.data_ptr(), x.dV.data_ptr(),
-                      fe.small[6:8].data_ptr(), s)
-            nx, ny, nz = x.shape
-            _lib.call("petch_extend_velocity_dual", m.id, m.MT, m.MV, x.phi.data_ptr(),
-                      x.mask.data_ptr(), nx, ny, nz, x.dx, float(self.band), fe.V.data_ptr(),
-                      x.dV.data_ptr(), x.F.data_ptr(), x.dF.data_ptr(), 1, x.active.data_ptr(),
-                      fe.small[8:9].data_ptr(), x.ncell, fe.small[0:6].data_ptr(), s)
+            self._each(coverage)
+        self._each(rate_extend)
         grids, tg = self._grids(cur)
         _lib.call("petch_batch_advect_tangent", grids, tg, B, s)
         _lib.call("petch_batch_reinit_tangent", grids, tg, B, float(self.band + 2.0 * self.dx), s)
