@@ -36,6 +36,21 @@ MAX_BATCH = 64
 LANES = 8          # side streams for the per-instance kernels of a batched step
 
 
+def on_lanes(lanes, insts, fn):
+    """fn(x) for every instance, instance b on side stream b % len(lanes), forked from and joined
+    back into the current stream: the small per-instance kernels of different instances overlap
+    (parallel branches of a captured step graph).  Each instance's chain must touch only its own
+    buffers."""
+    main = torch.cuda.current_stream()
+    for ln in lanes:
+        ln.wait_stream(main)
+    for b, x in enumerate(insts):
+        with torch.cuda.stream(lanes[b % len(lanes)]):
+            fn(x)
+    for ln in lanes:
+        main.wait_stream(ln)
+
+
 class _Instance:
     """Device state of one instance."""
 
@@ -156,18 +171,7 @@ class BatchEngine:
         return g
 
     def _each(self, fn):
-        """fn(x) for every instance, instance b on side stream b % len(self.lanes), forked from
-        and joined back into the current stream: the small per-instance kernels of different
-        instances overlap (parallel branches of the captured step graph).  Each instance's chain
-        touches only its own buffers."""
-        main = torch.cuda.current_stream()
-        for ln in self.lanes:
-            ln.wait_stream(main)
-        for b, x in enumerate(self.inst):
-            with torch.cuda.stream(self.lanes[b % len(self.lanes)]):
-                fn(x)
-        for ln in self.lanes:
-            main.wait_stream(ln)
+        on_lanes(self.lanes, self.inst, fn)
 
     def _step(self, cold, cur):
         s = _sp()

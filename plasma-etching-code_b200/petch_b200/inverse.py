@@ -32,13 +32,13 @@ import torch
 
 from . import _lib
 from .adjoint import ND, apply_theta, radial_profile, run_etch_3d_tangent
+from .batch import LANES, on_lanes
 from .params import PAR
 from .threed import (MESH_ERR_HASH_FULL, MESH_ERR_TRI_OVERFLOW, MESH_ERR_VERT_OVERFLOW, DeviceMesh,
                      FluxEngine, _sp, chem_params, default_capacity, ion_params, make_trench_3d,
                      mesh_scratch_bytes)
 
 MAX_BATCH = 64
-LANES = 8          # side streams for the per-instance kernels of a batched step
 
 
 def trench_batch_specs(n=32, seed=0, dx=0.125, aspect=10.0, mask=1.0, Ly_cells=8, margin=2.0,
@@ -245,17 +245,7 @@ class BatchTangentEngine:
         return g, t
 
     def _each(self, fn):
-        """fn(x) for every instance on side stream b % len(self.lanes) (forked from and joined
-        back into the current stream), so the small per-instance kernels of different instances
-        overlap; each instance's chain touches only its own buffers."""
-        main = torch.cuda.current_stream()
-        for ln in self.lanes:
-            ln.wait_stream(main)
-        for b, x in enumerate(self.inst):
-            with torch.cuda.stream(self.lanes[b % len(self.lanes)]):
-                fn(x)
-        for ln in self.lanes:
-            main.wait_stream(ln)
+        on_lanes(self.lanes, self.inst, fn)
 
     def _step(self, cold, cur):
         s = _sp()
