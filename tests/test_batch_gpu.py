@@ -61,15 +61,11 @@ def test_batched_steps_follow_the_per_instance_runs():
         assert set(dev) == set(ref)
         for s in sorted(ref):
             assert abs(dev[s] - ref[s]) <= spec['dx'] + 1e-9, (b, s, dev[s], ref[s])
-        # same streams: the batch is far closer to its instance's own run than a run with other
-        # seeds is (rays that meet a triangle edge moved by an atomic-order rounding difference
-        # take another path from then on, so the two are not identical)
-        other = plain_run(spec, n_rays, n_steps, t_end, 8)
-        phi_b = eng.inst[b].phi.double().cpu().numpy()
-        band = np.abs(geo['phi']) < 4 * spec['dx']
-        same = np.abs(phi_b - geo['phi'])[band].mean()
-        indep = np.abs(other['phi'] - geo['phi'])[band].mean()
-        assert same < 0.6 * indep, (b, same, indep)
+    # With float-atomic tallies the two runs part after the first coverage round: the per-face
+    # sums differ in rounding, the coverage feeds the Russian-roulette decisions, and from then
+    # on the paths differ at Monte-Carlo noise level.  That the batch draws exactly the streams
+    # of the per-instance runs is checked with deterministic tallies
+    # (test_deterministic_gpu.py::test_batched_run_equals_per_instance_runs_exactly).
 
 
 def test_batched_trace_equals_per_instance_traces():
