@@ -250,9 +250,11 @@ class FluxEngine:
     def flux_coupled(self, n_ion, n_neu, seed, warm, bare_init=None, phi=None):
         """mc_flux_3d_coupled (threed.py:740-905) on the device.  The coverage starts from the
         previous step's (warm, nearest face) or from bare_init (a device float[F] the caller
-        supplies), else cold at 1.  flags.floor_charge_throttle scales the floor's ion results
-        before the fixed point (_apply_floor_charge_throttle); it needs the level set phi (the
-        engine's own when not given)."""
+        supplies), else cold at 1.  With flags.surface_charging and charge_alpha > 0 the
+        electron-shadowing factor scales m_i (threed.py:847-868); flags.floor_charge_throttle
+        then scales the floor's ion results (_apply_floor_charge_throttle; it needs the level
+        set phi, the engine's own when not given).  Each coverage round traces both neutral
+        species in one launch (petch_trace_neutral_pair)."""
         par, flags, m = self.par, self.flags, self.mesh
         s = _sp()
         A_src = float(self.geo['Lx'] * self.geo['Ly'])
