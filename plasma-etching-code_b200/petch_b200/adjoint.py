@@ -21,7 +21,6 @@ Forward mode is used because theta has three components: the cost is one tangent
 (no reverse sweep, no level-set checkpoints; memory independent of the number of steps).
 """
 import ctypes
-import math
 
 import numpy as np
 import torch

@@ -21,7 +21,6 @@ seed_offset = the instance's seed, so a batched run follows the per-instance run
 the summation order of float atomics).
 """
 import ctypes
-import time
 
 import numpy as np
 import torch

@@ -15,7 +15,6 @@ Host code only derives scalars (seeds, CFL substep count, float64 constants) the
 reference's host code does; no per-face or per-cell arithmetic happens on the CPU.
 """
 import ctypes
-import math
 import time
 import warnings
 

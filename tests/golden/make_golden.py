@@ -4,7 +4,9 @@ warp-lang replaced by warp_shim.py (a CPU stand-in: see its docstring for what i
 
 Run in a checkout that has the reference at /root/reference (or $PETCH_REFERENCE):
 
-    python tests/golden/make_golden.py [group ...]   # groups: levelset surface flux radiosity options redep dda knudsen gmres electron
+    python tests/golden/make_golden.py [group ...]
+
+groups: levelset surface flux radiosity options redep dda knudsen gmres electron
 
 The fixtures are committed; tests read only the .npz files, never the reference.
 """
