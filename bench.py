@@ -1,4 +1,4 @@
-"""Benchmark of the per-step 3D etch loop (the BASELINE metric: etch steps/s, with Mrays/s beside
+"""Benchmark of the per-step 3D etch loop (the headline metric: etch steps/s, with Mrays/s beside
 it) on the periodic trench workload: 128 x 64 x 640 float32 grid (8 x 4 x 40 um at dx 0.0625 um),
 SF6/O2 flags, 2^22 ion + 2^22 neutral rays per species per fixed-point iteration, 100 steps.
 
