@@ -5,7 +5,8 @@
  *
  * Conventions for every entry point:
  *   - all array arguments are DEVICE pointers owned by the caller; the library never allocates,
- *     frees or keeps them (scratch buffers are passed in too);
+ *     frees or keeps them (scratch buffers are passed in too) -- except the fused step's plan
+ *     (petch_plan), which allocates its workspace once and frees it in petch_destroy;
  *   - grids are (nx, ny, nz) C-order, z fastest: cell (i, j, k) is at (i * ny + j) * nz + k, node
  *     coordinates x = i * dx, y = j * dx, z = k * dx (as petch's make_trench_3d);
  *   - `stream` is a cudaStream_t (NULL = legacy default stream); work is enqueued, not waited on;
@@ -140,12 +141,19 @@ typedef struct petch_ion_params {  /* the float32 arguments of _trace3d_ion_yiel
     float sigma;        /* ion angular spread of the source (par['ion_ang_sigma']) */
 } petch_ion_params;
 
-/* Tracer configuration for this process (the autotuner's knobs): bvh_width 2 (binary LBVH,
+/* Tracer configuration for this process (knobs of the tuner, petch_b200.tune): bvh_width 2 (binary LBVH,
  * default) or 8 (quantised 8-wide BVH, built only by mesh builds made while it is configured); each warp runs traversal steps for all its lanes with an
  * open query, at most steps_per_round (default 64) and only while more than keep_lanes lanes
  * (0..31, default 12) still have one, between shading / refill rounds; once the ray pool is empty
  * a warp steps until its last query ends.  Applies to later trace / raycast calls. */
 int petch_tracer_config(int bvh_width, int steps_per_round, int keep_lanes);
+
+/* Warp-aggregated deposits for later trace calls (on = 1; default 0): lanes of a warp that
+ * deposit into the same tally entry in the same hit combine their values first and one lane
+ * issues the atomic (the reference deposits with one wp.atomic_add per tally per hit, threed.py:575,
+ * 648-652).  Results are the same estimator (bit-equal with deterministic tallies); the choice is
+ * a speed knob of the tuner. */
+int petch_tally_aggregation(int on);
 
 /* Replaces _gen_source + _trace3d_ion_yield (petch/threed.py:441-458, 599-712): n_ion ions
  * generated and traced on the device.  tally4 (16-byte aligned float4[max_tris]) receives per
@@ -714,6 +722,79 @@ int petch_advect_tangent(float* phi, float* tmp, float* dphi, float* dtmp, const
 int petch_reinit_tangent(float* phi, float* dphi, float* u_a, float* u_b, float* du_a, float* du_b,
                          int nx, int ny, int nz, double dx, float big, float cap, int n_iter,
                          void* stream);
+
+/* ------------------------------------------------------------------------------------------ */
+/* The fused step: a workspace planned once, one call per etch step                            */
+/* ------------------------------------------------------------------------------------------ */
+
+/* Everything one run needs (run_etch_3d's arguments, petch/threed.py:1643-1648, for the
+ * coverage-coupled Monte-Carlo path that Process(..., SF6O2(), ...).run() takes: faithful ions,
+ * Belen coverages, coverage-dependent neutral sticking; FSM reinit). */
+typedef struct petch_step_config {
+    int nx, ny, nz;                  /* grid (round(L / dx) nodes per axis) */
+    double dx, Lx, Ly, Lz;
+    double sub_top, mask_th, trench_width;
+    int hole;                        /* 1 hole, 0 trench */
+    double dt;                       /* t_end / n_steps */
+    int n_ion, n_neu;                /* rays per launch (n_neu <= 2^29) */
+    int seed_offset;                 /* step s uses seed s + seed_offset (threed.py:1690) */
+    int max_tris;                    /* face capacity of the two mesh buffers */
+    int n_fp;                        /* coverage rounds per step; 0: 4 cold, 1 warm (threed.py:897) */
+    int warm_start;                  /* flags.warm_start_coverage */
+    int n_smooth;                    /* par['flux_smooth'] */
+    float smooth_alpha;              /* par['flux_smooth_alpha'] */
+    float betaE, betaO;              /* par['betaE'], par['betaO'] */
+    petch_domain dom;                /* source plane, open top, lateral wrap */
+    petch_ion_params ion;            /* _trace3d_ion_yield's arguments */
+    petch_chem_params chem;          /* Belen chemistry and rate */
+} petch_step_config;
+
+typedef struct petch_plan_s petch_plan_t;
+
+/* Status accumulated over the steps since the plan was made. */
+typedef struct petch_step_status {
+    int steps;                       /* steps taken (the device step counter) */
+    int faces, max_faces;            /* the last step's face count, the largest seen */
+    int trace_errors, mesh_errors;   /* error bits OR-ed over the steps */
+    int nonfinite;                   /* non-finite surface velocities zeroed, summed */
+    int nsub;                        /* the last step's CFL substeps */
+    float vmax;                      /* the last step's max surface velocity */
+    long long queries;               /* BVH queries, summed */
+} petch_step_status;
+
+/* Plans a run of the fused step (the set-up of run_etch_3d, petch/threed.py:1649-1669): allocates
+ * one workspace (two mesh buffers of cfg->max_tris faces for the warm-started coverage, the
+ * per-face arrays, the level-set scratch grids), derives the mask and mask level set from the
+ * geometry (make_trench_3d, threed.py:32-59), and with seed_field = 1 writes the seed field into
+ * phi (the CSG field redistanced over 24 cells, zero nodes frozen); with seed_field = 0 phi keeps
+ * the caller's level set.  phi (float[nx*ny*nz], device) stays caller-owned and is advanced in
+ * place by petch_step.  Synchronises `stream` once (the mask cell count). */
+int petch_plan(const petch_step_config* cfg, float* phi, int seed_field, petch_plan_t** plan,
+               void* stream);
+
+/* One etch step of run_etch_3d (petch/threed.py:1671-1792): mesh + BVH, warm-started coverage,
+ * ions, the coverage fixed point (both neutral species per round in one launch), surface rate,
+ * velocity extension, CFL substeps and narrow-band advection, Eikonal reinit.  Issues only
+ * stream-ordered work (no synchronisation, no allocation, no host reads): seeds come from a
+ * device step counter and the substep count from the device (160 substep launches, each gated),
+ * so steps can be captured into a CUDA graph -- one graph for the first (cold) step and one for
+ * two consecutive warm steps, since the mesh / coverage buffers alternate.  With deterministic
+ * tallies the result equals run_etch_3d's bit for bit. */
+int petch_step(petch_plan_t* plan, void* stream);
+
+/* Sets which step the next petch_step call issues, for callers that capture steps into graphs
+ * out of order: step 0 is the cold step, and with warm-started coverage step s works on mesh
+ * buffer s % 2.  Only the host-side bookkeeping moves; the seeds still come from the device step
+ * counter, which counts executed steps. */
+int petch_plan_seek(petch_plan_t* plan, long long step);
+
+/* Reads the plan's accumulated status (synchronises `stream`).  Returns PETCH_E_OVERFLOW if a
+ * mesh outgrew max_tris (the level set is then invalid: plan again with more capacity) and
+ * PETCH_E_LIMIT if a tracer hit a traversal bound. */
+int petch_plan_status(petch_plan_t* plan, petch_step_status* status, void* stream);
+
+/* Frees the plan's workspace (after the work on its streams has finished). */
+int petch_destroy(petch_plan_t* plan);
 
 #ifdef __cplusplus
 }

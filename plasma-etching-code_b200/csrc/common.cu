@@ -39,7 +39,7 @@ int sm_count() {
 
 }  // namespace petch
 
-extern "C" int petch_abi_version(void) { return 2; }
+extern "C" int petch_abi_version(void) { return 3; }
 
 extern "C" int petch_launch_count(long long* n) {
     if (!n) {

@@ -47,6 +47,7 @@ constexpr unsigned kFull = 0xffffffffu;
 int g_bvh_width = 2;
 int g_steps = 64;
 int g_keep = 12;
+bool g_tally_agg = false;   // warp-aggregated deposits (petch_tally_aggregation)
 
 // Deterministic tallies (petch_set_deterministic): caller-registered scratch for 64-bit
 // fixed-point accumulators; NULL = float atomics.
@@ -58,6 +59,12 @@ constexpr float kTallyScale = 4294967296.0f;      // 2^32: one unit = 2^-32
 }  // namespace
 
 bool wide_bvh_enabled() { return g_bvh_width == 8; }
+
+namespace {
+// The tally mode word of a trace launch: kTallyDet with deterministic tallies, kTallyAgg with
+// warp aggregation configured.
+int tally_mode(bool det) { return (det ? 1 : 0) | (g_tally_agg ? 2 : 0); }
+}  // namespace
 
 namespace {
 
@@ -154,15 +161,68 @@ __global__ void k_zero_faces(const int* hdr, int MT, float* a, int na, float* b,
 }
 
 
-// One deposit into a tally.  det == 0: float atomic add into out[i].  det != 0: out is an int64
-// accumulator array (same indexing) and v is added in units of 2^-32 -- integer sums do not
-// depend on the order of the additions, so the result is the same on every run.
-__device__ __forceinline__ void tally(float* out, long long i, float v, int det) {
-    if (det)
-        atomicAdd(reinterpret_cast<unsigned long long*>(out) + i,
-                  (unsigned long long)__float2ll_rn(v * kTallyScale));
-    else
-        atomicAdd(out + i, v);
+// One deposit into a tally.  mode bit 0 (kTallyDet) clear: float atomic add into out[i].  Set:
+// out is an int64 accumulator array (same indexing) and v is added in units of 2^-32 -- integer
+// sums do not depend on the order of the additions, so the result is the same on every run.
+//
+// Mode bit 1 (kTallyAgg, petch_tally_aggregation): warp aggregation.  The lanes of a warp that
+// deposit into the same address in the same call (matched on the address, since lanes of one
+// warp may write different arrays: the two species of a paired launch, the instances of a
+// batched one) are found with one match instruction; the lowest of them adds the group's sum
+// (gathered by shuffles in lane order) and the others issue nothing.  With deterministic tallies
+// each lane converts its own deposit to fixed point before the integer sum, so the accumulator
+// receives exactly the sum of the per-deposit units either way.  The match costs every deposit a
+// few instructions, so it pays only where lanes of a warp often deposit on the same face.
+constexpr int kTallyDet = 1, kTallyAgg = 2;
+
+template <class T>
+__device__ __forceinline__ T group_sum(unsigned peers, T v) {
+    T s = T(0);
+    for (unsigned r = peers; r; r &= r - 1) s += __shfl_sync(peers, v, __ffs(r) - 1);
+    return s;
+}
+
+__device__ __forceinline__ void tally(float* out, long long i, float v, int mode) {
+    unsigned long long* acc = reinterpret_cast<unsigned long long*>(out) + i;
+    float* dst = out + i;
+    if (mode & kTallyAgg) {
+        const unsigned peers = __match_any_sync(
+            __activemask(), (mode & kTallyDet) ? reinterpret_cast<unsigned long long>(acc)
+                                               : reinterpret_cast<unsigned long long>(dst));
+        const bool lead = (threadIdx.x & 31) == __ffs(peers) - 1;
+        if (mode & kTallyDet) {
+            long long u = __float2ll_rn(v * kTallyScale);
+            if (peers & (peers - 1)) u = group_sum(peers, u);
+            if (lead) atomicAdd(acc, (unsigned long long)u);
+        } else {
+            if (peers & (peers - 1)) v = group_sum(peers, v);
+            if (lead) atomicAdd(dst, v);
+        }
+    } else if (mode & kTallyDet) {
+        atomicAdd(acc, (unsigned long long)__float2ll_rn(v * kTallyScale));
+    } else {
+        atomicAdd(dst, v);
+    }
+}
+
+// The float-atomic ion deposit (four yields-and-weight entries of one face plus cos * w),
+// aggregated as one group per face when `agg`.
+__device__ __forceinline__ void tally_ion(float4* tal4, float* ang, int f, float4 dep, float a,
+                                          bool agg) {
+    if (agg) {
+        const unsigned peers =
+            __match_any_sync(__activemask(), reinterpret_cast<unsigned long long>(tal4 + f));
+        if (peers & (peers - 1)) {
+            dep.x = group_sum(peers, dep.x);
+            dep.y = group_sum(peers, dep.y);
+            dep.z = group_sum(peers, dep.z);
+            dep.w = group_sum(peers, dep.w);
+            a = group_sum(peers, a);
+        }
+        if ((threadIdx.x & 31) != __ffs(peers) - 1) return;
+    }
+    atomicAdd(tal4 + f, dep);
+    atomicAdd(ang + f, a);
 }
 
 // The face's unit winding normal as stored by the mesh build (float32, bit-identical to
@@ -335,16 +395,16 @@ __device__ __forceinline__ bool ion_hit(const IonP& P, float4* tal4, float* ang,
     const float4 dep = make_float4(P.A_sp * fmaxf(sqrtE - sqrtf(P.Eth_sp), 0.0f) * f_sp * w,
                                    P.A_ie * fmaxf(sqrtE - sqrtf(P.Eth_ie), 0.0f) * f_ie * w,
                                    P.A_p * fmaxf(sqrtE - sqrtf(P.Eth_p), 0.0f) * f_ie * w, w);
-    if (det) {
+    if (det & kTallyDet) {
         float* t4 = reinterpret_cast<float*>(tal4);
         tally(t4, 4LL * f, dep.x, det);
         tally(t4, 4LL * f + 1, dep.y, det);
         tally(t4, 4LL * f + 2, dep.z, det);
         tally(t4, 4LL * f + 3, dep.w, det);
+        tally(ang, f, cosT * w, det);
     } else {
-        atomicAdd(tal4 + f, dep);
+        tally_ion(tal4, ang, f, dep, cosT * w, det & kTallyAgg);
     }
-    tally(ang, f, cosT * w, det);
     if (TAN) {
         const long long MT = T.m.MT;
         const float dsq = s.E > 0.0f ? 0.5f * s.dE / sqrtE : 0.0f;
@@ -661,8 +721,7 @@ __global__ void __launch_bounds__(kTB, S::kMinBlocks) k_trace(MeshView m, Domain
     extern __shared__ float4 s_wn[];
     const Tracer T = make_tracer(m, s_wn, WIDE);
     n = sh.count(m, n);
-    int st_ref[kWStack];
-    float st_t[kWStack];
+    LocalStack stk;
     int err = 0;
     if (WIDE && T.L > 0 && m.hdr[HDR_WLEVELS] < 0) {   // mesh built without the 8-wide tree
         err = 8;
@@ -700,8 +759,7 @@ __global__ void __launch_bounds__(kTB, S::kMinBlocks) k_trace(MeshView m, Domain
         for (int s = 0; s < steps; ++s) {
             if (__popc(__ballot_sync(kFull, phase == 1)) <= keep_now) break;
             if (phase == 1) {
-                bool fin = WIDE ? step_wide(T, q, st_ref, st_t, &err)
-                                : step_binary(T, q, st_ref, st_t, &err);
+                bool fin = WIDE ? step_wide(T, q, stk, &err) : step_binary(T, q, stk, &err);
                 if (fin) phase = 2;
             }
         }
@@ -850,8 +908,7 @@ k_trace_batch(BatchTable tab, MeshOffsets L, int MT, int MV, float beta, float b
     auto s_start = [&](int i) { return i < tab.B ? tab.it[i].ray_start : tab.total; };
     const int n = tab.total;
     const uint32_t stepv = step ? (uint32_t)*step : 0u;
-    int st_ref[kWStack];
-    float st_t[kWStack];
+    LocalStack stk;
     int err = 0;
     unsigned long long n_query = 0, n_visit = 0;
     int ray = -1, phase = 0, inst = 0;
@@ -914,7 +971,7 @@ k_trace_batch(BatchTable tab, MeshOffsets L, int MT, int MV, float beta, float b
         for (int s = 0; s < steps; ++s) {
             if (__popc(__ballot_sync(kFull, phase == 1)) <= keep_now) break;
             if (phase == 1) {
-                if (step_binary(T, q, st_ref, st_t, &err)) phase = 2;
+                if (step_binary(T, q, stk, &err)) phase = 2;
             }
         }
         if (phase == 2) {
@@ -1068,8 +1125,7 @@ __global__ void __launch_bounds__(kTB) k_raycast(MeshView m, const float* __rest
                                                  int* work, int wide) {
     extern __shared__ float4 s_wn[];
     const Tracer T = make_tracer(m, s_wn, wide);
-    int st_ref[kWStack];
-    float st_t[kWStack];
+    LocalStack stk;
     int err = 0;
     const bool missing = wide && T.L > 0 && m.hdr[HDR_WLEVELS] < 0;   // no 8-wide tree built
     if (missing) err = 8;
@@ -1079,7 +1135,7 @@ __global__ void __launch_bounds__(kTB) k_raycast(MeshView m, const float* __rest
                     make_float3(d[3 * i], d[3 * i + 1], d[3 * i + 2]), tmax, wide);
         if (missing) q.cur = kDone;
         if (q.cur != kDone)
-            while (!(wide ? step_wide(T, q, st_ref, st_t, &err) : step_binary(T, q, st_ref, st_t, &err))) {
+            while (!(wide ? step_wide(T, q, stk, &err) : step_binary(T, q, stk, &err))) {
             }
         face[i] = q.f;
         t[i] = q.f >= 0 ? q.t : 0.0f;
@@ -1211,6 +1267,12 @@ extern "C" int petch_tracer_config(int bvh_width, int steps_per_round, int keep_
     return PETCH_OK;
 }
 
+extern "C" int petch_tally_aggregation(int on) {
+    PETCH_REQUIRE(on == 0 || on == 1, "petch_tally_aggregation: on must be 0 or 1");
+    g_tally_agg = on != 0;
+    return PETCH_OK;
+}
+
 extern "C" int petch_trace_ions(const void* mesh, int max_tris, int max_verts,
                                 const petch_domain* dom, const petch_ion_params* p, uint32_t seed,
                                 int n_ion, float* tally4, float* ang, int* work, void* stream) {
@@ -1225,7 +1287,7 @@ extern "C" int petch_trace_ions(const void* mesh, int max_tris, int max_verts,
                 p->sigma};
     sh.tal4 = (float4*)tally4;
     sh.ang = ang;
-    sh.det = 0;
+    sh.det = tally_mode(false);
     k_zero_faces<<<grid_for(4LL * max_tris, 256), 256, 0, st>>>(m.hdr, max_tris, tally4, 4, ang, 1);
     PETCH_LAUNCH_CHECK("k_zero_faces");
     PETCH_CUDA(cudaMemsetAsync(work, 0, sizeof(int), st), "reset ray counter");
@@ -1237,7 +1299,7 @@ extern "C" int petch_trace_ions(const void* mesh, int max_tris, int max_verts,
     PETCH_DET_TAKE(a_a, (long long)max_tris);
     sh.tal4 = reinterpret_cast<float4*>(a_t);
     sh.ang = reinterpret_cast<float*>(a_a);
-    sh.det = 1;
+    sh.det = tally_mode(true);
     int rc = launch_trace(m, to_domain(dom), sh, seed, 0x696f6e73u, n_ion, work, st, "k_trace<ions>");
     if (rc) return rc;
     PETCH_DET_CONVERT(a_t, tally4, 4LL * max_tris);
@@ -1253,7 +1315,7 @@ extern "C" int petch_trace_neutrals(const void* mesh, int max_tris, int max_vert
     PETCH_REQUIRE(n_neu >= 0 && max_tris > 0 && max_verts > 0, "petch_trace_neutrals: bad size");
     cudaStream_t st = as_stream(stream);
     MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
-    NeutralShader sh{bare, beta, flux, 0};
+    NeutralShader sh{bare, beta, flux, tally_mode(false)};
     k_zero_faces<<<grid_for(max_tris, 256), 256, 0, st>>>(m.hdr, max_tris, flux, 1, nullptr, 0);
     PETCH_LAUNCH_CHECK("k_zero_faces");
     PETCH_CUDA(cudaMemsetAsync(work, 0, sizeof(int), st), "reset ray counter");
@@ -1264,7 +1326,7 @@ extern "C" int petch_trace_neutrals(const void* mesh, int max_tris, int max_vert
                             "k_trace<neutrals>");
     PETCH_DET_TAKE(a_f, (long long)max_tris);
     sh.flux = reinterpret_cast<float*>(a_f);
-    sh.det = 1;
+    sh.det = tally_mode(true);
     int rc = launch_trace(m, to_domain(dom), sh, seed, 0x6e657500u ^ stream_id, n_neu, work, st,
                           "k_trace<neutrals>");
     if (rc) return rc;
@@ -1284,7 +1346,8 @@ extern "C" int petch_trace_neutral_pair(const void* mesh, int max_tris, int max_
     cudaStream_t st = as_stream(stream);
     MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
     const uint32_t domain = 0x6e657500u ^ stream_id;
-    NeutralPairShader sh{bare, beta_a, beta_b, flux_a, flux_b, seed_b, domain, n_neu, 0};
+    NeutralPairShader sh{bare, beta_a, beta_b, flux_a, flux_b, seed_b, domain, n_neu,
+                         tally_mode(false)};
     k_zero_faces<<<grid_for(max_tris, 256), 256, 0, st>>>(m.hdr, max_tris, flux_a, 1, flux_b, 1);
     PETCH_LAUNCH_CHECK("k_zero_faces");
     PETCH_CUDA(cudaMemsetAsync(work, 0, sizeof(int), st), "reset ray counter");
@@ -1297,7 +1360,7 @@ extern "C" int petch_trace_neutral_pair(const void* mesh, int max_tris, int max_
     PETCH_DET_TAKE(a_b, (long long)max_tris);
     sh.flux_a = reinterpret_cast<float*>(a_a);
     sh.flux_b = reinterpret_cast<float*>(a_b);
-    sh.det = 1;
+    sh.det = tally_mode(true);
     int rc = launch_trace(m, to_domain(dom), sh, seed_a, domain, 2 * n_neu, work, st,
                           "k_trace<neutral pair>");
     if (rc) return rc;
@@ -1313,7 +1376,7 @@ extern "C" int petch_trace_electrons(const void* mesh, int max_tris, int max_ver
     PETCH_REQUIRE(n >= 0 && max_tris > 0 && max_verts > 0, "petch_trace_electrons: bad size");
     cudaStream_t st = as_stream(stream);
     MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
-    ElectronShader sh{sigma, flux, 0};
+    ElectronShader sh{sigma, flux, tally_mode(false)};
     k_zero_faces<<<grid_for(max_tris, 256), 256, 0, st>>>(m.hdr, max_tris, flux, 1, nullptr, 0);
     PETCH_LAUNCH_CHECK("k_zero_faces");
     PETCH_CUDA(cudaMemsetAsync(work, 0, sizeof(int), st), "reset ray counter");
@@ -1324,7 +1387,7 @@ extern "C" int petch_trace_electrons(const void* mesh, int max_tris, int max_ver
                             "k_trace<electrons>");
     PETCH_DET_TAKE(a_f, (long long)max_tris);
     sh.flux = reinterpret_cast<float*>(a_f);
-    sh.det = 1;
+    sh.det = tally_mode(true);
     int rc = launch_trace(m, to_domain(dom), sh, seed, 0x656c6563u, n, work, st,
                           "k_trace<electrons>");
     if (rc) return rc;
@@ -1442,13 +1505,14 @@ int trace_batch(int kind, const petch_batch_item* items, const petch_batch_tange
     if (total == 0) return PETCH_OK;
     const uint32_t domain = ion ? 0x696f6e73u : 0x6e657500u;
     DetArena arena;
-    const int det = arena.on() ? 1 : 0;
+    const int det = tally_mode(arena.on());
+    const bool det_on = det & kTallyDet;
     const long long per_out = (ion ? 4LL : 1LL) * max_tris;
     long long* acc_out[kMaxBatch] = {};
     long long* acc_ang[kMaxBatch] = {};
     long long* acc_d[kMaxBatch] = {};
     long long* acc_d2[kMaxBatch] = {};
-    if (det) {
+    if (det_on) {
         for (int b = 0; b < B; ++b) {
             PETCH_DET_TAKE(ao, per_out);
             acc_out[b] = ao;
@@ -1483,7 +1547,7 @@ int trace_batch(int kind, const petch_batch_item* items, const petch_batch_tange
     }
 #undef PETCH_LB
     PETCH_LAUNCH_CHECK("k_trace_batch");
-    if (det) {
+    if (det_on) {
         for (int b = 0; b < B; ++b) {
             PETCH_DET_CONVERT(acc_out[b], items[b].out, per_out);
             if (ion || pair) PETCH_DET_CONVERT(acc_ang[b], items[b].ang, (long long)max_tris);
@@ -1563,7 +1627,7 @@ extern "C" int petch_trace_redep(const void* mesh, int max_tris, int max_verts,
     PETCH_CUDA(cudaMemsetAsync(work, 0, sizeof(int), st), "reset ray counter");
     if (n == 0) return PETCH_OK;
     RedepShader sh;
-    sh.rr = NeutralShader{nullptr, s_redep, flux, 0};
+    sh.rr = NeutralShader{nullptr, s_redep, flux, tally_mode(false)};
     sh.cdf = cdf;
     sh.fn = fn;
     Domain D = to_domain(dom);
@@ -1573,7 +1637,7 @@ extern "C" int petch_trace_redep(const void* mesh, int max_tris, int max_verts,
         return launch_trace(m, D, sh, seed, 0x72656470u, n, work, st, "k_trace<redeposition>");
     PETCH_DET_TAKE(a_f, (long long)max_tris);
     sh.rr.flux = reinterpret_cast<float*>(a_f);
-    sh.rr.det = 1;
+    sh.rr.det = tally_mode(true);
     int rc = launch_trace(m, D, sh, seed, 0x72656470u, n, work, st, "k_trace<redeposition>");
     if (rc) return rc;
     PETCH_DET_CONVERT(a_f, flux, (long long)max_tris);
@@ -1610,7 +1674,7 @@ extern "C" int petch_trace_ions_tangent(const void* mesh, int max_tris, int max_
     sh.tal4 = (float4*)tally4;
     sh.ang = ang;
     sh.dtal = dtal;
-    sh.det = 0;
+    sh.det = tally_mode(false);
     k_zero_faces<<<grid_for(4LL * max_tris, 256), 256, 0, st>>>(m.hdr, max_tris, tally4, 4, ang, 1);
     PETCH_LAUNCH_CHECK("k_zero_faces");
     PETCH_CUDA(cudaMemsetAsync(dtal, 0, sizeof(float) * 3 * (size_t)max_tris, st), "zero dtal");
@@ -1626,7 +1690,7 @@ extern "C" int petch_trace_ions_tangent(const void* mesh, int max_tris, int max_
     sh.tal4 = reinterpret_cast<float4*>(a_t);
     sh.ang = reinterpret_cast<float*>(a_a);
     sh.dtal = reinterpret_cast<float*>(a_d);
-    sh.det = 1;
+    sh.det = tally_mode(true);
     int rc = launch_trace(m, to_domain(dom), sh, seed, 0x696f6e73u, n_ion, work, st,
                           "k_trace<ions, tangent>");
     if (rc) return rc;
@@ -1653,7 +1717,7 @@ extern "C" int petch_trace_neutral_pair_tangent(const void* mesh, int max_tris, 
     MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
     const uint32_t domain = 0x6e657500u ^ stream_id;
     NeutralTanPairShader sh{bare, dbare, beta_a, beta_b, flux_a, dflux_a, flux_b, dflux_b,
-                            seed_b, domain, n_neu, 0};
+                            seed_b, domain, n_neu, tally_mode(false)};
     k_zero_faces<<<grid_for(max_tris, 256), 256, 0, st>>>(m.hdr, max_tris, flux_a, 1, flux_b, 1);
     PETCH_LAUNCH_CHECK("k_zero_faces");
     PETCH_CUDA(cudaMemsetAsync(dflux_a, 0, sizeof(float) * 3 * (size_t)max_tris, st), "zero dflux");
@@ -1672,7 +1736,7 @@ extern "C" int petch_trace_neutral_pair_tangent(const void* mesh, int max_tris, 
     sh.dflux_a = reinterpret_cast<float*>(a_da);
     sh.flux_b = reinterpret_cast<float*>(a_fb);
     sh.dflux_b = reinterpret_cast<float*>(a_db);
-    sh.det = 1;
+    sh.det = tally_mode(true);
     int rc = launch_trace(m, to_domain(dom), sh, seed_a, domain, 2 * n_neu, work, st,
                           "k_trace<neutral pair, tangent>");
     if (rc) return rc;
@@ -1693,7 +1757,7 @@ extern "C" int petch_trace_neutrals_tangent(const void* mesh, int max_tris, int 
                   "petch_trace_neutrals_tangent: bad size");
     cudaStream_t st = as_stream(stream);
     MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
-    NeutralTanShader sh{bare, dbare, beta, flux, dflux, 0};
+    NeutralTanShader sh{bare, dbare, beta, flux, dflux, tally_mode(false)};
     k_zero_faces<<<grid_for(max_tris, 256), 256, 0, st>>>(m.hdr, max_tris, flux, 1, nullptr, 0);
     PETCH_LAUNCH_CHECK("k_zero_faces");
     PETCH_CUDA(cudaMemsetAsync(dflux, 0, sizeof(float) * 3 * (size_t)max_tris, st), "zero dflux");
@@ -1707,7 +1771,7 @@ extern "C" int petch_trace_neutrals_tangent(const void* mesh, int max_tris, int 
     PETCH_DET_TAKE(a_d, 3LL * max_tris);
     sh.flux = reinterpret_cast<float*>(a_f);
     sh.dflux = reinterpret_cast<float*>(a_d);
-    sh.det = 1;
+    sh.det = tally_mode(true);
     int rc = launch_trace(m, to_domain(dom), sh, seed, 0x6e657500u ^ stream_id, n_neu, work, st,
                           "k_trace<neutrals, tangent>");
     if (rc) return rc;
@@ -1726,7 +1790,8 @@ extern "C" int petch_trace_legacy(const void* mesh, int max_tris, int max_verts,
                   "petch_trace_legacy: bad size");
     cudaStream_t st = as_stream(stream);
     MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
-    LegacyShader sh{ion, n_reemit, specular, sigma, sticking, cos_thr, eta, flux, angacc, 0};
+    LegacyShader sh{ion, n_reemit, specular, sigma, sticking, cos_thr, eta, flux, angacc,
+                    tally_mode(false)};
     k_zero_faces<<<grid_for(max_tris, 256), 256, 0, st>>>(m.hdr, max_tris, flux, 1, angacc, 1);
     PETCH_LAUNCH_CHECK("k_zero_faces");
     PETCH_CUDA(cudaMemsetAsync(work, 0, sizeof(int), st), "reset ray counter");
@@ -1741,7 +1806,7 @@ extern "C" int petch_trace_legacy(const void* mesh, int max_tris, int max_verts,
     PETCH_DET_TAKE(a_a, (long long)max_tris);
     sh.flux = reinterpret_cast<float*>(a_f);
     sh.angacc = reinterpret_cast<float*>(a_a);
-    sh.det = 1;
+    sh.det = tally_mode(true);
     int rc = launch_trace(m, D, sh, seed, ion ? 0x6c696f6eu : 0x6c6e6575u, n, work, st,
                           "k_trace<legacy>");
     if (rc) return rc;

@@ -287,18 +287,36 @@ __device__ __forceinline__ float qbyte(uint32_t lo4, uint32_t hi4, int k) {
     return (float)((w >> (8 * (k & 3))) & 255u);
 }
 
-// Pop the nearest stacked entry that can still beat the current hit; false if none.
-__device__ __forceinline__ bool query_pop(Query& q, const int* st_ref, const float* st_t) {
-    while (q.sp > 0) {
-        --q.sp;
-        if (st_t[q.sp] <= q.t) {
-            q.cur = st_ref[q.sp];
-            return true;
+// Traversal stack: (node ref, entry distance) pairs in the lane's local memory, at most kWStack
+// deep (deeper pushes set error bit 1).  pop() takes the nearest stacked entry that can still
+// beat the current hit (entries beyond it are dropped without a fetch); false if none is left.
+// (A variant holding the top 4 or 8 entries in shared memory was measured on the trench
+// workload: 2-4 % slower, since its shared memory comes out of the L1 that caches the tree.)
+struct LocalStack {
+    int ref[kWStack];
+    float t[kWStack];
+    __device__ __forceinline__ void push(Query& q, int r, float tt, int* err) {
+        if (q.sp < kWStack) {
+            ref[q.sp] = r;
+            t[q.sp] = tt;
+            ++q.sp;
+        } else {
+            *err |= 1;
         }
     }
-    q.cur = kDone;
-    return false;
-}
+    __device__ __forceinline__ bool pop(Query& q) {
+        while (q.sp > 0) {
+            --q.sp;
+            if (t[q.sp] <= q.t) {
+                q.cur = ref[q.sp];
+                return true;
+            }
+        }
+        q.cur = kDone;
+        return false;
+    }
+};
+
 
 __device__ __forceinline__ void query_leaf(const Tracer& T, Query& q, int f0, int f1) {
     for (int f = f0; f < f1; ++f)
@@ -307,8 +325,8 @@ __device__ __forceinline__ void query_leaf(const Tracer& T, Query& q, int f0, in
 }
 
 // One step of the 8-wide traversal; returns true once the query has finished.
-__device__ __forceinline__ bool step_wide(const Tracer& T, Query& q, int* st_ref, float* st_t,
-                                          int* err) {
+template <class St>
+__device__ __forceinline__ bool step_wide(const Tracer& T, Query& q, St& st, int* err) {
     if (q.cur == kDone) return true;
     if (++q.visits > kMaxVisits) {
         *err |= 1;
@@ -364,15 +382,7 @@ __device__ __forceinline__ bool step_wide(const Tracer& T, Query& q, int* st_ref
                 cas(key[5], ch[5], key[6], ch[6]);
 #pragma unroll
                 for (int k = 7; k >= 1; --k)
-                    if (k < nh) {
-                        if (q.sp < kWStack) {
-                            st_ref[q.sp] = ch[k];
-                            st_t[q.sp] = key[k];
-                            ++q.sp;
-                        } else {
-                            *err |= 1;
-                        }
-                    }
+                    if (k < nh) st.push(q, ch[k], key[k], err);
                 q.cur = ch[0];
             } else {
                 int c = ch[0];
@@ -387,12 +397,12 @@ __device__ __forceinline__ bool step_wide(const Tracer& T, Query& q, int* st_ref
         int f0 = code >> 3;
         query_leaf(T, q, f0, f0 + (code & 7));
     }
-    return !query_pop(q, st_ref, st_t);
+    return !st.pop(q);
 }
 
 // One step of the binary traversal; returns true once the query has finished.
-__device__ __forceinline__ bool step_binary(const Tracer& T, Query& q, int* st_ref, float* st_t,
-                                            int* err) {
+template <class St>
+__device__ __forceinline__ bool step_binary(const Tracer& T, Query& q, St& st, int* err) {
     if (q.cur == kDone) return true;
     if (++q.visits > kMaxVisits) {
         *err |= 1;
@@ -409,13 +419,7 @@ __device__ __forceinline__ bool step_binary(const Tracer& T, Query& q, int* st_r
         int c0 = __float_as_int(n3.x), c1 = __float_as_int(n3.y);
         if (h0 && h1) {
             bool swap = t1 < t0;
-            if (q.sp < kWStack) {
-                st_ref[q.sp] = swap ? c0 : c1;
-                st_t[q.sp] = swap ? t0 : t1;
-                ++q.sp;
-            } else {
-                *err |= 1;
-            }
+            st.push(q, swap ? c0 : c1, swap ? t0 : t1, err);
             q.cur = swap ? c1 : c0;
             return false;
         }
@@ -427,7 +431,7 @@ __device__ __forceinline__ bool step_binary(const Tracer& T, Query& q, int* st_r
         int l = ~node;
         query_leaf(T, q, __ldg(T.m.leaf_start + l), __ldg(T.m.leaf_start + l + 1));
     }
-    return !query_pop(q, st_ref, st_t);
+    return !st.pop(q);
 }
 
 // Stage the top of the wide tree in shared memory (call from every thread of the block).

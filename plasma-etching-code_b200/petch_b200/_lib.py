@@ -70,6 +70,22 @@ class BatchTangentGrid(ctypes.Structure):
                 ("mask", ctypes.c_void_p), ("du_a", ctypes.c_void_p), ("du_b", ctypes.c_void_p)]
 
 
+class StepConfig(ctypes.Structure):
+    """petch_step_config."""
+    _fields_ = [("nx", I), ("ny", I), ("nz", I), ("dx", D), ("Lx", D), ("Ly", D), ("Lz", D),
+                ("sub_top", D), ("mask_th", D), ("trench_width", D), ("hole", I), ("dt", D),
+                ("n_ion", I), ("n_neu", I), ("seed_offset", I), ("max_tris", I), ("n_fp", I),
+                ("warm_start", I), ("n_smooth", I), ("smooth_alpha", F), ("betaE", F),
+                ("betaO", F), ("dom", Domain), ("ion", IonParams), ("chem", ChemParams)]
+
+
+class StepStatus(ctypes.Structure):
+    """petch_step_status."""
+    _fields_ = [("steps", I), ("faces", I), ("max_faces", I), ("trace_errors", I),
+                ("mesh_errors", I), ("nonfinite", I), ("nsub", I), ("vmax", F),
+                ("queries", L)]
+
+
 DP = ctypes.POINTER(Domain)
 IP = ctypes.POINTER(IonParams)
 CP = ctypes.POINTER(ChemParams)
@@ -101,6 +117,7 @@ SIGNATURES = {
     "petch_advect_sparse": [P, P, P, P, P, I, P, I, I, I, I, F, F, I, P],
     "petch_raycast": [P, I, I, P, P, I, F, P, P, P, P],
     "petch_tracer_config": [I, I, I],
+    "petch_tally_aggregation": [I],
     "petch_nearest_face": [P, I, I, P, I, F, P, P, P],
     "petch_gas_normals": [P, I, I, P, I, I, I, D, P, P],
     "petch_trace_ff": [P, I, I, DP, P, U, I, P, P, P],
@@ -151,6 +168,11 @@ SIGNATURES = {
     "petch_batch_reinit_tangent": [P, P, I, D, P],
     "petch_extend_velocity_dual": [P, I, I, P, P, I, I, I, D, D, P, P, P, P, I, P, P, I, P, P],
     "petch_warmstart_dual": [P, I, I, P, P, P, I, I, P, P, P, P],
+    "petch_plan": [ctypes.POINTER(StepConfig), P, I, ctypes.POINTER(P), P],
+    "petch_step": [P, P],
+    "petch_plan_status": [P, ctypes.POINTER(StepStatus), P],
+    "petch_plan_seek": [P, L],
+    "petch_destroy": [P],
 }
 
 # The library's tracer configuration at load (bvh_width, steps_per_round, keep_lanes): what

@@ -35,8 +35,27 @@ def test_abi_version():
     ("petch_advect", [None, None, None, None, None, 4, 4, 4, 1.0, 0.1, 1, None]),
     ("petch_reinit_eik", [None, None, None, None, 4, 4, 4, 0.25, 1.0, 1.0, 3, 0, None]),
     ("petch_seed_level_set", [None, None, 4, 4, 4, 0.25, 1.0, 1.0, 0.5, 0.2, 0.4, 1, None]),
+    ("petch_plan", [None, None, 1, None, None]),
+    ("petch_step", [None, None]),
+    ("petch_plan_status", [None, None, None]),
+    ("petch_plan_seek", [None, 0]),
 ])
 def test_null_pointers_rejected(name, args):
     rc = getattr(_lib.lib(), name)(*args)
     assert rc == 1  # PETCH_E_INVALID
     assert "null" in _lib.last_error()
+
+
+def test_plan_rejects_bad_configuration_before_touching_the_device():
+    """petch_plan checks the configuration first: a bad grid or ray count is PETCH_E_INVALID with
+    a message, and nothing is allocated (no GPU needed)."""
+    c = _lib.StepConfig()
+    c.nx, c.ny, c.nz, c.dx, c.dt, c.max_tris = 0, 4, 4, 0.25, 0.1, 1024
+    h = ctypes.c_void_p()
+    phi = ctypes.c_float(0.0)
+    rc = _lib.lib().petch_plan(ctypes.byref(c), ctypes.addressof(phi), 1, ctypes.byref(h), None)
+    assert rc == 1 and "bad grid" in _lib.last_error() and not h.value
+    c.nx, c.n_neu = 4, 1 << 29
+    rc = _lib.lib().petch_plan(ctypes.byref(c), ctypes.addressof(phi), 1, ctypes.byref(h), None)
+    assert rc == 1 and "ray counts" in _lib.last_error()
+    assert _lib.lib().petch_destroy(None) == 0

@@ -1,0 +1,192 @@
+"""Loop- and flux-level parity on the benchmark configurations.
+
+* Etch depth after every step within one grid cell of the oracle loop (oracle/oracle.py
+  run_etch_3d, the FP64 restatement of threed.py:1643-1795), on:
+  - the config-0 hole through the public API, Process(Domain.hole(14, 0.25, 6, 2, 18),
+    SF6O2(rate_scale=1.0), 3.0).run(40) (api.py:151-171), and at SF6O2's default rate_scale
+    0.025, where the front moves below the narrow-band speed limit and the depth follows the
+    fluxes;
+  - the 128 x 64 x 640 periodic trench of the headline benchmark (first 30 steps of its 100-step
+    schedule at 2^16 rays per species) with Monte-Carlo neutrals at rate_scale 1.0 and 0.1, and
+    with radiosity neutrals.
+  The oracle's depth histories are committed fixtures (tests/golden/loop.npz, written by
+  tests/golden/make_loop_golden.py).  The device and the oracle draw independent random streams.
+
+* Per-triangle flux on the config-0 mesh at the reference's 30 000 rays per launch against the
+  oracle at 2^23 rays (280x): the seed-averaged device tallies (256 seeds) agree with the oracle
+  per face within 3 sigma, and their relative L2 distance from the oracle, after the measured
+  Monte-Carlo noise of both sides is taken out in quadrature, is at most 2 %.  (That excess
+  estimate has its own noise floor, about noise x (2 / faces)^(1/4): with these counts ~0.5 %,
+  well under the 2 % bound.)
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle.oracle as orc
+import petch_b200 as petch
+from conftest import GOLDEN
+from gpu_helpers import cuda_ions, cuda_mesh, cuda_neutrals
+from petch_b200 import _lib, params
+from petch_b200 import threed as t3
+
+pytestmark = pytest.mark.gpu
+
+SF6O2_FLAGS = dict(chemistry="belen", yield_angular="viennaps", coverage_sticking=True,
+                   warm_start_coverage=True, sampling="sobol", ion_reflection=True)
+
+
+@pytest.fixture(scope="module")
+def gold():
+    return np.load(os.path.join(GOLDEN, "loop.npz"))
+
+
+def _case(gold, name):
+    return json.loads(str(gold[f"{name}_case"])), gold[f"{name}_hist"]
+
+
+def _device_history(case, deterministic=False):
+    g = case['geo']
+    par = dict(params.PAR, **case['par'])
+    fl = params.Flags(neutral_transport=case['transport'], **SF6O2_FLAGS)
+    geo = t3.run_etch_3d(Lx=g['Lx'], Ly=g['Ly'], Lz=g['Lz'], dx=g['dx'],
+                         trench_width=g['trench_width'], mask_th=g['mask_th'],
+                         sub_top=g['sub_top'], hole=g['hole'], t_end=g['t_end'],
+                         n_steps=g['n_steps'], par=par, flags=fl, n_ion=case['rays'],
+                         n_neu=case['rays'], reinit_method="fsm", verbose=False,
+                         record_depth_every=1)
+    return geo
+
+
+def _check_history(dev_hist, orc_hist, dx):
+    dev = dict(dev_hist)
+    assert sorted(dev) == [int(s) for s in orc_hist[:, 0]]
+    worst = 0.0
+    for s, d_orc in orc_hist:
+        diff = abs(dev[int(s)] - d_orc)
+        worst = max(worst, diff)
+        assert diff <= dx + 1e-9, (int(s), dev[int(s)], d_orc,
+                                   [dev[int(t)] for t in orc_hist[:, 0]], list(orc_hist[:, 1]))
+    print(f"depth history: {len(orc_hist)} steps, worst |device - oracle| {worst:.4f} um "
+          f"(dx {dx}), final {dev[int(orc_hist[-1, 0])]:.4f} vs {orc_hist[-1, 1]:.4f}")
+    return worst
+
+
+@pytest.mark.parametrize("name", ["c0_rs1", "c0_rs025"])
+def test_config0_process_depth_history(gold, name):
+    """The config-0 hole through Process.run and run_etch_3d: with deterministic tallies the two
+    calls are the same computation (level sets equal bit for bit), so run_etch_3d's per-step
+    depth history is the Process run's; every step within one cell of the oracle loop."""
+    case, hist = _case(gold, name)
+    g = case['geo']
+    dom = petch.Domain.hole(extent=g['Lx'], dx=g['dx'], diameter=g['trench_width'],
+                            mask=g['mask_th'], depth=g['sub_top'])
+    assert dom._geo['Lz'] == g['Lz']
+    _lib.set_deterministic(16 * t3.default_capacity((56, 56, 96)))
+    try:
+        res = petch.Process(dom, petch.SF6O2(rate_scale=case['par']['rate_scale']),
+                            duration=g['t_end']).run(steps=g['n_steps'])
+        geo = _device_history(case)
+    finally:
+        _lib.set_deterministic(0)
+    np.testing.assert_array_equal(res.phi, geo['phi'])
+    _check_history(geo['depth_history'], hist, g['dx'])
+    assert abs(res.depth - hist[-1, 1]) <= g['dx'] + 1e-9
+    assert hist[-1, 1] >= 2.0          # the hole etched (3 um at rate_scale 0.025, 18 at 1.0)
+
+
+@pytest.mark.parametrize("name", ["c1_mc", "c1_mc_rs01", "c1_rad"])
+def test_config1_trench_depth_history(gold, name):
+    """The headline trench (128 x 64 x 640), first 30 steps of the 100-step schedule at 2^16
+    rays per species: every step within one cell (0.0625 um) of the oracle loop."""
+    case, hist = _case(gold, name)
+    geo = _device_history(case)
+    _check_history(geo['depth_history'], hist, case['geo']['dx'])
+    assert hist[-1, 1] >= 0.5
+
+
+# ---------------------------------------------------------------------------------------------
+# per-triangle flux gate on config-0 meshes
+# ---------------------------------------------------------------------------------------------
+N_REF_RAYS = 30000          # Process's default rays per launch (api.py:156)
+N_SEEDS = 256
+N_ORACLE = 1 << 23
+
+
+@pytest.fixture(scope="module")
+def c0_meshes(gold):
+    """The config-0 seed field, and the level set after 10 oracle steps at rate_scale 1.0 (a
+    7.75 um deep hole): device and oracle meshes of the same field (identical topology)."""
+    case, _ = _case(gold, "c0_rs1")
+    g = case['geo']
+    par = dict(params.PAR, rate_scale=1.0)
+    fl = params.Flags(**SF6O2_FLAGS)
+    out = {}
+    phi_seed, _ = orc.seed(56, 56, 96, g['dx'], g['Lx'], g['Ly'], g['sub_top'], g['mask_th'],
+                           g['trench_width'], True)
+    out['seed'] = orc.seed_distance(phi_seed.astype(np.float32), g['dx']).astype(np.float32)
+    phi10, _, _ = orc.run_etch_3d(g['Lx'], g['Ly'], g['Lz'], g['dx'], g['trench_width'],
+                                  g['mask_th'], g['sub_top'], g['t_end'], g['n_steps'], True, par,
+                                  fl, N_REF_RAYS, N_REF_RAYS, steps=10)
+    out['etched'] = phi10.astype(np.float32)
+    geo = dict(Lx=g['Lx'], Ly=g['Ly'], Lz=g['Lz'], dx=g['dx'], sub_top=g['sub_top'],
+               mask_th=g['mask_th'], trench_width=g['trench_width'], hole=True, periodic_y=0)
+    return out, geo
+
+
+def _gate(runs, ref, n, N):
+    """runs: (S, F) per-seed device tallies at n rays; ref: (F,) oracle tallies at N rays.
+    Returns (bias, frac_3sigma, mean_z2, n_faces_tested)."""
+    S = runs.shape[0]
+    r = ref * (n / N)                              # oracle on the device runs' scale
+    xb = runs.mean(0)
+    var1 = runs.var(0, ddof=1)                     # one device run's per-face variance
+    var_mean = var1 / S                            # of the seed mean
+    var_ref = var1 * (n / N)                       # of the scaled oracle (same estimator)
+    denom = np.sum(r ** 2)
+    err2 = np.sum((xb - r) ** 2) / denom
+    noise2 = np.sum(var_mean + var_ref) / denom
+    bias = float(np.sqrt(max(err2 - noise2, 0.0)))
+    k = S * xb >= 30.0                             # faces with enough deposits for a z test
+    z = (xb[k] - r[k]) / np.sqrt(var_mean[k] + var_ref[k])
+    return bias, float(np.mean(np.abs(z) > 3.0)), float(np.mean(z ** 2)), int(k.sum())
+
+
+@pytest.mark.parametrize("which", ["seed", "etched"])
+def test_config0_neutral_flux_gate(c0_meshes, which):
+    fields, geo = c0_meshes
+    phi = fields[which]
+    m = cuda_mesh(phi, geo['dx'], geo)
+    o = orc.mesh_build(phi, geo['dx'], geo)
+    assert o.F == m.F
+    bare = np.random.default_rng(3).uniform(0.05, 1.0, m.F)
+    for beta in (0.7, 1.0):
+        runs = np.stack([cuda_neutrals(m, geo, bare, beta, 1000 + s, N_REF_RAYS)
+                         for s in range(N_SEEDS)])
+        ref = orc.trace_neutrals(o, geo, geo, bare, beta, 77, N_ORACLE)
+        bias, frac3, mz2, nf = _gate(runs, ref, N_REF_RAYS, N_ORACLE)
+        print(f"neutral {which} beta {beta}: bias {bias:.4f}, |z|>3 {frac3:.4f}, "
+              f"mean z^2 {mz2:.3f}, faces {nf} of {m.F}")
+        assert nf > 1000
+        assert bias <= 0.02, (which, beta, bias)
+        assert frac3 <= 0.01 and mz2 <= 1.3, (which, beta, frac3, mz2)
+
+
+@pytest.mark.parametrize("which", ["seed", "etched"])
+def test_config0_ion_flux_gate(c0_meshes, which):
+    fields, geo = c0_meshes
+    phi = fields[which]
+    m = cuda_mesh(phi, geo['dx'], geo)
+    o = orc.mesh_build(phi, geo['dx'], geo)
+    par = dict(params.PAR, periodic_y=0)
+    runs = np.stack([cuda_ions(m, geo, par, 2000 + s, N_REF_RAYS) for s in range(N_SEEDS)])
+    ref = orc.trace_ions(o, geo, par, 99, N_ORACLE)
+    for q in range(5):
+        bias, frac3, mz2, nf = _gate(runs[:, :, q], ref[:, q], N_REF_RAYS, N_ORACLE)
+        print(f"ion {which} tally {q}: bias {bias:.4f}, |z|>3 {frac3:.4f}, mean z^2 {mz2:.3f}, "
+              f"faces {nf} of {m.F}")
+        assert nf > 200
+        assert bias <= 0.02, (which, q, bias)
+        assert frac3 <= 0.01 and mz2 <= 1.3, (which, q, frac3, mz2)
