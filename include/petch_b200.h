@@ -87,7 +87,9 @@ int petch_reinit_eik(const float* phi_in, float* phi_out, float* u_a, float* u_b
  * The two Eikonal scratch grids live in a fixed device array of the library (16 MiB held by
  * every GPU that loads it, until exit), so the grid may have at most 2,097,152 cells; larger
  * grids are rejected with PETCH_E_INVALID.  Allocates nothing.  The first call on a device looks
- * up the array's device address (cudaGetSymbolAddress); make it before any stream capture.
+ * up the array's device address (cudaGetSymbolAddress); make it before any stream capture.  The
+ * address is kept for the life of the process: do not call it again after cudaDeviceReset (or
+ * any destruction of the device's primary context), which may move the array.
  * Calls share the array: calls whose kernels overlap on the GPU race.  Same arguments and
  * results as petch_reinit_eik otherwise. */
 int petch_reinit_eik_noalloc(const float* phi_in, float* phi_out, int nx, int ny, int nz,

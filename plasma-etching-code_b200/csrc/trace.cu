@@ -101,19 +101,22 @@ __device__ __forceinline__ float3 cosine_emit(Rng& g, float3 n) {
     return (st * cosf(ph)) * t + (st * sinf(ph)) * b + ct * n;
 }
 
-// Warp-cooperative refill: lanes with ray == -1 take consecutive ids from *counter.
+// Warp-cooperative refill: lanes with ray == -1 take consecutive ids from *counter.  The counter
+// is advanced in unsigned arithmetic: lanes that find the pool empty still advance it (each lane
+// at most once, since a lane with ray == -2 never asks again), so it ends at most one id per
+// resident lane above n, far below 2^32 for any n < 2^31, and no id wraps back below n.
 __device__ __forceinline__ bool refill(int& ray, int n, int* counter) {
     const int lane = threadIdx.x & 31;
     bool need = (ray == -1);
     unsigned mask = __ballot_sync(kFull, need);
     if (mask) {
         int leader = __ffs(mask) - 1;
-        int base = 0;
-        if (lane == leader) base = atomicAdd(counter, __popc(mask));
+        unsigned base = 0;
+        if (lane == leader) base = atomicAdd(reinterpret_cast<unsigned*>(counter), (unsigned)__popc(mask));
         base = __shfl_sync(kFull, base, leader);
         if (need) {
-            int idx = base + __popc(mask & ((1u << lane) - 1u));
-            ray = idx < n ? idx : -2;
+            const unsigned idx = base + (unsigned)__popc(mask & ((1u << lane) - 1u));
+            ray = idx < (unsigned)n ? (int)idx : -2;
             return ray >= 0;
         }
     }

@@ -8,7 +8,11 @@
 Same constructors, defaults and properties as the reference (petch/api.py:24-171); Process.run
 drives run_etch_3d on the GPU engine with the reference's config (reinit_method="fsm").
 """
+import io
+import os
 import time
+
+import numpy as np
 
 from . import threed as _t3
 from .params import PAR, Flags
@@ -87,47 +91,69 @@ class Result:
         return v, f
 
     def plot(self, path=None, show=False):
-        """Matplotlib x-z cross-section through the feature centre (if matplotlib is present)."""
+        """The etch profile in the x-z plane through the feature centre: the gas region shaded,
+        the front (phi = 0) in red, the fronts of recorded frames (run_etch_3d(record_frames=
+        True)) in grey, the substrate top dotted.  Returns the matplotlib Axes; `path` writes a
+        PNG, `show` opens a window."""
         import matplotlib
         if path is not None and not show:
             matplotlib.use("Agg")
         import matplotlib.pyplot as plt
         g = self._geo
-        jc = g['phi'].shape[1] // 2
-        phi = g['phi'][:, jc, :].T
-        fig, ax = plt.subplots(figsize=(5, 4))
-        ax.contourf(g['xs'], g['zs'], (phi < 0).astype(float), levels=[0.5, 1.5], colors=["#cfe8ff"])
-        ax.contour(g['xs'], g['zs'], phi, levels=[0.0], colors="k", linewidths=1.2)
-        ax.axhline(g['sub_top'], color="0.6", lw=0.6, ls="--")
-        ax.set_xlabel("x (um)")
-        ax.set_ylabel("z (um)")
-        ax.set_title(f"depth {self.depth:.1f} um  AR {self.aspect_ratio:.1f}  ({self.wall_time:.1f}s)")
-        ax.set_aspect("equal")
+        x, z = np.asarray(g['xs']), np.asarray(g['zs'])
+        phi = np.asarray(g['phi'])
+        xz = phi[:, phi.shape[1] // 2, :]
+        aspect = (z[-1] - z[0]) / max(x[-1] - x[0], 1e-9)
+        fig, ax = plt.subplots(figsize=(4.8, min(max(4.8 * aspect, 3.0), 9.0)))
+        ax.imshow((xz < 0).T, origin="lower", extent=(x[0], x[-1], z[0], z[-1]), cmap="Blues",
+                  vmin=0.0, vmax=2.5, interpolation="nearest", aspect="auto")
+        for fr in g.get('frames', ()):
+            ax.contour(x, z, np.asarray(fr['phi_xz']).T, levels=[0.0], colors="0.65",
+                       linewidths=0.5)
+        ax.contour(x, z, xz.T, levels=[0.0], colors="crimson", linewidths=1.0)
+        ax.plot([x[0], x[-1]], [g['sub_top'], g['sub_top']], ":", color="0.35", lw=0.8)
+        ax.set_xlabel("x [um]")
+        ax.set_ylabel("z [um]")
+        ax.set_title(f"centre depth {self.depth:.2f} um, max {self.max_depth:.2f} um, "
+                     f"AR {self.aspect_ratio:.2f}", fontsize=9)
         if path is not None:
-            fig.tight_layout()
-            fig.savefig(path, dpi=130)
+            fig.savefig(path, dpi=120, bbox_inches="tight")
         if show:
             plt.show()
         return ax
 
     def save(self, path):
-        """Write the surface mesh to `path`: legacy ASCII VTK PolyData, or Wavefront .obj."""
+        """Write the surface mesh to `path`: Wavefront OBJ for a .obj suffix, legacy ASCII VTK
+        PolyData (readable by ParaView / ViennaPS) otherwise."""
         v, f = self.mesh
+        writer = _MESH_WRITERS.get(os.path.splitext(str(path))[1].lower(), _vtk_polydata)
         with open(path, "w") as fh:
-            if str(path).lower().endswith(".obj"):
-                for p in v:
-                    fh.write(f"v {p[0]} {p[1]} {p[2]}\n")
-                for t in f:
-                    fh.write(f"f {t[0] + 1} {t[1] + 1} {t[2] + 1}\n")
-            else:
-                fh.write("# vtk DataFile Version 3.0\npetch surface\nASCII\nDATASET POLYDATA\n")
-                fh.write(f"POINTS {len(v)} float\n")
-                for p in v:
-                    fh.write(f"{p[0]} {p[1]} {p[2]}\n")
-                fh.write(f"POLYGONS {len(f)} {4 * len(f)}\n")
-                for t in f:
-                    fh.write(f"3 {int(t[0])} {int(t[1])} {int(t[2])}\n")
+            fh.write(writer(np.asarray(v, np.float32), np.asarray(f, np.int64)))
         return path
+
+
+def _table(rows, fmt):
+    """Rows of a numeric array as text, one line each (numpy formatting)."""
+    buf = io.StringIO()
+    if len(rows):
+        np.savetxt(buf, rows, fmt=fmt)
+    return buf.getvalue()
+
+
+def _vtk_polydata(v, f):
+    """Legacy VTK PolyData: the points block, then one polygon record (3, i, j, k) per face."""
+    head = "# vtk DataFile Version 3.0\npetch surface\nASCII\nDATASET POLYDATA\n"
+    polys = np.column_stack([np.full(len(f), 3, np.int64), f]) if len(f) else f
+    return (head + f"POINTS {len(v)} float\n" + _table(v, "%.9g")
+            + f"POLYGONS {len(f)} {4 * len(f)}\n" + _table(polys, "%d"))
+
+
+def _wavefront_obj(v, f):
+    """Wavefront OBJ: vertex records, then faces with 1-based indices."""
+    return _table(v, "v %.9g %.9g %.9g") + _table(f + 1, "f %d %d %d")
+
+
+_MESH_WRITERS = {".obj": _wavefront_obj, ".vtk": _vtk_polydata}
 
 
 class Process:

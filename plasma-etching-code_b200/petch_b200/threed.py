@@ -751,6 +751,11 @@ def run_etch_3d(Lx=10.0, Ly=4.0, Lz=14.0, dx=0.4, trench_width=4.0, mask_th=2.0,
     if flags is None:
         flags = DEFAULT_FLAGS
     _unsupported(flags, par)
+    if reinit_method in ("skfmm", "skfmm_full"):
+        warnings.warn(f"reinit_method={reinit_method!r} (scikit-fmm's fast marching, "
+                      "threed.py:1538-1549) runs as the device Jacobi Godunov-Eikonal reinit "
+                      "('fsm'): pass reinit_method='fsm' to silence this", UserWarning,
+                      stacklevel=2)
     nt = getattr(flags, "neutral_transport", "mc")
     hooks = hooks or {}
     mc_par = par
@@ -882,7 +887,9 @@ def _floor_indices(phi, ii, jj):
         nx, ny, nz = phi.shape
         if len(ii) == 0:
             return np.zeros(0, np.int64)
-        src = phi if phi.dtype == torch.float32 else phi.float()
+        # the scan tests phi < 0; a float64 field is reduced to its sign first (a float32 cast
+        # would turn negatives smaller than the float32 subnormals into -0.0, i.e. solid)
+        src = phi if phi.dtype == torch.float32 else torch.where(phi < 0, -1.0, 1.0).float()
         src = src.contiguous()
         cols = torch.from_numpy(np.stack([ii, jj], axis=1).astype(np.int32)).to(src.device)
         out = torch.empty(len(ii), dtype=torch.int32, device=src.device)

@@ -2,9 +2,10 @@
 threed.py / belen.py / chemistry.py, unmodified) on small seeded inputs, with the third-party
 warp-lang replaced by warp_shim.py (a CPU stand-in: see its docstring for what it restates).
 
-Run in a checkout that has the reference at /root/reference (or $PETCH_REFERENCE):
+Point it at a checkout of the reference project (its root, the folder holding src/petch) with
+--reference or the PETCH_REFERENCE environment variable:
 
-    python tests/golden/make_golden.py [group ...]
+    python tests/golden/make_golden.py --reference <path> [group ...]
 
 groups: levelset surface flux radiosity options redep dda knudsen gmres electron
 
@@ -17,10 +18,26 @@ import time
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("PETCH_REFERENCE", "/root/reference")
 sys.path.insert(0, HERE)
 import warp_shim  # noqa: E402
 
+
+def _reference_root(argv):
+    """The reference checkout from --reference <path> (removed from argv) or PETCH_REFERENCE."""
+    if "--reference" in argv:
+        i = argv.index("--reference")
+        if i + 1 >= len(argv):
+            raise SystemExit("--reference needs a path")
+        root = argv[i + 1]
+        del argv[i:i + 2]
+        return root
+    root = os.environ.get("PETCH_REFERENCE")
+    if not root:
+        raise SystemExit("give the reference checkout with --reference <path> or PETCH_REFERENCE")
+    return root
+
+
+REF = _reference_root(sys.argv)
 t3 = warp_shim.install(os.path.join(REF, "src", "petch"))
 
 

@@ -16,7 +16,10 @@ warm-started coverage; FSM reinit; seed offset 0):
               sub_top 35), rate_scale 1.0, the first 30 steps of the 100-step 2.0 schedule,
               2^16 rays per species (MC neutrals)
   c1_mc_rs01  the same trench at rate_scale 0.1 (below the narrow-band limit)
-  c1_rad      the same trench, neutral_transport='radiosity', rate_scale 1.0, 2^16 ions
+  c1_rad      the same trench, neutral_transport='radiosity', rate_scale 1.0, 2^22 ions (the
+              benchmark's count: the radiosity path does not smooth the ion yields, and at 2^16
+              ions on ~5e4 faces the oracle's own runs with two seeds part by 8 cells)
+  c1_rad_rs01 the same at rate_scale 0.1
 
 Each case stores the oracle's centre depth after every step and the case's arguments (JSON).
 Only the oracle runs here (no reference checkout is needed); the tests read the .npz.
@@ -54,8 +57,10 @@ CASES = {
     "c1_mc": dict(geo=C1, par=dict(rate_scale=1.0, periodic_y=1), rays=1 << 16, transport="mc"),
     "c1_mc_rs01": dict(geo=C1, par=dict(rate_scale=0.1, periodic_y=1), rays=1 << 16,
                        transport="mc"),
-    "c1_rad": dict(geo=C1, par=dict(rate_scale=1.0, periodic_y=1), rays=1 << 16,
+    "c1_rad": dict(geo=C1, par=dict(rate_scale=1.0, periodic_y=1), rays=1 << 22,
                    transport="radiosity"),
+    "c1_rad_rs01": dict(geo=C1, par=dict(rate_scale=0.1, periodic_y=1), rays=1 << 22,
+                        transport="radiosity"),
 }
 
 

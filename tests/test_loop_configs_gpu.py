@@ -15,7 +15,9 @@
 * Per-triangle flux on the config-0 mesh at the reference's 30 000 rays per launch against the
   oracle at 2^23 rays (280x): the seed-averaged device tallies (256 seeds) agree with the oracle
   per face within 3 sigma, and their relative L2 distance from the oracle, after the measured
-  Monte-Carlo noise of both sides is taken out in quadrature, is at most 2 %.  (That excess
+  Monte-Carlo noise of both sides is taken out in quadrature, is at most 2 %.  Coincident twin
+  faces (the seed field's zero sheet under the mask) are compared as one (see
+  coincident_groups).  (That excess
   estimate has its own noise floor, about noise x (2 / faces)^(1/4): with these counts ~0.5 %,
   well under the 2 % bound.)
 """
@@ -97,10 +99,11 @@ def test_config0_process_depth_history(gold, name):
     assert hist[-1, 1] >= 2.0          # the hole etched (3 um at rate_scale 0.025, 18 at 1.0)
 
 
-@pytest.mark.parametrize("name", ["c1_mc", "c1_mc_rs01", "c1_rad"])
+@pytest.mark.parametrize("name", ["c1_mc", "c1_mc_rs01", "c1_rad", "c1_rad_rs01"])
 def test_config1_trench_depth_history(gold, name):
     """The headline trench (128 x 64 x 640), first 30 steps of the 100-step schedule at 2^16
-    rays per species: every step within one cell (0.0625 um) of the oracle loop."""
+    rays per species (radiosity: 2^22 ions): every step within one cell (0.0625 um) of the
+    oracle loop."""
     case, hist = _case(gold, name)
     geo = _device_history(case)
     _check_history(geo['depth_history'], hist, case['geo']['dx'])
@@ -136,9 +139,27 @@ def c0_meshes(gold):
     return out, geo
 
 
-def _gate(runs, ref, n, N):
-    """runs: (S, F) per-seed device tallies at n rays; ref: (F,) oracle tallies at N rays.
-    Returns (bias, frac_3sigma, mean_z2, n_faces_tested)."""
+def coincident_groups(verts, faces):
+    """Group id per face: faces with the same three vertex positions share a group.  The seed
+    field is exactly 0 on the whole plane z = sub_top, also under the mask, so marching cubes
+    emits two coincident sheets there (mask underside, substrate top), reachable by rays that
+    enter the open solid from the launch-plane strip beyond the mesh (threed.py:449 launches over
+    [0, Lx] x [0, Ly], the mesh spans [0, (n - 1) dx]).  A closest-hit query cannot tell
+    coincident twins apart: each traversal (this one, the oracle's, Warp's) breaks the tie its
+    own way, so the gate compares their sum."""
+    tri = np.round(np.asarray(verts)[np.asarray(faces)] * 1e5).astype(np.int64)
+    keys = {}
+    return np.array([keys.setdefault(tuple(sorted(map(tuple, t))), len(keys)) for t in tri])
+
+
+def _gate(runs, ref, n, N, groups=None):
+    """runs: (S, F) per-seed device tallies at n rays; ref: (F,) oracle tallies at N rays;
+    groups: faces summed together (coincident twins).  Returns (bias, frac_3sigma, mean_z2,
+    n_groups_tested)."""
+    if groups is not None:
+        G = int(groups.max()) + 1
+        runs = np.stack([np.bincount(groups, r, G) for r in runs])
+        ref = np.bincount(groups, ref, G)
     S = runs.shape[0]
     r = ref * (n / N)                              # oracle on the device runs' scale
     xb = runs.mean(0)
@@ -161,12 +182,14 @@ def test_config0_neutral_flux_gate(c0_meshes, which):
     m = cuda_mesh(phi, geo['dx'], geo)
     o = orc.mesh_build(phi, geo['dx'], geo)
     assert o.F == m.F
+    np.testing.assert_array_equal(m.faces[:m.F].cpu().numpy(), o.faces)
+    groups = coincident_groups(o.verts, o.faces)
     bare = np.random.default_rng(3).uniform(0.05, 1.0, m.F)
     for beta in (0.7, 1.0):
         runs = np.stack([cuda_neutrals(m, geo, bare, beta, 1000 + s, N_REF_RAYS)
                          for s in range(N_SEEDS)])
         ref = orc.trace_neutrals(o, geo, geo, bare, beta, 77, N_ORACLE)
-        bias, frac3, mz2, nf = _gate(runs, ref, N_REF_RAYS, N_ORACLE)
+        bias, frac3, mz2, nf = _gate(runs, ref, N_REF_RAYS, N_ORACLE, groups)
         print(f"neutral {which} beta {beta}: bias {bias:.4f}, |z|>3 {frac3:.4f}, "
               f"mean z^2 {mz2:.3f}, faces {nf} of {m.F}")
         assert nf > 1000
@@ -180,11 +203,13 @@ def test_config0_ion_flux_gate(c0_meshes, which):
     phi = fields[which]
     m = cuda_mesh(phi, geo['dx'], geo)
     o = orc.mesh_build(phi, geo['dx'], geo)
+    np.testing.assert_array_equal(m.faces[:m.F].cpu().numpy(), o.faces)
+    groups = coincident_groups(o.verts, o.faces)
     par = dict(params.PAR, periodic_y=0)
     runs = np.stack([cuda_ions(m, geo, par, 2000 + s, N_REF_RAYS) for s in range(N_SEEDS)])
     ref = orc.trace_ions(o, geo, par, 99, N_ORACLE)
     for q in range(5):
-        bias, frac3, mz2, nf = _gate(runs[:, :, q], ref[:, q], N_REF_RAYS, N_ORACLE)
+        bias, frac3, mz2, nf = _gate(runs[:, :, q], ref[:, q], N_REF_RAYS, N_ORACLE, groups)
         print(f"ion {which} tally {q}: bias {bias:.4f}, |z|>3 {frac3:.4f}, mean z^2 {mz2:.3f}, "
               f"faces {nf} of {m.F}")
         assert nf > 200

@@ -30,12 +30,16 @@ def _field(seed, nx=40, ny=36, nz=48, dx=0.25):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("mode", [0, 1])
-def test_noalloc_reinit_matches_caller_scratch_reinit_on_two_calls(mode):
+@pytest.mark.parametrize("mode,shape", [(0, (40, 36, 48)), (1, (40, 36, 48)),
+                                        (0, (128, 128, 128))],
+                         ids=["mode0", "mode1", "mode0-at-limit"])
+def test_noalloc_reinit_matches_caller_scratch_reinit_on_two_calls(mode, shape):
+    """Two calls in a row; the last case fills the fixed array exactly (2^21 cells per grid, the
+    second grid ending at the array's end)."""
     import torch
     stream = torch.cuda.current_stream().cuda_stream
     for seed in (1, 2):                                  # two calls in a row, different inputs
-        phi_np, dx = _field(seed)
+        phi_np, dx = _field(seed, *shape)
         phi = torch.from_numpy(phi_np).cuda()
         nx, ny, nz = phi.shape
         band = 6 * dx
@@ -59,3 +63,11 @@ def test_noalloc_reinit_rejects_grids_beyond_its_fixed_scratch():
                                              None)
     assert rc == 1                                       # PETCH_E_INVALID
     assert "exceeds the fixed scratch" in _lib.last_error()
+
+
+def test_noalloc_reinit_rejects_one_cell_past_the_limit():
+    """2^21 + 1 cells (one more than each fixed scratch grid holds) is rejected."""
+    dummy = ctypes.c_void_p(16)
+    rc = _lib.lib().petch_reinit_eik_noalloc(dummy, dummy, (1 << 21) + 1, 1, 1, 0.25, 2.5, 1.75,
+                                             10, 0, None)
+    assert rc == 1 and "exceeds the fixed scratch" in _lib.last_error()
