@@ -66,6 +66,11 @@ int petch_advect(float* phi, float* tmp, const float* F, const uint8_t* mask,
                  const float* mask_phi, int nx, int ny, int nz, float inv_dx, float dt_sub,
                  int nsub, void* stream);
 
+/* Block shape of the row-mapped level-set stencils (knob of the tuner, petch_b200.tune): bz
+ * threads along z (a multiple of 32) by br grid rows, bz * br <= 256; default 128 x 2.  Applies
+ * to later reinit calls (single grid, batched, allocation-free).  Results do not depend on it. */
+int petch_stencil_config(int bz, int br);
+
 /* Replaces reinit_fsm + _eik_init + _eik_jacobi + _eik_solve (petch/threed.py:1421-1537):
  * Russo-Smereka frozen interface distance, n_iter Jacobi Godunov-Eikonal sweeps, then
  * phi_out = sign(phi_in) * min(U, cap) with sign(0) = +1.  big = band + 4 dx and
@@ -156,6 +161,10 @@ int petch_tracer_config(int bvh_width, int steps_per_round, int keep_lanes);
  * 648-652).  Results are the same estimator (bit-equal with deterministic tallies); the choice is
  * a speed knob of the tuner. */
 int petch_tally_aggregation(int on);
+
+/* The tracer settings in force: out[0] BVH width, [1] steps per round, [2] keep lanes, [3]
+ * warp-aggregated deposits (0 / 1). */
+int petch_tracer_settings(int* out);
 
 /* Replaces _gen_source + _trace3d_ion_yield (petch/threed.py:441-458, 599-712): n_ion ions
  * generated and traced on the device.  tally4 (16-byte aligned float4[max_tris]) receives per

@@ -1132,14 +1132,20 @@ def depth3d(geo, phi, half=1.0):
 
 def run_etch_3d(Lx, Ly, Lz, dx, trench_width, mask_th, sub_top, t_end, n_steps, hole, par, flags,
                 n_ion, n_neu, seed_offset=0, record_depth_every=0, max_seconds=None, steps=None,
-                stage_times=None, reinit_method="fsm", extend="gpu", surf_smooth=0.0):
+                stage_times=None, reinit_method="fsm", extend="gpu", surf_smooth=0.0,
+                phi_init=None, bare_init=None):
     """run_etch_3d (threed.py:1643-1795) with the oracle's stages (coverage-coupled MC path,
     radiosity or DDA neutrals, FSM reinit, nearest-face extension).  Runs `steps` (default n_steps) steps of the n_steps
     schedule.  Returns (phi, depth_history, stats); stage_times (list) receives one dict of stage
-    seconds per step."""
+    seconds per step.  phi_init: start from this level set instead of the seed field (mask and
+    mask level set as run_etch_3d's phi_init); bare_init: the first step's starting coverage on
+    phi_init's mesh (then that step runs the warm-start round count)."""
     nx, ny, nz = int(round(Lx / dx)), int(round(Ly / dx)), int(round(Lz / dx))
     phi_a, mask = seed(nx, ny, nz, dx, Lx, Ly, sub_top, mask_th, trench_width, hole)
-    phi = seed_distance(phi_a.astype(np.float32), dx).astype(np.float32)
+    if phi_init is None:
+        phi = seed_distance(phi_a.astype(np.float32), dx).astype(np.float32)
+    else:
+        phi = np.ascontiguousarray(phi_init, np.float32).reshape(nx, ny, nz).copy()
     mask_phi = phi.copy()
     geo = dict(Lx=Lx, Ly=Ly, Lz=Lz, dx=dx, sub_top=sub_top, mask_th=mask_th,
                trench_width=trench_width, hole=hole, xs=np.arange(nx) * dx,
@@ -1168,7 +1174,9 @@ def run_etch_3d(Lx, Ly, Lz, dx, trench_width, mask_th, sub_top, t_end, n_steps, 
                                                     step + seed_offset, tt=st)
         else:
             bi = None
-            if warm and prev is not None:
+            if step == 0 and bare_init is not None:
+                bi = np.asarray(bare_init, np.float64)
+            elif warm and prev is not None:
                 pm, pb = prev
                 q = pm.nearest(mesh.centroid.astype(np.float32).astype(np.float64))
                 bi = np.where(q >= 0, pb[np.maximum(q, 0)], 1.0)

@@ -9,6 +9,7 @@
 //   * the Jacobi Godunov-Eikonal reinit of petch_reinit_eik mode 0 (reinit_fsm, threed.py:
 //     1421-1537): init, n_iter - 1 sweeps and the finalising sweep, each one launch for the batch.
 // The instance table travels as a kernel parameter; blockIdx.y selects the instance.
+#include <algorithm>
 #include <cmath>
 #include "common.cuh"
 #include "levelset.cuh"
@@ -100,15 +101,21 @@ __global__ void k_b_adv_finish(BTable t) {
     }
 }
 
+// The Eikonal passes row-mapped (petch::RowShape: threadIdx.x along z, threadIdx.y a row of the
+// block's, blockIdx.x striding over the instance's nx * ny rows).
 __global__ void k_b_eik_init(BTable t, double band_r) {
     const int b = blockIdx.y;
     if (b >= t.B) return;
     const BGrid& x = t.it[b];
     const float inv_dx = (float)(1.0 / x.dx);
     const float big = (float)(band_r + 4.0 * x.dx);
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < x.g.n;
-         c += (long long)gridDim.x * blockDim.x)
-        x.ua[c] = eik_init_cell<false>(x.phi, c, x.g, inv_dx, big);
+    const int rows = x.g.nx * x.g.ny;
+    for (int row = blockIdx.x * blockDim.y + threadIdx.y; row < rows; row += gridDim.x * blockDim.y) {
+        const int i = row / x.g.ny, j = row - i * x.g.ny;
+        const long long base = (long long)row * x.g.nz;
+        for (int k = threadIdx.x; k < x.g.nz; k += blockDim.x)
+            x.ua[base + k] = eik_init_cell_at<false>(x.phi, base + k, i, j, k, x.g, inv_dx, big);
+    }
 }
 
 template <bool FINAL>
@@ -120,11 +127,16 @@ __global__ void k_b_eik_sweep(BTable t, double band_r, int parity) {
     float* out = parity ? x.ua : x.ub;
     const float dxf = (float)x.dx;
     const float big = (float)(band_r + 4.0 * x.dx), cap = (float)(band_r + x.dx);
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < x.g.n;
-         c += (long long)gridDim.x * blockDim.x) {
-        const float v = eik_sweep_cell<FINAL, false>(in, c, x.g, dxf, big, cap, x.phi);
-        if (FINAL) x.phi[c] = v;
-        else out[c] = v;
+    const int rows = x.g.nx * x.g.ny;
+    for (int row = blockIdx.x * blockDim.y + threadIdx.y; row < rows; row += gridDim.x * blockDim.y) {
+        const int i = row / x.g.ny, j = row - i * x.g.ny;
+        const long long base = (long long)row * x.g.nz;
+        for (int k = threadIdx.x; k < x.g.nz; k += blockDim.x) {
+            const float v = eik_sweep_cell_at<FINAL, false>(in, base + k, i, j, k, x.g, dxf, big,
+                                                            cap, x.phi);
+            if (FINAL) x.phi[base + k] = v;
+            else out[base + k] = v;
+        }
     }
 }
 
@@ -205,16 +217,20 @@ extern "C" int petch_batch_reinit(const petch_batch_grid* grids, int B, double b
         PETCH_REQUIRE(grids[b].dx == dx, "petch_batch_reinit: all grids need the same dx");
     const int n_iter = (int)std::ceil(band_r / dx) + 4;
     cudaStream_t st = as_stream(stream);
-    dim3 gc(grid_for(mc, kBB, 2), B);
-    k_b_eik_init<<<gc, kBB, 0, st>>>(t, band_r);
+    long long max_rows = 0;
+    for (int b = 0; b < B; ++b) max_rows = std::max(max_rows, (long long)grids[b].nx * grids[b].ny);
+    const RowShape rs = stencil_shape();
+    const dim3 blk(rs.bz, rs.br);
+    const dim3 gc(std::max(1, stencil_blocks(max_rows, rs) / std::max(1, B / 4)), B);
+    k_b_eik_init<<<gc, blk, 0, st>>>(t, band_r);
     PETCH_LAUNCH_CHECK("k_b_eik_init");
     int parity = 0;
     for (int it = 0; it < n_iter - 1; ++it) {
-        k_b_eik_sweep<false><<<gc, kBB, 0, st>>>(t, band_r, parity);
+        k_b_eik_sweep<false><<<gc, blk, 0, st>>>(t, band_r, parity);
         PETCH_LAUNCH_CHECK("k_b_eik_sweep");
         parity ^= 1;
     }
-    k_b_eik_sweep<true><<<gc, kBB, 0, st>>>(t, band_r, parity);
+    k_b_eik_sweep<true><<<gc, blk, 0, st>>>(t, band_r, parity);
     PETCH_LAUNCH_CHECK("k_b_eik_sweep<final>");
     return PETCH_OK;
 }

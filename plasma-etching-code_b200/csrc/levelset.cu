@@ -92,14 +92,20 @@ __global__ void __launch_bounds__(kBlock) k_advect(const float* __restrict__ phi
     }
 }
 
+// The Eikonal passes, row-mapped (see petch::RowShape): threadIdx.x runs along z, threadIdx.y
+// picks one of the block's rows, blocks stride over the nx * ny rows.
 template <bool SEED>
 __global__ void __launch_bounds__(kBlock) k_eik_init(const float* __restrict__ phi0,
                                                      float* __restrict__ U, Grid g, float inv_dx,
                                                      float big) {
     const petch::LGrid lg = petch::make_lgrid(g.nx, g.ny, g.nz);
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.n;
-         c += (long long)gridDim.x * blockDim.x)
-        U[c] = petch::eik_init_cell<SEED>(phi0, c, lg, inv_dx, big);
+    const int rows = g.nx * g.ny;
+    for (int row = blockIdx.x * blockDim.y + threadIdx.y; row < rows; row += gridDim.x * blockDim.y) {
+        const int i = row / g.ny, j = row - i * g.ny;
+        const long long base = (long long)row * g.nz;
+        for (int k = threadIdx.x; k < g.nz; k += blockDim.x)
+            U[base + k] = petch::eik_init_cell_at<SEED>(phi0, base + k, i, j, k, lg, inv_dx, big);
+    }
 }
 
 template <bool FINAL, bool SEED>
@@ -109,15 +115,39 @@ __global__ void __launch_bounds__(kBlock) k_eik_sweep(const float* __restrict__ 
                                                       float* __restrict__ phi_out, Grid g,
                                                       float dx, float big, float cap) {
     const petch::LGrid lg = petch::make_lgrid(g.nx, g.ny, g.nz);
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.n;
-         c += (long long)gridDim.x * blockDim.x) {
-        const float v = petch::eik_sweep_cell<FINAL, SEED>(Uin, c, lg, dx, big, cap, phi_in);
-        if (FINAL) phi_out[c] = v;
-        else Uout[c] = v;
+    const int rows = g.nx * g.ny;
+    for (int row = blockIdx.x * blockDim.y + threadIdx.y; row < rows; row += gridDim.x * blockDim.y) {
+        const int i = row / g.ny, j = row - i * g.ny;
+        const long long base = (long long)row * g.nz;
+        for (int k = threadIdx.x; k < g.nz; k += blockDim.x) {
+            const float v = petch::eik_sweep_cell_at<FINAL, SEED>(Uin, base + k, i, j, k, lg, dx,
+                                                                  big, cap, phi_in);
+            if (FINAL) phi_out[base + k] = v;
+            else Uout[base + k] = v;
+        }
     }
 }
 
+// Block shape of the row-mapped stencils (petch_stencil_config): bz threads along z x br rows.
+int g_row_bz = 128, g_row_br = 2;
+
 }  // namespace
+
+namespace petch {
+RowShape stencil_shape() { return RowShape{g_row_bz, g_row_br}; }
+int stencil_blocks(long long rows, const RowShape& s) {
+    return grid_for(rows, s.br, 2048 / (s.bz * s.br));
+}
+}  // namespace petch
+
+extern "C" int petch_stencil_config(int bz, int br) {
+    PETCH_REQUIRE(bz >= 32 && bz % 32 == 0 && br >= 1 && bz * br <= kBlock,
+                  "petch_stencil_config: bz a multiple of 32, bz * br <= %d (got %d x %d)", kBlock,
+                  bz, br);
+    g_row_bz = bz;
+    g_row_br = br;
+    return PETCH_OK;
+}
 
 extern "C" int petch_seed_level_set(float* phi, uint8_t* mask, int nx, int ny, int nz, double dx,
                                     double Lx, double Ly, double sub_top, double mask_th,
@@ -170,25 +200,27 @@ extern "C" int petch_reinit_eik(const float* phi_in, float* phi_out, float* u_a,
                   "petch_reinit_eik: scratch buffers must be distinct from phi");
     Grid g = make_grid(nx, ny, nz);
     cudaStream_t st = petch::as_stream(stream);
-    int blocks = petch::grid_for(g.n, kBlock);
+    const petch::RowShape rs = petch::stencil_shape();
+    const dim3 blk(rs.bz, rs.br);
+    const int blocks = petch::stencil_blocks((long long)nx * ny, rs);
     const float dxf = (float)dx, inv_dx = (float)(1.0 / dx);
     PETCH_REQUIRE(mode == 0 || mode == 1, "petch_reinit_eik: mode must be 0 or 1");
-    if (mode == 1) k_eik_init<true><<<blocks, kBlock, 0, st>>>(phi_in, u_a, g, inv_dx, big);
-    else k_eik_init<false><<<blocks, kBlock, 0, st>>>(phi_in, u_a, g, inv_dx, big);
+    if (mode == 1) k_eik_init<true><<<blocks, blk, 0, st>>>(phi_in, u_a, g, inv_dx, big);
+    else k_eik_init<false><<<blocks, blk, 0, st>>>(phi_in, u_a, g, inv_dx, big);
     PETCH_LAUNCH_CHECK("k_eik_init");
     float* a = u_a;
     float* b = u_b;
     for (int it = 0; it < n_iter - 1; ++it) {
-        k_eik_sweep<false, false><<<blocks, kBlock, 0, st>>>(a, b, nullptr, nullptr, g, dxf, big, cap);
+        k_eik_sweep<false, false><<<blocks, blk, 0, st>>>(a, b, nullptr, nullptr, g, dxf, big, cap);
         PETCH_LAUNCH_CHECK("k_eik_sweep");
         float* t = a;
         a = b;
         b = t;
     }
     if (mode == 1)
-        k_eik_sweep<true, true><<<blocks, kBlock, 0, st>>>(a, nullptr, phi_in, phi_out, g, dxf, big, cap);
+        k_eik_sweep<true, true><<<blocks, blk, 0, st>>>(a, nullptr, phi_in, phi_out, g, dxf, big, cap);
     else
-        k_eik_sweep<true, false><<<blocks, kBlock, 0, st>>>(a, nullptr, phi_in, phi_out, g, dxf, big, cap);
+        k_eik_sweep<true, false><<<blocks, blk, 0, st>>>(a, nullptr, phi_in, phi_out, g, dxf, big, cap);
     PETCH_LAUNCH_CHECK("k_eik_sweep<final>");
     return PETCH_OK;
 }
@@ -261,22 +293,24 @@ extern "C" int petch_reinit_eik_noalloc(const float* phi_in, float* phi_out, int
     float* b = base + kNoAllocMaxCells;
     Grid g = make_grid(nx, ny, nz);
     cudaStream_t st = petch::as_stream(stream);
-    int blocks = petch::grid_for(g.n, kBlock);
+    const petch::RowShape rs = petch::stencil_shape();
+    const dim3 blk(rs.bz, rs.br);
+    const int blocks = petch::stencil_blocks((long long)nx * ny, rs);
     const float dxf = (float)dx, inv_dx = (float)(1.0 / dx);
-    if (mode == 1) k_eik_init<true><<<blocks, kBlock, 0, st>>>(phi_in, a, g, inv_dx, big);
-    else k_eik_init<false><<<blocks, kBlock, 0, st>>>(phi_in, a, g, inv_dx, big);
+    if (mode == 1) k_eik_init<true><<<blocks, blk, 0, st>>>(phi_in, a, g, inv_dx, big);
+    else k_eik_init<false><<<blocks, blk, 0, st>>>(phi_in, a, g, inv_dx, big);
     PETCH_LAUNCH_CHECK("k_eik_init");
     for (int it = 0; it < n_iter - 1; ++it) {
-        k_eik_sweep<false, false><<<blocks, kBlock, 0, st>>>(a, b, nullptr, nullptr, g, dxf, big, cap);
+        k_eik_sweep<false, false><<<blocks, blk, 0, st>>>(a, b, nullptr, nullptr, g, dxf, big, cap);
         PETCH_LAUNCH_CHECK("k_eik_sweep");
         float* t = a;
         a = b;
         b = t;
     }
     if (mode == 1)
-        k_eik_sweep<true, true><<<blocks, kBlock, 0, st>>>(a, nullptr, phi_in, phi_out, g, dxf, big, cap);
+        k_eik_sweep<true, true><<<blocks, blk, 0, st>>>(a, nullptr, phi_in, phi_out, g, dxf, big, cap);
     else
-        k_eik_sweep<true, false><<<blocks, kBlock, 0, st>>>(a, nullptr, phi_in, phi_out, g, dxf, big, cap);
+        k_eik_sweep<true, false><<<blocks, blk, 0, st>>>(a, nullptr, phi_in, phi_out, g, dxf, big, cap);
     PETCH_LAUNCH_CHECK("k_eik_sweep<final>");
     return PETCH_OK;
 }

@@ -21,7 +21,17 @@ __host__ __device__ inline LGrid make_lgrid(int nx, int ny, int nz) {
     return g;
 }
 
+// (i, j, k) of cell c; 32-bit divisions when the grid has fewer than 2^31 cells (the 64-bit ones
+// cost several times more and dominate a stencil cell's instruction count).
 __device__ __forceinline__ void lsplit(const LGrid& g, long long c, int& i, int& j, int& k) {
+    if (g.n < (1LL << 31)) {
+        const unsigned cc = (unsigned)c, nz = (unsigned)g.nz, ny = (unsigned)g.ny;
+        const unsigned r = cc / nz;
+        k = (int)(cc - r * nz);
+        i = (int)(r / ny);
+        j = (int)(r - (unsigned)i * ny);
+        return;
+    }
     long long r = c / g.nz;
     k = (int)(c - r * g.nz);
     i = (int)(r / g.ny);
@@ -32,10 +42,9 @@ __device__ __forceinline__ void lsplit(const LGrid& g, long long c, int& i, int&
 // one-sided difference at the domain faces.  Every operation is rounded on its own (no fused
 // multiply-add), so every kernel that advects -- dense, band list, batched, tangent -- produces
 // the same bits.
-__device__ __forceinline__ float advect_cell(const float* __restrict__ phi, long long c,
-                                             const LGrid& g, float inv_dx, float f, float dt) {
-    int i, j, k;
-    lsplit(g, c, i, j, k);
+__device__ __forceinline__ float advect_cell_at(const float* __restrict__ phi, long long c, int i,
+                                                int j, int k, const LGrid& g, float inv_dx,
+                                                float f, float dt) {
     const float v = phi[c];
     const long long st[3] = {g.plane, (long long)g.nz, 1};
     const int pos[3] = {i, j, k};
@@ -50,6 +59,13 @@ __device__ __forceinline__ float advect_cell(const float* __restrict__ phi, long
         gg = __fadd_rn(gg, __fadd_rn(__fmul_rn(t, t), __fmul_rn(s, s)));
     }
     return __fsub_rn(v, __fmul_rn(__fmul_rn(dt, f), __fsqrt_rn(gg)));
+}
+
+__device__ __forceinline__ float advect_cell(const float* __restrict__ phi, long long c,
+                                             const LGrid& g, float inv_dx, float f, float dt) {
+    int i, j, k;
+    lsplit(g, c, i, j, k);
+    return advect_cell_at(phi, c, i, j, k, g, inv_dx, f, dt);
 }
 
 // Godunov solution of |grad U| = 1 from the three upwind neighbour minima (threed.py:1421-1452):
@@ -81,10 +97,9 @@ __device__ __forceinline__ bool frozen(float u) { return signbit(u); }
 // of opposite sign) get the sub-cell distance min(|phi0| / max(|grad phi0|, 0.5), 1.8 dx),
 // frozen; others `big`.  SEED: nodes where phi0 is exactly 0 are frozen at distance 0.
 template <bool SEED>
-__device__ __forceinline__ float eik_init_cell(const float* __restrict__ phi0, long long c,
-                                               const LGrid& g, float inv_dx, float big) {
-    int i, j, k;
-    lsplit(g, c, i, j, k);
+__device__ __forceinline__ float eik_init_cell_at(const float* __restrict__ phi0, long long c,
+                                                  int i, int j, int k, const LGrid& g,
+                                                  float inv_dx, float big) {
     float v = phi0[c];
     float oxm = phi0[i >= 1 ? c - g.plane : c];
     float oxp = phi0[i <= g.nx - 2 ? c + g.plane : c];
@@ -108,19 +123,26 @@ __device__ __forceinline__ float eik_init_cell(const float* __restrict__ phi0, l
     return big;
 }
 
+template <bool SEED>
+__device__ __forceinline__ float eik_init_cell(const float* __restrict__ phi0, long long c,
+                                               const LGrid& g, float inv_dx, float big) {
+    int i, j, k;
+    lsplit(g, c, i, j, k);
+    return eik_init_cell_at<SEED>(phi0, c, i, j, k, g, inv_dx, big);
+}
+
 // One Jacobi sweep of _eik_jacobi (threed.py:1482-1512) for cell c; FINAL returns
 // sign(phi_in) * min(U, cap) (reinit_fsm's finalisation, threed.py:1535-1537) instead of U.
 template <bool FINAL, bool SEED>
-__device__ __forceinline__ float eik_sweep_cell(const float* __restrict__ Uin, long long c,
-                                                const LGrid& g, float dx, float big, float cap,
-                                                const float* __restrict__ phi_in) {
+__device__ __forceinline__ float eik_sweep_cell_at(const float* __restrict__ Uin, long long c,
+                                                   int i, int j, int k, const LGrid& g, float dx,
+                                                   float big, float cap,
+                                                   const float* __restrict__ phi_in) {
     float u = Uin[c];
     float un;
     if (frozen(u)) {
         un = FINAL ? fabsf(u) : u;
     } else {
-        int i, j, k;
-        lsplit(g, c, i, j, k);
         float um = (i >= 1) ? fabsf(Uin[c - g.plane]) : big;
         float up = (i <= g.nx - 2) ? fabsf(Uin[c + g.plane]) : big;
         float ax = fminf(um, up);
@@ -139,6 +161,24 @@ __device__ __forceinline__ float eik_sweep_cell(const float* __restrict__ Uin, l
     }
     return un;
 }
+
+template <bool FINAL, bool SEED>
+__device__ __forceinline__ float eik_sweep_cell(const float* __restrict__ Uin, long long c,
+                                                const LGrid& g, float dx, float big, float cap,
+                                                const float* __restrict__ phi_in) {
+    int i = 0, j = 0, k = 0;
+    if (!frozen(Uin[c])) lsplit(g, c, i, j, k);
+    return eik_sweep_cell_at<FINAL, SEED>(Uin, c, i, j, k, g, dx, big, cap, phi_in);
+}
+
+// Row-mapped stencil launches: a block of (bz, br) threads covers br rows (i, j) of the grid,
+// threadIdx.x running along z (coalesced), with one division per row instead of per cell; blocks
+// stride over the nx * ny rows.  The block shape is a tuning knob (petch_stencil_config).
+struct RowShape {
+    int bz, br;
+};
+RowShape stencil_shape();
+int stencil_blocks(long long rows, const RowShape& s);
 
 // run_etch_3d's CFL substep count (threed.py:1750-1756) from the device-side rate statistics:
 // nsub = clamp(ceil(Vmax dt / (0.4 dx)), 1, 160), Vmax = max(max V if finite (0 without faces),

@@ -1270,6 +1270,15 @@ extern "C" int petch_tracer_config(int bvh_width, int steps_per_round, int keep_
     return PETCH_OK;
 }
 
+extern "C" int petch_tracer_settings(int* out) {
+    PETCH_REQUIRE(out, "petch_tracer_settings: null pointer");
+    out[0] = g_bvh_width;
+    out[1] = g_steps;
+    out[2] = g_keep;
+    out[3] = g_tally_agg ? 1 : 0;
+    return PETCH_OK;
+}
+
 extern "C" int petch_tally_aggregation(int on) {
     PETCH_REQUIRE(on == 0 || on == 1, "petch_tally_aggregation: on must be 0 or 1");
     g_tally_agg = on != 0;

@@ -118,6 +118,8 @@ SIGNATURES = {
     "petch_raycast": [P, I, I, P, P, I, F, P, P, P, P],
     "petch_tracer_config": [I, I, I],
     "petch_tally_aggregation": [I],
+    "petch_stencil_config": [I, I],
+    "petch_tracer_settings": [P],
     "petch_nearest_face": [P, I, I, P, I, F, P, P, P],
     "petch_gas_normals": [P, I, I, P, I, I, I, D, P, P],
     "petch_trace_ff": [P, I, I, DP, P, U, I, P, P, P],

@@ -95,13 +95,14 @@ class StepPlan:
         self.steps_done += 1
 
     def capture(self):
-        """Capture the cold first step, a pair of warm steps and a single warm step into CUDA
-        graphs (capturing enqueues nothing: the graphs run on replay).  A warm step s uses mesh
-        buffer s % 2, so the pair graph starts on an odd step and the single graph runs an odd
-        step: the schedule is cold, pairs, and a single step when the remaining count is odd."""
+        """Capture the cold first step, a pair of warm steps and a single odd and a single even
+        warm step into CUDA graphs (capturing enqueues nothing: the graphs run on replay).  A
+        warm step s uses mesh buffer s % 2, so the pair graph starts on an odd step: run()
+        replays cold, pairs, and a single step when the remaining count is odd; replay_step()
+        replays one step at a time."""
         _lib.call("petch_prepare_device")
         graphs = {}
-        for key, first, n in (("cold", 0, 1), ("warm2", 1, 2), ("warm1", 1, 1)):
+        for key, first, n in (("cold", 0, 1), ("warm2", 1, 2), ("warm1", 1, 1), ("warm0", 2, 1)):
             g = torch.cuda.CUDAGraph()
             _lib.call("petch_plan_seek", self.h, first)
             with torch.cuda.graph(g):
@@ -136,6 +137,17 @@ class StepPlan:
             g.replay()
             self.steps_done += k
             n -= k
+
+    def replay_step(self):
+        """Advance one step by replaying its graph (cold, odd or even warm step)."""
+        if self.graphs is None:
+            self.capture()
+        s = self.steps_done
+        if s == 0 or not self.cfg.warm_start:
+            self.graphs["cold"].replay()
+        else:
+            self.graphs["warm1" if s % 2 else "warm0"].replay()
+        self.steps_done += 1
 
     def status(self, check=True):
         """The plan's accumulated status (one synchronising read); raises on device errors."""

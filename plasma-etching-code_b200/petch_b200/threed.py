@@ -733,7 +733,7 @@ def run_etch_3d(Lx=10.0, Ly=4.0, Lz=14.0, dx=0.4, trench_width=4.0, mask_th=2.0,
                 n_ion=20000, n_neu=20000, reinit_every=1, extend="gpu",
                 reinit_method="skfmm", verbose=True, record_depth_every=0, seed_offset=0,
                 rays_per_point=None, record_frames=False, surf_smooth=0.0,
-                etch_stop_z=None, max_tris=None, phi_init=None, hooks=None):
+                etch_stop_z=None, max_tris=None, phi_init=None, hooks=None, tune=False):
     """run_etch_3d (threed.py:1643-1795) on the device.  Same arguments and the same returned
     `geo` dict (numpy phi / mask, `timings` per stage from CUDA events, optional depth_history /
     frames).
@@ -745,7 +745,9 @@ def run_etch_3d(Lx=10.0, Ly=4.0, Lz=14.0, dx=0.4, trench_width=4.0, mask_th=2.0,
     mask re-pin after each reinit.
     Extensions: phi_init (host or device initial level set, replacing the seed field; the mask
     and mask_phi still come from the geometry), max_tris (initial face capacity, grown on
-    demand), hooks (dict of callables: before_step(step, eng), after_step(step, eng, status))."""
+    demand), hooks (dict of callables: before_step(step, eng), after_step(step, eng, status)),
+    tune (True or a petch_b200.tune.Tuner: pick the tracer and stencil settings per size bucket
+    by timing them on this run's surfaces, cached; geo['tuning'] lists the choices)."""
     if par is None:
         par = PAR
     if flags is None:
@@ -780,6 +782,10 @@ def run_etch_3d(Lx=10.0, Ly=4.0, Lz=14.0, dx=0.4, trench_width=4.0, mask_th=2.0,
     coupled = getattr(flags, "coverage_sticking", False)
     redepo = getattr(flags, "redeposition", False)
     eng = EtchEngine(geo, par, flags, max_tris=max_tris)
+    tuner = None
+    if tune:
+        from .tune import Tuner
+        tuner = tune if isinstance(tune, Tuner) else Tuner()
     st_timer = EventTimer()
     step = 0
     while step < n_steps:
@@ -789,6 +795,8 @@ def run_etch_3d(Lx=10.0, Ly=4.0, Lz=14.0, dx=0.4, trench_width=4.0, mask_th=2.0,
         eng.small.zero_()
         st_timer.start("mesh")
         eng.build_mesh()
+        if tuner is not None and tuner.ensure(eng, eng.mesh.n_faces()):
+            eng.build_mesh()              # the chosen BVH width needs its own tree
         st_timer.stop("mesh")
         if rays_per_point is not None:
             F_now = eng.mesh.n_faces()
@@ -870,6 +878,8 @@ def run_etch_3d(Lx=10.0, Ly=4.0, Lz=14.0, dx=0.4, trench_width=4.0, mask_th=2.0,
     timings['total'] = time.time() - t_wall
     geo['timings'] = timings
     geo['engine'] = eng
+    if tuner is not None:
+        geo['tuning'] = dict(tuner.chosen)
     for k in ('phi_dev', 'mask_dev', 'mask_phi_dev'):
         geo.pop(k, None)
     return geo

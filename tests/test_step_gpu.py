@@ -83,8 +83,9 @@ def test_petch_step_equals_run_etch_3d(g):
 
 
 def test_graph_replay_equals_eager_steps():
-    """The plan's CUDA graphs (cold step, warm pair, warm single) replayed over 8 steps equal 8
-    eager petch_step calls bit for bit (deterministic tallies)."""
+    """The plan's CUDA graphs replayed over 8 steps -- cold step, warm pairs and an odd single,
+    or one step at a time -- equal 8 eager petch_step calls bit for bit (deterministic
+    tallies)."""
     par = _par(True)
     kw = dict(**HOLE, t_end=0.8, n_steps=8, par=par, flags=SF6O2, n_ion=30000, n_neu=30000)
     _lib.set_deterministic(16 * t3.default_capacity(grid_shape(8.0, 8.0, 12.0, 0.25)))
@@ -95,13 +96,17 @@ def test_graph_replay_equals_eager_steps():
         graph = StepPlan(**kw)
         graph.run()                       # cold, 3 warm pairs, 1 warm single
         st_g = graph.status()
-        a, b = eager.phi.clone(), graph.phi.clone()
-        eager.close()
-        graph.close()
+        single = StepPlan(**kw)
+        for _ in range(8):
+            single.replay_step()          # cold, then odd / even single-step graphs
+        st_s = single.status()
+        a, b, c = eager.phi.clone(), graph.phi.clone(), single.phi.clone()
+        for p in (eager, graph, single):
+            p.close()
     finally:
         _lib.set_deterministic(0)
-    assert st_e['steps'] == st_g['steps'] == 8
-    assert torch.equal(a, b)
+    assert st_e['steps'] == st_g['steps'] == st_s['steps'] == 8
+    assert torch.equal(a, b) and torch.equal(a, c)
 
 
 def test_capacity_overflow_is_reported():
