@@ -433,6 +433,8 @@ typedef struct petch_batch_grid {
     const int* stats;        /* petch_surface_rate's stats: [1] = float bits of max V */
     const int* hdr;          /* the mesh header: [0] = face count */
     int* sub;                /* out, int[2]: [0] substeps, [1] float bits of dt / nsub */
+    const int* hold;         /* device int or NULL: nonzero leaves this level set unchanged (no
+                              * substeps, no reinit) -- a step whose mesh overflowed */
 } petch_batch_grid;
 
 /* Replaces, for B <= 64 instances at once, run_etch_3d's CFL substep count and advect_3d_gpu
@@ -768,7 +770,7 @@ typedef struct petch_step_status {
     int faces, max_faces;            /* the last step's face count, the largest seen */
     int trace_errors, mesh_errors;   /* error bits OR-ed over the steps */
     int nonfinite;                   /* non-finite surface velocities zeroed, summed */
-    int nsub;                        /* the last step's CFL substeps */
+    int nsub, nsub_max;              /* the last step's CFL substeps, the largest count seen */
     float vmax;                      /* the last step's max surface velocity */
     long long queries;               /* BVH queries, summed */
 } petch_step_status;
@@ -800,7 +802,9 @@ int petch_step(petch_plan_t* plan, void* stream);
 int petch_plan_seek(petch_plan_t* plan, long long step);
 
 /* Reads the plan's accumulated status (synchronises `stream`).  Returns PETCH_E_OVERFLOW if a
- * mesh outgrew max_tris (the level set is then invalid: plan again with more capacity) and
+ * mesh outgrew max_tris: such a step leaves the level set and the step counter unchanged (so do
+ * the steps after it, whose meshes overflow the same way), and status->steps counts the steps
+ * done -- plan again with more capacity from the level set and continue from there.  Returns
  * PETCH_E_LIMIT if a tracer hit a traversal bound. */
 int petch_plan_status(petch_plan_t* plan, petch_step_status* status, void* stream);
 

@@ -39,7 +39,10 @@ struct BGrid {
     const int* stats;        // [1]: float bits of max V
     const int* hdr;          // mesh header ([0] = faces)
     int* sub;                // [0] nsub, [1] float bits of dt / nsub
+    const int* hold;         // non-NULL and nonzero: leave this level set as it is this step
 };
+
+__device__ __forceinline__ bool held(const BGrid& x) { return x.hold && *x.hold; }
 
 struct BTable {
     BGrid it[kMaxInst];
@@ -53,6 +56,7 @@ __global__ void k_b_nsub(BTable t) {
     if (b >= t.B) return;
     const BGrid& x = t.it[b];
     cfl_substeps(x.hdr[HDR_F], x.stats, x.dt, x.dx, x.sub);
+    if (held(x)) x.sub[0] = 0;
 }
 
 // tmp = phi with the mask cells pinned (the first substep's write target).
@@ -107,6 +111,7 @@ __global__ void k_b_eik_init(BTable t, double band_r) {
     const int b = blockIdx.y;
     if (b >= t.B) return;
     const BGrid& x = t.it[b];
+    if (held(x)) return;
     const float inv_dx = (float)(1.0 / x.dx);
     const float big = (float)(band_r + 4.0 * x.dx);
     const int rows = x.g.nx * x.g.ny;
@@ -123,6 +128,7 @@ __global__ void k_b_eik_sweep(BTable t, double band_r, int parity) {
     const int b = blockIdx.y;
     if (b >= t.B) return;
     const BGrid& x = t.it[b];
+    if (held(x)) return;
     const float* in = parity ? x.ub : x.ua;
     float* out = parity ? x.ua : x.ub;
     const float dxf = (float)x.dx;
@@ -174,6 +180,7 @@ int make_table(const petch_batch_grid* grids, int B, BTable* t, long long* max_c
         x.stats = s.stats;
         x.hdr = s.hdr;
         x.sub = s.sub;
+        x.hold = s.hold;
         if (x.g.n > mc) mc = x.g.n;
     }
     *max_cells = mc;

@@ -28,10 +28,12 @@ namespace {
 // [8] band cells listed for the advection, [9..10] CFL substeps and dt bits, [11] step counter,
 // [12] tracer error bits OR-ed over steps, [13] mesh error bits OR-ed over steps, [14]
 // non-finite velocities summed over steps, [15] largest face count seen, [16..17] uint64
-// BVH queries summed over steps, [18] the last step's face count, [19] the last step's substeps.
+// BVH queries summed over steps, [18] the last step's face count, [19] the last step's substeps,
+// [20] held: this step's mesh outgrew the capacity, so the level set stays as it was, [21] the
+// largest substep count seen.
 constexpr int W_WORK = 0, W_STATS = 6, W_NACTIVE = 8, W_SUB = 9, W_STEP = 11, W_TERR = 12,
               W_MERR = 13, W_NONFINITE = 14, W_FMAX = 15, W_QUERIES = 16, W_F = 18, W_NSUB = 19,
-              W_COUNT = 20;
+              W_HOLD = 20, W_NSUBMAX = 21, W_COUNT = 22;
 constexpr int kPerStepWords = 11;   // [0, 11) are reset at the start of each step
 
 __global__ void k_fill(float* a, int n, float v) {
@@ -45,15 +47,24 @@ __global__ void k_mask_list(const uint8_t* mask, long long n, int* idx, int* cou
         if (mask[c]) idx[atomicAdd(count, 1)] = (int)c;
 }
 
-// Fold one step's status into the plan's accumulated words.
+// A mesh that outgrew its buffers (face / vertex overflow, hash table full) holds the step: the
+// advection and reinit leave the level set unchanged and the step counter stays, so the host can
+// plan again with more capacity and repeat the step.
+__global__ void k_hold(int* w, const int* hdr) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) w[W_HOLD] = (hdr[HDR_ERR] & 7) != 0;
+}
+
+// Fold one step's status into the plan's accumulated words and advance the step counter.
 __global__ void k_accumulate(int* w, const int* hdr) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (!w[W_HOLD]) w[W_STEP] += 1;
     w[W_TERR] |= w[W_WORK + 1];
     w[W_MERR] |= hdr[HDR_ERR];
     w[W_NONFINITE] += w[W_STATS];
     w[W_FMAX] = max(w[W_FMAX], hdr[HDR_F]);
     w[W_F] = hdr[HDR_F];
     w[W_NSUB] = w[W_SUB];
+    w[W_NSUBMAX] = max(w[W_NSUBMAX], w[W_SUB]);
     unsigned long long* q = reinterpret_cast<unsigned long long*>(w + W_QUERIES);
     *q += *reinterpret_cast<const unsigned long long*>(w + W_WORK + 2);
 }
@@ -151,6 +162,7 @@ petch_batch_grid grid_of(const petch_plan_s* p) {
     g.stats = p->words + W_STATS;
     g.hdr = reinterpret_cast<const int*>(p->mesh[p->cur]);   // the header is segment 0
     g.sub = p->words + W_SUB;
+    g.hold = p->words + W_HOLD;
     return g;
 }
 
@@ -306,13 +318,15 @@ extern "C" int petch_step(petch_plan_s* p, void* stream) {
     PETCH_TRY(petch_extend_velocity(p->mesh[cur], MT, MV, p->phi, p->mask, c.nx, c.ny, c.nz, c.dx,
                                     4.0 * c.dx, p->V, p->F, 1, p->active, w + W_NACTIVE,
                                     (int)p->ncell, w + W_WORK, stream));
-    // CFL substeps on the device, narrow-band advection, Eikonal reinit (band 4dx + 2dx)
+    // CFL substeps on the device, narrow-band advection, Eikonal reinit (band 4dx + 2dx); all
+    // skipped when the mesh overflowed
+    k_hold<<<1, 32, 0, st>>>(w, reinterpret_cast<const int*>(p->mesh[cur]));
+    PETCH_LAUNCH_CHECK("k_hold");
     const petch_batch_grid g = grid_of(p);
     PETCH_TRY(petch_batch_advect(&g, 1, stream));
     PETCH_TRY(petch_batch_reinit(&g, 1, 4.0 * c.dx + 2.0 * c.dx, stream));
     k_accumulate<<<1, 32, 0, st>>>(w, reinterpret_cast<const int*>(p->mesh[cur]));
     PETCH_LAUNCH_CHECK("k_accumulate");
-    PETCH_TRY(petch_batch_step_advance(w + W_STEP, stream));
     if (c.warm_start) p->cur = prev;
     p->steps_done += 1;
     return PETCH_OK;
@@ -340,12 +354,14 @@ extern "C" int petch_plan_status(petch_plan_s* p, petch_step_status* s, void* st
     s->mesh_errors = h[W_MERR];
     s->nonfinite = h[W_NONFINITE];
     s->nsub = h[W_NSUB];
+    s->nsub_max = h[W_NSUBMAX];
     std::memcpy(&s->queries, h + W_QUERIES, sizeof(long long));
     std::memcpy(&s->vmax, h + W_STATS + 1, sizeof(float));
     if (h[W_MERR] & (1 | 2 | 4)) {
-        set_error("petch_step: mesh capacity %d exceeded (error bits %d); the level set is no "
-                  "longer valid -- plan again with a larger max_tris",
-                  p->MT, h[W_MERR]);
+        set_error("petch_step: mesh capacity %d exceeded (error bits %d, largest mesh %d faces); "
+                  "that step and the ones after it left the level set unchanged -- plan again "
+                  "with a larger max_tris and repeat them from step %d",
+                  p->MT, h[W_MERR], h[W_FMAX], h[W_STEP]);
         return PETCH_E_OVERFLOW;
     }
     if (h[W_TERR]) {

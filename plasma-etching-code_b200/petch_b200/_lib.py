@@ -56,7 +56,8 @@ class BatchGrid(ctypes.Structure):
                 ("active", ctypes.c_void_p), ("n_active", ctypes.c_void_p),
                 ("max_active", ctypes.c_int), ("nx", ctypes.c_int), ("ny", ctypes.c_int),
                 ("nz", ctypes.c_int), ("dx", ctypes.c_double), ("dt", ctypes.c_double),
-                ("stats", ctypes.c_void_p), ("hdr", ctypes.c_void_p), ("sub", ctypes.c_void_p)]
+                ("stats", ctypes.c_void_p), ("hdr", ctypes.c_void_p), ("sub", ctypes.c_void_p),
+                ("hold", ctypes.c_void_p)]
 
 
 class BatchTangent(ctypes.Structure):
@@ -82,7 +83,7 @@ class StepConfig(ctypes.Structure):
 class StepStatus(ctypes.Structure):
     """petch_step_status."""
     _fields_ = [("steps", I), ("faces", I), ("max_faces", I), ("trace_errors", I),
-                ("mesh_errors", I), ("nonfinite", I), ("nsub", I), ("vmax", F),
+                ("mesh_errors", I), ("nonfinite", I), ("nsub", I), ("nsub_max", I), ("vmax", F),
                 ("queries", L)]
 
 

@@ -42,11 +42,12 @@ def supported(flags, par):
 class StepPlan:
     """A planned run of the fused step on a device level set (float32, caller-visible as
     `self.phi`).  phi_init: initial level set (host or device array); None writes the seed field
-    (make_trench_3d's CSG field, redistanced)."""
+    (make_trench_3d's CSG field, redistanced).  dt: the step length, when not t_end / n_steps
+    (a plan that continues another run)."""
 
     def __init__(self, Lx, Ly, Lz, dx, trench_width, mask_th, sub_top, hole, t_end, n_steps,
                  par=None, flags=None, n_ion=20000, n_neu=20000, seed_offset=0, max_tris=None,
-                 phi_init=None):
+                 phi_init=None, dt=None):
         par = dict(PAR if par is None else par)
         flags = flags or DEFAULT_FLAGS
         if not supported(flags, par):
@@ -60,7 +61,7 @@ class StepPlan:
         c.dx, c.Lx, c.Ly, c.Lz = float(dx), float(Lx), float(Ly), float(Lz)
         c.sub_top, c.mask_th, c.trench_width = float(sub_top), float(mask_th), float(trench_width)
         c.hole = int(bool(hole))
-        c.dt = float(t_end) / int(n_steps)
+        c.dt = float(t_end) / int(n_steps) if dt is None else float(dt)
         c.n_ion, c.n_neu = int(n_ion), int(n_neu)
         c.seed_offset = int(seed_offset)
         c.max_tris = int(max_tris or default_capacity((nx, ny, nz)))
@@ -101,13 +102,15 @@ class StepPlan:
         replays cold, pairs, and a single step when the remaining count is odd; replay_step()
         replays one step at a time."""
         _lib.call("petch_prepare_device")
-        graphs = {}
+        graphs, self.graph_launches = {}, {}
         for key, first, n in (("cold", 0, 1), ("warm2", 1, 2), ("warm1", 1, 1), ("warm0", 2, 1)):
             g = torch.cuda.CUDAGraph()
             _lib.call("petch_plan_seek", self.h, first)
+            n0 = _lib.launch_count()
             with torch.cuda.graph(g):
                 for _ in range(n):
                     _lib.call("petch_step", self.h, _sp())
+            self.graph_launches[key] = _lib.launch_count() - n0
             graphs[key] = g
         _lib.call("petch_plan_seek", self.h, self.steps_done)
         self.graphs = graphs
@@ -139,15 +142,15 @@ class StepPlan:
             n -= k
 
     def replay_step(self):
-        """Advance one step by replaying its graph (cold, odd or even warm step)."""
+        """Advance one step by replaying its graph (cold, odd or even warm step); returns the
+        library kernel launches the replayed graph holds."""
         if self.graphs is None:
             self.capture()
         s = self.steps_done
-        if s == 0 or not self.cfg.warm_start:
-            self.graphs["cold"].replay()
-        else:
-            self.graphs["warm1" if s % 2 else "warm0"].replay()
+        key = "cold" if s == 0 or not self.cfg.warm_start else ("warm1" if s % 2 else "warm0")
+        self.graphs[key].replay()
         self.steps_done += 1
+        return self.graph_launches[key]
 
     def status(self, check=True):
         """The plan's accumulated status (one synchronising read); raises on device errors."""

@@ -733,7 +733,8 @@ def run_etch_3d(Lx=10.0, Ly=4.0, Lz=14.0, dx=0.4, trench_width=4.0, mask_th=2.0,
                 n_ion=20000, n_neu=20000, reinit_every=1, extend="gpu",
                 reinit_method="skfmm", verbose=True, record_depth_every=0, seed_offset=0,
                 rays_per_point=None, record_frames=False, surf_smooth=0.0,
-                etch_stop_z=None, max_tris=None, phi_init=None, hooks=None, tune=False):
+                etch_stop_z=None, max_tris=None, phi_init=None, hooks=None, tune=False,
+                engine="auto"):
     """run_etch_3d (threed.py:1643-1795) on the device.  Same arguments and the same returned
     `geo` dict (numpy phi / mask, `timings` per stage from CUDA events, optional depth_history /
     frames).
@@ -747,7 +748,12 @@ def run_etch_3d(Lx=10.0, Ly=4.0, Lz=14.0, dx=0.4, trench_width=4.0, mask_th=2.0,
     and mask_phi still come from the geometry), max_tris (initial face capacity, grown on
     demand), hooks (dict of callables: before_step(step, eng), after_step(step, eng, status)),
     tune (True or a petch_b200.tune.Tuner: pick the tracer and stencil settings per size bucket
-    by timing them on this run's surfaces, cached; geo['tuning'] lists the choices)."""
+    by timing them on this run's surfaces, cached; geo['tuning'] lists the choices), engine:
+    "fused" runs every step as one call of the library's fused step (petch_plan / petch_step:
+    no host work or synchronisation inside a step; the coverage-coupled Monte-Carlo path with
+    FSM reinit, nearest-face extension, reinit every step, no surface smoothing, etch stop,
+    rays_per_point, hooks or tuner), "stages" composes each step from the stage calls here
+    (every option), "auto" (default) the fused step whenever the arguments allow it."""
     if par is None:
         par = PAR
     if flags is None:
@@ -758,6 +764,20 @@ def run_etch_3d(Lx=10.0, Ly=4.0, Lz=14.0, dx=0.4, trench_width=4.0, mask_th=2.0,
                       "threed.py:1538-1549) runs as the device Jacobi Godunov-Eikonal reinit "
                       "('fsm'): pass reinit_method='fsm' to silence this", UserWarning,
                       stacklevel=2)
+    if engine not in ("auto", "fused", "stages"):
+        raise ValueError(f"engine must be 'auto', 'fused' or 'stages', not {engine!r}")
+    if engine != "stages":
+        from .plan import supported
+        fusable = (supported(flags, par) and reinit_method != "gpu" and extend == "gpu"
+                   and reinit_every == 1 and not surf_smooth and rays_per_point is None
+                   and etch_stop_z is None and not hooks and not tune)
+        if engine == "fused" and not fusable:
+            raise ValueError("engine='fused' runs the coverage-coupled MC path with the default "
+                             "level-set options, without hooks or tuner")
+        if fusable:
+            return _run_fused(Lx, Ly, Lz, dx, trench_width, mask_th, sub_top, t_end, n_steps,
+                              hole, par, flags, n_ion, n_neu, verbose, record_depth_every,
+                              seed_offset, record_frames, max_tris, phi_init)
     nt = getattr(flags, "neutral_transport", "mc")
     hooks = hooks or {}
     mc_par = par
@@ -882,6 +902,78 @@ def run_etch_3d(Lx=10.0, Ly=4.0, Lz=14.0, dx=0.4, trench_width=4.0, mask_th=2.0,
         geo['tuning'] = dict(tuner.chosen)
     for k in ('phi_dev', 'mask_dev', 'mask_phi_dev'):
         geo.pop(k, None)
+    return geo
+
+
+def _run_fused(Lx, Ly, Lz, dx, trench_width, mask_th, sub_top, t_end, n_steps, hole, par, flags,
+               n_ion, n_neu, verbose, record_depth_every, seed_offset, record_frames, max_tris,
+               phi_init):
+    """run_etch_3d on the fused step (plan.StepPlan): steps are enqueued without host work in
+    between and the plan's status is read once per chunk of steps (every step when the depth,
+    frames or progress are recorded).  A mesh that outgrows the capacity holds its step on the
+    device; the run then plans again from the held level set with twice the capacity (or 1.5x
+    the largest mesh seen) and repeats the step, the new plan starting its coverage cold."""
+    from .plan import StepPlan
+    torch.cuda.init()
+    t_wall = time.time()
+    nx, ny, nz = grid_shape(Lx, Ly, Lz, dx)
+    geo = dict(xs=np.arange(nx) * dx, ys=np.arange(ny) * dx, zs=np.arange(nz) * dx, dx=dx, Lx=Lx,
+               Ly=Ly, Lz=Lz, sub_top=sub_top, trench_width=trench_width, hole=hole,
+               mask_th=mask_th)
+    dt = t_end / n_steps
+    MT = int(max_tris or default_capacity((nx, ny, nz)))
+    kw = dict(Lx=Lx, Ly=Ly, Lz=Lz, dx=dx, trench_width=trench_width, mask_th=mask_th,
+              sub_top=sub_top, hole=hole, par=par, flags=flags, n_ion=n_ion, n_neu=n_neu)
+    per_step = bool(record_depth_every or record_frames or verbose)
+    chunk = 1 if per_step else 16
+    done, issued, nsub_max, nonfinite = 0, 0, 0, 0
+    plan = StepPlan(**kw, t_end=t_end, n_steps=n_steps, seed_offset=seed_offset, max_tris=MT,
+                    phi_init=phi_init, dt=dt)
+    base = 0                              # steps completed before the current plan
+    while done < n_steps:
+        k = min(chunk, n_steps - done)
+        for _ in range(k):
+            plan.step()
+        st = plan.status(check=False)
+        if st['status'] == 3:             # PETCH_E_OVERFLOW: the held steps are repeated
+            done = base + st['steps']
+            MT = max(2 * MT, int(1.5 * st['max_faces']))
+            phi_now = plan.phi
+            plan.close()
+            geo['depth_history'] = [h for h in geo.get('depth_history', []) if h[0] <= done]
+            geo['frames'] = [f for f in geo.get('frames', []) if f['step'] <= done]
+            plan = StepPlan(**kw, t_end=dt * (n_steps - done), n_steps=n_steps - done,
+                            seed_offset=seed_offset + done, max_tris=MT, phi_init=phi_now, dt=dt)
+            base = done
+            continue
+        if st['status'] != 0:
+            plan.close()
+            raise _lib.PetchError(st['status'], "run_etch_3d (fused step)", _lib.last_error())
+        done = base + st['steps']
+        nsub_max = max(nsub_max, st['nsub_max'])
+        if st['nonfinite'] > nonfinite:
+            warnings.warn(f"steps up to {done}: {st['nonfinite'] - nonfinite} non-finite surface "
+                          "velocities (NaN/inf) zeroed; check flux normalization / coverage if "
+                          "this persists.", RuntimeWarning)
+            nonfinite = st['nonfinite']
+        step = done - 1
+        if record_depth_every and (step % record_depth_every == 0 or step == n_steps - 1):
+            d_now = _depth3d(dict(geo, phi=plan.phi))
+            geo.setdefault('depth_history', []).append((step + 1, d_now))
+            if record_frames:
+                geo.setdefault('frames', []).append(
+                    dict(step=step + 1, t=(step + 1) / n_steps * t_end, depth=d_now,
+                         phi_xz=plan.phi[:, ny // 2, :].double().cpu().numpy()))
+        if verbose and step % 5 == 0:
+            print(f"  step {step:3d}/{n_steps}  faces {st['faces']:5d}  "
+                  f"depth ~ {_depth3d(dict(geo, phi=plan.phi)):5.2f}  Vmax {st['vmax']:.3f}")
+    plan.close()
+    _, mask = seed_field(nx, ny, nz, dx, Lx, Ly, sub_top, mask_th, trench_width, hole)
+    geo['phi'] = plan.phi.double().cpu().numpy()
+    geo['mask'] = mask.bool().cpu().numpy()
+    geo['timings'] = dict(flux=0.0, extend=0.0, reinit=0.0, mesh=0.0, advect=0.0, rate=0.0,
+                          total=time.time() - t_wall, nsub_max=nsub_max, fused=True)
+    geo['engine'] = plan
     return geo
 
 

@@ -12,9 +12,11 @@ row-mapped Eikonal passes.
 
 The tracer trial is the step's dominant launch: both neutral species of a coverage round
 (petch_trace_neutral_pair) on the current mesh with the coverage warm-started from the previous
-step's, as the loop runs it; the stencil trial is the reinit of the current level set.  Each
-candidate is timed `reps` times with CUDA events, the candidates interleaved, and the median
-decides.  Buckets: face count (tracer) and cell count (stencil) by powers of two.
+step's, as the loop runs it; the stencil trial is the reinit of the current level set.  A coarse
+pass times every candidate, a fine pass (larger trials, more timings) the few fastest, and the
+fastest of the fine pass is chosen; every timing is the minimum over repeats (CUDA events), each
+after an untimed run of the same candidate.  Buckets: face count (tracer) and cell count
+(stencil) by powers of two.
 
 Enable in run_etch_3d with tune=True (or a Tuner); the cache file is $PETCH_TUNE_CACHE, else
 ~/.cache/petch_b200/tune.json.
@@ -57,12 +59,13 @@ def bucket(n):
 
 
 class Tuner:
-    """rays: rays per species of a tracer trial; reps: timings per candidate; path: cache file
-    (None: the default; False: memory only)."""
+    """rays: rays per species of a coarse tracer trial (fine trials take twice as many); reps:
+    timings per candidate in the coarse pass (three times as many in the fine pass); top:
+    candidates of the fine pass; path: cache file (None: the default; False: memory only)."""
 
-    def __init__(self, rays=1 << 19, reps=3, path=None, tracer_grid=TRACER_GRID,
-                 stencil_grid=STENCIL_GRID):
-        self.rays, self.reps = int(rays), int(reps)
+    def __init__(self, rays=1 << 19, reps=2, path=None, tracer_grid=TRACER_GRID,
+                 stencil_grid=STENCIL_GRID, top=4):
+        self.rays, self.reps, self.top = int(rays), int(reps), int(top)
         self.path = default_cache_path() if path is None else path
         self.tracer_grid, self.stencil_grid = tuple(tracer_grid), tuple(stencil_grid)
         self.cache = self._load()
@@ -103,17 +106,18 @@ class Tuner:
         return pre + str(b)
 
     # ---- measurement ----
-    def _time(self, fns, reps):
-        """fns: {config: callable enqueueing one trial on the current stream}.  Median ms per
-        config over `reps` interleaved rounds (each trial bracketed by CUDA events)."""
+    @staticmethod
+    def _time(fns, reps):
+        """fns: {config: callable enqueueing one trial on the current stream}.  The fastest of
+        `reps` timings per config (CUDA events); each timing follows an untimed run of the same
+        config, so it does not inherit another config's cache state, and the configs take turns
+        (order reversed every round)."""
         out = {c: [] for c in fns}
-        for fn in fns.values():
-            fn()                                        # warm-up (caches, lazy state)
-        torch.cuda.synchronize()
         order = list(fns)
         for r in range(reps):
             evs = []
             for c in (order if r % 2 == 0 else order[::-1]):
+                fns[c]()
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 e0.record()
                 fns[c]()
@@ -122,12 +126,25 @@ class Tuner:
             torch.cuda.synchronize()
             for c, e0, e1 in evs:
                 out[c].append(e0.elapsed_time(e1))
-        return {c: float(np.median(v)) for c, v in out.items()}
+        return {c: float(np.min(v)) for c, v in out.items()}
 
-    def tracer_trials(self, eng, grid=None, reps=None):
-        """Median ms of the neutral-pair trial for each tracer config of `grid` on eng's current
-        level set (meshes rebuilt here: binary and, for width 8, with the wide tree), coverage
-        warm-started from eng's previous mesh when it has one."""
+    def _search(self, trial, grid, reps, top):
+        """Coarse pass (every config, `reps` timings at the trial's base size), then a fine pass
+        on the `top` fastest (three times the timings, twice the size).  Returns {config: ms} of
+        the fine pass (the decision) for those, the coarse ms for the rest."""
+        coarse = self._time({c: trial(c, 1) for c in grid}, reps)
+        best = sorted(coarse, key=coarse.get)[:max(1, top)]
+        fine = self._time({c: trial(c, 2) for c in best}, 3 * reps)
+        res = dict(coarse)
+        for c in best:
+            res[c] = fine[c] / 2.0
+        return res, best
+
+    def tracer_trials(self, eng, grid=None, reps=None, exhaustive=False):
+        """ms per `rays` rays of the neutral-pair trial for each tracer config of `grid` on eng's
+        current level set (meshes rebuilt here: binary and, for width 8, with the wide tree),
+        coverage warm-started from eng's previous mesh when it has one.  The search of _search,
+        or with exhaustive=True the fine timing for every config."""
         from .threed import DeviceMesh, _sp
         grid = tuple(grid or self.tracer_grid)
         meshes, bares = {}, {}
@@ -147,38 +164,47 @@ class Tuner:
         betaE = float(eng.par.get('betaE', 0.7))
         betaO = float(eng.par.get('betaO', 1.0))
 
-        def trial(cfg):
+        def trial(cfg, scale):
             def run():
                 apply_tracer(cfg)
                 m = meshes[cfg[0]]
                 _lib.call("petch_trace_neutral_pair", m.id, m.MT, m.MV, ctypes.byref(eng.dom),
-                          bares[cfg[0]].data_ptr(), betaE, betaO, 7, 8, 0, self.rays,
+                          bares[cfg[0]].data_ptr(), betaE, betaO, 7, 8, 0, scale * self.rays,
                           flux_a.data_ptr(), flux_b.data_ptr(), work.data_ptr(), _sp())
             return run
 
         try:
-            res = self._time({c: trial(c) for c in grid}, reps or self.reps)
+            if exhaustive:
+                res = self._time({c: trial(c, 2) for c in grid}, 3 * (reps or self.reps))
+                res = {c: v / 2.0 for c, v in res.items()}
+            else:
+                res, _ = self._search(trial, grid, reps or self.reps, self.top)
         finally:
             apply_tracer(TRACER_DEFAULT)
         if int(work[1].item()):
             raise RuntimeError(f"tuner trial: tracer error bits {int(work[1].item())}")
         return res
 
-    def stencil_trials(self, eng, grid=None, reps=None):
-        """Median ms of the reinit of eng's level set (into scratch) for each block shape."""
+    def stencil_trials(self, eng, grid=None, reps=None, exhaustive=False):
+        """ms of the reinit of eng's level set (into scratch) for each block shape (search or,
+        with exhaustive=True, the fine timing of every shape)."""
         from .levelset import reinit_fsm_dev
         grid = tuple(grid or self.stencil_grid)
         out = torch.empty_like(eng.phi)
         band = 6.0 * eng.dx
 
-        def trial(cfg):
+        def trial(cfg, scale):
             def run():
                 apply_stencil(cfg)
-                reinit_fsm_dev(eng.phi, eng.dx, band, out=out, scratch=(eng.ua, eng.ub))
+                for _ in range(scale):
+                    reinit_fsm_dev(eng.phi, eng.dx, band, out=out, scratch=(eng.ua, eng.ub))
             return run
 
         try:
-            return self._time({c: trial(c) for c in grid}, reps or self.reps)
+            if exhaustive:
+                res = self._time({c: trial(c, 2) for c in grid}, 3 * (reps or self.reps))
+                return {c: v / 2.0 for c, v in res.items()}
+            return self._search(trial, grid, reps or self.reps, self.top)[0]
         finally:
             apply_stencil(STENCIL_DEFAULT)
 

@@ -54,7 +54,8 @@ def _config(g, par, t_end, n_steps, n, seed_offset=0, max_tris=None):
 @pytest.mark.parametrize("g", [HOLE, TRENCH], ids=["hole", "trench"])
 def test_petch_step_equals_run_etch_3d(g):
     """Seven steps through the C ABI alone (plan with the seed field, petch_step x 7, status,
-    destroy) against run_etch_3d with the same arguments: level sets equal bit for bit."""
+    destroy) against run_etch_3d's stage-by-stage engine with the same arguments: level sets
+    equal bit for bit."""
     par = _par(g['hole'])
     n, steps, t_end = 30000, 7, 0.7
     c, shape = _config(g, par, t_end, steps, n, seed_offset=5)
@@ -73,7 +74,8 @@ def test_petch_step_equals_run_etch_3d(g):
             torch.cuda.synchronize()
             _lib.call("petch_destroy", h)
         geo = t3.run_etch_3d(**g, t_end=t_end, n_steps=steps, par=par, flags=SF6O2, n_ion=n,
-                             n_neu=n, reinit_method="fsm", verbose=False, seed_offset=5)
+                             n_neu=n, reinit_method="fsm", verbose=False, seed_offset=5,
+                             engine="stages")
     finally:
         _lib.set_deterministic(0)
     assert st.steps == steps and st.trace_errors == 0 and st.mesh_errors & 7 == 0
@@ -118,3 +120,36 @@ def test_capacity_overflow_is_reported():
     plan.close()
     assert st['status'] == 3                     # PETCH_E_OVERFLOW
     assert st['mesh_errors'] & 1
+
+
+def test_run_etch_3d_fused_equals_stages_with_depth_history():
+    """run_etch_3d's two engines (the fused step, the default for these arguments, and the
+    stage-by-stage composition) give the same level set and depth history bit for bit."""
+    par = _par(False)
+    kw = dict(**TRENCH, t_end=0.6, n_steps=6, par=par, flags=SF6O2, n_ion=30000, n_neu=30000,
+              reinit_method="fsm", verbose=False, record_depth_every=1)
+    _lib.set_deterministic(1 << 22)
+    try:
+        a = t3.run_etch_3d(**kw, engine="fused")
+        b = t3.run_etch_3d(**kw, engine="stages")
+        c = t3.run_etch_3d(**kw)
+    finally:
+        _lib.set_deterministic(0)
+    assert a['timings'].get('fused') and not b['timings'].get('fused') and c['timings'].get('fused')
+    np.testing.assert_array_equal(a['phi'], b['phi'])
+    np.testing.assert_array_equal(a['mask'], b['mask'])
+    assert a['depth_history'] == b['depth_history'] and len(a['depth_history']) == 6
+
+
+def test_fused_run_regrows_capacity():
+    """A fused run whose mesh outgrows max_tris holds the step on the device, plans again with
+    more capacity from the held level set and finishes: the depth follows the stage engine's
+    (which regrows in place) within one cell."""
+    par = _par(True)
+    kw = dict(**HOLE, t_end=0.6, n_steps=6, par=par, flags=SF6O2, n_ion=30000, n_neu=30000,
+              reinit_method="fsm", verbose=False, record_depth_every=1, max_tris=2048)
+    a = t3.run_etch_3d(**kw, engine="fused")
+    b = t3.run_etch_3d(**kw, engine="stages")
+    assert [s for s, _ in a['depth_history']] == list(range(1, 7))
+    for (s, da), (_, db) in zip(a['depth_history'], b['depth_history']):
+        assert abs(da - db) <= HOLE['dx'] + 1e-9, (s, da, db)
