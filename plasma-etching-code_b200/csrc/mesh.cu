@@ -221,6 +221,13 @@ __global__ void k_mc_totals(const int4* bsum, const int4* boff, int nb, MeshView
     m.hdr[HDR_ERR] = err;
     int Fc = F < m.MT ? F : m.MT;
     int Lc = L < m.MT ? L : m.MT;
+    // An overflowed mesh is incomplete (the faces past the capacity were not emitted, and a leaf
+    // can straddle the capacity): publish it with no BVH leaves, so no ray or point query can
+    // reach a face index at or beyond max_tris.  The counts stay for the caller to regrow.
+    if (err) {
+        m.hdr[HDR_L] = 0;
+        Lc = 0;
+    }
     m.leaf_start[Lc] = Fc;
 }
 

@@ -214,7 +214,7 @@ __device__ __forceinline__ HitRec closest_hit(const MeshView& m, int L, const Ra
             if (h1) { node = c1; continue; }
         } else {
             int l = ~node;
-            int f0 = __ldg(m.leaf_start + l), f1 = __ldg(m.leaf_start + l + 1);
+            int f0 = __ldg(m.leaf_start + l), f1 = min(__ldg(m.leaf_start + l + 1), m.MT);
             for (int f = f0; f < f1; ++f)
                 if (hit_triangle(r, tri_v(m.tri, f, 0), tri_v(m.tri, f, 1), tri_v(m.tri, f, 2), h.t))
                     h.f = f;
@@ -318,7 +318,9 @@ struct LocalStack {
 };
 
 
+// Faces f0 .. f1 - 1 of one leaf; a face index is never taken past the buffer's capacity.
 __device__ __forceinline__ void query_leaf(const Tracer& T, Query& q, int f0, int f1) {
+    f1 = min(f1, T.m.MT);
     for (int f = f0; f < f1; ++f)
         if (hit_triangle(q.r, tri_v(T.m.tri, f, 0), tri_v(T.m.tri, f, 1), tri_v(T.m.tri, f, 2), q.t))
             q.f = f;
@@ -536,7 +538,7 @@ __device__ __forceinline__ int nearest_prim(const MeshView& m, int L, float3 p, 
             if (h1) { node = c1; continue; }
         } else {
             int l = ~node;
-            int f0 = __ldg(m.leaf_start + l), f1 = __ldg(m.leaf_start + l + 1);
+            int f0 = __ldg(m.leaf_start + l), f1 = min(__ldg(m.leaf_start + l + 1), m.MT);
             for (int f = f0; f < f1; ++f) {
                 float d2;
                 if (CENTROID) {
