@@ -575,8 +575,8 @@ def tuning_report(tuner):
         rows[key] = {"chosen": choice, "chosen_ms": trials.get(str(list(choice))),
                      "default_ms": trials.get(default), "candidates": len(trials)}
     return {"buckets": rows, "seconds": round(tuner.seconds, 2),
-            "knobs": "tracer: [bvh_width, steps per round, keep lanes, aggregated tallies]; "
-                     "stencil: [threads along z, rows per block]",
+            "knobs": "tracer: [bvh_width, steps per round, keep lanes, aggregated tallies, "
+                     "leaf grouping]; stencil: [threads along z, rows per block]",
             "trial": f"neutral-pair launch at {tuner.rays} rays per species on the run's mesh "
                      f"(median of {tuner.reps}); reinit of the run's level set"}
 

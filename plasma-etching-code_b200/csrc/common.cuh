@@ -30,6 +30,19 @@ inline int grid_for(long long n, int block, int per_sm = 8) {
     return (int)want;
 }
 
+// The single-instance ion and neutral-pair traces (petch_trace_ions, petch_trace_neutral_pair)
+// with the seed read on the device: seed_add + (*step + seed_off) * seed_mul, so that a captured
+// etch step takes its seeds from a device step counter (trace.cu).
+int trace_ions_stepped(const void* mesh, int max_tris, int max_verts, const petch_domain* dom,
+                       const petch_ion_params* p, const int* step, uint32_t seed_mul,
+                       uint32_t seed_off, uint32_t seed_add, int n_ion, float* tally4, float* ang,
+                       int* work, void* stream);
+int trace_neutral_pair_stepped(const void* mesh, int max_tris, int max_verts,
+                               const petch_domain* dom, const float* bare, float beta_a,
+                               float beta_b, const int* step, uint32_t seed_mul, uint32_t seed_off,
+                               uint32_t seed_add_a, uint32_t seed_add_b, uint32_t stream_id,
+                               int n_neu, float* flux_a, float* flux_b, int* work, void* stream);
+
 }  // namespace petch
 
 #define PETCH_LAUNCH_CHECK(what)                                   \

@@ -12,8 +12,8 @@
 // and the first (cold) step, with its four coverage rounds, is a separate capture.
 //
 // The stages are the library's own entry points, called in the order run_etch_3d calls them
-// (the batched forms with one instance where those read their seed or substep count from the
-// device), so a plan's steps equal run_etch_3d's bit for bit with deterministic tallies.
+// (forms that read the seed or the substep count from the device where those vary by step), so
+// a plan's steps equal run_etch_3d's bit for bit with deterministic tallies.
 #include <cmath>
 #include <cstring>
 #include <new>
@@ -166,20 +166,6 @@ petch_batch_grid grid_of(const petch_plan_s* p) {
     return g;
 }
 
-petch_batch_item item_of(const petch_plan_s* p, int kind) {
-    petch_batch_item it;
-    std::memset(&it, 0, sizeof(it));
-    it.mesh = p->mesh[p->cur];
-    it.dom = p->cfg.dom;
-    it.ion = p->cfg.ion;
-    it.bare = kind == 0 ? nullptr : p->bare[p->cur];
-    it.out = kind == 0 ? p->tal4 : p->flux_a;
-    it.ang = kind == 0 ? p->ang : p->flux_b;
-    it.n_rays = kind == 0 ? p->cfg.n_ion : p->cfg.n_neu;
-    it.seed = (uint32_t)p->cfg.seed_offset;
-    return it;
-}
-
 #define PETCH_TRY(call)          \
     do {                         \
         int _rc = (call);        \
@@ -285,9 +271,11 @@ extern "C" int petch_step(petch_plan_s* p, void* stream) {
         k_fill<<<grid_for(MT, 256), 256, 0, st>>>(p->bare[cur], MT, 1.0f);
         PETCH_LAUNCH_CHECK("k_fill");
     }
-    // ions (seed (step + seed_offset) * 9 + 1) and their post-processing
-    const petch_batch_item ions = item_of(p, 0);
-    PETCH_TRY(petch_trace_batch(0, &ions, 1, MT, MV, 0.0f, w + W_STEP, 9, 1, w + W_WORK, stream));
+    // ions (seed (step + seed_offset) * 9 + 1, step from the device counter) and their
+    // post-processing
+    const uint32_t off = (uint32_t)c.seed_offset;
+    PETCH_TRY(trace_ions_stepped(p->mesh[cur], MT, MV, &c.dom, &c.ion, w + W_STEP, 9, off, 1,
+                                 c.n_ion, p->tal4, p->ang, w + W_WORK, stream));
     const double A_src = c.Lx * c.Ly;
     float* y_sp = p->y;
     float* y_ie = p->y + MT;
@@ -300,9 +288,9 @@ extern "C" int petch_step(petch_plan_s* p, void* stream) {
     const int n_fp = c.n_fp > 0 ? c.n_fp : (cold ? 4 : 1);
     const float norm_neu = c.n_neu > 0 ? (float)(A_src / c.n_neu) : 0.0f;
     for (int it = 0; it < n_fp; ++it) {
-        const petch_batch_item neu = item_of(p, 1);
-        PETCH_TRY(petch_trace_batch_pair(&neu, 1, MT, MV, c.betaE, c.betaO, w + W_STEP, 9,
-                                         2 + 2 * it, 3 + 2 * it, w + W_WORK, stream));
+        PETCH_TRY(trace_neutral_pair_stepped(p->mesh[cur], MT, MV, &c.dom, p->bare[cur], c.betaE,
+                                             c.betaO, w + W_STEP, 9, off, 2 + 2 * it, 3 + 2 * it,
+                                             0, c.n_neu, p->flux_a, p->flux_b, w + W_WORK, stream));
         PETCH_TRY(petch_norm_smooth(p->mesh[cur], MT, MV, p->flux_a, norm_neu, 0.0f, 8.0f, 1,
                                     c.n_smooth, c.smooth_alpha, p->m_F, p->tmp5, p->tmp5 + MT,
                                     stream));

@@ -48,6 +48,7 @@ int g_bvh_width = 2;
 int g_steps = 64;
 int g_keep = 12;
 bool g_tally_agg = false;   // warp-aggregated deposits (petch_tally_aggregation)
+int g_group = 2;            // leaf grouping of the binary traversal (petch_tracer_grouping)
 
 // Deterministic tallies (petch_set_deterministic): caller-registered scratch for 64-bit
 // fixed-point accumulators; NULL = float atomics.
@@ -330,7 +331,7 @@ struct NeutralPairShader {
     float beta_a, beta_b;
     float* flux_a;
     float* flux_b;
-    uint32_t seed_b, domain;
+    uint32_t seed_delta, domain;   // species b's seed minus species a's (the launch's seed)
     int n;
     int det;
     static constexpr int kMaxBounce = 1024;
@@ -338,7 +339,7 @@ struct NeutralPairShader {
     __device__ __forceinline__ int count(const MeshView&, int n2) const { return n2; }
     __device__ __forceinline__ void init(Rng& g, const Tracer&, const Domain& D, int ray, float3& o,
                                          float3& d, RayState& s) const {
-        if (ray >= n) g.init(seed_b, domain, (uint32_t)(ray - n));
+        if (ray >= n) g.init(g.key.x + seed_delta, domain, (uint32_t)(ray - n));
         source(g, false, 0.0f, D, o, d);
         s.w = 1.0f;
     }
@@ -594,7 +595,7 @@ struct NeutralTanPairShader {
     float* dflux_a;         // [3][MT]
     float* flux_b;
     float* dflux_b;         // [3][MT]
-    uint32_t seed_b, domain;
+    uint32_t seed_delta, domain;   // species b's seed minus species a's (the launch's seed)
     int n;
     int det;
     static constexpr int kMaxBounce = 1024;
@@ -602,7 +603,7 @@ struct NeutralTanPairShader {
     __device__ __forceinline__ int count(const MeshView&, int n2) const { return n2; }
     __device__ __forceinline__ void init(Rng& g, const Tracer&, const Domain& D, int ray, float3& o,
                                          float3& d, RayState& s) const {
-        if (ray >= n) g.init(seed_b, domain, (uint32_t)(ray - n));
+        if (ray >= n) g.init(g.key.x + seed_delta, domain, (uint32_t)(ray - n));
         source(g, false, 0.0f, D, o, d);
         s.w = 1.0f;
         s.dw[0] = s.dw[1] = s.dw[2] = 0.0f;
@@ -712,6 +713,37 @@ __global__ void k_redep_apply(MeshView m, const float* __restrict__ flux,
     if ((threadIdx.x & 31) == 0 && stats) atomicMax(stats + 1, __float_as_int(vmax));
 }
 
+// Launch controls of the persistent tracers: traversal steps per warp round, lanes kept
+// traversing, leaf grouping (0 = off), and, when `step` is set, the seed taken on the device:
+// seed + (*step + seed_off) * seed_mul (the step counter of a captured etch step).
+struct TraceCtl {
+    int steps, keep, group;
+    const int* step;
+    uint32_t seed_mul, seed_off;
+};
+
+// Binary traversal steps of a warp with the node and leaf halves grouped: each iteration runs
+// leaf steps for the lanes at a leaf when they are at least 1/group of the open lanes, otherwise
+// node steps for the lanes at an internal node, so the triangle and the box paths do not take
+// turns inside one iteration with few lanes each (each iteration advances at least one lane).
+template <class St>
+__device__ __forceinline__ void grouped_steps(const Tracer& T, Query& q, St& stk, int& phase,
+                                              int steps, int keep_now, int group, int* err) {
+    for (int s = 0; s < steps; ++s) {
+        const bool open = phase == 1;
+        const int no = __popc(__ballot_sync(kFull, open));
+        if (no <= keep_now) break;
+        const bool at_leaf = open && q.cur < 0;
+        const int nl = __popc(__ballot_sync(kFull, at_leaf));
+        const bool leaves = nl * group >= no;
+        if (open && at_leaf == leaves) {
+            const bool fin = visit_bound(q, err) ||
+                             (leaves ? step_binary_leaf(T, q, stk) : step_binary_node(T, q, stk, err));
+            if (fin) phase = 2;
+        }
+    }
+}
+
 // Persistent tracer.  Each warp loops: refill lanes whose ray ended (one atomic per warp), run
 // traversal steps on every lane with an open query (up to `steps`, and only while more than
 // `keep` lanes still have one), then resolve the lanes whose query finished -- a miss wraps laterally (periodic domains, <= 256 wraps per bounce, then one
@@ -719,10 +751,11 @@ __global__ void k_redep_apply(MeshView m, const float* __restrict__ flux,
 // (new query) or ends the ray.
 template <class S, bool WIDE>
 __global__ void __launch_bounds__(kTB, S::kMinBlocks) k_trace(MeshView m, Domain D, S sh, uint32_t seed,
-                                               uint32_t domain, int n, int steps, int keep,
-                                               int* work) {
+                                               uint32_t domain, int n, TraceCtl c, int* work) {
     extern __shared__ float4 s_wn[];
     const Tracer T = make_tracer(m, s_wn, WIDE);
+    const int steps = c.steps, keep = c.keep;
+    if (c.step) seed += ((uint32_t)*c.step + c.seed_off) * c.seed_mul;
     n = sh.count(m, n);
     LocalStack stk;
     int err = 0;
@@ -759,6 +792,9 @@ __global__ void __launch_bounds__(kTB, S::kMinBlocks) k_trace(MeshView m, Domain
         // done (keep 0): each round makes progress.
         pool_empty = pool_empty || __any_sync(kFull, ray == -2);
         const int keep_now = pool_empty ? 0 : keep;
+        if (!WIDE && c.group > 0)
+            grouped_steps(T, q, stk, phase, steps, keep_now, c.group, &err);
+        else
         for (int s = 0; s < steps; ++s) {
             if (__popc(__ballot_sync(kFull, phase == 1)) <= keep_now) break;
             if (phase == 1) {
@@ -899,7 +935,7 @@ __global__ void __launch_bounds__(kTB, (KIND == 1 || KIND == 4) ? kTraceMinBlock
                                                                 : kTraceMinBlocks))
 k_trace_batch(BatchTable tab, MeshOffsets L, int MT, int MV, float beta, float beta2,
               const int* step, uint32_t seed_mul, uint32_t seed_add, uint32_t seed_add2,
-              uint32_t domain, int steps, int keep, int det, int* work) {
+              uint32_t domain, int steps, int keep, int group, int det, int* work) {
     constexpr bool ION = KIND == 0 || KIND == 2;
     constexpr bool TAN = KIND == 2 || KIND == 3 || KIND == 5;
     constexpr bool PAIR = KIND == 4 || KIND == 5;
@@ -971,12 +1007,15 @@ k_trace_batch(BatchTable tab, MeshOffsets L, int MT, int MV, float beta, float b
         if (__all_sync(kFull, ray == -2)) break;
         pool_empty = pool_empty || __any_sync(kFull, ray == -2);
         const int keep_now = pool_empty ? 0 : keep;
-        for (int s = 0; s < steps; ++s) {
-            if (__popc(__ballot_sync(kFull, phase == 1)) <= keep_now) break;
-            if (phase == 1) {
-                if (step_binary(T, q, stk, &err)) phase = 2;
+        if (group > 0)
+            grouped_steps(T, q, stk, phase, steps, keep_now, group, &err);
+        else
+            for (int s = 0; s < steps; ++s) {
+                if (__popc(__ballot_sync(kFull, phase == 1)) <= keep_now) break;
+                if (phase == 1) {
+                    if (step_binary(T, q, stk, &err)) phase = 2;
+                }
             }
-        }
         if (phase == 2) {
             const BatchItem& it = s_it[inst];
             float3 o = q.r.o, d = q.r.d;
@@ -1243,16 +1282,17 @@ extern "C" int petch_set_deterministic(void* scratch, long long scratch_bytes) {
 
 template <class S>
 static int launch_trace(const MeshView& m, const Domain& D, const S& sh, uint32_t seed,
-                        uint32_t domain, int n, int* work, cudaStream_t st, const char* what) {
-    const int steps = g_steps, keep = g_keep;
+                        uint32_t domain, int n, int* work, cudaStream_t st, const char* what,
+                        const int* step = nullptr, uint32_t seed_mul = 0, uint32_t seed_off = 0) {
+    const TraceCtl c{g_steps, g_keep, g_group, step, seed_mul, seed_off};
     if (g_bvh_width == 2) {
         // binary traversal reads no tree from shared memory: launching without the 12 KB of the
         // wide tree's top leaves the L1 / shared split and the resident blocks to the registers
         k_trace<S, false><<<persistent_blocks((const void*)k_trace<S, false>, kTB, 0), kTB, 0, st>>>(
-            m, D, sh, seed, domain, n, steps, keep, work);
+            m, D, sh, seed, domain, n, c, work);
     } else {
         k_trace<S, true><<<persistent_blocks((const void*)k_trace<S, true>, kTB), kTB, kSmemBytes, st>>>(
-            m, D, sh, seed, domain, n, steps, keep, work);
+            m, D, sh, seed, domain, n, c, work);
     }
     PETCH_LAUNCH_CHECK(what);
     return PETCH_OK;
@@ -1276,6 +1316,14 @@ extern "C" int petch_tracer_settings(int* out) {
     out[1] = g_steps;
     out[2] = g_keep;
     out[3] = g_tally_agg ? 1 : 0;
+    out[4] = g_group;
+    return PETCH_OK;
+}
+
+extern "C" int petch_tracer_grouping(int group) {
+    PETCH_REQUIRE(group == 0 || (group >= 2 && group <= 8),
+                  "petch_tracer_grouping: group must be 0 (off) or 2..8");
+    g_group = group;
     return PETCH_OK;
 }
 
@@ -1285,9 +1333,14 @@ extern "C" int petch_tally_aggregation(int on) {
     return PETCH_OK;
 }
 
-extern "C" int petch_trace_ions(const void* mesh, int max_tris, int max_verts,
-                                const petch_domain* dom, const petch_ion_params* p, uint32_t seed,
-                                int n_ion, float* tally4, float* ang, int* work, void* stream) {
+namespace petch {
+
+// petch_trace_ions with the seed seed_add + (*step + seed_off) * seed_mul read on the device
+// (step NULL: seed_add itself).
+int trace_ions_stepped(const void* mesh, int max_tris, int max_verts, const petch_domain* dom,
+                       const petch_ion_params* p, const int* step, uint32_t seed_mul,
+                       uint32_t seed_off, uint32_t seed_add, int n_ion, float* tally4, float* ang,
+                       int* work, void* stream) {
     PETCH_REQUIRE(mesh && dom && p && tally4 && ang && work, "petch_trace_ions: null pointer");
     PETCH_REQUIRE(n_ion >= 0 && max_tris > 0 && max_verts > 0, "petch_trace_ions: bad size");
     PETCH_REQUIRE(((uintptr_t)tally4 & 15) == 0, "petch_trace_ions: tally4 must be 16-byte aligned");
@@ -1306,17 +1359,28 @@ extern "C" int petch_trace_ions(const void* mesh, int max_tris, int max_verts,
     if (n_ion == 0) return PETCH_OK;
     DetArena arena;
     if (!arena.on())
-        return launch_trace(m, to_domain(dom), sh, seed, 0x696f6e73u, n_ion, work, st, "k_trace<ions>");
+        return launch_trace(m, to_domain(dom), sh, seed_add, 0x696f6e73u, n_ion, work, st,
+                            "k_trace<ions>", step, seed_mul, seed_off);
     PETCH_DET_TAKE(a_t, 4LL * max_tris);
     PETCH_DET_TAKE(a_a, (long long)max_tris);
     sh.tal4 = reinterpret_cast<float4*>(a_t);
     sh.ang = reinterpret_cast<float*>(a_a);
     sh.det = tally_mode(true);
-    int rc = launch_trace(m, to_domain(dom), sh, seed, 0x696f6e73u, n_ion, work, st, "k_trace<ions>");
+    int rc = launch_trace(m, to_domain(dom), sh, seed_add, 0x696f6e73u, n_ion, work, st,
+                          "k_trace<ions>", step, seed_mul, seed_off);
     if (rc) return rc;
     PETCH_DET_CONVERT(a_t, tally4, 4LL * max_tris);
     PETCH_DET_CONVERT(a_a, ang, (long long)max_tris);
     return PETCH_OK;
+}
+
+}  // namespace petch
+
+extern "C" int petch_trace_ions(const void* mesh, int max_tris, int max_verts,
+                                const petch_domain* dom, const petch_ion_params* p, uint32_t seed,
+                                int n_ion, float* tally4, float* ang, int* work, void* stream) {
+    return petch::trace_ions_stepped(mesh, max_tris, max_verts, dom, p, nullptr, 0, 0, seed, n_ion,
+                                     tally4, ang, work, stream);
 }
 
 extern "C" int petch_trace_neutrals(const void* mesh, int max_tris, int max_verts,
@@ -1346,11 +1410,15 @@ extern "C" int petch_trace_neutrals(const void* mesh, int max_tris, int max_vert
     return PETCH_OK;
 }
 
-extern "C" int petch_trace_neutral_pair(const void* mesh, int max_tris, int max_verts,
-                                        const petch_domain* dom, const float* bare, float beta_a,
-                                        float beta_b, uint32_t seed_a, uint32_t seed_b,
-                                        uint32_t stream_id, int n_neu, float* flux_a,
-                                        float* flux_b, int* work, void* stream) {
+namespace petch {
+
+// petch_trace_neutral_pair with the seeds seed_add_{a,b} + (*step + seed_off) * seed_mul read on
+// the device (step NULL: seed_add_a and seed_add_b themselves).
+int trace_neutral_pair_stepped(const void* mesh, int max_tris, int max_verts,
+                               const petch_domain* dom, const float* bare, float beta_a,
+                               float beta_b, const int* step, uint32_t seed_mul, uint32_t seed_off,
+                               uint32_t seed_add_a, uint32_t seed_add_b, uint32_t stream_id,
+                               int n_neu, float* flux_a, float* flux_b, int* work, void* stream) {
     PETCH_REQUIRE(mesh && dom && flux_a && flux_b && work, "petch_trace_neutral_pair: null pointer");
     PETCH_REQUIRE(flux_a != flux_b, "petch_trace_neutral_pair: flux_a and flux_b must differ");
     PETCH_REQUIRE(n_neu >= 0 && n_neu < (1 << 30) && max_tris > 0 && max_verts > 0,
@@ -1358,27 +1426,39 @@ extern "C" int petch_trace_neutral_pair(const void* mesh, int max_tris, int max_
     cudaStream_t st = as_stream(stream);
     MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
     const uint32_t domain = 0x6e657500u ^ stream_id;
-    NeutralPairShader sh{bare, beta_a, beta_b, flux_a, flux_b, seed_b, domain, n_neu,
-                         tally_mode(false)};
+    NeutralPairShader sh{bare, beta_a, beta_b, flux_a, flux_b, seed_add_b - seed_add_a, domain,
+                         n_neu, tally_mode(false)};
     k_zero_faces<<<grid_for(max_tris, 256), 256, 0, st>>>(m.hdr, max_tris, flux_a, 1, flux_b, 1);
     PETCH_LAUNCH_CHECK("k_zero_faces");
     PETCH_CUDA(cudaMemsetAsync(work, 0, sizeof(int), st), "reset ray counter");
     if (n_neu == 0) return PETCH_OK;
     DetArena arena;
     if (!arena.on())
-        return launch_trace(m, to_domain(dom), sh, seed_a, domain, 2 * n_neu, work, st,
-                            "k_trace<neutral pair>");
+        return launch_trace(m, to_domain(dom), sh, seed_add_a, domain, 2 * n_neu, work, st,
+                            "k_trace<neutral pair>", step, seed_mul, seed_off);
     PETCH_DET_TAKE(a_a, (long long)max_tris);
     PETCH_DET_TAKE(a_b, (long long)max_tris);
     sh.flux_a = reinterpret_cast<float*>(a_a);
     sh.flux_b = reinterpret_cast<float*>(a_b);
     sh.det = tally_mode(true);
-    int rc = launch_trace(m, to_domain(dom), sh, seed_a, domain, 2 * n_neu, work, st,
-                          "k_trace<neutral pair>");
+    int rc = launch_trace(m, to_domain(dom), sh, seed_add_a, domain, 2 * n_neu, work, st,
+                          "k_trace<neutral pair>", step, seed_mul, seed_off);
     if (rc) return rc;
     PETCH_DET_CONVERT(a_a, flux_a, (long long)max_tris);
     PETCH_DET_CONVERT(a_b, flux_b, (long long)max_tris);
     return PETCH_OK;
+}
+
+}  // namespace petch
+
+extern "C" int petch_trace_neutral_pair(const void* mesh, int max_tris, int max_verts,
+                                        const petch_domain* dom, const float* bare, float beta_a,
+                                        float beta_b, uint32_t seed_a, uint32_t seed_b,
+                                        uint32_t stream_id, int n_neu, float* flux_a,
+                                        float* flux_b, int* work, void* stream) {
+    return petch::trace_neutral_pair_stepped(mesh, max_tris, max_verts, dom, bare, beta_a, beta_b,
+                                             nullptr, 0, 0, seed_a, seed_b, stream_id, n_neu,
+                                             flux_a, flux_b, work, stream);
 }
 
 extern "C" int petch_trace_electrons(const void* mesh, int max_tris, int max_verts,
@@ -1451,7 +1531,7 @@ void launch_batch(const BatchTable& tab, const MeshOffsets& L, int max_tris, int
                   uint32_t seed_add2, uint32_t domain, int det, int* work, cudaStream_t st) {
     k_trace_batch<KIND><<<persistent_blocks((const void*)k_trace_batch<KIND>, kTB, 0), kTB, 0, st>>>(
         tab, L, max_tris, max_verts, beta, beta2, step, seed_mul, seed_add, seed_add2, domain,
-        g_steps, g_keep, det, work);
+        g_steps, g_keep, g_group, det, work);
 }
 
 // kind: 0 ions, 1 neutrals, 2 ions with energy tangents, 3 neutrals with weight tangents,
@@ -1729,7 +1809,7 @@ extern "C" int petch_trace_neutral_pair_tangent(const void* mesh, int max_tris, 
     MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
     const uint32_t domain = 0x6e657500u ^ stream_id;
     NeutralTanPairShader sh{bare, dbare, beta_a, beta_b, flux_a, dflux_a, flux_b, dflux_b,
-                            seed_b, domain, n_neu, tally_mode(false)};
+                            seed_b - seed_a, domain, n_neu, tally_mode(false)};
     k_zero_faces<<<grid_for(max_tris, 256), 256, 0, st>>>(m.hdr, max_tris, flux_a, 1, flux_b, 1);
     PETCH_LAUNCH_CHECK("k_zero_faces");
     PETCH_CUDA(cudaMemsetAsync(dflux_a, 0, sizeof(float) * 3 * (size_t)max_tris, st), "zero dflux");

@@ -292,7 +292,33 @@ __device__ __forceinline__ float qbyte(uint32_t lo4, uint32_t hi4, int k) {
 // beat the current hit (entries beyond it are dropped without a fetch); false if none is left.
 // (A variant holding the top 4 or 8 entries in shared memory was measured on the trench
 // workload: 2-4 % slower, since its shared memory comes out of the L1 that caches the tree.)
+#ifndef PETCH_STACK_PACKED
+#define PETCH_STACK_PACKED 1
+#endif
 struct LocalStack {
+#if PETCH_STACK_PACKED
+    int2 e[kWStack];          // (ref, entry distance bits): one 8-byte access per push / pop
+    __device__ __forceinline__ void push(Query& q, int r, float tt, int* err) {
+        if (q.sp < kWStack) {
+            e[q.sp] = make_int2(r, __float_as_int(tt));
+            ++q.sp;
+        } else {
+            *err |= 1;
+        }
+    }
+    __device__ __forceinline__ bool pop(Query& q) {
+        while (q.sp > 0) {
+            --q.sp;
+            const int2 x = e[q.sp];
+            if (__int_as_float(x.y) <= q.t) {
+                q.cur = x.x;
+                return true;
+            }
+        }
+        q.cur = kDone;
+        return false;
+    }
+#else
     int ref[kWStack];
     float t[kWStack];
     __device__ __forceinline__ void push(Query& q, int r, float tt, int* err) {
@@ -315,6 +341,7 @@ struct LocalStack {
         q.cur = kDone;
         return false;
     }
+#endif
 };
 
 
@@ -402,38 +429,51 @@ __device__ __forceinline__ bool step_wide(const Tracer& T, Query& q, St& st, int
     return !st.pop(q);
 }
 
-// One step of the binary traversal; returns true once the query has finished.
+// One step of the binary traversal; returns true once the query has finished.  The internal-node
+// and leaf halves are also callable on their own (a warp can run one kind of step at a time for
+// the lanes at that kind of node, see k_trace).
 template <class St>
-__device__ __forceinline__ bool step_binary(const Tracer& T, Query& q, St& st, int* err) {
-    if (q.cur == kDone) return true;
+__device__ __forceinline__ bool step_binary_node(const Tracer& T, Query& q, St& st, int* err) {
+    const float4* n = T.m.nodes + 4 * q.cur;
+    float4 n0 = __ldg(n), n1 = __ldg(n + 1), n2 = __ldg(n + 2), n3 = __ldg(n + 3);
+    float t0, t1;
+    bool h0 = slab(q.r, n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, q.t, t0);
+    bool h1 = slab(q.r, n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, q.t, t1);
+    int c0 = __float_as_int(n3.x), c1 = __float_as_int(n3.y);
+    if (h0 && h1) {
+        bool swap = t1 < t0;
+        st.push(q, swap ? c0 : c1, swap ? t0 : t1, err);
+        q.cur = swap ? c1 : c0;
+        return false;
+    }
+    if (h0 || h1) {
+        q.cur = h0 ? c0 : c1;
+        return false;
+    }
+    return !st.pop(q);
+}
+
+template <class St>
+__device__ __forceinline__ bool step_binary_leaf(const Tracer& T, Query& q, St& st) {
+    const int l = ~q.cur;
+    query_leaf(T, q, __ldg(T.m.leaf_start + l), __ldg(T.m.leaf_start + l + 1));
+    return !st.pop(q);
+}
+
+__device__ __forceinline__ bool visit_bound(Query& q, int* err) {
     if (++q.visits > kMaxVisits) {
         *err |= 1;
         q.cur = kDone;
         return true;
     }
-    const int node = q.cur;
-    if (node >= 0) {
-        const float4* n = T.m.nodes + 4 * node;
-        float4 n0 = __ldg(n), n1 = __ldg(n + 1), n2 = __ldg(n + 2), n3 = __ldg(n + 3);
-        float t0, t1;
-        bool h0 = slab(q.r, n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, q.t, t0);
-        bool h1 = slab(q.r, n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, q.t, t1);
-        int c0 = __float_as_int(n3.x), c1 = __float_as_int(n3.y);
-        if (h0 && h1) {
-            bool swap = t1 < t0;
-            st.push(q, swap ? c0 : c1, swap ? t0 : t1, err);
-            q.cur = swap ? c1 : c0;
-            return false;
-        }
-        if (h0 || h1) {
-            q.cur = h0 ? c0 : c1;
-            return false;
-        }
-    } else {
-        int l = ~node;
-        query_leaf(T, q, __ldg(T.m.leaf_start + l), __ldg(T.m.leaf_start + l + 1));
-    }
-    return !st.pop(q);
+    return false;
+}
+
+template <class St>
+__device__ __forceinline__ bool step_binary(const Tracer& T, Query& q, St& st, int* err) {
+    if (q.cur == kDone) return true;
+    if (visit_bound(q, err)) return true;
+    return q.cur >= 0 ? step_binary_node(T, q, st, err) : step_binary_leaf(T, q, st);
 }
 
 // Stage the top of the wide tree in shared memory (call from every thread of the block).

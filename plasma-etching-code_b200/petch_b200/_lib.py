@@ -121,6 +121,7 @@ SIGNATURES = {
     "petch_tally_aggregation": [I],
     "petch_stencil_config": [I, I],
     "petch_tracer_settings": [P],
+    "petch_tracer_grouping": [I],
     "petch_nearest_face": [P, I, I, P, I, F, P, P, P],
     "petch_gas_normals": [P, I, I, P, I, I, I, D, P, P],
     "petch_trace_ff": [P, I, I, DP, P, U, I, P, P, P],
@@ -181,6 +182,7 @@ SIGNATURES = {
 # The library's tracer configuration at load (bvh_width, steps_per_round, keep_lanes): what
 # petch_tracer_config restores to.
 TRACER_DEFAULT = (2, 64, 12)
+TRACER_GROUPING_DEFAULT = 2
 
 _det_scratch = None
 

@@ -2,11 +2,13 @@
 candidates on the run's own surface, once per (device, size bucket), and caches the choice in
 memory and in a JSON file so later runs (and later steps in the same bucket) just apply it.
 
-Tracer knobs (petch_tracer_config, petch_tally_aggregation):
+Tracer knobs (petch_tracer_config, petch_tally_aggregation, petch_tracer_grouping):
     bvh_width     2 (binary LBVH) or 8 (quantised 8-wide BVH, top levels in shared memory)
     steps         traversal steps a warp runs for its open queries between shading rounds
     keep          lanes that may still be traversing when a warp stops to shade and refill
-    aggregate     warp-aggregated deposits
+    aggregate     warp-aggregated deposits (tried against the fastest candidates)
+    grouping      leaf grouping of the binary traversal (0 off, or the 1/g share of open lanes
+                  at a leaf that switches a warp iteration to triangle tests)
 Stencil knob (petch_stencil_config): the block shape (threads along z x grid rows) of the
 row-mapped Eikonal passes.
 
@@ -31,10 +33,12 @@ import torch
 
 from . import _lib
 
-TRACER_GRID = tuple((w, s, k, a) for w in (2, 8) for s in (32, 64, 128) for k in (8, 12, 16)
-                    for a in (0, 1))
+# tracer settings: (bvh_width, steps, keep, aggregate, grouping); grouping only acts on the
+# binary traversal, so the 8-wide candidates carry 0
+TRACER_GRID = tuple((w, s, k, 0, g) for w in (2, 8) for s in (32, 64, 128) for k in (8, 12, 16)
+                    for g in ((0, 2, 3) if w == 2 else (0,)))
 STENCIL_GRID = ((32, 8), (64, 4), (128, 2), (256, 1), (64, 2), (128, 1))
-TRACER_DEFAULT = (2, 64, 12, 0)
+TRACER_DEFAULT = (2, 64, 12, 0, 2)
 STENCIL_DEFAULT = (128, 2)
 
 
@@ -44,9 +48,10 @@ def default_cache_path():
 
 
 def apply_tracer(cfg):
-    w, s, k, a = (int(v) for v in cfg)
+    w, s, k, a, g = (int(v) for v in cfg)
     _lib.call("petch_tracer_config", w, s, k)
     _lib.call("petch_tally_aggregation", a)
+    _lib.call("petch_tracer_grouping", g)
 
 
 def apply_stencil(cfg):
@@ -128,12 +133,15 @@ class Tuner:
                 out[c].append(e0.elapsed_time(e1))
         return {c: float(np.min(v)) for c, v in out.items()}
 
-    def _search(self, trial, grid, reps, top):
+    def _search(self, trial, grid, reps, top, twin=None):
         """Coarse pass (every config, `reps` timings at the trial's base size), then a fine pass
-        on the `top` fastest (three times the timings, twice the size).  Returns {config: ms} of
-        the fine pass (the decision) for those, the coarse ms for the rest."""
+        on the `top` fastest -- and on twin(c) of the two fastest, when given: a setting the
+        coarse grid leaves at one value -- with three times the timings at twice the size.
+        Returns {config: ms}: the fine pass (the decision) where run, the coarse pass elsewhere."""
         coarse = self._time({c: trial(c, 1) for c in grid}, reps)
         best = sorted(coarse, key=coarse.get)[:max(1, top)]
+        if twin is not None:
+            best += [t for t in (twin(c) for c in best[:2]) if t is not None and t not in best]
         fine = self._time({c: trial(c, 2) for c in best}, 3 * reps)
         res = dict(coarse)
         for c in best:
@@ -178,7 +186,8 @@ class Tuner:
                 res = self._time({c: trial(c, 2) for c in grid}, 3 * (reps or self.reps))
                 res = {c: v / 2.0 for c, v in res.items()}
             else:
-                res, _ = self._search(trial, grid, reps or self.reps, self.top)
+                res, _ = self._search(trial, grid, reps or self.reps, self.top,
+                                      twin=lambda c: (c[0], c[1], c[2], 1 - c[3], c[4]))
         finally:
             apply_tracer(TRACER_DEFAULT)
         if int(work[1].item()):
@@ -241,8 +250,8 @@ class Tuner:
 
 
 def tracer_settings():
-    """(bvh_width, steps, keep, aggregate) in force in the library."""
-    out = (ctypes.c_int * 4)()
+    """(bvh_width, steps, keep, aggregate, grouping) in force in the library."""
+    out = (ctypes.c_int * 5)()
     _lib.call("petch_tracer_settings", out)
     return tuple(out)
 

@@ -210,3 +210,27 @@ def test_neutral_pair_equals_two_single_launches(hole):
                   1, 2, 0, 10, f.data_ptr(), f.data_ptr(), torch.zeros(6, dtype=torch.int32,
                                                                     device="cuda").data_ptr(),
                   stream())
+
+
+@pytest.mark.parametrize("group", [0, 3, 4])
+def test_leaf_grouping_is_bit_exact(group):
+    """Leaf grouping only reorders which lanes of a warp step when; every lane's traversal is
+    unchanged, so with deterministic tallies the ion and neutral tallies equal the default's
+    (grouping 2) bit for bit."""
+    phi, geo = small_feature(False)
+    m = cuda_mesh(phi, geo['dx'], geo)
+    from petch_b200 import _lib
+    par = dict(params.PAR, periodic_y=1)
+    bare = np.random.default_rng(5).uniform(0.05, 1.0, m.F)
+    _lib.set_deterministic(8 * m.MT + (1 << 16))
+    try:
+        ref_n = cuda_neutrals(m, geo, bare, 0.7, 3, 400_000)
+        ref_i = cuda_ions(m, geo, par, 4, 400_000)
+        _lib.call("petch_tracer_grouping", group)
+        got_n = cuda_neutrals(m, geo, bare, 0.7, 3, 400_000)
+        got_i = cuda_ions(m, geo, par, 4, 400_000)
+    finally:
+        _lib.call("petch_tracer_grouping", _lib.TRACER_GROUPING_DEFAULT)
+        _lib.set_deterministic(0)
+    np.testing.assert_array_equal(got_n, ref_n)
+    np.testing.assert_array_equal(got_i, ref_i)
