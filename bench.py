@@ -555,7 +555,7 @@ def tuning_pass(par, flags):
     tuner's ray count); returns the tuner frozen, so the timed runs only apply its choices."""
     from petch_b200 import threed as t3
     from petch_b200.tune import Tuner
-    tuner = Tuner(path=False)
+    tuner = Tuner(rays=RAYS, path=False)
     t0 = time.time()
     t3.run_etch_3d(**WORKLOAD, t_end=T_END, n_steps=N_STEPS, par=par, flags=flags,
                    n_ion=TUNE_RAYS, n_neu=TUNE_RAYS, reinit_method="fsm", verbose=False,
@@ -569,16 +569,21 @@ def tuning_report(tuner):
     from petch_b200.tune import STENCIL_DEFAULT, TRACER_DEFAULT
     rows = {}
     for key, choice in sorted(tuner.chosen.items()):
-        trials = tuner.trials.get(key, {})
+        trials = tuner.trials.get(key, {"coarse": {}, "fine": {}})
         kind = key.split("|")[1]
         default = str(list(TRACER_DEFAULT if kind == "tracer" else STENCIL_DEFAULT))
-        rows[key] = {"chosen": choice, "chosen_ms": trials.get(str(list(choice))),
-                     "default_ms": trials.get(default), "candidates": len(trials)}
+        c = str(list(choice))
+        rows[key] = {"chosen": choice, "candidates": len(trials["coarse"]),
+                     "coarse_ms": {"chosen": trials["coarse"].get(c),
+                                   "default": trials["coarse"].get(default)},
+                     "fine_ms": {"chosen": trials["fine"].get(c),
+                                 "default": trials["fine"].get(default)}}
     return {"buckets": rows, "seconds": round(tuner.seconds, 2),
             "knobs": "tracer: [bvh_width, steps per round, keep lanes, aggregated tallies, "
                      "leaf grouping]; stencil: [threads along z, rows per block]",
-            "trial": f"neutral-pair launch at {tuner.rays} rays per species on the run's mesh "
-                     f"(median of {tuner.reps}); reinit of the run's level set"}
+            "trial": f"neutral-pair launch on the run's mesh: coarse pass at {tuner.rays // 2} "
+                     f"rays per species, fine pass (the decision) at {tuner.rays}, fastest of the "
+                     "repeats; reinit of the run's level set"}
 
 
 def fused_run(par, flags, W, K, tuner, world, local, dist):

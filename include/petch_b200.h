@@ -148,11 +148,12 @@ typedef struct petch_ion_params {  /* the float32 arguments of _trace3d_ion_yiel
     float sigma;        /* ion angular spread of the source (par['ion_ang_sigma']) */
 } petch_ion_params;
 
-/* Tracer configuration for this process (knobs of the tuner, petch_b200.tune): bvh_width 2 (binary LBVH,
- * default) or 8 (quantised 8-wide BVH, built only by mesh builds made while it is configured); each warp runs traversal steps for all its lanes with an
- * open query, at most steps_per_round (default 64) and only while more than keep_lanes lanes
- * (0..31, default 12) still have one, between shading / refill rounds; once the ray pool is empty
- * a warp steps until its last query ends.  Applies to later trace / raycast calls. */
+/* Tracer configuration for this process (knobs of the tuner, petch_b200.tune): bvh_width 2
+ * (binary LBVH, default) or 8 (quantised 8-wide BVH, built only by mesh builds made while it is
+ * configured); each warp runs traversal steps for all its lanes with an open query, at most
+ * steps_per_round (default 32) and only while more than keep_lanes lanes (0..31, default 16)
+ * still have one, between shading / refill rounds; once the ray pool is empty a warp steps until
+ * its last query ends.  Applies to later trace / raycast calls. */
 int petch_tracer_config(int bvh_width, int steps_per_round, int keep_lanes);
 
 /* Warp-aggregated deposits for later trace calls (on = 1; default 0): lanes of a warp that

@@ -43,10 +43,11 @@ constexpr unsigned kFull = 0xffffffffu;
 // Tracer configuration (process-wide host state, set by petch_tracer_config): BVH width,
 // traversal steps per warp round, and how many lanes may still be traversing when a warp stops
 // stepping to shade and refill (only while the ray pool has rays).  The defaults were the fastest
-// of a sweep over neutral fluxes on the 8x4x40 trench (bare coverage 0.25 and 0.06).
+// of a sweep over the 8x4x40 trench's 100-step run at 2^22 rays with leaf grouping 2 (within
+// ~2 % of 64 steps / keep 12; grouping off is 25 % slower).
 int g_bvh_width = 2;
-int g_steps = 64;
-int g_keep = 12;
+int g_steps = 32;
+int g_keep = 16;
 bool g_tally_agg = false;   // warp-aggregated deposits (petch_tally_aggregation)
 int g_group = 2;            // leaf grouping of the binary traversal (petch_tracer_grouping)
 

@@ -181,7 +181,7 @@ SIGNATURES = {
 
 # The library's tracer configuration at load (bvh_width, steps_per_round, keep_lanes): what
 # petch_tracer_config restores to.
-TRACER_DEFAULT = (2, 64, 12)
+TRACER_DEFAULT = (2, 32, 16)
 TRACER_GROUPING_DEFAULT = 2
 
 _det_scratch = None

@@ -35,10 +35,10 @@ from . import _lib
 
 # tracer settings: (bvh_width, steps, keep, aggregate, grouping); grouping only acts on the
 # binary traversal, so the 8-wide candidates carry 0
-TRACER_GRID = tuple((w, s, k, 0, g) for w in (2, 8) for s in (32, 64, 128) for k in (8, 12, 16)
-                    for g in ((0, 2, 3) if w == 2 else (0,)))
+TRACER_GRID = (tuple((2, s, k, 0, g) for s in (32, 64, 128) for k in (8, 12, 16) for g in (2, 3))
+               + ((2, 32, 16, 0, 0), (8, 32, 16, 0, 0), (8, 64, 12, 0, 0)))
 STENCIL_GRID = ((32, 8), (64, 4), (128, 2), (256, 1), (64, 2), (128, 1))
-TRACER_DEFAULT = (2, 64, 12, 0, 2)
+TRACER_DEFAULT = (2, 32, 16, 0, 2)
 STENCIL_DEFAULT = (128, 2)
 
 
@@ -64,11 +64,12 @@ def bucket(n):
 
 
 class Tuner:
-    """rays: rays per species of a coarse tracer trial (fine trials take twice as many); reps:
-    timings per candidate in the coarse pass (three times as many in the fine pass); top:
-    candidates of the fine pass; path: cache file (None: the default; False: memory only)."""
+    """rays: rays per species of a fine tracer trial (coarse trials take half), best the run's
+    own count, since the launch tail depends on it; reps: timings per candidate in the coarse
+    pass (three times as many in the fine pass); top: candidates of the fine pass; path: cache
+    file (None: the default; False: memory only)."""
 
-    def __init__(self, rays=1 << 19, reps=2, path=None, tracer_grid=TRACER_GRID,
+    def __init__(self, rays=1 << 20, reps=2, path=None, tracer_grid=TRACER_GRID,
                  stencil_grid=STENCIL_GRID, top=4):
         self.rays, self.reps, self.top = int(rays), int(reps), int(top)
         self.path = default_cache_path() if path is None else path
@@ -134,25 +135,22 @@ class Tuner:
         return {c: float(np.min(v)) for c, v in out.items()}
 
     def _search(self, trial, grid, reps, top, twin=None):
-        """Coarse pass (every config, `reps` timings at the trial's base size), then a fine pass
-        on the `top` fastest -- and on twin(c) of the two fastest, when given: a setting the
-        coarse grid leaves at one value -- with three times the timings at twice the size.
-        Returns {config: ms}: the fine pass (the decision) where run, the coarse pass elsewhere."""
+        """Coarse pass (every config, `reps` timings at half the trial size), then a fine pass on
+        the `top` fastest -- and on twin(c) of the two fastest, when given: a setting the coarse
+        grid leaves at one value -- with three times the timings at the full trial size.  Returns
+        ({config: ms} of the coarse pass, {config: ms} of the fine pass, which decides)."""
         coarse = self._time({c: trial(c, 1) for c in grid}, reps)
         best = sorted(coarse, key=coarse.get)[:max(1, top)]
         if twin is not None:
             best += [t for t in (twin(c) for c in best[:2]) if t is not None and t not in best]
         fine = self._time({c: trial(c, 2) for c in best}, 3 * reps)
-        res = dict(coarse)
-        for c in best:
-            res[c] = fine[c] / 2.0
-        return res, best
+        return coarse, fine
 
     def tracer_trials(self, eng, grid=None, reps=None, exhaustive=False):
-        """ms per `rays` rays of the neutral-pair trial for each tracer config of `grid` on eng's
+        """Timings (ms) of the neutral-pair trial for the tracer configs of `grid` on eng's
         current level set (meshes rebuilt here: binary and, for width 8, with the wide tree),
-        coverage warm-started from eng's previous mesh when it has one.  The search of _search,
-        or with exhaustive=True the fine timing for every config."""
+        coverage warm-started from eng's previous mesh when it has one: (coarse, fine) of
+        _search, or with exhaustive=True the fine timing of every config."""
         from .threed import DeviceMesh, _sp
         grid = tuple(grid or self.tracer_grid)
         meshes, bares = {}, {}
@@ -177,17 +175,16 @@ class Tuner:
                 apply_tracer(cfg)
                 m = meshes[cfg[0]]
                 _lib.call("petch_trace_neutral_pair", m.id, m.MT, m.MV, ctypes.byref(eng.dom),
-                          bares[cfg[0]].data_ptr(), betaE, betaO, 7, 8, 0, scale * self.rays,
+                          bares[cfg[0]].data_ptr(), betaE, betaO, 7, 8, 0, scale * self.rays // 2,
                           flux_a.data_ptr(), flux_b.data_ptr(), work.data_ptr(), _sp())
             return run
 
         try:
             if exhaustive:
                 res = self._time({c: trial(c, 2) for c in grid}, 3 * (reps or self.reps))
-                res = {c: v / 2.0 for c, v in res.items()}
             else:
-                res, _ = self._search(trial, grid, reps or self.reps, self.top,
-                                      twin=lambda c: (c[0], c[1], c[2], 1 - c[3], c[4]))
+                res = self._search(trial, grid, reps or self.reps, self.top,
+                                   twin=lambda c: (c[0], c[1], c[2], 1 - c[3], c[4]))
         finally:
             apply_tracer(TRACER_DEFAULT)
         if int(work[1].item()):
@@ -195,8 +192,8 @@ class Tuner:
         return res
 
     def stencil_trials(self, eng, grid=None, reps=None, exhaustive=False):
-        """ms of the reinit of eng's level set (into scratch) for each block shape (search or,
-        with exhaustive=True, the fine timing of every shape)."""
+        """Timings (ms) of the reinit of eng's level set (into scratch) for the block shapes:
+        (coarse, fine) of _search, or with exhaustive=True the fine timing of every shape."""
         from .levelset import reinit_fsm_dev
         grid = tuple(grid or self.stencil_grid)
         out = torch.empty_like(eng.phi)
@@ -211,11 +208,15 @@ class Tuner:
 
         try:
             if exhaustive:
-                res = self._time({c: trial(c, 2) for c in grid}, 3 * (reps or self.reps))
-                return {c: v / 2.0 for c, v in res.items()}
-            return self._search(trial, grid, reps or self.reps, self.top)[0]
+                return self._time({c: trial(c, 2) for c in grid}, 3 * (reps or self.reps))
+            return self._search(trial, grid, reps or self.reps, self.top)
         finally:
             apply_stencil(STENCIL_DEFAULT)
+
+    def _record(self, key, coarse, fine):
+        self.trials[key] = {"coarse": {str(list(c)): round(v, 4) for c, v in coarse.items()},
+                            "fine": {str(list(c)): round(v, 4) for c, v in fine.items()}}
+        self.cache[key] = list(min(fine, key=fine.get))
 
     # ---- choose and apply ----
     def ensure(self, eng, n_faces):
@@ -231,14 +232,12 @@ class Tuner:
             if kt is None or ks is None:
                 raise RuntimeError("frozen tuner without a cached choice for this device")
         if kt not in self.cache:
-            res = self.tracer_trials(eng)
-            self.trials[kt] = {str(list(c)): round(v, 4) for c, v in res.items()}
-            self.cache[kt] = list(min(res, key=res.get))
+            coarse, fine = self.tracer_trials(eng)
+            self._record(kt, coarse, fine)
             changed = True
         if ks not in self.cache:
-            res = self.stencil_trials(eng)
-            self.trials[ks] = {str(list(c)): round(v, 4) for c, v in res.items()}
-            self.cache[ks] = list(min(res, key=res.get))
+            coarse, fine = self.stencil_trials(eng)
+            self._record(ks, coarse, fine)
             changed = True
         if changed:
             self._store()
