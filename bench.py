@@ -370,51 +370,89 @@ def batched_summary(world, rank, dist):
     """The batched forward: 64 ragged holes (diameter U[2,8] um, mask U[1,3] um, extent d + 8 um,
     dx 0.25, 24 um grid height; ion energy, F / ion and O / F ratios drawn per instance, seed 0),
     30 steps, 2^20 rays per species per step per instance, each step one CUDA graph replay;
-    beside it the plain per-instance loop (run_etch_3d one instance after another) on the first
-    16 instances.  Values are instance-steps/s; device time from CUDA events, max over ranks."""
+    beside it the plain per-instance loop on the first 16 instances, timed on two equal bases:
+      replays: the steps alone -- the batch's graph replays against each instance's own fused
+        step graphs (petch_plan / petch_step, captured per instance), plans, captures and
+        set-up outside the timed interval on both sides (CUDA events);
+      whole calls: everything from the level-set seeds to the last step on both sides -- the
+        BatchEngine built, captured and run against run_etch_3d called once per instance (host
+        clock, synchronised at both ends).
+    Values are instance-steps/s, max over ranks."""
     import torch
     from petch_b200 import params, threed as t3
     from petch_b200.batch import BatchEngine, hole_batch_specs
+    from petch_b200.plan import StepPlan
     fl = params.Flags(chemistry="belen", yield_angular="viennaps", coverage_sticking=True,
                       ion_reflection=True, warm_start_coverage=True)
     specs = hole_batch_specs(BATCH_N, seed=0)
-    eng = BatchEngine(specs, fl, n_ion=BATCH_RAYS, n_neu=BATCH_RAYS, t_end=BATCH_T_END,
-                      n_steps=BATCH_STEPS, seed_offset=1000 * rank)
-    launches = eng.capture()
     flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda")
-    flush.fill_(1.0)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
+    t0 = time.perf_counter()
+    eng = BatchEngine(specs, fl, n_ion=BATCH_RAYS, n_neu=BATCH_RAYS, t_end=BATCH_T_END,
+                      n_steps=BATCH_STEPS, seed_offset=1000 * rank)
+    launches = eng.capture()
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t0
+    flush.fill_(1.0)
+    torch.cuda.synchronize()
     clk = Clocks(int(os.environ.get("LOCAL_RANK", "0")))
     sec = eng.run()
     clocks = clk.stop()
     depths = eng.depths()
+    whole_s = setup_s + sec
     n_plain = BATCH_PLAIN_SAMPLE
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
+
+    def plain_kw(sp):
+        return dict(Lx=sp['Lx'], Ly=sp['Ly'], Lz=sp['Lz'], dx=sp['dx'],
+                    trench_width=sp['trench_width'], mask_th=sp['mask_th'],
+                    sub_top=sp['sub_top'], hole=True, t_end=BATCH_T_END, n_steps=BATCH_STEPS,
+                    par=dict(params.PAR, **sp['par']), flags=fl, n_ion=BATCH_RAYS,
+                    n_neu=BATCH_RAYS, seed_offset=1000 * rank)
+
+    # whole calls: run_etch_3d per instance, set-up included
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
     plain_depths = []
     for sp in specs[:n_plain]:
-        par = dict(params.PAR, **sp['par'])
-        g = t3.run_etch_3d(Lx=sp['Lx'], Ly=sp['Ly'], Lz=sp['Lz'], dx=sp['dx'],
-                           trench_width=sp['trench_width'], mask_th=sp['mask_th'],
-                           sub_top=sp['sub_top'], hole=True, t_end=BATCH_T_END,
-                           n_steps=BATCH_STEPS, par=par, flags=fl, n_ion=BATCH_RAYS,
-                           n_neu=BATCH_RAYS, reinit_method="fsm", verbose=False,
-                           seed_offset=1000 * rank)
+        g = t3.run_etch_3d(**plain_kw(sp), reinit_method="fsm", verbose=False)
         plain_depths.append(t3.center_depth_3d(g))
-    e1.record()
     torch.cuda.synchronize()
-    plain_s = e0.elapsed_time(e1) / 1e3
-    sec, plain_s = rank_reduce([sec, plain_s], "max", dist, world)
+    plain_whole_s = time.perf_counter() - t0
+    # replays: each instance's fused step graphs, plans and captures outside the interval
+    plain_replay_s = 0.0
+    for sp in specs[:n_plain]:
+        plan = StepPlan(**plain_kw(sp))
+        plan.capture()
+        flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        plan.run()
+        e1.record()
+        torch.cuda.synchronize()
+        plain_replay_s += e0.elapsed_time(e1) / 1e3
+        plan.status()
+        plan.close()
+    sec, whole_s, plain_replay_s, plain_whole_s = rank_reduce(
+        [sec, whole_s, plain_replay_s, plain_whole_s], "max", dist, world)
     dd = np.abs(np.array(depths[:n_plain]) - np.array(plain_depths))
     same = _batched_paths_equal(specs[:2], fl)
-    return {"value": world * BATCH_N * BATCH_STEPS / sec, "unit": "instance-steps/s",
+    batch_steps = world * BATCH_N * BATCH_STEPS
+    plain_steps = world * n_plain * BATCH_STEPS
+    return {"value": batch_steps / sec, "unit": "instance-steps/s",
             "seconds": sec, "instances": BATCH_N, "steps": BATCH_STEPS,
             "rays_per_species": BATCH_RAYS,
-            "plain_loop": {"value": world * n_plain * BATCH_STEPS / plain_s,
-                           "unit": "instance-steps/s", "seconds": plain_s,
-                           "sample": f"first {n_plain} instances, run_etch_3d one after another"},
+            "with_setup": {"value": batch_steps / whole_s, "seconds": whole_s,
+                           "setup_seconds": setup_s},
+            "plain_loop": {"replays": {"value": plain_steps / plain_replay_s,
+                                       "seconds": plain_replay_s},
+                           "whole_calls": {"value": plain_steps / plain_whole_s,
+                                           "seconds": plain_whole_s},
+                           "unit": "instance-steps/s",
+                           "sample": f"first {n_plain} instances, one after another"},
+            "ratio": {"replays": (batch_steps / sec) / (plain_steps / plain_replay_s),
+                      "whole_calls": (batch_steps / whole_s) / (plain_steps / plain_whole_s)},
             "graph_launches_per_step": launches, "clocks": clocks,
             "max_depth_diff_vs_plain_um": float(dd.max()),
             "depth_diff_note": "float-atomic tallies: the per-face sums differ in rounding "
@@ -424,7 +462,7 @@ def batched_summary(world, rank, dist):
             "deterministic_runs_equal": same,
             "workload": "64 ragged holes (configs: batched forward), 30 steps, 2^20 rays per "
                         "species, each step one CUDA graph, seed 0",
-            "l2": "256 MB flush before the timed run; instances' working sets exceed L2"}
+            "l2": "256 MB flush before each timed run; instances' working sets exceed L2"}
 
 
 def _batched_paths_equal(specs, fl):
@@ -503,7 +541,8 @@ def differentiation_summary():
         beside central differences with relative step 1e-3, 8 seeds;
       slope_check: a sub-limit etch (rate_scale 0.05; at 1.0 the front moves at the narrow-band
         limit and the profile hardly depends on theta), tangent beside the seed-averaged slope of
-        the loss (relative step 0.1, common random numbers, 32 seeds)."""
+        the loss (relative step 0.1, common random numbers, 32 seeds); again at 2^20 rays, where
+        the front is smoother and the shape feedback the tangents omit is smaller."""
     import torch
     from petch_b200 import _lib, params, threed as t3
     from petch_b200.adjoint import apply_theta, radial_profile, run_etch_3d_tangent
@@ -532,6 +571,9 @@ def differentiation_summary():
                      n_neu=30000)
         sc = _grad_check(small, np.array([100.0, 0.1, 0.05]), np.array([150.0, 0.2, 0.055]),
                          range(200, 232), 0.1, radial_profile, run_etch_3d_tangent)
+        sc_hi = _grad_check(dict(small, n_ion=1 << 20, n_neu=1 << 20), np.array([100.0, 0.1, 0.05]),
+                            np.array([150.0, 0.2, 0.055]), range(200, 232), 0.1, radial_profile,
+                            run_etch_3d_tangent)
     finally:
         _lib.set_deterministic(0)
     return {"bwd_fwd_ratio": tan / fwd, "forward_s": fwd, "tangent_run_s": tan,
@@ -541,6 +583,8 @@ def differentiation_summary():
             "slope_check": dict(sc, workload="8 x 8 x 12 um hole, diameter 4, mask 1, 6 steps "
                                 "of 0.1, 30000 rays, theta0 = (100 eV, 0.1, 0.05), target "
                                 "(150, 0.2, 0.055) seed 1"),
+            "slope_check_2e20_rays": dict(sc_hi, workload="the slope check at 2^20 rays per "
+                                          "species: a smoother front, less shape feedback"),
             "method": "forward-mode tangents (3 directions) through every stage; deterministic "
                       "tallies; mesh, hit topology and random decisions held fixed (the fluxes' "
                       "surface-shape feedback is not differentiated)"}
@@ -605,6 +649,7 @@ def fused_run(par, flags, W, K, tuner, world, local, dist):
         flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda")
         plan = StepPlan(**WORKLOAD, t_end=T_END, n_steps=N_STEPS, par=par, flags=flags,
                         n_ion=RAYS, n_neu=RAYS, max_tris=1 << 20, seed_offset=1000 * dist_rank(dist, world))
+        plan.timing(True)
         plan.capture()
         for _ in range(W):
             plan.replay_step()
@@ -612,7 +657,7 @@ def fused_run(par, flags, W, K, tuner, world, local, dist):
         if world > 1:
             dist.barrier()
         clk = Clocks(local)
-        ev, launches = [], 0
+        ev, launches, trace_ms, faces = [], 0, [], []
         for _ in range(K):
             flush.fill_(1.0)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -620,6 +665,10 @@ def fused_run(par, flags, W, K, tuner, world, local, dist):
             launches += plan.replay_step()
             e1.record()
             ev.append((e0, e1))
+            # the step's neutral-pair launch by the plan's own events (graph event nodes), and
+            # the face count it traced; read between steps, outside the timed intervals
+            trace_ms.append(plan.trace_ms())
+            faces.append(plan.status(check=False)['faces'])
         torch.cuda.synchronize()
         clocks = clk.stop()
         step_ms = [a.elapsed_time(b) for a, b in ev]
@@ -633,7 +682,35 @@ def fused_run(par, flags, W, K, tuner, world, local, dist):
     (launches,) = rank_reduce([launches], "sum", dist, world)
     return {"total_s": total_s, "ms_per_step": 1e3 * total_s / K, "launches": int(launches),
             "clocks": clocks, "faces_last_step": st['faces'], "tracer_settings": settings,
-            "step_ms_first_last": [step_ms[0], step_ms[-1]], "nsub_max": st['nsub_max']}
+            "step_ms_first_last": [step_ms[0], step_ms[-1]], "nsub_max": st['nsub_max'],
+            "trace_ms": trace_ms, "faces": faces, "step_ms": step_ms}
+
+
+def roofline(name, launch_ms, F_launch, step_s, source):
+    """Roofline line of the dominant tracer launch: algorithmic HBM bytes of each launch from that
+    launch's own face count -- read the surface once (tracer triangles 48 B, BVH node 64 B per
+    leaf, leaf start 4 B, coverage 4 B per face) and write the tallies once (ions: 20 B per face;
+    neutrals: both species of a round in one launch, 2 x 4 B) -- over the launches' device
+    time."""
+    launch_ms = np.asarray(launch_ms, np.float64)
+    F_launch = np.asarray(F_launch, np.float64)
+    hbm, src = peaks()
+    tally = 20 if name == "k_ions" else 8
+    per_face = (48 + 4 + tally) + (64 + 4)
+    algo = F_launch * per_face
+    achieved = float(algo.sum() / (launch_ms.sum() / 1e3) / 1e9)
+    return {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": hbm,
+            "unit": "GB/s", "frac": achieved / hbm, "traffic": TRACE_TRAFFIC,
+            "traffic_source": TRACE_TRAFFIC_SOURCE,
+            "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs)" if src == "measured" else src,
+            "algorithmic_bytes_per_launch": int(algo.mean()),
+            "algorithmic_bytes_first_last": [int(algo[0]), int(algo[-1])],
+            "bytes_per_face": per_face, "launch_ms": float(launch_ms.mean()),
+            "launches": len(launch_ms),
+            "share_of_timed": float(launch_ms.sum() / 1e3 / step_s) if step_s else 0.0,
+            "timing_source": source,
+            "note": "ray traversal: BVH and triangles stay in L2, so this kernel is latency / "
+                    "L2 bound; HBM fraction reported as the contract asks, rays/s beside it"}
 
 
 def dist_rank(dist, world):
@@ -662,32 +739,13 @@ def run_b200(args):
     value = world * K / total_s
     # ---- roofline of the dominant kernel (live CUDA events over the timed region) ----
     dom_name = max(kms, key=lambda k: sum(kms[k])) if kms else None
-    hbm, src = peaks()
     roof = None
     if dom_name:
-        launch_ms = np.asarray(kms[dom_name], np.float64)
-        # algorithmic HBM bytes of each launch from that launch's own face count: read the
-        # surface once (tracer triangles 48 B, BVH node 64 B per leaf, leaf start 4 B, coverage
-        # 4 B per face) and write the tallies once (ions: 20 B per face; neutrals: both species
-        # of a round in one launch, 2 x 4 B)
-        tally = 20 if dom_name == "k_ions" else 8
-        per_face = (48 + 4 + tally) + (64 + 4)
         F_launch = np.asarray(info.get('F_launch', []), np.float64)
-        if len(F_launch) != len(launch_ms):
-            F_launch = np.full(len(launch_ms), float(info['F']))
-        algo = F_launch * per_face
-        achieved = float(algo.sum() / (launch_ms.sum() / 1e3) / 1e9)
-        roof = {"kernel": dom_name, "bound": "hbm", "achieved": achieved, "peak": hbm,
-                "unit": "GB/s", "frac": achieved / hbm, "traffic": TRACE_TRAFFIC,
-                "traffic_source": TRACE_TRAFFIC_SOURCE,
-                "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs)" if src == "measured" else src,
-                "algorithmic_bytes_per_launch": int(algo.mean()),
-                "algorithmic_bytes_first_last": [int(algo[0]), int(algo[-1])],
-                "bytes_per_face": per_face, "launch_ms": float(launch_ms.mean()),
-                "launches": len(launch_ms),
-                "share_of_timed": float(launch_ms.sum() / 1e3 / total_s) if total_s else 0.0,
-                "note": "ray traversal: BVH and triangles stay in L2, so this kernel is latency / "
-                        "L2 bound; HBM fraction reported as the contract asks, rays/s beside it"}
+        if len(F_launch) != len(kms[dom_name]):
+            F_launch = np.full(len(kms[dom_name]), float(info['F']))
+        roof = roofline(dom_name, kms[dom_name], F_launch, total_s,
+                        "CUDA events around each launch in the stage-by-stage run")
     mrays = float(np.sum(rays)) * world / total_s / 1e6
     q_tot = float(sum(a for a, _ in work_q)) * world
     v_tot = float(sum(b for _, b in work_q)) * world
@@ -712,8 +770,16 @@ def run_b200(args):
                     path="fused step (petch_plan / petch_step), one CUDA graph replay per step",
                     tracer_settings=f['tracer_settings'], faces_last_step=f['faces_last_step'],
                     step_ms_first_last=f['step_ms_first_last'])
-        if roof is not None:
-            roof["share_of_fused_step"] = float(roof["launch_ms"] / (1e3 * f['total_s'] / K))
+        if roof is not None and f['trace_ms']:
+            # the headline run's own launches: the plan's events around the neutral-pair launch
+            # inside each replayed graph, that step's face count, the replayed steps' time
+            extra = {k: roof[k] for k in ("bvh_queries_per_s", "node_visits_per_s",
+                                          "node_fetch_GBps", "visits_per_query")}
+            roof = roofline("k_neutrals", f['trace_ms'], f['faces'], sum(f['step_ms']) / 1e3,
+                            "plan event nodes around the neutral-pair launch in each replayed "
+                            "step graph of the headline run")
+            roof.update(extra, traversal_rates_source="the stage-by-stage run's BVH query and "
+                                                      "node-visit counters over its trace time")
     out = {"metric": METRIC, "value": head['value'], "unit": "steps/s", "n_gpus": world,
            "steps": K, "warmup": W, "ms_per_step": 1e3 * head['total_s'] / K,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,

@@ -816,6 +816,16 @@ int petch_plan_seek(petch_plan_t* plan, long long step);
  * PETCH_E_LIMIT if a tracer hit a traversal bound. */
 int petch_plan_status(petch_plan_t* plan, petch_step_status* status, void* stream);
 
+/* Device timing of the step's dominant launches (no reference counterpart): with on = 1 the plan
+ * creates two CUDA events that every later petch_step records on its stream, before its first
+ * and after its last neutral-pair trace launch (a warm step has one), as external event nodes
+ * when the step is captured into a graph, so graph replays record them too; on = 0 frees them.
+ * Enable before capturing. */
+int petch_plan_timing(petch_plan_t* plan, int on);
+
+/* Milliseconds between those two events of the last step issued (waits for its end event). */
+int petch_plan_trace_ms(petch_plan_t* plan, float* ms);
+
 /* Frees the plan's workspace (after the work on its streams has finished). */
 int petch_destroy(petch_plan_t* plan);
 

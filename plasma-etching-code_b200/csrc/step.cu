@@ -69,6 +69,17 @@ __global__ void k_accumulate(int* w, const int* hdr) {
     *q += *reinterpret_cast<const unsigned long long*>(w + W_WORK + 2);
 }
 
+// Records a timing event on st: a plain record, or an external event node when st is being
+// captured into a graph (so that every replay records it).
+cudaError_t record_timing_event(cudaEvent_t ev, cudaStream_t st) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing(st, &cs);
+    if (e != cudaSuccess) return e;
+    return cs == cudaStreamCaptureStatusActive
+               ? cudaEventRecordWithFlags(ev, st, cudaEventRecordExternal)
+               : cudaEventRecord(ev, st);
+}
+
 }  // namespace
 }  // namespace petch
 
@@ -93,6 +104,7 @@ struct petch_plan_s {
     int cur;
     long long steps_done;
     void* arena;                    // one allocation holds every buffer above
+    cudaEvent_t trace_ev[2];        // petch_plan_timing: recorded around the neutral-pair traces
 };
 
 namespace {
@@ -288,9 +300,13 @@ extern "C" int petch_step(petch_plan_s* p, void* stream) {
     const int n_fp = c.n_fp > 0 ? c.n_fp : (cold ? 4 : 1);
     const float norm_neu = c.n_neu > 0 ? (float)(A_src / c.n_neu) : 0.0f;
     for (int it = 0; it < n_fp; ++it) {
+        if (it == 0 && p->trace_ev[0])
+            PETCH_CUDA(record_timing_event(p->trace_ev[0], st), "petch_step: timing event");
         PETCH_TRY(trace_neutral_pair_stepped(p->mesh[cur], MT, MV, &c.dom, p->bare[cur], c.betaE,
                                              c.betaO, w + W_STEP, 9, off, 2 + 2 * it, 3 + 2 * it,
                                              0, c.n_neu, p->flux_a, p->flux_b, w + W_WORK, stream));
+        if (it == n_fp - 1 && p->trace_ev[1])
+            PETCH_CUDA(record_timing_event(p->trace_ev[1], st), "petch_step: timing event");
         PETCH_TRY(petch_norm_smooth(p->mesh[cur], MT, MV, p->flux_a, norm_neu, 0.0f, 8.0f, 1,
                                     c.n_smooth, c.smooth_alpha, p->m_F, p->tmp5, p->tmp5 + MT,
                                     stream));
@@ -359,8 +375,31 @@ extern "C" int petch_plan_status(petch_plan_s* p, petch_step_status* s, void* st
     return PETCH_OK;
 }
 
+extern "C" int petch_plan_timing(petch_plan_s* p, int on) {
+    PETCH_REQUIRE(p, "petch_plan_timing: null plan");
+    for (int i = 0; i < 2; ++i) {
+        if (on && !p->trace_ev[i])
+            PETCH_CUDA(cudaEventCreate(&p->trace_ev[i]), "petch_plan_timing: event");
+        if (!on && p->trace_ev[i]) {
+            PETCH_CUDA(cudaEventDestroy(p->trace_ev[i]), "petch_plan_timing: event");
+            p->trace_ev[i] = nullptr;
+        }
+    }
+    return PETCH_OK;
+}
+
+extern "C" int petch_plan_trace_ms(petch_plan_s* p, float* ms) {
+    PETCH_REQUIRE(p && ms, "petch_plan_trace_ms: null pointer");
+    PETCH_REQUIRE(p->trace_ev[0] && p->trace_ev[1], "petch_plan_trace_ms: timing is off");
+    PETCH_CUDA(cudaEventSynchronize(p->trace_ev[1]), "petch_plan_trace_ms: sync");
+    PETCH_CUDA(cudaEventElapsedTime(ms, p->trace_ev[0], p->trace_ev[1]),
+               "petch_plan_trace_ms: elapsed time");
+    return PETCH_OK;
+}
+
 extern "C" int petch_destroy(petch_plan_s* p) {
     if (!p) return PETCH_OK;
+    petch_plan_timing(p, 0);
     cudaError_t e = cudaFree(p->arena);
     delete p;
     if (e != cudaSuccess) return cuda_fail(e, "petch_destroy");

@@ -176,6 +176,8 @@ SIGNATURES = {
     "petch_step": [P, P],
     "petch_plan_status": [P, ctypes.POINTER(StepStatus), P],
     "petch_plan_seek": [P, L],
+    "petch_plan_timing": [P, I],
+    "petch_plan_trace_ms": [P, ctypes.POINTER(ctypes.c_float)],
     "petch_destroy": [P],
 }
 

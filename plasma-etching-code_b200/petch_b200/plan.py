@@ -152,6 +152,17 @@ class StepPlan:
         self.steps_done += 1
         return self.graph_launches[key]
 
+    def timing(self, on=True):
+        """Record CUDA events around each step's neutral-pair trace launches (enable before
+        capture(): the graphs then record them on every replay)."""
+        _lib.call("petch_plan_timing", self.h, int(bool(on)))
+
+    def trace_ms(self):
+        """Device milliseconds of the last step's neutral-pair trace launches (waits for them)."""
+        ms = ctypes.c_float()
+        _lib.call("petch_plan_trace_ms", self.h, ctypes.byref(ms))
+        return float(ms.value)
+
     def status(self, check=True):
         """The plan's accumulated status (one synchronising read); raises on device errors."""
         st = _lib.StepStatus()

@@ -272,3 +272,84 @@ def test_autograd_function_returns_the_jacobian_product():
     np.testing.assert_allclose(theta.grad.numpy(), want, rtol=0.1, atol=1e-6)
     loss = profile_loss(theta.detach().requires_grad_(True), cfg, np.nan_to_num(p2) + 0.1)
     assert torch.isfinite(loss)
+
+
+_HOLE = dict(Lx=8.0, Ly=8.0, Lz=12.0, dx=0.25, trench_width=4.0, mask_th=1.0, sub_top=8.0,
+             hole=True)
+_FLAGS = dict(chemistry="belen", yield_angular="viennaps", coverage_sticking=True,
+              ion_reflection=True, warm_start_coverage=True)
+
+
+def _crn_slope(cfg, theta, k, h_rel, seeds, **kw):
+    """Seed-mean tangent and central difference (common random numbers) of the radial profile
+    along theta_k, averaged over the bins every run defines."""
+    tan, fd = [], []
+    for s in seeds:
+        phi, dphi, geo, _ = run_etch_3d_tangent(theta, seed_offset=s, **cfg, **kw)
+        p, J = radial_profile(phi, geo, dphi)
+        h = h_rel * theta[k]
+        tp, tm = np.array(theta, float), np.array(theta, float)
+        tp[k] += h
+        tm[k] -= h
+        pp = radial_profile(run_etch_3d_tangent(tp, seed_offset=s, **cfg, **kw)[0], geo)[0]
+        pm = radial_profile(run_etch_3d_tangent(tm, seed_offset=s, **cfg, **kw)[0], geo)[0]
+        ok = np.isfinite(p) & np.isfinite(pp) & np.isfinite(pm) & (p > -0.5)
+        tan.append(J[ok, k].mean())
+        fd.append(((pp - pm)[ok] / (2 * h)).mean())
+    return np.array(tan), np.array(fd)
+
+
+def test_loop_tangent_with_a_uniform_rate_matches_central_differences(monkeypatch):
+    """The level-set half of the loop tangent (extension, advection, reinit, the profile) over 6
+    steps: with every face's velocity set to rate_scale * 24 um/min (no tracing), the profile's
+    rate_scale tangent equals its central difference, and both equal depth / rate_scale (the
+    front moves about half a cell per step)."""
+    from petch_b200 import adjoint
+
+    class UniformRate(adjoint.TangentEngine):
+        def flux_tangent(self, n_ion, n_neu, seed, warm):
+            pass
+
+        def rate_extend_tangent(self, band):
+            rs = float(self.par['rate_scale'])
+            self.V.fill_(24.0 * rs)
+            self.dV.zero_()
+            self.dV[2].fill_(24.0)
+            self.small[6:8].zero_()
+            self.small[7:8].view(torch.float32).fill_(24.0 * rs)
+            m = self.mesh
+            nx, ny, nz = self.shape
+            _lib.call("petch_extend_velocity_dual", m.id, m.MT, m.MV, self.phi.data_ptr(),
+                      self.mask.data_ptr(), nx, ny, nz, self.dx, float(band), self.V.data_ptr(),
+                      self.dV.data_ptr(), self.F.data_ptr(), self.dF.data_ptr(), 1,
+                      self.active.data_ptr(), self.small[8:9].data_ptr(), self.ncell,
+                      self.small[0:6].data_ptr(), t3._sp())
+
+    monkeypatch.setattr(adjoint, "TangentEngine", UniformRate)
+    fl = petch.Flags(**_FLAGS)
+    flat = dict(_HOLE, Lx=4.0, Ly=4.0, trench_width=8.0, hole=False)
+    for geo_kw in (_HOLE, dict(_HOLE, Lx=16.0, Ly=16.0, trench_width=12.0), flat):
+        cfg = dict(geo_kw, t_end=0.6, n_steps=6, flags=fl, n_ion=1000, n_neu=1000)
+        theta = np.array([100.0, 0.1, 0.05])
+        tan, fd = _crn_slope(cfg, theta, 2, 0.01, [0])
+        phi, _, geo, _ = run_etch_3d_tangent(theta, seed_offset=0, **cfg)
+        p = radial_profile(phi, geo)[0]
+        etched = p[np.isfinite(p) & (p > -0.5)].mean()
+        assert abs(tan[0] - fd[0]) <= 0.03 * abs(fd[0]), (geo_kw, tan, fd)
+        assert abs(tan[0] * theta[2] - etched) <= 0.03 * etched, (geo_kw, tan, etched)
+
+
+def test_one_step_loop_tangent_matches_the_seed_averaged_difference():
+    """The first step's mesh does not depend on theta, so holding it fixed is exact there: the
+    one-step profile tangent equals the common-random-number central difference (16 seeds,
+    30000 rays) along mean ion energy and rate_scale, within 3 % plus three standard errors."""
+    fl = petch.Flags(**_FLAGS)
+    cfg = dict(_HOLE, t_end=0.1, n_steps=1, flags=fl, n_ion=30000, n_neu=30000)
+    _lib.set_deterministic(8 * 16 * 131072)
+    try:
+        for k in (0, 2):
+            tan, fd = _crn_slope(cfg, np.array([100.0, 0.1, 0.05]), k, 0.02, range(300, 316))
+            se = fd.std(ddof=1) / np.sqrt(len(fd))
+            assert abs(tan.mean() - fd.mean()) <= 0.03 * abs(fd.mean()) + 3 * se, (k, tan, fd)
+    finally:
+        _lib.set_deterministic(0)

@@ -111,6 +111,39 @@ def test_graph_replay_equals_eager_steps():
     assert torch.equal(a, b) and torch.equal(a, c)
 
 
+def test_trace_timing_events_in_eager_steps_and_graph_replays():
+    """petch_plan_timing: the events around a step's neutral-pair launch are recorded by eager
+    steps and by every replay of a captured graph (external event nodes), and bracket less than
+    the whole step; timing leaves the results unchanged (bit-equal level sets)."""
+    par = _par(True)
+    kw = dict(**HOLE, t_end=0.6, n_steps=6, par=par, flags=SF6O2, n_ion=1 << 18, n_neu=1 << 18)
+    _lib.set_deterministic(16 * t3.default_capacity(grid_shape(8.0, 8.0, 12.0, 0.25)))
+    try:
+        plain = StepPlan(**kw)
+        plain.run(use_graph=False)
+        timed = StepPlan(**kw)
+        timed.timing(True)
+        timed.step()
+        assert timed.trace_ms() > 0.0                    # the cold step, eager
+        timed.capture()
+        ms = []
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            timed.replay_step()
+            e1.record()
+            torch.cuda.synchronize()
+            ms.append((timed.trace_ms(), e0.elapsed_time(e1)))
+        a, b = plain.phi.clone(), timed.phi.clone()
+        for p in (plain, timed):
+            p.close()
+    finally:
+        _lib.set_deterministic(0)
+    assert torch.equal(a, b)
+    for t, step in ms:
+        assert 0.0 < t < step, ms
+
+
 def test_capacity_overflow_is_reported():
     par = _par(True)
     plan = StepPlan(**HOLE, t_end=0.2, n_steps=2, par=par, flags=SF6O2, n_ion=1000, n_neu=1000,
