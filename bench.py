@@ -109,10 +109,10 @@ def rank_reduce(values, op, dist, world):
 
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one neutral-pair launch of this
 # workload, from the ncu capture summarised in profiles/k_trace_neutral_pair_trench_c1_deep.md.
-TRACE_TRAFFIC = 2203299000 + 3442106000
-TRACE_TRAFFIC_SOURCE = ("ncu --set full, the step-60 launch (301,728 faces, 38.6 MB algorithmic): "
-                        "2.203 GB read + 3.442 GB written, per launch; the traversal stacks' "
-                        "local-memory lines spilled through L2")
+TRACE_TRAFFIC = 2247642000 + 3198055000
+TRACE_TRAFFIC_SOURCE = ("ncu --set full, the step-60 launch (301,914 faces, 38.6 MB algorithmic): "
+                        "2.248 GB read + 3.198 GB written, per launch; the traversal stacks' and "
+                        "register spills' local-memory lines overflowing L1 and L2")
 
 
 def peaks():
@@ -523,10 +523,13 @@ def _grad_check(cfg, theta0, theta_t, seeds, h_rel, radial_profile, run):
             Lm = loss(radial_profile(run(tm, seed_offset=s, **cfg)[0], geo)[0])[0]
             g_fd[i, k] = (Lp - Lm) / (2 * h)
     names = ("Emean", "O_F", "rate_scale")
+    tan, fd = g_tan / len(seeds), g_fd.mean(0)
+    se = g_fd.std(0, ddof=1) / np.sqrt(len(seeds))
     return {"loss": float(np.mean(losses)),
-            "grad_tangent": dict(zip(names, map(float, g_tan / len(seeds)))),
-            "grad_fd": dict(zip(names, map(float, g_fd.mean(0)))),
-            "grad_fd_stderr": dict(zip(names, map(float, g_fd.std(0, ddof=1) / np.sqrt(len(seeds))))),
+            "grad_tangent": dict(zip(names, map(float, tan))),
+            "grad_fd": dict(zip(names, map(float, fd))),
+            "grad_fd_stderr": dict(zip(names, map(float, se))),
+            "rel_err_vs_fd": dict(zip(names, map(float, (tan - fd) / np.maximum(np.abs(fd), 1e-300)))),
             "fd_step_rel": h_rel, "seeds": len(seeds)}
 
 
@@ -569,6 +572,9 @@ def differentiation_summary():
         small = dict(Lx=8.0, Ly=8.0, Lz=12.0, dx=0.25, trench_width=4.0, mask_th=1.0,
                      sub_top=8.0, hole=True, t_end=0.6, n_steps=6, flags=fl, n_ion=30000,
                      n_neu=30000)
+        c3_sub = _grad_check(cfg, np.array([100.0, 0.1, 0.025]), np.array([150.0, 0.2, 0.0275]),
+                             range(100, 100 + 4 * DIFF_SEEDS), 0.1, radial_profile,
+                             run_etch_3d_tangent)
         sc = _grad_check(small, np.array([100.0, 0.1, 0.05]), np.array([150.0, 0.2, 0.055]),
                          range(200, 232), 0.1, radial_profile, run_etch_3d_tangent)
         sc_hi = _grad_check(dict(small, n_ion=1 << 20, n_neu=1 << 20), np.array([100.0, 0.1, 0.05]),
@@ -580,6 +586,10 @@ def differentiation_summary():
             "config3": dict(c3, workload="config-0 hole, 20 steps of the 40-step 3.0 schedule, "
                             "30000 rays per species, theta0 = (100 eV, 0.1, 1.0), target "
                             "(150, 0.2, 1.1) seed 1"),
+            "config3_subsaturated": dict(c3_sub, workload="the config-0 hole and schedule of "
+                                         "config3 at rate_scale 0.025 (SF6O2's default, below "
+                                         "the narrow-band speed limit), target (150, 0.2, "
+                                         "0.0275) seed 1, relative step 0.1, 32 seeds"),
             "slope_check": dict(sc, workload="8 x 8 x 12 um hole, diameter 4, mask 1, 6 steps "
                                 "of 0.1, 30000 rays, theta0 = (100 eV, 0.1, 0.05), target "
                                 "(150, 0.2, 0.055) seed 1"),
@@ -793,6 +803,9 @@ def run_b200(args):
     for k in ("tracer_settings", "faces_last_step", "step_ms_first_last"):
         if k in head:
             out[k] = head[k]
+    if rank == 0 and not args.no_e2e:
+        # right after the headline run, before the secondary sections load the device
+        out["e2e"] = e2e(par, flags, W, K, info['phi_W'])
     if tuner is not None:
         out["tuning"] = tuning_report(tuner)
     if not args.no_radiosity:
@@ -807,8 +820,6 @@ def run_b200(args):
         out["inverse_design"] = inverse_design_summary(world, rank, dist, args.inverse_iters)
     if rank == 0 and not args.no_published:
         out["published_config"] = published_config_summary()
-    if rank == 0 and not args.no_e2e:
-        out["e2e"] = e2e(par, flags, W, K, info['phi_W'])
     if rank == 0 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(par, flags, dict(phi=info['phi_last'],
                                                             bare=info['bare_last'],

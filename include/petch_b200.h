@@ -163,11 +163,11 @@ int petch_tracer_config(int bvh_width, int steps_per_round, int keep_lanes);
  * a speed knob of the tuner. */
 int petch_tally_aggregation(int on);
 
-/* Leaf grouping of the binary traversal for later trace calls (knob of the tuner): 0 off, or
- * g in 2..8 -- each warp iteration then runs the triangle tests of the lanes at a leaf when they
- * are at least 1/g of the lanes with an open query, otherwise the box tests of the lanes at an
- * internal node, instead of both paths in every iteration.  Default 2.  Results do not depend
- * on it (each lane's traversal order is unchanged). */
+/* Leaf grouping of the traversal (binary and 8-wide) for later trace calls (knob of the tuner):
+ * 0 off, or g in 2..8 -- each warp iteration then runs the triangle tests of the lanes at a leaf
+ * when they are at least 1/g of the lanes with an open query, otherwise the box tests of the
+ * lanes at an internal node, instead of both paths in every iteration.  Default 2.  Results do
+ * not depend on it (each lane's traversal order is unchanged). */
 int petch_tracer_grouping(int group);
 
 /* The tracer settings in force: out[0] BVH width, [1] steps per round, [2] keep lanes, [3]

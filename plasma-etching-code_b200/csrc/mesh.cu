@@ -163,41 +163,61 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* total)
     return incl - v;
 }
 
-// Pass 1: per node, cube configuration + owned-edge crossings; per block, packed totals.
-// info bits: 0-7 cube config (corner c solid <=> phi > 0), 8-10 owned x/y/z edge crossed,
-// 11 cube exists (node is not on a max face).
-__global__ void __launch_bounds__(kB) k_mc_count(const float* __restrict__ phi, Dims d, Morton mo,
-                                                 uint32_t npad, uint16_t* __restrict__ info,
+// Pass 1a, grid order: per node, cube configuration + owned-edge crossings (info bits: 0-7 cube
+// config (corner c solid <=> phi > 0), 8-10 owned x/y/z edge crossed, 11 cube exists (node is not
+// on a max face)).  Threads run along z (one block row per grid row), so the node and its seven
+// upper neighbours are read as contiguous row segments.
+constexpr int kMcZ = 128, kMcRows = 2;
+
+__global__ void __launch_bounds__(kMcZ * kMcRows) k_mc_classify(const float* __restrict__ phi,
+                                                                Dims d,
+                                                                uint16_t* __restrict__ info_lin) {
+    const int rows = d.nx * d.ny;
+    for (int row = blockIdx.x * kMcRows + threadIdx.y; row < rows; row += gridDim.x * kMcRows) {
+        const int i = row / d.ny, j = row - (row / d.ny) * d.ny;
+        const long long base = (long long)row * d.nz;
+        for (int k = threadIdx.x; k < d.nz; k += kMcZ) {
+            const long long c = base + k;
+            const bool s0 = phi[c] > 0.0f;
+            uint32_t cross = 0;
+            if (i + 1 < d.nx) cross |= (uint32_t)(s0 != (phi[c + d.plane] > 0.0f)) << 0;
+            if (j + 1 < d.ny) cross |= (uint32_t)(s0 != (phi[c + d.nz] > 0.0f)) << 1;
+            if (k + 1 < d.nz) cross |= (uint32_t)(s0 != (phi[c + 1] > 0.0f)) << 2;
+            uint32_t inf = cross << 8;
+            if (i + 1 < d.nx && j + 1 < d.ny && k + 1 < d.nz) {
+                uint32_t cfg = 0;
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const long long cc = c + (q & 1) * d.plane + ((q >> 1) & 1) * (long long)d.nz +
+                                         ((q >> 2) & 1);
+                    cfg |= (uint32_t)(phi[cc] > 0.0f) << q;
+                }
+                inf |= cfg | (1u << 11);
+            }
+            info_lin[c] = (uint16_t)inf;
+        }
+    }
+}
+
+// Pass 1b, Morton order: each node's info gathered from the grid-order pass, and per block the
+// packed totals (faces, vertices, BVH leaves) the later passes offset from.
+__global__ void __launch_bounds__(kB) k_mc_count(const uint16_t* __restrict__ info_lin, Dims d,
+                                                 Morton mo, uint32_t npad,
+                                                 uint16_t* __restrict__ info,
                                                  int4* __restrict__ bsum) {
     uint32_t t = blockIdx.x * kB + threadIdx.x;
     uint32_t nt = 0, nv = 0, nl = 0;
     if (t < npad) {
         int c3[3];
         m_decode(mo, t, c3);
-        int i = c3[0], j = c3[1], k = c3[2];
-        uint16_t inf = 0;
-        if (i < d.nx && j < d.ny && k < d.nz) {
-            long long c = i * d.plane + (long long)j * d.nz + k;
-            bool s0 = phi[c] > 0.0f;
-            uint32_t cross = 0;
-            if (i + 1 < d.nx) cross |= (uint32_t)(s0 != (phi[c + d.plane] > 0.0f)) << 0;
-            if (j + 1 < d.ny) cross |= (uint32_t)(s0 != (phi[c + d.nz] > 0.0f)) << 1;
-            if (k + 1 < d.nz) cross |= (uint32_t)(s0 != (phi[c + 1] > 0.0f)) << 2;
-            inf = (uint16_t)(cross << 8);
-            if (i + 1 < d.nx && j + 1 < d.ny && k + 1 < d.nz) {
-                uint32_t cfg = 0;
-#pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    long long cc = c + (q & 1) * d.plane + ((q >> 1) & 1) * (long long)d.nz + ((q >> 2) & 1);
-                    cfg |= (uint32_t)(phi[cc] > 0.0f) << q;
-                }
-                inf |= (uint16_t)(cfg | (1u << 11));
-                nt = c_mc.ntri[cfg];
-            }
-            nv = __popc(cross);
+        uint32_t inf = 0;
+        if (c3[0] < d.nx && c3[1] < d.ny && c3[2] < d.nz) {
+            inf = info_lin[c3[0] * d.plane + (long long)c3[1] * d.nz + c3[2]];
+            if ((inf >> 11) & 1u) nt = c_mc.ntri[inf & 255u];
+            nv = __popc((inf >> 8) & 7u);
             nl = nt > 0;
         }
-        info[t] = inf;
+        info[t] = (uint16_t)inf;
     }
     uint32_t tot;
     block_excl_scan(nt | (nv << 11) | (nl << 21), &tot);
@@ -820,7 +840,16 @@ extern "C" int petch_mesh_build(const float* phi, int nx, int ny, int nz, double
     Dims d{nx, ny, nz, (long long)ny * nz};
     MeshView m = mesh_view(mesh, max_tris, max_verts);
 
-    k_mc_count<<<nb, kB, 0, st>>>(phi, d, mo, npad, s.info, s.bsum);
+    // the grid-order info lives in voff's space until k_mc_verts writes the vertex offsets
+    // (npad >= cells, 4 bytes per node >= 2 bytes per cell)
+    uint16_t* info_lin = reinterpret_cast<uint16_t*>(s.voff);
+    {
+        const int rows = nx * ny;
+        const int gb = (rows + kMcRows - 1) / kMcRows;
+        k_mc_classify<<<gb, dim3(kMcZ, kMcRows), 0, st>>>(phi, d, info_lin);
+        PETCH_LAUNCH_CHECK("k_mc_classify");
+    }
+    k_mc_count<<<nb, kB, 0, st>>>(info_lin, d, mo, npad, s.info, s.bsum);
     PETCH_LAUNCH_CHECK("k_mc_count");
     PETCH_CUDA(cub::DeviceScan::ExclusiveScan(s.cub_tmp, s.cub_bytes, s.bsum, s.boff, Int4Add(),
                                               make_int4(0, 0, 0, 0), nb, st),

@@ -22,20 +22,25 @@ constexpr int kTB = 128;
 #define PETCH_TRACE_MIN_BLOCKS 8
 #endif
 #ifndef PETCH_TRACE_MIN_BLOCKS_RR
-#define PETCH_TRACE_MIN_BLOCKS_RR 12
+#define PETCH_TRACE_MIN_BLOCKS_RR 9
+#endif
+#ifndef PETCH_TRACE_MIN_BLOCKS_RR_BATCH
+#define PETCH_TRACE_MIN_BLOCKS_RR_BATCH 12
 #endif
 #ifndef PETCH_TRACE_MIN_BLOCKS_RR_TAN
 #define PETCH_TRACE_MIN_BLOCKS_RR_TAN 10
 #endif
 // Resident blocks of the persistent tracers per SM (the binary-traversal launches use no shared
 // memory, so registers alone set them): 8 x 4 warps (<= 64 registers per thread) for the ion
-// shaders; 12 x 4 (<= 40 registers) for the single-instance Russian-roulette neutral shaders,
-// whose traversal-bound loop gains more from the extra warps than it loses to spills (trench
-// workload: 10 -> 12 blocks 1.8 % faster, 16 blocks at 32 registers 12 % slower) and the batched
-// neutral kinds (64 ragged holes: +1.7 %); 10 x 4 (<= 48 registers) for the neutral tangent
-// shaders, which carry three weight tangents per ray.
+// shaders; 9 x 4 (<= 56 registers) for the single-instance Russian-roulette neutral shaders
+// (trench workload, 100-step run with leaf grouping: 12 blocks at 40 registers spill ~300 B per
+// thread and run 4.8 % slower, 10 blocks 2.9 % slower, 8 blocks at 64 registers 0.5 % slower);
+// 12 x 4 (<= 40 registers) for the batched neutral kinds (64 ragged holes: +1.7 % against 10);
+// 10 x 4 (<= 48 registers) for the neutral tangent shaders, which carry three weight tangents
+// per ray.
 constexpr int kTraceMinBlocks = PETCH_TRACE_MIN_BLOCKS;
 constexpr int kTraceMinBlocksRR = PETCH_TRACE_MIN_BLOCKS_RR;
+constexpr int kTraceMinBlocksRRBatch = PETCH_TRACE_MIN_BLOCKS_RR_BATCH;
 constexpr int kTraceMinBlocksRRTan = PETCH_TRACE_MIN_BLOCKS_RR_TAN;
 constexpr long long kMaxRounds = 1LL << 24;   // per-warp bound on tracer rounds (error bit 4)
 constexpr unsigned kFull = 0xffffffffu;
@@ -723,11 +728,12 @@ struct TraceCtl {
     uint32_t seed_mul, seed_off;
 };
 
-// Binary traversal steps of a warp with the node and leaf halves grouped: each iteration runs
-// leaf steps for the lanes at a leaf when they are at least 1/group of the open lanes, otherwise
-// node steps for the lanes at an internal node, so the triangle and the box paths do not take
-// turns inside one iteration with few lanes each (each iteration advances at least one lane).
-template <class St>
+// Traversal steps of a warp (binary or 8-wide tree) with the node and leaf halves grouped: each
+// iteration runs leaf steps for the lanes at a leaf when they are at least 1/group of the open
+// lanes, otherwise node steps for the lanes at an internal node, so the triangle and the box
+// paths do not take turns inside one iteration with few lanes each (each iteration advances at
+// least one lane).
+template <bool WIDE, class St>
 __device__ __forceinline__ void grouped_steps(const Tracer& T, Query& q, St& stk, int& phase,
                                               int steps, int keep_now, int group, int* err) {
     for (int s = 0; s < steps; ++s) {
@@ -738,8 +744,11 @@ __device__ __forceinline__ void grouped_steps(const Tracer& T, Query& q, St& stk
         const int nl = __popc(__ballot_sync(kFull, at_leaf));
         const bool leaves = nl * group >= no;
         if (open && at_leaf == leaves) {
-            const bool fin = visit_bound(q, err) ||
-                             (leaves ? step_binary_leaf(T, q, stk) : step_binary_node(T, q, stk, err));
+            bool fin = visit_bound(q, err);
+            if (!fin) {
+                if (WIDE) fin = leaves ? step_wide_leaf(T, q, stk) : step_wide_node(T, q, stk, err);
+                else fin = leaves ? step_binary_leaf(T, q, stk) : step_binary_node(T, q, stk, err);
+            }
             if (fin) phase = 2;
         }
     }
@@ -793,8 +802,8 @@ __global__ void __launch_bounds__(kTB, S::kMinBlocks) k_trace(MeshView m, Domain
         // done (keep 0): each round makes progress.
         pool_empty = pool_empty || __any_sync(kFull, ray == -2);
         const int keep_now = pool_empty ? 0 : keep;
-        if (!WIDE && c.group > 0)
-            grouped_steps(T, q, stk, phase, steps, keep_now, c.group, &err);
+        if (c.group > 0)
+            grouped_steps<WIDE>(T, q, stk, phase, steps, keep_now, c.group, &err);
         else
         for (int s = 0; s < steps; ++s) {
             if (__popc(__ballot_sync(kFull, phase == 1)) <= keep_now) break;
@@ -931,7 +940,7 @@ __global__ void k_zero_batch(BatchTable tab, MeshOffsets L, int MT, int MV, int 
 // stream of ray r of its own kind-1 launch; 5 the same with the weight tangents of kind 3 (the
 // second species' into dout2).
 template <int KIND>
-__global__ void __launch_bounds__(kTB, (KIND == 1 || KIND == 4) ? kTraceMinBlocksRR
+__global__ void __launch_bounds__(kTB, (KIND == 1 || KIND == 4) ? kTraceMinBlocksRRBatch
                                     : ((KIND == 3 || KIND == 5) ? kTraceMinBlocksRRTan
                                                                 : kTraceMinBlocks))
 k_trace_batch(BatchTable tab, MeshOffsets L, int MT, int MV, float beta, float beta2,
@@ -1009,7 +1018,7 @@ k_trace_batch(BatchTable tab, MeshOffsets L, int MT, int MV, float beta, float b
         pool_empty = pool_empty || __any_sync(kFull, ray == -2);
         const int keep_now = pool_empty ? 0 : keep;
         if (group > 0)
-            grouped_steps(T, q, stk, phase, steps, keep_now, group, &err);
+            grouped_steps<false>(T, q, stk, phase, steps, keep_now, group, &err);
         else
             for (int s = 0; s < steps; ++s) {
                 if (__popc(__ballot_sync(kFull, phase == 1)) <= keep_now) break;
@@ -1088,11 +1097,58 @@ struct GridArgs {
 };
 
 // extend_velocity_gpu / _extend_kernel (threed.py:1324-1346): cells with |phi| < band take the
-// velocity of the nearest face (search radius first limited to band + 2 dx, widened to the
-// reference's 1e6 if nothing is found there); all other cells get 0.  With fold != 0, mask cells
-// are written as -1 (the advection's pinned-cell marker) and band cells with F > 0 are listed in
-// `active` for the sparse advection.  With dV (tangents [3][MT]) the same nearest face also gives
+// velocity of the nearest face, all other cells get 0.  With fold != 0, mask cells are written as
+// -1 (the advection's pinned-cell marker) and band cells with F > 0 are listed in `active` for
+// the sparse advection.  With dV (tangents [3][MT]) the same nearest face also gives
 // dF[c + k n] = dV[f + k MT] on the band (0 elsewhere), as petch_extend_tangent.
+//
+// Each warp walks 32 consecutive cells at a time (a z-run of a column, of which only the few
+// cells near the front are in the band) and queues its band cells in shared memory; whenever 32
+// are queued, the warp runs 32 nearest-face queries with every lane busy.  A query first searches
+// within |phi| + 1.5 dx (phi is a distance to the front, which the mesh follows to within a
+// cell), then within band + 2 dx, then without a limit: each stage returns the nearest face
+// within its radius (exact ties to the lower face index), so the result is the global nearest
+// face whichever stage finds one.  Pinned cells skip the query unless tangents are wanted.
+constexpr int kExtQ = 64;   // queue slots per warp: < 32 carried over + 32 added
+
+template <bool CENTROID>
+__device__ __forceinline__ void extend_cell(const MeshView& m, int L, const GridArgs& G,
+                                            long long c, float v, bool pinned,
+                                            const float* __restrict__ V, float* __restrict__ Fs,
+                                            int fold, int* active, int* n_active, int max_active,
+                                            const float* __restrict__ dV, float* __restrict__ dF,
+                                            int* err) {
+    float out = 0.0f;
+    float dout[3] = {0.0f, 0.0f, 0.0f};
+    if (!pinned || dV) {
+        const long long r = c / G.nz;
+        const int k = (int)(c - r * G.nz);
+        const int i = (int)(r / G.ny);
+        const int j = (int)(r - (long long)i * G.ny);
+        const float3 p = make_float3((float)(i * G.dx), (float)(j * G.dx), (float)(k * G.dx));
+        const float r_near = (float)(G.band + 2.0 * G.dx);
+        const float r_small = fabsf(v) + (float)(1.5 * G.dx);
+        int f = -1;
+        if (r_small < r_near) f = nearest_prim<CENTROID>(m, L, p, r_small * r_small, err);
+        if (f < 0) f = nearest_prim<CENTROID>(m, L, p, r_near * r_near, err);
+        if (f < 0) f = nearest_prim<CENTROID>(m, L, p, 1.0e12f, err);
+        if (f >= 0) {
+            out = V[f];
+            if (dV)
+                for (int q = 0; q < 3; ++q) dout[q] = dV[f + (long long)q * m.MT];
+        }
+    }
+    if (pinned) out = -1.0f;
+    Fs[c] = out;
+    if (dF)
+        for (int q = 0; q < 3; ++q) dF[c + q * G.n] = dout[q];
+    if (fold && active && out > 0.0f) {
+        const int s = atomicAdd(n_active, 1);
+        if (s < max_active) active[s] = (int)c;
+        else *err |= 2;
+    }
+}
+
 template <bool CENTROID>
 __global__ void __launch_bounds__(kTB) k_extend(MeshView m, GridArgs G, const float* __restrict__ phi,
                                                 const uint8_t* __restrict__ mask,
@@ -1100,38 +1156,59 @@ __global__ void __launch_bounds__(kTB) k_extend(MeshView m, GridArgs G, const fl
                                                 int fold, int* active, int* n_active, int max_active,
                                                 int* work, const float* __restrict__ dV = nullptr,
                                                 float* __restrict__ dF = nullptr) {
+    __shared__ long long s_cell[kTB / 32][kExtQ];
+    __shared__ float s_phi[kTB / 32][kExtQ];
     const int L = min(m.hdr[HDR_L], m.MT);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    long long* qc = s_cell[wid];
+    float* qv = s_phi[wid];
     int err = 0;
-    const float r_near = (float)(G.band + 2.0 * G.dx);
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < G.n;
-         c += (long long)gridDim.x * blockDim.x) {
-        float v = phi[c];
-        bool pinned = fold && mask && mask[c];
-        float out = 0.0f;
-        float dout[3] = {0.0f, 0.0f, 0.0f};
-        if ((double)fabsf(v) < G.band) {
-            long long r = c / G.nz;
-            int k = (int)(c - r * G.nz);
-            int i = (int)(r / G.ny);
-            int j = (int)(r - (long long)i * G.ny);
-            float3 p = make_float3((float)(i * G.dx), (float)(j * G.dx), (float)(k * G.dx));
-            int f = nearest_prim<CENTROID>(m, L, p, r_near * r_near, &err);
-            if (f < 0) f = nearest_prim<CENTROID>(m, L, p, 1.0e12f, &err);
-            if (f >= 0) {
-                out = V[f];
-                if (dV)
-                    for (int q = 0; q < 3; ++q) dout[q] = dV[f + (long long)q * m.MT];
+    int nq = 0;                                      // warp-uniform queue length
+    const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long base = ((long long)blockIdx.x * (blockDim.x >> 5) + wid) * 32; base < G.n;
+         base += warps * 32) {
+        const long long c = base + lane;
+        const bool in = c < G.n;
+        const float v = in ? phi[c] : 0.0f;
+        const bool band = in && (double)fabsf(v) < G.band;
+        if (in && !band) {
+            Fs[c] = (fold && mask && mask[c]) ? -1.0f : 0.0f;
+            if (dF)
+                for (int q = 0; q < 3; ++q) dF[c + q * G.n] = 0.0f;
+        }
+        const unsigned bal = __ballot_sync(kFull, band);
+        if (band) {
+            const int slot = nq + __popc(bal & ((1u << lane) - 1u));
+            qc[slot] = c;
+            qv[slot] = v;
+        }
+        nq += __popc(bal);
+        __syncwarp();
+        if (nq >= 32) {
+            const long long cc = qc[lane];
+            const float vv = qv[lane];
+            const int rest = nq - 32;
+            long long tc = 0;
+            float tv = 0.0f;
+            if (lane < rest) {
+                tc = qc[32 + lane];
+                tv = qv[32 + lane];
             }
+            __syncwarp();
+            if (lane < rest) {
+                qc[lane] = tc;
+                qv[lane] = tv;
+            }
+            nq = rest;
+            __syncwarp();
+            extend_cell<CENTROID>(m, L, G, cc, vv, fold && mask && mask[cc], V, Fs, fold, active,
+                                  n_active, max_active, dV, dF, &err);
         }
-        if (pinned) out = -1.0f;
-        Fs[c] = out;
-        if (dF)
-            for (int q = 0; q < 3; ++q) dF[c + q * G.n] = dout[q];
-        if (fold && active && out > 0.0f) {
-            int s = atomicAdd(n_active, 1);
-            if (s < max_active) active[s] = (int)c;
-            else err |= 2;
-        }
+    }
+    if (lane < nq) {
+        const long long cc = qc[lane];
+        extend_cell<CENTROID>(m, L, G, cc, qv[lane], fold && mask && mask[cc], V, Fs, fold, active,
+                              n_active, max_active, dV, dF, &err);
     }
     if (err) atomicOr(work + 1, err);
 }

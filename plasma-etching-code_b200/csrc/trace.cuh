@@ -290,8 +290,10 @@ __device__ __forceinline__ float qbyte(uint32_t lo4, uint32_t hi4, int k) {
 // Traversal stack: (node ref, entry distance) pairs in the lane's local memory, at most kWStack
 // deep (deeper pushes set error bit 1).  pop() takes the nearest stacked entry that can still
 // beat the current hit (entries beyond it are dropped without a fetch); false if none is left.
-// (A variant holding the top 4 or 8 entries in shared memory was measured on the trench
-// workload: 2-4 % slower, since its shared memory comes out of the L1 that caches the tree.)
+// (Variants measured on the trench workload: the top 4 or 8 entries in shared memory, 2-4 %
+// slower, since its shared memory comes out of the L1 that caches the tree; node references
+// only, each popped entry culled by its own box tests instead of its stored distance, 4.5 %
+// slower.)
 #ifndef PETCH_STACK_PACKED
 #define PETCH_STACK_PACKED 1
 #endif
@@ -353,17 +355,12 @@ __device__ __forceinline__ void query_leaf(const Tracer& T, Query& q, int f0, in
             q.f = f;
 }
 
-// One step of the 8-wide traversal; returns true once the query has finished.
+// One step of the 8-wide traversal; returns true once the query has finished.  The internal-node
+// and leaf halves are also callable on their own, as the binary traversal's (leaf grouping).
 template <class St>
-__device__ __forceinline__ bool step_wide(const Tracer& T, Query& q, St& st, int* err) {
-    if (q.cur == kDone) return true;
-    if (++q.visits > kMaxVisits) {
-        *err |= 1;
-        q.cur = kDone;
-        return true;
-    }
+__device__ __forceinline__ bool step_wide_node(const Tracer& T, Query& q, St& st, int* err) {
     const int cur = q.cur;
-    if (cur >= 0) {
+    {
         float4 v0, v1, v2, v3, v4, v5;
         if (cur < T.nsm) {
             const float4* p = T.snodes + 6 * cur;
@@ -421,12 +418,27 @@ __device__ __forceinline__ bool step_wide(const Tracer& T, Query& q, St& st, int
             }
             return false;
         }
-    } else {
-        int code = -cur - 1;
-        int f0 = code >> 3;
-        query_leaf(T, q, f0, f0 + (code & 7));
     }
     return !st.pop(q);
+}
+
+template <class St>
+__device__ __forceinline__ bool step_wide_leaf(const Tracer& T, Query& q, St& st) {
+    const int code = -q.cur - 1;
+    const int f0 = code >> 3;
+    query_leaf(T, q, f0, f0 + (code & 7));
+    return !st.pop(q);
+}
+
+template <class St>
+__device__ __forceinline__ bool step_wide(const Tracer& T, Query& q, St& st, int* err) {
+    if (q.cur == kDone) return true;
+    if (++q.visits > kMaxVisits) {
+        *err |= 1;
+        q.cur = kDone;
+        return true;
+    }
+    return q.cur >= 0 ? step_wide_node(T, q, st, err) : step_wide_leaf(T, q, st);
 }
 
 // One step of the binary traversal; returns true once the query has finished.  The internal-node

@@ -7,7 +7,7 @@ Tracer knobs (petch_tracer_config, petch_tally_aggregation, petch_tracer_groupin
     steps         traversal steps a warp runs for its open queries between shading rounds
     keep          lanes that may still be traversing when a warp stops to shade and refill
     aggregate     warp-aggregated deposits (tried against the fastest candidates)
-    grouping      leaf grouping of the binary traversal (0 off, or the 1/g share of open lanes
+    grouping      leaf grouping of the traversal (0 off, or the 1/g share of open lanes
                   at a leaf that switches a warp iteration to triangle tests)
 Stencil knob (petch_stencil_config): the block shape (threads along z x grid rows) of the
 row-mapped Eikonal passes.
@@ -33,10 +33,9 @@ import torch
 
 from . import _lib
 
-# tracer settings: (bvh_width, steps, keep, aggregate, grouping); grouping only acts on the
-# binary traversal, so the 8-wide candidates carry 0
+# tracer settings: (bvh_width, steps, keep, aggregate, grouping)
 TRACER_GRID = (tuple((2, s, k, 0, g) for s in (32, 64, 128) for k in (8, 12, 16) for g in (2, 3))
-               + ((2, 32, 16, 0, 0), (8, 32, 16, 0, 0), (8, 64, 12, 0, 0)))
+               + ((2, 32, 16, 0, 0), (8, 32, 16, 0, 2), (8, 64, 12, 0, 2), (8, 32, 16, 0, 0)))
 STENCIL_GRID = ((32, 8), (64, 4), (128, 2), (256, 1), (64, 2), (128, 1))
 TRACER_DEFAULT = (2, 32, 16, 0, 2)
 STENCIL_DEFAULT = (128, 2)

@@ -234,3 +234,27 @@ def test_leaf_grouping_is_bit_exact(group):
         _lib.set_deterministic(0)
     np.testing.assert_array_equal(got_n, ref_n)
     np.testing.assert_array_equal(got_i, ref_i)
+
+
+def test_leaf_grouping_on_the_wide_tree_is_bit_exact():
+    """The 8-wide traversal with leaf grouping (2 and 3) equals the 8-wide traversal without it,
+    bit for bit with deterministic tallies."""
+    from petch_b200 import _lib
+    phi, geo = small_feature(False)
+    par = dict(params.PAR, periodic_y=1)
+    _lib.call("petch_tracer_config", 8, 32, 16)
+    try:
+        m = cuda_mesh(phi, geo['dx'], geo)
+        bare = np.random.default_rng(6).uniform(0.05, 1.0, m.F)
+        _lib.set_deterministic(8 * m.MT + (1 << 16))
+        _lib.call("petch_tracer_grouping", 0)
+        ref_n = cuda_neutrals(m, geo, bare, 0.7, 3, 400_000)
+        ref_i = cuda_ions(m, geo, par, 4, 400_000)
+        for group in (2, 3):
+            _lib.call("petch_tracer_grouping", group)
+            np.testing.assert_array_equal(cuda_neutrals(m, geo, bare, 0.7, 3, 400_000), ref_n)
+            np.testing.assert_array_equal(cuda_ions(m, geo, par, 4, 400_000), ref_i)
+    finally:
+        _lib.call("petch_tracer_grouping", _lib.TRACER_GROUPING_DEFAULT)
+        _lib.call("petch_tracer_config", *_lib.TRACER_DEFAULT)
+        _lib.set_deterministic(0)
