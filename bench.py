@@ -856,12 +856,13 @@ def e2e(par, flags, W, K, phi_W):
     cells = phi0.size
     return {"value": K / dt, "unit": "steps/s", "steps": K, "window": f"{W}..{W + K - 1}",
             "h2d_bytes_per_step": int(phi0.nbytes / K),
-            "d2h_bytes_per_step": int(4 * n_cols + (8 + 1) * cells / K),
+            "d2h_bytes_per_step": int(4 * n_cols + (4 + 1) * cells / K),
             "api": "petch_b200.run_etch_3d(phi_init=pinned host array, seed_offset=W, "
                    "record_depth_every=1): its fused-step engine, default tracer settings",
             "timed": "host clock around the whole call: set-up, upload of the level set entering "
                      "step W, the K steps of the window with the depth read back each step (the "
-                     "first with a cold 4-round coverage start), final phi (float64) and mask to "
+                     "first with a cold 4-round coverage start), final phi (float32 through "
+                     "pinned memory, widened to float64 on the host) and mask to "
                      f"the host; bytes per step: the upload and the final read spread over the "
                      f"K steps plus {n_cols} floor indices (int32) per step",
             "final_depth_um": float(geo['depth_history'][-1][1])}

@@ -395,6 +395,8 @@ __device__ __forceinline__ bool step_wide_node(const Tracer& T, Query& q, St& st
             nh += hit;
         }
         if (nh > 0) {
+            // children hit are visited front to back (sorted by entry distance); visiting them
+            // unsorted measured 25 % slower on the trench workload (more visits)
             if (nh > 1) {
                 cas(key[0], ch[0], key[1], ch[1]); cas(key[2], ch[2], key[3], ch[3]);
                 cas(key[4], ch[4], key[5], ch[5]); cas(key[6], ch[6], key[7], ch[7]);

@@ -893,7 +893,7 @@ def run_etch_3d(Lx=10.0, Ly=4.0, Lz=14.0, dx=0.4, trench_width=4.0, mask_th=2.0,
     ms = st_timer.totals_ms()
     for k, v in ms.items():
         timings[k] = float(np.sum(v)) / 1e3
-    geo['phi'] = eng.phi.double().cpu().numpy()
+    geo['phi'] = _to_host_f64(eng.phi)
     geo['mask'] = eng.mask.bool().cpu().numpy()
     timings['total'] = time.time() - t_wall
     geo['timings'] = timings
@@ -969,12 +969,21 @@ def _run_fused(Lx, Ly, Lz, dx, trench_width, mask_th, sub_top, t_end, n_steps, h
                   f"depth ~ {_depth3d(dict(geo, phi=plan.phi)):5.2f}  Vmax {st['vmax']:.3f}")
     plan.close()
     _, mask = seed_field(nx, ny, nz, dx, Lx, Ly, sub_top, mask_th, trench_width, hole)
-    geo['phi'] = plan.phi.double().cpu().numpy()
+    geo['phi'] = _to_host_f64(plan.phi)
     geo['mask'] = mask.bool().cpu().numpy()
     geo['timings'] = dict(flux=0.0, extend=0.0, reinit=0.0, mesh=0.0, advect=0.0, rate=0.0,
                           total=time.time() - t_wall, nsub_max=nsub_max, fused=True)
     geo['engine'] = plan
     return geo
+
+
+def _to_host_f64(t):
+    """A device float32 array as a float64 numpy array: the float32 copy goes through pinned
+    memory (half the bytes of a float64 copy, at the pinned rate) and is widened on the host."""
+    host = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+    host.copy_(t, non_blocking=True)
+    torch.cuda.current_stream().synchronize()
+    return host.double().numpy()
 
 
 # ---- depth metrics (threed.py:1798-1869) ----
