@@ -542,6 +542,17 @@ int petch_radiosity_solve(const void* mesh, int max_tris, int max_verts, const i
                           double betaE, double betaO, int n_iter, float* g_E, float* g_O,
                           double* work2, void* stream);
 
+/* petch_radiosity_solve with the three recipe tangents (no reference counterpart: the reference's
+ * solve is not differentiated): dbare float[3][max_tris] the coverage tangents; the same primal
+ * bits in g_E / g_O, and dg_E / dg_O float[3][max_tris] the tangents of the clipped G (the form
+ * factors and the sky view are geometry, held fixed; 0 where the clips hold).  n_iter >= 1;
+ * work: double[16 * max_tris] scratch. */
+int petch_radiosity_solve_tangent(const void* mesh, int max_tris, int max_verts,
+                                  const int* row_ptr, const int* col, const double* sky, int n_ff,
+                                  const float* bare, const float* dbare, double betaE,
+                                  double betaO, int n_iter, float* g_E, float* g_O, float* dg_E,
+                                  float* dg_O, double* work, void* stream);
+
 /* ---- DDA neutral transport (deterministic discrete ordinates) ----
  * Replaces dda_neutral_flux (petch/dda.py:132-188) as called by mc_flux_3d_dda
  * (petch/threed.py:1211-1244).  petch_dda_prepare marches every (face, direction) ray of

@@ -120,7 +120,8 @@ __global__ void k_ff_sky(const int* __restrict__ hdr, int MT, const int* __restr
 // (y_in == nullptr), s = clip(bare * beta, 0, 1).  The last iteration writes clip(G, 0, 8) as
 // float; the others write x_i = (1 - s_i) G_i for the next.  Lane q of a group sums entries
 // q, q + kG, q + 2 kG, ... and the group reduces with a fixed butterfly, so every run sums in the
-// same order.
+// same order; products and sums are rounded explicitly (no contraction), so the tangent kernel's
+// primal below gives the same bits.
 constexpr int kG = 8;
 
 __global__ void __launch_bounds__(kRB) k_rad_iter(const int* __restrict__ hdr, int MT,
@@ -154,8 +155,8 @@ __global__ void __launch_bounds__(kRB) k_rad_iter(const int* __restrict__ hdr, i
                 for (int e = e0 + sub; e < e1; e += kG) {
                     const int j = __ldg(col + e);
                     const double b = (double)__ldg(bare + j), dj = __ldg(D + j);
-                    sE += (1.0 - fmin(fmax(b * betaE, 0.0), 1.0)) * dj;
-                    sO += (1.0 - fmin(fmax(b * betaO, 0.0), 1.0)) * dj;
+                    sE = __dadd_rn(sE, __dmul_rn(1.0 - fmin(fmax(b * betaE, 0.0), 1.0), dj));
+                    sO = __dadd_rn(sO, __dmul_rn(1.0 - fmin(fmax(b * betaO, 0.0), 1.0), dj));
                 }
             }
         }
@@ -164,14 +165,118 @@ __global__ void __launch_bounds__(kRB) k_rad_iter(const int* __restrict__ hdr, i
             sO += __shfl_xor_sync(0xffffffffu, sO, o);
         }
         if (sub == 0 && i < F) {
-            const double GE = D[i] + inv_nff * sE, GO = D[i] + inv_nff * sO;
+            const double GE = __dadd_rn(D[i], __dmul_rn(inv_nff, sE));
+            const double GO = __dadd_rn(D[i], __dmul_rn(inv_nff, sO));
             if (gE) {
                 gE[i] = (float)fmin(fmax(GE, 0.0), 8.0);
                 gO[i] = (float)fmin(fmax(GO, 0.0), 8.0);
             } else {
                 const double b = (double)bare[i];
-                y_out[i] = make_double2((1.0 - fmin(fmax(b * betaE, 0.0), 1.0)) * GE,
-                                        (1.0 - fmin(fmax(b * betaO, 0.0), 1.0)) * GO);
+                y_out[i] = make_double2(__dmul_rn(1.0 - fmin(fmax(b * betaE, 0.0), 1.0), GE),
+                                        __dmul_rn(1.0 - fmin(fmax(b * betaO, 0.0), 1.0), GO));
+            }
+        }
+    }
+}
+
+// k_rad_iter with the three recipe tangents (direction-major dbare [3][MT]): the primal exactly
+// as k_rad_iter computes it (the same entries, lanes and butterfly, so the same bits), and
+//   dx_j = -ds_j G_j + (1 - s_j) dG_j   (first iteration: -ds_j D_j),   dG_i = sum_j dx_j / n_ff,
+// with ds = beta dbare where 0 < bare beta < 1 (the clip's derivative, 0 at its bounds); the sky
+// view D does not depend on the recipe.  The last iteration writes clip(G, 0, 8) and its tangent
+// (0 where the clip holds).  y / dy hold x and dx: [MT] and [3][MT] double2 (E, O).
+constexpr int kND = 3;
+
+__device__ __forceinline__ double clip_ds(double b, double beta, double db) {
+    const double s = b * beta;
+    return (s > 0.0 && s < 1.0) ? beta * db : 0.0;
+}
+
+__global__ void __launch_bounds__(kRB) k_rad_iter_tan(const int* __restrict__ hdr, int MT,
+                                                      const int* __restrict__ row_ptr,
+                                                      const int* __restrict__ col,
+                                                      const double* __restrict__ D,
+                                                      const float* __restrict__ bare,
+                                                      const float* __restrict__ dbare,
+                                                      double betaE, double betaO, double inv_nff,
+                                                      const double2* __restrict__ y_in,
+                                                      const double2* __restrict__ dy_in,
+                                                      double2* __restrict__ y_out,
+                                                      double2* __restrict__ dy_out,
+                                                      float* __restrict__ gE, float* __restrict__ gO,
+                                                      float* __restrict__ dgE,
+                                                      float* __restrict__ dgO) {
+    const int F = min(hdr[HDR_F], MT);
+    const int sub = threadIdx.x & (kG - 1);
+    const int groups = (gridDim.x * blockDim.x) / kG;
+    const int first = (blockIdx.x * blockDim.x + threadIdx.x) / kG;
+    const int warp_first = first - ((threadIdx.x & 31) / kG);
+    for (int base = warp_first; base < F; base += groups) {
+        const int i = base + ((threadIdx.x & 31) / kG);
+        double sE = 0.0, sO = 0.0;
+        double tE[kND] = {0.0, 0.0, 0.0}, tO[kND] = {0.0, 0.0, 0.0};
+        if (i < F) {
+            const int e0 = row_ptr[i], e1 = row_ptr[i + 1];
+            if (y_in) {
+                for (int e = e0 + sub; e < e1; e += kG) {
+                    const int j = __ldg(col + e);
+                    const double2 x = y_in[j];
+                    sE += x.x;
+                    sO += x.y;
+#pragma unroll
+                    for (int k = 0; k < kND; ++k) {
+                        const double2 dx = dy_in[(long long)k * MT + j];
+                        tE[k] += dx.x;
+                        tO[k] += dx.y;
+                    }
+                }
+            } else {
+                for (int e = e0 + sub; e < e1; e += kG) {
+                    const int j = __ldg(col + e);
+                    const double b = (double)__ldg(bare + j), dj = __ldg(D + j);
+                    sE = __dadd_rn(sE, __dmul_rn(1.0 - fmin(fmax(b * betaE, 0.0), 1.0), dj));
+                    sO = __dadd_rn(sO, __dmul_rn(1.0 - fmin(fmax(b * betaO, 0.0), 1.0), dj));
+#pragma unroll
+                    for (int k = 0; k < kND; ++k) {
+                        const double db = (double)__ldg(dbare + (long long)k * MT + j);
+                        tE[k] -= clip_ds(b, betaE, db) * dj;
+                        tO[k] -= clip_ds(b, betaO, db) * dj;
+                    }
+                }
+            }
+        }
+        for (int o = kG / 2; o > 0; o >>= 1) {
+            sE += __shfl_xor_sync(0xffffffffu, sE, o);
+            sO += __shfl_xor_sync(0xffffffffu, sO, o);
+#pragma unroll
+            for (int k = 0; k < kND; ++k) {
+                tE[k] += __shfl_xor_sync(0xffffffffu, tE[k], o);
+                tO[k] += __shfl_xor_sync(0xffffffffu, tO[k], o);
+            }
+        }
+        if (sub == 0 && i < F) {
+            const double GE = __dadd_rn(D[i], __dmul_rn(inv_nff, sE));
+            const double GO = __dadd_rn(D[i], __dmul_rn(inv_nff, sO));
+            if (gE) {
+                gE[i] = (float)fmin(fmax(GE, 0.0), 8.0);
+                gO[i] = (float)fmin(fmax(GO, 0.0), 8.0);
+#pragma unroll
+                for (int k = 0; k < kND; ++k) {
+                    dgE[(long long)k * MT + i] = (GE > 0.0 && GE < 8.0) ? (float)(inv_nff * tE[k]) : 0.0f;
+                    dgO[(long long)k * MT + i] = (GO > 0.0 && GO < 8.0) ? (float)(inv_nff * tO[k]) : 0.0f;
+                }
+            } else {
+                const double b = (double)bare[i];
+                const double cE = 1.0 - fmin(fmax(b * betaE, 0.0), 1.0);
+                const double cO = 1.0 - fmin(fmax(b * betaO, 0.0), 1.0);
+                y_out[i] = make_double2(__dmul_rn(cE, GE), __dmul_rn(cO, GO));
+#pragma unroll
+                for (int k = 0; k < kND; ++k) {
+                    const double db = (double)dbare[(long long)k * MT + i];
+                    dy_out[(long long)k * MT + i] =
+                        make_double2(cE * inv_nff * tE[k] - clip_ds(b, betaE, db) * GE,
+                                     cO * inv_nff * tO[k] - clip_ds(b, betaO, db) * GO);
+                }
             }
         }
     }
@@ -322,6 +427,41 @@ extern "C" int petch_radiosity_solve(const void* mesh, int max_tris, int max_ver
                                            last ? g_E : nullptr, last ? g_O : nullptr);
         PETCH_LAUNCH_CHECK("k_rad_iter");
         yin = yout;
+    }
+    return PETCH_OK;
+}
+
+extern "C" int petch_radiosity_solve_tangent(const void* mesh, int max_tris, int max_verts,
+                                             const int* row_ptr, const int* col,
+                                             const double* sky, int n_ff, const float* bare,
+                                             const float* dbare, double betaE, double betaO,
+                                             int n_iter, float* g_E, float* g_O, float* dg_E,
+                                             float* dg_O, double* work, void* stream) {
+    PETCH_REQUIRE(mesh && row_ptr && col && sky && bare && dbare && g_E && g_O && dg_E && dg_O &&
+                      work,
+                  "petch_radiosity_solve_tangent: null pointer");
+    PETCH_REQUIRE(max_tris > 0 && n_ff >= 1 && n_iter >= 1,
+                  "petch_radiosity_solve_tangent: bad size");
+    cudaStream_t st = as_stream(stream);
+    MeshView m = mesh_view(const_cast<void*>(mesh), max_tris, max_verts);
+    double2* ya = reinterpret_cast<double2*>(work);
+    double2* yb = ya + max_tris;
+    double2* dya = yb + max_tris;
+    double2* dyb = dya + (long long)kND * max_tris;
+    const double2 *yin = nullptr, *dyin = nullptr;
+    const int blocks = grid_for((long long)max_tris * kG, kRB);
+    for (int it = 0; it < n_iter; ++it) {
+        const bool last = it == n_iter - 1;
+        double2* yout = (it & 1) ? yb : ya;
+        double2* dyout = (it & 1) ? dyb : dya;
+        k_rad_iter_tan<<<blocks, kRB, 0, st>>>(m.hdr, max_tris, row_ptr, col, sky, bare, dbare,
+                                               betaE, betaO, 1.0 / n_ff, yin, dyin,
+                                               last ? nullptr : yout, last ? nullptr : dyout,
+                                               last ? g_E : nullptr, last ? g_O : nullptr,
+                                               last ? dg_E : nullptr, last ? dg_O : nullptr);
+        PETCH_LAUNCH_CHECK("k_rad_iter_tan");
+        yin = yout;
+        dyin = dyout;
     }
     return PETCH_OK;
 }

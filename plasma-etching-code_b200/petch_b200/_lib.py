@@ -128,6 +128,7 @@ SIGNATURES = {
     "petch_ff_scratch_bytes": [I, I, LLP],
     "petch_ff_matrix": [P, I, I, P, I, P, P, P, P, L, P],
     "petch_radiosity_solve": [P, I, I, P, P, P, I, P, D, D, I, P, P, P, P],
+    "petch_radiosity_solve_tangent": [P, I, I, P, P, P, I, P, P, D, D, I, P, P, P, P, P, P],
     "petch_radiosity_gmres_scratch_bytes": [I, I, LLP],
     "petch_radiosity_gmres": [P, I, I, P, P, P, I, P, D, D, I, I, P, P, L, P, P],
     "petch_dda_scratch_bytes": [I, I, I, I, I, LLP],

@@ -13,7 +13,10 @@ runs its primal computation unchanged and carries three tangent directions:
     which keeps the tangent an unbiased estimate of the derivative of the expected deposits);
   * normalisation / smoothing (linear), Belen coverages and surface rate (float64 duals), the
     coverage fixed point and its warm start, the velocity extension (nearest face fixed);
-  * the narrow-band advection (upwind choices fixed) and the Eikonal reinit (branches fixed).
+  * the narrow-band advection (upwind choices fixed) and the Eikonal reinit (branches fixed);
+  * on the radiosity path (neutral_transport="radiosity", Jacobi solve): the unsmoothed ion
+    yields' energy tangents and the coverage tangents through every Jacobi sweep (the form
+    factors and sky view are geometry).
 Held fixed: the surface mesh and hit topology — the fluxes' dependence on the shape of the
 surface is not differentiated (a pathwise derivative of a ray tally with respect to the surface
 would need visibility-boundary terms, which are out of scope), and the CFL substep count.
@@ -151,6 +154,56 @@ class TangentEngine(EtchEngine):
                       self.dbare.data_ptr(), s)
         self.yields = (self.y[0].data_ptr(), self.y[1].data_ptr(), self.y[2].data_ptr())
 
+    def flux_radiosity_tangent(self, phi, n_ion, seed, n_ff=64, n_fp=4, n_iter=40):
+        """mc_flux_3d_radiosity (threed.py:923-991) with tangents: the faithful ions of
+        _ions_deterministic (unsmoothed yields) with their energy tangents, the form factors and
+        the sky view as geometry (held fixed), then n_fp rounds of the two-species Jacobi solve
+        with the coverage tangents (petch_radiosity_solve_tangent) and the Belen coverage
+        update with its tangents, from bare = 1."""
+        par, m = self.par, self.mesh
+        s = _sp()
+        A_src = float(self.geo['Lx'] * self.geo['Ly'])
+        work = self.small[0:6]
+        _lib.call("petch_trace_ions_tangent", m.id, m.MT, m.MV, ctypes.byref(self.dom),
+                  ctypes.byref(self.ionp), int(seed * 9 + 1) & 0xffffffff, int(n_ion),
+                  self.tal4.data_ptr(), self.ang.data_ptr(), self.dtal.data_ptr(),
+                  work.data_ptr(), s)
+        norm = float(A_src / n_ion)
+        _lib.call("petch_ion_post", m.id, m.MT, m.MV, self.tal4.data_ptr(), self.ang.data_ptr(),
+                  norm, 0, 1.0, self.y[0].data_ptr(), self.y[1].data_ptr(), self.y[2].data_ptr(),
+                  self.m_i.data_ptr(), self.cos_i.data_ptr(), self.tmp5.data_ptr(), s)
+        for q in range(3):                     # d y_q: direction 0 only (ion energy)
+            self.dtal_in[0].copy_(self.dtal[q])
+            _lib.call("petch_norm_smooth_tangent", m.id, m.MT, m.MV, self.dtal_in.data_ptr(),
+                      self.dtal_in.data_ptr(), norm, 0.0, 0.0, 0, 0, 1.0, 1,
+                      self.dy[q].data_ptr(), self.ttmp[0].data_ptr(), self.ttmp[1].data_ptr(), s)
+        r = self._radiosity_buffers(n_ff)
+        if r.get('work_tan') is None or r['work_tan'].numel() < 16 * m.MT:
+            r['work_tan'] = torch.empty(16 * m.MT, device="cuda", dtype=torch.float64)
+        nx, ny, nz = phi.shape
+        _lib.call("petch_gas_normals", m.id, m.MT, m.MV, phi.data_ptr(), nx, ny, nz,
+                  float(self.geo['dx']), r['fn'].data_ptr(), s)
+        _lib.call("petch_trace_ff", m.id, m.MT, m.MV, ctypes.byref(self.dom), r['fn'].data_ptr(),
+                  int(seed) & 0xffffffff, int(n_ff), r['hit'].data_ptr(), work.data_ptr(), s)
+        _lib.call("petch_ff_matrix", m.id, m.MT, m.MV, r['hit'].data_ptr(), int(n_ff),
+                  r['row_ptr'].data_ptr(), r['col'].data_ptr(), r['sky'].data_ptr(),
+                  r['scratch'].data_ptr(), r['scratch'].numel(), s)
+        self.bare.fill_(1.0)
+        self.dbare.zero_()
+        betaE, betaO = float(par.get('betaE', 0.7)), float(par.get('betaO', 1.0))
+        for _ in range(n_fp):
+            _lib.call("petch_radiosity_solve_tangent", m.id, m.MT, m.MV, r['row_ptr'].data_ptr(),
+                      r['col'].data_ptr(), r['sky'].data_ptr(), int(n_ff), self.bare.data_ptr(),
+                      self.dbare.data_ptr(), betaE, betaO, int(n_iter), self.m_F.data_ptr(),
+                      self.m_O.data_ptr(), self.dm_F.data_ptr(), self.dm_O.data_ptr(),
+                      r['work_tan'].data_ptr(), s)
+            _lib.call("petch_belen_bare_tangent", m.id, m.MT, m.MV, ctypes.byref(self.chem),
+                      self.dOflux, self.m_F.data_ptr(), self.dm_F.data_ptr(), self.m_O.data_ptr(),
+                      self.dm_O.data_ptr(), self.y[1].data_ptr(), self.dy[1].data_ptr(),
+                      self.y[2].data_ptr(), self.dy[2].data_ptr(), self.bare.data_ptr(),
+                      self.dbare.data_ptr(), s)
+        self.yields = (self.y[0].data_ptr(), self.y[1].data_ptr(), self.y[2].data_ptr())
+
     def rate_extend_tangent(self, band):
         m = self.mesh
         s = _sp()
@@ -187,7 +240,7 @@ def run_etch_3d_tangent(theta, Lx, Ly, Lz, dx, trench_width, mask_th, sub_top, t
                         n_steps=20, hole=True, par=None, flags=None, n_ion=30000, n_neu=30000,
                         seed_offset=0, max_tris=None):
     """run_etch_3d (FSM reinit, nearest-face extension, coverage-coupled SF6/O2 flux with
-    faithful ions) at recipe theta, carrying d/dtheta.  Returns (phi, dphi[3], geo) as numpy
+    faithful ions; Monte-Carlo or radiosity neutrals) at recipe theta, carrying d/dtheta.  Returns (phi, dphi[3], geo) as numpy
     float64 (phi: (nx, ny, nz); dphi: (3, nx, ny, nz)) plus timings (device seconds)."""
     par = apply_theta(dict(par or PAR), theta)
     flags = flags or DEFAULT_FLAGS
@@ -195,9 +248,12 @@ def run_etch_3d_tangent(theta, Lx, Ly, Lz, dx, trench_width, mask_th, sub_top, t
             and getattr(flags, "chemistry", "langmuir") == "belen"):
         raise NotImplementedError("the recipe gradient follows the coverage-coupled SF6/O2 path "
                                   "with faithful ions (belen, ion_reflection, coverage_sticking)")
-    if getattr(flags, "neutral_transport", "mc") != "mc" or getattr(flags, "redeposition", False):
-        raise NotImplementedError("the recipe gradient follows Monte-Carlo neutrals without "
-                                  "redeposition")
+    transport = getattr(flags, "neutral_transport", "mc")
+    if transport not in ("mc", "radiosity") or getattr(flags, "redeposition", False):
+        raise NotImplementedError("the recipe gradient follows Monte-Carlo or radiosity neutrals "
+                                  "without redeposition")
+    if transport == "radiosity" and par.get('radiosity_solver', 'jacobi') == 'gmres':
+        raise NotImplementedError("the recipe gradient follows the radiosity path's Jacobi solve")
     if getattr(flags, "floor_charge_throttle", False):
         raise NotImplementedError("the recipe gradient does not include the floor-charging throttle")
     if getattr(flags, "surface_charging", False) and float(par.get('charge_alpha', 0.0)) > 0.0:
@@ -218,7 +274,10 @@ def run_etch_3d_tangent(theta, Lx, Ly, Lz, dx, trench_width, mask_th, sub_top, t
         seed = step + seed_offset
         eng.small.zero_()
         eng.build_mesh()
-        eng.flux_tangent(n_ion, n_neu, seed, warm)
+        if transport == "radiosity":
+            eng.flux_radiosity_tangent(eng.phi, n_ion, seed)
+        else:
+            eng.flux_tangent(n_ion, n_neu, seed, warm)
         eng.rate_extend_tangent(band)
         st = eng.sync_status()
         if st['mesh_err'] & (MESH_ERR_TRI_OVERFLOW | MESH_ERR_VERT_OVERFLOW | MESH_ERR_HASH_FULL):

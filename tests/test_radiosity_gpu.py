@@ -215,3 +215,49 @@ def test_radiosity_loop_depth_matches_oracle_loop(hole):
     for s in sorted(orc_hist):
         assert abs(dev_hist[s] - orc_hist[s]) <= dx + 1e-9, (s, dev_hist[s], orc_hist[s])
     assert max(orc_hist.values()) > 2 * dx
+
+
+def test_radiosity_solve_tangent_matches_finite_differences(rd):
+    """petch_radiosity_solve_tangent: its primal equals petch_radiosity_solve bit for bit, and its
+    tangents along three random coverage directions match central differences of the 40-sweep
+    solve per face (the solve is deterministic given the form-factor hits)."""
+    m, geo, phi, par, flags = device_case(rd, "hole")
+    F, n_ff, n_iter, MT = m.F, 64, 40, m.MT
+    fe = engine(m, geo, par, flags)
+    hit = torch.full((MT * n_ff,), -1, dtype=torch.int32, device="cuda")
+    hit[:F * n_ff] = torch.from_numpy(rd["hole_hit"]).cuda()
+    r = fe._radiosity_buffers(n_ff)
+    _lib.call("petch_ff_matrix", m.id, m.MT, m.MV, hit.data_ptr(), n_ff, r['row_ptr'].data_ptr(),
+              r['col'].data_ptr(), r['sky'].data_ptr(), r['scratch'].data_ptr(),
+              r['scratch'].numel(), stream())
+    rng = np.random.default_rng(3)
+    bare = torch.zeros(MT, device="cuda")
+    bare[:F] = torch.from_numpy(rng.uniform(0.2, 0.9, F).astype(np.float32)).cuda()
+    dbare = torch.zeros((3, MT), device="cuda")
+    dbare[:, :F] = torch.from_numpy(rng.normal(0.0, 1.0, (3, F)).astype(np.float32)).cuda()
+    f32 = dict(device="cuda", dtype=torch.float32)
+    gE, gO = torch.zeros(MT, **f32), torch.zeros(MT, **f32)
+    dgE, dgO = torch.zeros((3, MT), **f32), torch.zeros((3, MT), **f32)
+    work = torch.empty(16 * MT, device="cuda", dtype=torch.float64)
+
+    def solve(b):
+        _lib.call("petch_radiosity_solve", m.id, m.MT, m.MV, r['row_ptr'].data_ptr(),
+                  r['col'].data_ptr(), r['sky'].data_ptr(), n_ff, b.data_ptr(), 0.7, 1.0, n_iter,
+                  fe.m_F.data_ptr(), fe.m_O.data_ptr(), r['work2'].data_ptr(), stream())
+        return fe.m_F[:F].double().cpu().numpy(), fe.m_O[:F].double().cpu().numpy()
+
+    _lib.call("petch_radiosity_solve_tangent", m.id, m.MT, m.MV, r['row_ptr'].data_ptr(),
+              r['col'].data_ptr(), r['sky'].data_ptr(), n_ff, bare.data_ptr(), dbare.data_ptr(),
+              0.7, 1.0, n_iter, gE.data_ptr(), gO.data_ptr(), dgE.data_ptr(), dgO.data_ptr(),
+              work.data_ptr(), stream())
+    pE, pO = solve(bare)
+    np.testing.assert_array_equal(gE[:F].double().cpu().numpy(), pE)
+    np.testing.assert_array_equal(gO[:F].double().cpu().numpy(), pO)
+    h = 1e-2
+    for k in range(3):
+        ep, op = solve(bare + h * dbare[k])
+        em, om = solve(bare - h * dbare[k])
+        for fd, t in (((ep - em) / (2 * h), dgE[k, :F]), ((op - om) / (2 * h), dgO[k, :F])):
+            t = t.double().cpu().numpy()
+            scale = np.abs(fd).max()
+            assert np.abs(t - fd).max() <= 2e-3 * scale, (k, np.abs(t - fd).max(), scale)
