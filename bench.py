@@ -109,10 +109,10 @@ def rank_reduce(values, op, dist, world):
 
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one neutral-pair launch of this
 # workload, from the ncu capture summarised in profiles/k_trace_neutral_pair_trench_c1_deep.md.
-TRACE_TRAFFIC = 2247642000 + 3198055000
-TRACE_TRAFFIC_SOURCE = ("ncu --set full, the step-60 launch (301,914 faces, 38.6 MB algorithmic): "
-                        "2.248 GB read + 3.198 GB written, per launch; the traversal stacks' and "
-                        "register spills' local-memory lines overflowing L1 and L2")
+TRACE_TRAFFIC = 143980288 + 79863040
+TRACE_TRAFFIC_SOURCE = ("ncu --set full, the step-60 launch (300,504 faces, 38.5 MB algorithmic): "
+                        "144.0 MB read + 79.9 MB written, per launch (5.8x the algorithmic bytes: "
+                        "the traversal stacks' local-memory lines that leave L2)")
 
 
 def peaks():
