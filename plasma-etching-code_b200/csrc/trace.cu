@@ -25,15 +25,16 @@ constexpr int kTB = 128;
 #define PETCH_TRACE_MIN_BLOCKS_RR 9
 #endif
 #ifndef PETCH_TRACE_MIN_BLOCKS_RR_TAN
-#define PETCH_TRACE_MIN_BLOCKS_RR_TAN 10
+#define PETCH_TRACE_MIN_BLOCKS_RR_TAN 8
 #endif
 // Resident blocks of the persistent tracers per SM (the binary-traversal launches use no shared
 // memory, so registers alone set them): 8 x 4 warps (<= 64 registers per thread) for the ion
 // shaders; 9 x 4 (<= 56 registers) for the Russian-roulette neutral shaders, single-instance and
 // batched (trench workload, 100-step run with leaf grouping: 12 blocks at 40 registers spill
 // ~300 B per thread and run 4.8 % slower, 10 blocks 2.9 % slower, 8 blocks at 64 registers 0.5 %
-// slower; 64 ragged holes: 12 blocks 9 % slower, 10 blocks 1.3 % slower); 10 x 4 (<= 48
-// registers) for the neutral tangent shaders, which carry three weight tangents per ray.
+// slower; 64 ragged holes: 12 blocks 9 % slower, 10 blocks 1.3 % slower); 8 x 4 (<= 64
+// registers) for the neutral tangent shaders, which carry three weight tangents per ray (the
+// batched inverse design's device time 8 % below 10 blocks at 48 registers).
 constexpr int kTraceMinBlocks = PETCH_TRACE_MIN_BLOCKS;
 constexpr int kTraceMinBlocksRR = PETCH_TRACE_MIN_BLOCKS_RR;
 constexpr int kTraceMinBlocksRRTan = PETCH_TRACE_MIN_BLOCKS_RR_TAN;
