@@ -95,15 +95,16 @@ class StepPlan:
         _lib.call("petch_step", self.h, _sp())
         self.steps_done += 1
 
-    def capture(self):
-        """Capture the cold first step, a pair of warm steps and a single odd and a single even
-        warm step into CUDA graphs (capturing enqueues nothing: the graphs run on replay).  A
-        warm step s uses mesh buffer s % 2, so the pair graph starts on an odd step: run()
-        replays cold, pairs, and a single step when the remaining count is odd; replay_step()
-        replays one step at a time."""
+    def capture(self, pair=True):
+        """Capture the cold first step, a pair of warm steps (pair=True) and a single odd and a
+        single even warm step into CUDA graphs (capturing enqueues nothing: the graphs run on
+        replay).  A warm step s uses mesh buffer s % 2, so the pair graph starts on an odd step:
+        run() replays cold, pairs, and a single step when the remaining count is odd;
+        replay_step() replays one step at a time."""
         _lib.call("petch_prepare_device")
         graphs, self.graph_launches = {}, {}
-        for key, first, n in (("cold", 0, 1), ("warm2", 1, 2), ("warm1", 1, 1), ("warm0", 2, 1)):
+        keys = (("cold", 0, 1), ("warm2", 1, 2), ("warm1", 1, 1), ("warm0", 2, 1))
+        for key, first, n in (k for k in keys if pair or k[0] != "warm2"):
             g = torch.cuda.CUDAGraph()
             _lib.call("petch_plan_seek", self.h, first)
             n0 = _lib.launch_count()
@@ -124,7 +125,7 @@ class StepPlan:
             for _ in range(n):
                 self.step()
             return
-        if self.graphs is None:
+        if self.graphs is None or "warm2" not in self.graphs:
             self.capture()
         warm = bool(self.cfg.warm_start)
         while n > 0:
@@ -145,7 +146,7 @@ class StepPlan:
         """Advance one step by replaying its graph (cold, odd or even warm step); returns the
         library kernel launches the replayed graph holds."""
         if self.graphs is None:
-            self.capture()
+            self.capture(pair=False)
         s = self.steps_done
         key = "cold" if s == 0 or not self.cfg.warm_start else ("warm1" if s % 2 else "warm0")
         self.graphs[key].replay()

@@ -905,12 +905,16 @@ def run_etch_3d(Lx=10.0, Ly=4.0, Lz=14.0, dx=0.4, trench_width=4.0, mask_th=2.0,
     return geo
 
 
+FUSED_GRAPH_MIN_STEPS = 6
+
+
 def _run_fused(Lx, Ly, Lz, dx, trench_width, mask_th, sub_top, t_end, n_steps, hole, par, flags,
                n_ion, n_neu, verbose, record_depth_every, seed_offset, record_frames, max_tris,
                phi_init):
     """run_etch_3d on the fused step (plan.StepPlan): steps are enqueued without host work in
-    between and the plan's status is read once per chunk of steps (every step when the depth,
-    frames or progress are recorded).  A mesh that outgrows the capacity holds its step on the
+    between (from captured CUDA graphs for runs of FUSED_GRAPH_MIN_STEPS steps or more) and the
+    plan's status is read once per chunk of steps (every step when the depth, frames or progress
+    are recorded).  A mesh that outgrows the capacity holds its step on the
     device; the run then plans again from the held level set with twice the capacity (or 1.5x
     the largest mesh seen) and repeats the step, the new plan starting its coverage cold."""
     from .plan import StepPlan
@@ -926,6 +930,9 @@ def _run_fused(Lx, Ly, Lz, dx, trench_width, mask_th, sub_top, t_end, n_steps, h
               sub_top=sub_top, hole=hole, par=par, flags=flags, n_ion=n_ion, n_neu=n_neu)
     per_step = bool(record_depth_every or record_frames or verbose)
     chunk = 1 if per_step else 16
+    # runs of a few steps or more replay each step from a captured CUDA graph (one launch per
+    # step instead of ~200; the capture costs a few milliseconds once per plan)
+    use_graph = n_steps >= FUSED_GRAPH_MIN_STEPS
     done, issued, nsub_max, nonfinite = 0, 0, 0, 0
     plan = StepPlan(**kw, t_end=t_end, n_steps=n_steps, seed_offset=seed_offset, max_tris=MT,
                     phi_init=phi_init, dt=dt)
@@ -933,7 +940,10 @@ def _run_fused(Lx, Ly, Lz, dx, trench_width, mask_th, sub_top, t_end, n_steps, h
     while done < n_steps:
         k = min(chunk, n_steps - done)
         for _ in range(k):
-            plan.step()
+            if use_graph:
+                plan.replay_step()
+            else:
+                plan.step()
         st = plan.status(check=False)
         if st['status'] == 3:             # PETCH_E_OVERFLOW: the held steps are repeated
             done = base + st['steps']
