@@ -452,7 +452,10 @@ typedef struct petch_batch_grid {
 int petch_batch_advect(const petch_batch_grid* grids, int B, void* stream);
 
 /* Replaces, for B <= 64 instances with the same dx, reinit_fsm (petch/threed.py:1515-1537) as
- * petch_reinit_eik mode 0 with band = band_r, in place on each phi.  Graph-capturable. */
+ * petch_reinit_eik mode 0 with band = band_r, in place on each phi: the same values, with each
+ * sweep restricted per grid row to the z range the front's distances can have reached (the row
+ * ranges live in each instance's tmp grid, which must be 8-byte aligned; nz >= 4).
+ * Graph-capturable. */
 int petch_batch_reinit(const petch_batch_grid* grids, int B, double band_r, void* stream);
 
 /* The tangent state of one instance for the batched tangent stages (direction-major [3][n]

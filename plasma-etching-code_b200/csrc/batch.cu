@@ -106,7 +106,28 @@ __global__ void k_b_adv_finish(BTable t) {
 }
 
 // The Eikonal passes row-mapped (petch::RowShape: threadIdx.x along z, threadIdx.y a row of the
-// block's, blockIdx.x striding over the instance's nx * ny rows).
+// block's, blockIdx.x striding over the instance's nx * ny rows), each row restricted to the z
+// range the sweeps can have reached.  A cell keeps `big` until a face neighbour holds a finite
+// value, so after sweep s a row's finite cells lie within its own range of sweep s - 1 widened by
+// one cell and its four lateral neighbours' ranges; the row ranges (int2 per row: nz - kmin,
+// kmax + 1, 0 = empty, so a union is a max) ping-pong in the advection's scratch grid tmp, which
+// is free during the reinit.  Cells outside a row's range are not touched: the init writes the
+// starting field into both sweep buffers, so they hold `big`, as the dense sweep would leave them.
+__device__ __forceinline__ int2* row_ranges(const BGrid& x, int which) {
+    return reinterpret_cast<int2*>(x.tmp) + (long long)which * x.g.nx * x.g.ny;
+}
+
+__global__ void k_b_rows_clear(BTable t) {
+    const int b = blockIdx.y;
+    if (b >= t.B) return;
+    const BGrid& x = t.it[b];
+    if (held(x)) return;
+    int2* r = row_ranges(x, 0);
+    const int rows = x.g.nx * x.g.ny;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < rows; q += gridDim.x * blockDim.x)
+        r[q] = make_int2(0, 0);
+}
+
 __global__ void k_b_eik_init(BTable t, double band_r) {
     const int b = blockIdx.y;
     if (b >= t.B) return;
@@ -114,12 +135,20 @@ __global__ void k_b_eik_init(BTable t, double band_r) {
     if (held(x)) return;
     const float inv_dx = (float)(1.0 / x.dx);
     const float big = (float)(band_r + 4.0 * x.dx);
-    const int rows = x.g.nx * x.g.ny;
+    const int rows = x.g.nx * x.g.ny, nz = x.g.nz;
+    int2* r0 = row_ranges(x, 0);
     for (int row = blockIdx.x * blockDim.y + threadIdx.y; row < rows; row += gridDim.x * blockDim.y) {
         const int i = row / x.g.ny, j = row - i * x.g.ny;
-        const long long base = (long long)row * x.g.nz;
-        for (int k = threadIdx.x; k < x.g.nz; k += blockDim.x)
-            x.ua[base + k] = eik_init_cell_at<false>(x.phi, base + k, i, j, k, x.g, inv_dx, big);
+        const long long base = (long long)row * nz;
+        for (int k = threadIdx.x; k < nz; k += blockDim.x) {
+            const float v = eik_init_cell_at<false>(x.phi, base + k, i, j, k, x.g, inv_dx, big);
+            x.ua[base + k] = v;
+            x.ub[base + k] = v;
+            if (v != big) {
+                atomicMax(&r0[row].x, nz - k);
+                atomicMax(&r0[row].y, k + 1);
+            }
+        }
     }
 }
 
@@ -131,17 +160,44 @@ __global__ void k_b_eik_sweep(BTable t, double band_r, int parity) {
     if (held(x)) return;
     const float* in = parity ? x.ub : x.ua;
     float* out = parity ? x.ua : x.ub;
+    const int2* rin = row_ranges(x, parity);
+    int2* rout = row_ranges(x, parity ^ 1);
     const float dxf = (float)x.dx;
     const float big = (float)(band_r + 4.0 * x.dx), cap = (float)(band_r + x.dx);
-    const int rows = x.g.nx * x.g.ny;
+    const int nx = x.g.nx, ny = x.g.ny, nz = x.g.nz, rows = nx * ny;
     for (int row = blockIdx.x * blockDim.y + threadIdx.y; row < rows; row += gridDim.x * blockDim.y) {
-        const int i = row / x.g.ny, j = row - i * x.g.ny;
-        const long long base = (long long)row * x.g.nz;
-        for (int k = threadIdx.x; k < x.g.nz; k += blockDim.x) {
-            const float v = eik_sweep_cell_at<FINAL, false>(in, base + k, i, j, k, x.g, dxf, big,
-                                                            cap, x.phi);
-            if (FINAL) x.phi[base + k] = v;
-            else out[base + k] = v;
+        const int i = row / ny, j = row - i * ny;
+        const long long base = (long long)row * nz;
+        int2 e = rin[row];
+        if (i >= 1) { const int2 f = rin[row - ny]; e = make_int2(max(e.x, f.x), max(e.y, f.y)); }
+        if (i + 1 < nx) { const int2 f = rin[row + ny]; e = make_int2(max(e.x, f.x), max(e.y, f.y)); }
+        if (j >= 1) { const int2 f = rin[row - 1]; e = make_int2(max(e.x, f.x), max(e.y, f.y)); }
+        if (j + 1 < ny) { const int2 f = rin[row + 1]; e = make_int2(max(e.x, f.x), max(e.y, f.y)); }
+        int k0 = nz, k1 = -1;                 // this sweep's range [k0, k1], widened by one cell
+        if (e.y > 0) {
+            k0 = max(nz - e.x - 1, 0);
+            k1 = min(e.y, nz - 1);
+        }
+        if (!FINAL && threadIdx.x == 0)
+            rout[row] = e.y > 0 ? make_int2(nz - k0, k1 + 1) : make_int2(0, 0);
+        if (FINAL) {
+            // every cell gets its final value; outside the range U is `big`, so the value is
+            // sign(phi) * cap without the solve
+            for (int k = threadIdx.x; k < nz; k += blockDim.x) {
+                float v;
+                if (k >= k0 && k <= k1) {
+                    v = eik_sweep_cell_at<true, false>(in, base + k, i, j, k, x.g, dxf, big, cap,
+                                                       x.phi);
+                } else {
+                    const float sg = x.phi[base + k] < 0.0f ? -1.0f : 1.0f;
+                    v = __fadd_rn(__fmul_rn(sg, fminf(big, cap)), 0.0f);
+                }
+                x.phi[base + k] = v;
+            }
+        } else {
+            for (int k = k0 + threadIdx.x; k <= k1; k += blockDim.x)
+                out[base + k] = eik_sweep_cell_at<false, false>(in, base + k, i, j, k, x.g, dxf,
+                                                                big, cap, x.phi);
         }
     }
 }
@@ -222,6 +278,9 @@ extern "C" int petch_batch_reinit(const petch_batch_grid* grids, int B, double b
     const double dx = grids[0].dx;
     for (int b = 1; b < B; ++b)
         PETCH_REQUIRE(grids[b].dx == dx, "petch_batch_reinit: all grids need the same dx");
+    for (int b = 0; b < B; ++b)   // two row-range arrays (16 bytes per row) fit in tmp
+        PETCH_REQUIRE(grids[b].nz >= 4 && ((uintptr_t)grids[b].tmp & 7) == 0,
+                      "petch_batch_reinit: grid %d needs nz >= 4 and an 8-byte aligned tmp", b);
     const int n_iter = (int)std::ceil(band_r / dx) + 4;
     cudaStream_t st = as_stream(stream);
     long long max_rows = 0;
@@ -229,6 +288,8 @@ extern "C" int petch_batch_reinit(const petch_batch_grid* grids, int B, double b
     const RowShape rs = stencil_shape();
     const dim3 blk(rs.bz, rs.br);
     const dim3 gc(std::max(1, stencil_blocks(max_rows, rs) / std::max(1, B / 4)), B);
+    k_b_rows_clear<<<dim3(grid_for(max_rows, kBB, 2), B), kBB, 0, st>>>(t);
+    PETCH_LAUNCH_CHECK("k_b_rows_clear");
     k_b_eik_init<<<gc, blk, 0, st>>>(t, band_r);
     PETCH_LAUNCH_CHECK("k_b_eik_init");
     int parity = 0;
