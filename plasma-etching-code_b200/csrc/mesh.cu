@@ -170,8 +170,9 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* total)
 constexpr int kMcZ = 128, kMcRows = 2;
 
 __global__ void __launch_bounds__(kMcZ * kMcRows) k_mc_classify(const float* __restrict__ phi,
-                                                                Dims d,
-                                                                uint16_t* __restrict__ info_lin) {
+                                                                Dims d, Morton mo,
+                                                                uint16_t* __restrict__ info_lin,
+                                                                int* __restrict__ bflag) {
     const int rows = d.nx * d.ny;
     for (int row = blockIdx.x * kMcRows + threadIdx.y; row < rows; row += gridDim.x * kMcRows) {
         const int i = row / d.ny, j = row - (row / d.ny) * d.ny;
@@ -195,6 +196,11 @@ __global__ void __launch_bounds__(kMcZ * kMcRows) k_mc_classify(const float* __r
                 inf |= cfg | (1u << 11);
             }
             info_lin[c] = (uint16_t)inf;
+            // mark the Morton block of a node that emits a vertex or a face (the count pass
+            // skips the blocks no such node falls in)
+            const uint32_t cfg = inf & 255u;
+            if (cross || ((inf >> 11) & 1u && cfg != 0u && cfg != 255u))
+                atomicOr(bflag + (m_encode(mo, i, j, k) / kB), 1);
         }
     }
 }
@@ -202,28 +208,41 @@ __global__ void __launch_bounds__(kMcZ * kMcRows) k_mc_classify(const float* __r
 // Pass 1b, Morton order: each node's info gathered from the grid-order pass, and per block the
 // packed totals (faces, vertices, BVH leaves) the later passes offset from.
 __global__ void __launch_bounds__(kB) k_mc_count(const uint16_t* __restrict__ info_lin, Dims d,
-                                                 Morton mo, uint32_t npad,
+                                                 Morton mo, uint32_t npad, uint32_t nb,
                                                  uint16_t* __restrict__ info,
-                                                 int4* __restrict__ bsum) {
-    uint32_t t = blockIdx.x * kB + threadIdx.x;
-    uint32_t nt = 0, nv = 0, nl = 0;
-    if (t < npad) {
-        int c3[3];
-        m_decode(mo, t, c3);
-        uint32_t inf = 0;
-        if (c3[0] < d.nx && c3[1] < d.ny && c3[2] < d.nz) {
-            inf = info_lin[c3[0] * d.plane + (long long)c3[1] * d.nz + c3[2]];
-            if ((inf >> 11) & 1u) nt = c_mc.ntri[inf & 255u];
-            nv = __popc((inf >> 8) & 7u);
-            nl = nt > 0;
+                                                 int4* __restrict__ bsum,
+                                                 int* __restrict__ bflag) {
+    // each CTA walks Morton blocks (kB nodes each) with a stride of the grid: a launch of tens of
+    // thousands of mostly empty blocks would cost more in block scheduling than their work
+    for (uint32_t mb = blockIdx.x; mb < nb; mb += gridDim.x) {
+        const uint32_t t = mb * kB + threadIdx.x;
+        const bool act = bflag[mb] != 0;
+        __syncthreads();                      // every thread has read the flag
+        if (!act) {
+            // no node of this block emits anything: zero info (no cube, no crossing) and totals
+            if (t < npad) info[t] = 0;
+            if (threadIdx.x == 0) bsum[mb] = make_int4(0, 0, 0, 0);
+            continue;
         }
-        info[t] = (uint16_t)inf;
+        if (threadIdx.x == 0) bflag[mb] = 0;  // cleared for the next build
+        uint32_t nt = 0, nv = 0, nl = 0;
+        if (t < npad) {
+            int c3[3];
+            m_decode(mo, t, c3);
+            uint32_t inf = 0;
+            if (c3[0] < d.nx && c3[1] < d.ny && c3[2] < d.nz) {
+                inf = info_lin[c3[0] * d.plane + (long long)c3[1] * d.nz + c3[2]];
+                if ((inf >> 11) & 1u) nt = c_mc.ntri[inf & 255u];
+                nv = __popc((inf >> 8) & 7u);
+                nl = nt > 0;
+            }
+            info[t] = (uint16_t)inf;
+        }
+        uint32_t tot;
+        block_excl_scan(nt | (nv << 11) | (nl << 21), &tot);
+        if (threadIdx.x == 0)
+            bsum[mb] = make_int4((int)(tot & 2047u), (int)((tot >> 11) & 1023u), (int)(tot >> 21), 0);
     }
-    uint32_t tot;
-    block_excl_scan(nt | (nv << 11) | (nl << 21), &tot);
-    if (threadIdx.x == 0)
-        bsum[blockIdx.x] = make_int4((int)(tot & 2047u), (int)((tot >> 11) & 1023u),
-                                     (int)(tot >> 21), 0);
 }
 
 __global__ void k_mc_totals(const int4* bsum, const int4* boff, int nb, MeshView m) {
@@ -253,68 +272,77 @@ __global__ void k_mc_totals(const int4* bsum, const int4* boff, int nb, MeshView
 
 // Pass 2: vertices on crossed owned edges, interpolated at phi = 0 from the edge's lower node.
 __global__ void __launch_bounds__(kB) k_mc_verts(const float* __restrict__ phi, Dims d, Morton mo,
-                                                 uint32_t npad, const uint16_t* __restrict__ info,
+                                                 uint32_t npad, uint32_t nb,
+                                                 const uint16_t* __restrict__ info,
+                                                 const int4* __restrict__ bsum,
                                                  const int4* __restrict__ boff,
                                                  uint32_t* __restrict__ voff, double dx,
                                                  MeshView m) {
-    uint32_t t = blockIdx.x * kB + threadIdx.x;
-    uint32_t cross = (t < npad) ? ((info[t] >> 8) & 7u) : 0u;
-    uint32_t nv = __popc(cross), tot;
-    uint32_t ex = block_excl_scan(nv, &tot);
-    if (!nv) return;
-    uint32_t base = (uint32_t)boff[blockIdx.x].y + ex;
-    voff[t] = base;
-    int c3[3];
-    m_decode(mo, t, c3);
-    long long c = c3[0] * d.plane + (long long)c3[1] * d.nz + c3[2];
-    float va = phi[c];
-    const long long step[3] = {d.plane, (long long)d.nz, 1};
-    uint32_t r = 0;
-    for (int a = 0; a < 3; ++a) {
-        if (!((cross >> a) & 1u)) continue;
-        uint32_t v = base + r++;
-        if (v >= (uint32_t)m.MV) continue;
-        float vb = phi[c + step[a]];
-        float tt = va / (va - vb);
-        float p[3] = {(float)c3[0], (float)c3[1], (float)c3[2]};
-        p[a] = p[a] + tt;
-        for (int q = 0; q < 3; ++q) {
-            m.vnode[3 * v + q] = p[q];
-            m.verts[3 * v + q] = (float)((double)p[q] * dx);
+    for (uint32_t mb = blockIdx.x; mb < nb; mb += gridDim.x) {
+        if (bsum[mb].y == 0) continue;        // no vertex in this block
+        const uint32_t t = mb * kB + threadIdx.x;
+        const uint32_t cross = (t < npad) ? ((info[t] >> 8) & 7u) : 0u;
+        uint32_t nv = __popc(cross), tot;
+        const uint32_t ex = block_excl_scan(nv, &tot);
+        if (!nv) continue;
+        const uint32_t base = (uint32_t)boff[mb].y + ex;
+        voff[t] = base;
+        int c3[3];
+        m_decode(mo, t, c3);
+        const long long c = c3[0] * d.plane + (long long)c3[1] * d.nz + c3[2];
+        const float va = phi[c];
+        const long long step[3] = {d.plane, (long long)d.nz, 1};
+        uint32_t r = 0;
+        for (int a = 0; a < 3; ++a) {
+            if (!((cross >> a) & 1u)) continue;
+            uint32_t v = base + r++;
+            if (v >= (uint32_t)m.MV) continue;
+            float vb = phi[c + step[a]];
+            float tt = va / (va - vb);
+            float p[3] = {(float)c3[0], (float)c3[1], (float)c3[2]};
+            p[a] = p[a] + tt;
+            for (int q = 0; q < 3; ++q) {
+                m.vnode[3 * v + q] = p[q];
+                m.verts[3 * v + q] = (float)((double)p[q] * dx);
+            }
         }
     }
 }
 
 // Pass 3: faces (global vertex ids from the owner nodes' offsets) and BVH leaves.
-__global__ void __launch_bounds__(kB) k_mc_faces(Dims d, Morton mo, uint32_t npad,
+__global__ void __launch_bounds__(kB) k_mc_faces(Dims d, Morton mo, uint32_t npad, uint32_t nb,
                                                  const uint16_t* __restrict__ info,
+                                                 const int4* __restrict__ bsum,
                                                  const int4* __restrict__ boff,
                                                  const uint32_t* __restrict__ voff, MeshView m) {
-    uint32_t t = blockIdx.x * kB + threadIdx.x;
-    uint32_t inf = (t < npad) ? info[t] : 0u;
-    uint32_t cfg = inf & 255u;
-    uint32_t nt = ((inf >> 11) & 1u) ? c_mc.ntri[cfg] : 0u;
-    uint32_t tot;
-    uint32_t ex = block_excl_scan(nt | ((nt > 0) << 16), &tot);
-    if (!nt) return;
-    int f0 = boff[blockIdx.x].x + (int)(ex & 0xffffu);
-    int leaf = boff[blockIdx.x].z + (int)(ex >> 16);
-    int c3[3];
-    m_decode(mo, t, c3);
-    for (uint32_t q = 0; q < nt; ++q) {
-        int f = f0 + (int)q;
-        if (f >= m.MT) break;
-        for (int s = 0; s < 3; ++s) {
-            int e = c_mc.tri[cfg][3 * q + s];
-            int cc = mc::edge_corner(e), ax = mc::edge_axis(e);
-            uint32_t to = m_encode(mo, c3[0] + (cc & 1), c3[1] + ((cc >> 1) & 1), c3[2] + ((cc >> 2) & 1));
-            uint32_t oc = (info[to] >> 8) & 7u;
-            m.faces[3 * f + s] = (int)(voff[to] + __popc(oc & ((1u << ax) - 1u)));
+    for (uint32_t mb = blockIdx.x; mb < nb; mb += gridDim.x) {
+        if (bsum[mb].x == 0) continue;        // no face (hence no leaf) in this block
+        const uint32_t t = mb * kB + threadIdx.x;
+        const uint32_t inf = (t < npad) ? info[t] : 0u;
+        const uint32_t cfg = inf & 255u;
+        const uint32_t nt = ((inf >> 11) & 1u) ? c_mc.ntri[cfg] : 0u;
+        uint32_t tot;
+        const uint32_t ex = block_excl_scan(nt | ((nt > 0) << 16), &tot);
+        if (!nt) continue;
+        const int f0 = boff[mb].x + (int)(ex & 0xffffu);
+        const int leaf = boff[mb].z + (int)(ex >> 16);
+        int c3[3];
+        m_decode(mo, t, c3);
+        for (uint32_t q = 0; q < nt; ++q) {
+            int f = f0 + (int)q;
+            if (f >= m.MT) break;
+            for (int s = 0; s < 3; ++s) {
+                int e = c_mc.tri[cfg][3 * q + s];
+                int cc = mc::edge_corner(e), ax = mc::edge_axis(e);
+                uint32_t to = m_encode(mo, c3[0] + (cc & 1), c3[1] + ((cc >> 1) & 1), c3[2] + ((cc >> 2) & 1));
+                uint32_t oc = (info[to] >> 8) & 7u;
+                m.faces[3 * f + s] = (int)(voff[to] + __popc(oc & ((1u << ax) - 1u)));
+            }
         }
-    }
-    if (leaf < m.MT) {
-        m.leaf_code[leaf] = t;
-        m.leaf_start[leaf] = f0;
+        if (leaf < m.MT) {
+            m.leaf_code[leaf] = t;
+            m.leaf_start[leaf] = f0;
+        }
     }
 }
 
@@ -737,6 +765,7 @@ __global__ void __launch_bounds__(128) k_wide_level(MeshView m, int level) {
 
 struct Scratch {
     uint16_t* info;
+    int* bflag;      // per Morton block of kB nodes: some node emits a vertex or a face
     uint32_t* voff;
     int4* bsum;
     int4* boff;
@@ -773,6 +802,7 @@ int scratch_layout(int nx, int ny, int nz, int MT, char* base, Scratch* s, bool*
         return base ? base + at : nullptr;
     };
     s->info = (uint16_t*)take(2 * npad);
+    s->bflag = (int*)take(4 * nb);
     s->voff = (uint32_t*)take(4 * npad);
     s->bsum = (int4*)take(16 * nb);
     s->boff = (int4*)take(16 * nb);
@@ -846,19 +876,21 @@ extern "C" int petch_mesh_build(const float* phi, int nx, int ny, int nz, double
     {
         const int rows = nx * ny;
         const int gb = (rows + kMcRows - 1) / kMcRows;
-        k_mc_classify<<<gb, dim3(kMcZ, kMcRows), 0, st>>>(phi, d, info_lin);
+        k_mc_classify<<<gb, dim3(kMcZ, kMcRows), 0, st>>>(phi, d, mo, info_lin, s.bflag);
         PETCH_LAUNCH_CHECK("k_mc_classify");
     }
-    k_mc_count<<<nb, kB, 0, st>>>(info_lin, d, mo, npad, s.info, s.bsum);
+    const int pb = grid_for(nb, 1, 8);   // block-stride passes: 8 CTAs per SM at most
+    k_mc_count<<<pb, kB, 0, st>>>(info_lin, d, mo, npad, (uint32_t)nb, s.info, s.bsum, s.bflag);
     PETCH_LAUNCH_CHECK("k_mc_count");
     PETCH_CUDA(cub::DeviceScan::ExclusiveScan(s.cub_tmp, s.cub_bytes, s.bsum, s.boff, Int4Add(),
                                               make_int4(0, 0, 0, 0), nb, st),
                "cub exclusive scan");
     k_mc_totals<<<1, 1, 0, st>>>(s.bsum, s.boff, nb, m);
     PETCH_LAUNCH_CHECK("k_mc_totals");
-    k_mc_verts<<<nb, kB, 0, st>>>(phi, d, mo, npad, s.info, s.boff, s.voff, dx, m);
+    k_mc_verts<<<pb, kB, 0, st>>>(phi, d, mo, npad, (uint32_t)nb, s.info, s.bsum, s.boff, s.voff,
+                                  dx, m);
     PETCH_LAUNCH_CHECK("k_mc_verts");
-    k_mc_faces<<<nb, kB, 0, st>>>(d, mo, npad, s.info, s.boff, s.voff, m);
+    k_mc_faces<<<pb, kB, 0, st>>>(d, mo, npad, (uint32_t)nb, s.info, s.bsum, s.boff, s.voff, m);
     PETCH_LAUNCH_CHECK("k_mc_faces");
 
     FaceParams fp{dx, Lx, Ly, sub_top, mask_th, width, hole};
