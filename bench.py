@@ -536,7 +536,8 @@ def _grad_check(cfg, theta0, theta_t, seeds, h_rel, radial_profile, run):
 def differentiation_summary():
     """The recipe gradient (forward-mode tangents of every stage; mesh, hit topology and random
     decisions held fixed) with deterministic tallies.
-      cost: the tangent run's device time over the plain forward run's on the config-0 hole
+      cost: the tangent run's device time over the plain forward run's (each after one warm
+        call) on the config-0 hole
         (extent 14, dx 0.25, diameter 6, mask 2, depth 18, 30000 rays per species, the first 20
         steps of the 40-step 3.0 schedule);
       config3: dLoss/dtheta there (loss = MSE of the 32-bin radial depth profile against the
@@ -559,10 +560,12 @@ def differentiation_summary():
         theta0 = np.array([100.0, 0.1, 1.0])
         run_etch_3d_tangent(theta0, seed_offset=0, **cfg)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        fwd_kw = dict(geo_kw, t_end=1.5, n_steps=DIFF_STEPS, par=apply_theta(dict(params.PAR), theta0),
+                      flags=fl, n_ion=30000, n_neu=30000, reinit_method="fsm", verbose=False)
+        t3.run_etch_3d(**fwd_kw)          # warm: the first deterministic call allocates its tallies
+        torch.cuda.synchronize()
         e0.record()
-        t3.run_etch_3d(**geo_kw, t_end=1.5, n_steps=DIFF_STEPS,
-                       par=apply_theta(dict(params.PAR), theta0), flags=fl, n_ion=30000,
-                       n_neu=30000, reinit_method="fsm", verbose=False)
+        t3.run_etch_3d(**fwd_kw)
         e1.record()
         torch.cuda.synchronize()
         fwd = e0.elapsed_time(e1) / 1e3
