@@ -114,7 +114,8 @@ int petch_reinit_eik_noalloc(const float* phi_in, float* phi_out, int nx, int ny
  *  10 nbrw f32[3*MT] max(0, n_i.n_j) 11..15 BVH (leaf codes, leaf starts, nodes, links, flags) */
 #define PETCH_MESH_SEGMENTS 16
 
-/* Byte offsets of the segments and the total size of a mesh buffer for the given capacities. */
+/* Byte offsets of the segments and the total size of a mesh buffer for the given capacities
+ * (0 < max_tris < 2^28). */
 int petch_mesh_layout(int max_tris, int max_verts, long long* offsets, int n_offsets,
                       long long* total_bytes);
 

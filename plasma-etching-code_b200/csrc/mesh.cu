@@ -487,7 +487,8 @@ __device__ __forceinline__ int delta(const uint32_t* code, int L, int i, int j) 
 }
 
 // Karras (2012) radix-tree construction over the Morton-ordered leaves.  Child links: internal
-// node i >= 0, leaf l as ~l.  Parent links store (parent << 1) | slot.
+// node i >= 0, leaf l as ~l, each followed by its traversal ref (leaf_ref for a leaf).  Parent
+// links store (parent << 1) | slot.
 __global__ void __launch_bounds__(kB) k_bvh_internal(MeshView m) {
     const int L = min(m.hdr[HDR_L], m.MT);
     const uint32_t* code = m.leaf_code;
@@ -510,7 +511,10 @@ __global__ void __launch_bounds__(kB) k_bvh_internal(MeshView m) {
         int gamma = i + s * d + min(d, 0);
         int left = (min(i, j) == gamma) ? ~gamma : gamma;
         int right = (max(i, j) == gamma + 1) ? ~(gamma + 1) : gamma + 1;
-        m.nodes[4 * i + 3] = make_float4(__int_as_float(left), __int_as_float(right), 0.0f, 0.0f);
+        const int tl = left < 0 ? leaf_ref(m, ~left) : left;
+        const int tr = right < 0 ? leaf_ref(m, ~right) : right;
+        m.nodes[4 * i + 3] = make_float4(__int_as_float(left), __int_as_float(right),
+                                         __int_as_float(tl), __int_as_float(tr));
         if (left < 0) m.parent[m.MT + ~left] = (i << 1) | 0;
         else m.parent[left] = (i << 1) | 0;
         if (right < 0) m.parent[m.MT + ~right] = (i << 1) | 1;
@@ -604,14 +608,6 @@ __device__ __forceinline__ Box slot_box(const float4* nodes, int p, int slot) {
 __device__ __forceinline__ float box_area(const Box& b) {
     float x = b.hi[0] - b.lo[0], y = b.hi[1] - b.lo[1], z = b.hi[2] - b.lo[2];
     return x * y + y * z + z * x;
-}
-
-__device__ __forceinline__ int leaf_ref(const MeshView& m, int l) {
-    int s = m.leaf_start[l], e = m.leaf_start[l + 1];
-    int Fc = min(m.hdr[HDR_F], m.MT);
-    s = min(s, Fc);
-    e = min(e, Fc);
-    return -((s << 3) | (e - s)) - 1;
 }
 
 // Quantise `nc` child boxes into node w.
@@ -824,6 +820,7 @@ using namespace petch;
 extern "C" int petch_mesh_layout(int max_tris, int max_verts, long long* offsets, int n_offsets,
                                  long long* total_bytes) {
     PETCH_REQUIRE(max_tris > 0 && max_verts > 0, "petch_mesh_layout: capacities must be > 0");
+    PETCH_REQUIRE(max_tris < (1 << 28), "petch_mesh_layout: max_tris must be below 2^28");
     MeshLayout L = mesh_layout(max_tris, max_verts);
     if (offsets)
         for (int s = 0; s < n_offsets && s < SEG_COUNT; ++s) offsets[s] = L.off[s];
@@ -853,6 +850,7 @@ extern "C" int petch_mesh_build(const float* phi, int nx, int ny, int nz, double
     PETCH_REQUIRE(phi && mesh && scratch, "petch_mesh_build: null pointer");
     PETCH_REQUIRE(nx > 1 && ny > 1 && nz > 1 && dx > 0, "petch_mesh_build: bad grid");
     PETCH_REQUIRE(max_tris > 0 && max_verts > 0, "petch_mesh_build: capacities must be > 0");
+    PETCH_REQUIRE(max_tris < (1 << 28), "petch_mesh_build: max_tris must be below 2^28");
     Scratch s;
     bool ok = false;
     int rc = scratch_layout(nx, ny, nz, max_tris, (char*)scratch, &s, &ok);

@@ -94,6 +94,21 @@ struct MeshView {
 
 MeshView mesh_view(void* base, int max_tris, int max_verts);
 
+// Binary BVH internal node i: nodes[4i] = (lo.x, hi.x, lo.y, hi.y) of child 0, nodes[4i + 1] the
+// same of child 1, nodes[4i + 2] = (lo.z, hi.z) of child 0 then of child 1, nodes[4i + 3] = the
+// two children's links (internal node j as j, leaf l as ~l) followed by their traversal refs
+// (internal node j as j, leaf l as leaf_ref(l)).  The traversal ref of a leaf carries its face
+// range, so a resumable query reaches the faces without a lookup in leaf_start.
+
+// Traversal ref of leaf l: -(start * 8 + count) - 1 over its faces [start, start + count), clipped
+// at the published face count (the encoding of the 8-wide node's leaf children; face capacities
+// stay below 2^28).
+__device__ __forceinline__ int leaf_ref(const MeshView& m, int l) {
+    const int Fc = min(m.hdr[HDR_F], m.MT);
+    const int s = min(m.leaf_start[l], Fc), e = min(m.leaf_start[l + 1], Fc);
+    return -((s << 3) | (e - s)) - 1;
+}
+
 // Whether mesh builds add the 8-wide BVH (the tracer configuration's BVH width is 8).
 bool wide_bvh_enabled();
 

@@ -742,8 +742,9 @@ __device__ __forceinline__ void grouped_steps(const Tracer& T, Query& q, St& stk
         if (open && at_leaf == leaves) {
             bool fin = visit_bound(q, err);
             if (!fin) {
-                if (WIDE) fin = leaves ? step_wide_leaf(T, q, stk) : step_wide_node(T, q, stk, err);
-                else fin = leaves ? step_binary_leaf(T, q, stk) : step_binary_node(T, q, stk, err);
+                if (leaves) fin = step_leaf(T, q, stk);
+                else if (WIDE) fin = step_wide_node(T, q, stk, err);
+                else fin = step_binary_node(T, q, stk, err);
             }
             if (fin) phase = 2;
         }

@@ -269,7 +269,7 @@ __device__ __forceinline__ void query_begin(Query& q, const Tracer& T, float3 o,
     q.sp = 0;
     q.visits = 0;
     if (wide) q.cur = T.WN > 0 ? 0 : kDone;
-    else q.cur = T.L <= 0 ? kDone : (T.L == 1 ? ~0 : 0);
+    else q.cur = T.L <= 0 ? kDone : (T.L == 1 ? leaf_ref(T.m, 0) : 0);
 }
 
 __device__ __forceinline__ void cas(float& ka, int& va, float& kb, int& vb) {
@@ -355,6 +355,18 @@ __device__ __forceinline__ void query_leaf(const Tracer& T, Query& q, int f0, in
             q.f = f;
 }
 
+// Leaf step of either tree: q.cur = -(start * 8 + count) - 1 (leaf_ref); all the leaf's faces in
+// ascending order.  (Capping a step at 1, 2 or 3 triangles, the rest left in q.cur for the next
+// step so a warp's leaf lanes test similar counts, measured 8 %, 3.5 % and 2 % slower on the
+// trench workload: the extra steps cost more than the divergence they remove.)
+template <class St>
+__device__ __forceinline__ bool step_leaf(const Tracer& T, Query& q, St& st) {
+    const int code = -q.cur - 1;
+    const int f0 = code >> 3;
+    query_leaf(T, q, f0, f0 + (code & 7));
+    return !st.pop(q);
+}
+
 // One step of the 8-wide traversal; returns true once the query has finished.  The internal-node
 // and leaf halves are also callable on their own, as the binary traversal's (leaf grouping).
 template <class St>
@@ -425,14 +437,6 @@ __device__ __forceinline__ bool step_wide_node(const Tracer& T, Query& q, St& st
 }
 
 template <class St>
-__device__ __forceinline__ bool step_wide_leaf(const Tracer& T, Query& q, St& st) {
-    const int code = -q.cur - 1;
-    const int f0 = code >> 3;
-    query_leaf(T, q, f0, f0 + (code & 7));
-    return !st.pop(q);
-}
-
-template <class St>
 __device__ __forceinline__ bool step_wide(const Tracer& T, Query& q, St& st, int* err) {
     if (q.cur == kDone) return true;
     if (++q.visits > kMaxVisits) {
@@ -440,12 +444,13 @@ __device__ __forceinline__ bool step_wide(const Tracer& T, Query& q, St& st, int
         q.cur = kDone;
         return true;
     }
-    return q.cur >= 0 ? step_wide_node(T, q, st, err) : step_wide_leaf(T, q, st);
+    return q.cur >= 0 ? step_wide_node(T, q, st, err) : step_leaf(T, q, st);
 }
 
 // One step of the binary traversal; returns true once the query has finished.  The internal-node
 // and leaf halves are also callable on their own (a warp can run one kind of step at a time for
-// the lanes at that kind of node, see k_trace).
+// the lanes at that kind of node, see k_trace).  Children are followed by their traversal refs
+// (the node's last two words), so a leaf child's faces need no lookup.
 template <class St>
 __device__ __forceinline__ bool step_binary_node(const Tracer& T, Query& q, St& st, int* err) {
     const float4* n = T.m.nodes + 4 * q.cur;
@@ -453,7 +458,7 @@ __device__ __forceinline__ bool step_binary_node(const Tracer& T, Query& q, St& 
     float t0, t1;
     bool h0 = slab(q.r, n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, q.t, t0);
     bool h1 = slab(q.r, n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, q.t, t1);
-    int c0 = __float_as_int(n3.x), c1 = __float_as_int(n3.y);
+    int c0 = __float_as_int(n3.z), c1 = __float_as_int(n3.w);
     if (h0 && h1) {
         bool swap = t1 < t0;
         st.push(q, swap ? c0 : c1, swap ? t0 : t1, err);
@@ -464,13 +469,6 @@ __device__ __forceinline__ bool step_binary_node(const Tracer& T, Query& q, St& 
         q.cur = h0 ? c0 : c1;
         return false;
     }
-    return !st.pop(q);
-}
-
-template <class St>
-__device__ __forceinline__ bool step_binary_leaf(const Tracer& T, Query& q, St& st) {
-    const int l = ~q.cur;
-    query_leaf(T, q, __ldg(T.m.leaf_start + l), __ldg(T.m.leaf_start + l + 1));
     return !st.pop(q);
 }
 
@@ -487,7 +485,7 @@ template <class St>
 __device__ __forceinline__ bool step_binary(const Tracer& T, Query& q, St& st, int* err) {
     if (q.cur == kDone) return true;
     if (visit_bound(q, err)) return true;
-    return q.cur >= 0 ? step_binary_node(T, q, st, err) : step_binary_leaf(T, q, st);
+    return q.cur >= 0 ? step_binary_node(T, q, st, err) : step_leaf(T, q, st);
 }
 
 // Stage the top of the wide tree in shared memory (call from every thread of the block).

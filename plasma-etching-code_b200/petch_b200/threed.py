@@ -928,8 +928,17 @@ def _run_fused(Lx, Ly, Lz, dx, trench_width, mask_th, sub_top, t_end, n_steps, h
     MT = int(max_tris or default_capacity((nx, ny, nz)))
     kw = dict(Lx=Lx, Ly=Ly, Lz=Lz, dx=dx, trench_width=trench_width, mask_th=mask_th,
               sub_top=sub_top, hole=hole, par=par, flags=flags, n_ion=n_ion, n_neu=n_neu)
-    per_step = bool(record_depth_every or record_frames or verbose)
+    per_step = bool(record_frames or verbose)
     chunk = 1 if per_step else 16
+    # depths without frames or progress: each step's centre-column floors are scanned on the
+    # device right after it (into one slot per step of the chunk) and read back with the chunk's
+    # status, so recording depths adds no host synchronisation
+    floors_dev = None
+    if record_depth_every and not per_step:
+        I, J = center_columns(geo)
+        if len(I):
+            cols_dev = torch.from_numpy(np.stack([I, J], axis=1).astype(np.int32)).cuda()
+            floors_dev = torch.empty((chunk, len(I)), dtype=torch.int32, device="cuda")
     # runs of a few steps or more replay each step from a captured CUDA graph (one launch per
     # step instead of ~200; the capture costs a few milliseconds once per plan)
     use_graph = n_steps >= FUSED_GRAPH_MIN_STEPS
@@ -939,12 +948,22 @@ def _run_fused(Lx, Ly, Lz, dx, trench_width, mask_th, sub_top, t_end, n_steps, h
     base = 0                              # steps completed before the current plan
     while done < n_steps:
         k = min(chunk, n_steps - done)
-        for _ in range(k):
+        first = done
+        for i in range(k):
             if use_graph:
                 plan.replay_step()
             else:
                 plan.step()
+            if floors_dev is not None:
+                _lib.call("petch_column_floors", plan.phi.data_ptr(), nx, ny, nz,
+                          cols_dev.data_ptr(), cols_dev.shape[0], floors_dev[i].data_ptr(), _sp())
         st = plan.status(check=False)
+        if record_depth_every and not per_step and st['status'] in (0, 3):
+            fl = floors_dev[:k].cpu().numpy() if floors_dev is not None else None
+            for s_ in range(first, base + st['steps']):   # the steps that completed
+                if s_ % record_depth_every == 0 or s_ == n_steps - 1:
+                    d_now = _depth_from_floors(geo, fl[s_ - first] if fl is not None else None)
+                    geo.setdefault('depth_history', []).append((s_ + 1, d_now))
         if st['status'] == 3:             # PETCH_E_OVERFLOW: the held steps are repeated
             done = base + st['steps']
             MT = max(2 * MT, int(1.5 * st['max_faces']))
@@ -967,7 +986,8 @@ def _run_fused(Lx, Ly, Lz, dx, trench_width, mask_th, sub_top, t_end, n_steps, h
                           "this persists.", RuntimeWarning)
             nonfinite = st['nonfinite']
         step = done - 1
-        if record_depth_every and (step % record_depth_every == 0 or step == n_steps - 1):
+        if per_step and record_depth_every and (step % record_depth_every == 0
+                                                or step == n_steps - 1):
             d_now = _depth3d(dict(geo, phi=plan.phi))
             geo.setdefault('depth_history', []).append((step + 1, d_now))
             if record_frames:
@@ -1052,7 +1072,17 @@ def _depth3d(geo, half=1.0):
     """center_depth_3d: sub_top - median floor over the central columns inside the opening.
     geo['phi'] may be a host array or the engine's device level set."""
     I, J = center_columns(geo, half)
-    k = _floor_indices(geo['phi'], I, J)
+    return _depth_from_floors(geo, _floor_indices(geo['phi'], I, J))
+
+
+def _depth_from_floors(geo, k):
+    """sub_top - the median of the floors zs[k] of the columns whose top cell is gas (k >= 0);
+    0 when there are none."""
+    if k is None:
+        return 0.0
+    k = np.asarray(k, np.int64)
+    if (k == -2).any():
+        raise ValueError("depth metric: a column index lies outside the grid")
     floors = geo['zs'][k[k >= 0]]
     if floors.size == 0:
         return 0.0
