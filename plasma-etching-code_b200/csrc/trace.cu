@@ -148,6 +148,54 @@ __device__ __forceinline__ bool periodic_wrap(const Domain& D, float3& o, float3
     return false;
 }
 
+// Lateral position after the wraps of a ray that moves by `dist` along one axis from `p` in
+// [0, L]: each exit through a face re-enters 1e-4 inside the opposite one (periodic_wrap), so
+// after the first exit every full crossing covers L - 1e-4.  Adds the number of exits to `k`.
+__device__ __forceinline__ float wrap_axis(float p, float dist, float L, float& k) {
+    const float span = L - 1.0e-4f;
+    if (dist > 0.0f) {
+        const float e = p + dist - L;            // past the far face
+        if (e <= 0.0f) return p + dist;
+        const float n = floorf(e / span);
+        k += 1.0f + n;
+        return fminf(fmaxf(1.0e-4f + (e - n * span), 0.0f), L);
+    }
+    const float e = -(p + dist);                 // past the near face
+    if (e <= 0.0f) return p + dist;
+    const float n = floorf(e / span);
+    k += 1.0f + n;
+    return fminf(fmaxf(span - (e - n * span), 0.0f), L);
+}
+
+// A ray above every face (o.z > ztop, the top of the BVH root box) hits nothing until it comes
+// down to ztop.  Wrapped one miss at a time (_apply_bc), such a ray costs a query per lateral
+// crossing -- two thirds of the neutral queries in a deep trench.  This takes it there in one
+// step, through the same wraps (counted into `wraps`; the axes wrap independently, as each
+// periodic_wrap moves one coordinate), leaving o on the z = ztop plane.  Returns false when the
+// ray never comes down (d.z >= 0) or needs more wraps than the 256 a bounce may take: the
+// step-by-step wraps end such a ray too, with nothing deposited.
+__device__ __forceinline__ bool descend_wrapped(const Domain& D, float ztop, float3& o, float3 d,
+                                                int& wraps) {
+    if (!(o.z > ztop)) return true;
+    if (!(d.z < 0.0f)) return false;
+    const float t = (o.z - ztop) / -d.z;
+    float k = 0.0f;
+    float x = o.x, y = o.y;
+    if (fabsf(d.x) > 1.0e-9f) x = wrap_axis(o.x, t * d.x, D.lx, k);
+    else x = o.x + t * d.x;
+    if (fabsf(d.y) > 1.0e-9f) y = wrap_axis(o.y, t * d.y, D.ly, k);
+    else y = o.y + t * d.y;
+    if (!(k <= (float)(256 - wraps))) return false;   // also catches an infinite t
+    wraps += (int)k;
+    o = make_float3(x, y, ztop);
+    return true;
+}
+
+// Top of the mesh's BVH root box (+inf for a mesh without leaves).
+__device__ __forceinline__ float root_top(const MeshView& m, int L) {
+    return L > 0 ? __int_as_float(__ldg(m.hdr + HDR_ROOTBOX + 5)) : 3.0e38f;
+}
+
 }  // namespace
 }  // namespace petch
 
@@ -788,9 +836,14 @@ __global__ void __launch_bounds__(kTB, S::kMinBlocks) k_trace(MeshView m, Domain
             sh.init(g, T, D, ray, o, d, rs);
             rs.bounce = 0;
             rs.wraps = 0;
-            query_begin(q, T, o, d, 1.0e6f, WIDE);
-            ++n_query;
-            phase = q.cur == kDone ? 2 : 1;   // an empty mesh: the query is over at once
+            if (D.periodic && !descend_wrapped(D, root_top(T.m, T.L), o, d, rs.wraps)) {
+                ray = -1;                     // never reaches the surface
+                phase = 0;
+            } else {
+                query_begin(q, T, o, d, 1.0e6f, WIDE);
+                ++n_query;
+                phase = q.cur == kDone ? 2 : 1;   // an empty mesh: the query is over at once
+            }
         }
         if (__all_sync(kFull, ray == -2)) break;
         // Traverse while more than `keep` lanes still have an open query (at most `steps` steps),
@@ -814,7 +867,10 @@ __global__ void __launch_bounds__(kTB, S::kMinBlocks) k_trace(MeshView m, Domain
             bool cont;
             if (q.f < 0) {
                 cont = D.periodic && rs.wraps < 256 && periodic_wrap(D, o, d);
-                if (cont) ++rs.wraps;
+                if (cont) {
+                    ++rs.wraps;
+                    cont = descend_wrapped(D, root_top(T.m, T.L), o, d, rs.wraps);
+                }
             } else {
                 cont = sh.hit(g, T, q.f, q.t, o, d, rs);
                 rs.wraps = 0;
@@ -1007,9 +1063,14 @@ k_trace_batch(BatchTable tab, MeshOffsets L, int MT, int MV, float beta, float b
             rs.bounce = 0;
             rs.wraps = 0;
             rs.id = ray;
-            query_begin(q, T, o, d, 1.0e6f, false);
-            ++n_query;
-            phase = q.cur == kDone ? 2 : 1;
+            if (it.D.periodic && !descend_wrapped(it.D, root_top(T.m, T.L), o, d, rs.wraps)) {
+                ray = -1;                     // never reaches the surface
+                phase = 0;
+            } else {
+                query_begin(q, T, o, d, 1.0e6f, false);
+                ++n_query;
+                phase = q.cur == kDone ? 2 : 1;
+            }
         }
         if (__all_sync(kFull, ray == -2)) break;
         pool_empty = pool_empty || __any_sync(kFull, ray == -2);
@@ -1029,7 +1090,10 @@ k_trace_batch(BatchTable tab, MeshOffsets L, int MT, int MV, float beta, float b
             bool cont;
             if (q.f < 0) {
                 cont = it.D.periodic && rs.wraps < 256 && periodic_wrap(it.D, o, d);
-                if (cont) ++rs.wraps;
+                if (cont) {
+                    ++rs.wraps;
+                    cont = descend_wrapped(it.D, root_top(T.m, T.L), o, d, rs.wraps);
+                }
             } else {
                 if (KIND == 0)
                     cont = ion_hit(it.P, reinterpret_cast<float4*>(it.out), it.ang, g, T, q.f, q.t,

@@ -34,7 +34,7 @@ import torch
 from . import _lib
 
 # tracer settings: (bvh_width, steps, keep, aggregate, grouping)
-TRACER_GRID = (tuple((2, s, k, 0, g) for s in (32, 64, 128) for k in (12, 16, 20) for g in (2, 3))
+TRACER_GRID = (tuple((2, s, k, 0, g) for s in (32, 64, 128) for k in (8, 12, 16) for g in (2, 3))
                + ((2, 32, 16, 0, 0), (8, 32, 16, 0, 2), (8, 64, 12, 0, 2), (8, 32, 16, 0, 0)))
 STENCIL_GRID = ((32, 8), (64, 4), (128, 2), (256, 1), (64, 2), (128, 1))
 TRACER_DEFAULT = (2, 32, 16, 0, 2)
