@@ -139,7 +139,9 @@ int petch_mesh_build(const float* phi, int nx, int ny, int nz, double dx, double
 typedef struct petch_domain {
     float lx, ly, lz;   /* source plane extent and open top (Lx, Ly, Lz) */
     float z_src;        /* source plane height, Lz - dx */
-    int periodic;       /* 1: periodic x/y wrap for rays that miss (par['periodic_y']) */
+    int periodic;       /* 1: periodic x/y wrap for rays that miss (par['periodic_y']); a ray
+                           above the surface takes its wraps down to the mesh's top in one step
+                           (the same re-entry points, wrap count and 256-wrap limit) */
 } petch_domain;
 
 typedef struct petch_ion_params {  /* the float32 arguments of _trace3d_ion_yield */
