@@ -136,13 +136,19 @@ class Tuner:
     def _search(self, trial, grid, reps, top, twin=None):
         """Coarse pass (every config, `reps` timings at half the trial size), then a fine pass on
         the `top` fastest -- and on twin(c) of the two fastest, when given: a setting the coarse
-        grid leaves at one value -- with three times the timings at the full trial size.  Returns
-        ({config: ms} of the coarse pass, {config: ms} of the fine pass, which decides)."""
+        grid leaves at one value -- with three times the timings at the full trial size, then a
+        duel of the fine pass's two fastest (alternating, six times the timings), whose times
+        replace theirs.  Settings a few per cent apart can swap places between passes of a few
+        timings; the duel settles the choice between the two that matter.  Returns ({config: ms}
+        of the coarse pass, {config: ms} of the fine pass and the duel, which decides)."""
         coarse = self._time({c: trial(c, 1) for c in grid}, reps)
         best = sorted(coarse, key=coarse.get)[:max(1, top)]
         if twin is not None:
             best += [t for t in (twin(c) for c in best[:2]) if t is not None and t not in best]
         fine = self._time({c: trial(c, 2) for c in best}, 3 * reps)
+        pair = sorted(fine, key=fine.get)[:2]
+        if len(pair) == 2:
+            fine.update(self._time({c: trial(c, 2) for c in pair}, 6 * reps))
         return coarse, fine
 
     def tracer_trials(self, eng, grid=None, reps=None, exhaustive=False):
