@@ -744,7 +744,10 @@ def run_b200(args):
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
     par, flags = sf6o2()
     W, K = args.warmup, min(args.steps, N_STEPS - args.warmup)
-    tuner = None if args.no_tune else tuning_pass(par, flags)
+    if args.tracer:
+        from petch_b200.tune import apply_tracer
+        apply_tracer(tuple(int(v) for v in args.tracer.split(",")))
+    tuner = None if (args.no_tune or args.tracer) else tuning_pass(par, flags)
     r = timed_run(par, flags, W, K, world, rank, local, dist, tuner=tuner, keep_state=True)
     geo, kms, info, rays, work_q = r['geo'], r['kms'], r['info'], r['rays'], r['work_q']
     total_s = r['total_s']
@@ -963,6 +966,8 @@ def main():
     ap.add_argument("--no-transports", action="store_true")
     ap.add_argument("--no-inverse", action="store_true")
     ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--tracer", default=None,
+                    help="fixed tracer settings bvh_width,steps,keep,aggregated,grouping (no tuning)")
     ap.add_argument("--no-fused", action="store_true")
     ap.add_argument("--inverse-iters", type=int, default=3)
     args = ap.parse_args()
