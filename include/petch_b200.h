@@ -843,6 +843,11 @@ int petch_plan_timing(petch_plan_t* plan, int on);
 /* Milliseconds between those two events of the last step issued (waits for its end event). */
 int petch_plan_trace_ms(petch_plan_t* plan, float* ms);
 
+/* The plan's mask (make_trench_3d's mask, petch/threed.py:50-55: 1 for the cells of the
+ * un-etched mask the loop pins, uint8 per cell in phi's layout) copied into host memory of
+ * nx * ny * nz bytes, on `stream`; waits for the copy. */
+int petch_plan_mask(petch_plan_t* plan, unsigned char* host_mask, void* stream);
+
 /* Frees the plan's workspace (after the work on its streams has finished). */
 int petch_destroy(petch_plan_t* plan);
 

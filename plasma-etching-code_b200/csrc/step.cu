@@ -16,12 +16,44 @@
 // a plan's steps equal run_etch_3d's bit for bit with deterministic tallies.
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include "common.cuh"
 #include "mesh.cuh"
 
 namespace petch {
 namespace {
+
+// Plan workspaces come from a memory pool of the library's own, one per device, that keeps up to
+// kPoolKeep bytes of freed workspace for the next plan: a caller that plans once per run (as
+// run_etch_3d does) then pays cudaMalloc's and cudaFree's device-wide synchronisation once, not
+// per run.  Freed memory above the threshold goes back to the driver at the next
+// synchronisation.
+constexpr unsigned long long kPoolKeep = 8ULL << 30;
+
+int plan_pool(cudaMemPool_t* out) {
+    static std::mutex mu;
+    static cudaMemPool_t pools[64] = {};
+    int dev = 0;
+    PETCH_CUDA(cudaGetDevice(&dev), "petch_plan: cudaGetDevice");
+    PETCH_REQUIRE(dev >= 0 && dev < 64, "petch_plan: device ordinal %d out of range", dev);
+    std::lock_guard<std::mutex> lock(mu);
+    if (!pools[dev]) {
+        cudaMemPoolProps props;
+        std::memset(&props, 0, sizeof(props));
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t pool = nullptr;
+        PETCH_CUDA(cudaMemPoolCreate(&pool, &props), "petch_plan: cudaMemPoolCreate");
+        unsigned long long keep = kPoolKeep;
+        PETCH_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep),
+                   "petch_plan: pool release threshold");
+        pools[dev] = pool;
+    }
+    *out = pools[dev];
+    return PETCH_OK;
+}
 
 // Device words of a plan (int32): [0..5] the tracers' work words (ray counter, error bits,
 // uint64 queries, uint64 visits), [6..7] surface-rate stats (non-finite count, max V bits),
@@ -215,14 +247,22 @@ extern "C" int petch_plan(const petch_step_config* cfg, float* phi, int seed_fie
         return rc;
     }
     const long long bytes = carve(p, nullptr);
-    cudaError_t e = cudaMalloc(&p->arena, (size_t)bytes);
+    cudaMemPool_t pool = nullptr;
+    rc = plan_pool(&pool);
+    if (rc) {
+        delete p;
+        return rc;
+    }
+    cudaError_t e = cudaMallocFromPoolAsync(&p->arena, (size_t)bytes, pool, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);   // usable from any stream from here on
     if (e != cudaSuccess) {
         delete p;
         return cuda_fail(e, "petch_plan: workspace allocation");
     }
     carve(p, (char*)p->arena);
     auto fail = [&](int code) {
-        cudaFree(p->arena);
+        cudaStreamSynchronize(st);
+        cudaFreeAsync(p->arena, st);
         delete p;
         return code;
     };
@@ -397,10 +437,23 @@ extern "C" int petch_plan_trace_ms(petch_plan_s* p, float* ms) {
     return PETCH_OK;
 }
 
+extern "C" int petch_plan_mask(petch_plan_s* p, unsigned char* host_mask, void* stream) {
+    PETCH_REQUIRE(p && host_mask, "petch_plan_mask: null pointer");
+    cudaStream_t st = as_stream(stream);
+    PETCH_CUDA(cudaMemcpyAsync(host_mask, p->mask, (size_t)p->ncell, cudaMemcpyDeviceToHost, st),
+               "petch_plan_mask: copy");
+    PETCH_CUDA(cudaStreamSynchronize(st), "petch_plan_mask: sync");
+    return PETCH_OK;
+}
+
 extern "C" int petch_destroy(petch_plan_s* p) {
     if (!p) return PETCH_OK;
     petch_plan_timing(p, 0);
-    cudaError_t e = cudaFree(p->arena);
+    // as cudaFree would: no work of the plan may still be running when its workspace returns to
+    // the pool (work on any stream, hence the device-wide wait)
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaFreeAsync(p->arena, 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
     delete p;
     if (e != cudaSuccess) return cuda_fail(e, "petch_destroy");
     return PETCH_OK;

@@ -179,6 +179,7 @@ SIGNATURES = {
     "petch_plan_seek": [P, L],
     "petch_plan_timing": [P, I],
     "petch_plan_trace_ms": [P, ctypes.POINTER(ctypes.c_float)],
+    "petch_plan_mask": [P, P, P],
     "petch_destroy": [P],
 }
 

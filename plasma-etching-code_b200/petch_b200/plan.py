@@ -88,6 +88,8 @@ class StepPlan:
         self.h = h
         self.steps_done = 0
         self.graphs = None
+        self.graph_launches = {}
+        self._cap_stream = None
 
     def step(self):
         """Enqueue one step on the current stream."""
@@ -95,28 +97,46 @@ class StepPlan:
         _lib.call("petch_step", self.h, _sp())
         self.steps_done += 1
 
+    # graph key -> (the step it is captured at, steps it holds)
+    _GRAPH_STEPS = {"cold": (0, 1), "warm2": (1, 2), "warm1": (1, 1), "warm0": (2, 1)}
+
+    def _capture_graph(self, key):
+        """Capture one graph on a side stream.  Capturing is host work only and waits for
+        nothing, so it overlaps the steps the device is still running."""
+        first, n = self._GRAPH_STEPS[key]
+        if self._cap_stream is None:
+            _lib.call("petch_prepare_device")
+            self._cap_stream = torch.cuda.Stream()
+        g = torch.cuda.CUDAGraph()
+        _lib.call("petch_plan_seek", self.h, first)
+        n0 = _lib.launch_count()
+        try:
+            with torch.cuda.stream(self._cap_stream):
+                g.capture_begin()
+                try:
+                    for _ in range(n):
+                        _lib.call("petch_step", self.h, _sp())
+                finally:
+                    g.capture_end()
+        finally:
+            _lib.call("petch_plan_seek", self.h, self.steps_done)
+        if self.graphs is None:
+            self.graphs = {}
+        self.graphs[key] = g
+        self.graph_launches[key] = _lib.launch_count() - n0
+        return g
+
     def capture(self, pair=True):
         """Capture the cold first step, a pair of warm steps (pair=True) and a single odd and a
         single even warm step into CUDA graphs (capturing enqueues nothing: the graphs run on
         replay).  A warm step s uses mesh buffer s % 2, so the pair graph starts on an odd step:
         run() replays cold, pairs, and a single step when the remaining count is odd;
         replay_step() replays one step at a time."""
-        _lib.call("petch_prepare_device")
-        graphs, self.graph_launches = {}, {}
-        keys = (("cold", 0, 1), ("warm2", 1, 2), ("warm1", 1, 1), ("warm0", 2, 1))
-        for key, first, n in (k for k in keys if pair or k[0] != "warm2"):
-            g = torch.cuda.CUDAGraph()
-            _lib.call("petch_plan_seek", self.h, first)
-            n0 = _lib.launch_count()
-            with torch.cuda.graph(g):
-                for _ in range(n):
-                    _lib.call("petch_step", self.h, _sp())
-            self.graph_launches[key] = _lib.launch_count() - n0
-            graphs[key] = g
-        _lib.call("petch_plan_seek", self.h, self.steps_done)
-        self.graphs = graphs
-        torch.cuda.synchronize()
-        return graphs
+        self.graphs, self.graph_launches = {}, {}
+        for key in ("cold", "warm2", "warm1", "warm0"):
+            if pair or key != "warm2":
+                self._capture_graph(key)
+        return self.graphs
 
     def run(self, n=None, use_graph=True):
         """Advance n steps (default: the rest of the schedule) by graph replays, or eagerly."""
@@ -144,14 +164,26 @@ class StepPlan:
 
     def replay_step(self):
         """Advance one step by replaying its graph (cold, odd or even warm step); returns the
-        library kernel launches the replayed graph holds."""
-        if self.graphs is None:
-            self.capture(pair=False)
+        library kernel launches it holds.  Without captured graphs the plan's first step runs
+        eagerly, and each graph is captured at its first use, while the device still runs the
+        steps before it (a run that replays step by step then never waits for a capture)."""
         s = self.steps_done
+        if self.graphs is None and s == 0:
+            self.graphs = {}
+            n0 = _lib.launch_count()
+            self.step()
+            return _lib.launch_count() - n0
         key = "cold" if s == 0 or not self.cfg.warm_start else ("warm1" if s % 2 else "warm0")
-        self.graphs[key].replay()
+        g = (self.graphs or {}).get(key) or self._capture_graph(key)
+        g.replay()
         self.steps_done += 1
         return self.graph_launches[key]
+
+    def mask_host(self):
+        """The plan's mask (the pinned, un-etched mask cells) as a host bool array."""
+        out = np.empty(self.shape, dtype=np.uint8)
+        _lib.call("petch_plan_mask", self.h, out.ctypes.data, _sp())
+        return out.view(np.bool_)
 
     def timing(self, on=True):
         """Record CUDA events around each step's neutral-pair trace launches (enable before

@@ -186,3 +186,22 @@ def test_fused_run_regrows_capacity():
     assert [s for s, _ in a['depth_history']] == list(range(1, 7))
     for (s, da), (_, db) in zip(a['depth_history'], b['depth_history']):
         assert abs(da - db) <= HOLE['dx'] + 1e-9, (s, da, db)
+
+
+@pytest.mark.parametrize("g", [HOLE, TRENCH], ids=["hole", "trench"])
+def test_plan_mask_equals_the_seed_mask(g):
+    """petch_plan_mask hands back the mask the plan pinned (make_trench_3d's), the one
+    run_etch_3d's fused engine returns as geo['mask']."""
+    from petch_b200.levelset import seed_field
+    plan = StepPlan(**g, t_end=0.2, n_steps=2, par=_par(g['hole']), flags=SF6O2, n_ion=1000,
+                    n_neu=1000)
+    try:
+        got = plan.mask_host()
+    finally:
+        plan.close()
+    nx, ny, nz = grid_shape(g['Lx'], g['Ly'], g['Lz'], g['dx'])
+    _, mask = seed_field(nx, ny, nz, g['dx'], g['Lx'], g['Ly'], g['sub_top'], g['mask_th'],
+                         g['trench_width'], g['hole'])
+    want = mask.bool().cpu().numpy()
+    assert got.dtype == np.bool_ and got.shape == want.shape and want.any()
+    np.testing.assert_array_equal(got, want)
