@@ -806,7 +806,9 @@ typedef struct petch_step_status {
  * geometry (make_trench_3d, threed.py:32-59), and with seed_field = 1 writes the seed field into
  * phi (the CSG field redistanced over 24 cells, zero nodes frozen); with seed_field = 0 phi keeps
  * the caller's level set.  phi (float[nx*ny*nz], device) stays caller-owned and is advanced in
- * place by petch_step.  Synchronises `stream` once (the mask cell count). */
+ * place by petch_step.  Synchronises `stream` (the workspace allocation, the mask cell count).
+ * The workspace comes from a memory pool of the library's own per device that keeps up to 8 GB
+ * of freed workspace for the next plan. */
 int petch_plan(const petch_step_config* cfg, float* phi, int seed_field, petch_plan_t** plan,
                void* stream);
 
@@ -848,7 +850,8 @@ int petch_plan_trace_ms(petch_plan_t* plan, float* ms);
  * nx * ny * nz bytes, on `stream`; waits for the copy. */
 int petch_plan_mask(petch_plan_t* plan, unsigned char* host_mask, void* stream);
 
-/* Frees the plan's workspace (after the work on its streams has finished). */
+/* Returns the plan's workspace to the library's pool, after waiting for the device (work of the
+ * plan on any stream has finished when it returns). */
 int petch_destroy(petch_plan_t* plan);
 
 #ifdef __cplusplus
