@@ -22,21 +22,26 @@ constexpr int kTB = 128;
 #define PETCH_TRACE_MIN_BLOCKS 8
 #endif
 #ifndef PETCH_TRACE_MIN_BLOCKS_RR
-#define PETCH_TRACE_MIN_BLOCKS_RR 9
+#define PETCH_TRACE_MIN_BLOCKS_RR 8
+#endif
+#ifndef PETCH_TRACE_MIN_BLOCKS_RR_BATCH
+#define PETCH_TRACE_MIN_BLOCKS_RR_BATCH 9
 #endif
 #ifndef PETCH_TRACE_MIN_BLOCKS_RR_TAN
 #define PETCH_TRACE_MIN_BLOCKS_RR_TAN 8
 #endif
 // Resident blocks of the persistent tracers per SM (the binary-traversal launches use no shared
 // memory, so registers alone set them): 8 x 4 warps (<= 64 registers per thread) for the ion
-// shaders; 9 x 4 (<= 56 registers) for the Russian-roulette neutral shaders, single-instance and
-// batched (trench workload, 100-step run with leaf grouping: 12 blocks at 40 registers spill
-// ~300 B per thread and run 4.8 % slower, 10 blocks 2.9 % slower, 8 blocks at 64 registers 0.5 %
-// slower; 64 ragged holes: 12 blocks 9 % slower, 10 blocks 1.3 % slower); 8 x 4 (<= 64
-// registers) for the neutral tangent shaders, which carry three weight tangents per ray (the
-// batched inverse design's device time 8 % below 10 blocks at 48 registers).
+// shaders; 8 x 4 (<= 64 registers, no spills) for the single-instance Russian-roulette neutral
+// shaders (trench workload, 100-step run: 1.1 % faster than 9 blocks at 56 registers, which
+// spill ~90 B per thread, and than 10 blocks at 48; 12 blocks at 40 registers spill ~300 B and
+// ran 4.8 % slower); 9 x 4 (<= 56 registers) for the batched neutral kinds (64 ragged holes: 12
+// blocks 9 % slower, 10 blocks 1.3 % slower); 8 x 4 (<= 64 registers) for the neutral tangent
+// shaders, which carry three weight tangents per ray (the batched inverse design's device time
+// 8 % below 10 blocks at 48 registers).
 constexpr int kTraceMinBlocks = PETCH_TRACE_MIN_BLOCKS;
 constexpr int kTraceMinBlocksRR = PETCH_TRACE_MIN_BLOCKS_RR;
+constexpr int kTraceMinBlocksRRBatch = PETCH_TRACE_MIN_BLOCKS_RR_BATCH;
 constexpr int kTraceMinBlocksRRTan = PETCH_TRACE_MIN_BLOCKS_RR_TAN;
 constexpr long long kMaxRounds = 1LL << 24;   // per-warp bound on tracer rounds (error bit 4)
 constexpr unsigned kFull = 0xffffffffu;
@@ -1005,7 +1010,7 @@ __global__ void k_zero_batch(BatchTable tab, MeshOffsets L, int MT, int MV, int 
 // stream of ray r of its own kind-1 launch; 5 the same with the weight tangents of kind 3 (the
 // second species' into dout2).
 template <int KIND>
-__global__ void __launch_bounds__(kTB, (KIND == 1 || KIND == 4) ? kTraceMinBlocksRR
+__global__ void __launch_bounds__(kTB, (KIND == 1 || KIND == 4) ? kTraceMinBlocksRRBatch
                                     : ((KIND == 3 || KIND == 5) ? kTraceMinBlocksRRTan
                                                                 : kTraceMinBlocks))
 k_trace_batch(BatchTable tab, MeshOffsets L, int MT, int MV, float beta, float beta2,
