@@ -109,9 +109,9 @@ def rank_reduce(values, op, dist, world):
 
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one neutral-pair launch of this
 # workload, from the ncu capture summarised in profiles/k_trace_neutral_pair_trench_c1_deep.md.
-TRACE_TRAFFIC = 99855360 + 98135808
-TRACE_TRAFFIC_SOURCE = ("ncu --set full, the step-60 launch (299,886 faces, 38.4 MB algorithmic): "
-                        "99.9 MB read + 98.1 MB written, per launch (5.2x the algorithmic bytes: "
+TRACE_TRAFFIC = 48977664 + 11716352
+TRACE_TRAFFIC_SOURCE = ("ncu --set full, the step-60 launch (301,482 faces, 38.6 MB algorithmic): "
+                        "49.0 MB read + 11.7 MB written, per launch (1.57x the algorithmic bytes: "
                         "the traversal stacks' local-memory lines that leave L2)")
 
 
