@@ -36,9 +36,9 @@ constexpr int kTB = 128;
 // shaders (trench workload, 100-step run: 1.1 % faster than 9 blocks at 56 registers, which
 // spill ~90 B per thread, and than 10 blocks at 48; 12 blocks at 40 registers spill ~300 B and
 // ran 4.8 % slower); 9 x 4 (<= 56 registers) for the batched neutral kinds (64 ragged holes: 12
-// blocks 9 % slower, 10 blocks 1.3 % slower, 8 blocks 2 % slower); 8 x 4 (<= 64 registers) for the neutral tangent
-// shaders, which carry three weight tangents per ray (the batched inverse design's device time
-// 8 % below 10 blocks at 48 registers).
+// blocks 9 % slower, 10 blocks 1.3 % slower, 8 blocks 2 % slower); 8 x 4 (<= 64 registers) for
+// the neutral tangent shaders, which carry three weight tangents per ray (the batched inverse
+// design's device time 8 % below 10 blocks at 48 registers).
 constexpr int kTraceMinBlocks = PETCH_TRACE_MIN_BLOCKS;
 constexpr int kTraceMinBlocksRR = PETCH_TRACE_MIN_BLOCKS_RR;
 constexpr int kTraceMinBlocksRRBatch = PETCH_TRACE_MIN_BLOCKS_RR_BATCH;
