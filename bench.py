@@ -108,7 +108,7 @@ def rank_reduce(values, op, dist, world):
 
 
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one neutral-pair launch of this
-# workload, from the ncu capture summarised in profiles/k_trace_neutral_pair_trench_c1_deep.md.
+# workload, from one `ncu --set full` capture of the deep-step (step 60) launch.
 TRACE_TRAFFIC = 48977664 + 11716352
 TRACE_TRAFFIC_SOURCE = ("ncu --set full, the step-60 launch (301,482 faces, 38.6 MB algorithmic): "
                         "49.0 MB read + 11.7 MB written, per launch (1.57x the algorithmic bytes: "
