@@ -18,6 +18,7 @@
 #include <cstring>
 #include <mutex>
 #include <new>
+#include <nvtx3/nvToolsExt.h>
 #include "common.cuh"
 #include "mesh.cuh"
 
@@ -216,6 +217,26 @@ petch_batch_grid grid_of(const petch_plan_s* p) {
         if (_rc) return _rc;     \
     } while (0)
 
+// NVTX ranges of petch_step: one over the step and one per stage (next() closes the previous
+// stage's), all closed on every exit path.  They mark the host calls that enqueue the work (a
+// profiler's timeline shows them beside the kernels launched); a captured graph's replays make
+// no host calls and carry none.
+struct NvtxStages {
+    bool open = false;
+    NvtxStages() { nvtxRangePushA("petch_step"); }
+    void next(const char* name) {
+        if (open) nvtxRangePop();
+        nvtxRangePushA(name);
+        open = true;
+    }
+    ~NvtxStages() {
+        if (open) nvtxRangePop();
+        nvtxRangePop();
+    }
+    NvtxStages(const NvtxStages&) = delete;
+    NvtxStages& operator=(const NvtxStages&) = delete;
+};
+
 }  // namespace
 
 extern "C" int petch_plan(const petch_step_config* cfg, float* phi, int seed_field,
@@ -310,12 +331,15 @@ extern "C" int petch_step(petch_plan_s* p, void* stream) {
     const bool cold = p->steps_done == 0 || !c.warm_start;
     const int cur = p->cur, prev = 1 - cur;
     int* w = p->words;
+    NvtxStages stage;
     PETCH_CUDA(cudaMemsetAsync(w, 0, 4 * kPerStepWords, st), "petch_step: step words");
     // mesh: marching cubes, geometry, adjacency, BVH
+    stage.next("mesh");
     PETCH_TRY(petch_mesh_build(p->phi, c.nx, c.ny, c.nz, c.dx, c.Lx, c.Ly, c.sub_top, c.mask_th,
                                c.trench_width, c.hole, p->mesh[cur], MT, MV, p->mesh_scratch,
                                p->mesh_scratch_bytes, stream));
     // coverage: warm start from the previous mesh, or cold at 1
+    stage.next("flux");
     if (!cold) {
         PETCH_TRY(petch_warmstart(p->mesh[prev], MT, MV, p->bare[prev], p->mesh[cur], MT, MV,
                                   p->bare[cur], w + W_WORK, stream));
@@ -357,6 +381,7 @@ extern "C" int petch_step(petch_plan_s* p, void* stream) {
                                    p->cos_i, y_ie, y_ip, p->bare[cur], stream));
     }
     // surface rate, then the velocity into the band (mask cells folded to -1, band list)
+    stage.next("rate + extend");
     PETCH_TRY(petch_surface_rate(p->mesh[cur], MT, MV, &c.chem, p->m_i, p->m_F, p->m_O, p->cos_i,
                                  y_sp, y_ie, y_ip, p->V, w + W_STATS, stream));
     PETCH_TRY(petch_extend_velocity(p->mesh[cur], MT, MV, p->phi, p->mask, c.nx, c.ny, c.nz, c.dx,
@@ -364,6 +389,7 @@ extern "C" int petch_step(petch_plan_s* p, void* stream) {
                                     (int)p->ncell, w + W_WORK, stream));
     // CFL substeps on the device, narrow-band advection, Eikonal reinit (band 4dx + 2dx); all
     // skipped when the mesh overflowed
+    stage.next("advect + reinit");
     k_hold<<<1, 32, 0, st>>>(w, reinterpret_cast<const int*>(p->mesh[cur]));
     PETCH_LAUNCH_CHECK("k_hold");
     const petch_batch_grid g = grid_of(p);

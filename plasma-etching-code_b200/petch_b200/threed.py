@@ -40,7 +40,9 @@ def _sp():
 
 class EventTimer:
     """CUDA-event intervals on the current stream, grouped by name; read once at the end of a run
-    (no per-interval synchronisation)."""
+    (no per-interval synchronisation).  Each interval is also an NVTX range of the same name (a
+    start / end range, so intervals of different names may overlap), for a profiler's
+    timeline."""
 
     def __init__(self):
         self.open = {}
@@ -53,12 +55,14 @@ class EventTimer:
     def start(self, name):
         e = self._ev()
         e.record()
-        self.open[name] = e
+        self.open[name] = (e, torch.cuda.nvtx.range_start(name))
 
     def stop(self, name):
         e = self._ev()
         e.record()
-        self.pairs.setdefault(name, []).append((self.open.pop(name), e))
+        e0, rid = self.open.pop(name)
+        torch.cuda.nvtx.range_end(rid)
+        self.pairs.setdefault(name, []).append((e0, e))
 
     def totals_ms(self):
         torch.cuda.current_stream().synchronize()
