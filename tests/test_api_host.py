@@ -56,3 +56,28 @@ def test_plot_writes_png(tmp_path):
     ax = res.plot(path=p)
     assert os.path.getsize(p) > 1000
     assert "centre depth" in ax.get_title()
+
+
+def test_depth_from_floors_matches_the_host_scan():
+    """The fused engine's recorded depths come from device floor indices read back per chunk;
+    turning indices into a depth is the host scan's last step (sub_top - median floor of the
+    columns whose top cell is gas), checked here against center_depth_3d on a host level set."""
+    from petch_b200 import threed as t3
+    nx, ny, nz, dx = 12, 10, 40, 0.25
+    geo = dict(xs=np.arange(nx) * dx, ys=np.arange(ny) * dx, zs=np.arange(nz) * dx, dx=dx,
+               Lx=nx * dx, Ly=ny * dx, sub_top=6.0, trench_width=1.5, hole=True)
+    rng = np.random.default_rng(3)
+    floor = rng.integers(5, 30, (nx, ny))
+    phi = np.ones((nx, ny, nz))
+    for i in range(nx):
+        for j in range(ny):
+            phi[i, j, floor[i, j]:] = -1.0                 # gas from the floor to the top
+    I, J = t3.center_columns(geo)
+    k = t3._floor_indices(phi, I, J)
+    assert t3._depth_from_floors(geo, k) == t3.center_depth_3d(dict(geo, phi=phi))
+    assert t3._depth_from_floors(geo, k) == pytest.approx(
+        geo['sub_top'] - np.median(geo['zs'][floor[I, J]]))
+    assert t3._depth_from_floors(geo, None) == 0.0        # no centre columns
+    assert t3._depth_from_floors(geo, np.full(4, -1)) == 0.0   # no column open to the top
+    with pytest.raises(ValueError):
+        t3._depth_from_floors(geo, np.array([3, -2]))     # a column outside the grid
